@@ -1,0 +1,319 @@
+"""Benchmark: SIMPLE outer iterations/s (+ assembled elements/s) on the
+128^3 skewed lid-driven cavity (2.1M hex8, interior nodes displaced by
+U(-0.2h, 0.2h), Gaussian initial velocity sigma 0.1, seeded), mixed FP32/FP64
+form against the plain FP64 GPU form.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+A step is one SIMPLE outer iteration (momentum assembly + solve, mass-flow
+update, pressure-correction assembly + solve to rtol 1e-8, corrections,
+gradients). Inputs are generated on the host, uploaded once, and the timed
+region runs with every field resident in HBM (working set > L2, so no flush).
+With N > 1 (torchrun) every rank runs an independent replica: the path has no
+exchange step at this size ("replicas only").
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+HBM_FALLBACK = 6650.0
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return HBM_FALLBACK, "fallback"
+
+
+def traffic_from_profile(name):
+    """Per-launch DRAM bytes recorded from an ncu capture in profiles/ (or None)."""
+    p = os.path.join(ROOT, "profiles", name)
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        if line.strip().startswith("traffic_bytes_per_launch:"):
+            try:
+                return float(line.split(":", 1)[1].split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+class ClockSampler:
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index=0):
+        self.index = index
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.FIELDS,
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
+                self.samples.append([v.strip() for v in out.stdout.strip().split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        self._t.join(timeout=10)
+
+    def summary(self):
+        sm, smax, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for s in self.samples:
+            try:
+                sm.append(float(s[0]))
+                smax = max(smax, float(s[1]))
+                for n, v in zip(names, s[3:7]):
+                    if v.lower().startswith("active"):
+                        reasons.add(n)
+            except (ValueError, IndexError):
+                continue
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax or None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def workload(n):
+    from openaccel_b200 import meshgen
+
+    m = meshgen.cavity(n, perturb=0.2, seed=12345)
+    U0 = meshgen.initial_velocity(m, sigma=0.1, seed=12345)
+    return m, U0
+
+
+def algorithmic_bytes_momentum(nn, ne, nnz, mixed):
+    """SURVEY-defined algorithmic bytes of one momentum assembly: nodal inputs
+    13 doubles (x3, U3, mu, rho, V, grad p3, div) = 104 B/node; element inputs
+    32 B connectivity + 96 B mDot; outputs 3x3 blocks + rhs + DU."""
+    val = 4 if mixed else 8
+    return 104 * nn + 128 * ne + 9 * val * nnz + 3 * val * nn + 24 * nn
+
+
+def run_ours(args, rank, world):
+    import torch
+
+    from openaccel_b200 import runtime as rt
+
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
+    torch.cuda.set_device(dev)
+    m, U0 = workload(args.n)
+    gm = rt.Mesh(m)
+
+    def make(prec):
+        f = rt.Flow(gm, rt.default_settings(precision=prec, pc_rtol=args.pc_rtol, mom_rtol=args.mom_rtol))
+        f.set_field("U", U0)
+        f.initialize()
+        return f
+
+    def timed(f, steps, warmup):
+        stream = torch.cuda.ExternalStream(f.stream_handle(), device=dev)
+        stats = []
+        for _ in range(warmup):
+            stats += f.simple_iterate(1)
+        f.sync()
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        l0 = rt.launch_count()
+        e0.record(stream)
+        for _ in range(steps):
+            stats += f.simple_iterate(1)
+        e1.record(stream)
+        e1.synchronize()
+        launches = rt.launch_count() - l0
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        if world > 1:
+            t = torch.tensor([ms], device=dev)
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms, stats, launches
+
+    # mixed form: headline
+    fm = make(rt.OA_PREC_MIXED)
+    with ClockSampler(dev.index) as clk:
+        ms_mixed, st_mixed, launches = timed(fm, args.steps, args.warmup)
+    # FP64 form: same workload, same steps
+    f64 = make(rt.OA_PREC_FP64)
+    ms_64, st_64, _ = timed(f64, args.steps, args.warmup)
+
+    # kernel timing for the roofline and elements/s (CUDA events on the flow stream)
+    t_mom = fm.time_kernel("momentum", reps=5)
+    t_pc = fm.time_kernel("pcorr", reps=5)
+    t_mom64 = f64.time_kernel("momentum", reps=5)
+    t_pc64 = f64.time_kernel("pcorr", reps=5)
+
+    # e2e: public API with pinned host buffers, copies inside the timed region
+    fe = make(rt.OA_PREC_MIXED)
+    Uh = torch.empty(3 * m.nn, dtype=torch.float64, pin_memory=True)
+    ph = torch.empty(m.nn, dtype=torch.float64, pin_memory=True)
+    Uh.copy_(torch.from_numpy(U0.ravel()))
+    ph.zero_()
+    import ctypes as C
+
+    L = rt.lib()
+    dp = C.POINTER(C.c_double)
+
+    def e2e_step():
+        rt._check(L.oa_flow_set_field(fe.h, b"U", C.cast(Uh.data_ptr(), dp), Uh.numel()))
+        rt._check(L.oa_flow_set_field(fe.h, b"p", C.cast(ph.data_ptr(), dp), ph.numel()))
+        fe.simple_iterate(1)
+        rt._check(L.oa_flow_get_field(fe.h, b"U", C.cast(Uh.data_ptr(), dp), Uh.numel()))
+        rt._check(L.oa_flow_get_field(fe.h, b"p", C.cast(ph.data_ptr(), dp), ph.numel()))
+
+    for _ in range(args.warmup):
+        e2e_step()
+    stream_e = torch.cuda.ExternalStream(fe.stream_handle(), device=dev)
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream_e)
+    for _ in range(args.steps):
+        e2e_step()
+    e1.record(stream_e)
+    e1.synchronize()
+    ms_e2e = e0.elapsed_time(e1)
+    if world > 1:
+        t = torch.tensor([ms_e2e], device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms_e2e = float(t.item())
+
+    peak, peak_kind = measured_peaks()
+    alg = algorithmic_bytes_momentum(m.nn, m.ne, gm.nnz, True)
+    achieved = alg / (t_mom * 1e-3) / 1e9
+    traffic = traffic_from_profile("momentum_assembly_mixed_128.md")
+    value = world * args.steps / (ms_mixed * 1e-3)
+    value64 = world * args.steps / (ms_64 * 1e-3)
+    res = {
+        "metric": "SIMPLE outer iters/s (mixed FP32/FP64 form; FP64 form and assembled elems/s beside it)",
+        "value": value,
+        "unit": "outer_iters/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms_mixed / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32+f64",
+        "data": "synthetic",
+        "config": {"workload": f"lid-driven cavity {args.n}^3 hex8 skewed +-20%, Re=100, U0~N(0,0.1)",
+                   "elements": m.ne, "nodes": m.nn, "nnz": gm.nnz, "pc_rtol": args.pc_rtol,
+                   "mom_rtol": args.mom_rtol, "l2": "inputs larger than L2 (no flush)",
+                   "parallelism": f"replicas x{world}"},
+        "fp64_outer_iters_per_s": value64,
+        "mixed_over_fp64": value / value64,
+        "assembled_elems_per_s": {"mixed": 2 * m.ne / ((t_mom + t_pc) * 1e-3),
+                                  "fp64": 2 * m.ne / ((t_mom64 + t_pc64) * 1e-3)},
+        "kernel_ms": {"momentum_mixed": t_mom, "pcorr_mixed": t_pc, "momentum_fp64": t_mom64,
+                      "pcorr_fp64": t_pc64},
+        "continuity_rms_last": {"mixed": st_mixed[-1]["continuity_rms"], "fp64": st_64[-1]["continuity_rms"]},
+        "pc_iters_last": {"mixed": st_mixed[-1]["pc_iters"], "fp64": st_64[-1]["pc_iters"]},
+        "roofline": {"bound": "hbm", "kernel": "k_momentum (mixed)", "achieved": achieved, "peak": peak,
+                     "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
+                     "algorithmic_bytes": alg, "traffic": traffic},
+        "e2e": {"value": world * args.steps / (ms_e2e * 1e-3), "unit": "outer_iters/s",
+                "h2d_bytes_per_step": 32 * m.nn, "d2h_bytes_per_step": 32 * m.nn},
+        "gpu_launches": launches,
+        "clocks": clk.summary(),
+    }
+    return res
+
+
+def cpu_sample(args, threads):
+    """Oracle (CPU FP64 restatement) on the same workload: one SIMPLE outer
+    iteration with all host threads."""
+    from oracle import pyoracle as po
+
+    po.set_threads(threads)
+    m, U0 = workload(args.cpu_n)
+    c = po.FlowCase(m, po.default_settings(pc_rtol=args.pc_rtol, mom_rtol=args.mom_rtol, pc_maxit=20000,
+                                           mom_maxit=1000), U0=U0)
+    c.initialize()
+    t0 = time.perf_counter()
+    c.simple_iteration()
+    dt = time.perf_counter() - t0
+    return dt, m
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=128)
+    ap.add_argument("--cpu-n", type=int, default=128)
+    ap.add_argument("--pc-rtol", type=float, default=1e-8)
+    ap.add_argument("--mom-rtol", type=float, default=1e-6)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    threads = os.cpu_count() or 1
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        dt, m = cpu_sample(args, threads)
+        v = 1.0 / dt
+        print(json.dumps({
+            "impl": "reference",
+            "metric": "SIMPLE outer iters/s (mixed FP32/FP64 form; FP64 form and assembled elems/s beside it)",
+            "value": v, "unit": "outer_iters/s", "higher_is_better": True, "n_gpus": world,
+            "steps": 1, "warmup": 0, "ms_per_step": dt * 1e3, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"lid-driven cavity {args.cpu_n}^3 hex8 skewed +-20%, Re=100, U0~N(0,0.1)"},
+            "cpu_baseline": {"value": v, "unit": "outer_iters/s", "cores": threads, "kind": "port",
+                             "sample": f"1 SIMPLE outer iteration of the {args.cpu_n}^3 workload "
+                                       "(oracle restatement; the reference binary cannot be built)"},
+            "e2e": {"value": v, "unit": "outer_iters/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        }))
+        return
+
+    if world > 1:
+        import torch
+
+        torch.distributed.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    res = run_ours(args, rank, world)
+    if rank == 0 and not args.no_cpu:
+        dt, m = cpu_sample(args, threads)
+        res["cpu_baseline"] = {"value": 1.0 / dt, "unit": "outer_iters/s", "cores": threads, "kind": "port",
+                               "sample": f"1 SIMPLE outer iteration of the {args.cpu_n}^3 workload, FP64 oracle "
+                                         "restatement, all host threads"}
+    if rank == 0:
+        print(json.dumps(res))
+    if world > 1:
+        import torch
+
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,147 @@
+/* openaccel_b200 — C-ABI of the B200 (sm_100a) CVFEM assembly and SIMPLE
+ * pressure-correction engine.
+ *
+ * The entry points replace OpenAccel's element assembly, CSR scatter and
+ * pressure-correction linear solve behind the reference's assembler /
+ * linear-system API. Each declaration names the reference interface it stands
+ * in for (paths relative to the reference project root). Plain pointers and
+ * sizes only; every function returns an oa_status (0 = success) and leaves a
+ * message for oa_last_error() on failure, mirroring errorMsg()
+ * (src/basic/macros.cpp:21-24), which throws std::runtime_error.
+ *
+ * Threading: a handle is not re-entrant; each flow handle owns one CUDA stream
+ * and all its work is ordered on it.
+ */
+#ifndef OPENACCEL_B200_H
+#define OPENACCEL_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum oa_status {
+  OA_OK = 0,
+  OA_ERR_ARG = 1,         /* invalid argument or size */
+  OA_ERR_MESH = 2,        /* unsupported or invalid mesh (orientation, topology) */
+  OA_ERR_GEOMETRY = 3,    /* non-positive Jacobian / volume */
+  OA_ERR_CUDA = 4,        /* CUDA runtime error */
+  OA_ERR_SOLVER = 5,      /* Krylov breakdown, stagnation or non-finite residual */
+  OA_ERR_NOT_READY = 6    /* call out of sequence */
+} oa_status;
+
+enum { OA_TOPO_HEX8 = 8, OA_TOPO_TET4 = 4 };
+enum { OA_PREC_FP64 = 0, OA_PREC_MIXED = 1 };
+
+typedef struct oa_mesh oa_mesh;
+typedef struct oa_flow oa_flow;
+
+/* Settings of the steady laminar segregated-flow solve. Field meanings follow
+ * the reference controls (src/controls/controls.h:60-245) and the cavity example
+ * (examples/cavity/input.i). */
+typedef struct oa_flow_settings {
+  double rho, mu;               /* density, dynamic viscosity */
+  double urf_u, urf_p;          /* velocity / pressure relaxation factors */
+  double dt;                    /* physical timescale (false transient) */
+  double grad_urf;              /* gradient under-relaxation (nodeField.h:152) */
+  double mdot_urf;              /* mass-flow relaxation (relaxMass_) */
+  double wall_rhs_relax;        /* wall-node rhs relaxation (navierStokesAssembler.cpp:237) */
+  int u_shifted, u_grad_shifted, p_shifted, p_grad_shifted; /* linear_linear interpolation */
+  int ref_node;                 /* pressure-level node, -1 for none */
+  int mom_maxit;
+  double mom_rtol;
+  int pc_maxit;
+  double pc_rtol;
+  int precision;                /* OA_PREC_FP64 or OA_PREC_MIXED */
+} oa_flow_settings;
+
+typedef struct oa_iter_stats {
+  int mom_iters, pc_iters, pc_refinements;
+  double mom_res, pc_res;
+  double continuity_rms;        /* RMS of the pressure-correction rhs before the solve */
+} oa_iter_stats;
+
+/* Last error message of the calling thread ("" when none). */
+const char* oa_last_error(void);
+/* Library version string. */
+const char* oa_version(void);
+
+/* Mesh set-up: replaces the STK mesh + mesh::updateDualNodalVolumeField_ /
+ * updateExposedAreaVectorField_ (src/mesh/meshGeometry.cpp:1277-1527) and the
+ * reduced-stencil CSR graph of nodeGraph::buildGraph_
+ * (src/mesh/graph/nodeGraph.cpp:29-469). coords[nn][3], conn[ne][8] (Nalu hex8
+ * ordering), boundary faces as (element, face ordinal, boundary index). */
+int oa_mesh_create(const double* coords, int nn, const int* conn, int ne, int topo,
+                   const int* face_elem, const int* face_ord, const int* face_bnd, int nf,
+                   oa_mesh** out);
+void oa_mesh_destroy(oa_mesh* m);
+/* CSR graph of the mesh (columns sorted ascending): nnz, then row_ptr[nn+1],
+ * cols[nnz]. Mirrors the CRSNodeGraph consumed by Matrix::rowCols(). */
+int oa_mesh_nnz(const oa_mesh* m, int* nnz);
+int oa_mesh_graph(const oa_mesh* m, int* row_ptr, int* cols);
+/* Dual nodal volumes (host copy), mesh::updateDualNodalVolumeField_. */
+int oa_mesh_dual_volume(const oa_mesh* m, double* vol);
+
+/* Flow state: replaces the fieldBroker/flowModel fields U, p, mDot, du, grad U,
+ * grad p, div (src/realm/fieldBroker.cpp) for one domain of no-slip walls.
+ * bnd_velocity[nbnd][3] are the wall velocities by boundary index. */
+int oa_flow_create(oa_mesh* m, const oa_flow_settings* s, const double* bnd_velocity, int nbnd,
+                   oa_flow** out);
+void oa_flow_destroy(oa_flow* f);
+/* Host <-> device copies of a named field: "U" [nn][3], "p" [nn], "gradU"
+ * [nn][9], "gradP" [nn][3], "du" [nn][3], "div" [nn], "mDot" [ne][12],
+ * "sideU" [nn][3]. n is the number of doubles. */
+int oa_flow_set_field(oa_flow* f, const char* name, const double* host, long n);
+int oa_flow_get_field(oa_flow* f, const char* name, double* host, long n);
+/* Device pointer of a named field (for callers that keep data resident). */
+int oa_flow_field_device_ptr(oa_flow* f, const char* name, double** dev);
+
+/* navierStokesEquation::initialize / postInitialize and
+ * pressureCorrectionEquation::initialize
+ * (src/equation/flow/navierStokes/navierStokesEquation.cpp:86-133,
+ *  src/equation/flow/pressureCorrection/pressureCorrectionEquation.cpp:60-71):
+ * velocity and pressure gradients, initial mass flow, divergence. */
+int oa_flow_initialize(oa_flow* f);
+
+/* Momentum assembly: navierStokesAssembler::assemble + computeDUCoefficients
+ * (src/assemble/flow/segregatedFlow/navierStokesAssembler/navierStokesAssembler.cpp:84-239,
+ *  ...ElemTerms.cpp:15-441, ...NodeTerms.cpp:16-149,
+ *  ...ElemBoundaryConditions.cpp:2659-2981). The system stays on the device;
+ * when A (BSR 3x3, [nnz][9]) / b ([nn][3]) are non-null FP64 host copies are
+ * written (the Context getAMatrix()/getBVector() dump). */
+int oa_assemble_momentum(oa_flow* f, double* A, double* b);
+/* Pressure-correction assembly: pressureCorrectionAssembler::assemble +
+ * adjustMatrixForPressureReference
+ * (src/assemble/flow/segregatedFlow/pressureCorrectionAssembler/pressureCorrectionAssemblerElemTerms.cpp:17-616,
+ *  pressureCorrectionAssembler.cpp:19-63). Optional FP64 host copies of A [nnz], b [nn]. */
+int oa_assemble_pcorr(oa_flow* f, double* A, double* b);
+/* flowModel::updateMassFlowRateInterior_ (src/model/flow/flowModel.cpp:5272-5687). */
+int oa_update_mdot(oa_flow* f);
+/* flowModel::updateMassDivergenceField_ (flowModel.cpp:13541-14948, interior). */
+int oa_update_div(oa_flow* f);
+/* nodeField::updateGradientField (src/field/nodeField/nodeField.hpp:3253-4948);
+ * which = 0: pressure, 1: velocity. */
+int oa_update_gradient(oa_flow* f, int which);
+/* Linear solve of the last assembled system: linearSystem::solve()
+ * (src/equation/linearSystem.h:416-462). sys = 0 momentum (x [nn][3]), 1
+ * pressure correction (x [nn]); x may be NULL (result kept on the device). */
+int oa_solve(oa_flow* f, int sys, double rtol, int maxit, double* x, int* iters, double* res);
+/* n SIMPLE outer iterations: segregatedFlowEquations::solve
+ * (src/equation/flow/segregatedFlowEquations.cpp:76-297). stats may be NULL. */
+int oa_simple_iterate(oa_flow* f, int n, oa_iter_stats* stats);
+/* Wait for the flow's stream. */
+int oa_flow_sync(oa_flow* f);
+
+/* Measurement hooks (no counterpart in the reference, which has no device):
+ * the cudaStream_t all of the flow's work is ordered on (so callers can time
+ * it with CUDA events), the number of kernels this library has launched so
+ * far, and the mean device time of `reps` back-to-back launches of one
+ * assembly kernel (which = 0 momentum, 1 pressure correction, 2 mass flow,
+ * 3 velocity gradient) timed with CUDA events on the flow's stream. */
+int oa_flow_stream(oa_flow* f, void** stream);
+int oa_launch_count(long long* count);
+int oa_time_kernel(oa_flow* f, int which, int reps, double* ms_per_launch);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

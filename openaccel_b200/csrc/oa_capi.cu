@@ -1,0 +1,616 @@
+// C-ABI of the B200 CVFEM engine: mesh and flow handles, assembly entry
+// points, Krylov solves and the SIMPLE outer iteration driver.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "oa_internal.h"
+#include "oa_krylov.h"
+
+namespace oa {
+
+static thread_local std::string g_last_error;
+static std::atomic<long long> g_launches{0};
+void count_launches(long long n) { g_launches += n; }
+void set_error(const std::string& msg) { g_last_error = msg; }
+int fail(int code, const std::string& msg) {
+  g_last_error = msg;
+  return code;
+}
+
+__global__ void k_axpy(int n, double* y, const double* x, double a) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) y[i] += a * x[i];
+}
+template <class T>
+__global__ void k_to_double(size_t n, const T* a, double* b) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) b[i] = double(a[i]);
+}
+template <class T>
+__global__ void k_from_double(size_t n, const double* a, T* b) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) b[i] = T(a[i]);
+}
+__global__ void k_sumsq(int n, const double* v, double* out) {
+  // single block ordered reduction (used once per outer iteration)
+  __shared__ double sh[256];
+  double s = 0.0;
+  for (int i = threadIdx.x; i < n; i += 256) s += v[i] * v[i];
+  sh[threadIdx.x] = s;
+  __syncthreads();
+  for (int st = 128; st > 0; st >>= 1) {
+    if (threadIdx.x < st) sh[threadIdx.x] += sh[threadIdx.x + st];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *out = sh[0];
+}
+
+}  // namespace oa
+
+using namespace oa;
+
+struct oa_mesh {
+  DeviceMesh m;
+  cudaStream_t st = nullptr;
+};
+
+struct oa_flow {
+  Flow f;
+  KrylovSolver<1, double, double> pc64;
+  KrylovSolver<3, double, double> mom64;
+  KrylovSolver<1, float, float> pc32;
+  KrylovSolver<3, float, float> mom32;
+  double* ir_r = nullptr;   // FP64 residual for refinement
+  double* ir_x = nullptr;   // FP64 accumulated solution
+  float* ir_r32 = nullptr;
+  double* scal = nullptr;   // [4] device scalars
+  double* hscal = nullptr;  // pinned
+};
+
+namespace {
+
+template <class T>
+int dalloc(T** p, size_t n) {
+  cudaError_t e = cudaMalloc(p, sizeof(T) * (n ? n : 1));
+  if (e != cudaSuccess) return fail(OA_ERR_CUDA, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+  return OA_OK;
+}
+
+bool mixed(const Flow& f) { return f.s.precision == OA_PREC_MIXED; }
+
+int check_err_flag(Flow& f, const char* what) {
+  int h = 0;
+  OA_CUDA(cudaMemcpyAsync(&h, f.err_dev, sizeof(int), cudaMemcpyDeviceToHost, f.stream));
+  OA_CUDA(cudaStreamSynchronize(f.stream));
+  if (h) {
+    OA_CUDA(cudaMemsetAsync(f.err_dev, 0, sizeof(int), f.stream));
+    OA_CUDA(cudaStreamSynchronize(f.stream));
+    return fail(OA_ERR_GEOMETRY, std::string(what) + ": singular Jacobian (det <= 1e6*realmin)");
+  }
+  return OA_OK;
+}
+
+int copy_out_matrix(Flow& f, const void* dev, size_t n, double* host) {
+  if (!host) return OA_OK;
+  if (mixed(f)) {
+    double* tmp = nullptr;
+    if (int s = dalloc(&tmp, n)) return s;
+    k_to_double<float><<<(unsigned)((n + 255) / 256), 256, 0, f.stream>>>(n, static_cast<const float*>(dev), tmp);
+    OA_CUDA(cudaMemcpyAsync(host, tmp, sizeof(double) * n, cudaMemcpyDeviceToHost, f.stream));
+    OA_CUDA(cudaStreamSynchronize(f.stream));
+    cudaFree(tmp);
+  } else {
+    OA_CUDA(cudaMemcpyAsync(host, dev, sizeof(double) * n, cudaMemcpyDeviceToHost, f.stream));
+    OA_CUDA(cudaStreamSynchronize(f.stream));
+  }
+  return OA_OK;
+}
+
+double* field_ptr(Flow& f, const std::string& n, size_t* len) {
+  const size_t nn = f.mesh->nn, ne = f.mesh->ne;
+  if (n == "U") { *len = 3 * nn; return f.U; }
+  if (n == "p") { *len = nn; return f.p; }
+  if (n == "gradU") { *len = 9 * nn; return f.gradU; }
+  if (n == "gradP") { *len = 3 * nn; return f.gradP; }
+  if (n == "du") { *len = 3 * nn; return f.du; }
+  if (n == "div") { *len = nn; return f.div; }
+  if (n == "mDot") { *len = 12 * ne; return f.mDot; }
+  if (n == "sideU") { *len = 3 * nn; return f.sideU; }
+  if (n == "rho") { *len = nn; return f.rho; }
+  if (n == "mu") { *len = nn; return f.mu; }
+  *len = 0;
+  return nullptr;
+}
+
+// Momentum solve: BiCGStab with 3x3 block Jacobi; U += x (correctField_ with
+// relaxation 1, navierStokesEquation.cpp:186-201).
+int solve_momentum(oa_flow* h, double rtol, int maxit, int* iters, double* res, bool apply) {
+  Flow& f = h->f;
+  DeviceMesh& m = *f.mesh;
+  if (mixed(f)) {
+    if (int s = h->mom32.setup(m.nn, m.row_ptr, m.cols, m.diag, f.stream)) return s;
+    float* x = nullptr;
+    if (int s = h->mom32.solve<float>(static_cast<const float*>(f.b.A_mom), static_cast<const float*>(f.b.b_mom), x,
+                                      rtol, maxit, iters, res, 10))
+      return s;
+    k_to_double<float><<<(3 * m.nn + 255) / 256, 256, 0, f.stream>>>(3 * (size_t)m.nn, x, f.b.x_mom);
+    count_launches(1);
+  } else {
+    if (int s = h->mom64.setup(m.nn, m.row_ptr, m.cols, m.diag, f.stream)) return s;
+    double* x = nullptr;
+    if (int s = h->mom64.solve<double>(static_cast<const double*>(f.b.A_mom),
+                                       static_cast<const double*>(f.b.b_mom), x, rtol, maxit, iters, res, 10))
+      return s;
+    OA_CUDA(cudaMemcpyAsync(f.b.x_mom, x, sizeof(double) * 3 * m.nn, cudaMemcpyDeviceToDevice, f.stream));
+  }
+  if (apply) k_axpy<<<(3 * m.nn + 255) / 256, 256, 0, f.stream>>>(3 * m.nn, f.U, f.b.x_mom, 1.0);
+  count_launches(1);
+  OA_CUDA(cudaGetLastError());
+  return OA_OK;
+}
+
+// Pressure-correction solve into f.b.x_pc. FP64: BiCGStab to rtol. Mixed:
+// iterative refinement, FP64 residual r = b - A x, FP32 BiCGStab on A d = r to
+// a loose inner tolerance, x += d, until ||r|| <= rtol ||b||.
+int solve_pcorr(oa_flow* h, double rtol, int maxit, int* iters, double* res, int* refinements) {
+  Flow& f = h->f;
+  DeviceMesh& m = *f.mesh;
+  if (!mixed(f)) {
+    if (int s = h->pc64.setup(m.nn, m.row_ptr, m.cols, m.diag, f.stream)) return s;
+    double* x = nullptr;
+    if (int s = h->pc64.solve<double>(static_cast<const double*>(f.b.A_pc), f.b.b_pc, x, rtol, maxit, iters, res, 20))
+      return s;
+    OA_CUDA(cudaMemcpyAsync(f.b.x_pc, x, sizeof(double) * m.nn, cudaMemcpyDeviceToDevice, f.stream));
+    if (refinements) *refinements = 0;
+    return OA_OK;
+  }
+  if (int s = h->pc32.setup(m.nn, m.row_ptr, m.cols, m.diag, f.stream)) return s;
+  const float* A = static_cast<const float*>(f.b.A_pc);
+  OA_CUDA(cudaMemsetAsync(f.b.x_pc, 0, sizeof(double) * m.nn, f.stream));
+  // ||b||
+  k_sumsq<<<1, 256, 0, f.stream>>>(m.nn, f.b.b_pc, h->scal);
+  count_launches(1);
+  OA_CUDA(cudaMemcpyAsync(h->hscal, h->scal, sizeof(double), cudaMemcpyDeviceToHost, f.stream));
+  OA_CUDA(cudaStreamSynchronize(f.stream));
+  const double bnorm = std::sqrt(h->hscal[0]);
+  int total = 0, nref = 0;
+  double rel = bnorm > 0 ? 1.0 : 0.0;
+  OA_CUDA(cudaMemcpyAsync(h->ir_r, f.b.b_pc, sizeof(double) * m.nn, cudaMemcpyDeviceToDevice, f.stream));
+  while (rel > rtol && total < maxit && nref < 20) {
+    k_from_double<float><<<(m.nn + 255) / 256, 256, 0, f.stream>>>(m.nn, h->ir_r, h->ir_r32);
+    count_launches(1);
+    float* d = nullptr;
+    int it = 0;
+    double r_in = 0.0;
+    // inner tolerance: enough digits for FP32 without stalling
+    const double inner = std::max(rtol / rel, 2e-4);
+    if (int s = h->pc32.solve<float>(A, h->ir_r32, d, std::min(inner, 0.1), maxit - total, &it, &r_in, 20)) return s;
+    total += it;
+    add_correction<float>(m.nn, f.b.x_pc, d, f.stream);
+    if (int s = fp64_residual<float>(m.nn, m.row_ptr, m.cols, A, f.b.x_pc, f.b.b_pc, h->ir_r, h->pc32.partials,
+                                     h->scal + 1, f.stream))
+      return s;
+    OA_CUDA(cudaMemcpyAsync(h->hscal + 1, h->scal + 1, sizeof(double), cudaMemcpyDeviceToHost, f.stream));
+    OA_CUDA(cudaStreamSynchronize(f.stream));
+    rel = bnorm > 0 ? h->hscal[1] / bnorm : 0.0;
+    ++nref;
+    if (!(rel < INFINITY)) return fail(OA_ERR_SOLVER, "pressure refinement: non-finite residual");
+    if (it == 0) break;
+  }
+  if (iters) *iters = total;
+  if (res) *res = rel;
+  if (refinements) *refinements = nref;
+  return OA_OK;
+}
+
+int continuity_rms(oa_flow* h, double* out) {
+  Flow& f = h->f;
+  k_sumsq<<<1, 256, 0, f.stream>>>(f.mesh->nn, f.b.b_pc, h->scal + 2);
+  count_launches(1);
+  OA_CUDA(cudaMemcpyAsync(h->hscal + 2, h->scal + 2, sizeof(double), cudaMemcpyDeviceToHost, f.stream));
+  OA_CUDA(cudaStreamSynchronize(f.stream));
+  *out = std::sqrt(h->hscal[2] / f.mesh->nn);
+  return OA_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* oa_last_error(void) { return g_last_error.c_str(); }
+const char* oa_version(void) { return "openaccel_b200 0.1 (sm_100a)"; }
+
+int oa_mesh_create(const double* coords, int nn, const int* conn, int ne, int topo, const int* face_elem,
+                   const int* face_ord, const int* face_bnd, int nf, oa_mesh** out) {
+  if (!out || !coords || !conn || nn <= 0 || ne <= 0 || nf < 0) return fail(OA_ERR_ARG, "oa_mesh_create: bad arguments");
+  if (topo != OA_TOPO_HEX8) return fail(OA_ERR_MESH, "oa_mesh_create: only hex8 meshes are supported by this build");
+  *out = nullptr;
+  for (long k = 0; k < 8L * ne; ++k)
+    if (conn[k] < 0 || conn[k] >= nn) return fail(OA_ERR_MESH, "oa_mesh_create: connectivity index out of range");
+  for (int f = 0; f < nf; ++f)
+    if (face_elem[f] < 0 || face_elem[f] >= ne || face_ord[f] < 0 || face_ord[f] > 5)
+      return fail(OA_ERR_MESH, "oa_mesh_create: boundary face out of range");
+  static const int LRt[12][2] = {{0, 1}, {1, 2}, {2, 3}, {0, 3}, {4, 5}, {5, 6},
+                                 {6, 7}, {4, 7}, {0, 4}, {1, 5}, {2, 6}, {3, 7}};
+  static const int FN[6][4] = {{0, 1, 5, 4}, {1, 2, 6, 5}, {2, 3, 7, 6}, {0, 4, 7, 3}, {0, 3, 2, 1}, {4, 5, 6, 7}};
+  oa_mesh* M = new oa_mesh();
+  DeviceMesh& m = M->m;
+  m.nn = nn;
+  m.ne = ne;
+  m.nf = nf;
+  // node -> element-by-corner table
+  std::vector<int> n2e(8L * nn, -1);
+  for (int e = 0; e < ne; ++e)
+    for (int a = 0; a < 8; ++a) {
+      int& slot = n2e[8L * conn[8L * e + a] + a];
+      if (slot != -1) {
+        delete M;
+        return fail(OA_ERR_MESH,
+                    "oa_mesh_create: a node is the same local corner of two elements; the row-owner kernels "
+                    "need a consistently oriented hex block");
+      }
+      slot = e;
+    }
+  // reduced-stencil graph: row i = {i} U {j : (i,j) is an SCS L/R pair}
+  std::vector<int> cnt(nn + 1, 0);
+  for (int e = 0; e < ne; ++e)
+    for (int ip = 0; ip < 12; ++ip) {
+      cnt[conn[8L * e + LRt[ip][0]] + 1] += 1;
+      cnt[conn[8L * e + LRt[ip][1]] + 1] += 1;
+    }
+  for (int i = 0; i < nn; ++i) cnt[i + 1] += cnt[i] + 0;
+  std::vector<int> nbr(cnt[nn]);
+  std::vector<int> pos(cnt.begin(), cnt.end() - 1);
+  for (int e = 0; e < ne; ++e)
+    for (int ip = 0; ip < 12; ++ip) {
+      const int L = conn[8L * e + LRt[ip][0]], R = conn[8L * e + LRt[ip][1]];
+      nbr[pos[L]++] = R;
+      nbr[pos[R]++] = L;
+    }
+  m.h_row_ptr.assign(nn + 1, 0);
+  m.h_diag.assign(nn, 0);
+  m.h_cols.clear();
+  m.h_cols.reserve((size_t)nn * 7);
+  std::vector<int> tmp;
+  for (int i = 0; i < nn; ++i) {
+    tmp.assign(nbr.begin() + cnt[i], nbr.begin() + cnt[i + 1]);
+    tmp.push_back(i);
+    std::sort(tmp.begin(), tmp.end());
+    tmp.erase(std::unique(tmp.begin(), tmp.end()), tmp.end());
+    for (size_t k = 0; k < tmp.size(); ++k)
+      if (tmp[k] == i) m.h_diag[i] = (int)k;
+    m.h_cols.insert(m.h_cols.end(), tmp.begin(), tmp.end());
+    m.h_row_ptr[i + 1] = (int)m.h_cols.size();
+  }
+  m.nnz = m.h_row_ptr[nn];
+  m.h_conn.assign(conn, conn + 8L * ne);
+  m.h_face_elem.assign(face_elem, face_elem + nf);
+  m.h_face_ord.assign(face_ord, face_ord + nf);
+  m.h_face_bnd.assign(face_bnd, face_bnd + nf);
+  // boundary faces
+  std::vector<uint8_t> fmask(ne, 0);
+  std::vector<int> wall(nn, 0);
+  for (int f = 0; f < nf; ++f) {
+    fmask[face_elem[f]] |= (uint8_t)(1u << face_ord[f]);
+    for (int k = 0; k < 4; ++k) wall[conn[8L * face_elem[f] + FN[face_ord[f]][k]]] = 1;
+  }
+  int st = OA_OK;
+  if ((st = dalloc(&m.x, 3L * nn)) || (st = dalloc(&m.conn, 8L * ne)) || (st = dalloc(&m.n2e, 8L * nn)) ||
+      (st = dalloc(&m.row_ptr, nn + 1L)) || (st = dalloc(&m.cols, (size_t)m.nnz)) || (st = dalloc(&m.diag, (size_t)nn)) ||
+      (st = dalloc(&m.face_mask, (size_t)ne)) || (st = dalloc(&m.vol, (size_t)nn)) || (st = dalloc(&m.wscv, 8L * ne)) ||
+      (st = dalloc(&m.wall_node, (size_t)nn))) {
+    oa_mesh_destroy(M);
+    return st;
+  }
+  cudaStreamCreateWithFlags(&M->st, cudaStreamNonBlocking);
+  cudaMemcpy(m.x, coords, sizeof(double) * 3 * nn, cudaMemcpyHostToDevice);
+  cudaMemcpy(m.conn, conn, sizeof(int) * 8 * ne, cudaMemcpyHostToDevice);
+  cudaMemcpy(m.n2e, n2e.data(), sizeof(int) * 8 * nn, cudaMemcpyHostToDevice);
+  cudaMemcpy(m.row_ptr, m.h_row_ptr.data(), sizeof(int) * (nn + 1), cudaMemcpyHostToDevice);
+  cudaMemcpy(m.cols, m.h_cols.data(), sizeof(int) * m.nnz, cudaMemcpyHostToDevice);
+  cudaMemcpy(m.diag, m.h_diag.data(), sizeof(int) * nn, cudaMemcpyHostToDevice);
+  cudaMemcpy(m.face_mask, fmask.data(), ne, cudaMemcpyHostToDevice);
+  cudaMemcpy(m.wall_node, wall.data(), sizeof(int) * nn, cudaMemcpyHostToDevice);
+  cudaError_t ce = cudaDeviceSynchronize();
+  if (ce == cudaSuccess) ce = cudaGetLastError();
+  if (ce != cudaSuccess) {
+    oa_mesh_destroy(M);
+    return fail(OA_ERR_CUDA, std::string("mesh upload: ") + cudaGetErrorString(ce));
+  }
+  if ((st = launch_geometry(m, M->st))) {
+    oa_mesh_destroy(M);
+    return st;
+  }
+  *out = M;
+  return OA_OK;
+}
+
+void oa_mesh_destroy(oa_mesh* M) {
+  if (!M) return;
+  DeviceMesh& m = M->m;
+  void* ptrs[] = {m.x, m.conn, m.n2e, m.row_ptr, m.cols, m.diag, m.face_mask, m.vol, m.wscv, m.wall_node};
+  for (void* p : ptrs)
+    if (p) cudaFree(p);
+  if (M->st) cudaStreamDestroy(M->st);
+  delete M;
+}
+
+int oa_mesh_nnz(const oa_mesh* M, int* nnz) {
+  if (!M || !nnz) return fail(OA_ERR_ARG, "oa_mesh_nnz: null argument");
+  *nnz = M->m.nnz;
+  return OA_OK;
+}
+
+int oa_mesh_graph(const oa_mesh* M, int* row_ptr, int* cols) {
+  if (!M || !row_ptr || !cols) return fail(OA_ERR_ARG, "oa_mesh_graph: null argument");
+  std::memcpy(row_ptr, M->m.h_row_ptr.data(), sizeof(int) * (M->m.nn + 1));
+  std::memcpy(cols, M->m.h_cols.data(), sizeof(int) * M->m.nnz);
+  return OA_OK;
+}
+
+int oa_mesh_dual_volume(const oa_mesh* M, double* vol) {
+  if (!M || !vol) return fail(OA_ERR_ARG, "oa_mesh_dual_volume: null argument");
+  OA_CUDA(cudaMemcpy(vol, M->m.vol, sizeof(double) * M->m.nn, cudaMemcpyDeviceToHost));
+  return OA_OK;
+}
+
+int oa_flow_create(oa_mesh* M, const oa_flow_settings* s, const double* bnd_velocity, int nbnd, oa_flow** out) {
+  if (!M || !s || !out || nbnd < 0 || (nbnd > 0 && !bnd_velocity)) return fail(OA_ERR_ARG, "oa_flow_create: bad arguments");
+  if (s->urf_u <= 0 || s->urf_p <= 0 || s->dt <= 0) return fail(OA_ERR_ARG, "oa_flow_create: relaxation/timescale must be > 0");
+  if (s->precision != OA_PREC_FP64 && s->precision != OA_PREC_MIXED) return fail(OA_ERR_ARG, "oa_flow_create: unknown precision");
+  if (s->ref_node >= M->m.nn) return fail(OA_ERR_ARG, "oa_flow_create: ref_node out of range");
+  *out = nullptr;
+  oa_flow* H = new oa_flow();
+  Flow& f = H->f;
+  f.mesh = &M->m;
+  f.s = *s;
+  const size_t nn = M->m.nn, ne = M->m.ne, nnz = M->m.nnz;
+  const size_t tm = s->precision == OA_PREC_MIXED ? sizeof(float) : sizeof(double);
+  int st = OA_OK;
+  if ((st = dalloc(&f.U, 3 * nn)) || (st = dalloc(&f.p, nn)) || (st = dalloc(&f.gradU, 9 * nn)) ||
+      (st = dalloc(&f.gradP, 3 * nn)) || (st = dalloc(&f.du, 3 * nn)) || (st = dalloc(&f.div, nn)) ||
+      (st = dalloc(&f.mDot, 12 * ne)) || (st = dalloc(&f.rho, nn)) || (st = dalloc(&f.mu, nn)) ||
+      (st = dalloc(&f.sideU, 3 * nn)) || (st = dalloc(&f.b.b_pc, nn)) || (st = dalloc(&f.b.x_mom, 3 * nn)) ||
+      (st = dalloc(&f.b.x_pc, nn)) || (st = dalloc(&f.err_dev, 1)) || (st = dalloc(&H->ir_r, nn)) ||
+      (st = dalloc(&H->ir_r32, nn)) || (st = dalloc(&H->scal, 4))) {
+    oa_flow_destroy(H);
+    return st;
+  }
+  if (cudaMalloc(&f.b.A_mom, tm * 9 * nnz) != cudaSuccess || cudaMalloc(&f.b.b_mom, tm * 3 * nn) != cudaSuccess ||
+      cudaMalloc(&f.b.A_pc, tm * nnz) != cudaSuccess || cudaMallocHost(&H->hscal, 4 * sizeof(double)) != cudaSuccess) {
+    oa_flow_destroy(H);
+    return fail(OA_ERR_CUDA, "oa_flow_create: device allocation failed");
+  }
+  cudaStreamCreateWithFlags(&f.stream, cudaStreamNonBlocking);
+  // constant properties, zero fields
+  std::vector<double> h(nn, s->rho);
+  cudaMemcpy(f.rho, h.data(), sizeof(double) * nn, cudaMemcpyHostToDevice);
+  std::fill(h.begin(), h.end(), s->mu);
+  cudaMemcpy(f.mu, h.data(), sizeof(double) * nn, cudaMemcpyHostToDevice);
+  cudaMemset(f.U, 0, sizeof(double) * 3 * nn);
+  cudaMemset(f.p, 0, sizeof(double) * nn);
+  cudaMemset(f.gradU, 0, sizeof(double) * 9 * nn);
+  cudaMemset(f.gradP, 0, sizeof(double) * 3 * nn);
+  cudaMemset(f.du, 0, sizeof(double) * 3 * nn);
+  cudaMemset(f.div, 0, sizeof(double) * nn);
+  cudaMemset(f.mDot, 0, sizeof(double) * 12 * ne);
+  cudaMemset(f.err_dev, 0, sizeof(int));
+  // node-side wall velocity, boundary by boundary in index order
+  // (nodeField::updateBoundarySideFieldSpecifiedValue sets parts in turn)
+  std::vector<double> side(3 * nn, 0.0);
+  {
+    static const int FN[6][4] = {{0, 1, 5, 4}, {1, 2, 6, 5}, {2, 3, 7, 6}, {0, 4, 7, 3}, {0, 3, 2, 1}, {4, 5, 6, 7}};
+    const DeviceMesh& m = M->m;
+    for (int bnd = 0; bnd < nbnd; ++bnd)
+      for (int fc = 0; fc < m.nf; ++fc) {
+        if (m.h_face_bnd[fc] != bnd) continue;
+        for (int k = 0; k < 4; ++k) {
+          const int nd = m.h_conn[8L * m.h_face_elem[fc] + FN[m.h_face_ord[fc]][k]];
+          for (int d = 0; d < 3; ++d) side[3L * nd + d] = bnd_velocity[3 * bnd + d];
+        }
+      }
+  }
+  cudaMemcpy(f.sideU, side.data(), sizeof(double) * 3 * nn, cudaMemcpyHostToDevice);
+  cudaError_t ce = cudaDeviceSynchronize();
+  if (ce == cudaSuccess) ce = cudaGetLastError();
+  if (ce != cudaSuccess) {
+    oa_flow_destroy(H);
+    return fail(OA_ERR_CUDA, std::string("oa_flow_create: ") + cudaGetErrorString(ce));
+  }
+  *out = H;
+  return OA_OK;
+}
+
+void oa_flow_destroy(oa_flow* H) {
+  if (!H) return;
+  Flow& f = H->f;
+  void* ptrs[] = {f.U, f.p, f.gradU, f.gradP, f.du, f.div, f.mDot, f.rho, f.mu, f.sideU, f.b.A_mom, f.b.b_mom,
+                  f.b.A_pc, f.b.b_pc, f.b.x_mom, f.b.x_pc, f.err_dev, H->ir_r, H->ir_r32, H->scal};
+  for (void* p : ptrs)
+    if (p) cudaFree(p);
+  if (H->hscal) cudaFreeHost(H->hscal);
+  H->pc64.release();
+  H->mom64.release();
+  H->pc32.release();
+  H->mom32.release();
+  if (f.stream) cudaStreamDestroy(f.stream);
+  delete H;
+}
+
+int oa_flow_set_field(oa_flow* H, const char* name, const double* host, long n) {
+  if (!H || !name || !host) return fail(OA_ERR_ARG, "oa_flow_set_field: null argument");
+  size_t len = 0;
+  double* d = field_ptr(H->f, name, &len);
+  if (!d) return fail(OA_ERR_ARG, std::string("oa_flow_set_field: unknown field ") + name);
+  if ((size_t)n != len) return fail(OA_ERR_ARG, std::string("oa_flow_set_field: size mismatch for ") + name);
+  OA_CUDA(cudaMemcpyAsync(d, host, sizeof(double) * len, cudaMemcpyHostToDevice, H->f.stream));
+  OA_CUDA(cudaStreamSynchronize(H->f.stream));
+  return OA_OK;
+}
+
+int oa_flow_get_field(oa_flow* H, const char* name, double* host, long n) {
+  if (!H || !name || !host) return fail(OA_ERR_ARG, "oa_flow_get_field: null argument");
+  size_t len = 0;
+  double* d = field_ptr(H->f, name, &len);
+  if (!d) return fail(OA_ERR_ARG, std::string("oa_flow_get_field: unknown field ") + name);
+  if ((size_t)n != len) return fail(OA_ERR_ARG, std::string("oa_flow_get_field: size mismatch for ") + name);
+  OA_CUDA(cudaMemcpyAsync(host, d, sizeof(double) * len, cudaMemcpyDeviceToHost, H->f.stream));
+  OA_CUDA(cudaStreamSynchronize(H->f.stream));
+  return OA_OK;
+}
+
+int oa_flow_field_device_ptr(oa_flow* H, const char* name, double** dev) {
+  if (!H || !name || !dev) return fail(OA_ERR_ARG, "oa_flow_field_device_ptr: null argument");
+  size_t len = 0;
+  *dev = field_ptr(H->f, name, &len);
+  if (!*dev) return fail(OA_ERR_ARG, std::string("oa_flow_field_device_ptr: unknown field ") + name);
+  return OA_OK;
+}
+
+int oa_flow_initialize(oa_flow* H) {
+  if (!H) return fail(OA_ERR_ARG, "oa_flow_initialize: null handle");
+  Flow& f = H->f;
+  int s;
+  if ((s = launch_gradient(f, 1)) || (s = launch_init_mdot(f)) || (s = launch_div(f)) || (s = launch_gradient(f, 0)))
+    return s;
+  return check_err_flag(f, "oa_flow_initialize");
+}
+
+int oa_assemble_momentum(oa_flow* H, double* A, double* b) {
+  if (!H) return fail(OA_ERR_ARG, "oa_assemble_momentum: null handle");
+  Flow& f = H->f;
+  if (int s = launch_momentum(f, mixed(f))) return s;
+  if (int s = check_err_flag(f, "oa_assemble_momentum")) return s;
+  if (int s = copy_out_matrix(f, f.b.A_mom, 9 * (size_t)f.mesh->nnz, A)) return s;
+  return copy_out_matrix(f, f.b.b_mom, 3 * (size_t)f.mesh->nn, b);
+}
+
+int oa_assemble_pcorr(oa_flow* H, double* A, double* b) {
+  if (!H) return fail(OA_ERR_ARG, "oa_assemble_pcorr: null handle");
+  Flow& f = H->f;
+  if (int s = launch_pcorr(f, mixed(f))) return s;
+  if (int s = check_err_flag(f, "oa_assemble_pcorr")) return s;
+  if (int s = copy_out_matrix(f, f.b.A_pc, (size_t)f.mesh->nnz, A)) return s;
+  if (b) {
+    OA_CUDA(cudaMemcpyAsync(b, f.b.b_pc, sizeof(double) * f.mesh->nn, cudaMemcpyDeviceToHost, f.stream));
+    OA_CUDA(cudaStreamSynchronize(f.stream));
+  }
+  return OA_OK;
+}
+
+int oa_update_mdot(oa_flow* H) {
+  if (!H) return fail(OA_ERR_ARG, "oa_update_mdot: null handle");
+  if (int s = launch_update_mdot(H->f)) return s;
+  return check_err_flag(H->f, "oa_update_mdot");
+}
+
+int oa_update_div(oa_flow* H) {
+  if (!H) return fail(OA_ERR_ARG, "oa_update_div: null handle");
+  return launch_div(H->f);
+}
+
+int oa_update_gradient(oa_flow* H, int which) {
+  if (!H || (which != 0 && which != 1)) return fail(OA_ERR_ARG, "oa_update_gradient: bad arguments");
+  return launch_gradient(H->f, which);
+}
+
+int oa_solve(oa_flow* H, int sys, double rtol, int maxit, double* x, int* iters, double* res) {
+  if (!H || (sys != 0 && sys != 1) || maxit <= 0) return fail(OA_ERR_ARG, "oa_solve: bad arguments");
+  Flow& f = H->f;
+  int s;
+  if (sys == 0) {
+    if ((s = solve_momentum(H, rtol, maxit, iters, res, false))) return s;
+    if (x) {
+      OA_CUDA(cudaMemcpyAsync(x, f.b.x_mom, sizeof(double) * 3 * f.mesh->nn, cudaMemcpyDeviceToHost, f.stream));
+    }
+  } else {
+    if ((s = solve_pcorr(H, rtol, maxit, iters, res, nullptr))) return s;
+    if (x) {
+      OA_CUDA(cudaMemcpyAsync(x, f.b.x_pc, sizeof(double) * f.mesh->nn, cudaMemcpyDeviceToHost, f.stream));
+    }
+  }
+  OA_CUDA(cudaStreamSynchronize(f.stream));
+  return OA_OK;
+}
+
+// segregatedFlowEquations::solve (segregatedFlowEquations.cpp:76-297): momentum
+// predictor, one pressure-correction sub-iteration, mass-flow and velocity
+// corrections, gradient updates.
+int oa_simple_iterate(oa_flow* H, int n, oa_iter_stats* stats) {
+  if (!H || n < 0) return fail(OA_ERR_ARG, "oa_simple_iterate: bad arguments");
+  Flow& f = H->f;
+  const bool mx = mixed(f);
+  for (int it = 0; it < n; ++it) {
+    oa_iter_stats st{};
+    int s;
+    // momentum predictor (navierStokesEquation::solve)
+    if ((s = launch_momentum(f, mx))) return s;
+    if ((s = solve_momentum(H, f.s.mom_rtol, f.s.mom_maxit, &st.mom_iters, &st.mom_res, true))) return s;
+    if ((s = launch_update_mdot(f))) return s;
+    // pressure correction (pressureCorrectionEquation::solve)
+    if ((s = launch_pcorr(f, mx))) return s;
+    if ((s = continuity_rms(H, &st.continuity_rms))) return s;
+    if ((s = solve_pcorr(H, f.s.pc_rtol, f.s.pc_maxit, &st.pc_iters, &st.pc_res, &st.pc_refinements))) return s;
+    k_axpy<<<(f.mesh->nn + 255) / 256, 256, 0, f.stream>>>(f.mesh->nn, f.p, f.b.x_pc, f.s.urf_p);
+    count_launches(1);
+    // corrections
+    if ((s = launch_update_mdot(f)) || (s = launch_div(f)) || (s = launch_axpy_du_gradp(f, +1.0)) ||
+        (s = launch_gradient(f, 0)) || (s = launch_axpy_du_gradp(f, -1.0)) || (s = launch_gradient(f, 1)))
+      return s;
+    if ((s = check_err_flag(f, "oa_simple_iterate"))) return s;
+    if (stats) stats[it] = st;
+  }
+  return OA_OK;
+}
+
+int oa_flow_stream(oa_flow* H, void** stream) {
+  if (!H || !stream) return fail(OA_ERR_ARG, "oa_flow_stream: null argument");
+  *stream = (void*)H->f.stream;
+  return OA_OK;
+}
+
+int oa_launch_count(long long* count) {
+  if (!count) return fail(OA_ERR_ARG, "oa_launch_count: null argument");
+  *count = g_launches.load();
+  return OA_OK;
+}
+
+int oa_time_kernel(oa_flow* H, int which, int reps, double* ms) {
+  if (!H || !ms || reps <= 0 || which < 0 || which > 3) return fail(OA_ERR_ARG, "oa_time_kernel: bad arguments");
+  Flow& f = H->f;
+  cudaEvent_t e0, e1;
+  OA_CUDA(cudaEventCreate(&e0));
+  OA_CUDA(cudaEventCreate(&e1));
+  // one untimed launch, then reps timed ones
+  for (int r = 0; r <= reps; ++r) {
+    if (r == 1) OA_CUDA(cudaEventRecord(e0, f.stream));
+    int s = OA_OK;
+    if (which == 0) s = launch_momentum(f, mixed(f));
+    else if (which == 1) s = launch_pcorr(f, mixed(f));
+    else if (which == 2) s = launch_update_mdot(f);
+    else s = launch_gradient(f, 1);
+    if (s) return s;
+  }
+  OA_CUDA(cudaEventRecord(e1, f.stream));
+  OA_CUDA(cudaEventSynchronize(e1));
+  float t = 0.f;
+  OA_CUDA(cudaEventElapsedTime(&t, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  *ms = t / reps;
+  return check_err_flag(f, "oa_time_kernel");
+}
+
+int oa_flow_sync(oa_flow* H) {
+  if (!H) return fail(OA_ERR_ARG, "oa_flow_sync: null handle");
+  OA_CUDA(cudaStreamSynchronize(H->f.stream));
+  return OA_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,87 @@
+// Internal structures of the B200 CVFEM engine (not part of the C-ABI).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/openaccel_b200.h"
+
+namespace oa {
+
+// Device-resident mesh: hex8 connectivity, node -> incident-element-by-corner
+// table, reduced-stencil CSR graph, wall faces and static FP64 geometry.
+// POD view of the device arrays, passed to kernels by value.
+struct MeshView {
+  int nn = 0, ne = 0, nf = 0, nnz = 0;
+  double* x = nullptr;         // [nn][3]
+  int* conn = nullptr;         // [ne][8]
+  int* n2e = nullptr;          // [nn][8]: element where the node is corner c, or -1
+  int* row_ptr = nullptr;      // [nn+1]
+  int* cols = nullptr;         // [nnz]
+  int* diag = nullptr;         // [nn] offset of the diagonal within the row
+  uint8_t* face_mask = nullptr;  // [ne] bit f: face f is a no-slip wall face
+  double* vol = nullptr;       // [nn] dual nodal volume
+  double* wscv = nullptr;      // [ne][8] SCV volume fractions
+  int* wall_node = nullptr;    // [nn] 1 on wall nodes
+};
+
+struct DeviceMesh : MeshView {
+  int topo = OA_TOPO_HEX8;
+  int geom_err = 0;
+  // host copies needed for set-up and parity dumps
+  std::vector<int> h_row_ptr, h_cols, h_diag;
+  std::vector<int> h_conn, h_face_elem, h_face_ord, h_face_bnd;
+  const MeshView& view() const { return *this; }
+};
+
+struct Buffers {
+  // matrices / vectors in the working precision
+  void* A_mom = nullptr;   // [nnz][9]
+  void* b_mom = nullptr;   // [nn][3]
+  void* A_pc = nullptr;    // [nnz]
+  double* b_pc = nullptr;  // [nn]
+  double* x_mom = nullptr; // [nn][3]
+  double* x_pc = nullptr;  // [nn]
+};
+
+struct Flow {
+  DeviceMesh* mesh = nullptr;
+  oa_flow_settings s{};
+  cudaStream_t stream = nullptr;
+  // fields (FP64)
+  double *U = nullptr, *p = nullptr, *gradU = nullptr, *gradP = nullptr, *du = nullptr,
+         *div = nullptr, *mDot = nullptr, *rho = nullptr, *mu = nullptr, *sideU = nullptr;
+  Buffers b;
+  // Krylov workspace (allocated on first solve)
+  std::vector<void*> work;
+  double* red = nullptr;        // reduction partials
+  double* red_host = nullptr;   // pinned
+  int* err_dev = nullptr;       // device error flags
+  int last_mom_iters = 0, last_pc_iters = 0;
+  double last_mom_res = 0, last_pc_res = 0, last_cont = 0;
+};
+
+void set_error(const std::string& msg);
+void count_launches(long long n);
+int fail(int code, const std::string& msg);
+
+#define OA_CUDA(call)                                                              \
+  do {                                                                             \
+    cudaError_t e_ = (call);                                                       \
+    if (e_ != cudaSuccess)                                                         \
+      return ::oa::fail(OA_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+// kernels / launchers (oa_kernels.cu)
+int launch_geometry(DeviceMesh& m, cudaStream_t st);
+int launch_pcorr(Flow& f, bool mixed);
+int launch_momentum(Flow& f, bool mixed);
+int launch_init_mdot(Flow& f);
+int launch_update_mdot(Flow& f);
+int launch_div(Flow& f);
+int launch_gradient(Flow& f, int which);
+int launch_axpy_du_gradp(Flow& f, double sign);
+
+}  // namespace oa

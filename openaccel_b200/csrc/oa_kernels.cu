@@ -1,0 +1,920 @@
+// Hand-written sm_100a kernels of the hex8 CVFEM hot path: geometry
+// precompute, pressure-correction and momentum assembly (row-owner, written
+// once per CSR row), mass-flow update, divergence and Green-Gauss gradients.
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "oa_internal.h"
+#include "oa_rowlane.cuh"
+
+namespace oa {
+
+using namespace hex8;
+
+constexpr double SMALL = 2.220446049250313e-16;  // src/basic/types.h:179
+constexpr int BLOCK = 128;                        // 16 rows per block
+
+template <int I, int N>
+struct StaticFor {
+  template <class F>
+  __device__ __forceinline__ static void run(F&& f) {
+    f(std::integral_constant<int, I>{});
+    StaticFor<I + 1, N>::run(f);
+  }
+};
+template <int N>
+struct StaticFor<N, N> {
+  template <class F>
+  __device__ __forceinline__ static void run(F&&) {}
+};
+
+__device__ __forceinline__ void load3(const double* __restrict__ p, int n, double (&v)[3]) {
+  v[0] = __ldg(p + 3 * n);
+  v[1] = __ldg(p + 3 * n + 1);
+  v[2] = __ldg(p + 3 * n + 2);
+}
+
+// ---------------------------------------------------------------------------
+// Geometry precompute (FP64, once per mesh)
+
+// Grandy hex volume by 24 triangular facets (CalculateHexVolume.F).
+__device__ double hex_volume(const double (&v)[8][3]) {
+  constexpr int T[24][3] = {{0, 8, 1},  {8, 2, 1},  {3, 2, 8},  {3, 8, 0},  {6, 9, 5},  {7, 9, 6},
+                            {4, 9, 7},  {4, 5, 9},  {10, 0, 1}, {5, 10, 1}, {4, 10, 5}, {4, 0, 10},
+                            {7, 6, 11}, {6, 2, 11}, {2, 3, 11}, {3, 7, 11}, {6, 12, 2}, {5, 12, 6},
+                            {5, 1, 12}, {1, 2, 12}, {0, 4, 13}, {4, 7, 13}, {7, 3, 13}, {3, 0, 13}};
+  constexpr int Q[6][4] = {{0, 1, 2, 3}, {4, 5, 6, 7}, {0, 1, 5, 4},
+                           {3, 2, 6, 7}, {1, 2, 6, 5}, {0, 3, 7, 4}};
+  double c[14][3];
+#pragma unroll
+  for (int n = 0; n < 8; ++n)
+#pragma unroll
+    for (int k = 0; k < 3; ++k) c[n][k] = v[n][k];
+#pragma unroll
+  for (int f = 0; f < 6; ++f)
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+      c[8 + f][k] = 0.25 * (v[Q[f][0]][k] + v[Q[f][1]][k] + v[Q[f][2]][k] + v[Q[f][3]][k]);
+  double vol = 0.0;
+#pragma unroll
+  for (int t = 0; t < 24; ++t) {
+    const double* P = c[T[t][0]];
+    const double* R1 = c[T[t][1]];
+    const double* R2 = c[T[t][2]];
+    const double f0 = P[0] + R1[0] + R2[0], f1 = P[1] + R1[1] + R2[1], f2 = P[2] + R1[2] + R2[2];
+    vol += f0 * ((R1[1] - P[1]) * (R2[2] - P[2]) - (R2[1] - P[1]) * (R1[2] - P[2])) -
+           f1 * ((R1[0] - P[0]) * (R2[2] - P[2]) - (R2[0] - P[0]) * (R1[2] - P[2])) +
+           f2 * ((R1[0] - P[0]) * (R2[1] - P[1]) - (R2[0] - P[0]) * (R1[1] - P[1]));
+  }
+  return vol / 18.0;
+}
+
+// SCV volume of corner 0 in the canonical frame: sub-hex
+// {0, mid01, face0123, mid03, mid04, face0145, centroid, face0347}
+// (hex_scv_det table row 1).
+__device__ __forceinline__ double corner0_scv(const double (&x)[8][3], const Corner0Points& p) {
+  double v[8][3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    v[0][k] = x[0][k];
+    v[1][k] = p.m01[k];
+    v[2][k] = p.fB[k];
+    v[3][k] = p.m03[k];
+    v[4][k] = p.m04[k];
+    v[5][k] = p.fF[k];
+    v[6][k] = p.cen[k];
+    v[7][k] = p.fL[k];
+  }
+  return hex_volume(v);
+}
+
+__device__ __forceinline__ void gather_x(const MeshView& m, int e, uint32_t pw, double (&x)[8][3],
+                                         int (&nd)[8]) {
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    nd[k] = __ldg(m.conn + 8 * e + perm_at(pw, k));
+    load3(m.x, nd[k], x[k]);
+  }
+}
+
+struct GeoArgs {
+  MeshView m;
+  double* scv;  // [ne][8] raw SCV volumes (scratch)
+  int* err;
+};
+
+// Element kernel: SCV volumes of all 8 corners, stored as volume fractions
+// (the scv weights of pressureCorrectionAssemblerElemTerms.cpp:349-368).
+__global__ void __launch_bounds__(BLOCK) k_scv(GeoArgs a) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= a.m.ne) return;
+  double vols[8];
+  double Vel = 0.0;
+#pragma unroll 1
+  for (int c = 0; c < 8; ++c) {
+    double x[8][3];
+    int nd[8];
+    gather_x(a.m, e, perm_word(c), x, nd);
+    Corner0Points p;
+    corner0_points(x, p);
+    vols[c] = corner0_scv(x, p);
+    if (!(vols[c] > 0.0)) a.err[0] = 1;
+  }
+#pragma unroll
+  for (int c = 0; c < 8; ++c) Vel += vols[c];
+  const double iV = 1.0 / Vel;
+#pragma unroll
+  for (int c = 0; c < 8; ++c) {
+    a.scv[8 * e + c] = vols[c];
+    a.m.wscv[8 * e + c] = vols[c] * iV;
+  }
+}
+
+// Row kernel: dual nodal volume = sum of incident SCV volumes
+// (mesh::updateDualNodalVolumeField_).
+__global__ void __launch_bounds__(BLOCK) k_dual_volume(GeoArgs a) {
+  const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 3;
+  const int c = threadIdx.x & 7;
+  const bool rv = row < a.m.nn;
+  const int e = rv ? a.m.n2e[8 * row + c] : -1;
+  double v = (e >= 0) ? a.scv[8 * e + c] : 0.0;
+  v = rowsum8(v);
+  if (rv && c == 0) a.m.vol[row] = v;
+}
+
+int launch_geometry(DeviceMesh& m, cudaStream_t st) {
+  GeoArgs a{m.view(), nullptr, nullptr};
+  OA_CUDA(cudaMallocAsync(&a.scv, sizeof(double) * 8 * (size_t)m.ne, st));
+  OA_CUDA(cudaMallocAsync(&a.err, sizeof(int), st));
+  OA_CUDA(cudaMemsetAsync(a.err, 0, sizeof(int), st));
+  k_scv<<<(m.ne + BLOCK - 1) / BLOCK, BLOCK, 0, st>>>(a);
+  k_dual_volume<<<(int)(((size_t)m.nn * 8 + BLOCK - 1) / BLOCK), BLOCK, 0, st>>>(a);
+  OA_CUDA(cudaGetLastError());
+  int herr = 0;
+  OA_CUDA(cudaMemcpyAsync(&herr, a.err, sizeof(int), cudaMemcpyDeviceToHost, st));
+  OA_CUDA(cudaFreeAsync(a.scv, st));
+  OA_CUDA(cudaFreeAsync(a.err, st));
+  OA_CUDA(cudaStreamSynchronize(st));
+  m.geom_err = herr;
+  if (herr) return fail(OA_ERR_GEOMETRY, "non-positive sub-control volume in mesh");
+  return OA_OK;
+}
+
+// ---------------------------------------------------------------------------
+// CSR row write-out shared by the assembly kernels. Each lane publishes its
+// three edge-neighbour blocks with their column ids; lane s of the row then
+// emits CSR slot s (s, s+8, ...), summing the matching contributions in lane
+// order. The diagonal block is already reduced in every lane.
+template <int B, class TM>
+__device__ __forceinline__ void write_row(int row, bool rv, int c, int lane, const TM (&diag)[B],
+                                          const TM (&nb)[3][B], const int (&nbc)[3],
+                                          const MeshView& m, TM* __restrict__ A, TM* sh_val,
+                                          int* sh_col, bool offdiag_zero) {
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    sh_col[lane * 3 + k] = nbc[k];
+#pragma unroll
+    for (int b = 0; b < B; ++b) sh_val[(lane * 3 + k) * B + b] = nb[k][b];
+  }
+  __syncwarp();
+  if (rv) {
+    const int rp = __ldg(m.row_ptr + row);
+    const int len = __ldg(m.row_ptr + row + 1) - rp;
+    const int dof = __ldg(m.diag + row);
+    const int base = lane & ~7;
+    for (int s = c; s < len; s += 8) {
+      TM out[B];
+      if (s == dof) {
+#pragma unroll
+        for (int b = 0; b < B; ++b) out[b] = diag[b];
+      } else {
+#pragma unroll
+        for (int b = 0; b < B; ++b) out[b] = TM(0);
+        if (!offdiag_zero) {
+          const int col = __ldg(m.cols + rp + s);
+#pragma unroll
+          for (int c2 = 0; c2 < 8; ++c2)
+#pragma unroll
+            for (int k = 0; k < 3; ++k)
+              if (sh_col[(base + c2) * 3 + k] == col) {
+#pragma unroll
+                for (int b = 0; b < B; ++b) out[b] += sh_val[((base + c2) * 3 + k) * B + b];
+              }
+        }
+      }
+#pragma unroll
+      for (int b = 0; b < B; ++b) A[(size_t)(rp + s) * B + b] = out[b];
+    }
+  }
+  __syncwarp();
+}
+
+// ---------------------------------------------------------------------------
+// Pressure-correction assembly
+// (pressureCorrectionAssemblerElemTerms.cpp:17-616, incompressible, stationary
+// frame; adjustMatrixForPressureReference, pressureCorrectionAssembler.cpp:19-63).
+struct PcArgs {
+  MeshView m;
+  const double *U, *p, *gradP, *du, *mDot, *rho;
+  void* A;
+  double* b;
+  int ref_node;
+  int* err;
+};
+
+template <bool USH, bool PGSH, class TF>
+__global__ void __launch_bounds__(BLOCK) k_pcorr(PcArgs a) {
+  __shared__ TF sh_val[BLOCK * 3];
+  __shared__ int sh_col[BLOCK * 3];
+  const int lane = threadIdx.x & 31;
+  const int warp_base = threadIdx.x & ~31;
+  const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 3;
+  const int c = threadIdx.x & 7;
+  const bool rv = row < a.m.nn;
+  const int e = rv ? __ldg(a.m.n2e + 8 * row + c) : -1;
+  TF diag[1] = {TF(0)};
+  TF nb[3][1] = {{TF(0)}, {TF(0)}, {TF(0)}};
+  int nbc[3] = {-1, -1, -1};
+  double rhs = 0.0;
+  if (e >= 0) {
+    const uint32_t pw = perm_word(c);
+    const uint32_t iw = ip_word(c);
+    double x[8][3];
+    int nd[8];
+    gather_x(a.m, e, pw, x, nd);
+    Corner0Points P;
+    corner0_points(x, P);
+    double Aq[3][3];
+    corner0_areas(P, Aq[0], Aq[1], Aq[2]);
+    // element-centre pressure gradient by SCV volume fractions
+    double Gp[3] = {0.0, 0.0, 0.0};
+    double pn[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const double w = __ldg(a.m.wscv + 8 * e + perm_at(pw, k));
+      double gp[3];
+      load3(a.gradP, nd[k], gp);
+#pragma unroll
+      for (int j = 0; j < 3; ++j) Gp[j] += w * gp[j];
+      pn[k] = __ldg(a.p + nd[k]);
+    }
+    const double rho0 = __ldg(a.rho + nd[0]);
+    int err = 0;
+    StaticFor<0, 3>::run([&](auto qc) {
+      constexpr int q = decltype(qc)::value;
+      constexpr int IP = q == 0 ? 0 : (q == 1 ? 3 : 8);
+      constexpr int R = q == 0 ? 1 : (q == 1 ? 3 : 4);
+      using PG = ScsPt<IP, PGSH>;
+      using PV = ScsPt<IP, USH>;
+      const InvJac J = inv_jacobian<PG>(x, &err);
+      double u[3] = {0, 0, 0}, duip[3] = {0, 0, 0}, dp[3] = {0, 0, 0};
+      StaticFor<0, 8>::run([&](auto nc) {
+        constexpr int n = decltype(nc)::value;
+        constexpr double N = shape_at<PV, n>();
+        if (N != 0.0) {
+          double un[3], dn[3];
+          load3(a.U, nd[n], un);
+          load3(a.du, nd[n], dn);
+#pragma unroll
+          for (int j = 0; j < 3; ++j) {
+            u[j] += N * un[j];
+            duip[j] += N * dn[j];
+          }
+        }
+      });
+      double g[8][3];
+      StaticFor<0, 8>::run([&](auto nc) {
+        constexpr int n = decltype(nc)::value;
+        grad_n<PG, n>(J, g[n]);
+        if (!grad_is_zero<PG, n>()) {
+#pragma unroll
+          for (int j = 0; j < 3; ++j) dp[j] += g[n][j] * pn[n];
+        }
+      });
+      const int pk = (iw >> (5 * q)) & 31;
+      const double tm = (pk & 1) ? -__ldg(a.mDot + 12 * e + (pk >> 1)) : __ldg(a.mDot + 12 * e + (pk >> 1));
+      const double rhoHR = tm > 0 ? rho0 : __ldg(a.rho + nd[R]);
+      // lhs: -rhoHR * D_ip . (grad N_n) A  (FP32 in the mixed form)
+      const TF rh = TF(rhoHR);
+      TF dA[3];
+#pragma unroll
+      for (int j = 0; j < 3; ++j) dA[j] = TF(duip[j]) * TF(Aq[q][j]);
+      StaticFor<0, 8>::run([&](auto nc) {
+        constexpr int n = decltype(nc)::value;
+        if (!grad_is_zero<PG, n>()) {
+          TF f = TF(0);
+#pragma unroll
+          for (int j = 0; j < 3; ++j) f += -rh * dA[j] * TF(g[n][j]);
+          constexpr int sl = nb_slot(n);
+          if (sl < 0)
+            diag[0] += f;
+          else
+            nb[sl][0] += f;
+        }
+      });
+      double mm = 0.0;
+#pragma unroll
+      for (int j = 0; j < 3; ++j) {
+        mm += rhoHR * u[j] * Aq[q][j];
+        mm -= rhoHR * duip[j] * (dp[j] - Gp[j]) * Aq[q][j];
+      }
+      rhs -= mm;
+    });
+    if (err) a.err[0] = 1;
+    nbc[0] = nd[1];
+    nbc[1] = nd[3];
+    nbc[2] = nd[4];
+  }
+  diag[0] = rowsum8(diag[0]);
+  rhs = rowsum8(rhs);
+  const bool refrow = rv && row == a.ref_node;
+  write_row<1, TF>(row, rv, c, lane, diag, nb, nbc, a.m, static_cast<TF*>(a.A),
+                   sh_val + warp_base * 3, sh_col + warp_base * 3, refrow);
+  if (rv && c == 0) a.b[row] = refrow ? 0.0 : rhs;
+}
+
+// ---------------------------------------------------------------------------
+// Momentum assembly (navierStokesAssemblerElemTerms.cpp:15-441 upwind,
+// incompressible; no-slip walls ...ElemBoundaryConditions.cpp:2659-2981 with
+// IP_ZERO_NORMAL_STRESS_FIXED_VEL__; node terms ...NodeTerms.cpp:16-149;
+// postAssemble_ relaxation phiAssembler.h:967-1006 and wall rhs relaxation
+// navierStokesAssembler.cpp:241-385; computeDUCoefficients :84-232).
+struct MomArgs {
+  MeshView m;
+  const double *U, *gradP, *div, *mDot, *rho, *mu, *sideU;
+  void* A;
+  void* b;
+  double* du;
+  double dt, urf_inv, wall_relax;
+  int* err;
+};
+
+// Zero-normal-stress wall term at the exposed ip of canonical face FC nearest
+// corner 0 (IP_ZERO_NORMAL_STRESS_FIXED_VEL__).
+template <int FC, bool USH, bool UGSH, class TF>
+__device__ __forceinline__ void wall_face(const MomArgs& a, const double (&x)[8][3], const int (&nd)[8],
+                                          const TF (&Uc)[8][3], const TF (&mu)[8], TF (&diag)[9],
+                                          TF (&nb)[3][9], TF (&rhs)[3], int* err) {
+  constexpr int f0 = face_node(FC, 0), f1 = face_node(FC, 1), f2 = face_node(FC, 2), f3 = face_node(FC, 3);
+  double Af[3];
+  face_area_at_first(x[f0], x[f1], x[f2], x[f3], Af);
+  using PT = FacePt<FC, 0, UGSH>;
+  const InvJac J = inv_jacobian<PT>(x, err);
+  // face-node velocities replaced by the wall (node-side) values
+  TF Ue[8][3];
+#pragma unroll
+  for (int n = 0; n < 8; ++n)
+#pragma unroll
+    for (int k = 0; k < 3; ++k) Ue[n][k] = Uc[n][k];
+  StaticFor<0, 4>::run([&](auto kc) {
+    constexpr int fn = face_node(FC, decltype(kc)::value);
+    double s[3];
+    load3(a.sideU, nd[fn], s);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) Ue[fn][k] = TF(s[k]);
+  });
+  // bilinear face shape at the face ip (identity when shifted)
+  TF muB;
+  if (USH) {
+    muB = mu[f0];
+  } else {
+    muB = TF(0.5625) * mu[f0] + TF(0.1875) * mu[f1] + TF(0.0625) * mu[f2] + TF(0.1875) * mu[f3];
+  }
+  const double amag = sqrt(Af[0] * Af[0] + Af[1] * Af[1] + Af[2] * Af[2]);
+  TF nx[3], ax[3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    nx[i] = TF(Af[i] / amag);
+    ax[i] = TF(Af[i]);
+  }
+  StaticFor<0, 8>::run([&](auto nc) {
+    constexpr int n = decltype(nc)::value;
+    if (!grad_is_zero<PT, n>()) {
+      constexpr bool on_face = (n == f0 || n == f1 || n == f2 || n == f3);
+      constexpr int sl = nb_slot(n);
+      double gd[3];
+      grad_n<PT, n>(J, gd);
+      TF g[3] = {TF(gd[0]), TF(gd[1]), TF(gd[2])};
+#pragma unroll
+      for (int j = 0; j < 3; ++j) {
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+          const TF om = TF(1) - nx[i] * nx[i];
+          TF lf = -muB * g[j] * ax[j] * om;
+          if (!on_face) {
+            if (sl < 0) diag[3 * i + i] += lf; else nb[sl][3 * i + i] += lf;
+          }
+          rhs[i] -= lf * Ue[n][i];
+          lf = -muB * g[i] * ax[j] * om;
+          if (!on_face) {
+            if (sl < 0) diag[3 * i + j] += lf; else nb[sl][3 * i + j] += lf;
+          }
+          rhs[i] -= lf * Ue[n][j];
+#pragma unroll
+          for (int l = 0; l < 3; ++l) {
+            if (l == i) continue;
+            const TF nil = nx[i] * nx[l];
+            lf = muB * g[j] * ax[j] * nil;
+            if (!on_face) {
+              if (sl < 0) diag[3 * i + l] += lf; else nb[sl][3 * i + l] += lf;
+            }
+            rhs[i] -= lf * Ue[n][l];
+            lf = muB * g[l] * ax[j] * nil;
+            if (!on_face) {
+              if (sl < 0) diag[3 * i + j] += lf; else nb[sl][3 * i + j] += lf;
+            }
+            rhs[i] -= lf * Ue[n][j];
+          }
+        }
+      }
+    }
+  });
+}
+
+template <bool USH, bool UGSH, class TF>
+__global__ void __launch_bounds__(BLOCK) k_momentum(MomArgs a) {
+  __shared__ TF sh_val[BLOCK * 3 * 9];
+  __shared__ int sh_col[BLOCK * 3];
+  const int lane = threadIdx.x & 31;
+  const int warp_base = threadIdx.x & ~31;
+  const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 3;
+  const int c = threadIdx.x & 7;
+  const bool rv = row < a.m.nn;
+  const int e = rv ? __ldg(a.m.n2e + 8 * row + c) : -1;
+  TF diag[9], nb[3][9], rhs[3];
+#pragma unroll
+  for (int k = 0; k < 9; ++k) {
+    diag[k] = TF(0);
+    nb[0][k] = nb[1][k] = nb[2][k] = TF(0);
+  }
+  rhs[0] = rhs[1] = rhs[2] = TF(0);
+  int nbc[3] = {-1, -1, -1};
+  if (e >= 0) {
+    const uint32_t pw = perm_word(c);
+    const uint32_t iw = ip_word(c);
+    double x[8][3];
+    int nd[8];
+    gather_x(a.m, e, pw, x, nd);
+    TF Uc[8][3], mu[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      double u[3];
+      load3(a.U, nd[k], u);
+      Uc[k][0] = TF(u[0]);
+      Uc[k][1] = TF(u[1]);
+      Uc[k][2] = TF(u[2]);
+      mu[k] = TF(__ldg(a.mu + nd[k]));
+    }
+    Corner0Points P;
+    corner0_points(x, P);
+    double Aq[3][3];
+    corner0_areas(P, Aq[0], Aq[1], Aq[2]);
+    int err = 0;
+    StaticFor<0, 3>::run([&](auto qc) {
+      constexpr int q = decltype(qc)::value;
+      constexpr int IP = q == 0 ? 0 : (q == 1 ? 3 : 8);
+      constexpr int R = q == 0 ? 1 : (q == 1 ? 3 : 4);
+      constexpr int RS = nb_slot(R);
+      using PG = ScsPt<IP, UGSH>;
+      using PV = ScsPt<IP, USH>;
+      const int pk = (iw >> (5 * q)) & 31;
+      const double tmd = (pk & 1) ? -__ldg(a.mDot + 12 * e + (pk >> 1)) : __ldg(a.mDot + 12 * e + (pk >> 1));
+      const TF tm = TF(tmd);
+      TF muIp = TF(0);
+      StaticFor<0, 8>::run([&](auto nc) {
+        constexpr int n = decltype(nc)::value;
+        constexpr double N = shape_at<PV, n>();
+        if (N != 0.0) muIp += TF(N) * mu[n];
+      });
+      // upwind advection (row L = corner 0)
+      const TF fl = TF(0.5) * (tm + fabs(tm));
+      const TF fr = TF(0.5) * (tm - fabs(tm));
+#pragma unroll
+      for (int i = 0; i < 3; ++i) {
+        const TF up = tmd > 0 ? Uc[0][i] : Uc[R][i];
+        rhs[i] -= tm * up;
+        diag[3 * i + i] += fl;
+        nb[RS][3 * i + i] += fr;
+      }
+      // viscous stress incl. transpose
+      const InvJac J = inv_jacobian<PG>(x, &err);
+      TF ax[3] = {TF(Aq[q][0]), TF(Aq[q][1]), TF(Aq[q][2])};
+      StaticFor<0, 8>::run([&](auto nc) {
+        constexpr int n = decltype(nc)::value;
+        if (!grad_is_zero<PG, n>()) {
+          constexpr int sl = nb_slot(n);
+          double gd[3];
+          grad_n<PG, n>(J, gd);
+          const TF g[3] = {TF(gd[0]), TF(gd[1]), TF(gd[2])};
+#pragma unroll
+          for (int i = 0; i < 3; ++i) {
+            TF lc = TF(0);
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+              lc += -muIp * g[j] * ax[j];
+              const TF fj = -muIp * g[i] * ax[j];
+              if (sl < 0) diag[3 * i + j] += fj; else nb[sl][3 * i + j] += fj;
+              rhs[i] -= fj * Uc[n][j];
+            }
+            if (sl < 0) diag[3 * i + i] += lc; else nb[sl][3 * i + i] += lc;
+            rhs[i] -= lc * Uc[n][i];
+          }
+        }
+      });
+    });
+    // no-slip wall faces touching this corner
+    const uint8_t fm = __ldg(a.m.face_mask + e);
+    if (fm) {
+      const uint32_t fw = face_word(c);
+      if (fm & (1u << ((fw >> 0) & 7))) wall_face<0, USH, UGSH, TF>(a, x, nd, Uc, mu, diag, nb, rhs, &err);
+      if (fm & (1u << ((fw >> 3) & 7))) wall_face<3, USH, UGSH, TF>(a, x, nd, Uc, mu, diag, nb, rhs, &err);
+      if (fm & (1u << ((fw >> 6) & 7))) wall_face<4, USH, UGSH, TF>(a, x, nd, Uc, mu, diag, nb, rhs, &err);
+    }
+    if (err) a.err[0] = 1;
+    nbc[0] = nd[1];
+    nbc[1] = nd[3];
+    nbc[2] = nd[4];
+  }
+#pragma unroll
+  for (int k = 0; k < 9; ++k) diag[k] = rowsum8(diag[k]);
+#pragma unroll
+  for (int k = 0; k < 3; ++k) rhs[k] = rowsum8(rhs[k]);
+  if (rv) {
+    // node terms, relaxation, wall rhs relaxation, DU
+    const double vol = __ldg(a.m.vol + row);
+    const double dv = __ldg(a.div + row);
+    const double rho = __ldg(a.rho + row);
+    const double lf = rho * vol / a.dt;
+    double un[3], gp[3];
+    load3(a.U, row, un);
+    load3(a.gradP, row, gp);
+    const bool wall = __ldg(a.m.wall_node + row) != 0;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      double d = double(diag[4 * k]);
+      if (dv < 0) d += -dv;
+      d += lf;
+      d *= a.urf_inv;
+      diag[4 * k] = TF(d);
+      double r = double(rhs[k]);
+      r -= -dv * un[k];
+      r -= gp[k] * vol;
+      if (wall) r *= a.wall_relax;
+      rhs[k] = TF(r);
+    }
+    if (c == 0) {
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        a.du[3 * row + k] = vol / (double(diag[4 * k]) + SMALL);
+        static_cast<TF*>(a.b)[3 * row + k] = rhs[k];
+      }
+    }
+  }
+  write_row<9, TF>(row, rv, c, lane, diag, nb, nbc, a.m, static_cast<TF*>(a.A),
+                   sh_val + warp_base * 3 * 9, sh_col + warp_base * 3, false);
+}
+
+// ---------------------------------------------------------------------------
+// Mass flow: element kernels over all 12 SCS ips.
+struct MdotArgs {
+  MeshView m;
+  const double *U, *p, *gradP, *du, *rho;
+  double* mDot;
+  double urf;
+  int init;
+  int* err;
+};
+
+// Full 27-point subdivision and 12 SCS area vectors (hex_scs_det).
+__device__ __forceinline__ void scs_areas_all(const double (&x)[8][3], double (&A)[12][3]) {
+  double p[27][3];
+#pragma unroll
+  for (int n = 0; n < 8; ++n)
+#pragma unroll
+    for (int k = 0; k < 3; ++k) p[n][k] = x[n][k];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    p[8][k] = 0.5 * (x[0][k] + x[1][k]);
+    p[9][k] = 0.5 * (x[1][k] + x[2][k]);
+    p[10][k] = 0.5 * (x[2][k] + x[3][k]);
+    p[11][k] = 0.5 * (x[3][k] + x[0][k]);
+    p[12][k] = 0.25 * (x[0][k] + x[1][k] + x[2][k] + x[3][k]);
+    p[13][k] = 0.5 * (x[4][k] + x[5][k]);
+    p[14][k] = 0.5 * (x[5][k] + x[6][k]);
+    p[15][k] = 0.5 * (x[6][k] + x[7][k]);
+    p[16][k] = 0.5 * (x[7][k] + x[4][k]);
+    p[17][k] = 0.25 * (x[4][k] + x[5][k] + x[6][k] + x[7][k]);
+    p[18][k] = 0.5 * (x[1][k] + x[5][k]);
+    p[19][k] = 0.5 * (x[0][k] + x[4][k]);
+    p[20][k] = 0.25 * (x[0][k] + x[1][k] + x[4][k] + x[5][k]);
+    p[21][k] = 0.5 * (x[3][k] + x[7][k]);
+    p[22][k] = 0.5 * (x[2][k] + x[6][k]);
+    p[23][k] = 0.25 * (x[2][k] + x[3][k] + x[6][k] + x[7][k]);
+    p[24][k] = 0.25 * (x[1][k] + x[2][k] + x[5][k] + x[6][k]);
+    p[25][k] = 0.25 * (x[0][k] + x[3][k] + x[4][k] + x[7][k]);
+    double s = 0.0;
+#pragma unroll
+    for (int n = 0; n < 8; ++n) s += x[n][k];
+    p[26][k] = 0.125 * s;
+  }
+  constexpr int Q[12][4] = {{20, 8, 12, 26},  {24, 9, 12, 26},  {10, 12, 26, 23}, {11, 25, 26, 12},
+                            {13, 20, 26, 17}, {17, 14, 24, 26}, {17, 15, 23, 26}, {16, 17, 26, 25},
+                            {19, 20, 26, 25}, {20, 18, 24, 26}, {22, 23, 26, 24}, {21, 25, 26, 23}};
+#pragma unroll
+  for (int ip = 0; ip < 12; ++ip) quad_area(p[Q[ip][0]], p[Q[ip][1]], p[Q[ip][2]], p[Q[ip][3]], A[ip]);
+}
+
+// initializeMassFlowRateInterior_ (flowModel.cpp:3303-3470) when init != 0,
+// otherwise updateMassFlowRateInterior_ (flowModel.cpp:5272-5687).
+template <bool USH, bool PGSH>
+__global__ void __launch_bounds__(BLOCK) k_mdot(MdotArgs a) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= a.m.ne) return;
+  double x[8][3];
+  int nd[8];
+  gather_x(a.m, e, perm_word(0), x, nd);
+  double A[12][3];
+  scs_areas_all(x, A);
+  double Gp[3] = {0.0, 0.0, 0.0}, pn[8];
+  if (!a.init) {
+#pragma unroll
+    for (int n = 0; n < 8; ++n) {
+      const double w = __ldg(a.m.wscv + 8 * e + n);
+      double gp[3];
+      load3(a.gradP, nd[n], gp);
+#pragma unroll
+      for (int j = 0; j < 3; ++j) Gp[j] += w * gp[j];
+      pn[n] = __ldg(a.p + nd[n]);
+    }
+  }
+  int err = 0;
+  StaticFor<0, 12>::run([&](auto ic) {
+    constexpr int IP = decltype(ic)::value;
+    using PV = ScsPt<IP, USH>;
+    using PG = ScsPt<IP, PGSH>;
+    double u[3] = {0, 0, 0}, duip[3] = {0, 0, 0}, rhoIp = 0.0;
+    StaticFor<0, 8>::run([&](auto nc) {
+      constexpr int n = decltype(nc)::value;
+      constexpr double N = shape_at<PV, n>();
+      if (N != 0.0) {
+        double un[3];
+        load3(a.U, nd[n], un);
+        rhoIp += N * __ldg(a.rho + nd[n]);
+#pragma unroll
+        for (int j = 0; j < 3; ++j) u[j] += N * un[j];
+        if (!a.init) {
+          double dn[3];
+          load3(a.du, nd[n], dn);
+#pragma unroll
+          for (int j = 0; j < 3; ++j) duip[j] += N * dn[j];
+        }
+      }
+    });
+    double m = 0.0;
+    if (a.init) {
+#pragma unroll
+      for (int j = 0; j < 3; ++j) m += rhoIp * u[j] * A[IP][j];
+      a.mDot[12 * e + IP] = m;
+    } else {
+      const InvJac J = inv_jacobian<PG>(x, &err);
+      double dp[3] = {0, 0, 0};
+      StaticFor<0, 8>::run([&](auto nc) {
+        constexpr int n = decltype(nc)::value;
+        if (!grad_is_zero<PG, n>()) {
+          double g[3];
+          grad_n<PG, n>(J, g);
+#pragma unroll
+          for (int j = 0; j < 3; ++j) dp[j] += g[j] * pn[n];
+        }
+      });
+      const double old = a.mDot[12 * e + IP];
+      const double tU = old / rhoIp;
+      const double rhoUp = tU > 0 ? __ldg(a.rho + nd[lr(IP, 0)]) : __ldg(a.rho + nd[lr(IP, 1)]);
+#pragma unroll
+      for (int j = 0; j < 3; ++j) {
+        m += rhoUp * u[j] * A[IP][j];
+        m -= rhoUp * duip[j] * (dp[j] - Gp[j]) * A[IP][j];
+      }
+      a.mDot[12 * e + IP] = a.urf * m + (1.0 - a.urf) * old;
+    }
+  });
+  if (err) a.err[0] = 1;
+}
+
+// ---------------------------------------------------------------------------
+// Divergence: div_n = sum of outgoing SCS mass flows (interior part of
+// updateMassDivergenceField_; wall side flows are zero).
+struct DivArgs {
+  MeshView m;
+  const double* mDot;
+  double* div;
+};
+
+__global__ void __launch_bounds__(BLOCK) k_div(DivArgs a) {
+  const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 3;
+  const int c = threadIdx.x & 7;
+  const bool rv = row < a.m.nn;
+  const int e = rv ? __ldg(a.m.n2e + 8 * row + c) : -1;
+  double s = 0.0;
+  if (e >= 0) {
+    const uint32_t iw = ip_word(c);
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      const int pk = (iw >> (5 * q)) & 31;
+      const double m = __ldg(a.mDot + 12 * e + (pk >> 1));
+      s += (pk & 1) ? -m : m;
+    }
+  }
+  s = rowsum8(s);
+  if (rv && c == 0) a.div[row] = s;
+}
+
+// ---------------------------------------------------------------------------
+// Green-Gauss nodal gradient with under-relaxation and incremental form
+// (nodeField::updateGradientField, nodeField.hpp:3253-3445 interior,
+// :4732-4930 boundary faces). NC = field components.
+struct GradArgs {
+  MeshView m;
+  const double* phi;
+  double* grad;
+  double gurf;
+};
+
+template <int NC, bool SH>
+__global__ void __launch_bounds__(BLOCK) k_gradient(GradArgs a) {
+  const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 3;
+  const int c = threadIdx.x & 7;
+  const bool rv = row < a.m.nn;
+  const int e = rv ? __ldg(a.m.n2e + 8 * row + c) : -1;
+  double acc[NC][3];
+#pragma unroll
+  for (int i = 0; i < NC; ++i) acc[i][0] = acc[i][1] = acc[i][2] = 0.0;
+  if (e >= 0) {
+    const uint32_t pw = perm_word(c);
+    double x[8][3];
+    int nd[8];
+    gather_x(a.m, e, pw, x, nd);
+    double ph[8][NC];
+#pragma unroll
+    for (int k = 0; k < 8; ++k)
+#pragma unroll
+      for (int i = 0; i < NC; ++i) ph[k][i] = __ldg(a.phi + NC * nd[k] + i);
+    Corner0Points P;
+    corner0_points(x, P);
+    double Aq[3][3];
+    corner0_areas(P, Aq[0], Aq[1], Aq[2]);
+    StaticFor<0, 3>::run([&](auto qc) {
+      constexpr int q = decltype(qc)::value;
+      constexpr int IP = q == 0 ? 0 : (q == 1 ? 3 : 8);
+      using PV = ScsPt<IP, SH>;
+      double pip[NC];
+#pragma unroll
+      for (int i = 0; i < NC; ++i) pip[i] = 0.0;
+      StaticFor<0, 8>::run([&](auto nc) {
+        constexpr int n = decltype(nc)::value;
+        constexpr double N = shape_at<PV, n>();
+        if (N != 0.0) {
+#pragma unroll
+          for (int i = 0; i < NC; ++i) pip[i] += N * ph[n][i];
+        }
+      });
+#pragma unroll
+      for (int i = 0; i < NC; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) acc[i][j] += (pip[i] - ph[0][i]) * Aq[q][j];
+    });
+    if (!SH) {
+      // boundary faces: bilinear face value at the face ip nearest the node
+      const uint8_t fm = __ldg(a.m.face_mask + e);
+      if (fm) {
+        const uint32_t fw = face_word(c);
+        StaticFor<0, 3>::run([&](auto qc) {
+          constexpr int q = decltype(qc)::value;
+          constexpr int FC = q == 0 ? 0 : (q == 1 ? 3 : 4);
+          if (fm & (1u << ((fw >> (3 * q)) & 7))) {
+            constexpr int f0 = face_node(FC, 0), f1 = face_node(FC, 1), f2 = face_node(FC, 2),
+                          f3 = face_node(FC, 3);
+            double Af[3];
+            face_area_at_first(x[f0], x[f1], x[f2], x[f3], Af);
+#pragma unroll
+            for (int i = 0; i < NC; ++i) {
+              const double pip = 0.5625 * ph[f0][i] + 0.1875 * ph[f1][i] + 0.0625 * ph[f2][i] +
+                                 0.1875 * ph[f3][i];
+#pragma unroll
+              for (int j = 0; j < 3; ++j) acc[i][j] += (pip - ph[0][i]) * Af[j];
+            }
+          }
+        });
+      }
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < NC; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j) acc[i][j] = rowsum8(acc[i][j]);
+  if (rv && c == 0) {
+    const double iv = 1.0 / __ldg(a.m.vol + row);
+#pragma unroll
+    for (int i = 0; i < NC; ++i)
+#pragma unroll
+      for (int j = 0; j < 3; ++j) {
+        const size_t k = (size_t)3 * NC * row + 3 * i + j;
+        a.grad[k] = (1.0 - a.gurf) * a.grad[k] + a.gurf * acc[i][j] * iv;
+      }
+  }
+}
+
+// U += sign * du * gradP / urf_p on all nodes (segregatedFlowEquations.cpp:134-278)
+__global__ void k_vel_correct(int n3, double* U, const double* du, const double* gradP, double f) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n3) U[i] += f * du[i] * gradP[i];
+}
+
+// ---------------------------------------------------------------------------
+// launchers
+static int grid_rows(int nn) { return (int)(((size_t)nn * 8 + BLOCK - 1) / BLOCK); }
+
+int launch_pcorr(Flow& f, bool mixed) {
+  PcArgs a{f.mesh->view(), f.U, f.p, f.gradP, f.du, f.mDot, f.rho, f.b.A_pc, f.b.b_pc, f.s.ref_node, f.err_dev};
+  const int g = grid_rows(f.mesh->nn);
+  const bool us = f.s.u_shifted, ps = f.s.p_grad_shifted;
+#define OA_PC(US, PS, T)                                                                    \
+  if (us == US && ps == PS) k_pcorr<US, PS, T><<<g, BLOCK, 0, f.stream>>>(a);
+  if (mixed) {
+    OA_PC(true, true, float) OA_PC(true, false, float) OA_PC(false, true, float) OA_PC(false, false, float)
+  } else {
+    OA_PC(true, true, double) OA_PC(true, false, double) OA_PC(false, true, double) OA_PC(false, false, double)
+  }
+#undef OA_PC
+  count_launches(1);
+  OA_CUDA(cudaGetLastError());
+  return OA_OK;
+}
+
+int launch_momentum(Flow& f, bool mixed) {
+  MomArgs a{f.mesh->view(), f.U, f.gradP, f.div, f.mDot, f.rho, f.mu, f.sideU, f.b.A_mom, f.b.b_mom, f.du,
+            f.s.dt, 1.0 / f.s.urf_u, f.s.wall_rhs_relax, f.err_dev};
+  const int g = grid_rows(f.mesh->nn);
+  const bool us = f.s.u_shifted, gs = f.s.u_grad_shifted;
+#define OA_MOM(US, GS, T)                                                                   \
+  if (us == US && gs == GS) k_momentum<US, GS, T><<<g, BLOCK, 0, f.stream>>>(a);
+  if (mixed) {
+    OA_MOM(true, true, float) OA_MOM(true, false, float) OA_MOM(false, true, float) OA_MOM(false, false, float)
+  } else {
+    OA_MOM(true, true, double) OA_MOM(true, false, double) OA_MOM(false, true, double) OA_MOM(false, false, double)
+  }
+#undef OA_MOM
+  count_launches(1);
+  OA_CUDA(cudaGetLastError());
+  return OA_OK;
+}
+
+static int launch_mdot_impl(Flow& f, int init) {
+  MdotArgs a{f.mesh->view(), f.U, f.p, f.gradP, f.du, f.rho, f.mDot, f.s.mdot_urf, init, f.err_dev};
+  const int g = (f.mesh->ne + BLOCK - 1) / BLOCK;
+  const bool us = f.s.u_shifted, ps = f.s.p_grad_shifted;
+  if (us && ps) k_mdot<true, true><<<g, BLOCK, 0, f.stream>>>(a);
+  else if (us && !ps) k_mdot<true, false><<<g, BLOCK, 0, f.stream>>>(a);
+  else if (!us && ps) k_mdot<false, true><<<g, BLOCK, 0, f.stream>>>(a);
+  else k_mdot<false, false><<<g, BLOCK, 0, f.stream>>>(a);
+  count_launches(1);
+  OA_CUDA(cudaGetLastError());
+  return OA_OK;
+}
+int launch_init_mdot(Flow& f) { return launch_mdot_impl(f, 1); }
+int launch_update_mdot(Flow& f) { return launch_mdot_impl(f, 0); }
+
+int launch_div(Flow& f) {
+  DivArgs a{f.mesh->view(), f.mDot, f.div};
+  k_div<<<grid_rows(f.mesh->nn), BLOCK, 0, f.stream>>>(a);
+  count_launches(1);
+  OA_CUDA(cudaGetLastError());
+  return OA_OK;
+}
+
+int launch_gradient(Flow& f, int which) {
+  const int g = grid_rows(f.mesh->nn);
+  if (which == 0) {
+    GradArgs a{f.mesh->view(), f.p, f.gradP, f.s.grad_urf};
+    if (f.s.p_shifted) k_gradient<1, true><<<g, BLOCK, 0, f.stream>>>(a);
+    else k_gradient<1, false><<<g, BLOCK, 0, f.stream>>>(a);
+  } else {
+    GradArgs a{f.mesh->view(), f.U, f.gradU, f.s.grad_urf};
+    if (f.s.u_shifted) k_gradient<3, true><<<g, BLOCK, 0, f.stream>>>(a);
+    else k_gradient<3, false><<<g, BLOCK, 0, f.stream>>>(a);
+  }
+  count_launches(1);
+  OA_CUDA(cudaGetLastError());
+  return OA_OK;
+}
+
+int launch_axpy_du_gradp(Flow& f, double sign) {
+  const int n3 = 3 * f.mesh->nn;
+  k_vel_correct<<<(n3 + 255) / 256, 256, 0, f.stream>>>(n3, f.U, f.du, f.gradP, sign / f.s.urf_p);
+  count_launches(1);
+  OA_CUDA(cudaGetLastError());
+  return OA_OK;
+}
+
+}  // namespace oa

@@ -1,0 +1,412 @@
+// Pressure-correction / momentum Krylov solve on the device: BiCGStab
+// (van der Vorst 1992) right-preconditioned by point or 3x3 block Jacobi.
+//
+// The reference hands its systems to liblinsolve (PETSc / Trilinos / HYPRE,
+// src/equation/linearSystem.h:416-462), which is absent from the reference
+// checkout; the algorithm here is the published one. All scalars live on the
+// device and every reduction is a fixed two-stage tree (block partials, then
+// an ordered single-block sum), so results are bitwise reproducible run to
+// run. A device "done" flag lets chunks of iterations be launched without
+// host round trips; kernels after convergence return immediately.
+#include <cuda_runtime.h>
+
+#include <cmath>
+
+#include "oa_internal.h"
+#include "oa_krylov.h"
+
+namespace oa {
+
+constexpr int KB = 256;        // threads per block for vector kernels
+constexpr int MAX_PARTIALS = 2048;
+
+struct KScal {
+  double rho, alpha, omega, bnorm, rnorm;
+  double d0, d1, d2;  // reduced dots of the current phase
+  int done, iters, status;
+};
+
+template <class T>
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// block-level fixed-order reduction of up to 3 values; thread 0 writes partials
+template <int NV>
+__device__ __forceinline__ void block_reduce_store(double (&v)[NV], double* partials, int nblocks_stride) {
+  __shared__ double sh[NV][KB / 32];
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+#pragma unroll
+  for (int k = 0; k < NV; ++k) {
+    double s = warp_sum<double>(v[k]);
+    if (l == 0) sh[k][w] = s;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int k = 0; k < NV; ++k) {
+      double s = 0.0;
+      for (int i = 0; i < KB / 32; ++i) s += sh[k][i];
+      partials[k * nblocks_stride + blockIdx.x] = s;
+    }
+  }
+}
+
+// ordered final sum of the partials by one block
+template <int NV>
+__device__ __forceinline__ void final_reduce(const double* partials, int nb, double (&out)[NV]) {
+  __shared__ double sh[NV][KB];
+#pragma unroll
+  for (int k = 0; k < NV; ++k) {
+    double s = 0.0;
+    for (int i = threadIdx.x; i < nb; i += KB) s += partials[k * MAX_PARTIALS + i];
+    sh[k][threadIdx.x] = s;
+  }
+  __syncthreads();
+  for (int st = KB / 2; st > 0; st >>= 1) {
+    if (threadIdx.x < st)
+#pragma unroll
+      for (int k = 0; k < NV; ++k) sh[k][threadIdx.x] += sh[k][threadIdx.x + st];
+    __syncthreads();
+  }
+#pragma unroll
+  for (int k = 0; k < NV; ++k) out[k] = sh[k][0];
+}
+
+// y = A x for a BSR matrix with BxB row-major blocks; optional partial dots
+// (y.w1, y.w2) with vectors of the same length.
+template <int B, class TM, class TV, int ND>
+__global__ void __launch_bounds__(KB) k_spmv(int nn, const int* __restrict__ rp, const int* __restrict__ cols,
+                                              const TM* __restrict__ A, const TV* __restrict__ x,
+                                              TV* __restrict__ y, const TV* __restrict__ w1,
+                                              const TV* __restrict__ w2, double* partials, const KScal* sc) {
+  if (sc && sc->done) return;
+  double v[ND > 0 ? ND : 1];
+#pragma unroll
+  for (int k = 0; k < (ND > 0 ? ND : 1); ++k) v[k] = 0.0;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nn * B; t += gridDim.x * blockDim.x) {
+    const int i = t / B, m = t - i * B;
+    double s = 0.0;
+    const int a = __ldg(rp + i), bnd = __ldg(rp + i + 1);
+    for (int k = a; k < bnd; ++k) {
+      const int j = __ldg(cols + k);
+#pragma unroll
+      for (int q = 0; q < B; ++q) s += double(A[(size_t)k * B * B + B * m + q]) * double(x[B * j + q]);
+    }
+    y[t] = TV(s);
+    if (ND > 0) v[0] += double(TV(s)) * double(w1[t]);
+    if (ND > 1) v[1] += double(TV(s)) * double(w2[t]);
+  }
+  if (ND > 0) block_reduce_store<ND>(reinterpret_cast<double(&)[ND]>(v), partials, MAX_PARTIALS);
+}
+
+// z = Minv v (point or 3x3 block Jacobi)
+template <int B, class TV>
+__global__ void k_prec(int nn, const double* __restrict__ Minv, const TV* __restrict__ v, TV* __restrict__ z,
+                       const KScal* sc) {
+  if (sc->done) return;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nn * B) return;
+  if (B == 1) {
+    z[t] = TV(Minv[t] * double(v[t]));
+  } else {
+    const int i = t / 3, m = t - 3 * i;
+    const double* M = Minv + 9 * (size_t)i + 3 * m;
+    z[t] = TV(M[0] * double(v[3 * i]) + M[1] * double(v[3 * i + 1]) + M[2] * double(v[3 * i + 2]));
+  }
+}
+
+template <int B, class TM>
+__global__ void k_build_minv(int nn, const int* __restrict__ rp, const int* __restrict__ dg, const TM* __restrict__ A,
+                             double* Minv) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nn) return;
+  const TM* d = A + (size_t)(rp[i] + dg[i]) * B * B;
+  if (B == 1) {
+    Minv[i] = 1.0 / double(d[0]);
+  } else {
+    double a[9];
+    for (int k = 0; k < 9; ++k) a[k] = double(d[k]);
+    const double det = a[0] * (a[4] * a[8] - a[5] * a[7]) - a[1] * (a[3] * a[8] - a[5] * a[6]) +
+                       a[2] * (a[3] * a[7] - a[4] * a[6]);
+    const double id = 1.0 / det;
+    double* r = Minv + 9 * (size_t)i;
+    r[0] = (a[4] * a[8] - a[5] * a[7]) * id;
+    r[1] = (a[2] * a[7] - a[1] * a[8]) * id;
+    r[2] = (a[1] * a[5] - a[2] * a[4]) * id;
+    r[3] = (a[5] * a[6] - a[3] * a[8]) * id;
+    r[4] = (a[0] * a[8] - a[2] * a[6]) * id;
+    r[5] = (a[2] * a[3] - a[0] * a[5]) * id;
+    r[6] = (a[3] * a[7] - a[4] * a[6]) * id;
+    r[7] = (a[1] * a[6] - a[0] * a[7]) * id;
+    r[8] = (a[0] * a[4] - a[1] * a[3]) * id;
+  }
+}
+
+// init: x = 0, r = rh = b, p = v = 0; partial ||b||^2
+template <class TV, class TB>
+__global__ void __launch_bounds__(KB) k_init(int n, const TB* __restrict__ b, TV* x, TV* r, TV* rh, TV* p, TV* v,
+                                              double* partials) {
+  double s[1] = {0.0};
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+    const TV bv = TV(b[t]);
+    x[t] = TV(0);
+    r[t] = bv;
+    rh[t] = bv;
+    p[t] = TV(0);
+    v[t] = TV(0);
+    s[0] += double(bv) * double(bv);
+  }
+  block_reduce_store<1>(s, partials, MAX_PARTIALS);
+}
+
+__global__ void __launch_bounds__(KB) k_init_scalars(KScal* sc, const double* partials, int nb, double rtol) {
+  double o[1];
+  final_reduce<1>(partials, nb, o);
+  if (threadIdx.x == 0) {
+    sc->bnorm = sqrt(o[0]);
+    sc->rnorm = sc->bnorm;
+    sc->rho = sc->alpha = sc->omega = 1.0;
+    sc->d0 = o[0];  // rh.r for the first iteration equals ||b||^2
+    sc->iters = 0;
+    sc->status = 0;
+    sc->done = (sc->bnorm == 0.0 || !(sc->bnorm < INFINITY)) ? 1 : 0;
+    if (!(sc->bnorm < INFINITY)) sc->status = 2;
+  }
+}
+
+// p = r + beta (p - omega v), beta = (rho1/rho)(alpha/omega), rho1 = sc->d0
+template <class TV>
+__global__ void k_p_update(int n, TV* p, const TV* r, const TV* v, const KScal* sc) {
+  if (sc->done) return;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const double beta = (sc->d0 / sc->rho) * (sc->alpha / sc->omega);
+  p[t] = TV(double(r[t]) + beta * (double(p[t]) - sc->omega * double(v[t])));
+}
+
+// alpha = rho1 / (rh.v)
+__global__ void __launch_bounds__(KB) k_alpha(KScal* sc, const double* partials, int nb) {
+  if (sc->done) return;
+  double o[1];
+  final_reduce<1>(partials, nb, o);
+  if (threadIdx.x == 0) {
+    if (o[0] == 0.0 || !(fabs(o[0]) < INFINITY)) {
+      sc->done = 1;
+      sc->status = 1;
+      return;
+    }
+    sc->alpha = sc->d0 / o[0];
+  }
+}
+
+// s = r - alpha v (stored in r)
+template <class TV>
+__global__ void k_s_update(int n, TV* r, const TV* v, const KScal* sc) {
+  if (sc->done) return;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  r[t] = TV(double(r[t]) - sc->alpha * double(v[t]));
+}
+
+// omega = (t.s)/(t.t)
+__global__ void __launch_bounds__(KB) k_omega(KScal* sc, const double* partials, int nb) {
+  if (sc->done) return;
+  double o[2];
+  final_reduce<2>(partials, nb, o);
+  if (threadIdx.x == 0) sc->omega = o[1] > 0.0 ? o[0] / o[1] : 0.0;
+}
+
+// x += alpha ph + omega sh; r = s - omega t; partials r.r, rh.r
+template <class TV>
+__global__ void __launch_bounds__(KB) k_x_update(int n, TV* x, TV* r, const TV* ph, const TV* sh, const TV* t,
+                                                  const TV* rh, double* partials, const KScal* sc) {
+  if (sc->done) return;
+  double v[2] = {0.0, 0.0};
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    x[i] = TV(double(x[i]) + sc->alpha * double(ph[i]) + sc->omega * double(sh[i]));
+    const TV rn = TV(double(r[i]) - sc->omega * double(t[i]));
+    r[i] = rn;
+    v[0] += double(rn) * double(rn);
+    v[1] += double(rh[i]) * double(rn);
+  }
+  block_reduce_store<2>(v, partials, MAX_PARTIALS);
+}
+
+// rho <- rho1; rho1 <- rh.r; convergence test
+__global__ void __launch_bounds__(KB) k_end_iter(KScal* sc, const double* partials, int nb, double rtol, int maxit) {
+  if (sc->done) return;
+  double o[2];
+  final_reduce<2>(partials, nb, o);
+  if (threadIdx.x == 0) {
+    sc->rho = sc->d0;
+    sc->d0 = o[1];
+    sc->rnorm = sqrt(o[0]);
+    sc->iters += 1;
+    if (!(sc->rnorm < INFINITY)) {
+      sc->done = 1;
+      sc->status = 2;
+    } else if (sc->rnorm <= rtol * sc->bnorm || sc->iters >= maxit) {
+      sc->done = 1;
+    } else if (sc->omega == 0.0 || sc->d0 == 0.0) {
+      sc->done = 1;
+      sc->status = 1;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+template <int B, class TM, class TV>
+int KrylovSolver<B, TM, TV>::setup(int nn_, const int* rp_, const int* cols_, const int* dg_, cudaStream_t st_) {
+  if (nn == nn_ && rp == rp_) return OA_OK;
+  release();
+  nn = nn_;
+  rp = rp_;
+  cols = cols_;
+  dg = dg_;
+  st = st_;
+  const size_t n = (size_t)B * nn;
+  for (int k = 0; k < 8; ++k) OA_CUDA(cudaMalloc(&vec[k], sizeof(TV) * n));
+  OA_CUDA(cudaMalloc(&Minv, sizeof(double) * (size_t)B * B * nn));
+  OA_CUDA(cudaMalloc(&partials, sizeof(double) * 3 * MAX_PARTIALS));
+  OA_CUDA(cudaMalloc(&scal, sizeof(KScal)));
+  OA_CUDA(cudaMallocHost(&hscal, sizeof(KScal)));
+  return OA_OK;
+}
+
+template <int B, class TM, class TV>
+void KrylovSolver<B, TM, TV>::release() {
+  for (auto& v : vec) {
+    if (v) cudaFree(v);
+    v = nullptr;
+  }
+  if (Minv) cudaFree(Minv);
+  if (partials) cudaFree(partials);
+  if (scal) cudaFree(scal);
+  if (hscal) cudaFreeHost(hscal);
+  Minv = nullptr;
+  partials = nullptr;
+  scal = nullptr;
+  hscal = nullptr;
+  nn = 0;
+  rp = nullptr;
+}
+
+template <int B, class TM, class TV>
+template <class TB>
+int KrylovSolver<B, TM, TV>::solve(const TM* A, const TB* b, TV*& xout, double rtol, int maxit, int* iters,
+                                   double* res, int check_every) {
+  const int n = B * nn;
+  // work vectors: x r rh p v ph sh t
+  TV *x = static_cast<TV*>(vec[0]), *r = static_cast<TV*>(vec[1]), *rh = static_cast<TV*>(vec[2]),
+     *p = static_cast<TV*>(vec[3]), *v = static_cast<TV*>(vec[4]), *ph = static_cast<TV*>(vec[5]),
+     *sh = static_cast<TV*>(vec[6]), *t = static_cast<TV*>(vec[7]);
+  KScal* sc = static_cast<KScal*>(scal);
+  const int gfull = (n + KB - 1) / KB;                 // element-wise kernels
+  const int gv = gfull < MAX_PARTIALS ? gfull : MAX_PARTIALS;  // reducing kernels (grid-stride)
+  const int gr = (nn + KB - 1) / KB;
+  k_build_minv<B, TM><<<gr, KB, 0, st>>>(nn, rp, dg, A, Minv);
+  k_init<TV, TB><<<gv, KB, 0, st>>>(n, b, x, r, rh, p, v, partials);
+  k_init_scalars<<<1, KB, 0, st>>>(sc, partials, gv, rtol);
+  count_launches(3);
+  OA_CUDA(cudaGetLastError());
+  int done_iters = 0;
+  while (true) {
+    for (int it = 0; it < check_every; ++it) {
+      k_p_update<TV><<<gfull, KB, 0, st>>>(n, p, r, v, sc);
+      k_prec<B, TV><<<gfull, KB, 0, st>>>(nn, Minv, p, ph, sc);
+      k_spmv<B, TM, TV, 1><<<gv, KB, 0, st>>>(nn, rp, cols, A, ph, v, rh, nullptr, partials, sc);
+      k_alpha<<<1, KB, 0, st>>>(sc, partials, gv);
+      k_s_update<TV><<<gfull, KB, 0, st>>>(n, r, v, sc);
+      k_prec<B, TV><<<gfull, KB, 0, st>>>(nn, Minv, r, sh, sc);
+      k_spmv<B, TM, TV, 2><<<gv, KB, 0, st>>>(nn, rp, cols, A, sh, t, r, t, partials, sc);
+      k_omega<<<1, KB, 0, st>>>(sc, partials, gv);
+      k_x_update<TV><<<gv, KB, 0, st>>>(n, x, r, ph, sh, t, rh, partials, sc);
+      k_end_iter<<<1, KB, 0, st>>>(sc, partials, gv, rtol, maxit);
+    }
+    count_launches(10L * check_every);
+    OA_CUDA(cudaGetLastError());
+    done_iters += check_every;
+    OA_CUDA(cudaMemcpyAsync(hscal, sc, sizeof(KScal), cudaMemcpyDeviceToHost, st));
+    OA_CUDA(cudaStreamSynchronize(st));
+    const KScal* h = static_cast<const KScal*>(hscal);
+    if (h->done || done_iters >= maxit) break;
+  }
+  const KScal* h = static_cast<const KScal*>(hscal);
+  if (iters) *iters = h->iters;
+  if (res) *res = h->bnorm > 0 ? h->rnorm / h->bnorm : 0.0;
+  xout = x;
+  if (h->status == 2) return fail(OA_ERR_SOLVER, "BiCGStab: non-finite residual");
+  return OA_OK;
+}
+
+template struct KrylovSolver<1, double, double>;
+template struct KrylovSolver<3, double, double>;
+template struct KrylovSolver<1, float, float>;
+template struct KrylovSolver<3, float, float>;
+template int KrylovSolver<1, double, double>::solve<double>(const double*, const double*, double*&, double, int, int*, double*, int);
+template int KrylovSolver<3, double, double>::solve<double>(const double*, const double*, double*&, double, int, int*, double*, int);
+template int KrylovSolver<1, float, float>::solve<double>(const float*, const double*, float*&, double, int, int*, double*, int);
+template int KrylovSolver<1, float, float>::solve<float>(const float*, const float*, float*&, double, int, int*, double*, int);
+template int KrylovSolver<3, float, float>::solve<float>(const float*, const float*, float*&, double, int, int*, double*, int);
+
+// ---------------------------------------------------------------------------
+// FP64 residual for iterative refinement: r = b - A x (A in its stored
+// precision, arithmetic in FP64), with partial ||r||^2.
+template <class TM>
+__global__ void __launch_bounds__(KB) k_residual(int nn, const int* __restrict__ rp, const int* __restrict__ cols,
+                                                  const TM* __restrict__ A, const double* __restrict__ x,
+                                                  const double* __restrict__ b, double* __restrict__ r,
+                                                  double* partials) {
+  double v[1] = {0.0};
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nn; i += gridDim.x * blockDim.x) {
+    double s = 0.0;
+    for (int k = rp[i]; k < rp[i + 1]; ++k) s += double(A[k]) * x[cols[k]];
+    const double ri = b[i] - s;
+    r[i] = ri;
+    v[0] += ri * ri;
+  }
+  block_reduce_store<1>(v, partials, MAX_PARTIALS);
+}
+
+__global__ void __launch_bounds__(KB) k_norm_out(const double* partials, int nb, double* out) {
+  double o[1];
+  final_reduce<1>(partials, nb, o);
+  if (threadIdx.x == 0) *out = sqrt(o[0]);
+}
+
+template <class TV>
+__global__ void k_add_correction(int n, double* x, const TV* d) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) x[i] += double(d[i]);
+}
+
+template <class TM>
+int fp64_residual(int nn, const int* rp, const int* cols, const TM* A, const double* x, const double* b, double* r,
+                  double* partials, double* norm_dev, cudaStream_t st) {
+  const int gf = (nn + KB - 1) / KB;
+  const int g = gf < MAX_PARTIALS ? gf : MAX_PARTIALS;
+  k_residual<TM><<<g, KB, 0, st>>>(nn, rp, cols, A, x, b, r, partials);
+  k_norm_out<<<1, KB, 0, st>>>(partials, g, norm_dev);
+  count_launches(2);
+  OA_CUDA(cudaGetLastError());
+  return OA_OK;
+}
+template int fp64_residual<float>(int, const int*, const int*, const float*, const double*, const double*, double*,
+                                  double*, double*, cudaStream_t);
+template int fp64_residual<double>(int, const int*, const int*, const double*, const double*, const double*, double*,
+                                   double*, double*, cudaStream_t);
+
+template <class TV>
+int add_correction(int n, double* x, const TV* d, cudaStream_t st) {
+  k_add_correction<TV><<<(n + KB - 1) / KB, KB, 0, st>>>(n, x, d);
+  count_launches(1);
+  OA_CUDA(cudaGetLastError());
+  return OA_OK;
+}
+template int add_correction<float>(int, double*, const float*, cudaStream_t);
+template int add_correction<double>(int, double*, const double*, cudaStream_t);
+
+}  // namespace oa

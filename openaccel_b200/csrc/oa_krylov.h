@@ -1,0 +1,36 @@
+// Device Krylov solver interface (internal).
+#pragma once
+#include <cuda_runtime.h>
+
+namespace oa {
+
+// BiCGStab on a BSR matrix with BxB blocks; matrix values TM, vectors TV.
+template <int B, class TM, class TV>
+struct KrylovSolver {
+  int nn = 0;
+  const int *rp = nullptr, *cols = nullptr, *dg = nullptr;
+  cudaStream_t st = nullptr;
+  void* vec[8] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+  double* Minv = nullptr;
+  double* partials = nullptr;
+  void* scal = nullptr;
+  void* hscal = nullptr;
+
+  int setup(int nn, const int* rp, const int* cols, const int* dg, cudaStream_t st);
+  void release();
+  ~KrylovSolver() { release(); }
+  // Solve A x = b from x0 = 0; xout points at the solver-owned solution.
+  template <class TB>
+  int solve(const TM* A, const TB* b, TV*& xout, double rtol, int maxit, int* iters, double* res,
+            int check_every);
+};
+
+// r = b - A x in FP64 arithmetic (A scalar CSR in its stored precision);
+// ||r|| written to norm_dev.
+template <class TM>
+int fp64_residual(int nn, const int* rp, const int* cols, const TM* A, const double* x, const double* b, double* r,
+                  double* partials, double* norm_dev, cudaStream_t st);
+template <class TV>
+int add_correction(int n, double* x, const TV* d, cudaStream_t st);
+
+}  // namespace oa

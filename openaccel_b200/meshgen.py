@@ -1,0 +1,151 @@
+"""Seeded synthetic meshes and initial fields for the CVFEM flow workloads.
+
+The reference reads Exodus meshes through STK; the workloads here are
+generated in memory with the same element/face conventions:
+
+* hex8 node ordering and face ordinals follow the Nalu hex8 master element
+  (``external/nalu/src/master_element/Hex8CVFEM.C:415-422``): element
+  ``(i, j, k)`` has nodes ``(i,j,k), (i+1,j,k), (i+1,j+1,k), (i,j+1,k)`` and the
+  same four at ``k+1``; faces 0..5 are y-, x+, y+, x-, z-, z+.
+* nodes are numbered lexicographically, ``id = i + (nx+1)*(j + (ny+1)*k)``,
+  so CSR columns sorted by node id run -z, -y, -x, self, +x, +y, +z.
+* boundary faces carry a boundary index; node-side Dirichlet values are
+  applied boundary by boundary in index order, so nodes shared by two
+  boundaries keep the value of the later one (the reference sets node-side
+  fields part by part, ``nodeField.hpp:1224-1300``).
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+
+import numpy as np
+
+# hex8 face ordinal -> element-local nodes (outward orientation)
+HEX_FACE_NODES = np.array(
+    [[0, 1, 5, 4], [1, 2, 6, 5], [2, 3, 7, 6], [0, 4, 7, 3], [0, 3, 2, 1], [4, 5, 6, 7]],
+    dtype=np.int32,
+)
+
+
+@dataclass
+class HexMesh:
+    """Unstructured view of a logically structured hex8 block."""
+
+    nx: int
+    ny: int
+    nz: int
+    coords: np.ndarray  # (nn, 3) float64
+    conn: np.ndarray  # (ne, 8) int32
+    face_elem: np.ndarray  # (nf,) int32
+    face_ord: np.ndarray  # (nf,) int32
+    face_bnd: np.ndarray  # (nf,) int32
+    bnd_velocity: np.ndarray  # (nbnd, 3) float64 (no-slip wall velocity)
+    meta: dict = field(default_factory=dict)
+
+    @property
+    def nn(self) -> int:
+        return self.coords.shape[0]
+
+    @property
+    def ne(self) -> int:
+        return self.conn.shape[0]
+
+    @property
+    def nf(self) -> int:
+        return self.face_elem.shape[0]
+
+
+def _node_id(i, j, k, nx, ny):
+    return i + (nx + 1) * (j + (ny + 1) * k)
+
+
+def hex_block(nx, ny, nz, x1d=None, y1d=None, z1d=None):
+    """Nodes and connectivity of an nx*ny*nz hex8 block (lexicographic ids)."""
+    x1d = np.linspace(0.0, 1.0, nx + 1) if x1d is None else np.asarray(x1d, np.float64)
+    y1d = np.linspace(0.0, 1.0, ny + 1) if y1d is None else np.asarray(y1d, np.float64)
+    z1d = np.linspace(0.0, 1.0, nz + 1) if z1d is None else np.asarray(z1d, np.float64)
+    Z, Y, X = np.meshgrid(z1d, y1d, x1d, indexing="ij")
+    coords = np.stack([X.ravel(), Y.ravel(), Z.ravel()], axis=1).astype(np.float64)
+    k, j, i = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+    i, j, k = i.ravel(), j.ravel(), k.ravel()
+    n0 = _node_id(i, j, k, nx, ny)
+    sx, sy = 1, nx + 1
+    sz = (nx + 1) * (ny + 1)
+    conn = np.stack(
+        [n0, n0 + sx, n0 + sx + sy, n0 + sy, n0 + sz, n0 + sz + sx, n0 + sz + sx + sy, n0 + sz + sy],
+        axis=1,
+    ).astype(np.int32)
+    return coords, conn
+
+
+def _elem_id(i, j, k, nx, ny):
+    return i + nx * (j + ny * k)
+
+
+def block_faces(nx, ny, nz):
+    """All boundary faces of the block as (elem, ordinal, side) with side in
+    {'x-','x+','y-','y+','z-','z+'}, in a fixed order (side, then element id)."""
+    out = {}
+    a, b = np.meshgrid(np.arange(ny), np.arange(nz), indexing="ij")  # j,k for x faces
+    out["x-"] = (_elem_id(0, a, b, nx, ny).ravel(), 3)
+    out["x+"] = (_elem_id(nx - 1, a, b, nx, ny).ravel(), 1)
+    a, b = np.meshgrid(np.arange(nx), np.arange(nz), indexing="ij")
+    out["y-"] = (_elem_id(a, 0, b, nx, ny).ravel(), 0)
+    out["y+"] = (_elem_id(a, ny - 1, b, nx, ny).ravel(), 2)
+    a, b = np.meshgrid(np.arange(nx), np.arange(ny), indexing="ij")
+    out["z-"] = (_elem_id(a, b, 0, nx, ny).ravel(), 4)
+    out["z+"] = (_elem_id(a, b, nz - 1, nx, ny).ravel(), 5)
+    return {s: (np.sort(e).astype(np.int32), o) for s, (e, o) in out.items()}
+
+
+def cavity(n, perturb=0.0, seed=12345, lid_velocity=(1.0, 0.0, 0.0)):
+    """Lid-driven cavity on the unit cube with n^3 hex8 elements.
+
+    Boundary 0 is the lid (z = 1) moving with ``lid_velocity``; boundary 1 is
+    the other five no-slip faces. Boundary 1 is applied last, so the lid's edge
+    nodes carry zero wall velocity (the cavity example lists the lid first).
+    ``perturb`` displaces interior nodes by U(-perturb*h, perturb*h) per
+    coordinate (numpy PCG64 stream ``seed``).
+    """
+    coords, conn = hex_block(n, n, n)
+    if perturb > 0.0:
+        h = 1.0 / n
+        rng = np.random.Generator(np.random.PCG64(seed))
+        noise = rng.uniform(-perturb * h, perturb * h, size=coords.shape)
+        idx = np.arange(coords.shape[0])
+        i = idx % (n + 1)
+        j = (idx // (n + 1)) % (n + 1)
+        k = idx // ((n + 1) * (n + 1))
+        interior = (i > 0) & (i < n) & (j > 0) & (j < n) & (k > 0) & (k < n)
+        coords[interior] += noise[interior]
+    faces = block_faces(n, n, n)
+    fe, fo, fb = [], [], []
+    for side in ["z+"]:
+        e, o = faces[side]
+        fe.append(e), fo.append(np.full_like(e, o)), fb.append(np.zeros_like(e))
+    for side in ["x-", "x+", "y-", "y+", "z-"]:
+        e, o = faces[side]
+        fe.append(e), fo.append(np.full_like(e, o)), fb.append(np.ones_like(e))
+    bnd_velocity = np.array([list(lid_velocity), [0.0, 0.0, 0.0]], dtype=np.float64)
+    return HexMesh(
+        n, n, n, coords, conn,
+        np.concatenate(fe).astype(np.int32), np.concatenate(fo).astype(np.int32),
+        np.concatenate(fb).astype(np.int32), bnd_velocity,
+        meta={"kind": "cavity", "n": n, "perturb": perturb, "seed": seed},
+    )
+
+
+def initial_velocity(mesh: HexMesh, sigma=0.0, seed=12345):
+    """Zero, or seeded Gaussian N(0, sigma^2) on interior nodes (walls keep 0)."""
+    U = np.zeros((mesh.nn, 3), dtype=np.float64)
+    if sigma > 0.0:
+        rng = np.random.Generator(np.random.PCG64(seed + 1))
+        g = rng.normal(0.0, sigma, size=U.shape)
+        nx, ny, nz = mesh.nx, mesh.ny, mesh.nz
+        idx = np.arange(mesh.nn)
+        i = idx % (nx + 1)
+        j = (idx // (nx + 1)) % (ny + 1)
+        k = idx // ((nx + 1) * (ny + 1))
+        interior = (i > 0) & (i < nx) & (j > 0) & (j < ny) & (k > 0) & (k < nz)
+        U[interior] = g[interior]
+    return U

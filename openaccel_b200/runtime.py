@@ -1,0 +1,271 @@
+"""ctypes binding of the C-ABI in ``include/openaccel_b200.h``.
+
+There is no CPU fallback: if ``_lib/libopenaccel_b200.so`` is missing or cannot
+be loaded, every entry point raises. ``OpenAccelError`` carries the library's
+status code and ``oa_last_error()`` message, the counterpart of the reference's
+``errorMsg`` -> ``std::runtime_error`` convention (src/basic/macros.cpp:21-24).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_lib", "libopenaccel_b200.so")
+
+OA_TOPO_HEX8 = 8
+OA_TOPO_TET4 = 4
+OA_PREC_FP64 = 0
+OA_PREC_MIXED = 1
+
+# every symbol the header declares; checked by tests on CPU
+EXPORTS = [
+    "oa_last_error", "oa_version", "oa_mesh_create", "oa_mesh_destroy", "oa_mesh_nnz", "oa_mesh_graph",
+    "oa_mesh_dual_volume", "oa_flow_create", "oa_flow_destroy", "oa_flow_set_field", "oa_flow_get_field",
+    "oa_flow_field_device_ptr", "oa_flow_initialize", "oa_assemble_momentum", "oa_assemble_pcorr",
+    "oa_update_mdot", "oa_update_div", "oa_update_gradient", "oa_solve", "oa_simple_iterate", "oa_flow_sync",
+    "oa_flow_stream", "oa_launch_count", "oa_time_kernel",
+]
+
+
+class OpenAccelError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"openaccel_b200 status {status}: {msg}")
+        self.status = status
+
+
+class FlowSettings(C.Structure):
+    _fields_ = [
+        ("rho", C.c_double), ("mu", C.c_double), ("urf_u", C.c_double), ("urf_p", C.c_double),
+        ("dt", C.c_double), ("grad_urf", C.c_double), ("mdot_urf", C.c_double),
+        ("wall_rhs_relax", C.c_double), ("u_shifted", C.c_int), ("u_grad_shifted", C.c_int),
+        ("p_shifted", C.c_int), ("p_grad_shifted", C.c_int), ("ref_node", C.c_int),
+        ("mom_maxit", C.c_int), ("mom_rtol", C.c_double), ("pc_maxit", C.c_int), ("pc_rtol", C.c_double),
+        ("precision", C.c_int),
+    ]
+
+
+class IterStats(C.Structure):
+    _fields_ = [
+        ("mom_iters", C.c_int), ("pc_iters", C.c_int), ("pc_refinements", C.c_int),
+        ("mom_res", C.c_double), ("pc_res", C.c_double), ("continuity_rms", C.c_double),
+    ]
+
+
+def default_settings(**kw) -> FlowSettings:
+    """Cavity-example defaults (examples/cavity/input.i: urf 0.9 / 0.1, physical
+    timescale 1, linear_linear interpolation, pressure level at node 0) and the
+    controls.h defaults (gradient urf 0.5625, relaxMass 1)."""
+    d = dict(rho=1.0, mu=0.01, urf_u=0.9, urf_p=0.1, dt=1.0, grad_urf=0.5625, mdot_urf=1.0,
+             wall_rhs_relax=0.75, u_shifted=1, u_grad_shifted=1, p_shifted=1, p_grad_shifted=1,
+             ref_node=0, mom_maxit=200, mom_rtol=1e-6, pc_maxit=5000, pc_rtol=1e-8,
+             precision=OA_PREC_FP64)
+    d.update(kw)
+    return FlowSettings(**d)
+
+
+_lib = None
+
+
+def lib():
+    """Load the CUDA library (raises if it is absent: no fallback path)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise OpenAccelError(-1, f"CUDA library not built: {LIB_PATH} (run python -m openaccel_b200.build)")
+    L = C.CDLL(LIB_PATH)
+    P = C.POINTER
+    dp, ip, vp = P(C.c_double), P(C.c_int), C.c_void_p
+    sig = {
+        "oa_last_error": (C.c_char_p, []),
+        "oa_version": (C.c_char_p, []),
+        "oa_mesh_create": (C.c_int, [dp, C.c_int, ip, C.c_int, C.c_int, ip, ip, ip, C.c_int, P(vp)]),
+        "oa_mesh_destroy": (None, [vp]),
+        "oa_mesh_nnz": (C.c_int, [vp, ip]),
+        "oa_mesh_graph": (C.c_int, [vp, ip, ip]),
+        "oa_mesh_dual_volume": (C.c_int, [vp, dp]),
+        "oa_flow_create": (C.c_int, [vp, P(FlowSettings), dp, C.c_int, P(vp)]),
+        "oa_flow_destroy": (None, [vp]),
+        "oa_flow_set_field": (C.c_int, [vp, C.c_char_p, dp, C.c_long]),
+        "oa_flow_get_field": (C.c_int, [vp, C.c_char_p, dp, C.c_long]),
+        "oa_flow_field_device_ptr": (C.c_int, [vp, C.c_char_p, P(dp)]),
+        "oa_flow_initialize": (C.c_int, [vp]),
+        "oa_assemble_momentum": (C.c_int, [vp, dp, dp]),
+        "oa_assemble_pcorr": (C.c_int, [vp, dp, dp]),
+        "oa_update_mdot": (C.c_int, [vp]),
+        "oa_update_div": (C.c_int, [vp]),
+        "oa_update_gradient": (C.c_int, [vp, C.c_int]),
+        "oa_solve": (C.c_int, [vp, C.c_int, C.c_double, C.c_int, dp, ip, dp]),
+        "oa_simple_iterate": (C.c_int, [vp, C.c_int, P(IterStats)]),
+        "oa_flow_sync": (C.c_int, [vp]),
+        "oa_flow_stream": (C.c_int, [vp, P(vp)]),
+        "oa_launch_count": (C.c_int, [P(C.c_longlong)]),
+        "oa_time_kernel": (C.c_int, [vp, C.c_int, C.c_int, dp]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = L
+    return L
+
+
+def launch_count() -> int:
+    n = C.c_longlong()
+    _check(lib().oa_launch_count(C.byref(n)))
+    return n.value
+
+
+def _check(status: int):
+    if status != 0:
+        raise OpenAccelError(status, lib().oa_last_error().decode())
+
+
+def _dp(a):
+    return None if a is None else a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def _ip(a):
+    return a.ctypes.data_as(C.POINTER(C.c_int))
+
+
+class Mesh:
+    """Device mesh (oa_mesh_create) from a ``meshgen.HexMesh``-like object."""
+
+    def __init__(self, mesh):
+        self.src = mesh
+        self.nn, self.ne = int(mesh.coords.shape[0]), int(mesh.conn.shape[0])
+        x = np.ascontiguousarray(mesh.coords, np.float64)
+        conn = np.ascontiguousarray(mesh.conn, np.int32)
+        fe = np.ascontiguousarray(mesh.face_elem, np.int32)
+        fo = np.ascontiguousarray(mesh.face_ord, np.int32)
+        fb = np.ascontiguousarray(mesh.face_bnd, np.int32)
+        h = C.c_void_p()
+        _check(lib().oa_mesh_create(_dp(x), self.nn, _ip(conn), self.ne, OA_TOPO_HEX8, _ip(fe), _ip(fo),
+                                    _ip(fb), int(fe.shape[0]), C.byref(h)))
+        self.h = h
+        n = C.c_int()
+        _check(lib().oa_mesh_nnz(self.h, C.byref(n)))
+        self.nnz = n.value
+
+    def graph(self):
+        rp = np.zeros(self.nn + 1, np.int32)
+        cols = np.zeros(self.nnz, np.int32)
+        _check(lib().oa_mesh_graph(self.h, _ip(rp), _ip(cols)))
+        return rp, cols
+
+    def dual_volume(self):
+        v = np.zeros(self.nn)
+        _check(lib().oa_mesh_dual_volume(self.h, _dp(v)))
+        return v
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().oa_mesh_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Flow:
+    """Segregated laminar flow state on the device (oa_flow_create)."""
+
+    FIELD_SHAPES = {"U": 3, "p": 1, "gradU": 9, "gradP": 3, "du": 3, "div": 1, "sideU": 3, "rho": 1, "mu": 1}
+
+    def __init__(self, mesh: Mesh, settings: FlowSettings | None = None):
+        self.mesh = mesh
+        self.settings = settings or default_settings()
+        bv = np.ascontiguousarray(mesh.src.bnd_velocity, np.float64)
+        h = C.c_void_p()
+        _check(lib().oa_flow_create(mesh.h, C.byref(self.settings), _dp(bv), int(bv.shape[0]), C.byref(h)))
+        self.h = h
+
+    def _len(self, name):
+        if name == "mDot":
+            return 12 * self.mesh.ne
+        return self.FIELD_SHAPES[name] * self.mesh.nn
+
+    def set_field(self, name, values):
+        v = np.ascontiguousarray(values, np.float64).ravel()
+        _check(lib().oa_flow_set_field(self.h, name.encode(), _dp(v), v.size))
+
+    def get_field(self, name):
+        v = np.zeros(self._len(name))
+        _check(lib().oa_flow_get_field(self.h, name.encode(), _dp(v), v.size))
+        return v
+
+    def device_ptr(self, name) -> int:
+        p = C.POINTER(C.c_double)()
+        _check(lib().oa_flow_field_device_ptr(self.h, name.encode(), C.byref(p)))
+        return C.cast(p, C.c_void_p).value
+
+    def initialize(self):
+        _check(lib().oa_flow_initialize(self.h))
+
+    def assemble_momentum(self, copy=True):
+        A = np.zeros(9 * self.mesh.nnz) if copy else None
+        b = np.zeros(3 * self.mesh.nn) if copy else None
+        _check(lib().oa_assemble_momentum(self.h, _dp(A), _dp(b)))
+        return A, b
+
+    def assemble_pcorr(self, copy=True):
+        A = np.zeros(self.mesh.nnz) if copy else None
+        b = np.zeros(self.mesh.nn) if copy else None
+        _check(lib().oa_assemble_pcorr(self.h, _dp(A), _dp(b)))
+        return A, b
+
+    def update_mdot(self):
+        _check(lib().oa_update_mdot(self.h))
+
+    def update_div(self):
+        _check(lib().oa_update_div(self.h))
+
+    def update_gradient(self, which):
+        _check(lib().oa_update_gradient(self.h, {"p": 0, "U": 1}.get(which, which)))
+
+    def solve(self, sys, rtol, maxit):
+        n = 3 * self.mesh.nn if sys in (0, "momentum") else self.mesh.nn
+        x = np.zeros(n)
+        it, res = C.c_int(), C.c_double()
+        _check(lib().oa_solve(self.h, 0 if sys in (0, "momentum") else 1, rtol, maxit, _dp(x), C.byref(it),
+                              C.byref(res)))
+        return x, it.value, res.value
+
+    def simple_iterate(self, n=1):
+        st = (IterStats * max(n, 1))()
+        _check(lib().oa_simple_iterate(self.h, n, st))
+        return [dict(mom_iters=s.mom_iters, pc_iters=s.pc_iters, pc_refinements=s.pc_refinements,
+                     mom_res=s.mom_res, pc_res=s.pc_res, continuity_rms=s.continuity_rms) for s in st[:n]]
+
+    def sync(self):
+        _check(lib().oa_flow_sync(self.h))
+
+    def stream_handle(self) -> int:
+        p = C.c_void_p()
+        _check(lib().oa_flow_stream(self.h, C.byref(p)))
+        return p.value or 0
+
+    def time_kernel(self, which, reps=5) -> float:
+        """Mean device time (ms) of one assembly kernel, CUDA events on the flow stream."""
+        ms = C.c_double()
+        w = {"momentum": 0, "pcorr": 1, "mdot": 2, "gradU": 3}.get(which, which)
+        _check(lib().oa_time_kernel(self.h, w, reps, C.byref(ms)))
+        return ms.value
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().oa_flow_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,808 @@
+// Oracle (test infrastructure only): CPU FP64 restatement of OpenAccel's
+// CVFEM assembly + SIMPLE pressure-correction hot path for hex8 meshes.
+// Only tests, the smoke check and the bench CPU-baseline leg use it.
+//
+// Each routine names the reference routine it restates (paths relative to the
+// reference project root). Element loops are element-centric exactly as in the
+// reference and scatter through a literal restatement of
+// assembler<N>::applyCoeff_ (src/assemble/assembler.h:311-453), including the
+// reduced-stencil lumping of missing columns into the diagonal block.
+#include "oracle.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+#include <set>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "hex8_master.hpp"
+
+namespace {
+
+using oracle::hex8::LR;
+using oracle::hex8::NPE;
+using oracle::hex8::NSCS;
+constexpr double SMALL = 2.220446049250313e-16;  // src/basic/types.h:179
+
+int g_threads = 1;
+
+template <class F>
+void parallel_for(long n, F f) {
+  if (g_threads <= 1 || n < 4096) {
+    for (long i = 0; i < n; ++i) f(i);
+    return;
+  }
+  std::vector<std::thread> th;
+  const long chunk = (n + g_threads - 1) / g_threads;
+  for (int t = 0; t < g_threads; ++t) {
+    const long a = t * chunk, b = std::min(n, a + chunk);
+    if (a >= b) break;
+    th.emplace_back([=, &f] {
+      for (long i = a; i < b; ++i) f(i);
+    });
+  }
+  for (auto& x : th) x.join();
+}
+
+struct Case {
+  orc_settings s;
+  int nn, ne, nf, nbnd;
+  std::vector<double> x;
+  std::vector<int> conn;
+  std::vector<int> fElem, fOrd, fBnd;
+  std::vector<double> bndU;
+  // geometry
+  std::vector<double> vol, faceArea;  // vol[nn], faceArea[nf][4][3]
+  // graph (reduced stencil, sorted columns)
+  std::vector<int> rowPtr, cols, diagOff;
+  // fields
+  std::vector<double> U, p, gradU, gradP, du, div, mDot, rho, mu, sideU, wallNode;
+  // element -> list of boundary faces
+  std::vector<std::vector<int>> elemFaces;
+  // last assembled systems (for the solver inside simple_iteration)
+  std::vector<double> Am, bm, xm, Ap, bp, xp;
+};
+
+// ---------------------------------------------------------------------------
+// graph: nodeGraph::buildGraph_ reduced stencil (src/mesh/graph/nodeGraph.cpp:29-98)
+void build_graph(Case& c) {
+  std::vector<std::set<int>> st(c.nn);
+  for (int e = 0; e < c.ne; ++e) {
+    const int* en = &c.conn[8 * e];
+    for (int ip = 0; ip < NSCS; ++ip) {
+      const int L = en[LR[ip][0]], R = en[LR[ip][1]];
+      st[L].insert(L);
+      st[L].insert(R);
+      st[R].insert(L);
+      st[R].insert(R);
+    }
+  }
+  c.rowPtr.assign(c.nn + 1, 0);
+  for (int i = 0; i < c.nn; ++i) c.rowPtr[i + 1] = c.rowPtr[i] + (int)st[i].size();
+  c.cols.resize(c.rowPtr[c.nn]);
+  c.diagOff.resize(c.nn);
+  for (int i = 0; i < c.nn; ++i) {
+    int k = c.rowPtr[i];
+    for (int j : st[i]) {
+      if (j == i) c.diagOff[i] = k - c.rowPtr[i];
+      c.cols[k++] = j;
+    }
+  }
+}
+
+// applyCoeff_ (src/assemble/assembler.h:311-453): element nodes sorted by
+// column id; for each row the sorted columns are searched monotonically in the
+// row's sorted column list; a column absent from the row is added to the
+// diagonal block (deductUnfound). lhs is [(n*N)x(n*N)] row-major with
+// row = node*N+m, col = node*N+n.
+template <int N>
+void apply_coeff(Case& c, double* A, double* b, const int* nodes, int n, const double* rhs,
+                 const double* lhs) {
+  int perm[8];
+  std::iota(perm, perm + n, 0);
+  std::sort(perm, perm + n, [&](int a, int bb) { return nodes[a] < nodes[bb]; });
+  for (int r = 0; r < n; ++r) {
+    const int pr = perm[r];
+    const int row = nodes[pr];
+    const double* lrow = &lhs[N * N * pr * n];
+    const double* rr = &rhs[N * pr];
+    const int beg = c.rowPtr[row], len = c.rowPtr[row + 1] - beg;
+    double* vals = &A[(long)N * N * beg];
+    double* diag = &A[(long)N * N * (beg + c.diagOff[row])];
+    int off = 0, offOld = 0;
+    for (int j = 0; j < n; ++j) {
+      const int pj = perm[j];
+      const int col = nodes[pj];
+      while (off < len && c.cols[beg + off] != col) ++off;
+      if (off < len) {
+        for (int m = 0; m < N; ++m)
+          for (int q = 0; q < N; ++q) vals[N * N * off + N * m + q] += lrow[N * n * m + N * pj + q];
+        offOld = off;
+      } else {
+        for (int m = 0; m < N; ++m)
+          for (int q = 0; q < N; ++q) diag[N * m + q] += lrow[N * n * m + N * pj + q];
+        off = offOld;
+      }
+    }
+    for (int k = 0; k < N; ++k) b[N * row + k] += rr[k];
+  }
+}
+
+void gather_coords(const Case& c, int e, double* xe) {
+  for (int a = 0; a < 8; ++a)
+    for (int k = 0; k < 3; ++k) xe[3 * a + k] = c.x[3 * c.conn[8 * e + a] + k];
+}
+
+// mesh::updateDualNodalVolumeField_ (src/mesh/meshGeometry.cpp:1277-1345)
+void dual_volume(Case& c) {
+  c.vol.assign(c.nn, 0.0);
+  for (int e = 0; e < c.ne; ++e) {
+    double xe[24], v[8];
+    gather_coords(c, e, xe);
+    oracle::hex8::scv_volumes(xe, v);
+    for (int a = 0; a < 8; ++a) c.vol[c.conn[8 * e + a]] += v[a];
+  }
+}
+
+// mesh::updateExposedAreaVectorField_ (src/mesh/meshGeometry.cpp:1441-1527)
+void exposed_areas(Case& c) {
+  c.faceArea.assign(12 * c.nf, 0.0);
+  for (int f = 0; f < c.nf; ++f) {
+    const int e = c.fElem[f], o = c.fOrd[f];
+    double xf[12];
+    for (int k = 0; k < 4; ++k) {
+      const int nd = c.conn[8 * e + oracle::hex8::FACE_NODES[o][k]];
+      for (int d = 0; d < 3; ++d) xf[3 * k + d] = c.x[3 * nd + d];
+    }
+    oracle::hex8::quad_face_areav(xf, &c.faceArea[12 * f]);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// flowModel::initializeMassFlowRateInterior_ (src/model/flow/flowModel.cpp:3303-3470)
+void init_mdot(Case& c) {
+  double N[96];
+  oracle::hex8::scs_shape(N, c.s.u_shifted);
+  parallel_for(c.ne, [&](long e) {
+    double xe[24], A[36];
+    gather_coords(c, (int)e, xe);
+    oracle::hex8::scs_areav(xe, A);
+    const int* en = &c.conn[8 * e];
+    for (int ip = 0; ip < NSCS; ++ip) {
+      double u[3] = {0, 0, 0}, rhoIp = 0.0;
+      for (int a = 0; a < 8; ++a) {
+        const double r = N[8 * ip + a];
+        rhoIp += r * c.rho[en[a]];
+        for (int j = 0; j < 3; ++j) u[j] += r * c.U[3 * en[a] + j];
+      }
+      double m = 0.0;
+      for (int j = 0; j < 3; ++j) m += rhoIp * u[j] * A[3 * ip + j];
+      c.mDot[12 * e + ip] = m;
+    }
+  });
+}
+
+// flowModel::updateMassFlowRateInterior_ (src/model/flow/flowModel.cpp:5272-5687),
+// incompressible stationary frame: rhoHR = upwind density (the blending factor
+// of rho is the zero dummy field, so the deferred correction vanishes).
+void update_mdot(Case& c) {
+  double Nv[96], Nc[96];
+  oracle::hex8::scs_shape(Nv, c.s.u_shifted);
+  oracle::hex8::scs_shape(Nc, false);
+  parallel_for(c.ne, [&](long e) {
+    const int* en = &c.conn[8 * e];
+    double xe[24], A[36], g[288], v[8], w[8];
+    gather_coords(c, (int)e, xe);
+    oracle::hex8::scs_areav(xe, A);
+    oracle::hex8::scv_volumes(xe, v);
+    double Vel = 0.0;
+    for (int a = 0; a < 8; ++a) Vel += v[a];
+    const double iV = 1.0 / Vel;
+    for (int a = 0; a < 8; ++a) w[a] = 0.0;
+    for (int a = 0; a < 8; ++a) w[a] += v[a] * iV;
+    oracle::hex8::grad_op(xe, g, c.s.p_grad_shifted);
+    for (int ip = 0; ip < NSCS; ++ip) {
+      const int il = LR[ip][0], ir = LR[ip][1];
+      double du[3] = {0, 0, 0}, u[3] = {0, 0, 0}, dp[3] = {0, 0, 0}, Gp[3] = {0, 0, 0};
+      double rhoIp = 0.0;
+      for (int a = 0; a < 8; ++a) {
+        const double r = Nv[8 * ip + a];
+        rhoIp += r * c.rho[en[a]];
+        for (int j = 0; j < 3; ++j) {
+          du[j] += r * c.du[3 * en[a] + j];
+          u[j] += r * c.U[3 * en[a] + j];
+          dp[j] += g[24 * ip + 3 * a + j] * c.p[en[a]];
+          Gp[j] += w[a] * c.gradP[3 * en[a] + j];
+        }
+      }
+      const double tU = c.mDot[12 * e + ip] / rhoIp;
+      const double rhoUp = tU > 0 ? c.rho[en[il]] : c.rho[en[ir]];
+      double m = 0.0;
+      for (int j = 0; j < 3; ++j) {
+        m += rhoUp * u[j] * A[3 * ip + j];
+        m -= rhoUp * du[j] * (dp[j] - Gp[j]) * A[3 * ip + j];
+      }
+      c.mDot[12 * e + ip] = c.s.mdot_urf * m + (1.0 - c.s.mdot_urf) * c.mDot[12 * e + ip];
+    }
+  });
+}
+
+// flowModel::updateMassDivergenceField_ interior part (flowModel.cpp:13710-13760);
+// wall side mass flows are zero.
+void update_div(Case& c) {
+  std::fill(c.div.begin(), c.div.end(), 0.0);
+  for (int e = 0; e < c.ne; ++e) {
+    const int* en = &c.conn[8 * e];
+    for (int ip = 0; ip < NSCS; ++ip) {
+      const double m = c.mDot[12 * e + ip];
+      c.div[en[LR[ip][0]]] += m;
+      c.div[en[LR[ip][1]]] -= m;
+    }
+  }
+}
+
+// nodeField::updateGradientField (src/field/nodeField/nodeField.hpp:3253-3445
+// interior, :4732-4930 boundary, :6362-6398 relax). NC = field components.
+template <int NC>
+void update_gradient(Case& c, const std::vector<double>& phi, std::vector<double>& grad, bool shifted) {
+  const double g = c.s.grad_urf;
+  for (auto& v : grad) v *= (1.0 - g);
+  double N[96];
+  oracle::hex8::scs_shape(N, shifted);
+  for (int e = 0; e < c.ne; ++e) {
+    const int* en = &c.conn[8 * e];
+    double xe[24], A[36];
+    gather_coords(c, e, xe);
+    oracle::hex8::scs_areav(xe, A);
+    for (int ip = 0; ip < NSCS; ++ip) {
+      const int L = en[LR[ip][0]], R = en[LR[ip][1]];
+      double pip[NC];
+      for (int j = 0; j < NC; ++j) pip[j] = 0.0;
+      for (int a = 0; a < 8; ++a)
+        for (int j = 0; j < NC; ++j) pip[j] += N[8 * ip + a] * phi[NC * en[a] + j];
+      const double ivL = 1.0 / c.vol[L], ivR = 1.0 / c.vol[R];
+      for (int i = 0; i < NC; ++i)
+        for (int j = 0; j < 3; ++j) {
+          grad[3 * NC * L + 3 * i + j] += g * (pip[i] - phi[NC * L + i]) * A[3 * ip + j] * ivL;
+          grad[3 * NC * R + 3 * i + j] -= g * (pip[i] - phi[NC * R + i]) * A[3 * ip + j] * ivR;
+        }
+    }
+  }
+  double Nf[16];
+  oracle::hex8::face_shape(Nf, shifted);
+  for (int f = 0; f < c.nf; ++f) {
+    const int e = c.fElem[f], o = c.fOrd[f];
+    int fn[4];
+    for (int k = 0; k < 4; ++k) fn[k] = c.conn[8 * e + oracle::hex8::FACE_NODES[o][k]];
+    for (int ip = 0; ip < 4; ++ip) {
+      const int nn = fn[ip];
+      double pip[NC];
+      for (int j = 0; j < NC; ++j) pip[j] = 0.0;
+      for (int k = 0; k < 4; ++k)
+        for (int j = 0; j < NC; ++j) pip[j] += Nf[4 * ip + k] * phi[NC * fn[k] + j];
+      const double iv = 1.0 / c.vol[nn];
+      for (int i = 0; i < NC; ++i)
+        for (int j = 0; j < 3; ++j)
+          grad[3 * NC * nn + 3 * i + j] +=
+              g * (pip[i] - phi[NC * nn + i]) * c.faceArea[12 * f + 3 * ip + j] * iv;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// pressureCorrectionAssembler::assembleElemTermsInterior_
+// (src/assemble/flow/segregatedFlow/pressureCorrectionAssembler/
+//  pressureCorrectionAssemblerElemTerms.cpp:17-616), incompressible,
+// stationary frame; adjustMatrixForPressureReference
+// (pressureCorrectionAssembler.cpp:19-63). No-slip wall faces add rho*U_bc.A
+// with U_bc tangential to the flat walls, i.e. exact zeros, so they are omitted.
+void assemble_pcorr(Case& c, double* A, double* b) {
+  const int nnz = c.rowPtr[c.nn];
+  std::fill(A, A + nnz, 0.0);
+  std::fill(b, b + c.nn, 0.0);
+  double Nv[96], Nc[96];
+  oracle::hex8::scs_shape(Nv, c.s.u_shifted);
+  oracle::hex8::scs_shape(Nc, false);
+  for (int e = 0; e < c.ne; ++e) {
+    const int* en = &c.conn[8 * e];
+    double xe[24], Ar[36], g[288], v[8], w[8], lhs[64], rhs[8];
+    std::fill(lhs, lhs + 64, 0.0);
+    std::fill(rhs, rhs + 8, 0.0);
+    gather_coords(c, e, xe);
+    oracle::hex8::scs_areav(xe, Ar);
+    oracle::hex8::scv_volumes(xe, v);
+    double Vel = 0.0;
+    for (int a = 0; a < 8; ++a) Vel += v[a];
+    const double iV = 1.0 / Vel;
+    for (int a = 0; a < 8; ++a) w[a] = 0.0;
+    for (int a = 0; a < 8; ++a) w[a] += v[a] * iV;
+    oracle::hex8::grad_op(xe, g, c.s.p_grad_shifted);
+    for (int ip = 0; ip < NSCS; ++ip) {
+      const int il = LR[ip][0], ir = LR[ip][1];
+      const double tm = c.mDot[12 * e + ip];
+      double u[3] = {0, 0, 0}, du[3] = {0, 0, 0}, dp[3] = {0, 0, 0}, Gp[3] = {0, 0, 0};
+      for (int a = 0; a < 8; ++a) {
+        const double r = Nv[8 * ip + a];
+        for (int j = 0; j < 3; ++j) {
+          u[j] += r * c.U[3 * en[a] + j];
+          du[j] += r * c.du[3 * en[a] + j];
+          dp[j] += g[24 * ip + 3 * a + j] * c.p[en[a]];
+          Gp[j] += w[a] * c.gradP[3 * en[a] + j];
+        }
+      }
+      const double rhoHR = tm > 0 ? c.rho[en[il]] : c.rho[en[ir]];
+      for (int a = 0; a < 8; ++a) {
+        double f = 0.0;
+        for (int j = 0; j < 3; ++j) f += -rhoHR * du[j] * g[24 * ip + 3 * a + j] * Ar[3 * ip + j];
+        lhs[8 * il + a] += f;
+        lhs[8 * ir + a] -= f;
+      }
+      double m = 0.0;
+      for (int j = 0; j < 3; ++j) {
+        m += rhoHR * u[j] * Ar[3 * ip + j];
+        m -= rhoHR * du[j] * (dp[j] - Gp[j]) * Ar[3 * ip + j];
+      }
+      rhs[il] -= m;
+      rhs[ir] += m;
+    }
+    apply_coeff<1>(c, A, b, en, 8, rhs, lhs);
+  }
+  if (c.s.ref_node >= 0) {
+    const int r = c.s.ref_node;
+    const double d = A[c.rowPtr[r] + c.diagOff[r]];
+    for (int k = c.rowPtr[r]; k < c.rowPtr[r + 1]; ++k) A[k] = 0.0;
+    A[c.rowPtr[r] + c.diagOff[r]] = d;
+    b[r] = 0.0;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// navierStokesAssembler momentum system:
+//  node terms   navierStokesAssemblerNodeTerms.cpp:16-149 (steady, no body force,
+//               stationary frame)
+//  interior     navierStokesAssemblerElemTerms.cpp:15-441 (upwind, beta = 0 dummy,
+//               incompressible)
+//  no-slip wall navierStokesAssemblerElemBoundaryConditions.cpp:2659-2981 with
+//               IP_ZERO_NORMAL_STRESS_FIXED_VEL__ (:592-654), laminar
+//  post         phiAssembler.h:748-753 + :967-1006 (diag / urf),
+//               navierStokesAssembler.cpp:234-385 (wall-node rhs * 0.75)
+//  DU           navierStokesAssembler.cpp:84-232 (SIMPLE, steady)
+void assemble_momentum(Case& c, double* A, double* b) {
+  const int nnz = c.rowPtr[c.nn];
+  std::fill(A, A + 9L * nnz, 0.0);
+  std::fill(b, b + 3L * c.nn, 0.0);
+  // node terms, one applyCoeff_ per node
+  for (int i = 0; i < c.nn; ++i) {
+    double lhs[9] = {0}, rhs[3] = {0};
+    const double rho = c.rho[i], vol = c.vol[i], dv = c.div[i];
+    const double lf = rho * vol / c.s.dt;
+    for (int k = 0; k < 3; ++k) {
+      if (dv < 0) lhs[4 * k] += -dv;
+      rhs[k] -= -dv * c.U[3 * i + k];
+      rhs[k] -= c.gradP[3 * i + k] * vol;
+      lhs[4 * k] += lf;
+    }
+    apply_coeff<3>(c, A, b, &i, 1, rhs, lhs);
+  }
+  // interior elements
+  double Nv[96], Nc[96];
+  oracle::hex8::scs_shape(Nv, c.s.u_shifted);
+  oracle::hex8::scs_shape(Nc, false);
+  std::vector<double> lhs(576), rhs(24);
+  for (int e = 0; e < c.ne; ++e) {
+    const int* en = &c.conn[8 * e];
+    std::fill(lhs.begin(), lhs.end(), 0.0);
+    std::fill(rhs.begin(), rhs.end(), 0.0);
+    double xe[24], Ar[36], g[288], Ue[24], mue[8];
+    gather_coords(c, e, xe);
+    for (int a = 0; a < 8; ++a) {
+      mue[a] = c.mu[en[a]];
+      for (int k = 0; k < 3; ++k) Ue[3 * a + k] = c.U[3 * en[a] + k];
+    }
+    oracle::hex8::scs_areav(xe, Ar);
+    oracle::hex8::grad_op(xe, g, c.s.u_grad_shifted);
+    for (int ip = 0; ip < NSCS; ++ip) {
+      const int il = LR[ip][0], ir = LR[ip][1];
+      const double tm = c.mDot[12 * e + ip];
+      double muIp = 0.0;
+      for (int a = 0; a < 8; ++a) muIp += Nv[8 * ip + a] * mue[a];
+      for (int i = 0; i < 3; ++i) {
+        const double up = tm > 0 ? Ue[3 * il + i] : Ue[3 * ir + i];
+        const double af = tm * up;
+        const int iL = 3 * il + i, iR = 3 * ir + i;
+        const int rowL = iL * 24, rowR = iR * 24;
+        rhs[iL] -= af;
+        rhs[iR] += af;
+        const double fl = 0.5 * (tm + std::fabs(tm));
+        lhs[rowL + 3 * il + i] += fl;
+        lhs[rowR + 3 * il + i] -= fl;
+        const double fr = 0.5 * (tm - std::fabs(tm));
+        lhs[rowR + 3 * ir + i] -= fr;
+        lhs[rowL + 3 * ir + i] += fr;
+      }
+      for (int a = 0; a < 8; ++a) {
+        const double* ga = &g[24 * ip + 3 * a];
+        for (int i = 0; i < 3; ++i) {
+          const int iL = 3 * il + i, iR = 3 * ir + i;
+          const int rowL = iL * 24, rowR = iR * 24;
+          double lc = 0.0;
+          for (int j = 0; j < 3; ++j) {
+            const double axj = Ar[3 * ip + j];
+            const double uj = Ue[3 * a + j];
+            lc += -muIp * ga[j] * axj;
+            const double fj = -muIp * ga[i] * axj;
+            lhs[rowL + 3 * a + j] += fj;
+            lhs[rowR + 3 * a + j] -= fj;
+            rhs[iL] -= fj * uj;
+            rhs[iR] += fj * uj;
+          }
+          lhs[rowL + 3 * a + i] += lc;
+          lhs[rowR + 3 * a + i] -= lc;
+          rhs[iL] -= lc * Ue[3 * a + i];
+          rhs[iR] += lc * Ue[3 * a + i];
+        }
+      }
+    }
+    apply_coeff<3>(c, A, b, en, 8, rhs.data(), lhs.data());
+  }
+  // no-slip walls (laminar): zero normal stress with fixed velocity
+  double Nf[16];
+  oracle::hex8::face_shape(Nf, c.s.u_shifted);
+  for (int f = 0; f < c.nf; ++f) {
+    const int e = c.fElem[f], o = c.fOrd[f];
+    const int* en = &c.conn[8 * e];
+    std::fill(lhs.begin(), lhs.end(), 0.0);
+    std::fill(rhs.begin(), rhs.end(), 0.0);
+    double xe[24], g[96], Ue[24], bcm[8], muf[4];
+    gather_coords(c, e, xe);
+    for (int a = 0; a < 8; ++a) {
+      bcm[a] = 1.0;
+      for (int k = 0; k < 3; ++k) Ue[3 * a + k] = c.U[3 * en[a] + k];
+    }
+    for (int k = 0; k < 4; ++k) {
+      const int ic = oracle::hex8::FACE_NODES[o][k];
+      muf[k] = c.mu[en[ic]];
+      bcm[ic] = 0.0;
+      for (int d = 0; d < 3; ++d) Ue[3 * ic + d] = c.sideU[3 * en[ic] + d];
+    }
+    oracle::hex8::face_grad_op(o, xe, g, c.s.u_grad_shifted);
+    const double* av = &c.faceArea[12 * f];
+    for (int ip = 0; ip < 4; ++ip) {
+      const int nn = oracle::hex8::FACE_NODES[o][ip];
+      double asq = 0.0;
+      for (int j = 0; j < 3; ++j) asq += av[3 * ip + j] * av[3 * ip + j];
+      const double amag = std::sqrt(asq);
+      double muB = 0.0;
+      for (int k = 0; k < 4; ++k) muB += Nf[4 * ip + k] * muf[k];
+      double nx[3];
+      for (int i = 0; i < 3; ++i) nx[i] = av[3 * ip + i] / amag;
+      for (int a = 0; a < 8; ++a) {
+        const double* ga = &g[24 * ip + 3 * a];
+        for (int j = 0; j < 3; ++j) {
+          const double axj = av[3 * ip + j];
+          const double gj = ga[j];
+          const double uj = Ue[3 * a + j];
+          for (int i = 0; i < 3; ++i) {
+            const int iR = 3 * nn + i, rowR = iR * 24;
+            const double gi = ga[i], ui = Ue[3 * a + i], ni = nx[i];
+            const double om = 1.0 - ni * ni;
+            double lf = -muB * gj * axj * om;
+            lhs[rowR + 3 * a + i] += lf * bcm[a];
+            rhs[iR] -= lf * ui;
+            lf = -muB * gi * axj * om;
+            lhs[rowR + 3 * a + j] += lf * bcm[a];
+            rhs[iR] -= lf * uj;
+            for (int l = 0; l < 3; ++l) {
+              if (i == l) continue;
+              const double nil = ni * nx[l];
+              const double ul = Ue[3 * a + l], gl = ga[l];
+              lf = muB * gj * axj * nil;
+              lhs[rowR + 3 * a + l] += lf * bcm[a];
+              rhs[iR] -= lf * ul;
+              lf = muB * gl * axj * nil;
+              lhs[rowR + 3 * a + j] += lf * bcm[a];
+              rhs[iR] -= lf * uj;
+            }
+          }
+        }
+      }
+    }
+    apply_coeff<3>(c, A, b, en, 8, rhs.data(), lhs.data());
+  }
+  // relaxation of the diagonal, wall-node rhs relaxation
+  const double ui = 1.0 / c.s.urf_u;
+  for (int i = 0; i < c.nn; ++i) {
+    double* d = &A[9L * (c.rowPtr[i] + c.diagOff[i])];
+    for (int k = 0; k < 3; ++k) d[4 * k] *= ui;
+  }
+  for (int i = 0; i < c.nn; ++i)
+    if (c.wallNode[i] != 0.0)
+      for (int k = 0; k < 3; ++k) b[3 * i + k] *= c.s.wall_rhs_relax;
+  // DU coefficients
+  for (int i = 0; i < c.nn; ++i) {
+    const double* d = &A[9L * (c.rowPtr[i] + c.diagOff[i])];
+    for (int k = 0; k < 3; ++k) c.du[3 * i + k] = c.vol[i] / (d[4 * k] + SMALL);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Krylov: BiCGStab, right-preconditioned by (block-)Jacobi. The reference's
+// solver library (liblinsolve over PETSc/Trilinos/HYPRE) is absent; this is the
+// published van der Vorst algorithm.
+void spmv(const Case& c, int bs, const double* A, const double* x, double* y) {
+  parallel_for(c.nn, [&](long i) {
+    for (int m = 0; m < bs; ++m) {
+      double s = 0.0;
+      for (int k = c.rowPtr[i]; k < c.rowPtr[i + 1]; ++k) {
+        const int j = c.cols[k];
+        for (int q = 0; q < bs; ++q) s += A[(long)bs * bs * k + bs * m + q] * x[bs * j + q];
+      }
+      y[bs * i + m] = s;
+    }
+  });
+}
+
+void invert3(const double* a, double* r) {
+  const double det = a[0] * (a[4] * a[8] - a[5] * a[7]) - a[1] * (a[3] * a[8] - a[5] * a[6]) +
+                     a[2] * (a[3] * a[7] - a[4] * a[6]);
+  const double id = 1.0 / det;
+  r[0] = (a[4] * a[8] - a[5] * a[7]) * id;
+  r[1] = (a[2] * a[7] - a[1] * a[8]) * id;
+  r[2] = (a[1] * a[5] - a[2] * a[4]) * id;
+  r[3] = (a[5] * a[6] - a[3] * a[8]) * id;
+  r[4] = (a[0] * a[8] - a[2] * a[6]) * id;
+  r[5] = (a[2] * a[3] - a[0] * a[5]) * id;
+  r[6] = (a[3] * a[7] - a[4] * a[6]) * id;
+  r[7] = (a[1] * a[6] - a[0] * a[7]) * id;
+  r[8] = (a[0] * a[4] - a[1] * a[3]) * id;
+}
+
+double dot(long n, const double* a, const double* b) {
+  double s = 0.0;
+  for (long i = 0; i < n; ++i) s += a[i] * b[i];
+  return s;
+}
+
+int bicgstab(const Case& c, int bs, const double* A, const double* b, double* x, double rtol,
+             int maxit, double* res) {
+  const long n = (long)bs * c.nn;
+  std::vector<double> Minv((long)bs * bs * c.nn);
+  for (int i = 0; i < c.nn; ++i) {
+    const double* d = &A[(long)bs * bs * (c.rowPtr[i] + c.diagOff[i])];
+    if (bs == 1)
+      Minv[i] = 1.0 / d[0];
+    else
+      invert3(d, &Minv[9L * i]);
+  }
+  auto prec = [&](const double* v, double* z) {
+    for (int i = 0; i < c.nn; ++i) {
+      if (bs == 1) {
+        z[i] = Minv[i] * v[i];
+      } else {
+        for (int m = 0; m < 3; ++m)
+          z[3 * i + m] = Minv[9L * i + 3 * m] * v[3 * i] + Minv[9L * i + 3 * m + 1] * v[3 * i + 1] +
+                         Minv[9L * i + 3 * m + 2] * v[3 * i + 2];
+      }
+    }
+  };
+  std::vector<double> r(n), rh(n), pv(n, 0.0), v(n, 0.0), s(n), t(n), ph(n), sh(n);
+  std::fill(x, x + n, 0.0);
+  for (long i = 0; i < n; ++i) r[i] = b[i];
+  const double bn = std::sqrt(dot(n, b, b));
+  if (bn == 0.0) {
+    *res = 0.0;
+    return 0;
+  }
+  rh = r;
+  double rho = 1, alpha = 1, omega = 1;
+  int it = 0;
+  double rn = bn;
+  for (it = 0; it < maxit; ++it) {
+    if (rn <= rtol * bn) break;
+    const double rho1 = dot(n, rh.data(), r.data());
+    if (rho1 == 0.0) break;
+    const double beta = (rho1 / rho) * (alpha / omega);
+    for (long i = 0; i < n; ++i) pv[i] = r[i] + beta * (pv[i] - omega * v[i]);
+    prec(pv.data(), ph.data());
+    spmv(c, bs, A, ph.data(), v.data());
+    alpha = rho1 / dot(n, rh.data(), v.data());
+    for (long i = 0; i < n; ++i) s[i] = r[i] - alpha * v[i];
+    prec(s.data(), sh.data());
+    spmv(c, bs, A, sh.data(), t.data());
+    const double tt = dot(n, t.data(), t.data());
+    omega = tt > 0 ? dot(n, t.data(), s.data()) / tt : 0.0;
+    for (long i = 0; i < n; ++i) {
+      x[i] += alpha * ph[i] + omega * sh[i];
+      r[i] = s[i] - omega * t[i];
+    }
+    rho = rho1;
+    rn = std::sqrt(dot(n, r.data(), r.data()));
+    if (omega == 0.0) {
+      ++it;
+      break;
+    }
+  }
+  *res = rn / bn;
+  return it;
+}
+
+// ---------------------------------------------------------------------------
+// One SIMPLE outer iteration: segregatedFlowEquations::solve
+// (src/equation/flow/segregatedFlowEquations.cpp:76-297) with
+// navierStokesEquation::solve (navierStokesEquation.cpp:157-222) and
+// pressureCorrectionEquation::solve (pressureCorrectionEquation.cpp:89-150),
+// one pressure sub-iteration, no compressibility, no frame motion.
+void simple_iteration(Case& c, orc_iter_stats* st) {
+  const int nnz = c.rowPtr[c.nn];
+  c.Am.resize(9L * nnz);
+  c.bm.resize(3L * c.nn);
+  c.xm.resize(3L * c.nn);
+  c.Ap.resize(nnz);
+  c.bp.resize(c.nn);
+  c.xp.resize(c.nn);
+  // momentum predictor
+  assemble_momentum(c, c.Am.data(), c.bm.data());
+  double res = 0.0;
+  const int mi = bicgstab(c, 3, c.Am.data(), c.bm.data(), c.xm.data(), c.s.mom_rtol, c.s.mom_maxit, &res);
+  for (long i = 0; i < 3L * c.nn; ++i) c.U[i] += c.xm[i];
+  update_mdot(c);
+  if (st) {
+    st->mom_iters[0] = mi;
+    st->mom_res = res;
+  }
+  // pressure correction
+  assemble_pcorr(c, c.Ap.data(), c.bp.data());
+  if (st) {
+    double s2 = 0.0;
+    for (int i = 0; i < c.nn; ++i) s2 += c.bp[i] * c.bp[i];
+    st->continuity_rms = std::sqrt(s2 / c.nn);
+  }
+  const int pi = bicgstab(c, 1, c.Ap.data(), c.bp.data(), c.xp.data(), c.s.pc_rtol, c.s.pc_maxit, &res);
+  for (int i = 0; i < c.nn; ++i) c.p[i] += c.s.urf_p * c.xp[i];
+  if (st) {
+    st->pc_iters = pi;
+    st->pc_res = res;
+  }
+  update_mdot(c);
+  update_div(c);
+  const double iu = 1.0 / c.s.urf_p;
+  for (long i = 0; i < 3L * c.nn; ++i) c.U[i] += iu * c.du[i] * c.gradP[i];
+  update_gradient<1>(c, c.p, c.gradP, c.s.p_shifted);
+  for (long i = 0; i < 3L * c.nn; ++i) c.U[i] -= iu * c.du[i] * c.gradP[i];
+  update_gradient<3>(c, c.U, c.gradU, c.s.u_shifted);
+}
+
+}  // namespace
+
+extern "C" {
+
+void orc_set_threads(int n) { g_threads = n < 1 ? 1 : n; }
+
+void orc_hex8_scs_areav(const double* x, double* areav) { oracle::hex8::scs_areav(x, areav); }
+int orc_hex8_scv_volumes(const double* x, double* vol) {
+  return oracle::hex8::scv_volumes(x, vol) ? 0 : 1;
+}
+int orc_hex8_grad_op(const double* x, double* gradop, int shifted) {
+  return oracle::hex8::grad_op(x, gradop, shifted != 0);
+}
+void orc_hex8_shape(double* shape, int shifted) { oracle::hex8::scs_shape(shape, shifted != 0); }
+
+void* orc_case_create(int nn, int ne, const double* x, const int* conn, int nf, const int* face_elem,
+                      const int* face_ord, const int* face_bnd, int nbnd, const double* bnd_velocity,
+                      const orc_settings* s) {
+  Case* c = new Case();
+  c->s = *s;
+  c->nn = nn;
+  c->ne = ne;
+  c->nf = nf;
+  c->nbnd = nbnd;
+  c->x.assign(x, x + 3L * nn);
+  c->conn.assign(conn, conn + 8L * ne);
+  c->fElem.assign(face_elem, face_elem + nf);
+  c->fOrd.assign(face_ord, face_ord + nf);
+  c->fBnd.assign(face_bnd, face_bnd + nf);
+  c->bndU.assign(bnd_velocity, bnd_velocity + 3L * nbnd);
+  build_graph(*c);
+  dual_volume(*c);
+  exposed_areas(*c);
+  c->U.assign(3L * nn, 0.0);
+  c->p.assign(nn, 0.0);
+  c->gradU.assign(9L * nn, 0.0);
+  c->gradP.assign(3L * nn, 0.0);
+  c->du.assign(3L * nn, 0.0);
+  c->div.assign(nn, 0.0);
+  c->mDot.assign(12L * ne, 0.0);
+  c->rho.assign(nn, s->rho);
+  c->mu.assign(nn, s->mu);
+  c->sideU.assign(3L * nn, 0.0);
+  c->wallNode.assign(nn, 0.0);
+  // node side velocity: boundaries applied in order, later ones overwrite shared
+  // nodes (nodeField::updateBoundarySideFieldSpecifiedValue, setToValue per part)
+  for (int bnd = 0; bnd < nbnd; ++bnd)
+    for (int f = 0; f < nf; ++f) {
+      if (c->fBnd[f] != bnd) continue;
+      for (int k = 0; k < 4; ++k) {
+        const int nd = c->conn[8 * c->fElem[f] + oracle::hex8::FACE_NODES[c->fOrd[f]][k]];
+        for (int d = 0; d < 3; ++d) c->sideU[3 * nd + d] = c->bndU[3 * bnd + d];
+        c->wallNode[nd] = 1.0;
+      }
+    }
+  return c;
+}
+
+void orc_case_destroy(void* h) { delete static_cast<Case*>(h); }
+
+double* orc_case_field(void* h, const char* name, long* len) {
+  Case* c = static_cast<Case*>(h);
+  std::vector<double>* v = nullptr;
+  const std::string n(name);
+  if (n == "U") v = &c->U;
+  else if (n == "p") v = &c->p;
+  else if (n == "gradU") v = &c->gradU;
+  else if (n == "gradP") v = &c->gradP;
+  else if (n == "du") v = &c->du;
+  else if (n == "div") v = &c->div;
+  else if (n == "mDot") v = &c->mDot;
+  else if (n == "rho") v = &c->rho;
+  else if (n == "mu") v = &c->mu;
+  else if (n == "vol") v = &c->vol;
+  else if (n == "faceArea") v = &c->faceArea;
+  else if (n == "sideU") v = &c->sideU;
+  else if (n == "wallNode") v = &c->wallNode;
+  else if (n == "x") v = &c->x;
+  if (!v) {
+    *len = 0;
+    return nullptr;
+  }
+  *len = (long)v->size();
+  return v->data();
+}
+
+int orc_case_nnz(void* h) {
+  Case* c = static_cast<Case*>(h);
+  return c->rowPtr[c->nn];
+}
+
+void orc_case_graph(void* h, int* row_ptr, int* cols) {
+  Case* c = static_cast<Case*>(h);
+  std::copy(c->rowPtr.begin(), c->rowPtr.end(), row_ptr);
+  std::copy(c->cols.begin(), c->cols.end(), cols);
+}
+
+// navierStokesEquation::initialize/postInitialize and
+// pressureCorrectionEquation::initialize (velocity gradient, pressure gradient,
+// mass flow rate, divergence).
+void orc_initialize(void* h) {
+  Case* c = static_cast<Case*>(h);
+  update_gradient<3>(*c, c->U, c->gradU, c->s.u_shifted);
+  init_mdot(*c);
+  update_div(*c);
+  update_gradient<1>(*c, c->p, c->gradP, c->s.p_shifted);
+}
+
+void orc_assemble_momentum(void* h, double* A, double* b) {
+  assemble_momentum(*static_cast<Case*>(h), A, b);
+}
+void orc_assemble_pcorr(void* h, double* A, double* b) {
+  assemble_pcorr(*static_cast<Case*>(h), A, b);
+}
+void orc_update_mdot(void* h) { update_mdot(*static_cast<Case*>(h)); }
+void orc_update_div(void* h) { update_div(*static_cast<Case*>(h)); }
+void orc_update_grad_p(void* h) {
+  Case* c = static_cast<Case*>(h);
+  update_gradient<1>(*c, c->p, c->gradP, c->s.p_shifted);
+}
+void orc_update_grad_u(void* h) {
+  Case* c = static_cast<Case*>(h);
+  update_gradient<3>(*c, c->U, c->gradU, c->s.u_shifted);
+}
+int orc_bicgstab(void* h, int bs, const double* A, const double* b, double* x, double rtol, int maxit,
+                 double* res) {
+  return bicgstab(*static_cast<Case*>(h), bs, A, b, x, rtol, maxit, res);
+}
+void orc_simple_iteration(void* h, orc_iter_stats* st) { simple_iteration(*static_cast<Case*>(h), st); }
+
+}  // extern "C"

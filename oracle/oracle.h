@@ -1,0 +1,92 @@
+/* Oracle (test infrastructure only): C interface of the CPU FP64 restatement
+ * of OpenAccel's CVFEM assembly and SIMPLE pressure-correction path.
+ *
+ * Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg load
+ * this library, and only as the checker. The shipped GPU path never calls it.
+ *
+ * Every function restates a reference routine; the citing comment sits beside
+ * the implementation in oracle.cpp. Parity status: the reference cannot be
+ * built here (Trilinos/STK, yaml-cpp, MPI, gfortran and the liblinsolve
+ * submodule are absent) and ships no golden vectors, so this restatement is
+ * pinned by analytic known-answer tests (tests/test_oracle_kat.py) and by the
+ * committed fixtures it generates; parity against the reference binary itself
+ * is unpinned.
+ */
+#ifndef OPENACCEL_ORACLE_H
+#define OPENACCEL_ORACLE_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Settings of the laminar, steady, incompressible segregated-flow case; the
+ * defaults in the Python mirror follow controls.h and examples/cavity/input.i. */
+typedef struct orc_settings {
+  double rho;          /* density */
+  double mu;           /* dynamic viscosity */
+  double urf_u;        /* velocity relaxation factor */
+  double urf_p;        /* pressure relaxation factor */
+  double dt;           /* physical timescale (false transient) */
+  double grad_urf;     /* gradient under-relaxation (nodeField.h:152) */
+  double mdot_urf;     /* mass-flow relaxation (relaxMass_) */
+  double wall_rhs_relax; /* boundary rhs relaxation (navierStokesAssembler.cpp:237) */
+  int u_shifted;       /* velocity interpolation linear_linear */
+  int u_grad_shifted;  /* velocity gradient interpolation linear_linear */
+  int p_shifted;       /* pressure interpolation linear_linear */
+  int p_grad_shifted;  /* pressure gradient interpolation linear_linear */
+  int ref_node;        /* pressure-level node (row fixed), -1 for none */
+  int mom_maxit;
+  double mom_rtol;
+  int pc_maxit;
+  double pc_rtol;
+} orc_settings;
+
+typedef struct orc_iter_stats {
+  int mom_iters[1];
+  double mom_res;
+  int pc_iters;
+  double pc_res;
+  double continuity_rms; /* RMS of the PC rhs before the solve */
+} orc_iter_stats;
+
+/* ---- stateless geometry kernels (per element) ---- */
+void orc_hex8_scs_areav(const double* x /*[8][3]*/, double* areav /*[12][3]*/);
+int orc_hex8_scv_volumes(const double* x, double* vol /*[8]*/);
+int orc_hex8_grad_op(const double* x, double* gradop /*[12][8][3]*/, int shifted);
+void orc_hex8_shape(double* shape /*[12][8]*/, int shifted);
+
+/* ---- case object ---- */
+void* orc_case_create(int nn, int ne, const double* x, const int* conn, int nf,
+                      const int* face_elem, const int* face_ord, const int* face_bnd,
+                      int nbnd, const double* bnd_velocity, const orc_settings* s);
+void orc_case_destroy(void* h);
+/* Pointer to a named field of the case (see oracle.cpp for the list); *len
+ * receives the number of doubles. */
+double* orc_case_field(void* h, const char* name, long* len);
+int orc_case_nnz(void* h);
+void orc_case_graph(void* h, int* row_ptr /*nn+1*/, int* cols /*nnz*/);
+
+/* initialisation: mDot from U, gradients, divergence */
+void orc_initialize(void* h);
+/* assembled momentum system (BSR 3x3, row-major blocks) incl. node terms,
+ * interior, no-slip walls, relaxation; also updates du */
+void orc_assemble_momentum(void* h, double* A, double* b);
+/* pressure-correction system incl. reference-pressure row */
+void orc_assemble_pcorr(void* h, double* A, double* b);
+void orc_update_mdot(void* h);
+void orc_update_div(void* h);
+void orc_update_grad_p(void* h);
+void orc_update_grad_u(void* h);
+/* BiCGStab with (block-)Jacobi preconditioning; returns iterations, res = final
+ * relative residual. bs = 1 or 3. */
+int orc_bicgstab(void* h, int bs, const double* A, const double* b, double* x,
+                 double rtol, int maxit, double* res);
+/* one SIMPLE outer iteration (segregatedFlowEquations::solve) */
+void orc_simple_iteration(void* h, orc_iter_stats* st);
+/* thread count used by the element loops and SpMV (1 = serial) */
+void orc_set_threads(int n);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

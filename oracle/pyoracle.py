@@ -1,0 +1,221 @@
+"""Oracle (test infrastructure only): ctypes view of oracle/_build/liboracle.so.
+
+Imported only by tests/, ``__graft_entry__.smoke()`` and bench.py's CPU
+baseline leg, always as the checker. The product (``openaccel_b200``) never
+imports this module.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "_build", "liboracle.so")
+_lib = None
+
+
+class Settings(C.Structure):
+    _fields_ = [
+        ("rho", C.c_double),
+        ("mu", C.c_double),
+        ("urf_u", C.c_double),
+        ("urf_p", C.c_double),
+        ("dt", C.c_double),
+        ("grad_urf", C.c_double),
+        ("mdot_urf", C.c_double),
+        ("wall_rhs_relax", C.c_double),
+        ("u_shifted", C.c_int),
+        ("u_grad_shifted", C.c_int),
+        ("p_shifted", C.c_int),
+        ("p_grad_shifted", C.c_int),
+        ("ref_node", C.c_int),
+        ("mom_maxit", C.c_int),
+        ("mom_rtol", C.c_double),
+        ("pc_maxit", C.c_int),
+        ("pc_rtol", C.c_double),
+    ]
+
+
+class IterStats(C.Structure):
+    _fields_ = [
+        ("mom_iters", C.c_int * 1),
+        ("mom_res", C.c_double),
+        ("pc_iters", C.c_int),
+        ("pc_res", C.c_double),
+        ("continuity_rms", C.c_double),
+    ]
+
+
+def default_settings(**kw) -> Settings:
+    """Cavity-example settings (examples/cavity/input.i:46-53) with
+    linear_linear velocity interpolation and the controls.h defaults."""
+    d = dict(rho=1.0, mu=0.01, urf_u=0.9, urf_p=0.1, dt=1.0, grad_urf=0.5625, mdot_urf=1.0,
+             wall_rhs_relax=0.75, u_shifted=1, u_grad_shifted=1, p_shifted=1, p_grad_shifted=1,
+             ref_node=0, mom_maxit=200, mom_rtol=1e-12, pc_maxit=5000, pc_rtol=1e-12)
+    d.update(kw)
+    return Settings(**d)
+
+
+def build():
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            build()
+        L = C.CDLL(_LIB_PATH)
+        P = C.POINTER
+        dp, ip = P(C.c_double), P(C.c_int)
+        L.orc_case_create.restype = C.c_void_p
+        L.orc_case_create.argtypes = [C.c_int, C.c_int, dp, ip, C.c_int, ip, ip, ip, C.c_int, dp,
+                                      P(Settings)]
+        L.orc_case_destroy.argtypes = [C.c_void_p]
+        L.orc_case_field.restype = dp
+        L.orc_case_field.argtypes = [C.c_void_p, C.c_char_p, P(C.c_long)]
+        L.orc_case_nnz.restype = C.c_int
+        L.orc_case_nnz.argtypes = [C.c_void_p]
+        L.orc_case_graph.argtypes = [C.c_void_p, ip, ip]
+        for name in ["orc_initialize", "orc_update_mdot", "orc_update_div", "orc_update_grad_p",
+                     "orc_update_grad_u"]:
+            getattr(L, name).argtypes = [C.c_void_p]
+        L.orc_assemble_momentum.argtypes = [C.c_void_p, dp, dp]
+        L.orc_assemble_pcorr.argtypes = [C.c_void_p, dp, dp]
+        L.orc_bicgstab.restype = C.c_int
+        L.orc_bicgstab.argtypes = [C.c_void_p, C.c_int, dp, dp, dp, C.c_double, C.c_int, dp]
+        L.orc_simple_iteration.argtypes = [C.c_void_p, P(IterStats)]
+        L.orc_set_threads.argtypes = [C.c_int]
+        L.orc_hex8_scs_areav.argtypes = [dp, dp]
+        L.orc_hex8_scv_volumes.argtypes = [dp, dp]
+        L.orc_hex8_scv_volumes.restype = C.c_int
+        L.orc_hex8_grad_op.argtypes = [dp, dp, C.c_int]
+        L.orc_hex8_grad_op.restype = C.c_int
+        L.orc_hex8_shape.argtypes = [dp, C.c_int]
+        _lib = L
+    return _lib
+
+
+def _dp(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def _ip(a):
+    return a.ctypes.data_as(C.POINTER(C.c_int))
+
+
+def set_threads(n: int):
+    lib().orc_set_threads(int(n))
+
+
+class FlowCase:
+    """Oracle flow case over a ``meshgen.HexMesh``."""
+
+    def __init__(self, mesh, settings: Settings | None = None, U0=None):
+        self.mesh = mesh
+        self.settings = settings or default_settings()
+        self._keep = [np.ascontiguousarray(mesh.coords, np.float64),
+                      np.ascontiguousarray(mesh.conn, np.int32),
+                      np.ascontiguousarray(mesh.face_elem, np.int32),
+                      np.ascontiguousarray(mesh.face_ord, np.int32),
+                      np.ascontiguousarray(mesh.face_bnd, np.int32),
+                      np.ascontiguousarray(mesh.bnd_velocity, np.float64)]
+        x, conn, fe, fo, fb, bv = self._keep
+        self.h = lib().orc_case_create(mesh.nn, mesh.ne, _dp(x), _ip(conn), mesh.nf, _ip(fe), _ip(fo),
+                                       _ip(fb), bv.shape[0], _dp(bv), C.byref(self.settings))
+        self.nnz = lib().orc_case_nnz(self.h)
+        if U0 is not None:
+            self.field("U")[:] = np.asarray(U0, np.float64).ravel()
+
+    def close(self):
+        if self.h:
+            lib().orc_case_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def field(self, name: str) -> np.ndarray:
+        n = C.c_long(0)
+        p = lib().orc_case_field(self.h, name.encode(), C.byref(n))
+        if not p:
+            raise KeyError(name)
+        return np.ctypeslib.as_array(p, shape=(n.value,))
+
+    def graph(self):
+        rp = np.zeros(self.mesh.nn + 1, np.int32)
+        cols = np.zeros(self.nnz, np.int32)
+        lib().orc_case_graph(self.h, _ip(rp), _ip(cols))
+        return rp, cols
+
+    def initialize(self):
+        lib().orc_initialize(self.h)
+
+    def assemble_momentum(self):
+        A = np.zeros(9 * self.nnz)
+        b = np.zeros(3 * self.mesh.nn)
+        lib().orc_assemble_momentum(self.h, _dp(A), _dp(b))
+        return A, b
+
+    def assemble_pcorr(self):
+        A = np.zeros(self.nnz)
+        b = np.zeros(self.mesh.nn)
+        lib().orc_assemble_pcorr(self.h, _dp(A), _dp(b))
+        return A, b
+
+    def update_mdot(self):
+        lib().orc_update_mdot(self.h)
+
+    def update_div(self):
+        lib().orc_update_div(self.h)
+
+    def update_grad_p(self):
+        lib().orc_update_grad_p(self.h)
+
+    def update_grad_u(self):
+        lib().orc_update_grad_u(self.h)
+
+    def bicgstab(self, bs, A, b, rtol=1e-12, maxit=2000):
+        x = np.zeros_like(b)
+        res = C.c_double(0)
+        it = lib().orc_bicgstab(self.h, bs, _dp(A), _dp(b), _dp(x), rtol, maxit, C.byref(res))
+        return x, it, res.value
+
+    def simple_iteration(self):
+        st = IterStats()
+        lib().orc_simple_iteration(self.h, C.byref(st))
+        return dict(mom_iters=st.mom_iters[0], mom_res=st.mom_res, pc_iters=st.pc_iters,
+                    pc_res=st.pc_res, continuity_rms=st.continuity_rms)
+
+
+def hex8_scs_areav(x):
+    x = np.ascontiguousarray(x, np.float64).reshape(8, 3)
+    a = np.zeros((12, 3))
+    lib().orc_hex8_scs_areav(_dp(x), _dp(a))
+    return a
+
+
+def hex8_scv_volumes(x):
+    x = np.ascontiguousarray(x, np.float64).reshape(8, 3)
+    v = np.zeros(8)
+    lib().orc_hex8_scv_volumes(_dp(x), _dp(v))
+    return v
+
+
+def hex8_grad_op(x, shifted=True):
+    x = np.ascontiguousarray(x, np.float64).reshape(8, 3)
+    g = np.zeros((12, 8, 3))
+    err = lib().orc_hex8_grad_op(_dp(x), _dp(g), int(shifted))
+    return g, err
+
+
+def hex8_shape(shifted=True):
+    N = np.zeros((12, 8))
+    lib().orc_hex8_shape(_dp(N), int(shifted))
+    return N

@@ -1,0 +1,146 @@
+"""CPU checks of the oracle: analytic known answers, agreement with the
+reference's own compiled geometry templates (oracle/_ref), structural
+properties of the assembled systems, and the committed golden fixtures."""
+import ctypes as C
+import os
+
+import numpy as np
+import pytest
+
+from openaccel_b200 import meshgen
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+UNIT = np.array([[0, 0, 0], [1, 0, 0], [1, 1, 0], [0, 1, 0], [0, 0, 1], [1, 0, 1], [1, 1, 1], [0, 1, 1]], float)
+
+
+def test_unit_cube_scs_areas(oracle_mod):
+    a = oracle_mod.hex8_scs_areav(UNIT)
+    # every SCS of a unit cube is a quarter of a unit face, pointing L -> R
+    lr = [(0, 1), (1, 2), (2, 3), (0, 3), (4, 5), (5, 6), (6, 7), (4, 7), (0, 4), (1, 5), (2, 6), (3, 7)]
+    for ip, (l, r) in enumerate(lr):
+        d = UNIT[r] - UNIT[l]
+        np.testing.assert_allclose(a[ip], 0.25 * d, atol=1e-15)
+
+
+def test_scv_volumes_sum_to_element_volume(oracle_mod):
+    rng = np.random.default_rng(1)
+    for _ in range(20):
+        A = np.eye(3) + rng.uniform(-0.2, 0.2, (3, 3))
+        x = UNIT @ A.T + rng.uniform(-1, 1, 3)
+        v = oracle_mod.hex8_scv_volumes(x)
+        assert np.all(v > 0)
+        np.testing.assert_allclose(v.sum(), abs(np.linalg.det(A)), rtol=1e-13)
+
+
+def test_gradient_operator_exact_for_linear_fields(oracle_mod):
+    rng = np.random.default_rng(2)
+    x = UNIT + rng.uniform(-0.15, 0.15, UNIT.shape)
+    c = np.array([0.3, -1.2, 2.5])
+    f = x @ c
+    for shifted in (True, False):
+        g, err = oracle_mod.hex8_grad_op(x, shifted)
+        assert err == 0
+        np.testing.assert_allclose(np.einsum("ink,n->ik", g, f), np.tile(c, (12, 1)), rtol=1e-12, atol=1e-12)
+        # partition of unity: gradients sum to zero
+        np.testing.assert_allclose(g.sum(axis=1), 0.0, atol=1e-12)
+
+
+def test_closed_element_surface(oracle_mod):
+    # sum of outward SCS area vectors around each SCV plus its exposed faces is zero,
+    # equivalently: SCS areas are antisymmetric per element; here check that the
+    # 12 SCS areas of an affine element scale with the affine map
+    rng = np.random.default_rng(3)
+    A = np.eye(3) + rng.uniform(-0.3, 0.3, (3, 3))
+    a0 = oracle_mod.hex8_scs_areav(UNIT)
+    a1 = oracle_mod.hex8_scs_areav(UNIT @ A.T)
+    cof = np.linalg.det(A) * np.linalg.inv(A).T
+    np.testing.assert_allclose(a1, a0 @ cof.T, rtol=1e-12, atol=1e-14)
+
+
+REF_LIB = os.path.join(ROOT, "oracle", "_ref", "libnalu_hex8_ref.so")
+
+
+@pytest.mark.skipif(not os.path.exists(REF_LIB), reason="reference geometry library not built (needs the reference tree)")
+def test_oracle_matches_reference_geometry_templates(oracle_mod):
+    """Pin the restated master element against the reference's own
+    subdivide_hex_8 / quad_area_by_triangulation / hex_volume_grandy."""
+    L = C.CDLL(REF_LIB)
+    rng = np.random.default_rng(4)
+    for _ in range(200):
+        x = UNIT + rng.uniform(-0.24, 0.24, UNIT.shape)
+        a = np.zeros((12, 3))
+        v = np.zeros(8)
+        L.ref_hex8_scs_areav(x.ctypes.data_as(C.c_void_p), a.ctypes.data_as(C.c_void_p))
+        L.ref_hex8_scv_volumes(x.ctypes.data_as(C.c_void_p), v.ctypes.data_as(C.c_void_p))
+        np.testing.assert_allclose(oracle_mod.hex8_scs_areav(x), a, rtol=0, atol=4e-16)
+        np.testing.assert_allclose(oracle_mod.hex8_scv_volumes(x), v, rtol=0, atol=4e-16)
+
+
+def test_dual_volume_and_graph(oracle_mod):
+    m = meshgen.cavity(5, perturb=0.2, seed=7)
+    c = oracle_mod.FlowCase(m)
+    np.testing.assert_allclose(c.field("vol").sum(), 1.0, rtol=1e-13)
+    rp, cols = c.graph()
+    deg = np.diff(rp)
+    # interior nodes: self + 6 edge neighbours; corners: self + 3
+    assert deg.max() == 7 and deg.min() == 4
+    for i in range(m.nn):
+        row = cols[rp[i]:rp[i + 1]]
+        assert np.all(np.diff(row) > 0) and i in row
+
+
+def test_pcorr_row_sums_vanish(oracle_mod):
+    """Rhie-Chow Laplacian: sum_n dN_n/dx = 0, so every row of the
+    pressure-correction matrix sums to zero (lumping keeps row sums)."""
+    m = meshgen.cavity(4, perturb=0.2, seed=3)
+    rng = np.random.default_rng(5)
+    c = oracle_mod.FlowCase(m, U0=rng.normal(0, 0.1, (m.nn, 3)))
+    c.initialize()
+    c.field("du")[:] = rng.uniform(0.5, 1.5, 3 * m.nn)
+    A, b = c.assemble_pcorr()
+    rp, _ = c.graph()
+    rows = np.add.reduceat(A, rp[:-1])
+    scale = np.abs(A).max()
+    rows[0] = 0.0  # reference-pressure row keeps only its diagonal
+    assert np.abs(rows).max() < 1e-13 * scale
+
+
+def test_uniform_velocity_zero_divergence(oracle_mod):
+    m = meshgen.cavity(4, perturb=0.2, seed=9)
+    U = np.tile([0.3, -0.1, 0.2], (m.nn, 1))
+    c = oracle_mod.FlowCase(m, U0=U)
+    c.initialize()
+    div = c.field("div").reshape(-1)
+    # interior nodes: closed control surface, constant flux field -> zero net mass flow
+    idx = np.arange(m.nn)
+    i, j, k = idx % 5, (idx // 5) % 5, idx // 25
+    inner = (i > 0) & (i < 4) & (j > 0) & (j < 4) & (k > 0) & (k < 4)
+    assert np.abs(div[inner]).max() < 1e-15
+
+
+def test_gradient_converges_to_exact_on_linear_field(oracle_mod):
+    m = meshgen.cavity(4, perturb=0.0)
+    coef = np.array([0.7, -0.4, 1.3])
+    c = oracle_mod.FlowCase(m)
+    c.field("p")[:] = m.coords @ coef
+    for _ in range(60):
+        c.update_grad_p()
+    g = c.field("gradP").reshape(-1, 3)
+    idx = np.arange(m.nn)
+    i, j, k = idx % 5, (idx // 5) % 5, idx // 25
+    inner = (i > 0) & (i < 4) & (j > 0) & (j < 4) & (k > 0) & (k < 4)
+    np.testing.assert_allclose(g[inner], np.tile(coef, (inner.sum(), 1)), rtol=1e-12)
+
+
+GOLDEN = os.path.join(ROOT, "tests", "golden", "cavity4_perturbed.npz")
+
+
+def test_golden_fixture_regenerates(oracle_mod):
+    """The committed fixture (tests/golden/make_golden.py) is reproduced by
+    the current oracle bit for bit."""
+    from tests.golden.make_golden import generate
+
+    g = np.load(GOLDEN)
+    cur = generate(oracle_mod)
+    for k in g.files:
+        np.testing.assert_array_equal(cur[k], g[k], err_msg=k)
