@@ -5,6 +5,8 @@
 #include <algorithm>
 #include <atomic>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -182,7 +184,8 @@ int solve_pcorr(oa_flow* h, double rtol, int maxit, int* iters, double* res, int
   int total = 0, nref = 0;
   double rel = bnorm > 0 ? 1.0 : 0.0;
   OA_CUDA(cudaMemcpyAsync(h->ir_r, f.b.b_pc, sizeof(double) * m.nn, cudaMemcpyDeviceToDevice, f.stream));
-  while (rel > rtol && total < maxit && nref < 20) {
+  constexpr int INNER_CAP = 300;  // FP32 Krylov iterations per refinement
+  while (rel > rtol && total < maxit && nref < 40) {
     k_from_double<float><<<(m.nn + 255) / 256, 256, 0, f.stream>>>(m.nn, h->ir_r, h->ir_r32);
     count_launches(1);
     float* d = nullptr;
@@ -190,15 +193,22 @@ int solve_pcorr(oa_flow* h, double rtol, int maxit, int* iters, double* res, int
     double r_in = 0.0;
     // inner tolerance: enough digits for FP32 without stalling
     const double inner = std::max(rtol / rel, 2e-4);
-    if (int s = h->pc32.solve<float>(A, h->ir_r32, d, std::min(inner, 0.1), maxit - total, &it, &r_in, 20)) return s;
+    if (int s = h->pc32.solve<float>(A, h->ir_r32, d, std::min(inner, 0.1), std::min(INNER_CAP, maxit - total), &it,
+                                     &r_in, 20))
+      return s;
     total += it;
-    add_correction<float>(m.nn, f.b.x_pc, d, f.stream);
+    // a diverged inner solve contributes nothing; the next pass restarts from
+    // the FP64 residual
+    if (h->pc32.last_status != 3 && r_in < 1.0) add_correction<float>(m.nn, f.b.x_pc, d, f.stream);
     if (int s = fp64_residual<float>(m.nn, m.row_ptr, m.cols, A, f.b.x_pc, f.b.b_pc, h->ir_r, h->pc32.partials,
                                      h->scal + 1, f.stream))
       return s;
     OA_CUDA(cudaMemcpyAsync(h->hscal + 1, h->scal + 1, sizeof(double), cudaMemcpyDeviceToHost, f.stream));
     OA_CUDA(cudaStreamSynchronize(f.stream));
     rel = bnorm > 0 ? h->hscal[1] / bnorm : 0.0;
+    if (std::getenv("OA_DEBUG"))
+      std::fprintf(stderr, "[oa] pcorr refinement %d: inner iters %d inner res %.3e |b| %.3e rel %.3e\n", nref, it,
+                   r_in, bnorm, rel);
     ++nref;
     if (!(rel < INFINITY)) return fail(OA_ERR_SOLVER, "pressure refinement: non-finite residual");
     if (it == 0) break;

@@ -76,7 +76,7 @@ __device__ __forceinline__ void final_reduce(const double* partials, int nb, dou
 }
 
 // y = A x for a BSR matrix with BxB row-major blocks; optional partial dots
-// (y.w1, y.w2) with vectors of the same length.
+// (y.w1 and, for ND = 2, y.y).
 template <int B, class TM, class TV, int ND>
 __global__ void __launch_bounds__(KB) k_spmv(int nn, const int* __restrict__ rp, const int* __restrict__ cols,
                                               const TM* __restrict__ A, const TV* __restrict__ x,
@@ -95,9 +95,11 @@ __global__ void __launch_bounds__(KB) k_spmv(int nn, const int* __restrict__ rp,
 #pragma unroll
       for (int q = 0; q < B; ++q) s += double(A[(size_t)k * B * B + B * m + q]) * double(x[B * j + q]);
     }
-    y[t] = TV(s);
-    if (ND > 0) v[0] += double(TV(s)) * double(w1[t]);
-    if (ND > 1) v[1] += double(TV(s)) * double(w2[t]);
+    const TV ys = TV(s);
+    y[t] = ys;
+    // second dot is y.y, taken from the register (never re-read through y)
+    if (ND > 0) v[0] += double(ys) * double(w1[t]);
+    if (ND > 1) v[1] += double(ys) * double(ys);
   }
   if (ND > 0) block_reduce_store<ND>(reinterpret_cast<double(&)[ND]>(v), partials, MAX_PARTIALS);
 }
@@ -248,6 +250,9 @@ __global__ void __launch_bounds__(KB) k_end_iter(KScal* sc, const double* partia
     if (!(sc->rnorm < INFINITY)) {
       sc->done = 1;
       sc->status = 2;
+    } else if (sc->rnorm > 1e3 * sc->bnorm) {
+      sc->done = 1;  // diverging (seen with FP32 vectors on stiff systems)
+      sc->status = 3;
     } else if (sc->rnorm <= rtol * sc->bnorm || sc->iters >= maxit) {
       sc->done = 1;
     } else if (sc->omega == 0.0 || sc->d0 == 0.0) {
@@ -321,7 +326,7 @@ int KrylovSolver<B, TM, TV>::solve(const TM* A, const TB* b, TV*& xout, double r
       k_alpha<<<1, KB, 0, st>>>(sc, partials, gv);
       k_s_update<TV><<<gfull, KB, 0, st>>>(n, r, v, sc);
       k_prec<B, TV><<<gfull, KB, 0, st>>>(nn, Minv, r, sh, sc);
-      k_spmv<B, TM, TV, 2><<<gv, KB, 0, st>>>(nn, rp, cols, A, sh, t, r, t, partials, sc);
+      k_spmv<B, TM, TV, 2><<<gv, KB, 0, st>>>(nn, rp, cols, A, sh, t, r, nullptr, partials, sc);
       k_omega<<<1, KB, 0, st>>>(sc, partials, gv);
       k_x_update<TV><<<gv, KB, 0, st>>>(n, x, r, ph, sh, t, rh, partials, sc);
       k_end_iter<<<1, KB, 0, st>>>(sc, partials, gv, rtol, maxit);
@@ -338,6 +343,7 @@ int KrylovSolver<B, TM, TV>::solve(const TM* A, const TB* b, TV*& xout, double r
   if (iters) *iters = h->iters;
   if (res) *res = h->bnorm > 0 ? h->rnorm / h->bnorm : 0.0;
   xout = x;
+  last_status = h->status;
   if (h->status == 2) return fail(OA_ERR_SOLVER, "BiCGStab: non-finite residual");
   return OA_OK;
 }

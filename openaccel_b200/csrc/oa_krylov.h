@@ -15,6 +15,7 @@ struct KrylovSolver {
   double* partials = nullptr;
   void* scal = nullptr;
   void* hscal = nullptr;
+  int last_status = 0;  // 0 ok, 1 breakdown, 2 non-finite, 3 diverging
 
   int setup(int nn, const int* rp, const int* cols, const int* dg, cudaStream_t st);
   void release();
