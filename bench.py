@@ -125,7 +125,11 @@ def run_ours(args, rank, world):
     gm = rt.Mesh(m)
 
     def make(prec):
-        f = rt.Flow(gm, rt.default_settings(precision=prec, pc_rtol=args.pc_rtol, mom_rtol=args.mom_rtol))
+        # the mixed form replays its Krylov chunks as CUDA graphs; the plain FP64
+        # form launches every kernel from the host
+        graphs = 1 if (prec == rt.OA_PREC_MIXED and not args.no_graphs) else 0
+        f = rt.Flow(gm, rt.default_settings(precision=prec, pc_rtol=args.pc_rtol, mom_rtol=args.mom_rtol,
+                                            use_graphs=graphs))
         f.set_field("U", U0)
         f.initialize()
         return f
@@ -274,6 +278,7 @@ def main():
     ap.add_argument("--pc-rtol", type=float, default=1e-8)
     ap.add_argument("--mom-rtol", type=float, default=1e-6)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-graphs", action="store_true")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))

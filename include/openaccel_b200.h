@@ -52,6 +52,8 @@ typedef struct oa_flow_settings {
   int pc_maxit;
   double pc_rtol;
   int precision;                /* OA_PREC_FP64 or OA_PREC_MIXED */
+  int pc_amg;                   /* 1: aggregation-AMG preconditioned pressure solve, 0: Jacobi */
+  int use_graphs;               /* 1: replay Krylov iteration chunks as CUDA graphs */
 } oa_flow_settings;
 
 typedef struct oa_iter_stats {

@@ -19,6 +19,7 @@ namespace oa {
 static thread_local std::string g_last_error;
 static std::atomic<long long> g_launches{0};
 void count_launches(long long n) { g_launches += n; }
+long long launch_total() { return g_launches.load(); }
 void set_error(const std::string& msg) { g_last_error = msg; }
 int fail(int code, const std::string& msg) {
   g_last_error = msg;
@@ -68,6 +69,8 @@ struct oa_flow {
   KrylovSolver<3, double, double> mom64;
   KrylovSolver<1, float, float> pc32;
   KrylovSolver<3, float, float> mom32;
+  Amg<double> amg64;
+  Amg<float> amg32;
   double* ir_r = nullptr;   // FP64 residual for refinement
   double* ir_x = nullptr;   // FP64 accumulated solution
   float* ir_r32 = nullptr;
@@ -135,6 +138,7 @@ double* field_ptr(Flow& f, const std::string& n, size_t* len) {
 int solve_momentum(oa_flow* h, double rtol, int maxit, int* iters, double* res, bool apply) {
   Flow& f = h->f;
   DeviceMesh& m = *f.mesh;
+  h->mom64.use_graph = h->mom32.use_graph = f.s.use_graphs != 0;
   if (mixed(f)) {
     if (int s = h->mom32.setup(m.nn, m.row_ptr, m.cols, m.diag, f.stream)) return s;
     float* x = nullptr;
@@ -163,10 +167,29 @@ int solve_momentum(oa_flow* h, double rtol, int maxit, int* iters, double* res, 
 int solve_pcorr(oa_flow* h, double rtol, int maxit, int* iters, double* res, int* refinements) {
   Flow& f = h->f;
   DeviceMesh& m = *f.mesh;
+  if (f.s.pc_amg) {
+    Amg<double>* a64 = &h->amg64;
+    Amg<float>* a32 = &h->amg32;
+    if (!mixed(f) && !a64->ready) {
+      if (int s = a64->setup(m.nn, m.h_row_ptr.data(), m.h_cols.data(), m.h_diag.data(), m.row_ptr, m.cols, m.diag))
+        return s;
+    }
+    if (mixed(f) && !a32->ready) {
+      if (int s = a32->setup(m.nn, m.h_row_ptr.data(), m.h_cols.data(), m.h_diag.data(), m.row_ptr, m.cols, m.diag))
+        return s;
+    }
+    h->pc64.amg = mixed(f) ? nullptr : a64;
+    h->pc32.amg = mixed(f) ? a32 : nullptr;
+  } else {
+    h->pc64.amg = nullptr;
+    h->pc32.amg = nullptr;
+  }
+  h->pc64.use_graph = h->pc32.use_graph = f.s.use_graphs != 0;
   if (!mixed(f)) {
     if (int s = h->pc64.setup(m.nn, m.row_ptr, m.cols, m.diag, f.stream)) return s;
     double* x = nullptr;
-    if (int s = h->pc64.solve<double>(static_cast<const double*>(f.b.A_pc), f.b.b_pc, x, rtol, maxit, iters, res, 20))
+    if (int s = h->pc64.solve<double>(static_cast<const double*>(f.b.A_pc), f.b.b_pc, x, rtol, maxit, iters, res,
+                                      f.s.pc_amg ? 5 : 20))
       return s;
     OA_CUDA(cudaMemcpyAsync(f.b.x_pc, x, sizeof(double) * m.nn, cudaMemcpyDeviceToDevice, f.stream));
     if (refinements) *refinements = 0;
@@ -194,7 +217,7 @@ int solve_pcorr(oa_flow* h, double rtol, int maxit, int* iters, double* res, int
     // inner tolerance: enough digits for FP32 without stalling
     const double inner = std::max(rtol / rel, 2e-4);
     if (int s = h->pc32.solve<float>(A, h->ir_r32, d, std::min(inner, 0.1), std::min(INNER_CAP, maxit - total), &it,
-                                     &r_in, 20))
+                                     &r_in, f.s.pc_amg ? 5 : 20, nref > 0))
       return s;
     total += it;
     // a diverged inner solve contributes nothing; the next pass restarts from
@@ -449,6 +472,8 @@ void oa_flow_destroy(oa_flow* H) {
   H->mom64.release();
   H->pc32.release();
   H->mom32.release();
+  H->amg64.release();
+  H->amg32.release();
   if (f.stream) cudaStreamDestroy(f.stream);
   delete H;
 }

@@ -65,6 +65,7 @@ struct Flow {
 
 void set_error(const std::string& msg);
 void count_launches(long long n);
+long long launch_total();
 int fail(int code, const std::string& msg);
 
 #define OA_CUDA(call)                                                              \

@@ -1,5 +1,6 @@
 // Pressure-correction / momentum Krylov solve on the device: BiCGStab
-// (van der Vorst 1992) right-preconditioned by point or 3x3 block Jacobi.
+// (van der Vorst 1992) right-preconditioned by point or 3x3 block Jacobi, or
+// for scalar systems by the aggregation-AMG V-cycle of oa_amg.cu.
 //
 // The reference hands its systems to liblinsolve (PETSc / Trilinos / HYPRE,
 // src/equation/linearSystem.h:416-462), which is absent from the reference
@@ -11,6 +12,7 @@
 #include <cuda_runtime.h>
 
 #include <cmath>
+#include <type_traits>
 
 #include "oa_internal.h"
 #include "oa_krylov.h"
@@ -23,6 +25,8 @@ constexpr int MAX_PARTIALS = 2048;
 struct KScal {
   double rho, alpha, omega, bnorm, rnorm;
   double d0, d1, d2;  // reduced dots of the current phase
+  double rtol;
+  int maxit;
   int done, iters, status;
 };
 
@@ -164,10 +168,13 @@ __global__ void __launch_bounds__(KB) k_init(int n, const TB* __restrict__ b, TV
   block_reduce_store<1>(s, partials, MAX_PARTIALS);
 }
 
-__global__ void __launch_bounds__(KB) k_init_scalars(KScal* sc, const double* partials, int nb, double rtol) {
+__global__ void __launch_bounds__(KB) k_init_scalars(KScal* sc, const double* partials, int nb, double rtol,
+                                                      int maxit) {
   double o[1];
   final_reduce<1>(partials, nb, o);
   if (threadIdx.x == 0) {
+    sc->rtol = rtol;
+    sc->maxit = maxit;
     sc->bnorm = sqrt(o[0]);
     sc->rnorm = sc->bnorm;
     sc->rho = sc->alpha = sc->omega = 1.0;
@@ -238,7 +245,7 @@ __global__ void __launch_bounds__(KB) k_x_update(int n, TV* x, TV* r, const TV* 
 }
 
 // rho <- rho1; rho1 <- rh.r; convergence test
-__global__ void __launch_bounds__(KB) k_end_iter(KScal* sc, const double* partials, int nb, double rtol, int maxit) {
+__global__ void __launch_bounds__(KB) k_end_iter(KScal* sc, const double* partials, int nb) {
   if (sc->done) return;
   double o[2];
   final_reduce<2>(partials, nb, o);
@@ -253,7 +260,7 @@ __global__ void __launch_bounds__(KB) k_end_iter(KScal* sc, const double* partia
     } else if (sc->rnorm > 1e3 * sc->bnorm) {
       sc->done = 1;  // diverging (seen with FP32 vectors on stiff systems)
       sc->status = 3;
-    } else if (sc->rnorm <= rtol * sc->bnorm || sc->iters >= maxit) {
+    } else if (sc->rnorm <= sc->rtol * sc->bnorm || sc->iters >= sc->maxit) {
       sc->done = 1;
     } else if (sc->omega == 0.0 || sc->d0 == 0.0) {
       sc->done = 1;
@@ -291,6 +298,10 @@ void KrylovSolver<B, TM, TV>::release() {
   if (partials) cudaFree(partials);
   if (scal) cudaFree(scal);
   if (hscal) cudaFreeHost(hscal);
+  if (graph_exec) cudaGraphExecDestroy(graph_exec);
+  graph_exec = nullptr;
+  graph_A = nullptr;
+  graph_amg = nullptr;
   Minv = nullptr;
   partials = nullptr;
   scal = nullptr;
@@ -302,7 +313,7 @@ void KrylovSolver<B, TM, TV>::release() {
 template <int B, class TM, class TV>
 template <class TB>
 int KrylovSolver<B, TM, TV>::solve(const TM* A, const TB* b, TV*& xout, double rtol, int maxit, int* iters,
-                                   double* res, int check_every) {
+                                   double* res, int check_every, bool reuse_precond) {
   const int n = B * nn;
   // work vectors: x r rh p v ph sh t
   TV *x = static_cast<TV*>(vec[0]), *r = static_cast<TV*>(vec[1]), *rh = static_cast<TV*>(vec[2]),
@@ -312,27 +323,74 @@ int KrylovSolver<B, TM, TV>::solve(const TM* A, const TB* b, TV*& xout, double r
   const int gfull = (n + KB - 1) / KB;                 // element-wise kernels
   const int gv = gfull < MAX_PARTIALS ? gfull : MAX_PARTIALS;  // reducing kernels (grid-stride)
   const int gr = (nn + KB - 1) / KB;
+  constexpr bool kAmgOk = (B == 1) && std::is_same<TM, TV>::value;
+  const int* done_flag = &sc->done;
+  auto precond = [&](const TV* in, TV* out) -> int {
+    if constexpr (kAmgOk) {
+      if (amg) return amg->apply(reinterpret_cast<const TV*>(in), out, done_flag, st);
+    }
+    k_prec<B, TV><<<gfull, KB, 0, st>>>(nn, Minv, in, out, sc);
+    count_launches(1);
+    return OA_OK;
+  };
+  if constexpr (kAmgOk) {
+    if (amg && !reuse_precond) {
+      if (int s = amg->numeric(reinterpret_cast<const TV*>(A), st)) return s;
+    }
+  }
   k_build_minv<B, TM><<<gr, KB, 0, st>>>(nn, rp, dg, A, Minv);
   k_init<TV, TB><<<gv, KB, 0, st>>>(n, b, x, r, rh, p, v, partials);
-  k_init_scalars<<<1, KB, 0, st>>>(sc, partials, gv, rtol);
+  k_init_scalars<<<1, KB, 0, st>>>(sc, partials, gv, rtol, maxit);
   count_launches(3);
   OA_CUDA(cudaGetLastError());
-  int done_iters = 0;
-  while (true) {
+  // one chunk of check_every iterations; every kernel reads its scalars and
+  // the tolerance from device memory, so the chunk can be captured once
+  long long per_chunk = 0;
+  auto chunk = [&]() -> int {
+    const long long l0 = launch_total();
     for (int it = 0; it < check_every; ++it) {
       k_p_update<TV><<<gfull, KB, 0, st>>>(n, p, r, v, sc);
-      k_prec<B, TV><<<gfull, KB, 0, st>>>(nn, Minv, p, ph, sc);
+      if (int s = precond(p, ph)) return s;
       k_spmv<B, TM, TV, 1><<<gv, KB, 0, st>>>(nn, rp, cols, A, ph, v, rh, nullptr, partials, sc);
       k_alpha<<<1, KB, 0, st>>>(sc, partials, gv);
       k_s_update<TV><<<gfull, KB, 0, st>>>(n, r, v, sc);
-      k_prec<B, TV><<<gfull, KB, 0, st>>>(nn, Minv, r, sh, sc);
+      if (int s = precond(r, sh)) return s;
       k_spmv<B, TM, TV, 2><<<gv, KB, 0, st>>>(nn, rp, cols, A, sh, t, r, nullptr, partials, sc);
       k_omega<<<1, KB, 0, st>>>(sc, partials, gv);
       k_x_update<TV><<<gv, KB, 0, st>>>(n, x, r, ph, sh, t, rh, partials, sc);
-      k_end_iter<<<1, KB, 0, st>>>(sc, partials, gv, rtol, maxit);
+      k_end_iter<<<1, KB, 0, st>>>(sc, partials, gv);
     }
-    count_launches(10L * check_every);
+    count_launches(8L * check_every);
+    per_chunk = launch_total() - l0;
     OA_CUDA(cudaGetLastError());
+    return OA_OK;
+  };
+  if (use_graph && (graph_exec == nullptr || graph_A != (const void*)A || graph_chunk != check_every ||
+                    graph_amg != (const void*)amg)) {
+    if (graph_exec) cudaGraphExecDestroy(graph_exec);
+    graph_exec = nullptr;
+    cudaGraph_t g;
+    OA_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    const int cs = chunk();
+    const cudaError_t ce = cudaStreamEndCapture(st, &g);
+    if (cs) return cs;
+    if (ce != cudaSuccess) return fail(OA_ERR_CUDA, std::string("Krylov chunk capture: ") + cudaGetErrorString(ce));
+    OA_CUDA(cudaGraphInstantiate(&graph_exec, g, 0));
+    cudaGraphDestroy(g);
+    graph_A = A;
+    graph_amg = amg;
+    graph_chunk = check_every;
+    graph_launches = per_chunk;
+    count_launches(-per_chunk);  // captured, not launched
+  }
+  int done_iters = 0;
+  while (true) {
+    if (use_graph) {
+      OA_CUDA(cudaGraphLaunch(graph_exec, st));
+      count_launches(graph_launches);
+    } else if (int s = chunk()) {
+      return s;
+    }
     done_iters += check_every;
     OA_CUDA(cudaMemcpyAsync(hscal, sc, sizeof(KScal), cudaMemcpyDeviceToHost, st));
     OA_CUDA(cudaStreamSynchronize(st));
@@ -352,11 +410,11 @@ template struct KrylovSolver<1, double, double>;
 template struct KrylovSolver<3, double, double>;
 template struct KrylovSolver<1, float, float>;
 template struct KrylovSolver<3, float, float>;
-template int KrylovSolver<1, double, double>::solve<double>(const double*, const double*, double*&, double, int, int*, double*, int);
-template int KrylovSolver<3, double, double>::solve<double>(const double*, const double*, double*&, double, int, int*, double*, int);
-template int KrylovSolver<1, float, float>::solve<double>(const float*, const double*, float*&, double, int, int*, double*, int);
-template int KrylovSolver<1, float, float>::solve<float>(const float*, const float*, float*&, double, int, int*, double*, int);
-template int KrylovSolver<3, float, float>::solve<float>(const float*, const float*, float*&, double, int, int*, double*, int);
+template int KrylovSolver<1, double, double>::solve<double>(const double*, const double*, double*&, double, int, int*, double*, int, bool);
+template int KrylovSolver<3, double, double>::solve<double>(const double*, const double*, double*&, double, int, int*, double*, int, bool);
+template int KrylovSolver<1, float, float>::solve<double>(const float*, const double*, float*&, double, int, int*, double*, int, bool);
+template int KrylovSolver<1, float, float>::solve<float>(const float*, const float*, float*&, double, int, int*, double*, int, bool);
+template int KrylovSolver<3, float, float>::solve<float>(const float*, const float*, float*&, double, int, int*, double*, int, bool);
 
 // ---------------------------------------------------------------------------
 // FP64 residual for iterative refinement: r = b - A x (A in its stored

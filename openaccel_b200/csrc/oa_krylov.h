@@ -2,6 +2,8 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include "oa_amg.h"
+
 namespace oa {
 
 // BiCGStab on a BSR matrix with BxB blocks; matrix values TM, vectors TV.
@@ -16,14 +18,25 @@ struct KrylovSolver {
   void* scal = nullptr;
   void* hscal = nullptr;
   int last_status = 0;  // 0 ok, 1 breakdown, 2 non-finite, 3 diverging
+  // optional AMG preconditioner (scalar systems); null = point/block Jacobi
+  Amg<TV>* amg = nullptr;
+  // CUDA-graph replay of the iteration chunk (captured on first use)
+  bool use_graph = false;
+  cudaGraphExec_t graph_exec = nullptr;
+  const void* graph_A = nullptr;
+  const void* graph_amg = nullptr;
+  int graph_chunk = 0;
+  long long graph_launches = 0;
 
   int setup(int nn, const int* rp, const int* cols, const int* dg, cudaStream_t st);
   void release();
   ~KrylovSolver() { release(); }
   // Solve A x = b from x0 = 0; xout points at the solver-owned solution.
   template <class TB>
+  // reuse_precond: keep the preconditioner built for the same A by the
+  // previous call (iterative-refinement passes)
   int solve(const TM* A, const TB* b, TV*& xout, double rtol, int maxit, int* iters, double* res,
-            int check_every);
+            int check_every, bool reuse_precond = false);
 };
 
 // r = b - A x in FP64 arithmetic (A scalar CSR in its stored precision);

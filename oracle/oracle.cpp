@@ -10,6 +10,7 @@
 #include "oracle.h"
 
 #include <algorithm>
+#include <cstdint>
 #include <cmath>
 #include <cstring>
 #include <numeric>
@@ -60,11 +61,65 @@ struct Case {
   std::vector<int> rowPtr, cols, diagOff;
   // fields
   std::vector<double> U, p, gradU, gradP, du, div, mDot, rho, mu, sideU, wallNode;
-  // element -> list of boundary faces
-  std::vector<std::vector<int>> elemFaces;
+  // element colours (no two elements of a colour share a node), for the
+  // threaded CPU-baseline path
+  std::vector<std::vector<int>> colors;
   // last assembled systems (for the solver inside simple_iteration)
   std::vector<double> Am, bm, xm, Ap, bp, xp;
 };
+
+// Greedy element colouring over shared nodes (built once per case).
+void build_colors(Case& c) {
+  std::vector<uint32_t> used(c.nn, 0u);
+  std::vector<int> col(c.ne);
+  int nc = 0;
+  for (int e = 0; e < c.ne; ++e) {
+    uint32_t m = 0;
+    for (int a = 0; a < 8; ++a) m |= used[c.conn[8 * e + a]];
+    int k = 0;
+    while (k < 32 && (m >> k) & 1u) ++k;
+    col[e] = k;
+    nc = std::max(nc, k + 1);
+    for (int a = 0; a < 8; ++a) used[c.conn[8 * e + a]] |= (1u << k);
+  }
+  c.colors.assign(nc, {});
+  for (int e = 0; e < c.ne; ++e) c.colors[col[e]].push_back(e);
+}
+
+// Element loop that scatters into nodal/CSR storage. Serial: element order,
+// exactly as the reference's bucket loop. Threaded: colour by colour, so each
+// entry receives its contributions in colour order whatever the thread count.
+template <class F>
+void for_elements(const Case& c, F f) {
+  if (g_threads <= 1) {
+    for (int e = 0; e < c.ne; ++e) f(e);
+    return;
+  }
+  for (const auto& cl : c.colors) parallel_for((long)cl.size(), [&](long i) { f(cl[i]); });
+}
+
+// Ordered dot product: per-thread partial sums added in thread order.
+double pdot(long n, const double* a, const double* b) {
+  if (g_threads <= 1 || n < 65536) {
+    double s = 0.0;
+    for (long i = 0; i < n; ++i) s += a[i] * b[i];
+    return s;
+  }
+  std::vector<double> part(g_threads, 0.0);
+  std::vector<std::thread> th;
+  const long chunk = (n + g_threads - 1) / g_threads;
+  for (int t = 0; t < g_threads; ++t)
+    th.emplace_back([&, t] {
+      const long lo = t * chunk, hi = std::min(n, lo + chunk);
+      double s = 0.0;
+      for (long i = lo; i < hi; ++i) s += a[i] * b[i];
+      part[t] = s;
+    });
+  for (auto& x : th) x.join();
+  double s = 0.0;
+  for (double v : part) s += v;
+  return s;
+}
 
 // ---------------------------------------------------------------------------
 // graph: nodeGraph::buildGraph_ reduced stencil (src/mesh/graph/nodeGraph.cpp:29-98)
@@ -234,14 +289,14 @@ void update_mdot(Case& c) {
 // wall side mass flows are zero.
 void update_div(Case& c) {
   std::fill(c.div.begin(), c.div.end(), 0.0);
-  for (int e = 0; e < c.ne; ++e) {
+  for_elements(c, [&](int e) {
     const int* en = &c.conn[8 * e];
     for (int ip = 0; ip < NSCS; ++ip) {
       const double m = c.mDot[12 * e + ip];
       c.div[en[LR[ip][0]]] += m;
       c.div[en[LR[ip][1]]] -= m;
     }
-  }
+  });
 }
 
 // nodeField::updateGradientField (src/field/nodeField/nodeField.hpp:3253-3445
@@ -252,7 +307,7 @@ void update_gradient(Case& c, const std::vector<double>& phi, std::vector<double
   for (auto& v : grad) v *= (1.0 - g);
   double N[96];
   oracle::hex8::scs_shape(N, shifted);
-  for (int e = 0; e < c.ne; ++e) {
+  for_elements(c, [&](int e) {
     const int* en = &c.conn[8 * e];
     double xe[24], A[36];
     gather_coords(c, e, xe);
@@ -270,7 +325,7 @@ void update_gradient(Case& c, const std::vector<double>& phi, std::vector<double
           grad[3 * NC * R + 3 * i + j] -= g * (pip[i] - phi[NC * R + i]) * A[3 * ip + j] * ivR;
         }
     }
-  }
+  });
   double Nf[16];
   oracle::hex8::face_shape(Nf, shifted);
   for (int f = 0; f < c.nf; ++f) {
@@ -306,7 +361,7 @@ void assemble_pcorr(Case& c, double* A, double* b) {
   double Nv[96], Nc[96];
   oracle::hex8::scs_shape(Nv, c.s.u_shifted);
   oracle::hex8::scs_shape(Nc, false);
-  for (int e = 0; e < c.ne; ++e) {
+  for_elements(c, [&](int e) {
     const int* en = &c.conn[8 * e];
     double xe[24], Ar[36], g[288], v[8], w[8], lhs[64], rhs[8];
     std::fill(lhs, lhs + 64, 0.0);
@@ -349,7 +404,7 @@ void assemble_pcorr(Case& c, double* A, double* b) {
       rhs[ir] += m;
     }
     apply_coeff<1>(c, A, b, en, 8, rhs, lhs);
-  }
+  });
   if (c.s.ref_node >= 0) {
     const int r = c.s.ref_node;
     const double d = A[c.rowPtr[r] + c.diagOff[r]];
@@ -391,11 +446,9 @@ void assemble_momentum(Case& c, double* A, double* b) {
   double Nv[96], Nc[96];
   oracle::hex8::scs_shape(Nv, c.s.u_shifted);
   oracle::hex8::scs_shape(Nc, false);
-  std::vector<double> lhs(576), rhs(24);
-  for (int e = 0; e < c.ne; ++e) {
+  for_elements(c, [&](int e) {
     const int* en = &c.conn[8 * e];
-    std::fill(lhs.begin(), lhs.end(), 0.0);
-    std::fill(rhs.begin(), rhs.end(), 0.0);
+    std::vector<double> lhs(576, 0.0), rhs(24, 0.0);
     double xe[24], Ar[36], g[288], Ue[24], mue[8];
     gather_coords(c, e, xe);
     for (int a = 0; a < 8; ++a) {
@@ -447,10 +500,11 @@ void assemble_momentum(Case& c, double* A, double* b) {
       }
     }
     apply_coeff<3>(c, A, b, en, 8, rhs.data(), lhs.data());
-  }
+  });
   // no-slip walls (laminar): zero normal stress with fixed velocity
   double Nf[16];
   oracle::hex8::face_shape(Nf, c.s.u_shifted);
+  std::vector<double> lhs(576), rhs(24);
   for (int f = 0; f < c.nf; ++f) {
     const int e = c.fElem[f], o = c.fOrd[f];
     const int* en = &c.conn[8 * e];
@@ -560,11 +614,7 @@ void invert3(const double* a, double* r) {
   r[8] = (a[0] * a[4] - a[1] * a[3]) * id;
 }
 
-double dot(long n, const double* a, const double* b) {
-  double s = 0.0;
-  for (long i = 0; i < n; ++i) s += a[i] * b[i];
-  return s;
-}
+double dot(long n, const double* a, const double* b) { return pdot(n, a, b); }
 
 int bicgstab(const Case& c, int bs, const double* A, const double* b, double* x, double rtol,
              int maxit, double* res) {
@@ -578,7 +628,7 @@ int bicgstab(const Case& c, int bs, const double* A, const double* b, double* x,
       invert3(d, &Minv[9L * i]);
   }
   auto prec = [&](const double* v, double* z) {
-    for (int i = 0; i < c.nn; ++i) {
+    parallel_for(c.nn, [&](long i) {
       if (bs == 1) {
         z[i] = Minv[i] * v[i];
       } else {
@@ -586,7 +636,7 @@ int bicgstab(const Case& c, int bs, const double* A, const double* b, double* x,
           z[3 * i + m] = Minv[9L * i + 3 * m] * v[3 * i] + Minv[9L * i + 3 * m + 1] * v[3 * i + 1] +
                          Minv[9L * i + 3 * m + 2] * v[3 * i + 2];
       }
-    }
+    });
   };
   std::vector<double> r(n), rh(n), pv(n, 0.0), v(n, 0.0), s(n), t(n), ph(n), sh(n);
   std::fill(x, x + n, 0.0);
@@ -605,19 +655,19 @@ int bicgstab(const Case& c, int bs, const double* A, const double* b, double* x,
     const double rho1 = dot(n, rh.data(), r.data());
     if (rho1 == 0.0) break;
     const double beta = (rho1 / rho) * (alpha / omega);
-    for (long i = 0; i < n; ++i) pv[i] = r[i] + beta * (pv[i] - omega * v[i]);
+    parallel_for(n, [&](long i) { pv[i] = r[i] + beta * (pv[i] - omega * v[i]); });
     prec(pv.data(), ph.data());
     spmv(c, bs, A, ph.data(), v.data());
     alpha = rho1 / dot(n, rh.data(), v.data());
-    for (long i = 0; i < n; ++i) s[i] = r[i] - alpha * v[i];
+    parallel_for(n, [&](long i) { s[i] = r[i] - alpha * v[i]; });
     prec(s.data(), sh.data());
     spmv(c, bs, A, sh.data(), t.data());
     const double tt = dot(n, t.data(), t.data());
     omega = tt > 0 ? dot(n, t.data(), s.data()) / tt : 0.0;
-    for (long i = 0; i < n; ++i) {
+    parallel_for(n, [&](long i) {
       x[i] += alpha * ph[i] + omega * sh[i];
       r[i] = s[i] - omega * t[i];
-    }
+    });
     rho = rho1;
     rn = std::sqrt(dot(n, r.data(), r.data()));
     if (omega == 0.0) {
@@ -706,6 +756,7 @@ void* orc_case_create(int nn, int ne, const double* x, const int* conn, int nf, 
   c->fBnd.assign(face_bnd, face_bnd + nf);
   c->bndU.assign(bnd_velocity, bnd_velocity + 3L * nbnd);
   build_graph(*c);
+  build_colors(*c);
   dual_volume(*c);
   exposed_areas(*c);
   c->U.assign(3L * nn, 0.0);
