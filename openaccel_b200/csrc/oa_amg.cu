@@ -232,13 +232,13 @@ __global__ void k_gauss_jordan(int n, double* M) {
   }
 }
 
-// pre-smooth from zero and residual in one pass:
-// x = w Dinv b,  r = b - A x (x of the neighbours recomputed from b)
+// Downward step, row parallel: pre-smooth from zero, xs_i = w Dinv_i b_i, and
+// the residual r_i = b_i - sum_j a_ij xs_j (neighbours' xs formed from b).
 template <class T>
-__global__ void __launch_bounds__(AB) k_smooth0_resid(int n, const int* __restrict__ rp, const int* __restrict__ cols,
-                                                      const T* __restrict__ A, const T* __restrict__ dinv,
-                                                      const T* __restrict__ b, T* __restrict__ x, T* __restrict__ r,
-                                                      double w, const int* done) {
+__global__ void __launch_bounds__(AB) k_smooth_resid(int n, const int* __restrict__ rp, const int* __restrict__ cols,
+                                                     const T* __restrict__ A, const T* __restrict__ dinv,
+                                                     const T* __restrict__ b, T* __restrict__ xs, T* __restrict__ r,
+                                                     double w, const int* done) {
   if (*done) return;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
@@ -247,10 +247,13 @@ __global__ void __launch_bounds__(AB) k_smooth0_resid(int n, const int* __restri
     const int j = cols[k];
     s += double(A[k]) * (w * double(dinv[j]) * double(b[j]));
   }
-  x[i] = T(w * double(dinv[i]) * double(b[i]));
-  r[i] = T(double(b[i]) - s);
+  const double bi = double(b[i]);
+  xs[i] = T(w * double(dinv[i]) * bi);
+  r[i] = T(bi - s);
 }
 
+// restriction by the piecewise-constant prolongation: bc_c = sum of the
+// members' residuals, in member order
 template <class T>
 __global__ void k_restrict(int nc, const int* __restrict__ mptr, const int* __restrict__ mlist, const T* __restrict__ r,
                            T* __restrict__ bc, const int* done) {
@@ -262,26 +265,25 @@ __global__ void k_restrict(int nc, const int* __restrict__ mptr, const int* __re
   bc[c] = T(s);
 }
 
+// Fused upward step: prolong (t = xs + alpha P xc, formed on the fly for each
+// neighbour) and post-smooth, x_i = t_i + w Dinv_i (b_i - sum_j a_ij t_j).
+// Reads xs, writes x: out of place, no race between rows.
 template <class T>
-__global__ void k_prolong(int n, const int* __restrict__ agg, const T* __restrict__ x, const T* __restrict__ xc,
-                          T* __restrict__ t, double alpha, const int* done) {
-  if (*done) return;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n) t[i] = T(double(x[i]) + alpha * double(xc[agg[i]]));
-}
-
-// post-smooth: x = t + w Dinv (b - A t)
-template <class T>
-__global__ void __launch_bounds__(AB) k_post(int n, const int* __restrict__ rp, const int* __restrict__ cols,
-                                             const T* __restrict__ A, const T* __restrict__ dinv,
-                                             const T* __restrict__ b, const T* __restrict__ t, T* __restrict__ x,
-                                             double w, const int* done) {
+__global__ void __launch_bounds__(AB) k_up(int n, const int* __restrict__ rp, const int* __restrict__ cols,
+                                           const T* __restrict__ A, const T* __restrict__ dinv,
+                                           const int* __restrict__ agg, const T* __restrict__ b,
+                                           const T* __restrict__ xs, const T* __restrict__ xc, T* __restrict__ x,
+                                           double w, double alpha, const int* done) {
   if (*done) return;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   double s = 0.0;
-  for (int k = rp[i]; k < rp[i + 1]; ++k) s += double(A[k]) * double(t[cols[k]]);
-  x[i] = T(double(t[i]) + w * double(dinv[i]) * (double(b[i]) - s));
+  for (int k = rp[i]; k < rp[i + 1]; ++k) {
+    const int j = cols[k];
+    s += double(A[k]) * (double(xs[j]) + alpha * double(xc[agg[j]]));
+  }
+  const double ti = double(xs[i]) + alpha * double(xc[agg[i]]);
+  x[i] = T(ti + w * double(dinv[i]) * (double(b[i]) - s));
 }
 
 template <class T>
@@ -320,31 +322,29 @@ int Amg<T>::numeric(const T* A_fine, cudaStream_t st) {
 template <class T>
 int Amg<T>::apply(const T* v, T* z, const int* done, cudaStream_t st) {
   const int nl = (int)L.size();
-  // downward pass
+  // downward pass: smooth + residual (row parallel), then restriction
   for (int l = 0; l < nl; ++l) {
     AmgLevel<T>& lv = L[l];
     const T* b = l == 0 ? v : lv.b;
-    T* x = l == 0 ? z : lv.x;
-    const int g = (lv.n + AB - 1) / AB;
     if (l == nl - 1) {
-      k_dense_apply<T><<<g, AB, 0, st>>>(lv.n, dense_inv, b, x, done);
+      T* x = l == 0 ? z : lv.x;
+      k_dense_apply<T><<<(lv.n + AB - 1) / AB, AB, 0, st>>>(lv.n, dense_inv, b, x, done);
       break;
     }
-    k_smooth0_resid<T><<<g, AB, 0, st>>>(lv.n, lv.rp, lv.cols, lv.A, lv.dinv, b, x, lv.r, omega, done);
     AmgLevel<T>& c = L[l + 1];
+    k_smooth_resid<T><<<(lv.n + AB - 1) / AB, AB, 0, st>>>(lv.n, lv.rp, lv.cols, lv.A, lv.dinv, b, lv.t, lv.r, omega,
+                                                            done);
     k_restrict<T><<<(c.n + AB - 1) / AB, AB, 0, st>>>(c.n, lv.mptr, lv.mlist, lv.r, c.b, done);
   }
-  // upward pass
+  // upward pass: one fused prolong/post-smooth kernel per level
   for (int l = nl - 2; l >= 0; --l) {
     AmgLevel<T>& lv = L[l];
     const T* b = l == 0 ? v : lv.b;
     T* x = l == 0 ? z : lv.x;
-    const T* xc = L[l + 1].x;
-    const int g = (lv.n + AB - 1) / AB;
-    k_prolong<T><<<g, AB, 0, st>>>(lv.n, lv.agg, x, xc, lv.t, alpha, done);
-    k_post<T><<<g, AB, 0, st>>>(lv.n, lv.rp, lv.cols, lv.A, lv.dinv, b, lv.t, x, omega, done);
+    k_up<T><<<(lv.n + AB - 1) / AB, AB, 0, st>>>(lv.n, lv.rp, lv.cols, lv.A, lv.dinv, lv.agg, b, lv.t, L[l + 1].x,
+                                                  x, omega, alpha, done);
   }
-  count_launches(4 * (long long)(nl - 1) + 1);
+  count_launches(3 * (long long)(nl - 1) + 1);
   OA_CUDA(cudaGetLastError());
   return OA_OK;
 }

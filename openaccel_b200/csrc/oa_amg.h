@@ -26,7 +26,9 @@ struct AmgLevel {
   // Galerkin gather of the NEXT level's values: coarse entry c sums this
   // level's entries glist[gptr[c] .. gptr[c+1])
   int *gptr = nullptr, *glist = nullptr;
-  T *x = nullptr, *b = nullptr, *r = nullptr, *t = nullptr;  // cycle work vectors
+  // cycle work vectors: x (output, levels > 0), b (input, levels > 0), r
+  // (residual), t (pre-smoothed iterate)
+  T *x = nullptr, *b = nullptr, *r = nullptr, *t = nullptr;
   bool own_A = false;
 };
 

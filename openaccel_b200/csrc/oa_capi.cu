@@ -40,20 +40,6 @@ __global__ void k_from_double(size_t n, const double* a, T* b) {
   const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) b[i] = T(a[i]);
 }
-__global__ void k_sumsq(int n, const double* v, double* out) {
-  // single block ordered reduction (used once per outer iteration)
-  __shared__ double sh[256];
-  double s = 0.0;
-  for (int i = threadIdx.x; i < n; i += 256) s += v[i] * v[i];
-  sh[threadIdx.x] = s;
-  __syncthreads();
-  for (int st = 128; st > 0; st >>= 1) {
-    if (threadIdx.x < st) sh[threadIdx.x] += sh[threadIdx.x + st];
-    __syncthreads();
-  }
-  if (threadIdx.x == 0) *out = sh[0];
-}
-
 }  // namespace oa
 
 using namespace oa;
@@ -199,8 +185,7 @@ int solve_pcorr(oa_flow* h, double rtol, int maxit, int* iters, double* res, int
   const float* A = static_cast<const float*>(f.b.A_pc);
   OA_CUDA(cudaMemsetAsync(f.b.x_pc, 0, sizeof(double) * m.nn, f.stream));
   // ||b||
-  k_sumsq<<<1, 256, 0, f.stream>>>(m.nn, f.b.b_pc, h->scal);
-  count_launches(1);
+  if (int s = device_sumsq(m.nn, f.b.b_pc, h->scal, f.red, f.stream)) return s;
   OA_CUDA(cudaMemcpyAsync(h->hscal, h->scal, sizeof(double), cudaMemcpyDeviceToHost, f.stream));
   OA_CUDA(cudaStreamSynchronize(f.stream));
   const double bnorm = std::sqrt(h->hscal[0]);
@@ -215,7 +200,7 @@ int solve_pcorr(oa_flow* h, double rtol, int maxit, int* iters, double* res, int
     int it = 0;
     double r_in = 0.0;
     // inner tolerance: enough digits for FP32 without stalling
-    const double inner = std::max(rtol / rel, 2e-4);
+    const double inner = std::max(rtol / rel, f.s.pc_amg ? 1e-4 : 2e-4);
     if (int s = h->pc32.solve<float>(A, h->ir_r32, d, std::min(inner, 0.1), std::min(INNER_CAP, maxit - total), &it,
                                      &r_in, f.s.pc_amg ? 5 : 20, nref > 0))
       return s;
@@ -244,8 +229,7 @@ int solve_pcorr(oa_flow* h, double rtol, int maxit, int* iters, double* res, int
 
 int continuity_rms(oa_flow* h, double* out) {
   Flow& f = h->f;
-  k_sumsq<<<1, 256, 0, f.stream>>>(f.mesh->nn, f.b.b_pc, h->scal + 2);
-  count_launches(1);
+  if (int s = device_sumsq(f.mesh->nn, f.b.b_pc, h->scal + 2, f.red, f.stream)) return s;
   OA_CUDA(cudaMemcpyAsync(h->hscal + 2, h->scal + 2, sizeof(double), cudaMemcpyDeviceToHost, f.stream));
   OA_CUDA(cudaStreamSynchronize(f.stream));
   *out = std::sqrt(h->hscal[2] / f.mesh->nn);
@@ -411,7 +395,8 @@ int oa_flow_create(oa_mesh* M, const oa_flow_settings* s, const double* bnd_velo
       (st = dalloc(&f.mDot, 12 * ne)) || (st = dalloc(&f.rho, nn)) || (st = dalloc(&f.mu, nn)) ||
       (st = dalloc(&f.sideU, 3 * nn)) || (st = dalloc(&f.b.b_pc, nn)) || (st = dalloc(&f.b.x_mom, 3 * nn)) ||
       (st = dalloc(&f.b.x_pc, nn)) || (st = dalloc(&f.err_dev, 1)) || (st = dalloc(&H->ir_r, nn)) ||
-      (st = dalloc(&H->ir_r32, nn)) || (st = dalloc(&H->scal, 4))) {
+      (st = dalloc(&H->ir_r32, nn)) || (st = dalloc(&H->scal, 4)) ||
+      (st = dalloc(&f.red, (size_t)partials_size()))) {
     oa_flow_destroy(H);
     return st;
   }
@@ -464,7 +449,7 @@ void oa_flow_destroy(oa_flow* H) {
   if (!H) return;
   Flow& f = H->f;
   void* ptrs[] = {f.U, f.p, f.gradU, f.gradP, f.du, f.div, f.mDot, f.rho, f.mu, f.sideU, f.b.A_mom, f.b.b_mom,
-                  f.b.A_pc, f.b.b_pc, f.b.x_mom, f.b.x_pc, f.err_dev, H->ir_r, H->ir_r32, H->scal};
+                  f.b.A_pc, f.b.b_pc, f.b.x_mom, f.b.x_pc, f.err_dev, H->ir_r, H->ir_r32, H->scal, f.red};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (H->hscal) cudaFreeHost(H->hscal);

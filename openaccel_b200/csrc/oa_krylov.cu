@@ -463,6 +463,30 @@ template int fp64_residual<float>(int, const int*, const int*, const float*, con
 template int fp64_residual<double>(int, const int*, const int*, const double*, const double*, const double*, double*,
                                    double*, double*, cudaStream_t);
 
+__global__ void __launch_bounds__(KB) k_sumsq_partial(int n, const double* __restrict__ v, double* partials) {
+  double s[1] = {0.0};
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) s[0] += v[i] * v[i];
+  block_reduce_store<1>(s, partials, MAX_PARTIALS);
+}
+
+__global__ void __launch_bounds__(KB) k_sum_out(const double* partials, int nb, double* out) {
+  double o[1];
+  final_reduce<1>(partials, nb, o);
+  if (threadIdx.x == 0) *out = o[0];
+}
+
+int device_sumsq(int n, const double* v, double* out, double* partials, cudaStream_t st) {
+  const int gf = (n + KB - 1) / KB;
+  const int g = gf < MAX_PARTIALS ? gf : MAX_PARTIALS;
+  k_sumsq_partial<<<g, KB, 0, st>>>(n, v, partials);
+  k_sum_out<<<1, KB, 0, st>>>(partials, g, out);
+  count_launches(2);
+  OA_CUDA(cudaGetLastError());
+  return OA_OK;
+}
+
+int partials_size() { return 3 * MAX_PARTIALS; }
+
 template <class TV>
 int add_correction(int n, double* x, const TV* d, cudaStream_t st) {
   k_add_correction<TV><<<(n + KB - 1) / KB, KB, 0, st>>>(n, x, d);

@@ -46,5 +46,9 @@ int fp64_residual(int nn, const int* rp, const int* cols, const TM* A, const dou
                   double* partials, double* norm_dev, cudaStream_t st);
 template <class TV>
 int add_correction(int n, double* x, const TV* d, cudaStream_t st);
+// sum of squares of v into *out (device), ordered two-stage reduction;
+// partials must hold partials_size() doubles
+int device_sumsq(int n, const double* v, double* out, double* partials, cudaStream_t st);
+int partials_size();
 
 }  // namespace oa
