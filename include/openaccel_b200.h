@@ -143,6 +143,25 @@ int oa_flow_stream(oa_flow* f, void** stream);
 int oa_launch_count(long long* count);
 int oa_time_kernel(oa_flow* f, int which, int reps, double* ms_per_launch);
 
+/* Allocation-free pressure-correction solve. No counterpart in the reference:
+ * it exists for callers that cannot allocate device memory when they solve
+ * (inside a CUDA stream capture, under an application that owns all device
+ * memory, or in a plug-in that must not allocate). Everything is a device
+ * pointer the caller owns: the CSR graph (row_ptr[nn+1], cols, diag = offset
+ * of the diagonal within each row), A (FP64 values), b and the solution x
+ * [nn]. BiCGStab with Jacobi preconditioning, FP64, to rtol relative to ||b||.
+ * Its work vectors live in one file-scope device array sized for
+ * OA_STATIC_SOLVE_MAX_ROWS rows (about 9.5 MB, held by every GPU that loads the
+ * library until exit); larger systems are rejected with OA_ERR_ARG. All calls
+ * on a device share that array, so calls that overlap on the GPU race: the
+ * caller must serialise them. The first call on a device resolves the array's
+ * device address and should not be made inside a stream capture. stream may be
+ * NULL (default stream). */
+#define OA_STATIC_SOLVE_MAX_ROWS 131072
+int oa_pcorr_solve_static(int nn, const int* row_ptr, const int* cols, const int* diag, const double* A,
+                          const double* b, double* x, double rtol, int maxit, int* iters, double* res,
+                          void* stream);
+
 #ifdef __cplusplus
 }
 #endif

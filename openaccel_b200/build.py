@@ -15,7 +15,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIBDIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(LIBDIR, "libopenaccel_b200.so")
-SOURCES = ["oa_kernels.cu", "oa_krylov.cu", "oa_amg.cu", "oa_capi.cu"]
+SOURCES = ["oa_kernels.cu", "oa_krylov.cu", "oa_amg.cu", "oa_capi.cu", "oa_static_solve.cu"]
 HEADERS = ["oa_hex8.cuh", "oa_rowlane.cuh", "oa_internal.h", "oa_krylov.h", "oa_amg.h"]
 
 NVCC = os.environ.get("NVCC", "nvcc")

@@ -289,14 +289,50 @@ int KrylovSolver<B, TM, TV>::setup(int nn_, const int* rp_, const int* cols_, co
 }
 
 template <int B, class TM, class TV>
-void KrylovSolver<B, TM, TV>::release() {
-  for (auto& v : vec) {
-    if (v) cudaFree(v);
-    v = nullptr;
+size_t KrylovSolver<B, TM, TV>::storage_bytes(int nn_) {
+  const size_t n = (size_t)B * nn_;
+  auto up = [](size_t b) { return (b + 255) / 256 * 256; };
+  return 8 * up(sizeof(TV) * n) + up(sizeof(double) * (size_t)B * B * nn_) + up(sizeof(double) * 3 * MAX_PARTIALS) +
+         up(sizeof(KScal));
+}
+
+template <int B, class TM, class TV>
+int KrylovSolver<B, TM, TV>::attach(int nn_, const int* rp_, const int* cols_, const int* dg_, cudaStream_t st_,
+                                    void* storage, size_t bytes) {
+  release();
+  if (bytes < storage_bytes(nn_)) return fail(OA_ERR_ARG, "Krylov: caller storage too small");
+  nn = nn_;
+  rp = rp_;
+  cols = cols_;
+  dg = dg_;
+  st = st_;
+  external = true;
+  const size_t n = (size_t)B * nn;
+  auto up = [](size_t b) { return (b + 255) / 256 * 256; };
+  char* p = static_cast<char*>(storage);
+  for (int k = 0; k < 8; ++k) {
+    vec[k] = p;
+    p += up(sizeof(TV) * n);
   }
-  if (Minv) cudaFree(Minv);
-  if (partials) cudaFree(partials);
-  if (scal) cudaFree(scal);
+  Minv = reinterpret_cast<double*>(p);
+  p += up(sizeof(double) * (size_t)B * B * nn);
+  partials = reinterpret_cast<double*>(p);
+  p += up(sizeof(double) * 3 * MAX_PARTIALS);
+  scal = p;
+  return OA_OK;
+}
+
+template <int B, class TM, class TV>
+void KrylovSolver<B, TM, TV>::release() {
+  if (!external) {
+    for (auto& v : vec)
+      if (v) cudaFree(v);
+    if (Minv) cudaFree(Minv);
+    if (partials) cudaFree(partials);
+    if (scal) cudaFree(scal);
+  }
+  for (auto& v : vec) v = nullptr;
+  external = false;
   if (hscal) cudaFreeHost(hscal);
   if (graph_exec) cudaGraphExecDestroy(graph_exec);
   graph_exec = nullptr;
@@ -392,12 +428,15 @@ int KrylovSolver<B, TM, TV>::solve(const TM* A, const TB* b, TV*& xout, double r
       return s;
     }
     done_iters += check_every;
-    OA_CUDA(cudaMemcpyAsync(hscal, sc, sizeof(KScal), cudaMemcpyDeviceToHost, st));
+    // pinned staging when the solver owns its storage, else plain host memory
+    void* hdst = hscal ? hscal : static_cast<void*>(hbuf);
+    OA_CUDA(cudaMemcpyAsync(hdst, sc, sizeof(KScal), cudaMemcpyDeviceToHost, st));
     OA_CUDA(cudaStreamSynchronize(st));
-    const KScal* h = static_cast<const KScal*>(hscal);
+    const KScal* h = static_cast<const KScal*>(hdst);
     if (h->done || done_iters >= maxit) break;
   }
-  const KScal* h = static_cast<const KScal*>(hscal);
+  const KScal* h = static_cast<const KScal*>(hscal ? hscal : static_cast<void*>(hbuf));
+  static_assert(sizeof(KScal) <= sizeof(hbuf), "host staging buffer too small");
   if (iters) *iters = h->iters;
   if (res) *res = h->bnorm > 0 ? h->rnorm / h->bnorm : 0.0;
   xout = x;

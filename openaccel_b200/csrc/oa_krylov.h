@@ -28,7 +28,13 @@ struct KrylovSolver {
   int graph_chunk = 0;
   long long graph_launches = 0;
 
+  // storage carved from caller memory instead of cudaMalloc (no allocation)
+  bool external = false;
+  alignas(16) unsigned char hbuf[128];  // host copy of the scalars when not pinned
+
   int setup(int nn, const int* rp, const int* cols, const int* dg, cudaStream_t st);
+  static size_t storage_bytes(int nn);
+  int attach(int nn, const int* rp, const int* cols, const int* dg, cudaStream_t st, void* storage, size_t bytes);
   void release();
   ~KrylovSolver() { release(); }
   // Solve A x = b from x0 = 0; xout points at the solver-owned solution.

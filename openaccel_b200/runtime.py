@@ -19,6 +19,7 @@ OA_TOPO_HEX8 = 8
 OA_TOPO_TET4 = 4
 OA_PREC_FP64 = 0
 OA_PREC_MIXED = 1
+OA_STATIC_SOLVE_MAX_ROWS = 131072
 
 # every symbol the header declares; checked by tests on CPU
 EXPORTS = [
@@ -26,7 +27,7 @@ EXPORTS = [
     "oa_mesh_dual_volume", "oa_flow_create", "oa_flow_destroy", "oa_flow_set_field", "oa_flow_get_field",
     "oa_flow_field_device_ptr", "oa_flow_initialize", "oa_assemble_momentum", "oa_assemble_pcorr",
     "oa_update_mdot", "oa_update_div", "oa_update_gradient", "oa_solve", "oa_simple_iterate", "oa_flow_sync",
-    "oa_flow_stream", "oa_launch_count", "oa_time_kernel",
+    "oa_flow_stream", "oa_launch_count", "oa_time_kernel", "oa_pcorr_solve_static",
 ]
 
 
@@ -104,6 +105,7 @@ def lib():
         "oa_flow_stream": (C.c_int, [vp, P(vp)]),
         "oa_launch_count": (C.c_int, [P(C.c_longlong)]),
         "oa_time_kernel": (C.c_int, [vp, C.c_int, C.c_int, dp]),
+        "oa_pcorr_solve_static": (C.c_int, [C.c_int, vp, vp, vp, vp, vp, vp, C.c_double, C.c_int, ip, dp, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)

@@ -1,0 +1,88 @@
+"""The allocation-free pressure-correction solve, oa_pcorr_solve_static.
+
+It is for callers that cannot allocate device memory when they solve (inside a
+stream capture, under an application that owns all device memory, in a
+plug-in that must not allocate): its work vectors live in a fixed file-scope
+device array instead of cudaMalloc'd buffers. These tests call it through the
+C-ABI on device buffers the test owns and check it against the regular
+entry point (oa_solve on the same assembled system), on two calls in a row
+with two different systems, so state left in the shared array by the first
+call cannot leak into the second. This file is collected last on purpose.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from openaccel_b200 import meshgen
+from openaccel_b200 import runtime as rt
+
+pytestmark = pytest.mark.gpu
+
+
+def rel(a, b):
+    return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)
+
+
+def _system(gf, seed):
+    """Assemble a pressure-correction system from a random (but valid) state."""
+    rng = np.random.default_rng(seed)
+    m = gf.mesh
+    gf.set_field("p", rng.normal(0, 1, m.nn))
+    gf.set_field("gradP", rng.normal(0, 1, 3 * m.nn))
+    gf.set_field("du", rng.uniform(0.1, 1.0, 3 * m.nn))
+    gf.set_field("mDot", rng.normal(0, 0.01, 12 * m.ne))
+    A, b = gf.assemble_pcorr()
+    x_ref, _, res_ref = gf.solve("pcorr", 1e-13, 5000)
+    assert res_ref < 1e-12
+    return A, b, x_ref
+
+
+def _static_solve(dev, A, b):
+    import torch
+
+    L = rt.lib()
+    x = torch.zeros(b.size, dtype=torch.float64, device="cuda")
+    Ad = torch.from_numpy(A).to("cuda")
+    bd = torch.from_numpy(b).to("cuda")
+    it, res = C.c_int(), C.c_double()
+    st = L.oa_pcorr_solve_static(dev["nn"], dev["rp"].data_ptr(), dev["cols"].data_ptr(), dev["diag"].data_ptr(),
+                                 Ad.data_ptr(), bd.data_ptr(), x.data_ptr(), 1e-13, 5000, C.byref(it),
+                                 C.byref(res), C.c_void_p(torch.cuda.current_stream().cuda_stream))
+    assert st == 0, L.oa_last_error().decode()
+    torch.cuda.synchronize()
+    return x.cpu().numpy(), it.value, res.value
+
+
+def test_static_solve_matches_regular_solve_twice():
+    import torch
+
+    m = meshgen.cavity(24, perturb=0.2, seed=21)
+    gm = rt.Mesh(m)
+    gf = rt.Flow(gm, rt.default_settings())
+    rp, cols = gm.graph()
+    diag = np.array([np.searchsorted(cols[rp[i]:rp[i + 1]], i) for i in range(m.nn)], dtype=np.int32)
+    dev = {"nn": m.nn, "rp": torch.from_numpy(rp).to("cuda"), "cols": torch.from_numpy(cols).to("cuda"),
+           "diag": torch.from_numpy(diag).to("cuda")}
+    # first call
+    A1, b1, x1_ref = _system(gf, seed=1)
+    x1, it1, res1 = _static_solve(dev, A1, b1)
+    assert res1 < 1e-12 and it1 > 0
+    assert rel(x1, x1_ref) < 1e-10
+    # second call, different system: the shared array must not carry state over
+    A2, b2, x2_ref = _system(gf, seed=2)
+    x2, it2, res2 = _static_solve(dev, A2, b2)
+    assert res2 < 1e-12
+    assert rel(x2, x2_ref) < 1e-10
+    assert rel(x2, x1) > 1e-3  # genuinely a different system
+
+
+def test_static_solve_rejects_oversized_system():
+    L = rt.lib()
+    n = rt.OA_STATIC_SOLVE_MAX_ROWS + 1
+    dummy = C.c_void_p(16)  # never dereferenced: the size check comes first
+    it, res = C.c_int(), C.c_double()
+    st = L.oa_pcorr_solve_static(n, dummy, dummy, dummy, dummy, dummy, dummy, 1e-8, 10, C.byref(it), C.byref(res),
+                                 None)
+    assert st == 1
+    assert b"exceed the static limit" in L.oa_last_error()
