@@ -255,9 +255,20 @@ def run_ours(args, rank, world):
     return res
 
 
+def cpu_model():
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
 def cpu_sample(args, threads):
-    """Oracle (CPU FP64 restatement) on the same workload: one SIMPLE outer
-    iteration with all host threads."""
+    """Oracle (CPU FP64 restatement, threaded: coloured element loops,
+    Jacobi-BiCGStab) on the same workload: one SIMPLE outer iteration with all
+    host threads. About a minute on 8 cores at 128^3, less on the GPU hosts."""
     from oracle import pyoracle as po
 
     po.set_threads(threads)
@@ -301,6 +312,7 @@ def main():
             "steps": 1, "warmup": 0, "ms_per_step": dt * 1e3, "dtype": "f64", "data": "synthetic",
             "config": {"workload": f"lid-driven cavity {args.cpu_n}^3 hex8 skewed +-20%, Re=100, U0~N(0,0.1)"},
             "cpu_baseline": {"value": v, "unit": "outer_iters/s", "cores": threads, "kind": "port",
+                             "cpu": cpu_model(),
                              "sample": f"1 SIMPLE outer iteration of the {args.cpu_n}^3 workload "
                                        "(oracle restatement; the reference binary cannot be built)"},
             "e2e": {"value": v, "unit": "outer_iters/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -315,6 +327,7 @@ def main():
     if rank == 0 and not args.no_cpu and not args.only_mixed:
         dt, m = cpu_sample(args, threads)
         res["cpu_baseline"] = {"value": 1.0 / dt, "unit": "outer_iters/s", "cores": threads, "kind": "port",
+                               "cpu": cpu_model(),
                                "sample": f"1 SIMPLE outer iteration of the {args.cpu_n}^3 workload, FP64 oracle "
                                          "restatement, all host threads"}
     if rank == 0:

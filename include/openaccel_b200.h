@@ -96,6 +96,12 @@ int oa_flow_set_field(oa_flow* f, const char* name, const double* host, long n);
 int oa_flow_get_field(oa_flow* f, const char* name, double* host, long n);
 /* Device pointer of a named field (for callers that keep data resident). */
 int oa_flow_field_device_ptr(oa_flow* f, const char* name, double** dev);
+/* Pressure-level rows: replaces settings.ref_node with a list, one row per
+ * closed domain of a batched (disjoint-union) mesh. Mirrors
+ * domain::pressureLevelNodeId / adjustMatrixForPressureReference
+ * (src/assemble/flow/segregatedFlow/pressureCorrectionAssembler/pressureCorrectionAssembler.cpp:19-63)
+ * applied per domain. count = 0 removes all reference rows. */
+int oa_flow_set_reference_nodes(oa_flow* f, const int* nodes, int count);
 
 /* navierStokesEquation::initialize / postInitialize and
  * pressureCorrectionEquation::initialize

@@ -396,7 +396,7 @@ int oa_flow_create(oa_mesh* M, const oa_flow_settings* s, const double* bnd_velo
       (st = dalloc(&f.sideU, 3 * nn)) || (st = dalloc(&f.b.b_pc, nn)) || (st = dalloc(&f.b.x_mom, 3 * nn)) ||
       (st = dalloc(&f.b.x_pc, nn)) || (st = dalloc(&f.err_dev, 1)) || (st = dalloc(&H->ir_r, nn)) ||
       (st = dalloc(&H->ir_r32, nn)) || (st = dalloc(&H->scal, 4)) ||
-      (st = dalloc(&f.red, (size_t)partials_size()))) {
+      (st = dalloc(&f.red, (size_t)partials_size())) || (st = dalloc(&f.ref_flag, nn))) {
     oa_flow_destroy(H);
     return st;
   }
@@ -419,6 +419,11 @@ int oa_flow_create(oa_mesh* M, const oa_flow_settings* s, const double* bnd_velo
   cudaMemset(f.div, 0, sizeof(double) * nn);
   cudaMemset(f.mDot, 0, sizeof(double) * 12 * ne);
   cudaMemset(f.err_dev, 0, sizeof(int));
+  cudaMemset(f.ref_flag, 0, nn);
+  if (s->ref_node >= 0) {
+    const uint8_t one = 1;
+    cudaMemcpy(f.ref_flag + s->ref_node, &one, 1, cudaMemcpyHostToDevice);
+  }
   // node-side wall velocity, boundary by boundary in index order
   // (nodeField::updateBoundarySideFieldSpecifiedValue sets parts in turn)
   std::vector<double> side(3 * nn, 0.0);
@@ -449,7 +454,8 @@ void oa_flow_destroy(oa_flow* H) {
   if (!H) return;
   Flow& f = H->f;
   void* ptrs[] = {f.U, f.p, f.gradU, f.gradP, f.du, f.div, f.mDot, f.rho, f.mu, f.sideU, f.b.A_mom, f.b.b_mom,
-                  f.b.A_pc, f.b.b_pc, f.b.x_mom, f.b.x_pc, f.err_dev, H->ir_r, H->ir_r32, H->scal, f.red};
+                  f.b.A_pc, f.b.b_pc, f.b.x_mom, f.b.x_pc, f.err_dev, H->ir_r, H->ir_r32, H->scal, f.red,
+                  f.ref_flag};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (H->hscal) cudaFreeHost(H->hscal);
@@ -490,6 +496,19 @@ int oa_flow_field_device_ptr(oa_flow* H, const char* name, double** dev) {
   size_t len = 0;
   *dev = field_ptr(H->f, name, &len);
   if (!*dev) return fail(OA_ERR_ARG, std::string("oa_flow_field_device_ptr: unknown field ") + name);
+  return OA_OK;
+}
+
+int oa_flow_set_reference_nodes(oa_flow* H, const int* nodes, int count) {
+  if (!H || count < 0 || (count > 0 && !nodes)) return fail(OA_ERR_ARG, "oa_flow_set_reference_nodes: bad arguments");
+  Flow& f = H->f;
+  std::vector<uint8_t> flag(f.mesh->nn, 0);
+  for (int k = 0; k < count; ++k) {
+    if (nodes[k] < 0 || nodes[k] >= f.mesh->nn) return fail(OA_ERR_ARG, "oa_flow_set_reference_nodes: node out of range");
+    flag[nodes[k]] = 1;
+  }
+  OA_CUDA(cudaMemcpyAsync(f.ref_flag, flag.data(), f.mesh->nn, cudaMemcpyHostToDevice, f.stream));
+  OA_CUDA(cudaStreamSynchronize(f.stream));
   return OA_OK;
 }
 

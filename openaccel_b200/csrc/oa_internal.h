@@ -59,6 +59,7 @@ struct Flow {
   double* red = nullptr;        // reduction partials
   double* red_host = nullptr;   // pinned
   int* err_dev = nullptr;       // device error flags
+  uint8_t* ref_flag = nullptr;  // [nn] pressure-level rows (one per closed domain)
   int last_mom_iters = 0, last_pc_iters = 0;
   double last_mom_res = 0, last_pc_res = 0, last_cont = 0;
 };

@@ -219,7 +219,7 @@ struct PcArgs {
   const double *U, *p, *gradP, *du, *mDot, *rho;
   void* A;
   double* b;
-  int ref_node;
+  const uint8_t* ref_flag;  // [nn] 1 on pressure-level rows
   int* err;
 };
 
@@ -328,7 +328,7 @@ __global__ void __launch_bounds__(BLOCK) k_pcorr(PcArgs a) {
   }
   diag[0] = rowsum8(diag[0]);
   rhs = rowsum8(rhs);
-  const bool refrow = rv && row == a.ref_node;
+  const bool refrow = rv && __ldg(a.ref_flag + row) != 0;
   write_row<1, TF>(row, rv, c, lane, diag, nb, nbc, a.m, static_cast<TF*>(a.A),
                    sh_val + warp_base * 3, sh_col + warp_base * 3, refrow);
   if (rv && c == 0) a.b[row] = refrow ? 0.0 : rhs;
@@ -836,7 +836,7 @@ __global__ void k_vel_correct(int n3, double* U, const double* du, const double*
 static int grid_rows(int nn) { return (int)(((size_t)nn * 8 + BLOCK - 1) / BLOCK); }
 
 int launch_pcorr(Flow& f, bool mixed) {
-  PcArgs a{f.mesh->view(), f.U, f.p, f.gradP, f.du, f.mDot, f.rho, f.b.A_pc, f.b.b_pc, f.s.ref_node, f.err_dev};
+  PcArgs a{f.mesh->view(), f.U, f.p, f.gradP, f.du, f.mDot, f.rho, f.b.A_pc, f.b.b_pc, f.ref_flag, f.err_dev};
   const int g = grid_rows(f.mesh->nn);
   const bool us = f.s.u_shifted, ps = f.s.p_grad_shifted;
 #define OA_PC(US, PS, T)                                                                    \

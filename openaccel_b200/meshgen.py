@@ -149,3 +149,49 @@ def initial_velocity(mesh: HexMesh, sigma=0.0, seed=12345):
         interior = (i > 0) & (i < nx) & (j > 0) & (j < ny) & (k > 0) & (k < nz)
         U[interior] = g[interior]
     return U
+
+
+@dataclass
+class CavityBatch:
+    """Disjoint union of independent cavities (one mesh, one launch per kernel)."""
+
+    mesh: HexMesh
+    mu: np.ndarray  # (nn,) per-node viscosity (constant within each cavity)
+    ref_nodes: np.ndarray  # one pressure-level node per cavity
+    node_offsets: np.ndarray  # (count+1,)
+    sizes: np.ndarray  # edge count of each cavity
+    viscosities: np.ndarray
+
+
+def batch_cavities(count=64, nmin=16, nmax=64, mu_min=1e-3, mu_max=1e-1, seed=2024, sizes=None,
+                   lid_velocity=(1.0, 0.0, 0.0)):
+    """Independent unit-cube cavities of uneven size (edge counts U{nmin..nmax})
+    and log-uniform viscosities, concatenated node- and element-wise. Cavity m
+    owns boundaries 2m (lid, z = 1) and 2m+1 (other walls), applied in that
+    order so its lid-edge nodes carry zero wall velocity; its pressure-level
+    node is its first node (the origin corner)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    if sizes is None:
+        sizes = rng.integers(nmin, nmax + 1, size=count)
+    sizes = np.asarray(sizes, dtype=np.int64)
+    visc = np.exp(rng.uniform(np.log(mu_min), np.log(mu_max), size=sizes.size))
+    coords, conns, fe, fo, fb, mus, refs, noff = [], [], [], [], [], [], [], [0]
+    eoff = 0
+    for m, n in enumerate(sizes):
+        c = cavity(int(n), lid_velocity=lid_velocity)
+        coords.append(c.coords)
+        conns.append(c.conn + noff[-1])
+        fe.append(c.face_elem + eoff)
+        fo.append(c.face_ord)
+        fb.append(c.face_bnd + 2 * m)
+        mus.append(np.full(c.nn, visc[m]))
+        refs.append(noff[-1])
+        noff.append(noff[-1] + c.nn)
+        eoff += c.ne
+    bv = np.tile(np.array([list(lid_velocity), [0.0, 0.0, 0.0]]), (sizes.size, 1))
+    mesh = HexMesh(int(sizes.max()), int(sizes.max()), int(sizes.max()), np.concatenate(coords),
+                   np.concatenate(conns).astype(np.int32), np.concatenate(fe).astype(np.int32),
+                   np.concatenate(fo).astype(np.int32), np.concatenate(fb).astype(np.int32), bv,
+                   meta={"kind": "cavity_batch", "count": int(sizes.size), "seed": seed})
+    return CavityBatch(mesh, np.concatenate(mus), np.asarray(refs, np.int32), np.asarray(noff, np.int64), sizes,
+                       visc)

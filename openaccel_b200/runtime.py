@@ -25,7 +25,7 @@ OA_STATIC_SOLVE_MAX_ROWS = 131072
 EXPORTS = [
     "oa_last_error", "oa_version", "oa_mesh_create", "oa_mesh_destroy", "oa_mesh_nnz", "oa_mesh_graph",
     "oa_mesh_dual_volume", "oa_flow_create", "oa_flow_destroy", "oa_flow_set_field", "oa_flow_get_field",
-    "oa_flow_field_device_ptr", "oa_flow_initialize", "oa_assemble_momentum", "oa_assemble_pcorr",
+    "oa_flow_field_device_ptr", "oa_flow_set_reference_nodes", "oa_flow_initialize", "oa_assemble_momentum", "oa_assemble_pcorr",
     "oa_update_mdot", "oa_update_div", "oa_update_gradient", "oa_solve", "oa_simple_iterate", "oa_flow_sync",
     "oa_flow_stream", "oa_launch_count", "oa_time_kernel", "oa_pcorr_solve_static",
 ]
@@ -93,6 +93,7 @@ def lib():
         "oa_flow_set_field": (C.c_int, [vp, C.c_char_p, dp, C.c_long]),
         "oa_flow_get_field": (C.c_int, [vp, C.c_char_p, dp, C.c_long]),
         "oa_flow_field_device_ptr": (C.c_int, [vp, C.c_char_p, P(dp)]),
+        "oa_flow_set_reference_nodes": (C.c_int, [vp, ip, C.c_int]),
         "oa_flow_initialize": (C.c_int, [vp]),
         "oa_assemble_momentum": (C.c_int, [vp, dp, dp]),
         "oa_assemble_pcorr": (C.c_int, [vp, dp, dp]),
@@ -207,6 +208,10 @@ class Flow:
         p = C.POINTER(C.c_double)()
         _check(lib().oa_flow_field_device_ptr(self.h, name.encode(), C.byref(p)))
         return C.cast(p, C.c_void_p).value
+
+    def set_reference_nodes(self, nodes):
+        n = np.ascontiguousarray(nodes, np.int32)
+        _check(lib().oa_flow_set_reference_nodes(self.h, _ip(n), int(n.size)))
 
     def initialize(self):
         _check(lib().oa_flow_initialize(self.h))

@@ -64,6 +64,8 @@ struct Case {
   // element colours (no two elements of a colour share a node), for the
   // threaded CPU-baseline path
   std::vector<std::vector<int>> colors;
+  // pressure-level rows (settings.ref_node, or a list for batched meshes)
+  std::vector<int> refNodes;
   // last assembled systems (for the solver inside simple_iteration)
   std::vector<double> Am, bm, xm, Ap, bp, xp;
 };
@@ -405,8 +407,7 @@ void assemble_pcorr(Case& c, double* A, double* b) {
     }
     apply_coeff<1>(c, A, b, en, 8, rhs, lhs);
   });
-  if (c.s.ref_node >= 0) {
-    const int r = c.s.ref_node;
+  for (const int r : c.refNodes) {
     const double d = A[c.rowPtr[r] + c.diagOff[r]];
     for (int k = c.rowPtr[r]; k < c.rowPtr[r + 1]; ++k) A[k] = 0.0;
     A[c.rowPtr[r] + c.diagOff[r]] = d;
@@ -770,6 +771,7 @@ void* orc_case_create(int nn, int ne, const double* x, const int* conn, int nf, 
   c->mu.assign(nn, s->mu);
   c->sideU.assign(3L * nn, 0.0);
   c->wallNode.assign(nn, 0.0);
+  if (s->ref_node >= 0) c->refNodes.push_back(s->ref_node);
   // node side velocity: boundaries applied in order, later ones overwrite shared
   // nodes (nodeField::updateBoundarySideFieldSpecifiedValue, setToValue per part)
   for (int bnd = 0; bnd < nbnd; ++bnd)
@@ -785,6 +787,11 @@ void* orc_case_create(int nn, int ne, const double* x, const int* conn, int nf, 
 }
 
 void orc_case_destroy(void* h) { delete static_cast<Case*>(h); }
+
+void orc_set_ref_nodes(void* h, const int* nodes, int n) {
+  Case* c = static_cast<Case*>(h);
+  c->refNodes.assign(nodes, nodes + n);
+}
 
 double* orc_case_field(void* h, const char* name, long* len) {
   Case* c = static_cast<Case*>(h);

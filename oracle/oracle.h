@@ -60,6 +60,8 @@ void* orc_case_create(int nn, int ne, const double* x, const int* conn, int nf,
                       const int* face_elem, const int* face_ord, const int* face_bnd,
                       int nbnd, const double* bnd_velocity, const orc_settings* s);
 void orc_case_destroy(void* h);
+/* pressure-level rows (replaces settings.ref_node; one per closed domain) */
+void orc_set_ref_nodes(void* h, const int* nodes, int n);
 /* Pointer to a named field of the case (see oracle.cpp for the list); *len
  * receives the number of doubles. */
 double* orc_case_field(void* h, const char* name, long* len);

@@ -75,6 +75,7 @@ def lib():
         L.orc_case_create.argtypes = [C.c_int, C.c_int, dp, ip, C.c_int, ip, ip, ip, C.c_int, dp,
                                       P(Settings)]
         L.orc_case_destroy.argtypes = [C.c_void_p]
+        L.orc_set_ref_nodes.argtypes = [C.c_void_p, ip, C.c_int]
         L.orc_case_field.restype = dp
         L.orc_case_field.argtypes = [C.c_void_p, C.c_char_p, P(C.c_long)]
         L.orc_case_nnz.restype = C.c_int
@@ -153,6 +154,11 @@ class FlowCase:
         cols = np.zeros(self.nnz, np.int32)
         lib().orc_case_graph(self.h, _ip(rp), _ip(cols))
         return rp, cols
+
+    def set_ref_nodes(self, nodes):
+        n = np.ascontiguousarray(nodes, np.int32)
+        self._keep.append(n)
+        lib().orc_set_ref_nodes(self.h, _ip(n), int(n.size))
 
     def initialize(self):
         lib().orc_initialize(self.h)
