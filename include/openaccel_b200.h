@@ -168,6 +168,58 @@ int oa_pcorr_solve_static(int nn, const int* row_ptr, const int* cols, const int
                           const double* b, double* x, double rtol, int maxit, int* iters, double* res,
                           void* stream);
 
+/* ---- tet4 scalar diffusion (solid-domain energy equation) ----
+ * Replaces phiAssembler<1> in diffusion mode as the thermal energy assembler
+ * drives it in a solid domain: element terms
+ * (src/assemble/phiAssembler/phiAssemblerElemTerms.hpp:11-413), fixed-value
+ * walls (phiAssemblerElemBoundaryConditions.hpp:112-410), the solid source
+ * (src/assemble/heatTransfer/thermalEnergy/thermalEnergyAssemblerNodeTerms.cpp:25-97,
+ * generalised from one domain value to a value per node), relaxation
+ * (phiAssembler.h:748-753,967-1006; thermalEnergyAssembler.h:39-43), and the
+ * solve + clipped correction of thermalEnergyEquation::solve
+ * (src/equation/heatTransfer/thermalEnergy/thermalEnergyEquation.cpp:190-247).
+ * The mesh comes from oa_mesh_create with OA_TOPO_TET4 (conn[ne][4], face
+ * ordinals 0..3 of the Nalu tet4 element, Tet4CVFEM.C:416-421). */
+typedef struct oa_diffusion oa_diffusion;
+enum { OA_BND_FIXED_VALUE = 0, OA_BND_ZERO_FLUX = 1 };
+
+typedef struct oa_diffusion_settings {
+  int shifted;            /* linear_linear interpolation of Gamma (controls.h:95 temperature default) */
+  double urf;             /* diagonal relaxation (energy relaxation factor, controls.h:73) */
+  double wall_rhs_relax;  /* wall-node rhs relaxation (thermalEnergyAssembler.h:42) */
+  double lower_clip;      /* lower clip of the corrected field (thermalEnergyEquation.cpp:212-213) */
+  int maxit;
+  double rtol;
+  int precision;          /* OA_PREC_FP64 or OA_PREC_MIXED */
+  int amg;                /* 1: aggregation-AMG preconditioned BiCGStab, 0: Jacobi */
+  int use_graphs;         /* 1: replay Krylov iteration chunks as CUDA graphs */
+} oa_diffusion_settings;
+
+/* bnd_kind[nbnd] (OA_BND_*) and bnd_value[nbnd] (fixed values) by boundary
+ * index; node-side values are applied boundary by boundary in index order. */
+int oa_diffusion_create(oa_mesh* m, const oa_diffusion_settings* s, const int* bnd_kind, const double* bnd_value,
+                        int nbnd, oa_diffusion** out);
+void oa_diffusion_destroy(oa_diffusion* d);
+/* Node fields [nn]: "phi" (the transported scalar), "gamma" (diffusivity at
+ * nodes, phiAssembler.h:218-224), "src" (volumetric source), "sidePhi". */
+int oa_diffusion_set_field(oa_diffusion* d, const char* name, const double* host, long n);
+int oa_diffusion_get_field(oa_diffusion* d, const char* name, double* host, long n);
+int oa_diffusion_field_device_ptr(oa_diffusion* d, const char* name, double** dev);
+/* Assembly into the handle's CSR system (defect form); optional FP64 host
+ * copies of A [nnz] and b [nn]. */
+int oa_diffusion_assemble(oa_diffusion* d, double* A, double* b);
+/* Solve the last assembled system to rtol (linearSystem::solve(),
+ * src/equation/linearSystem.h:416-462); x [nn] may be NULL. */
+int oa_diffusion_solve(oa_diffusion* d, double rtol, int maxit, double* x, int* iters, double* res,
+                       int* refinements);
+/* One thermalEnergyEquation::solve step: assemble, solve to settings.rtol,
+ * phi += x clipped below at settings.lower_clip. */
+int oa_diffusion_step(oa_diffusion* d, int* iters, double* res, int* refinements);
+/* Measurement hooks (no reference counterpart): the handle's cudaStream_t and
+ * the mean device time of `reps` assembly launches. */
+int oa_diffusion_stream(oa_diffusion* d, void** stream);
+int oa_diffusion_time_assembly(oa_diffusion* d, int reps, double* ms_per_launch);
+
 #ifdef __cplusplus
 }
 #endif

@@ -6,6 +6,7 @@ with nvcc; the shared library exports the C-ABI declared in
 """
 from __future__ import annotations
 
+import concurrent.futures
 import os
 import subprocess
 import sys
@@ -15,8 +16,10 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIBDIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(LIBDIR, "libopenaccel_b200.so")
-SOURCES = ["oa_kernels.cu", "oa_krylov.cu", "oa_amg.cu", "oa_capi.cu", "oa_static_solve.cu"]
-HEADERS = ["oa_hex8.cuh", "oa_rowlane.cuh", "oa_internal.h", "oa_krylov.h", "oa_amg.h"]
+SOURCES = ["oa_kernels.cu", "oa_krylov.cu", "oa_amg.cu", "oa_capi.cu", "oa_static_solve.cu", "oa_scalar_solve.cu",
+           "oa_diffusion.cu"]
+HEADERS = ["oa_geom.cuh", "oa_hex8.cuh", "oa_tet4.cuh", "oa_rowlane.cuh", "oa_internal.h", "oa_krylov.h", "oa_amg.h",
+           "oa_scalar_solve.h"]
 
 NVCC = os.environ.get("NVCC", "nvcc")
 FLAGS = [
@@ -41,14 +44,17 @@ def build(force: bool = False, verbose: bool = False) -> str:
     if not force and not _stale():
         return LIB
     os.makedirs(LIBDIR, exist_ok=True)
-    objs = []
-    for src in SOURCES:
-        obj = os.path.join(LIBDIR, src.replace(".cu", ".o"))
+    objs = [os.path.join(LIBDIR, src.replace(".cu", ".o")) for src in SOURCES]
+
+    def compile_one(src, obj):
         cmd = [NVCC, *FLAGS, "-I", os.path.join(ROOT, "include"), "-c", os.path.join(CSRC, src), "-o", obj]
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)
-        objs.append(obj)
+
+    with concurrent.futures.ThreadPoolExecutor(max_workers=min(len(SOURCES), os.cpu_count() or 1)) as ex:
+        for f in [ex.submit(compile_one, s, o) for s, o in zip(SOURCES, objs)]:
+            f.result()
     tmp = LIB + ".tmp"
     cmd = [NVCC, "-shared", "-gencode", "arch=compute_100a,code=sm_100a", *objs, "-o", tmp, "-lcudart"]
     subprocess.run(cmd, check=True)

@@ -13,6 +13,7 @@
 
 #include "oa_internal.h"
 #include "oa_krylov.h"
+#include "oa_scalar_solve.h"
 
 namespace oa {
 
@@ -44,22 +45,11 @@ __global__ void k_from_double(size_t n, const double* a, T* b) {
 
 using namespace oa;
 
-struct oa_mesh {
-  DeviceMesh m;
-  cudaStream_t st = nullptr;
-};
-
 struct oa_flow {
   Flow f;
-  KrylovSolver<1, double, double> pc64;
   KrylovSolver<3, double, double> mom64;
-  KrylovSolver<1, float, float> pc32;
   KrylovSolver<3, float, float> mom32;
-  Amg<double> amg64;
-  Amg<float> amg32;
-  double* ir_r = nullptr;   // FP64 residual for refinement
-  double* ir_x = nullptr;   // FP64 accumulated solution
-  float* ir_r32 = nullptr;
+  ScalarSolve pc;           // pressure-correction solve
   double* scal = nullptr;   // [4] device scalars
   double* hscal = nullptr;  // pinned
 };
@@ -147,84 +137,21 @@ int solve_momentum(oa_flow* h, double rtol, int maxit, int* iters, double* res, 
   return OA_OK;
 }
 
-// Pressure-correction solve into f.b.x_pc. FP64: BiCGStab to rtol. Mixed:
-// iterative refinement, FP64 residual r = b - A x, FP32 BiCGStab on A d = r to
-// a loose inner tolerance, x += d, until ||r|| <= rtol ||b||.
+// Pressure-correction solve into f.b.x_pc (ScalarSolve: FP64 BiCGStab, or
+// FP32 inner iterations under FP64 iterative refinement).
 int solve_pcorr(oa_flow* h, double rtol, int maxit, int* iters, double* res, int* refinements) {
   Flow& f = h->f;
   DeviceMesh& m = *f.mesh;
-  if (f.s.pc_amg) {
-    Amg<double>* a64 = &h->amg64;
-    Amg<float>* a32 = &h->amg32;
-    if (!mixed(f) && !a64->ready) {
-      if (int s = a64->setup(m.nn, m.h_row_ptr.data(), m.h_cols.data(), m.h_diag.data(), m.row_ptr, m.cols, m.diag))
-        return s;
-    }
-    if (mixed(f) && !a32->ready) {
-      if (int s = a32->setup(m.nn, m.h_row_ptr.data(), m.h_cols.data(), m.h_diag.data(), m.row_ptr, m.cols, m.diag))
-        return s;
-    }
-    h->pc64.amg = mixed(f) ? nullptr : a64;
-    h->pc32.amg = mixed(f) ? a32 : nullptr;
-  } else {
-    h->pc64.amg = nullptr;
-    h->pc32.amg = nullptr;
-  }
-  h->pc64.use_graph = h->pc32.use_graph = f.s.use_graphs != 0;
-  if (!mixed(f)) {
-    if (int s = h->pc64.setup(m.nn, m.row_ptr, m.cols, m.diag, f.stream)) return s;
-    double* x = nullptr;
-    if (int s = h->pc64.solve<double>(static_cast<const double*>(f.b.A_pc), f.b.b_pc, x, rtol, maxit, iters, res,
-                                      f.s.pc_amg ? 5 : 20))
-      return s;
-    OA_CUDA(cudaMemcpyAsync(f.b.x_pc, x, sizeof(double) * m.nn, cudaMemcpyDeviceToDevice, f.stream));
-    if (refinements) *refinements = 0;
-    return OA_OK;
-  }
-  if (int s = h->pc32.setup(m.nn, m.row_ptr, m.cols, m.diag, f.stream)) return s;
-  const float* A = static_cast<const float*>(f.b.A_pc);
-  OA_CUDA(cudaMemsetAsync(f.b.x_pc, 0, sizeof(double) * m.nn, f.stream));
-  // ||b||
-  if (int s = device_sumsq(m.nn, f.b.b_pc, h->scal, f.red, f.stream)) return s;
-  OA_CUDA(cudaMemcpyAsync(h->hscal, h->scal, sizeof(double), cudaMemcpyDeviceToHost, f.stream));
-  OA_CUDA(cudaStreamSynchronize(f.stream));
-  const double bnorm = std::sqrt(h->hscal[0]);
-  int total = 0, nref = 0;
-  double rel = bnorm > 0 ? 1.0 : 0.0;
-  OA_CUDA(cudaMemcpyAsync(h->ir_r, f.b.b_pc, sizeof(double) * m.nn, cudaMemcpyDeviceToDevice, f.stream));
-  constexpr int INNER_CAP = 300;  // FP32 Krylov iterations per refinement
-  while (rel > rtol && total < maxit && nref < 40) {
-    k_from_double<float><<<(m.nn + 255) / 256, 256, 0, f.stream>>>(m.nn, h->ir_r, h->ir_r32);
-    count_launches(1);
-    float* d = nullptr;
-    int it = 0;
-    double r_in = 0.0;
-    // inner tolerance: enough digits for FP32 without stalling
-    const double inner = std::max(rtol / rel, f.s.pc_amg ? 1e-4 : 2e-4);
-    if (int s = h->pc32.solve<float>(A, h->ir_r32, d, std::min(inner, 0.1), std::min(INNER_CAP, maxit - total), &it,
-                                     &r_in, f.s.pc_amg ? 5 : 20, nref > 0))
-      return s;
-    total += it;
-    // a diverged inner solve contributes nothing; the next pass restarts from
-    // the FP64 residual
-    if (h->pc32.last_status != 3 && r_in < 1.0) add_correction<float>(m.nn, f.b.x_pc, d, f.stream);
-    if (int s = fp64_residual<float>(m.nn, m.row_ptr, m.cols, A, f.b.x_pc, f.b.b_pc, h->ir_r, h->pc32.partials,
-                                     h->scal + 1, f.stream))
-      return s;
-    OA_CUDA(cudaMemcpyAsync(h->hscal + 1, h->scal + 1, sizeof(double), cudaMemcpyDeviceToHost, f.stream));
-    OA_CUDA(cudaStreamSynchronize(f.stream));
-    rel = bnorm > 0 ? h->hscal[1] / bnorm : 0.0;
-    if (std::getenv("OA_DEBUG"))
-      std::fprintf(stderr, "[oa] pcorr refinement %d: inner iters %d inner res %.3e |b| %.3e rel %.3e\n", nref, it,
-                   r_in, bnorm, rel);
-    ++nref;
-    if (!(rel < INFINITY)) return fail(OA_ERR_SOLVER, "pressure refinement: non-finite residual");
-    if (it == 0) break;
-  }
-  if (iters) *iters = total;
-  if (res) *res = rel;
-  if (refinements) *refinements = nref;
-  return OA_OK;
+  ScalarGraph g;
+  g.nn = m.nn;
+  g.rp = m.row_ptr;
+  g.cols = m.cols;
+  g.diag = m.diag;
+  g.h_rp = m.h_row_ptr.data();
+  g.h_cols = m.h_cols.data();
+  g.h_diag = m.h_diag.data();
+  return h->pc.solve(g, mixed(f), f.s.pc_amg != 0, f.s.use_graphs != 0, f.b.A_pc, f.b.b_pc, f.b.x_pc, rtol, maxit,
+                     iters, res, refinements, f.stream, "pressure");
 }
 
 int continuity_rms(oa_flow* h, double* out) {
@@ -246,8 +173,17 @@ const char* oa_version(void) { return "openaccel_b200 0.1 (sm_100a)"; }
 int oa_mesh_create(const double* coords, int nn, const int* conn, int ne, int topo, const int* face_elem,
                    const int* face_ord, const int* face_bnd, int nf, oa_mesh** out) {
   if (!out || !coords || !conn || nn <= 0 || ne <= 0 || nf < 0) return fail(OA_ERR_ARG, "oa_mesh_create: bad arguments");
-  if (topo != OA_TOPO_HEX8) return fail(OA_ERR_MESH, "oa_mesh_create: only hex8 meshes are supported by this build");
+  if (topo != OA_TOPO_HEX8 && topo != OA_TOPO_TET4) return fail(OA_ERR_MESH, "oa_mesh_create: unknown topology");
   *out = nullptr;
+  if (topo == OA_TOPO_TET4) {
+    oa_mesh* M = new oa_mesh();
+    if (int s = create_tet4_mesh(M, coords, nn, conn, ne, face_elem, face_ord, face_bnd, nf)) {
+      oa_mesh_destroy(M);
+      return s;
+    }
+    *out = M;
+    return OA_OK;
+  }
   for (long k = 0; k < 8L * ne; ++k)
     if (conn[k] < 0 || conn[k] >= nn) return fail(OA_ERR_MESH, "oa_mesh_create: connectivity index out of range");
   for (int f = 0; f < nf; ++f)
@@ -351,7 +287,8 @@ int oa_mesh_create(const double* coords, int nn, const int* conn, int ne, int to
 void oa_mesh_destroy(oa_mesh* M) {
   if (!M) return;
   DeviceMesh& m = M->m;
-  void* ptrs[] = {m.x, m.conn, m.n2e, m.row_ptr, m.cols, m.diag, m.face_mask, m.vol, m.wscv, m.wall_node};
+  void* ptrs[] = {m.x,       m.conn,      m.n2e,      m.n2e_ptr,  m.n2f,       m.n2f_ptr, m.face_elem, m.face_ord,
+                  m.face_bnd, m.row_ptr, m.cols,     m.diag,     m.face_mask, m.vol,     m.wscv,      m.wall_node};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (M->st) cudaStreamDestroy(M->st);
@@ -382,6 +319,7 @@ int oa_flow_create(oa_mesh* M, const oa_flow_settings* s, const double* bnd_velo
   if (s->urf_u <= 0 || s->urf_p <= 0 || s->dt <= 0) return fail(OA_ERR_ARG, "oa_flow_create: relaxation/timescale must be > 0");
   if (s->precision != OA_PREC_FP64 && s->precision != OA_PREC_MIXED) return fail(OA_ERR_ARG, "oa_flow_create: unknown precision");
   if (s->ref_node >= M->m.nn) return fail(OA_ERR_ARG, "oa_flow_create: ref_node out of range");
+  if (M->m.topo != OA_TOPO_HEX8) return fail(OA_ERR_MESH, "oa_flow_create: the flow path needs a hex8 mesh");
   *out = nullptr;
   oa_flow* H = new oa_flow();
   Flow& f = H->f;
@@ -394,8 +332,7 @@ int oa_flow_create(oa_mesh* M, const oa_flow_settings* s, const double* bnd_velo
       (st = dalloc(&f.gradP, 3 * nn)) || (st = dalloc(&f.du, 3 * nn)) || (st = dalloc(&f.div, nn)) ||
       (st = dalloc(&f.mDot, 12 * ne)) || (st = dalloc(&f.rho, nn)) || (st = dalloc(&f.mu, nn)) ||
       (st = dalloc(&f.sideU, 3 * nn)) || (st = dalloc(&f.b.b_pc, nn)) || (st = dalloc(&f.b.x_mom, 3 * nn)) ||
-      (st = dalloc(&f.b.x_pc, nn)) || (st = dalloc(&f.err_dev, 1)) || (st = dalloc(&H->ir_r, nn)) ||
-      (st = dalloc(&H->ir_r32, nn)) || (st = dalloc(&H->scal, 4)) ||
+      (st = dalloc(&f.b.x_pc, nn)) || (st = dalloc(&f.err_dev, 1)) || (st = dalloc(&H->scal, 4)) ||
       (st = dalloc(&f.red, (size_t)partials_size())) || (st = dalloc(&f.ref_flag, nn))) {
     oa_flow_destroy(H);
     return st;
@@ -454,17 +391,14 @@ void oa_flow_destroy(oa_flow* H) {
   if (!H) return;
   Flow& f = H->f;
   void* ptrs[] = {f.U, f.p, f.gradU, f.gradP, f.du, f.div, f.mDot, f.rho, f.mu, f.sideU, f.b.A_mom, f.b.b_mom,
-                  f.b.A_pc, f.b.b_pc, f.b.x_mom, f.b.x_pc, f.err_dev, H->ir_r, H->ir_r32, H->scal, f.red,
+                  f.b.A_pc, f.b.b_pc, f.b.x_mom, f.b.x_pc, f.err_dev, H->scal, f.red,
                   f.ref_flag};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (H->hscal) cudaFreeHost(H->hscal);
-  H->pc64.release();
+  H->pc.release();
   H->mom64.release();
-  H->pc32.release();
   H->mom32.release();
-  H->amg64.release();
-  H->amg32.release();
   if (f.stream) cudaStreamDestroy(f.stream);
   delete H;
 }

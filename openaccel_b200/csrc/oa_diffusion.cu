@@ -1,0 +1,627 @@
+// tet4 scalar-diffusion path of the B200 CVFEM engine: tet4 mesh set-up,
+// the row-owner diffusion assembly kernel, and the C-ABI of the diffusion
+// handle (a solid-domain energy equation: Gamma-diffusion with a volumetric
+// source, fixed-value and zero-flux walls).
+//
+// Reference: src/assemble/phiAssembler/phiAssemblerElemTerms.hpp:11-413
+// (diffusion branch), phiAssemblerElemBoundaryConditions.hpp:112-410
+// (fixed-value wall), src/assemble/heatTransfer/thermalEnergy/
+// thermalEnergyAssemblerNodeTerms.cpp:25-97 (solid source), phiAssembler.h:
+// 748-753,967-1152 and thermalEnergyAssembler.h:39-43 (relaxation), and
+// src/equation/heatTransfer/thermalEnergy/thermalEnergyEquation.cpp:190-247
+// (assemble, solve, clipped correction).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <climits>
+#include <cstdint>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "oa_internal.h"
+#include "oa_scalar_solve.h"
+#include "oa_tet4.cuh"
+
+namespace oa {
+
+namespace {
+
+constexpr int DWARPS = 4;          // rows per 128-thread block
+constexpr int DIFF_MAX_ROW = 64;   // columns per row the row-owner kernel holds
+
+template <class T>
+int dalloc(T** p, size_t n) {
+  cudaError_t e = cudaMalloc(p, sizeof(T) * (n ? n : 1));
+  if (e != cudaSuccess) return fail(OA_ERR_CUDA, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+  return OA_OK;
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+__device__ __forceinline__ void load3(const double* __restrict__ p, int n, double (&v)[3]) {
+  v[0] = __ldg(p + 3 * n);
+  v[1] = __ldg(p + 3 * n + 1);
+  v[2] = __ldg(p + 3 * n + 2);
+}
+
+// ---------------------------------------------------------------------------
+// geometry set-up: SCV volumes per element, then dual volumes per node
+
+__global__ void k_tet_scv(MeshView m, double* __restrict__ scv, int* err) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= m.ne) return;
+  double x[4][3], v[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) load3(m.x, __ldg(m.conn + 4 * e + k), x[k]);
+  tet4::scv_volumes(x, v);
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    if (!(v[k] > 0.0)) err[0] = 1;
+    scv[4 * e + k] = v[k];
+  }
+}
+
+// mesh::updateDualNodalVolumeField_ (src/mesh/meshGeometry.cpp:1277-1345),
+// summed in ascending element order.
+__global__ void k_tet_dual_volume(MeshView m, const double* __restrict__ scv) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= m.nn) return;
+  double v = 0.0;
+  for (int k = m.n2e_ptr[i]; k < m.n2e_ptr[i + 1]; ++k) v += scv[m.n2e[k]];
+  m.vol[i] = v;
+}
+
+}  // namespace
+
+int create_tet4_mesh(oa_mesh* M, const double* coords, int nn, const int* conn, int ne, const int* face_elem,
+                     const int* face_ord, const int* face_bnd, int nf) {
+  DeviceMesh& m = M->m;
+  for (long k = 0; k < 4L * ne; ++k)
+    if (conn[k] < 0 || conn[k] >= nn) return fail(OA_ERR_MESH, "oa_mesh_create: connectivity index out of range");
+  for (int f = 0; f < nf; ++f)
+    if (face_elem[f] < 0 || face_elem[f] >= ne || face_ord[f] < 0 || face_ord[f] > 3 || face_bnd[f] < 0)
+      return fail(OA_ERR_MESH, "oa_mesh_create: boundary face out of range");
+  if (4L * ne > INT_MAX / 2) return fail(OA_ERR_MESH, "oa_mesh_create: too many elements for 32-bit incidence codes");
+  m.topo = OA_TOPO_TET4;
+  m.nn = nn;
+  m.ne = ne;
+  m.nf = nf;
+  // node -> (element, corner), ascending element
+  std::vector<int> n2e_ptr(nn + 1, 0), n2e(4L * ne);
+  for (long k = 0; k < 4L * ne; ++k) n2e_ptr[conn[k] + 1] += 1;
+  for (int i = 0; i < nn; ++i) n2e_ptr[i + 1] += n2e_ptr[i];
+  {
+    std::vector<int> pos(n2e_ptr.begin(), n2e_ptr.end() - 1);
+    for (int e = 0; e < ne; ++e)
+      for (int a = 0; a < 4; ++a) n2e[pos[conn[4L * e + a]]++] = 4 * e + a;
+  }
+  // node -> (boundary face, side position), ascending face
+  std::vector<int> n2f_ptr(nn + 1, 0), n2f(3L * nf);
+  std::vector<int> wall(nn, 0);
+  for (int f = 0; f < nf; ++f)
+    for (int k = 0; k < 3; ++k) {
+      const int nd = conn[4L * face_elem[f] + tet4::side_node(face_ord[f], k)];
+      n2f_ptr[nd + 1] += 1;
+      wall[nd] = 1;
+    }
+  for (int i = 0; i < nn; ++i) n2f_ptr[i + 1] += n2f_ptr[i];
+  {
+    std::vector<int> pos(n2f_ptr.begin(), n2f_ptr.end() - 1);
+    for (int f = 0; f < nf; ++f)
+      for (int k = 0; k < 3; ++k) n2f[pos[conn[4L * face_elem[f] + tet4::side_node(face_ord[f], k)]]++] = 4 * f + k;
+  }
+  // edge graph (every node pair of an element), sorted columns
+  m.h_row_ptr.assign(nn + 1, 0);
+  m.h_diag.assign(nn, 0);
+  m.h_cols.clear();
+  m.h_cols.reserve((size_t)nn * 16);
+  std::vector<int> tmp;
+  for (int i = 0; i < nn; ++i) {
+    tmp.clear();
+    for (int k = n2e_ptr[i]; k < n2e_ptr[i + 1]; ++k) {
+      const int e = n2e[k] >> 2;
+      for (int a = 0; a < 4; ++a) tmp.push_back(conn[4L * e + a]);
+    }
+    tmp.push_back(i);
+    std::sort(tmp.begin(), tmp.end());
+    tmp.erase(std::unique(tmp.begin(), tmp.end()), tmp.end());
+    if ((int)tmp.size() > DIFF_MAX_ROW)
+      return fail(OA_ERR_MESH, "oa_mesh_create: a tet4 node has more than 63 neighbours");
+    for (size_t k = 0; k < tmp.size(); ++k)
+      if (tmp[k] == i) m.h_diag[i] = (int)k;
+    m.h_cols.insert(m.h_cols.end(), tmp.begin(), tmp.end());
+    m.h_row_ptr[i + 1] = (int)m.h_cols.size();
+  }
+  m.nnz = m.h_row_ptr[nn];
+  m.h_conn.assign(conn, conn + 4L * ne);
+  m.h_face_elem.assign(face_elem, face_elem + nf);
+  m.h_face_ord.assign(face_ord, face_ord + nf);
+  m.h_face_bnd.assign(face_bnd, face_bnd + nf);
+  int st = OA_OK;
+  if ((st = dalloc(&m.x, 3L * nn)) || (st = dalloc(&m.conn, 4L * ne)) || (st = dalloc(&m.n2e, 4L * ne)) ||
+      (st = dalloc(&m.n2e_ptr, nn + 1L)) || (st = dalloc(&m.n2f, 3L * nf)) || (st = dalloc(&m.n2f_ptr, nn + 1L)) ||
+      (st = dalloc(&m.face_elem, (size_t)nf)) || (st = dalloc(&m.face_ord, (size_t)nf)) ||
+      (st = dalloc(&m.face_bnd, (size_t)nf)) || (st = dalloc(&m.row_ptr, nn + 1L)) ||
+      (st = dalloc(&m.cols, (size_t)m.nnz)) || (st = dalloc(&m.diag, (size_t)nn)) || (st = dalloc(&m.vol, (size_t)nn)) ||
+      (st = dalloc(&m.wall_node, (size_t)nn)))
+    return st;
+  cudaStreamCreateWithFlags(&M->st, cudaStreamNonBlocking);
+  cudaMemcpy(m.x, coords, sizeof(double) * 3 * nn, cudaMemcpyHostToDevice);
+  cudaMemcpy(m.conn, conn, sizeof(int) * 4 * (size_t)ne, cudaMemcpyHostToDevice);
+  cudaMemcpy(m.n2e, n2e.data(), sizeof(int) * n2e.size(), cudaMemcpyHostToDevice);
+  cudaMemcpy(m.n2e_ptr, n2e_ptr.data(), sizeof(int) * (nn + 1), cudaMemcpyHostToDevice);
+  if (nf) {
+    cudaMemcpy(m.n2f, n2f.data(), sizeof(int) * n2f.size(), cudaMemcpyHostToDevice);
+    cudaMemcpy(m.face_elem, face_elem, sizeof(int) * nf, cudaMemcpyHostToDevice);
+    cudaMemcpy(m.face_ord, face_ord, sizeof(int) * nf, cudaMemcpyHostToDevice);
+    cudaMemcpy(m.face_bnd, face_bnd, sizeof(int) * nf, cudaMemcpyHostToDevice);
+  }
+  cudaMemcpy(m.n2f_ptr, n2f_ptr.data(), sizeof(int) * (nn + 1), cudaMemcpyHostToDevice);
+  cudaMemcpy(m.row_ptr, m.h_row_ptr.data(), sizeof(int) * (nn + 1), cudaMemcpyHostToDevice);
+  cudaMemcpy(m.cols, m.h_cols.data(), sizeof(int) * m.nnz, cudaMemcpyHostToDevice);
+  cudaMemcpy(m.diag, m.h_diag.data(), sizeof(int) * nn, cudaMemcpyHostToDevice);
+  cudaMemcpy(m.wall_node, wall.data(), sizeof(int) * nn, cudaMemcpyHostToDevice);
+  cudaError_t ce = cudaDeviceSynchronize();
+  if (ce == cudaSuccess) ce = cudaGetLastError();
+  if (ce != cudaSuccess) return fail(OA_ERR_CUDA, std::string("tet4 mesh upload: ") + cudaGetErrorString(ce));
+  // dual volumes
+  double* scv = nullptr;
+  int* err = nullptr;
+  if ((st = dalloc(&scv, 4L * ne)) || (st = dalloc(&err, 1))) {
+    if (scv) cudaFree(scv);
+    return st;
+  }
+  cudaMemset(err, 0, sizeof(int));
+  k_tet_scv<<<(ne + 127) / 128, 128>>>(m.view(), scv, err);
+  k_tet_dual_volume<<<(nn + 127) / 128, 128>>>(m.view(), scv);
+  count_launches(2);
+  int herr = 0;
+  ce = cudaMemcpy(&herr, err, sizeof(int), cudaMemcpyDeviceToHost);
+  cudaFree(scv);
+  cudaFree(err);
+  if (ce != cudaSuccess) return fail(OA_ERR_CUDA, std::string("tet4 geometry: ") + cudaGetErrorString(ce));
+  m.geom_err = herr;
+  if (herr) return fail(OA_ERR_GEOMETRY, "non-positive sub-control volume in tet4 mesh");
+  return OA_OK;
+}
+
+namespace {
+
+// Per-handle view of the diffusion fields.
+struct DiffView {
+  const double* phi;
+  const double* gamma;
+  const double* src;
+  const double* side;      // node-side values of the fixed-value boundaries
+  const int* bnd_kind;     // OA_BND_* per boundary index
+  int nbnd;
+  double urf_inv;          // 1 / diagonal relaxation
+  double wall_relax;       // wall-node rhs factor
+};
+
+// Row-owner diffusion assembly. One warp per CSR row; lane l takes the l-th
+// incident item of the row (an element seen from one of its corners, or a
+// fixed-value boundary face seen from one of its side nodes), in 32-item
+// chunks. An element item adds the owner's share of the element's diffusion
+// operator,
+//   row(owner), col(k) += -dN_k/dx . S,   S = sum over the three SCS ips
+//   around the owner of Gamma_ip * A_ip (A pointing away from the owner),
+// with the defect rhs += grad(phi) . S. A face item adds the fixed-value flux
+// of its boundary ip: lhs on the off-face node only (the side nodes' columns
+// carry bcMultiplier 0) and rhs += Gamma_bip * grad(phi~) . A_bip with phi~ the
+// side values on the face nodes. The diagonal and rhs are warp sums; each
+// off-diagonal entry is summed by the lane owning its CSR slot over the items
+// in ascending order, so every entry is written once and the result does not
+// depend on scheduling.
+template <bool SH, class TM>
+__global__ void __launch_bounds__(32 * DWARPS) k_diffusion(MeshView m, DiffView d, TM* __restrict__ A,
+                                                             double* __restrict__ b, int* err) {
+  __shared__ double s_v[DWARPS][32][3];
+  __shared__ uint32_t s_s[DWARPS][32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int row = blockIdx.x * DWARPS + w;
+  if (row >= m.nn) return;  // whole warp
+  const int beg = __ldg(m.row_ptr + row), len = __ldg(m.row_ptr + row + 1) - beg, dslot = __ldg(m.diag + row);
+  const int colA = lane < len ? __ldg(m.cols + beg + lane) : -1;
+  const int colB = lane + 32 < len ? __ldg(m.cols + beg + lane + 32) : -1;
+  const int ea = __ldg(m.n2e_ptr + row), n_el = __ldg(m.n2e_ptr + row + 1) - ea;
+  const int fa = __ldg(m.n2f_ptr + row), n_fc = __ldg(m.n2f_ptr + row + 1) - fa;
+  const int nitems = n_el + n_fc;
+  // shape-function weights of Gamma at an SCS ip (edge nodes, other nodes) and
+  // at a tri3 boundary ip (own node, other nodes)
+  const double wn = SH ? 0.5 : 13.0 / 36.0, wf = SH ? 0.0 : 5.0 / 36.0;
+  const double fo = SH ? 1.0 : 1.0 - 7.0 / 36.0 - 7.0 / 36.0, ff = SH ? 0.0 : 7.0 / 36.0;
+  double accA = 0.0, accB = 0.0, dsum = 0.0, rsum = 0.0;
+  bool bad = false;
+  for (int base = 0; base < nitems; base += 32) {
+    const int it = base + lane;
+    double vd = 0.0, r = 0.0, v[3] = {0.0, 0.0, 0.0};
+    int nb[3] = {-1, -1, -1};
+    if (it < n_el) {
+      const int code = __ldg(m.n2e + ea + it);
+      const int e = code >> 2, a = code & 3;
+      double x[4][3], ph[4], gm[4];
+      int nd[4];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        nd[k] = __ldg(m.conn + 4 * e + tet4::perm_at(a, k));
+        load3(m.x, nd[k], x[k]);
+        ph[k] = __ldg(d.phi + nd[k]);
+        gm[k] = __ldg(d.gamma + nd[k]);
+      }
+      double Ar[3][3], g[4][3];
+      tet4::corner0_areas(x, Ar);
+      if (!tet4::grad_op(x, g)) bad = true;
+      // Gamma at the ips of edges 0-1, 0-2, 0-3
+      const double G1 = wn * (gm[0] + gm[1]) + wf * (gm[2] + gm[3]);
+      const double G2 = wn * (gm[0] + gm[2]) + wf * (gm[1] + gm[3]);
+      const double G3 = wn * (gm[0] + gm[3]) + wf * (gm[1] + gm[2]);
+      double S[3];
+#pragma unroll
+      for (int j = 0; j < 3; ++j) S[j] = G1 * Ar[0][j] + G2 * Ar[1][j] + G3 * Ar[2][j];
+      double c[4];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) c[k] = -(g[k][0] * S[0] + g[k][1] * S[1] + g[k][2] * S[2]);
+      vd = c[0];
+      r = -(c[0] * ph[0] + c[1] * ph[1] + c[2] * ph[2] + c[3] * ph[3]);
+#pragma unroll
+      for (int q = 0; q < 3; ++q) {
+        v[q] = c[q + 1];
+        nb[q] = nd[q + 1];
+      }
+    } else if (it < nitems) {
+      const int code = __ldg(m.n2f + fa + (it - n_el));
+      const int f = code >> 2, k = code & 3;
+      const int bnd = __ldg(m.face_bnd + f);
+      if (bnd < d.nbnd && __ldg(d.bnd_kind + bnd) == OA_BND_FIXED_VALUE) {
+        const int e = __ldg(m.face_elem + f), o = __ldg(m.face_ord + f);
+        // element nodes as (opposite node, side nodes in side order): a
+        // positively oriented ordering with the face opposite local node 0
+        double x[4][3], g[4][3], p[3][3], Af[3];
+        int nd[4];
+        nd[0] = __ldg(m.conn + 4 * e + tet4::opposite_node(o));
+#pragma unroll
+        for (int q = 0; q < 3; ++q) nd[q + 1] = __ldg(m.conn + 4 * e + tet4::side_node(o, q));
+#pragma unroll
+        for (int q = 0; q < 4; ++q) load3(m.x, nd[q], x[q]);
+        if (!tet4::grad_op(x, g)) bad = true;
+        double gs[3], grad_t[3];
+        const double po = __ldg(d.phi + nd[0]);
+#pragma unroll
+        for (int j = 0; j < 3; ++j) grad_t[j] = po * g[0][j];
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+#pragma unroll
+          for (int j = 0; j < 3; ++j) p[q][j] = x[q + 1][j];
+          gs[q] = __ldg(d.gamma + nd[q + 1]);
+          const double ps = __ldg(d.side + nd[q + 1]);
+#pragma unroll
+          for (int j = 0; j < 3; ++j) grad_t[j] += ps * g[q + 1][j];
+        }
+        double Aall[3][3];
+        tet4::tri_face_areas(p, Aall);
+#pragma unroll
+        for (int j = 0; j < 3; ++j) Af[j] = k == 0 ? Aall[0][j] : (k == 1 ? Aall[1][j] : Aall[2][j]);
+        const double gk = k == 0 ? gs[0] : (k == 1 ? gs[1] : gs[2]);
+        const double G = fo * gk + ff * (gs[0] + gs[1] + gs[2] - gk);
+        v[0] = -G * (g[0][0] * Af[0] + g[0][1] * Af[1] + g[0][2] * Af[2]);
+        nb[0] = nd[0];
+        r = G * (grad_t[0] * Af[0] + grad_t[1] * Af[1] + grad_t[2] * Af[2]);
+      }
+    }
+    dsum += warp_sum(vd);
+    rsum += warp_sum(r);
+    // CSR slots of the item's off-diagonal columns
+    int sl[3] = {-1, -1, -1};
+    for (int s = 0; s < len; ++s) {
+      const int cs = __shfl_sync(0xffffffffu, s < 32 ? colA : colB, s & 31);
+#pragma unroll
+      for (int q = 0; q < 3; ++q)
+        if (nb[q] == cs) sl[q] = s;
+    }
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      if (nb[q] >= 0 && sl[q] < 0) sl[q] = dslot;  // column outside the stencil: lumped into the diagonal
+      s_v[w][lane][q] = v[q];
+    }
+    s_s[w][lane] = (uint32_t)(sl[0] + 1) | (uint32_t)(sl[1] + 1) << 8 | (uint32_t)(sl[2] + 1) << 16;
+    __syncwarp();
+    const int cnt = min(32, nitems - base);
+    for (int i = 0; i < cnt; ++i) {
+      const uint32_t pk = s_s[w][i];
+#pragma unroll
+      for (int q = 0; q < 3; ++q) {
+        const int sq = (int)((pk >> (8 * q)) & 255u) - 1;
+        if (sq == lane) accA += s_v[w][i][q];
+        else if (sq == lane + 32) accB += s_v[w][i][q];
+      }
+    }
+    __syncwarp();
+  }
+  // diagonal: element share, then relaxation (diag / urf)
+  if (dslot == lane) accA = (accA + dsum) * d.urf_inv;
+  else if (dslot == lane + 32) accB = (accB + dsum) * d.urf_inv;
+  if (lane < len) A[beg + lane] = TM(accA);
+  if (lane + 32 < len) A[beg + lane + 32] = TM(accB);
+  if (lane == 0) {
+    double bb = __ldg(d.src + row) * __ldg(m.vol + row) + rsum;
+    if (__ldg(m.wall_node + row)) bb *= d.wall_relax;
+    b[row] = bb;
+  }
+  if (bad) err[0] = 1;
+}
+
+// phi <- phi + x, clipped below (equation::correctField_ with CLIP,
+// src/equation/equation.h:204-286).
+__global__ void k_correct_clip(int n, double* __restrict__ phi, const double* __restrict__ x, double lo) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double p = phi[i];
+  double v = p + 1.0 * (x[i] + 0.0);
+  if (v < lo) v = p + 1.0 * (lo - p);
+  phi[i] = v;
+}
+
+template <class T>
+__global__ void k_widen(size_t n, const T* a, double* b) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) b[i] = double(a[i]);
+}
+
+}  // namespace
+}  // namespace oa
+
+using namespace oa;
+
+struct oa_diffusion {
+  DeviceMesh* mesh = nullptr;
+  oa_diffusion_settings s{};
+  cudaStream_t stream = nullptr;
+  double *phi = nullptr, *gamma = nullptr, *src = nullptr, *side = nullptr;
+  int* bnd_kind = nullptr;
+  int nbnd = 0;
+  void* A = nullptr;       // [nnz] FP64 or FP32
+  double* b = nullptr;     // [nn]
+  double* x = nullptr;     // [nn]
+  int* err = nullptr;
+  bool assembled = false;
+  ScalarSolve solver;
+};
+
+namespace {
+
+bool dmixed(const oa_diffusion* H) { return H->s.precision == OA_PREC_MIXED; }
+
+double* diff_field(oa_diffusion* H, const std::string& n) {
+  if (n == "phi") return H->phi;
+  if (n == "gamma") return H->gamma;
+  if (n == "src") return H->src;
+  if (n == "sidePhi") return H->side;
+  return nullptr;
+}
+
+int launch_diffusion(oa_diffusion* H) {
+  DeviceMesh& m = *H->mesh;
+  DiffView d{H->phi, H->gamma, H->src, H->side, H->bnd_kind, H->nbnd, 1.0 / H->s.urf, H->s.wall_rhs_relax};
+  const int grid = (m.nn + DWARPS - 1) / DWARPS;
+  const bool sh = H->s.shifted != 0;
+  if (dmixed(H)) {
+    if (sh) k_diffusion<true, float><<<grid, 32 * DWARPS, 0, H->stream>>>(m.view(), d, (float*)H->A, H->b, H->err);
+    else k_diffusion<false, float><<<grid, 32 * DWARPS, 0, H->stream>>>(m.view(), d, (float*)H->A, H->b, H->err);
+  } else {
+    if (sh) k_diffusion<true, double><<<grid, 32 * DWARPS, 0, H->stream>>>(m.view(), d, (double*)H->A, H->b, H->err);
+    else k_diffusion<false, double><<<grid, 32 * DWARPS, 0, H->stream>>>(m.view(), d, (double*)H->A, H->b, H->err);
+  }
+  count_launches(1);
+  OA_CUDA(cudaGetLastError());
+  H->assembled = true;
+  return OA_OK;
+}
+
+int diff_check_err(oa_diffusion* H, const char* what) {
+  int h = 0;
+  OA_CUDA(cudaMemcpyAsync(&h, H->err, sizeof(int), cudaMemcpyDeviceToHost, H->stream));
+  OA_CUDA(cudaStreamSynchronize(H->stream));
+  if (h) {
+    OA_CUDA(cudaMemsetAsync(H->err, 0, sizeof(int), H->stream));
+    OA_CUDA(cudaStreamSynchronize(H->stream));
+    return fail(OA_ERR_GEOMETRY, std::string(what) + ": singular Jacobian (det <= 1e6*realmin)");
+  }
+  return OA_OK;
+}
+
+int diff_solve(oa_diffusion* H, double rtol, int maxit, int* iters, double* res, int* refinements) {
+  DeviceMesh& m = *H->mesh;
+  ScalarGraph g;
+  g.nn = m.nn;
+  g.rp = m.row_ptr;
+  g.cols = m.cols;
+  g.diag = m.diag;
+  g.h_rp = m.h_row_ptr.data();
+  g.h_cols = m.h_cols.data();
+  g.h_diag = m.h_diag.data();
+  return H->solver.solve(g, dmixed(H), H->s.amg != 0, H->s.use_graphs != 0, H->A, H->b, H->x, rtol, maxit, iters,
+                         res, refinements, H->stream, "diffusion");
+}
+
+}  // namespace
+
+extern "C" {
+
+int oa_diffusion_create(oa_mesh* M, const oa_diffusion_settings* s, const int* bnd_kind, const double* bnd_value,
+                        int nbnd, oa_diffusion** out) {
+  if (!M || !s || !out || nbnd < 0 || (nbnd > 0 && (!bnd_kind || !bnd_value)))
+    return fail(OA_ERR_ARG, "oa_diffusion_create: bad arguments");
+  *out = nullptr;
+  if (M->m.topo != OA_TOPO_TET4) return fail(OA_ERR_MESH, "oa_diffusion_create: the diffusion path needs a tet4 mesh");
+  if (!(s->urf > 0.0)) return fail(OA_ERR_ARG, "oa_diffusion_create: relaxation must be > 0");
+  if (s->precision != OA_PREC_FP64 && s->precision != OA_PREC_MIXED)
+    return fail(OA_ERR_ARG, "oa_diffusion_create: unknown precision");
+  for (int i = 0; i < nbnd; ++i)
+    if (bnd_kind[i] != OA_BND_FIXED_VALUE && bnd_kind[i] != OA_BND_ZERO_FLUX)
+      return fail(OA_ERR_ARG, "oa_diffusion_create: unknown boundary kind");
+  const DeviceMesh& m = M->m;
+  for (int f = 0; f < m.nf; ++f)
+    if (m.h_face_bnd[f] >= nbnd) return fail(OA_ERR_ARG, "oa_diffusion_create: a face names a boundary index >= nbnd");
+  oa_diffusion* H = new oa_diffusion();
+  H->mesh = &M->m;
+  H->s = *s;
+  H->nbnd = nbnd;
+  const size_t nn = m.nn, nnz = m.nnz;
+  const size_t tm = s->precision == OA_PREC_MIXED ? sizeof(float) : sizeof(double);
+  int st = OA_OK;
+  if ((st = dalloc(&H->phi, nn)) || (st = dalloc(&H->gamma, nn)) || (st = dalloc(&H->src, nn)) ||
+      (st = dalloc(&H->side, nn)) || (st = dalloc(&H->bnd_kind, (size_t)std::max(nbnd, 1))) ||
+      (st = dalloc(&H->b, nn)) || (st = dalloc(&H->x, nn)) || (st = dalloc(&H->err, 1))) {
+    oa_diffusion_destroy(H);
+    return st;
+  }
+  if (cudaMalloc(&H->A, tm * nnz) != cudaSuccess) {
+    oa_diffusion_destroy(H);
+    return fail(OA_ERR_CUDA, "oa_diffusion_create: device allocation failed");
+  }
+  cudaStreamCreateWithFlags(&H->stream, cudaStreamNonBlocking);
+  std::vector<double> h(nn, 0.0);
+  // node-side values of the fixed-value boundaries, boundary by boundary in
+  // index order (nodeField::updateBoundarySideFieldSpecifiedValue sets parts in
+  // turn); zero-flux boundaries write none
+  std::vector<double> side(nn, 0.0);
+  for (int bnd = 0; bnd < nbnd; ++bnd) {
+    if (bnd_kind[bnd] != OA_BND_FIXED_VALUE) continue;
+    for (int f = 0; f < m.nf; ++f) {
+      if (m.h_face_bnd[f] != bnd) continue;
+      for (int k = 0; k < 3; ++k)
+        side[m.h_conn[4L * m.h_face_elem[f] + tet4::side_node(m.h_face_ord[f], k)]] = bnd_value[bnd];
+    }
+  }
+  cudaMemcpy(H->phi, h.data(), sizeof(double) * nn, cudaMemcpyHostToDevice);
+  cudaMemcpy(H->src, h.data(), sizeof(double) * nn, cudaMemcpyHostToDevice);
+  std::fill(h.begin(), h.end(), 1.0);
+  cudaMemcpy(H->gamma, h.data(), sizeof(double) * nn, cudaMemcpyHostToDevice);
+  cudaMemcpy(H->side, side.data(), sizeof(double) * nn, cudaMemcpyHostToDevice);
+  if (nbnd) cudaMemcpy(H->bnd_kind, bnd_kind, sizeof(int) * nbnd, cudaMemcpyHostToDevice);
+  cudaMemset(H->err, 0, sizeof(int));
+  cudaError_t ce = cudaDeviceSynchronize();
+  if (ce == cudaSuccess) ce = cudaGetLastError();
+  if (ce != cudaSuccess) {
+    oa_diffusion_destroy(H);
+    return fail(OA_ERR_CUDA, std::string("oa_diffusion_create: ") + cudaGetErrorString(ce));
+  }
+  *out = H;
+  return OA_OK;
+}
+
+void oa_diffusion_destroy(oa_diffusion* H) {
+  if (!H) return;
+  void* ptrs[] = {H->phi, H->gamma, H->src, H->side, H->bnd_kind, H->A, H->b, H->x, H->err};
+  for (void* p : ptrs)
+    if (p) cudaFree(p);
+  H->solver.release();
+  if (H->stream) cudaStreamDestroy(H->stream);
+  delete H;
+}
+
+int oa_diffusion_set_field(oa_diffusion* H, const char* name, const double* host, long n) {
+  if (!H || !name || !host) return fail(OA_ERR_ARG, "oa_diffusion_set_field: null argument");
+  double* p = diff_field(H, name);
+  if (!p) return fail(OA_ERR_ARG, std::string("oa_diffusion_set_field: unknown field ") + name);
+  if (n != H->mesh->nn) return fail(OA_ERR_ARG, std::string("oa_diffusion_set_field: size mismatch for ") + name);
+  OA_CUDA(cudaMemcpyAsync(p, host, sizeof(double) * n, cudaMemcpyHostToDevice, H->stream));
+  OA_CUDA(cudaStreamSynchronize(H->stream));
+  return OA_OK;
+}
+
+int oa_diffusion_get_field(oa_diffusion* H, const char* name, double* host, long n) {
+  if (!H || !name || !host) return fail(OA_ERR_ARG, "oa_diffusion_get_field: null argument");
+  double* p = diff_field(H, name);
+  if (!p) return fail(OA_ERR_ARG, std::string("oa_diffusion_get_field: unknown field ") + name);
+  if (n != H->mesh->nn) return fail(OA_ERR_ARG, std::string("oa_diffusion_get_field: size mismatch for ") + name);
+  OA_CUDA(cudaMemcpyAsync(host, p, sizeof(double) * n, cudaMemcpyDeviceToHost, H->stream));
+  OA_CUDA(cudaStreamSynchronize(H->stream));
+  return OA_OK;
+}
+
+int oa_diffusion_field_device_ptr(oa_diffusion* H, const char* name, double** dev) {
+  if (!H || !name || !dev) return fail(OA_ERR_ARG, "oa_diffusion_field_device_ptr: null argument");
+  double* p = diff_field(H, name);
+  if (!p) return fail(OA_ERR_ARG, std::string("oa_diffusion_field_device_ptr: unknown field ") + name);
+  *dev = p;
+  return OA_OK;
+}
+
+int oa_diffusion_assemble(oa_diffusion* H, double* A, double* b) {
+  if (!H) return fail(OA_ERR_ARG, "oa_diffusion_assemble: null handle");
+  if (int s = launch_diffusion(H)) return s;
+  if (int s = diff_check_err(H, "oa_diffusion_assemble")) return s;
+  const size_t nnz = H->mesh->nnz, nn = H->mesh->nn;
+  if (A) {
+    if (dmixed(H)) {
+      double* tmp = nullptr;
+      if (int s = dalloc(&tmp, nnz)) return s;
+      k_widen<float><<<(unsigned)((nnz + 255) / 256), 256, 0, H->stream>>>(nnz, (const float*)H->A, tmp);
+      OA_CUDA(cudaMemcpyAsync(A, tmp, sizeof(double) * nnz, cudaMemcpyDeviceToHost, H->stream));
+      OA_CUDA(cudaStreamSynchronize(H->stream));
+      cudaFree(tmp);
+    } else {
+      OA_CUDA(cudaMemcpyAsync(A, H->A, sizeof(double) * nnz, cudaMemcpyDeviceToHost, H->stream));
+    }
+  }
+  if (b) OA_CUDA(cudaMemcpyAsync(b, H->b, sizeof(double) * nn, cudaMemcpyDeviceToHost, H->stream));
+  OA_CUDA(cudaStreamSynchronize(H->stream));
+  return OA_OK;
+}
+
+int oa_diffusion_solve(oa_diffusion* H, double rtol, int maxit, double* x, int* iters, double* res,
+                       int* refinements) {
+  if (!H || maxit <= 0 || !(rtol > 0.0)) return fail(OA_ERR_ARG, "oa_diffusion_solve: bad arguments");
+  if (!H->assembled) return fail(OA_ERR_NOT_READY, "oa_diffusion_solve: no assembled system");
+  if (int s = diff_solve(H, rtol, maxit, iters, res, refinements)) return s;
+  if (x) OA_CUDA(cudaMemcpyAsync(x, H->x, sizeof(double) * H->mesh->nn, cudaMemcpyDeviceToHost, H->stream));
+  OA_CUDA(cudaStreamSynchronize(H->stream));
+  return OA_OK;
+}
+
+int oa_diffusion_step(oa_diffusion* H, int* iters, double* res, int* refinements) {
+  if (!H) return fail(OA_ERR_ARG, "oa_diffusion_step: null handle");
+  if (int s = launch_diffusion(H)) return s;
+  if (int s = diff_check_err(H, "oa_diffusion_step")) return s;
+  if (int s = diff_solve(H, H->s.rtol, H->s.maxit, iters, res, refinements)) return s;
+  const int n = H->mesh->nn;
+  k_correct_clip<<<(n + 255) / 256, 256, 0, H->stream>>>(n, H->phi, H->x, H->s.lower_clip);
+  count_launches(1);
+  OA_CUDA(cudaGetLastError());
+  OA_CUDA(cudaStreamSynchronize(H->stream));
+  return OA_OK;
+}
+
+int oa_diffusion_stream(oa_diffusion* H, void** stream) {
+  if (!H || !stream) return fail(OA_ERR_ARG, "oa_diffusion_stream: null argument");
+  *stream = (void*)H->stream;
+  return OA_OK;
+}
+
+int oa_diffusion_time_assembly(oa_diffusion* H, int reps, double* ms) {
+  if (!H || !ms || reps <= 0) return fail(OA_ERR_ARG, "oa_diffusion_time_assembly: bad arguments");
+  cudaEvent_t e0, e1;
+  OA_CUDA(cudaEventCreate(&e0));
+  OA_CUDA(cudaEventCreate(&e1));
+  if (int s = launch_diffusion(H)) return s;
+  OA_CUDA(cudaEventRecord(e0, H->stream));
+  for (int i = 0; i < reps; ++i)
+    if (int s = launch_diffusion(H)) return s;
+  OA_CUDA(cudaEventRecord(e1, H->stream));
+  OA_CUDA(cudaEventSynchronize(e1));
+  float t = 0.f;
+  OA_CUDA(cudaEventElapsedTime(&t, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  *ms = double(t) / reps;
+  return diff_check_err(H, "oa_diffusion_time_assembly");
+}
+
+}  // extern "C"

@@ -16,6 +16,8 @@
 #pragma once
 #include <cstdint>
 
+#include "oa_geom.cuh"
+
 namespace oa {
 namespace hex8 {
 
@@ -214,31 +216,6 @@ __host__ __device__ constexpr double shape_at() {
   return shape(N, PT::s(0), PT::s(1), PT::s(2));
 }
 
-// Area vector of quad (a,b,c,d) by four triangles about the vertex mean
-// (CalculateQuadArea.F).
-__device__ __forceinline__ void quad_area(const double* a, const double* b, const double* c,
-                                          const double* d, double A[3]) {
-  double m[3], r1[3], r2[3];
-#pragma unroll
-  for (int k = 0; k < 3; ++k) m[k] = 0.25 * (a[k] + b[k] + c[k] + d[k]);
-  A[0] = A[1] = A[2] = 0.0;
-  const double* q[5] = {a, b, c, d, a};
-#pragma unroll
-  for (int k = 0; k < 3; ++k) r2[k] = a[k] - m[k];
-#pragma unroll
-  for (int t = 0; t < 4; ++t) {
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-      r1[k] = r2[k];
-      r2[k] = q[t + 1][k] - m[k];
-    }
-    A[0] += r1[1] * r2[2] - r2[1] * r1[2];
-    A[1] += r1[2] * r2[0] - r2[2] * r1[0];
-    A[2] += r1[0] * r2[1] - r2[0] * r1[1];
-  }
-#pragma unroll
-  for (int k = 0; k < 3; ++k) A[k] *= 0.5;
-}
 
 // Subdivision points a canonical corner-0 lane needs: edge midpoints to nodes
 // 1, 3, 4; centroids of faces (0,1,2,3), (0,1,4,5), (0,3,4,7); element centroid.

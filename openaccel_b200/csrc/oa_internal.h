@@ -10,20 +10,30 @@
 
 namespace oa {
 
-// Device-resident mesh: hex8 connectivity, node -> incident-element-by-corner
-// table, reduced-stencil CSR graph, wall faces and static FP64 geometry.
+// Device-resident mesh: connectivity, node -> incident-element table,
+// reduced-stencil CSR graph, wall faces and static FP64 geometry.
 // POD view of the device arrays, passed to kernels by value.
+//   hex8: n2e is [nn][8], the element where the node is corner c (or -1).
+//   tet4: n2e[n2e_ptr[i] .. n2e_ptr[i+1]) lists 4*element + corner for every
+//         element incident to node i, by ascending element; n2f likewise
+//         lists 4*face + k for every boundary face whose side node k is i.
 struct MeshView {
   int nn = 0, ne = 0, nf = 0, nnz = 0;
   double* x = nullptr;         // [nn][3]
-  int* conn = nullptr;         // [ne][8]
-  int* n2e = nullptr;          // [nn][8]: element where the node is corner c, or -1
+  int* conn = nullptr;         // [ne][8] (hex8) or [ne][4] (tet4)
+  int* n2e = nullptr;
+  int* n2e_ptr = nullptr;      // [nn+1] (tet4)
+  int* n2f = nullptr;          // (tet4)
+  int* n2f_ptr = nullptr;      // [nn+1] (tet4)
+  int* face_elem = nullptr;    // [nf] (tet4)
+  int* face_ord = nullptr;     // [nf] (tet4)
+  int* face_bnd = nullptr;     // [nf] (tet4)
   int* row_ptr = nullptr;      // [nn+1]
   int* cols = nullptr;         // [nnz]
   int* diag = nullptr;         // [nn] offset of the diagonal within the row
   uint8_t* face_mask = nullptr;  // [ne] bit f: face f is a no-slip wall face
   double* vol = nullptr;       // [nn] dual nodal volume
-  double* wscv = nullptr;      // [ne][8] SCV volume fractions
+  double* wscv = nullptr;      // [ne][8] SCV volume fractions (hex8)
   int* wall_node = nullptr;    // [nn] 1 on wall nodes
 };
 
@@ -75,6 +85,19 @@ int fail(int code, const std::string& msg);
     if (e_ != cudaSuccess)                                                         \
       return ::oa::fail(OA_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
   } while (0)
+
+}  // namespace oa
+
+struct oa_mesh {
+  oa::DeviceMesh m;
+  cudaStream_t st = nullptr;
+};
+
+namespace oa {
+
+// tet4 mesh set-up (oa_diffusion.cu): graph, incidence lists, dual volumes.
+int create_tet4_mesh(oa_mesh* M, const double* coords, int nn, const int* conn, int ne, const int* face_elem,
+                     const int* face_ord, const int* face_bnd, int nf);
 
 // kernels / launchers (oa_kernels.cu)
 int launch_geometry(DeviceMesh& m, cudaStream_t st);

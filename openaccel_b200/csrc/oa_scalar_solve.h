@@ -1,0 +1,45 @@
+// Scalar (1 dof per node) linear solve shared by the pressure-correction and
+// the scalar-diffusion paths (internal).
+#pragma once
+#include <cuda_runtime.h>
+
+#include "oa_amg.h"
+#include "oa_krylov.h"
+
+namespace oa {
+
+// CSR graph of a scalar system: device arrays and the host copies the AMG
+// set-up reads.
+struct ScalarGraph {
+  int nn = 0;
+  int *rp = nullptr, *cols = nullptr, *diag = nullptr;
+  const int *h_rp = nullptr, *h_cols = nullptr, *h_diag = nullptr;
+};
+
+// FP64: BiCGStab (AMG- or Jacobi-preconditioned) to rtol. Mixed: iterative
+// refinement with the FP64 residual r = b - A x (A in its stored FP32 values),
+// FP32 BiCGStab on A d = r to a loose inner tolerance, x += d, until
+// ||r|| <= rtol ||b||. The preconditioner hierarchy is built on first use and
+// its numeric part refreshed on every solve.
+struct ScalarSolve {
+  KrylovSolver<1, double, double> k64;
+  KrylovSolver<1, float, float> k32;
+  Amg<double> amg64;
+  Amg<float> amg32;
+  double* r = nullptr;      // FP64 residual
+  float* r32 = nullptr;     // its FP32 copy
+  double* scal = nullptr;   // [2] device scalars
+  double* hscal = nullptr;  // [2] pinned
+  double* partials = nullptr;
+  int n = 0;
+
+  int init(int n);
+  // A: const double* (mixed = false) or const float* (mixed = true); b and x
+  // FP64 device vectors of g.nn; x is overwritten. refinements may be null.
+  int solve(const ScalarGraph& g, bool mixed, bool amg, bool graphs, const void* A, const double* b, double* x,
+            double rtol, int maxit, int* iters, double* res, int* refinements, cudaStream_t st, const char* what);
+  void release();
+  ~ScalarSolve() { release(); }
+};
+
+}  // namespace oa

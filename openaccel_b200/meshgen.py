@@ -195,3 +195,113 @@ def batch_cavities(count=64, nmin=16, nmax=64, mu_min=1e-3, mu_max=1e-1, seed=20
                    meta={"kind": "cavity_batch", "count": int(sizes.size), "seed": seed})
     return CavityBatch(mesh, np.concatenate(mus), np.asarray(refs, np.int32), np.asarray(noff, np.int64), sizes,
                        visc)
+
+
+# tet4 face ordinal -> element-local nodes, outward orientation
+# (external/nalu/src/master_element/Tet4CVFEM.C:416-421)
+TET_SIDE_NODES = np.array([[0, 1, 3], [1, 2, 3], [0, 3, 2], [0, 2, 1]], dtype=np.int32)
+
+BND_FIXED_VALUE = 0
+BND_ZERO_FLUX = 1
+
+
+@dataclass
+class TetMesh:
+    """tet4 mesh with boundary faces (element, face ordinal, boundary index)."""
+
+    n: int
+    coords: np.ndarray  # (nn, 3) float64
+    conn: np.ndarray  # (ne, 4) int32
+    face_elem: np.ndarray
+    face_ord: np.ndarray
+    face_bnd: np.ndarray
+    bnd_kind: np.ndarray  # (nbnd,) BND_FIXED_VALUE / BND_ZERO_FLUX
+    bnd_value: np.ndarray  # (nbnd,) fixed values
+    meta: dict = field(default_factory=dict)
+
+    @property
+    def nn(self) -> int:
+        return self.coords.shape[0]
+
+    @property
+    def ne(self) -> int:
+        return self.conn.shape[0]
+
+    @property
+    def nf(self) -> int:
+        return self.face_elem.shape[0]
+
+
+def kuhn_tets(n, perturb=0.0, seed=12345):
+    """n^3 hex block on the unit cube, each hex split into the 6 Kuhn tets that
+    share its (0,0,0)-(1,1,1) diagonal, so face diagonals match between
+    neighbours. Node numbering as ``hex_block``; tet nodes are ordered for a
+    positive Jacobian. Returns (coords, conn)."""
+    coords, _ = hex_block(n, n, n)
+    if perturb > 0.0:
+        h = 1.0 / n
+        rng = np.random.Generator(np.random.PCG64(seed))
+        noise = rng.uniform(-perturb * h, perturb * h, size=coords.shape)
+        idx = np.arange(coords.shape[0])
+        i, j, k = idx % (n + 1), (idx // (n + 1)) % (n + 1), idx // ((n + 1) * (n + 1))
+        interior = (i > 0) & (i < n) & (j > 0) & (j < n) & (k > 0) & (k < n)
+        coords[interior] += noise[interior]
+    k, j, i = np.meshgrid(np.arange(n), np.arange(n), np.arange(n), indexing="ij")
+    n0 = _node_id(i.ravel(), j.ravel(), k.ravel(), n, n).astype(np.int64)
+    stride = np.array([1, n + 1, (n + 1) * (n + 1)], dtype=np.int64)
+    tets = []
+    for perm, sign in [((0, 1, 2), 1), ((1, 2, 0), 1), ((2, 0, 1), 1),
+                       ((0, 2, 1), -1), ((2, 1, 0), -1), ((1, 0, 2), -1)]:
+        p0 = n0
+        p1 = p0 + stride[perm[0]]
+        p2 = p1 + stride[perm[1]]
+        p3 = n0 + stride.sum()
+        tets.append(np.stack([p0, p1, p2, p3] if sign > 0 else [p0, p2, p1, p3], axis=1))
+    conn = np.stack(tets, axis=1).reshape(-1, 4).astype(np.int32)
+    return coords, conn
+
+
+def tet_boundary_faces(n, conn):
+    """Boundary faces of a ``kuhn_tets`` block by side: {'x-': (elems, ords), ...},
+    each sorted by (element, ordinal)."""
+    nodes = conn[:, TET_SIDE_NODES]  # (ne, 4, 3)
+    i = nodes % (n + 1)
+    j = (nodes // (n + 1)) % (n + 1)
+    k = nodes // ((n + 1) * (n + 1))
+    out = {}
+    for side, arr, val in [("x-", i, 0), ("x+", i, n), ("y-", j, 0), ("y+", j, n), ("z-", k, 0), ("z+", k, n)]:
+        e, o = np.nonzero(np.all(arr == val, axis=2))
+        out[side] = (e.astype(np.int32), o.astype(np.int32))
+    return out
+
+
+def conduction(n, sigma=1.0, seed=4242, perturb=0.0, t_left=0.0, t_right=1.0):
+    """Steady heat conduction on the unit cube split into 6 n^3 tets.
+
+    Boundary 0 (x = 0) holds ``t_left``, boundary 1 (x = 1) holds ``t_right``,
+    boundary 2 (the other four faces) is zero-flux. Conductivity is lognormal
+    per element (median 1, ``sigma``), projected to nodes as the
+    volume-weighted mean of the adjacent elements (the reference keeps the
+    diffusivity at nodes); the volumetric source is U[0, 1] per node. Returns
+    (TetMesh, gamma_node, source_node, gamma_elem)."""
+    coords, conn = kuhn_tets(n, perturb=perturb, seed=seed)
+    faces = tet_boundary_faces(n, conn)
+    fe, fo, fb = [], [], []
+    for bnd, sides in enumerate([["x-"], ["x+"], ["y-", "y+", "z-", "z+"]]):
+        for s in sides:
+            e, o = faces[s]
+            fe.append(e), fo.append(o), fb.append(np.full_like(e, bnd))
+    mesh = TetMesh(n, coords, conn, np.concatenate(fe), np.concatenate(fo), np.concatenate(fb),
+                   np.array([BND_FIXED_VALUE, BND_FIXED_VALUE, BND_ZERO_FLUX], np.int32),
+                   np.array([t_left, t_right, 0.0]),
+                   meta={"kind": "conduction", "n": n, "sigma": sigma, "seed": seed, "perturb": perturb})
+    rng = np.random.Generator(np.random.PCG64(seed + 7))
+    gamma_e = np.exp(sigma * rng.standard_normal(conn.shape[0]))
+    x = coords[conn]  # (ne, 4, 3)
+    vol_e = np.einsum("ij,ij->i", x[:, 1] - x[:, 0], np.cross(x[:, 2] - x[:, 0], x[:, 3] - x[:, 0])) / 6.0
+    flat = conn.ravel()
+    wsum = np.bincount(flat, weights=np.repeat(vol_e, 4), minlength=coords.shape[0])
+    gsum = np.bincount(flat, weights=np.repeat(vol_e * gamma_e, 4), minlength=coords.shape[0])
+    gamma_n = gsum / wsum
+    src = rng.uniform(0.0, 1.0, size=coords.shape[0])
+    return mesh, gamma_n, src, gamma_e

@@ -28,7 +28,13 @@ EXPORTS = [
     "oa_flow_field_device_ptr", "oa_flow_set_reference_nodes", "oa_flow_initialize", "oa_assemble_momentum", "oa_assemble_pcorr",
     "oa_update_mdot", "oa_update_div", "oa_update_gradient", "oa_solve", "oa_simple_iterate", "oa_flow_sync",
     "oa_flow_stream", "oa_launch_count", "oa_time_kernel", "oa_pcorr_solve_static",
+    "oa_diffusion_create", "oa_diffusion_destroy", "oa_diffusion_set_field", "oa_diffusion_get_field",
+    "oa_diffusion_field_device_ptr", "oa_diffusion_assemble", "oa_diffusion_solve", "oa_diffusion_step",
+    "oa_diffusion_stream", "oa_diffusion_time_assembly",
 ]
+
+OA_BND_FIXED_VALUE = 0
+OA_BND_ZERO_FLUX = 1
 
 
 class OpenAccelError(RuntimeError):
@@ -53,6 +59,24 @@ class IterStats(C.Structure):
         ("mom_iters", C.c_int), ("pc_iters", C.c_int), ("pc_refinements", C.c_int),
         ("mom_res", C.c_double), ("pc_res", C.c_double), ("continuity_rms", C.c_double),
     ]
+
+
+class DiffusionSettings(C.Structure):
+    _fields_ = [
+        ("shifted", C.c_int), ("urf", C.c_double), ("wall_rhs_relax", C.c_double), ("lower_clip", C.c_double),
+        ("maxit", C.c_int), ("rtol", C.c_double), ("precision", C.c_int), ("amg", C.c_int),
+        ("use_graphs", C.c_int),
+    ]
+
+
+def default_diffusion_settings(**kw) -> DiffusionSettings:
+    """Solid energy-equation defaults: linear_linear interpolation
+    (controls.h:95), energy relaxation 1 (controls.h:73), wall rhs relaxation
+    0.75 (thermalEnergyAssembler.h:42), clip at 0, Krylov to 1e-10."""
+    d = dict(shifted=1, urf=1.0, wall_rhs_relax=0.75, lower_clip=0.0, maxit=5000, rtol=1e-10,
+             precision=OA_PREC_FP64, amg=1, use_graphs=0)
+    d.update(kw)
+    return DiffusionSettings(**d)
 
 
 def default_settings(**kw) -> FlowSettings:
@@ -107,6 +131,16 @@ def lib():
         "oa_launch_count": (C.c_int, [P(C.c_longlong)]),
         "oa_time_kernel": (C.c_int, [vp, C.c_int, C.c_int, dp]),
         "oa_pcorr_solve_static": (C.c_int, [C.c_int, vp, vp, vp, vp, vp, vp, C.c_double, C.c_int, ip, dp, vp]),
+        "oa_diffusion_create": (C.c_int, [vp, P(DiffusionSettings), ip, dp, C.c_int, P(vp)]),
+        "oa_diffusion_destroy": (None, [vp]),
+        "oa_diffusion_set_field": (C.c_int, [vp, C.c_char_p, dp, C.c_long]),
+        "oa_diffusion_get_field": (C.c_int, [vp, C.c_char_p, dp, C.c_long]),
+        "oa_diffusion_field_device_ptr": (C.c_int, [vp, C.c_char_p, P(dp)]),
+        "oa_diffusion_assemble": (C.c_int, [vp, dp, dp]),
+        "oa_diffusion_solve": (C.c_int, [vp, C.c_double, C.c_int, dp, ip, dp, ip]),
+        "oa_diffusion_step": (C.c_int, [vp, ip, dp, ip]),
+        "oa_diffusion_stream": (C.c_int, [vp, P(vp)]),
+        "oa_diffusion_time_assembly": (C.c_int, [vp, C.c_int, dp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -136,7 +170,7 @@ def _ip(a):
 
 
 class Mesh:
-    """Device mesh (oa_mesh_create) from a ``meshgen.HexMesh``-like object."""
+    """Device mesh (oa_mesh_create) from a ``meshgen.HexMesh`` or ``meshgen.TetMesh``."""
 
     def __init__(self, mesh):
         self.src = mesh
@@ -147,7 +181,8 @@ class Mesh:
         fo = np.ascontiguousarray(mesh.face_ord, np.int32)
         fb = np.ascontiguousarray(mesh.face_bnd, np.int32)
         h = C.c_void_p()
-        _check(lib().oa_mesh_create(_dp(x), self.nn, _ip(conn), self.ne, OA_TOPO_HEX8, _ip(fe), _ip(fo),
+        self.topo = OA_TOPO_TET4 if conn.shape[1] == 4 else OA_TOPO_HEX8
+        _check(lib().oa_mesh_create(_dp(x), self.nn, _ip(conn), self.ne, self.topo, _ip(fe), _ip(fo),
                                     _ip(fb), int(fe.shape[0]), C.byref(h)))
         self.h = h
         n = C.c_int()
@@ -269,6 +304,77 @@ class Flow:
     def close(self):
         if getattr(self, "h", None):
             lib().oa_flow_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Diffusion:
+    """tet4 scalar diffusion on the device (oa_diffusion_create): the solid
+    energy equation of thermalEnergyEquation::solve with a per-node source."""
+
+    FIELDS = ("phi", "gamma", "src", "sidePhi")
+
+    def __init__(self, mesh: Mesh, settings: DiffusionSettings | None = None):
+        self.mesh = mesh
+        self.settings = settings or default_diffusion_settings()
+        bk = np.ascontiguousarray(mesh.src.bnd_kind, np.int32)
+        bv = np.ascontiguousarray(mesh.src.bnd_value, np.float64)
+        h = C.c_void_p()
+        _check(lib().oa_diffusion_create(mesh.h, C.byref(self.settings), _ip(bk), _dp(bv), int(bk.size),
+                                         C.byref(h)))
+        self.h = h
+
+    def set_field(self, name, values):
+        v = np.ascontiguousarray(values, np.float64).ravel()
+        _check(lib().oa_diffusion_set_field(self.h, name.encode(), _dp(v), v.size))
+
+    def get_field(self, name):
+        v = np.zeros(self.mesh.nn)
+        _check(lib().oa_diffusion_get_field(self.h, name.encode(), _dp(v), v.size))
+        return v
+
+    def device_ptr(self, name) -> int:
+        p = C.POINTER(C.c_double)()
+        _check(lib().oa_diffusion_field_device_ptr(self.h, name.encode(), C.byref(p)))
+        return C.cast(p, C.c_void_p).value
+
+    def assemble(self, copy=True):
+        A = np.zeros(self.mesh.nnz) if copy else None
+        b = np.zeros(self.mesh.nn) if copy else None
+        _check(lib().oa_diffusion_assemble(self.h, _dp(A), _dp(b)))
+        return A, b
+
+    def solve(self, rtol=None, maxit=None):
+        x = np.zeros(self.mesh.nn)
+        it, res, nref = C.c_int(), C.c_double(), C.c_int()
+        _check(lib().oa_diffusion_solve(self.h, self.settings.rtol if rtol is None else rtol,
+                                        self.settings.maxit if maxit is None else maxit, _dp(x), C.byref(it),
+                                        C.byref(res), C.byref(nref)))
+        return x, it.value, res.value, nref.value
+
+    def step(self):
+        it, res, nref = C.c_int(), C.c_double(), C.c_int()
+        _check(lib().oa_diffusion_step(self.h, C.byref(it), C.byref(res), C.byref(nref)))
+        return dict(iters=it.value, res=res.value, refinements=nref.value)
+
+    def stream_handle(self) -> int:
+        p = C.c_void_p()
+        _check(lib().oa_diffusion_stream(self.h, C.byref(p)))
+        return p.value or 0
+
+    def time_assembly(self, reps=5) -> float:
+        ms = C.c_double()
+        _check(lib().oa_diffusion_time_assembly(self.h, reps, C.byref(ms)))
+        return ms.value
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().oa_diffusion_destroy(self.h)
             self.h = None
 
     def __del__(self):

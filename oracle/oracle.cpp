@@ -731,6 +731,7 @@ void simple_iteration(Case& c, orc_iter_stats* st) {
 extern "C" {
 
 void orc_set_threads(int n) { g_threads = n < 1 ? 1 : n; }
+int orc_get_threads(void) { return g_threads; }
 
 void orc_hex8_scs_areav(const double* x, double* areav) { oracle::hex8::scs_areav(x, areav); }
 int orc_hex8_scv_volumes(const double* x, double* vol) {

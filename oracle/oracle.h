@@ -87,6 +87,42 @@ int orc_bicgstab(void* h, int bs, const double* A, const double* b, double* x,
 void orc_simple_iteration(void* h, orc_iter_stats* st);
 /* thread count used by the element loops and SpMV (1 = serial) */
 void orc_set_threads(int n);
+int orc_get_threads(void);
+
+/* ---- tet4 scalar diffusion (diffusion.cpp) ---- */
+enum { ORC_BND_FIXED_VALUE = 0, ORC_BND_ZERO_FLUX = 1 };
+
+typedef struct orc_diff_settings {
+  int shifted;           /* linear_linear interpolation of Gamma (temperature default) */
+  double urf;            /* diagonal relaxation (energy relaxation factor) */
+  double wall_rhs_relax; /* wall-node rhs relaxation (thermalEnergyAssembler.h:42) */
+  double lower_clip;     /* lower clip of the corrected field */
+  int maxit;
+  double rtol;
+} orc_diff_settings;
+
+void orc_tet4_scs_areav(const double* x /*[4][3]*/, double* areav /*[6][3]*/);
+int orc_tet4_scv_volumes(const double* x, double* vol /*[4]*/);
+int orc_tet4_grad_op(const double* x, double* gradop /*[4][3]*/);
+void orc_tet4_shape(double* shape /*[6][4]*/, int shifted);
+void orc_tri3_face_areav(const double* p /*[3][3]*/, double* areav /*[3][3]*/);
+
+/* bnd_kind[nbnd] (ORC_BND_*), bnd_value[nbnd] (fixed values) */
+void* orc_diff_create(int nn, int ne, const double* x, const int* conn, int nf, const int* face_elem,
+                      const int* face_ord, const int* face_bnd, int nbnd, const int* bnd_kind,
+                      const double* bnd_value, const orc_diff_settings* s);
+void orc_diff_destroy(void* h);
+/* fields: phi, gamma, src (per node), sidePhi, vol, wallNode, faceArea, x */
+double* orc_diff_field(void* h, const char* name, long* len);
+int orc_diff_nnz(void* h);
+void orc_diff_graph(void* h, int* row_ptr, int* cols);
+void orc_diff_assemble(void* h, double* A, double* b);
+int orc_diff_cg(void* h, const double* A, const double* b, double* x, double rtol, int maxit, double* res);
+int orc_diff_bicgstab(void* h, const double* A, const double* b, double* x, double rtol, int maxit,
+                      double* res);
+void orc_diff_spmv(void* h, const double* A, const double* x, double* y);
+/* one thermalEnergyEquation::solve step: assemble, BiCGStab, correct; returns iterations */
+int orc_diff_step(void* h, double* res);
 
 #ifdef __cplusplus
 }

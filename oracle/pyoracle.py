@@ -59,6 +59,26 @@ def default_settings(**kw) -> Settings:
     return Settings(**d)
 
 
+class DiffSettings(C.Structure):
+    _fields_ = [
+        ("shifted", C.c_int),
+        ("urf", C.c_double),
+        ("wall_rhs_relax", C.c_double),
+        ("lower_clip", C.c_double),
+        ("maxit", C.c_int),
+        ("rtol", C.c_double),
+    ]
+
+
+def default_diff_settings(**kw) -> DiffSettings:
+    """Solid energy-equation defaults: linear_linear interpolation
+    (controls.h:95), energy relaxation 1 (controls.h:73), wall rhs relaxation
+    0.75 (thermalEnergyAssembler.h:42), clip at 0, CG to 1e-10."""
+    d = dict(shifted=1, urf=1.0, wall_rhs_relax=0.75, lower_clip=0.0, maxit=20000, rtol=1e-10)
+    d.update(kw)
+    return DiffSettings(**d)
+
+
 def build():
     subprocess.run(["make", "-s", "-C", _HERE], check=True)
 
@@ -96,6 +116,31 @@ def lib():
         L.orc_hex8_grad_op.argtypes = [dp, dp, C.c_int]
         L.orc_hex8_grad_op.restype = C.c_int
         L.orc_hex8_shape.argtypes = [dp, C.c_int]
+        L.orc_get_threads.restype = C.c_int
+        L.orc_tet4_scs_areav.argtypes = [dp, dp]
+        L.orc_tet4_scv_volumes.argtypes = [dp, dp]
+        L.orc_tet4_scv_volumes.restype = C.c_int
+        L.orc_tet4_grad_op.argtypes = [dp, dp]
+        L.orc_tet4_grad_op.restype = C.c_int
+        L.orc_tet4_shape.argtypes = [dp, C.c_int]
+        L.orc_tri3_face_areav.argtypes = [dp, dp]
+        L.orc_diff_create.restype = C.c_void_p
+        L.orc_diff_create.argtypes = [C.c_int, C.c_int, dp, ip, C.c_int, ip, ip, ip, C.c_int, ip, dp,
+                                      P(DiffSettings)]
+        L.orc_diff_destroy.argtypes = [C.c_void_p]
+        L.orc_diff_field.restype = dp
+        L.orc_diff_field.argtypes = [C.c_void_p, C.c_char_p, P(C.c_long)]
+        L.orc_diff_nnz.restype = C.c_int
+        L.orc_diff_nnz.argtypes = [C.c_void_p]
+        L.orc_diff_graph.argtypes = [C.c_void_p, ip, ip]
+        L.orc_diff_assemble.argtypes = [C.c_void_p, dp, dp]
+        L.orc_diff_cg.restype = C.c_int
+        L.orc_diff_cg.argtypes = [C.c_void_p, dp, dp, dp, C.c_double, C.c_int, dp]
+        L.orc_diff_spmv.argtypes = [C.c_void_p, dp, dp, dp]
+        L.orc_diff_bicgstab.restype = C.c_int
+        L.orc_diff_bicgstab.argtypes = [C.c_void_p, dp, dp, dp, C.c_double, C.c_int, dp]
+        L.orc_diff_step.restype = C.c_int
+        L.orc_diff_step.argtypes = [C.c_void_p, dp]
         _lib = L
     return _lib
 
@@ -225,3 +270,113 @@ def hex8_shape(shifted=True):
     N = np.zeros((12, 8))
     lib().orc_hex8_shape(_dp(N), int(shifted))
     return N
+
+
+class DiffCase:
+    """Oracle tet4 scalar-diffusion case over a ``meshgen.TetMesh``."""
+
+    def __init__(self, mesh, gamma=None, src=None, settings: DiffSettings | None = None):
+        self.mesh = mesh
+        self.settings = settings or default_diff_settings()
+        self._keep = [np.ascontiguousarray(mesh.coords, np.float64),
+                      np.ascontiguousarray(mesh.conn, np.int32),
+                      np.ascontiguousarray(mesh.face_elem, np.int32),
+                      np.ascontiguousarray(mesh.face_ord, np.int32),
+                      np.ascontiguousarray(mesh.face_bnd, np.int32),
+                      np.ascontiguousarray(mesh.bnd_kind, np.int32),
+                      np.ascontiguousarray(mesh.bnd_value, np.float64)]
+        x, conn, fe, fo, fb, bk, bv = self._keep
+        self.h = lib().orc_diff_create(mesh.nn, mesh.ne, _dp(x), _ip(conn), mesh.nf, _ip(fe), _ip(fo), _ip(fb),
+                                       bk.shape[0], _ip(bk), _dp(bv), C.byref(self.settings))
+        self.nnz = lib().orc_diff_nnz(self.h)
+        if gamma is not None:
+            self.field("gamma")[:] = gamma
+        if src is not None:
+            self.field("src")[:] = src
+
+    def close(self):
+        if self.h:
+            lib().orc_diff_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def field(self, name: str) -> np.ndarray:
+        n = C.c_long(0)
+        p = lib().orc_diff_field(self.h, name.encode(), C.byref(n))
+        if not p:
+            raise KeyError(name)
+        return np.ctypeslib.as_array(p, shape=(n.value,))
+
+    def graph(self):
+        rp = np.zeros(self.mesh.nn + 1, np.int32)
+        cols = np.zeros(self.nnz, np.int32)
+        lib().orc_diff_graph(self.h, _ip(rp), _ip(cols))
+        return rp, cols
+
+    def assemble(self):
+        A = np.zeros(self.nnz)
+        b = np.zeros(self.mesh.nn)
+        lib().orc_diff_assemble(self.h, _dp(A), _dp(b))
+        return A, b
+
+    def cg(self, A, b, rtol=1e-10, maxit=20000):
+        x = np.zeros_like(b)
+        res = C.c_double(0)
+        it = lib().orc_diff_cg(self.h, _dp(A), _dp(b), _dp(x), rtol, maxit, C.byref(res))
+        return x, it, res.value
+
+    def bicgstab(self, A, b, rtol=1e-10, maxit=20000):
+        x = np.zeros_like(b)
+        res = C.c_double(0)
+        it = lib().orc_diff_bicgstab(self.h, _dp(A), _dp(b), _dp(x), rtol, maxit, C.byref(res))
+        return x, it, res.value
+
+    def spmv(self, A, x):
+        y = np.zeros(self.mesh.nn)
+        xx = np.ascontiguousarray(x, np.float64)
+        lib().orc_diff_spmv(self.h, _dp(A), _dp(xx), _dp(y))
+        return y
+
+    def step(self):
+        res = C.c_double(0)
+        it = lib().orc_diff_step(self.h, C.byref(res))
+        return it, res.value
+
+
+def tet4_scs_areav(x):
+    x = np.ascontiguousarray(x, np.float64).reshape(4, 3)
+    a = np.zeros((6, 3))
+    lib().orc_tet4_scs_areav(_dp(x), _dp(a))
+    return a
+
+
+def tet4_scv_volumes(x):
+    x = np.ascontiguousarray(x, np.float64).reshape(4, 3)
+    v = np.zeros(4)
+    lib().orc_tet4_scv_volumes(_dp(x), _dp(v))
+    return v
+
+
+def tet4_grad_op(x):
+    x = np.ascontiguousarray(x, np.float64).reshape(4, 3)
+    g = np.zeros((4, 3))
+    err = lib().orc_tet4_grad_op(_dp(x), _dp(g))
+    return g, err
+
+
+def tet4_shape(shifted=True):
+    N = np.zeros((6, 4))
+    lib().orc_tet4_shape(_dp(N), int(shifted))
+    return N
+
+
+def tri3_face_areav(p):
+    p = np.ascontiguousarray(p, np.float64).reshape(3, 3)
+    a = np.zeros((3, 3))
+    lib().orc_tri3_face_areav(_dp(p), _dp(a))
+    return a
