@@ -220,6 +220,40 @@ int oa_diffusion_step(oa_diffusion* d, int* iters, double* res, int* refinements
 int oa_diffusion_stream(oa_diffusion* d, void** stream);
 int oa_diffusion_time_assembly(oa_diffusion* d, int reps, double* ms_per_launch);
 
+/* ---- k-omega SST node-level model updates ----
+ * One fused node kernel replacing shearStressTransportModel::
+ * updateTurbulentDynamicViscosity (src/model/turbulence/RANS/shearStressTransport/
+ * shearStressTransportModel.cpp:597-678), updateFOneBlending (:95-174),
+ * updateTurbulentProduction (:176-420; incompressible, fixed frame; at wall
+ * nodes the production is the caller's wall-function value, or 0) and the
+ * steady node terms of the k and omega SST assemblers
+ * (src/assemble/turbulence/RANS/shearStressTransport/segregatedShearStressTransport/
+ * turbulentKineticEnergy/turbulentKineticEnergySSTAssemblerNodeTerms.cpp:13-127,
+ * turbulentEddyFrequency/turbulentEddyFrequencySSTAssemblerNodeTerms.cpp:13-218).
+ * Defaults of the constants: shearStressTransportModel.h:21-37, RANSModel.h:20-22,
+ * turbulenceModel.h:20. */
+typedef struct oa_sst_constants {
+  double sigma_k1, sigma_k2, sigma_w1, sigma_w2, beta1, beta2, gamma1, gamma2, a1, beta_star, prod_limit, cmu;
+} oa_sst_constants;
+
+/* Device pointers, [nn] unless noted. mut may alias mut_old (in-place
+ * relaxation mut = urf * new + (1 - urf) * old); pk_wall may be NULL. */
+typedef struct oa_sst_fields {
+  const double *k, *omega, *k_prev, *rho, *mu, *ymin;
+  const double *gradU;         /* [nn][9], row-major d u_i / d x_j */
+  const double *gradK, *gradW; /* [nn][3] */
+  const double *div, *vol, *mut_old, *pk_wall;
+  const int* wall_node;        /* 1 on no-slip wall nodes */
+  double *mut, *F1, *Pk;
+  double *k_diag, *k_rhs;      /* node-term diagonal / rhs of the k equation */
+  double *w_diag, *w_rhs;      /* same for omega */
+} oa_sst_fields;
+
+void oa_sst_default_constants(oa_sst_constants* c);
+/* Launch on `stream` (NULL: default stream); asynchronous. */
+int oa_sst_node_update(int nn, const oa_sst_constants* c, double dt, double mut_urf, const oa_sst_fields* f,
+                       void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -30,7 +30,7 @@ EXPORTS = [
     "oa_flow_stream", "oa_launch_count", "oa_time_kernel", "oa_pcorr_solve_static",
     "oa_diffusion_create", "oa_diffusion_destroy", "oa_diffusion_set_field", "oa_diffusion_get_field",
     "oa_diffusion_field_device_ptr", "oa_diffusion_assemble", "oa_diffusion_solve", "oa_diffusion_step",
-    "oa_diffusion_stream", "oa_diffusion_time_assembly",
+    "oa_diffusion_stream", "oa_diffusion_time_assembly", "oa_sst_default_constants", "oa_sst_node_update",
 ]
 
 OA_BND_FIXED_VALUE = 0
@@ -77,6 +77,22 @@ def default_diffusion_settings(**kw) -> DiffusionSettings:
              precision=OA_PREC_FP64, amg=1, use_graphs=0)
     d.update(kw)
     return DiffusionSettings(**d)
+
+
+SST_CONSTANTS = ("sigma_k1", "sigma_k2", "sigma_w1", "sigma_w2", "beta1", "beta2", "gamma1", "gamma2", "a1",
+                 "beta_star", "prod_limit", "cmu")
+SST_INPUTS = ("k", "omega", "k_prev", "rho", "mu", "ymin", "gradU", "gradK", "gradW", "div", "vol", "mut_old",
+              "pk_wall")
+SST_OUTPUTS = ("mut", "F1", "Pk", "k_diag", "k_rhs", "w_diag", "w_rhs")
+
+
+class SstConstants(C.Structure):
+    _fields_ = [(n, C.c_double) for n in SST_CONSTANTS]
+
+
+class SstFields(C.Structure):
+    _fields_ = ([(n, C.c_void_p) for n in SST_INPUTS] + [("wall_node", C.c_void_p)] +
+                [(n, C.c_void_p) for n in SST_OUTPUTS])
 
 
 def default_settings(**kw) -> FlowSettings:
@@ -141,6 +157,8 @@ def lib():
         "oa_diffusion_step": (C.c_int, [vp, ip, dp, ip]),
         "oa_diffusion_stream": (C.c_int, [vp, P(vp)]),
         "oa_diffusion_time_assembly": (C.c_int, [vp, C.c_int, dp]),
+        "oa_sst_default_constants": (None, [P(SstConstants)]),
+        "oa_sst_node_update": (C.c_int, [C.c_int, P(SstConstants), C.c_double, C.c_double, P(SstFields), vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -382,3 +400,17 @@ class Diffusion:
             self.close()
         except Exception:
             pass
+
+
+def sst_constants() -> SstConstants:
+    c = SstConstants()
+    lib().oa_sst_default_constants(C.byref(c))
+    return c
+
+
+def sst_node_update(nn: int, ptrs: dict, dt=1.0, mut_urf=1.0, constants: SstConstants | None = None, stream=0):
+    """Launch the fused SST node kernel on device pointers (ints) named as
+    ``SST_INPUTS`` / ``wall_node`` / ``SST_OUTPUTS``; asynchronous on ``stream``."""
+    f = SstFields(**{n: ptrs.get(n) for n in SST_INPUTS + ("wall_node",) + SST_OUTPUTS})
+    c = constants or sst_constants()
+    _check(lib().oa_sst_node_update(int(nn), C.byref(c), dt, mut_urf, C.byref(f), C.c_void_p(stream or None)))

@@ -124,6 +124,26 @@ void orc_diff_spmv(void* h, const double* A, const double* x, double* y);
 /* one thermalEnergyEquation::solve step: assemble, BiCGStab, correct; returns iterations */
 int orc_diff_step(void* h, double* res);
 
+/* ---- k-omega SST node-level updates (sst.cpp) ---- */
+typedef struct orc_sst_constants {
+  double sigma_k1, sigma_k2, sigma_w1, sigma_w2, beta1, beta2, gamma1, gamma2, a1, beta_star, prod_limit, cmu;
+} orc_sst_constants;
+
+typedef struct orc_sst_in {
+  const double *k, *omega, *k_prev, *rho, *mu, *ymin, *gradU /*[nn][9]*/, *gradK /*[nn][3]*/, *gradW /*[nn][3]*/,
+      *div, *vol, *mut_old, *pk_wall;
+  const int* wall_node;
+} orc_sst_in;
+
+typedef struct orc_sst_out {
+  double *mut, *F1, *Pk, *k_diag, *k_rhs, *w_diag, *w_rhs;
+} orc_sst_out;
+
+void orc_sst_default_constants(orc_sst_constants* c);
+/* mu_t, F1, P_k and the steady k / omega node-term diagonal and rhs per node */
+void orc_sst_nodes(int nn, const orc_sst_constants* c, double dt, double mut_urf, const orc_sst_in* in,
+                   orc_sst_out* out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -79,6 +79,24 @@ def default_diff_settings(**kw) -> DiffSettings:
     return DiffSettings(**d)
 
 
+class SstConstants(C.Structure):
+    _fields_ = [(n, C.c_double) for n in ("sigma_k1", "sigma_k2", "sigma_w1", "sigma_w2", "beta1", "beta2",
+                                           "gamma1", "gamma2", "a1", "beta_star", "prod_limit", "cmu")]
+
+
+SST_IN = ("k", "omega", "k_prev", "rho", "mu", "ymin", "gradU", "gradK", "gradW", "div", "vol", "mut_old",
+          "pk_wall")
+SST_OUT = ("mut", "F1", "Pk", "k_diag", "k_rhs", "w_diag", "w_rhs")
+
+
+class SstIn(C.Structure):
+    _fields_ = [(n, C.POINTER(C.c_double)) for n in SST_IN] + [("wall_node", C.POINTER(C.c_int))]
+
+
+class SstOut(C.Structure):
+    _fields_ = [(n, C.POINTER(C.c_double)) for n in SST_OUT]
+
+
 def build():
     subprocess.run(["make", "-s", "-C", _HERE], check=True)
 
@@ -139,6 +157,8 @@ def lib():
         L.orc_diff_spmv.argtypes = [C.c_void_p, dp, dp, dp]
         L.orc_diff_bicgstab.restype = C.c_int
         L.orc_diff_bicgstab.argtypes = [C.c_void_p, dp, dp, dp, C.c_double, C.c_int, dp]
+        L.orc_sst_default_constants.argtypes = [P(SstConstants)]
+        L.orc_sst_nodes.argtypes = [C.c_int, P(SstConstants), C.c_double, C.c_double, P(SstIn), P(SstOut)]
         L.orc_diff_step.restype = C.c_int
         L.orc_diff_step.argtypes = [C.c_void_p, dp]
         _lib = L
@@ -380,3 +400,23 @@ def tri3_face_areav(p):
     a = np.zeros((3, 3))
     lib().orc_tri3_face_areav(_dp(p), _dp(a))
     return a
+
+
+def sst_constants() -> SstConstants:
+    c = SstConstants()
+    lib().orc_sst_default_constants(C.byref(c))
+    return c
+
+
+def sst_nodes(fields: dict, dt=1.0, mut_urf=1.0, constants: SstConstants | None = None) -> dict:
+    """Node-level SST updates on numpy fields (``SST_IN`` names plus
+    ``wall_node``); returns the ``SST_OUT`` arrays."""
+    nn = fields["k"].shape[0]
+    keep = {n: np.ascontiguousarray(fields[n], np.float64) for n in SST_IN if fields.get(n) is not None}
+    wall = np.ascontiguousarray(fields["wall_node"], np.int32)
+    si = SstIn(**{n: (_dp(keep[n]) if n in keep else None) for n in SST_IN}, wall_node=_ip(wall))
+    outs = {n: np.zeros(nn) for n in SST_OUT}
+    so = SstOut(**{n: _dp(outs[n]) for n in SST_OUT})
+    c = constants or sst_constants()
+    lib().orc_sst_nodes(nn, C.byref(c), dt, mut_urf, C.byref(si), C.byref(so))
+    return outs
