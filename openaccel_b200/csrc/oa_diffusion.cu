@@ -214,15 +214,15 @@ struct DiffView {
 // with the defect rhs += grad(phi) . S. A face item adds the fixed-value flux
 // of its boundary ip: lhs on the off-face node only (the side nodes' columns
 // carry bcMultiplier 0) and rhs += Gamma_bip * grad(phi~) . A_bip with phi~ the
-// side values on the face nodes. The diagonal and rhs are warp sums; each
-// off-diagonal entry is summed by the lane owning its CSR slot over the items
-// in ascending order, so every entry is written once and the result does not
-// depend on scheduling.
+// side values on the face nodes. The diagonal and rhs are warp sums; the
+// off-diagonal entries are a segmented sum by CSR slot (__match_any_sync
+// groups, each summed in ascending lane order), so every entry is written once
+// and the result does not depend on scheduling.
 template <bool SH, class TM>
 __global__ void __launch_bounds__(32 * DWARPS) k_diffusion(MeshView m, DiffView d, TM* __restrict__ A,
                                                              double* __restrict__ b, int* err) {
-  __shared__ double s_v[DWARPS][32][3];
-  __shared__ uint32_t s_s[DWARPS][32];
+  __shared__ double s_val[DWARPS][32];
+  __shared__ double s_part[DWARPS][3][DIFF_MAX_ROW];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int row = blockIdx.x * DWARPS + w;
   if (row >= m.nn) return;  // whole warp
@@ -324,23 +324,29 @@ __global__ void __launch_bounds__(32 * DWARPS) k_diffusion(MeshView m, DiffView 
       for (int q = 0; q < 3; ++q)
         if (nb[q] == cs) sl[q] = s;
     }
+    // segmented sum by CSR slot: lanes holding the same slot (for the same
+    // off-diagonal position q) are summed by the lowest of them in ascending
+    // lane order; the slot's owner lane then adds the three position partials
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      s_part[w][q][lane] = 0.0;
+      s_part[w][q][lane + 32] = 0.0;
+    }
 #pragma unroll
     for (int q = 0; q < 3; ++q) {
       if (nb[q] >= 0 && sl[q] < 0) sl[q] = dslot;  // column outside the stencil: lumped into the diagonal
-      s_v[w][lane][q] = v[q];
-    }
-    s_s[w][lane] = (uint32_t)(sl[0] + 1) | (uint32_t)(sl[1] + 1) << 8 | (uint32_t)(sl[2] + 1) << 16;
-    __syncwarp();
-    const int cnt = min(32, nitems - base);
-    for (int i = 0; i < cnt; ++i) {
-      const uint32_t pk = s_s[w][i];
-#pragma unroll
-      for (int q = 0; q < 3; ++q) {
-        const int sq = (int)((pk >> (8 * q)) & 255u) - 1;
-        if (sq == lane) accA += s_v[w][i][q];
-        else if (sq == lane + 32) accB += s_v[w][i][q];
+      s_val[w][lane] = v[q];
+      __syncwarp();
+      const unsigned peers = __match_any_sync(0xffffffffu, sl[q]);
+      if (sl[q] >= 0 && lane == __ffs(peers) - 1) {
+        double sum = 0.0;
+        for (unsigned mk = peers; mk; mk &= mk - 1) sum += s_val[w][__ffs(mk) - 1];
+        s_part[w][q][sl[q]] = sum;
       }
+      __syncwarp();
     }
+    accA += s_part[w][0][lane] + s_part[w][1][lane] + s_part[w][2][lane];
+    accB += s_part[w][0][lane + 32] + s_part[w][1][lane + 32] + s_part[w][2][lane + 32];
     __syncwarp();
   }
   // diagonal: element share, then relaxation (diag / urf)
