@@ -129,7 +129,7 @@ def run_ours(args, rank, world):
         # form launches every kernel from the host
         graphs = 1 if (prec == rt.OA_PREC_MIXED and not args.no_graphs) else 0
         f = rt.Flow(gm, rt.default_settings(precision=prec, pc_rtol=args.pc_rtol, mom_rtol=args.mom_rtol,
-                                            use_graphs=graphs))
+                                            mom_maxit=args.mom_maxit, use_graphs=graphs))
         f.set_field("U", U0)
         f.initialize()
         return f
@@ -234,7 +234,7 @@ def run_ours(args, rank, world):
         "data": "synthetic",
         "config": {"workload": f"lid-driven cavity {args.n}^3 hex8 skewed +-20%, Re=100, U0~N(0,0.1)",
                    "elements": m.ne, "nodes": m.nn, "nnz": gm.nnz, "pc_rtol": args.pc_rtol,
-                   "mom_rtol": args.mom_rtol, "l2": "inputs larger than L2 (no flush)",
+                   "mom_rtol": args.mom_rtol, "mom_maxit": args.mom_maxit, "l2": "inputs larger than L2 (no flush)",
                    "parallelism": f"replicas x{world}"},
         "fp64_outer_iters_per_s": value64,
         "mixed_over_fp64": value / value64,
@@ -365,7 +365,7 @@ def cpu_sample(args, threads):
     po.set_threads(threads)
     m, U0 = workload(args.cpu_n)
     c = po.FlowCase(m, po.default_settings(pc_rtol=args.pc_rtol, mom_rtol=args.mom_rtol, pc_maxit=20000,
-                                           mom_maxit=1000), U0=U0)
+                                           mom_maxit=args.mom_maxit), U0=U0)
     c.initialize()
     t0 = time.perf_counter()
     c.simple_iteration()
@@ -382,7 +382,10 @@ def main():
     ap.add_argument("--n", type=int, default=128)
     ap.add_argument("--cpu-n", type=int, default=128)
     ap.add_argument("--pc-rtol", type=float, default=1e-8)
-    ap.add_argument("--mom-rtol", type=float, default=1e-6)
+    # momentum solver settings of the reference's cavity example
+    # (examples/cavity/input.i: linear_solver_settings default, rtol 1e-1, 20 iterations)
+    ap.add_argument("--mom-rtol", type=float, default=1e-1)
+    ap.add_argument("--mom-maxit", type=int, default=20)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-graphs", action="store_true")
     ap.add_argument("--only-mixed", action="store_true", help="time the mixed form only (profiling)")

@@ -6,6 +6,7 @@
 #include <vector>
 
 #include "oa_amg.h"
+#include "oa_amg_symbolic.h"
 #include "oa_internal.h"
 
 namespace oa {
@@ -13,38 +14,11 @@ namespace oa {
 constexpr int AB = 256;          // threads per block
 constexpr int COARSE_MAX = 256;  // coarsest level solved by a dense inverse
 
-// ---------------------------------------------------------------------------
-// host: greedy aggregation of a CSR graph (root + all its free neighbours,
-// then leftover rows join an adjacent aggregate)
-static int aggregate(int n, const std::vector<int>& rp, const std::vector<int>& cols, std::vector<int>& agg) {
-  agg.assign(n, -1);
-  int nc = 0;
-  for (int i = 0; i < n; ++i) {
-    if (agg[i] != -1) continue;
-    bool free_nb = true;
-    for (int k = rp[i]; k < rp[i + 1]; ++k)
-      if (cols[k] != i && agg[cols[k]] != -1) {
-        free_nb = false;
-        break;
-      }
-    if (!free_nb) continue;
-    agg[i] = nc;
-    for (int k = rp[i]; k < rp[i + 1]; ++k) agg[cols[k]] = nc;
-    ++nc;
-  }
-  std::vector<int> pass1(agg);
-  for (int i = 0; i < n; ++i) {
-    if (agg[i] != -1) continue;
-    int best = -1;
-    for (int k = rp[i]; k < rp[i + 1]; ++k)
-      if (pass1[cols[k]] != -1) {
-        best = pass1[cols[k]];
-        break;
-      }
-    agg[i] = best >= 0 ? best : nc++;
-  }
-  return nc;
-}
+// lanes per row for an average row length: 1, 8 or 32
+static int lanes_for(double avg) { return avg <= 6.0 ? 1 : (avg <= 24.0 ? 8 : 32); }
+
+static unsigned grid_for(long long rows, int lpr) { return (unsigned)((rows * lpr + AB - 1) / AB); }
+
 
 template <class T>
 static int upload(T** d, const std::vector<T>& h) {
@@ -65,6 +39,13 @@ static int dalloc(T** d, size_t n) {
 template <class T>
 int Amg<T>::setup(int n, const int* h_rp, const int* h_cols, const int* h_diag, int* d_rp, int* d_cols, int* d_diag) {
   release();
+  // tuning knobs: prolongation type, Jacobi damping, coarse-correction scaling
+  if (const char* e = std::getenv("OA_AMG_SMOOTHED")) smoothed = std::atoi(e) != 0;
+  omega = smoothed ? 0.8 : 0.7;
+  alpha = smoothed ? 1.0 : 1.8;
+  if (const char* e = std::getenv("OA_AMG_OMEGA")) omega = std::atof(e);
+  if (const char* e = std::getenv("OA_AMG_ALPHA")) alpha = std::atof(e);
+  if (const char* e = std::getenv("OA_AMG_OMEGA_P")) omega_p = std::atof(e);
   std::vector<int> rp(h_rp, h_rp + n + 1), cols(h_cols, h_cols + h_rp[n]), dg(h_diag, h_diag + n);
   int cur = n;
   for (int lev = 0;; ++lev) {
@@ -84,63 +65,93 @@ int Amg<T>::setup(int n, const int* h_rp, const int* h_cols, const int* h_diag, 
     int s;
     if ((s = dalloc(&lv.dinv, cur)) || (s = dalloc(&lv.r, cur)) || (s = dalloc(&lv.t, cur))) return s;
     if (lev > 0 && ((s = dalloc(&lv.x, cur)) || (s = dalloc(&lv.b, cur)))) return s;
+    lv.lpr_a = lanes_for(double(lv.nnz) / std::max(1, cur));
     const bool last = cur <= COARSE_MAX || lev >= 14;
     if (last) {
       L.push_back(lv);
       break;
     }
-    std::vector<int> agg;
-    const int nc = aggregate(cur, rp, cols, agg);
-    if (nc >= cur) return fail(OA_ERR_SOLVER, "AMG: aggregation made no progress");
-    // members of each aggregate, in row order
-    std::vector<int> mptr(nc + 1, 0), mlist(cur);
-    for (int i = 0; i < cur; ++i) mptr[agg[i] + 1]++;
-    for (int c = 0; c < nc; ++c) mptr[c + 1] += mptr[c];
-    {
-      std::vector<int> pos(mptr.begin(), mptr.end() - 1);
-      for (int i = 0; i < cur; ++i) mlist[pos[agg[i]]++] = i;
-    }
-    // coarse graph (sorted columns) and the gather list of each coarse entry
-    std::vector<int> crp(nc + 1, 0), ccols, cdg(nc, 0);
-    std::vector<int> tmp;
-    for (int c = 0; c < nc; ++c) {
-      tmp.clear();
-      for (int m = mptr[c]; m < mptr[c + 1]; ++m) {
-        const int i = mlist[m];
-        for (int k = rp[i]; k < rp[i + 1]; ++k) tmp.push_back(agg[cols[k]]);
+    int nc = 0;
+    std::vector<int> crp, ccols, cdg;
+    if (smoothed) {
+      sa::Level H;
+      if (!sa::build(cur, rp, cols, H))
+        return fail(OA_ERR_SOLVER, "AMG: smoothed-aggregation term lists exceed 32-bit offsets");
+      nc = H.nc;
+      if (nc >= cur) return fail(OA_ERR_SOLVER, "AMG: aggregation made no progress");
+      lv.nnz_t = H.trp[cur];
+      lv.nnz_p = H.prp[cur];
+      lv.lpr_p = lanes_for(double(lv.nnz_p) / cur);
+      lv.lpr_pt = lanes_for(double(lv.nnz_p) / H.nc);
+      lv.lpr_t = lanes_for(double(H.tta.size()) / std::max(1, lv.nnz_t));
+      lv.lpr_c = lanes_for(double(H.ctp.size()) / std::max(1, H.crp[H.nc]));
+      if ((s = upload(&lv.p_rp, H.prp)) || (s = upload(&lv.p_cols, H.pcols)) || (s = upload(&lv.p_diag, H.pdiag)) ||
+          (s = upload(&lv.pg_ptr, H.pgptr)) || (s = upload(&lv.pg_list, H.pglist)) ||
+          (s = upload(&lv.pt_rp, H.ptrp)) || (s = upload(&lv.pt_rows, H.ptrows)) || (s = upload(&lv.pt_src, H.ptsrc)) ||
+          (s = upload(&lv.tt_ptr, H.ttptr)) || (s = upload(&lv.tt_a, H.tta)) || (s = upload(&lv.tt_p, H.ttp)) ||
+          (s = upload(&lv.ct_ptr, H.ctptr)) || (s = upload(&lv.ct_p, H.ctp)) || (s = upload(&lv.ct_t, H.ctt)) ||
+          (s = dalloc(&lv.pv, H.pcols.size())) || (s = dalloc(&lv.ptv, H.pcols.size())) ||
+          (s = dalloc(&lv.tv, (size_t)lv.nnz_t)))
+        return s;
+      crp.swap(H.crp);
+      ccols.swap(H.ccols);
+      cdg.swap(H.cdg);
+    } else {
+      std::vector<int> agg;
+      nc = sa::aggregate(cur, rp, cols, agg);
+      if (nc >= cur) return fail(OA_ERR_SOLVER, "AMG: aggregation made no progress");
+      // members of each aggregate, in row order
+      std::vector<int> mptr(nc + 1, 0), mlist(cur);
+      for (int i = 0; i < cur; ++i) mptr[agg[i] + 1]++;
+      for (int c = 0; c < nc; ++c) mptr[c + 1] += mptr[c];
+      {
+        std::vector<int> pos(mptr.begin(), mptr.end() - 1);
+        for (int i = 0; i < cur; ++i) mlist[pos[agg[i]]++] = i;
       }
-      std::sort(tmp.begin(), tmp.end());
-      tmp.erase(std::unique(tmp.begin(), tmp.end()), tmp.end());
-      for (size_t q = 0; q < tmp.size(); ++q)
-        if (tmp[q] == c) cdg[c] = (int)q;
-      ccols.insert(ccols.end(), tmp.begin(), tmp.end());
-      crp[c + 1] = (int)ccols.size();
-    }
-    const int cnnz = crp[nc];
-    std::vector<int> gcnt(cnnz + 1, 0), target(rp[cur]);
-    for (int c = 0; c < nc; ++c)
-      for (int m = mptr[c]; m < mptr[c + 1]; ++m) {
-        const int i = mlist[m];
-        for (int k = rp[i]; k < rp[i + 1]; ++k) {
-          const int cj = agg[cols[k]];
-          const int pos = (int)(std::lower_bound(ccols.begin() + crp[c], ccols.begin() + crp[c + 1], cj) - ccols.begin());
-          target[k] = pos;
-          gcnt[pos + 1]++;
+      // coarse graph (sorted columns) and the gather list of each coarse entry
+      crp.assign(nc + 1, 0);
+      cdg.assign(nc, 0);
+      std::vector<int> tmp;
+      for (int c = 0; c < nc; ++c) {
+        tmp.clear();
+        for (int m = mptr[c]; m < mptr[c + 1]; ++m) {
+          const int i = mlist[m];
+          for (int k = rp[i]; k < rp[i + 1]; ++k) tmp.push_back(agg[cols[k]]);
         }
+        std::sort(tmp.begin(), tmp.end());
+        tmp.erase(std::unique(tmp.begin(), tmp.end()), tmp.end());
+        for (size_t q = 0; q < tmp.size(); ++q)
+          if (tmp[q] == c) cdg[c] = (int)q;
+        ccols.insert(ccols.end(), tmp.begin(), tmp.end());
+        crp[c + 1] = (int)ccols.size();
       }
-    for (int q = 0; q < cnnz; ++q) gcnt[q + 1] += gcnt[q];
-    std::vector<int> glist(rp[cur]);
-    {
-      std::vector<int> pos(gcnt.begin(), gcnt.end() - 1);
+      const int cnnz = crp[nc];
+      std::vector<int> gcnt(cnnz + 1, 0), target(rp[cur]);
       for (int c = 0; c < nc; ++c)
         for (int m = mptr[c]; m < mptr[c + 1]; ++m) {
           const int i = mlist[m];
-          for (int k = rp[i]; k < rp[i + 1]; ++k) glist[pos[target[k]]++] = k;
+          for (int k = rp[i]; k < rp[i + 1]; ++k) {
+            const int cj = agg[cols[k]];
+            const int pos =
+                (int)(std::lower_bound(ccols.begin() + crp[c], ccols.begin() + crp[c + 1], cj) - ccols.begin());
+            target[k] = pos;
+            gcnt[pos + 1]++;
+          }
         }
+      for (int q = 0; q < cnnz; ++q) gcnt[q + 1] += gcnt[q];
+      std::vector<int> glist(rp[cur]);
+      {
+        std::vector<int> pos(gcnt.begin(), gcnt.end() - 1);
+        for (int c = 0; c < nc; ++c)
+          for (int m = mptr[c]; m < mptr[c + 1]; ++m) {
+            const int i = mlist[m];
+            for (int k = rp[i]; k < rp[i + 1]; ++k) glist[pos[target[k]]++] = k;
+          }
+      }
+      if ((s = upload(&lv.agg, agg)) || (s = upload(&lv.mptr, mptr)) || (s = upload(&lv.mlist, mlist)) ||
+          (s = upload(&lv.gptr, gcnt)) || (s = upload(&lv.glist, glist)))
+        return s;
     }
-    if ((s = upload(&lv.agg, agg)) || (s = upload(&lv.mptr, mptr)) || (s = upload(&lv.mlist, mlist)) ||
-        (s = upload(&lv.gptr, gcnt)) || (s = upload(&lv.glist, glist)))
-      return s;
     L.push_back(lv);
     rp.swap(crp);
     cols.swap(ccols);
@@ -150,9 +161,6 @@ int Amg<T>::setup(int n, const int* h_rp, const int* h_cols, const int* h_diag, 
   coarse_n = L.back().n;
   if (cudaMalloc(&dense_inv, sizeof(double) * 2 * (size_t)coarse_n * coarse_n) != cudaSuccess)
     return fail(OA_ERR_CUDA, "AMG: dense coarse allocation failed");
-  // tuning knobs (Jacobi damping, coarse-correction scaling)
-  if (const char* e = std::getenv("OA_AMG_OMEGA")) omega = std::atof(e);
-  if (const char* e = std::getenv("OA_AMG_ALPHA")) alpha = std::atof(e);
   ready = true;
   return OA_OK;
 }
@@ -167,7 +175,9 @@ void Amg<T>::release() {
       cudaFree(v.diag);
     }
     if (v.own_A) cudaFree(v.A);
-    void* p[] = {v.dinv, v.agg, v.mptr, v.mlist, v.gptr, v.glist, v.r, v.t};
+    void* p[] = {v.dinv,   v.agg,   v.mptr,   v.mlist, v.gptr,   v.glist, v.r,      v.t,    v.p_rp,
+                 v.p_cols, v.p_diag, v.pg_ptr, v.pg_list, v.pv, v.ptv, v.pt_rp, v.pt_rows, v.pt_src, v.tv,
+                 v.tt_ptr, v.tt_a,   v.tt_p,   v.ct_ptr, v.ct_p, v.ct_t};
     for (void* q : p)
       if (q) cudaFree(q);
     if (l > 0) {
@@ -232,21 +242,33 @@ __global__ void k_gauss_jordan(int n, double* M) {
   }
 }
 
-// Downward step, row parallel: pre-smooth from zero, xs_i = w Dinv_i b_i, and
-// the residual r_i = b_i - sum_j a_ij xs_j (neighbours' xs formed from b).
-template <class T>
+// Sum of one value per lane over a group of LPR consecutive lanes (a row's
+// lanes), by a fixed xor butterfly: the same order every run.
+template <int LPR>
+__device__ __forceinline__ double group_sum(double v) {
+#pragma unroll
+  for (int o = LPR / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Downward step, LPR lanes per row: pre-smooth from zero, xs_i = w Dinv_i b_i,
+// and the residual r_i = b_i - sum_j a_ij xs_j (neighbours' xs formed from b).
+template <class T, int LPR>
 __global__ void __launch_bounds__(AB) k_smooth_resid(int n, const int* __restrict__ rp, const int* __restrict__ cols,
                                                      const T* __restrict__ A, const T* __restrict__ dinv,
                                                      const T* __restrict__ b, T* __restrict__ xs, T* __restrict__ r,
                                                      double w, const int* done) {
   if (*done) return;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = g / LPR, lane = g % LPR;
   double s = 0.0;
-  for (int k = rp[i]; k < rp[i + 1]; ++k) {
-    const int j = cols[k];
-    s += double(A[k]) * (w * double(dinv[j]) * double(b[j]));
-  }
+  if (i < n)
+    for (int k = rp[i] + lane; k < rp[i + 1]; k += LPR) {
+      const int j = cols[k];
+      s += double(A[k]) * (w * double(dinv[j]) * double(b[j]));
+    }
+  s = group_sum<LPR>(s);
+  if (i >= n || lane) return;
   const double bi = double(b[i]);
   xs[i] = T(w * double(dinv[i]) * bi);
   r[i] = T(bi - s);
@@ -298,6 +320,102 @@ __global__ void k_dense_apply(int n, const double* __restrict__ M, const T* __re
   x[i] = T(s);
 }
 
+// Smoothed prolongation, row parallel: P_iJ = [J == agg(i)] - wp Dinv_i
+// sum of the row's A entries whose column lies in aggregate J.
+template <class T>
+__global__ void k_sa_prolongator(int n, const int* __restrict__ p_rp, const int* __restrict__ p_diag,
+                                 const int* __restrict__ pg_ptr, const int* __restrict__ pg_list,
+                                 const T* __restrict__ A, const T* __restrict__ dinv, double wp, T* __restrict__ pv) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double di = double(dinv[i]);
+  const int e0 = p_rp[i];
+  for (int e = e0; e < p_rp[i + 1]; ++e) {
+    double s = 0.0;
+    for (int q = pg_ptr[e]; q < pg_ptr[e + 1]; ++q) s += double(A[pg_list[q]]);
+    pv[e] = T((e - e0 == p_diag[i] ? 1.0 : 0.0) - wp * di * s);
+  }
+}
+
+// out_e = sum over the entry's term list of a[ia] * b[ib], LPR lanes per entry.
+template <class T, int LPR>
+__global__ void __launch_bounds__(AB) k_pair_sum(int n_out, const int* __restrict__ ptr, const int* __restrict__ ia,
+                                                 const int* __restrict__ ib, const T* __restrict__ a,
+                                                 const T* __restrict__ b, T* __restrict__ out) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  const int e = g / LPR, lane = g % LPR;
+  double s = 0.0;
+  if (e < n_out)
+    for (int q = ptr[e] + lane; q < ptr[e + 1]; q += LPR) s += double(a[ia[q]]) * double(b[ib[q]]);
+  s = group_sum<LPR>(s);
+  if (e < n_out && lane == 0) out[e] = T(s);
+}
+
+// P^T values in coarse-row order (contiguous for the restriction)
+template <class T>
+__global__ void k_gather(int n, const int* __restrict__ idx, const T* __restrict__ src, T* __restrict__ dst) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q < n) dst[q] = src[idx[q]];
+}
+
+// restriction bc = P^T r, LPR lanes per coarse row
+template <class T, int LPR>
+__global__ void __launch_bounds__(AB) k_sa_restrict(int nc, const int* __restrict__ pt_rp,
+                                                    const int* __restrict__ pt_rows, const T* __restrict__ ptv,
+                                                    const T* __restrict__ r, T* __restrict__ bc, const int* done) {
+  if (*done) return;
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  const int c = g / LPR, lane = g % LPR;
+  double s = 0.0;
+  if (c < nc)
+    for (int q = pt_rp[c] + lane; q < pt_rp[c + 1]; q += LPR) s += double(ptv[q]) * double(r[pt_rows[q]]);
+  s = group_sum<LPR>(s);
+  if (c < nc && lane == 0) bc[c] = T(s);
+}
+
+// coarse correction in place: t_i += alpha (P xc)_i, LPR lanes per row
+template <class T, int LPR>
+__global__ void __launch_bounds__(AB) k_sa_prolong_add(int n, const int* __restrict__ p_rp,
+                                                       const int* __restrict__ p_cols, const T* __restrict__ pv,
+                                                       const T* __restrict__ xc, T* __restrict__ t, double alpha,
+                                                       const int* done) {
+  if (*done) return;
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = g / LPR, lane = g % LPR;
+  double s = 0.0;
+  if (i < n)
+    for (int e = p_rp[i] + lane; e < p_rp[i + 1]; e += LPR) s += double(pv[e]) * double(xc[p_cols[e]]);
+  s = group_sum<LPR>(s);
+  if (i < n && lane == 0) t[i] = T(double(t[i]) + alpha * s);
+}
+
+// post-smooth out of place, LPR lanes per row:
+// x_i = t_i + w Dinv_i (b_i - sum_j a_ij t_j)
+template <class T, int LPR>
+__global__ void __launch_bounds__(AB) k_post_smooth(int n, const int* __restrict__ rp, const int* __restrict__ cols,
+                                                    const T* __restrict__ A, const T* __restrict__ dinv,
+                                                    const T* __restrict__ b, const T* __restrict__ t,
+                                                    T* __restrict__ x, double w, const int* done) {
+  if (*done) return;
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = g / LPR, lane = g % LPR;
+  double s = 0.0;
+  if (i < n)
+    for (int k = rp[i] + lane; k < rp[i + 1]; k += LPR) s += double(A[k]) * double(t[cols[k]]);
+  s = group_sum<LPR>(s);
+  if (i < n && lane == 0) x[i] = T(double(t[i]) + w * double(dinv[i]) * (double(b[i]) - s));
+}
+
+#define OA_LPR_LAUNCH(lpr, kernel, T, rows, st, ...)                                         \
+  do {                                                                                        \
+    if ((lpr) == 1)                                                                           \
+      kernel<T, 1><<<grid_for(rows, 1), AB, 0, st>>>(__VA_ARGS__);                            \
+    else if ((lpr) == 8)                                                                      \
+      kernel<T, 8><<<grid_for(rows, 8), AB, 0, st>>>(__VA_ARGS__);                            \
+    else                                                                                      \
+      kernel<T, 32><<<grid_for(rows, 32), AB, 0, st>>>(__VA_ARGS__);                          \
+  } while (0)
+
 // ---------------------------------------------------------------------------
 template <class T>
 int Amg<T>::numeric(const T* A_fine, cudaStream_t st) {
@@ -306,15 +424,26 @@ int Amg<T>::numeric(const T* A_fine, cudaStream_t st) {
   for (size_t l = 0; l < L.size(); ++l) {
     AmgLevel<T>& v = L[l];
     k_dinv<T><<<(v.n + AB - 1) / AB, AB, 0, st>>>(v.n, v.rp, v.diag, v.A, v.dinv);
+    count_launches(1);
     if (l + 1 < L.size()) {
       AmgLevel<T>& c = L[l + 1];
-      k_galerkin<T><<<(c.nnz + AB - 1) / AB, AB, 0, st>>>(c.nnz, v.gptr, v.glist, v.A, c.A);
+      if (smoothed) {
+        k_sa_prolongator<T><<<(v.n + AB - 1) / AB, AB, 0, st>>>(v.n, v.p_rp, v.p_diag, v.pg_ptr, v.pg_list, v.A,
+                                                                v.dinv, omega_p, v.pv);
+        k_gather<T><<<(v.nnz_p + AB - 1) / AB, AB, 0, st>>>(v.nnz_p, v.pt_src, v.pv, v.ptv);
+        OA_LPR_LAUNCH(v.lpr_t, k_pair_sum, T, v.nnz_t, st, v.nnz_t, v.tt_ptr, v.tt_a, v.tt_p, v.A, v.pv, v.tv);
+        OA_LPR_LAUNCH(v.lpr_c, k_pair_sum, T, c.nnz, st, c.nnz, v.ct_ptr, v.ct_p, v.ct_t, v.pv, v.tv, c.A);
+        count_launches(4);
+      } else {
+        k_galerkin<T><<<(c.nnz + AB - 1) / AB, AB, 0, st>>>(c.nnz, v.gptr, v.glist, v.A, c.A);
+        count_launches(1);
+      }
     }
   }
   const AmgLevel<T>& cl = L.back();
   k_dense_fill<T><<<cl.n, 128, 0, st>>>(cl.n, cl.rp, cl.cols, cl.A, dense_inv);
   k_gauss_jordan<<<1, 1024, 0, st>>>(cl.n, dense_inv);
-  count_launches(2 * (long long)L.size() + 1);
+  count_launches(2);
   OA_CUDA(cudaGetLastError());
   return OA_OK;
 }
@@ -332,19 +461,30 @@ int Amg<T>::apply(const T* v, T* z, const int* done, cudaStream_t st) {
       break;
     }
     AmgLevel<T>& c = L[l + 1];
-    k_smooth_resid<T><<<(lv.n + AB - 1) / AB, AB, 0, st>>>(lv.n, lv.rp, lv.cols, lv.A, lv.dinv, b, lv.t, lv.r, omega,
-                                                            done);
-    k_restrict<T><<<(c.n + AB - 1) / AB, AB, 0, st>>>(c.n, lv.mptr, lv.mlist, lv.r, c.b, done);
+    OA_LPR_LAUNCH(lv.lpr_a, k_smooth_resid, T, lv.n, st, lv.n, lv.rp, lv.cols, lv.A, lv.dinv, b, lv.t, lv.r, omega,
+                  done);
+    if (smoothed)
+      OA_LPR_LAUNCH(lv.lpr_pt, k_sa_restrict, T, c.n, st, c.n, lv.pt_rp, lv.pt_rows, lv.ptv, lv.r, c.b, done);
+    else
+      k_restrict<T><<<(c.n + AB - 1) / AB, AB, 0, st>>>(c.n, lv.mptr, lv.mlist, lv.r, c.b, done);
   }
-  // upward pass: one fused prolong/post-smooth kernel per level
+  // upward pass: prolongation + post-smooth (one fused kernel for the
+  // piecewise-constant prolongation, two for the smoothed one)
   for (int l = nl - 2; l >= 0; --l) {
     AmgLevel<T>& lv = L[l];
     const T* b = l == 0 ? v : lv.b;
     T* x = l == 0 ? z : lv.x;
-    k_up<T><<<(lv.n + AB - 1) / AB, AB, 0, st>>>(lv.n, lv.rp, lv.cols, lv.A, lv.dinv, lv.agg, b, lv.t, L[l + 1].x,
-                                                  x, omega, alpha, done);
+    if (smoothed) {
+      OA_LPR_LAUNCH(lv.lpr_p, k_sa_prolong_add, T, lv.n, st, lv.n, lv.p_rp, lv.p_cols, lv.pv, L[l + 1].x, lv.t,
+                    alpha, done);
+      OA_LPR_LAUNCH(lv.lpr_a, k_post_smooth, T, lv.n, st, lv.n, lv.rp, lv.cols, lv.A, lv.dinv, b, lv.t, x, omega,
+                    done);
+    } else {
+      k_up<T><<<(lv.n + AB - 1) / AB, AB, 0, st>>>(lv.n, lv.rp, lv.cols, lv.A, lv.dinv, lv.agg, b, lv.t, L[l + 1].x,
+                                                    x, omega, alpha, done);
+    }
   }
-  count_launches(3 * (long long)(nl - 1) + 1);
+  count_launches((smoothed ? 4 : 3) * (long long)(nl - 1) + 1);
   OA_CUDA(cudaGetLastError());
   return OA_OK;
 }

@@ -2,11 +2,13 @@
 //
 // The reference's pressure-correction systems go to liblinsolve's PETSc /
 // Trilinos (ILU) / HYPRE (BoomerAMG) back ends (examples/cavity/input.i:61-77),
-// which are absent. This is an unsmoothed-aggregation AMG V-cycle built for
-// the device: the hierarchy's structure (aggregates, coarse graphs and the
-// fine-entry -> coarse-entry gather lists) depends only on the CSR graph and is
-// built once on the host; the numeric Galerkin products run on the device
-// every time the fine matrix is reassembled, as deterministic owner gathers.
+// which are absent. This is an aggregation AMG V-cycle built for the device,
+// with either the smoothed prolongation P = (I - wp Dinv A) P_tent (default)
+// or the piecewise-constant one with an over-corrected coarse correction. The
+// hierarchy's structure (aggregates, coarse graphs, and the term lists of P,
+// A P and P^T A P) depends only on the CSR graph and is built once on the host;
+// the numeric products run on the device every time the fine matrix is
+// reassembled, as deterministic owner sums.
 #pragma once
 #include <cuda_runtime.h>
 
@@ -26,6 +28,23 @@ struct AmgLevel {
   // Galerkin gather of the NEXT level's values: coarse entry c sums this
   // level's entries glist[gptr[c] .. gptr[c+1])
   int *gptr = nullptr, *glist = nullptr;
+  // smoothed prolongation P (CSR, n x nc): columns, offset of the row's own
+  // aggregate, per entry the A entries whose column lies in that aggregate,
+  // and values; P^T by coarse row (fine rows, P entry of each)
+  int *p_rp = nullptr, *p_cols = nullptr, *p_diag = nullptr, *pg_ptr = nullptr, *pg_list = nullptr;
+  T* pv = nullptr;
+  int *pt_rp = nullptr, *pt_rows = nullptr, *pt_src = nullptr;
+  T* ptv = nullptr;  // P^T values in coarse-row order
+  int nnz_p = 0;
+  // lanes per row of the row-parallel kernels (1, 8 or 32, from the average
+  // row length): A, P, P^T, and the T / coarse term lists
+  int lpr_a = 1, lpr_p = 1, lpr_pt = 1, lpr_t = 1, lpr_c = 1;
+  // T = A P values and term lists (A entry, P entry); the next level's values
+  // from term lists (P entry, T entry)
+  int nnz_t = 0;
+  T* tv = nullptr;
+  int *tt_ptr = nullptr, *tt_a = nullptr, *tt_p = nullptr;
+  int *ct_ptr = nullptr, *ct_p = nullptr, *ct_t = nullptr;
   // cycle work vectors: x (output, levels > 0), b (input, levels > 0), r
   // (residual), t (pre-smoothed iterate)
   T *x = nullptr, *b = nullptr, *r = nullptr, *t = nullptr;
@@ -38,10 +57,12 @@ struct Amg {
   double* dense_inv = nullptr;    // coarsest level inverse (FP64, n x n)
   double* h_dense = nullptr;      // pinned staging
   int coarse_n = 0;
-  double omega = 0.7;             // Jacobi damping
-  double alpha = 1.8;             // coarse-correction scaling (over-correction of the
-                                  // piecewise-constant prolongation; 1.8-2 halves the
-                                  // Krylov iterations on the 128^3 cavity)
+  bool smoothed = true;           // smoothed (true) or piecewise-constant prolongation
+  double omega = 0.8;             // Jacobi damping of the smoother
+  double omega_p = 0.74;          // prolongation smoothing, 4 / (3 rho(Dinv A)) with rho ~ 1.8
+  double alpha = 1.0;             // coarse-correction scaling (1.8 for the piecewise-constant
+                                  // prolongation, whose over-correction halves the Krylov
+                                  // iterations on the 128^3 cavity)
   int pre = 1, post = 1;          // smoothing sweeps
   bool ready = false;
 

@@ -219,7 +219,7 @@ struct DiffView {
 // groups, each summed in ascending lane order), so every entry is written once
 // and the result does not depend on scheduling.
 template <bool SH, class TM>
-__global__ void __launch_bounds__(32 * DWARPS) k_diffusion(MeshView m, DiffView d, TM* __restrict__ A,
+__global__ void __launch_bounds__(32 * DWARPS, 5) k_diffusion(MeshView m, DiffView d, TM* __restrict__ A,
                                                              double* __restrict__ b, int* err) {
   __shared__ double s_val[DWARPS][32];
   __shared__ double s_part[DWARPS][3][DIFF_MAX_ROW];

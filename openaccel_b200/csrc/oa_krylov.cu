@@ -11,6 +11,9 @@
 // host round trips; kernels after convergence return immediately.
 #include <cuda_runtime.h>
 
+#include <cstdio>
+#include <cstdlib>
+
 #include <cmath>
 #include <type_traits>
 
@@ -369,11 +372,20 @@ int KrylovSolver<B, TM, TV>::solve(const TM* A, const TB* b, TV*& xout, double r
     count_launches(1);
     return OA_OK;
   };
+  // OA_DEBUG: device time of the preconditioner set-up and of the whole solve
+  const bool dbg = std::getenv("OA_DEBUG") != nullptr;
+  cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
+  if (dbg)
+    for (auto& e : ev) {
+      cudaEventCreate(&e);
+    }
+  if (dbg) cudaEventRecord(ev[0], st);
   if constexpr (kAmgOk) {
     if (amg && !reuse_precond) {
       if (int s = amg->numeric(reinterpret_cast<const TV*>(A), st)) return s;
     }
   }
+  if (dbg) cudaEventRecord(ev[1], st);
   k_build_minv<B, TM><<<gr, KB, 0, st>>>(nn, rp, dg, A, Minv);
   k_init<TV, TB><<<gv, KB, 0, st>>>(n, b, x, r, rh, p, v, partials);
   k_init_scalars<<<1, KB, 0, st>>>(sc, partials, gv, rtol, maxit);
@@ -441,6 +453,16 @@ int KrylovSolver<B, TM, TV>::solve(const TM* A, const TB* b, TV*& xout, double r
   if (res) *res = h->bnorm > 0 ? h->rnorm / h->bnorm : 0.0;
   xout = x;
   last_status = h->status;
+  if (dbg) {
+    cudaEventRecord(ev[2], st);
+    cudaEventSynchronize(ev[2]);
+    float t_setup = 0.f, t_all = 0.f;
+    cudaEventElapsedTime(&t_setup, ev[0], ev[1]);
+    cudaEventElapsedTime(&t_all, ev[0], ev[2]);
+    std::fprintf(stderr, "[oa] BiCGStab<%d,%s> n %d iters %d: precond set-up %.3f ms, solve %.3f ms\n", B,
+                 sizeof(TV) == 4 ? "f32" : "f64", nn, h->iters, t_setup, t_all);
+    for (auto& e : ev) cudaEventDestroy(e);
+  }
   if (h->status == 2) return fail(OA_ERR_SOLVER, "BiCGStab: non-finite residual");
   return OA_OK;
 }
