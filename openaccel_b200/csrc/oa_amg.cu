@@ -14,8 +14,25 @@ namespace oa {
 constexpr int AB = 256;          // threads per block
 constexpr int COARSE_MAX = 256;  // coarsest level solved by a dense inverse
 
-// lanes per row for an average row length: 1, 8 or 32
-static int lanes_for(double avg) { return avg <= 6.0 ? 1 : (avg <= 24.0 ? 8 : 32); }
+// Lanes per row of the row-parallel kernels (1, 4, 8 or 32): levels with many
+// rows keep one lane per row for short rows and take 8 for long ones (the
+// first coarse level of the 128^3 cavity: 31 entries per row, 8 lanes measured
+// fastest against 1, 4 and 32); small levels spread each row over a group of
+// lanes so that the few rows still fill the SMs. OA_AMG_LANES_BIG overrides
+// the choice for long rows on large levels.
+static int lanes_for(double avg, long long rows) {
+  if (rows >= 100000) {
+    if (avg <= 16.0) return 1;
+    static const int big = [] {
+      const char* e = std::getenv("OA_AMG_LANES_BIG");
+      const int v = e ? std::atoi(e) : 0;
+      return (v == 1 || v == 4 || v == 8 || v == 32) ? v : 0;
+    }();
+    if (big) return big;
+    return 8;
+  }
+  return avg <= 4.0 ? 1 : (avg <= 24.0 ? 8 : 32);
+}
 
 static unsigned grid_for(long long rows, int lpr) { return (unsigned)((rows * lpr + AB - 1) / AB); }
 
@@ -65,7 +82,7 @@ int Amg<T>::setup(int n, const int* h_rp, const int* h_cols, const int* h_diag, 
     int s;
     if ((s = dalloc(&lv.dinv, cur)) || (s = dalloc(&lv.r, cur)) || (s = dalloc(&lv.t, cur))) return s;
     if (lev > 0 && ((s = dalloc(&lv.x, cur)) || (s = dalloc(&lv.b, cur)))) return s;
-    lv.lpr_a = lanes_for(double(lv.nnz) / std::max(1, cur));
+    lv.lpr_a = lanes_for(double(lv.nnz) / std::max(1, cur), cur);
     const bool last = cur <= COARSE_MAX || lev >= 14;
     if (last) {
       L.push_back(lv);
@@ -81,10 +98,10 @@ int Amg<T>::setup(int n, const int* h_rp, const int* h_cols, const int* h_diag, 
       if (nc >= cur) return fail(OA_ERR_SOLVER, "AMG: aggregation made no progress");
       lv.nnz_t = H.trp[cur];
       lv.nnz_p = H.prp[cur];
-      lv.lpr_p = lanes_for(double(lv.nnz_p) / cur);
-      lv.lpr_pt = lanes_for(double(lv.nnz_p) / H.nc);
-      lv.lpr_t = lanes_for(double(H.tta.size()) / std::max(1, lv.nnz_t));
-      lv.lpr_c = lanes_for(double(H.ctp.size()) / std::max(1, H.crp[H.nc]));
+      lv.lpr_p = lanes_for(double(lv.nnz_p) / cur, cur);
+      lv.lpr_pt = lanes_for(double(lv.nnz_p) / H.nc, H.nc);
+      lv.lpr_t = lanes_for(double(H.tta.size()) / std::max(1, lv.nnz_t), lv.nnz_t);
+      lv.lpr_c = lanes_for(double(H.ctp.size()) / std::max(1, H.crp[H.nc]), H.crp[H.nc]);
       if ((s = upload(&lv.p_rp, H.prp)) || (s = upload(&lv.p_cols, H.pcols)) || (s = upload(&lv.p_diag, H.pdiag)) ||
           (s = upload(&lv.pg_ptr, H.pgptr)) || (s = upload(&lv.pg_list, H.pglist)) ||
           (s = upload(&lv.pt_rp, H.ptrp)) || (s = upload(&lv.pt_rows, H.ptrows)) || (s = upload(&lv.pt_src, H.ptsrc)) ||
@@ -309,28 +326,33 @@ __global__ void __launch_bounds__(AB) k_up(int n, const int* __restrict__ rp, co
 }
 
 template <class T>
-__global__ void k_dense_apply(int n, const double* __restrict__ M, const T* __restrict__ b, T* __restrict__ x,
-                              const int* done) {
+__global__ void __launch_bounds__(AB) k_dense_apply(int n, const double* __restrict__ M, const T* __restrict__ b,
+                                                    T* __restrict__ x, const int* done) {
   if (*done) return;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const double* row = M + (size_t)i * 2 * n + n;
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = g / 32, lane = g % 32;  // one warp per row of the coarsest inverse
   double s = 0.0;
-  for (int j = 0; j < n; ++j) s += row[j] * double(b[j]);
-  x[i] = T(s);
+  if (i < n) {
+    const double* row = M + (size_t)i * 2 * n + n;
+    for (int j = lane; j < n; j += 32) s += row[j] * double(b[j]);
+  }
+  s = group_sum<32>(s);
+  if (i < n && lane == 0) x[i] = T(s);
 }
 
-// Smoothed prolongation, row parallel: P_iJ = [J == agg(i)] - wp Dinv_i
-// sum of the row's A entries whose column lies in aggregate J.
-template <class T>
-__global__ void k_sa_prolongator(int n, const int* __restrict__ p_rp, const int* __restrict__ p_diag,
-                                 const int* __restrict__ pg_ptr, const int* __restrict__ pg_list,
-                                 const T* __restrict__ A, const T* __restrict__ dinv, double wp, T* __restrict__ pv) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+// Smoothed prolongation: P_iJ = [J == agg(i)] - wp Dinv_i sum of the row's A
+// entries whose column lies in aggregate J; LPR lanes share a row's entries.
+template <class T, int LPR>
+__global__ void __launch_bounds__(AB) k_sa_prolongator(int n, const int* __restrict__ p_rp,
+                                                       const int* __restrict__ p_diag, const int* __restrict__ pg_ptr,
+                                                       const int* __restrict__ pg_list, const T* __restrict__ A,
+                                                       const T* __restrict__ dinv, double wp, T* __restrict__ pv) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = g / LPR, lane = g % LPR;
   if (i >= n) return;
   const double di = double(dinv[i]);
   const int e0 = p_rp[i];
-  for (int e = e0; e < p_rp[i + 1]; ++e) {
+  for (int e = e0 + lane; e < p_rp[i + 1]; e += LPR) {
     double s = 0.0;
     for (int q = pg_ptr[e]; q < pg_ptr[e + 1]; ++q) s += double(A[pg_list[q]]);
     pv[e] = T((e - e0 == p_diag[i] ? 1.0 : 0.0) - wp * di * s);
@@ -410,6 +432,8 @@ __global__ void __launch_bounds__(AB) k_post_smooth(int n, const int* __restrict
   do {                                                                                        \
     if ((lpr) == 1)                                                                           \
       kernel<T, 1><<<grid_for(rows, 1), AB, 0, st>>>(__VA_ARGS__);                            \
+    else if ((lpr) == 4)                                                                      \
+      kernel<T, 4><<<grid_for(rows, 4), AB, 0, st>>>(__VA_ARGS__);                            \
     else if ((lpr) == 8)                                                                      \
       kernel<T, 8><<<grid_for(rows, 8), AB, 0, st>>>(__VA_ARGS__);                            \
     else                                                                                      \
@@ -428,8 +452,8 @@ int Amg<T>::numeric(const T* A_fine, cudaStream_t st) {
     if (l + 1 < L.size()) {
       AmgLevel<T>& c = L[l + 1];
       if (smoothed) {
-        k_sa_prolongator<T><<<(v.n + AB - 1) / AB, AB, 0, st>>>(v.n, v.p_rp, v.p_diag, v.pg_ptr, v.pg_list, v.A,
-                                                                v.dinv, omega_p, v.pv);
+        OA_LPR_LAUNCH(v.lpr_p, k_sa_prolongator, T, v.n, st, v.n, v.p_rp, v.p_diag, v.pg_ptr, v.pg_list, v.A,
+                      v.dinv, omega_p, v.pv);
         k_gather<T><<<(v.nnz_p + AB - 1) / AB, AB, 0, st>>>(v.nnz_p, v.pt_src, v.pv, v.ptv);
         OA_LPR_LAUNCH(v.lpr_t, k_pair_sum, T, v.nnz_t, st, v.nnz_t, v.tt_ptr, v.tt_a, v.tt_p, v.A, v.pv, v.tv);
         OA_LPR_LAUNCH(v.lpr_c, k_pair_sum, T, c.nnz, st, c.nnz, v.ct_ptr, v.ct_p, v.ct_t, v.pv, v.tv, c.A);
@@ -457,7 +481,7 @@ int Amg<T>::apply(const T* v, T* z, const int* done, cudaStream_t st) {
     const T* b = l == 0 ? v : lv.b;
     if (l == nl - 1) {
       T* x = l == 0 ? z : lv.x;
-      k_dense_apply<T><<<(lv.n + AB - 1) / AB, AB, 0, st>>>(lv.n, dense_inv, b, x, done);
+      k_dense_apply<T><<<grid_for(lv.n, 32), AB, 0, st>>>(lv.n, dense_inv, b, x, done);
       break;
     }
     AmgLevel<T>& c = L[l + 1];
