@@ -30,6 +30,18 @@ sys.path.insert(0, ROOT)
 HBM_FALLBACK = 6650.0
 
 
+def max_over_ranks(value, device, world):
+    """The largest of every rank's value (time-like measurements are reported
+    as the slowest rank's); identity for one process."""
+    if world <= 1:
+        return value
+    import torch
+
+    t = torch.tensor([float(value)], device=device)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
 def measured_peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -153,10 +165,7 @@ def run_ours(args, rank, world):
         launches = rt.launch_count() - l0
         torch.cuda.synchronize()
         ms = e0.elapsed_time(e1)
-        if world > 1:
-            t = torch.tensor([ms], device=dev)
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-            ms = float(t.item())
+        ms = max_over_ranks(ms, dev, world)
         return ms, stats, launches
 
     # mixed form: headline
@@ -208,10 +217,7 @@ def run_ours(args, rank, world):
     e1.record(stream_e)
     e1.synchronize()
     ms_e2e = e0.elapsed_time(e1)
-    if world > 1:
-        t = torch.tensor([ms_e2e], device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms_e2e = float(t.item())
+    ms_e2e = max_over_ranks(ms_e2e, dev, world)
 
     peak, peak_kind = measured_peaks()
     alg = algorithmic_bytes_momentum(m.nn, m.ne, gm.nnz, True)
@@ -305,10 +311,7 @@ def run_conduction(args, rank, world):
             e1.synchronize()
             launches += rt.launch_count() - l0
             total += e0.elapsed_time(e1)
-        if world > 1:
-            t = torch.tensor([total], device=dev)
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-            total = float(t.item())
+        total = max_over_ranks(total, dev, world)
         return total, stats, launches
 
     dm = make(rt.OA_PREC_MIXED)
@@ -395,10 +398,7 @@ def run_batch(args, rank, world):
         e1.record(streams[0])
         e1.synchronize()
         ms = e0.elapsed_time(e1)
-        if world > 1:
-            t = torch.tensor([ms], device=dev)
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-            ms = float(t.item())
+        ms = max_over_ranks(ms, dev, world)
         return ms, rt.launch_count() - l0
 
     sb = [torch.cuda.ExternalStream(fb.stream_handle(), device=dev)]
@@ -517,14 +517,14 @@ def main():
             from openaccel_b200 import meshgen
 
             po.set_threads(threads)
-            mc, gam, src, _ = meshgen.conduction(args.cpu_n, sigma=1.0, seed=4242)
+            mc, gam, src, _ = meshgen.conduction(args.n, sigma=1.0, seed=4242)
             c = po.DiffCase(mc, gam, src, po.default_diff_settings(rtol=args.diff_rtol, maxit=20000))
             t0 = time.perf_counter()
             c.step()
             dt = time.perf_counter() - t0
             res["cpu_baseline"] = {"value": 1.0 / dt, "unit": "steps/s", "cores": threads, "kind": "port",
                                    "cpu": cpu_model(),
-                                   "sample": f"1 step of the {args.cpu_n}^3 x 6 conduction case, FP64 oracle "
+                                   "sample": f"1 step of the {args.n}^3 x 6 conduction case, FP64 oracle "
                                              "(Jacobi-BiCGStab), all host threads"}
         if rank == 0:
             print(json.dumps(res))

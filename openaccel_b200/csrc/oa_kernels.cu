@@ -402,7 +402,7 @@ __device__ __forceinline__ void wall_face(const MomArgs& a, const double (&x)[8]
 }
 
 template <bool USH, bool UGSH, class TF>
-__global__ void __launch_bounds__(BLOCK) k_momentum(MomArgs a) {
+__global__ void __launch_bounds__(BLOCK, sizeof(TF) == 4 ? 3 : 1) k_momentum(MomArgs a) {
   __shared__ TF sh_val[BLOCK * 3 * 9];
   __shared__ int sh_col[BLOCK * 3];
   const int lane = threadIdx.x & 31;
@@ -435,14 +435,20 @@ __global__ void __launch_bounds__(BLOCK) k_momentum(MomArgs a) {
       Uc[k][2] = TF(u[2]);
       mu[k] = TF(__ldg(a.mu + nd[k]));
     }
-    Corner0Points P;
-    corner0_points(x, P);
-    double Aq[3][3];
-    corner0_areas(P, Aq[0], Aq[1], Aq[2]);
     int err = 0;
     StaticFor<0, 3>::run([&](auto qc) {
       constexpr int q = decltype(qc)::value;
       constexpr int IP = q == 0 ? 0 : (q == 1 ? 3 : 8);
+      // this ip's SCS area, recomputed from the corner points (keeps fewer
+      // values live across the ip loop)
+      double Aip[3];
+      {
+        Corner0Points P;
+        corner0_points(x, P);
+        if (q == 0) quad_area(P.fF, P.m01, P.fB, P.cen, Aip);
+        if (q == 1) quad_area(P.m03, P.fL, P.cen, P.fB, Aip);
+        if (q == 2) quad_area(P.m04, P.fF, P.cen, P.fL, Aip);
+      }
       constexpr int R = q == 0 ? 1 : (q == 1 ? 3 : 4);
       constexpr int RS = nb_slot(R);
       using PG = ScsPt<IP, UGSH>;
@@ -468,7 +474,7 @@ __global__ void __launch_bounds__(BLOCK) k_momentum(MomArgs a) {
       }
       // viscous stress incl. transpose
       const InvJac J = inv_jacobian<PG>(x, &err);
-      TF ax[3] = {TF(Aq[q][0]), TF(Aq[q][1]), TF(Aq[q][2])};
+      TF ax[3] = {TF(Aip[0]), TF(Aip[1]), TF(Aip[2])};
       StaticFor<0, 8>::run([&](auto nc) {
         constexpr int n = decltype(nc)::value;
         if (!grad_is_zero<PG, n>()) {
