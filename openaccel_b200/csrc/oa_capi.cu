@@ -257,6 +257,7 @@ int oa_mesh_create(const double* coords, int nn, const int* conn, int ne, int to
   if ((st = dalloc(&m.x, 3L * nn)) || (st = dalloc(&m.conn, 8L * ne)) || (st = dalloc(&m.n2e, 8L * nn)) ||
       (st = dalloc(&m.row_ptr, nn + 1L)) || (st = dalloc(&m.cols, (size_t)m.nnz)) || (st = dalloc(&m.diag, (size_t)nn)) ||
       (st = dalloc(&m.face_mask, (size_t)ne)) || (st = dalloc(&m.vol, (size_t)nn)) || (st = dalloc(&m.wscv, 8L * ne)) ||
+      (st = dalloc(&m.scs_area, 36L * ne)) ||
       (st = dalloc(&m.wall_node, (size_t)nn))) {
     oa_mesh_destroy(M);
     return st;
@@ -288,7 +289,8 @@ void oa_mesh_destroy(oa_mesh* M) {
   if (!M) return;
   DeviceMesh& m = M->m;
   void* ptrs[] = {m.x,       m.conn,      m.n2e,      m.n2e_ptr,  m.n2f,       m.n2f_ptr, m.face_elem, m.face_ord,
-                  m.face_bnd, m.row_ptr, m.cols,     m.diag,     m.face_mask, m.vol,     m.wscv,      m.wall_node};
+                  m.face_bnd, m.row_ptr, m.cols,     m.diag,     m.face_mask, m.vol,     m.wscv,      m.wall_node,
+                  m.scs_area};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (M->st) cudaStreamDestroy(M->st);

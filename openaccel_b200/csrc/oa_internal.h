@@ -34,6 +34,7 @@ struct MeshView {
   uint8_t* face_mask = nullptr;  // [ne] bit f: face f is a no-slip wall face
   double* vol = nullptr;       // [nn] dual nodal volume
   double* wscv = nullptr;      // [ne][8] SCV volume fractions (hex8)
+  double* scs_area = nullptr;  // [ne][12][3] SCS area vectors, L -> R (hex8)
   int* wall_node = nullptr;    // [nn] 1 on wall nodes
 };
 

@@ -36,6 +36,16 @@ __device__ __forceinline__ void load3(const double* __restrict__ p, int n, doubl
   v[2] = __ldg(p + 3 * n + 2);
 }
 
+// SCS area vector of the ip packed in an ip word entry (original ip << 1 |
+// sign), from the per-element table, pointing away from the lane's corner.
+__device__ __forceinline__ void load_area(const MeshView& m, int e, int pk, double (&A)[3]) {
+  const double* a = m.scs_area + 36L * e + 3 * (pk >> 1);
+  const double sg = (pk & 1) ? -1.0 : 1.0;
+  A[0] = sg * __ldg(a);
+  A[1] = sg * __ldg(a + 1);
+  A[2] = sg * __ldg(a + 2);
+}
+
 // ---------------------------------------------------------------------------
 // Geometry precompute (FP64, once per mesh)
 
@@ -112,7 +122,10 @@ __global__ void __launch_bounds__(BLOCK) k_dual_volume(GeoArgs a) {
   if (rv && c == 0) a.m.vol[row] = v;
 }
 
+int launch_scs_area(DeviceMesh& m, cudaStream_t st);
+
 int launch_geometry(DeviceMesh& m, cudaStream_t st) {
+  if (int s = launch_scs_area(m, st)) return s;
   GeoArgs a{m.view(), nullptr, nullptr};
   OA_CUDA(cudaMallocAsync(&a.scv, sizeof(double) * 8 * (size_t)m.ne, st));
   OA_CUDA(cudaMallocAsync(&a.err, sizeof(int), st));
@@ -193,7 +206,7 @@ struct PcArgs {
 };
 
 template <bool USH, bool PGSH, class TF>
-__global__ void __launch_bounds__(BLOCK) k_pcorr(PcArgs a) {
+__global__ void __launch_bounds__(BLOCK, 4) k_pcorr(PcArgs a) {
   __shared__ TF sh_val[BLOCK * 3];
   __shared__ int sh_col[BLOCK * 3];
   const int lane = threadIdx.x & 31;
@@ -212,10 +225,9 @@ __global__ void __launch_bounds__(BLOCK) k_pcorr(PcArgs a) {
     double x[8][3];
     int nd[8];
     gather_x(a.m, e, pw, x, nd);
-    Corner0Points P;
-    corner0_points(x, P);
     double Aq[3][3];
-    corner0_areas(P, Aq[0], Aq[1], Aq[2]);
+#pragma unroll
+    for (int q = 0; q < 3; ++q) load_area(a.m, e, (iw >> (5 * q)) & 31, Aq[q]);
     // element-centre pressure gradient by SCV volume fractions
     double Gp[3] = {0.0, 0.0, 0.0};
     double pn[8];
@@ -439,16 +451,9 @@ __global__ void __launch_bounds__(BLOCK, sizeof(TF) == 4 ? 3 : 1) k_momentum(Mom
     StaticFor<0, 3>::run([&](auto qc) {
       constexpr int q = decltype(qc)::value;
       constexpr int IP = q == 0 ? 0 : (q == 1 ? 3 : 8);
-      // this ip's SCS area, recomputed from the corner points (keeps fewer
-      // values live across the ip loop)
+      // this ip's SCS area from the static per-element table
       double Aip[3];
-      {
-        Corner0Points P;
-        corner0_points(x, P);
-        if (q == 0) quad_area(P.fF, P.m01, P.fB, P.cen, Aip);
-        if (q == 1) quad_area(P.m03, P.fL, P.cen, P.fB, Aip);
-        if (q == 2) quad_area(P.m04, P.fF, P.cen, P.fL, Aip);
-      }
+      load_area(a.m, e, (iw >> (5 * q)) & 31, Aip);
       constexpr int R = q == 0 ? 1 : (q == 1 ? 3 : 4);
       constexpr int RS = nb_slot(R);
       using PG = ScsPt<IP, UGSH>;
@@ -600,17 +605,44 @@ __device__ __forceinline__ void scs_areas_all(const double (&x)[8][3], double (&
   for (int ip = 0; ip < 12; ++ip) quad_area(p[Q[ip][0]], p[Q[ip][1]], p[Q[ip][2]], p[Q[ip][3]], A[ip]);
 }
 
+// Static SCS area table [ne][12][3] (hex_scs_det; the mesh does not move), read
+// by the assembly, mass-flow and gradient kernels instead of recomputing the
+// element subdivision in every lane.
+__global__ void __launch_bounds__(BLOCK) k_scs_area(MeshView m) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= m.ne) return;
+  double x[8][3];
+  int nd[8];
+  gather_x(m, e, perm_word(0), x, nd);
+  double A[12][3];
+  scs_areas_all(x, A);
+#pragma unroll
+  for (int ip = 0; ip < 12; ++ip)
+#pragma unroll
+    for (int k = 0; k < 3; ++k) m.scs_area[36L * e + 3 * ip + k] = A[ip][k];
+}
+
+int launch_scs_area(DeviceMesh& m, cudaStream_t st) {
+  k_scs_area<<<(m.ne + BLOCK - 1) / BLOCK, BLOCK, 0, st>>>(m.view());
+  count_launches(1);
+  OA_CUDA(cudaGetLastError());
+  return OA_OK;
+}
+
 // initializeMassFlowRateInterior_ (flowModel.cpp:3303-3470) when init != 0,
 // otherwise updateMassFlowRateInterior_ (flowModel.cpp:5272-5687).
 template <bool USH, bool PGSH>
-__global__ void __launch_bounds__(BLOCK) k_mdot(MdotArgs a) {
+__global__ void __launch_bounds__(BLOCK, 3) k_mdot(MdotArgs a) {
   const int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= a.m.ne) return;
   double x[8][3];
   int nd[8];
   gather_x(a.m, e, perm_word(0), x, nd);
   double A[12][3];
-  scs_areas_all(x, A);
+#pragma unroll
+  for (int ip = 0; ip < 12; ++ip)
+#pragma unroll
+    for (int k = 0; k < 3; ++k) A[ip][k] = __ldg(a.m.scs_area + 36L * e + 3 * ip + k);
   double Gp[3] = {0.0, 0.0, 0.0}, pn[8];
   if (!a.init) {
 #pragma unroll
@@ -735,10 +767,10 @@ __global__ void __launch_bounds__(BLOCK) k_gradient(GradArgs a) {
     for (int k = 0; k < 8; ++k)
 #pragma unroll
       for (int i = 0; i < NC; ++i) ph[k][i] = __ldg(a.phi + NC * nd[k] + i);
-    Corner0Points P;
-    corner0_points(x, P);
+    const uint32_t iw = ip_word(c);
     double Aq[3][3];
-    corner0_areas(P, Aq[0], Aq[1], Aq[2]);
+#pragma unroll
+    for (int q = 0; q < 3; ++q) load_area(a.m, e, (iw >> (5 * q)) & 31, Aq[q]);
     StaticFor<0, 3>::run([&](auto qc) {
       constexpr int q = decltype(qc)::value;
       constexpr int IP = q == 0 ? 0 : (q == 1 ? 3 : 8);

@@ -21,6 +21,7 @@ __global__ void k_narrow(int n, const double* __restrict__ a, float* __restrict_
 }  // namespace
 
 int ScalarSolve::init(int nn) {
+  if (const char* e = std::getenv("OA_AMG_REFRESH")) refresh = std::max(1, std::atoi(e));
   if (n == nn && r) return OA_OK;
   release();
   n = nn;
@@ -70,10 +71,13 @@ int ScalarSolve::solve(const ScalarGraph& g, bool mixed, bool amg, bool graphs, 
   }
   k64.use_graph = k32.use_graph = graphs;
   const int check_every = amg ? 5 : 20;
+  // AMG numeric phase every refresh-th solve (the fine matrix is always the
+  // current one; the coarse operators may lag by refresh - 1 assemblies)
+  const bool reuse = amg && refresh > 1 && (solves++ % refresh) != 0;
   if (!mixed) {
     if (int s = k64.setup(g.nn, g.rp, g.cols, g.diag, st)) return s;
     double* xs = nullptr;
-    if (int s = k64.solve<double>(static_cast<const double*>(A), b, xs, rtol, maxit, iters, res, check_every))
+    if (int s = k64.solve<double>(static_cast<const double*>(A), b, xs, rtol, maxit, iters, res, check_every, reuse))
       return s;
     OA_CUDA(cudaMemcpyAsync(x, xs, sizeof(double) * g.nn, cudaMemcpyDeviceToDevice, st));
     if (refinements) *refinements = 0;
@@ -99,7 +103,7 @@ int ScalarSolve::solve(const ScalarGraph& g, bool mixed, bool amg, bool graphs, 
     // inner tolerance: enough digits for FP32 without stalling
     const double inner = std::max(rtol / rel, amg ? 1e-4 : 2e-4);
     if (int s = k32.solve<float>(A32, r32, d, std::min(inner, 0.1), std::min(INNER_CAP, maxit - total), &it, &r_in,
-                                 check_every, nref > 0))
+                                 check_every, reuse || nref > 0))
       return s;
     total += it;
     // a diverged inner solve contributes nothing; the next pass restarts from

@@ -32,6 +32,8 @@ struct ScalarSolve {
   double* hscal = nullptr;  // [2] pinned
   double* partials = nullptr;
   int n = 0;
+  int refresh = 1;       // AMG numeric phase every refresh-th solve
+  long long solves = 0;
 
   int init(int n);
   // A: const double* (mixed = false) or const float* (mixed = true); b and x
