@@ -425,6 +425,59 @@ def run_batch(args, rank, world):
     }
 
 
+def run_sst(args, rank, world):
+    """Fused k-omega SST node kernel (turbulent viscosity, F1, production, k and
+    omega node terms) on the 256 x 96 x 96 channel's node count (2,418,113
+    nodes) with seeded fields in the ranges of that case; a step is one launch."""
+    import torch
+
+    from openaccel_b200 import runtime as rt
+
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
+    torch.cuda.set_device(dev)
+    nn = 257 * 97 * 97
+    rng = np.random.default_rng(3)
+    host = dict(k=1e-3 * np.exp(0.2 * rng.standard_normal(nn)), omega=1e2 * np.exp(0.2 * rng.standard_normal(nn)),
+                rho=np.ones(nn), mu=np.full(nn, 1e-5), ymin=rng.uniform(1e-5, 0.5, nn),
+                gradU=rng.normal(0, 10, 9 * nn), gradK=rng.normal(0, 1e-3, 3 * nn), gradW=rng.normal(0, 10, 3 * nn),
+                div=rng.normal(0, 1e-6, nn), vol=np.full(nn, 1.0 / nn), mut_old=np.zeros(nn))
+    host["k_prev"] = host["k"].copy()
+    d = {n: torch.from_numpy(v).to(dev) for n, v in host.items()}
+    d["wall_node"] = torch.from_numpy((rng.uniform(size=nn) < 0.02).astype(np.int32)).to(dev)
+    for n in rt.SST_OUTPUTS:
+        d[n] = torch.empty(nn, dtype=torch.float64, device=dev)
+    ptrs = {n: t.data_ptr() for n, t in d.items()}
+    stream = torch.cuda.current_stream(dev)
+    for _ in range(args.warmup):
+        rt.sst_node_update(nn, ptrs, stream=stream.cuda_stream)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    l0 = rt.launch_count()
+    with ClockSampler(dev.index) as clk:
+        e0.record(stream)
+        for _ in range(args.steps):
+            rt.sst_node_update(nn, ptrs, stream=stream.cuda_stream)
+        e1.record(stream)
+        e1.synchronize()
+    ms = max_over_ranks(e0.elapsed_time(e1), dev, world)
+    # algorithmic bytes: 9 scalars + grad U (9) + grad k (3) + grad omega (3)
+    # doubles and a wall flag in, 7 doubles out (no wall production supplied)
+    alg = nn * (8 * (9 + 9 + 3 + 3) + 4 + 8 * 7)
+    t = ms * 1e-3 / args.steps
+    peak, peak_kind = measured_peaks()
+    return {
+        "metric": "SST node updates per second (fused mu_t, F1, P_k, k/omega node terms)", "value": world / t,
+        "unit": "launches/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "SST node kernel, 257 x 97 x 97 nodes (256 x 96 x 96 channel)", "nodes": nn,
+                   "l2": "inputs larger than L2 (no flush)"},
+        "roofline": {"bound": "hbm", "kernel": "k_sst_nodes", "achieved": alg / t / 1e9, "peak": peak, "unit": "GB/s",
+                     "frac": alg / t / 1e9 / peak, "peak_kind": peak_kind, "algorithmic_bytes": alg,
+                     "traffic": traffic_from_profile("k_sst_nodes_channel256.md")},
+        "gpu_launches": rt.launch_count() - l0, "clocks": clk.summary(),
+    }
+
+
 def cpu_model():
     try:
         for line in open("/proc/cpuinfo"):
@@ -468,7 +521,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-graphs", action="store_true")
     ap.add_argument("--only-mixed", action="store_true", help="time the mixed form only (profiling)")
-    ap.add_argument("--workload", default="cavity", choices=["cavity", "conduction", "batch"],
+    ap.add_argument("--workload", default="cavity", choices=["cavity", "conduction", "batch", "sst"],
                     help="cavity: the headline SIMPLE workload; conduction: the tet4 diffusion case (--n 96); "
                          "batch: 64 independent cavities, batched mixed form against a loop over the FP64 form")
     ap.add_argument("--batch-count", type=int, default=64)
@@ -501,8 +554,8 @@ def main():
         import torch
 
         torch.distributed.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
-    if args.workload == "batch":
-        res = run_batch(args, rank, world)
+    if args.workload in ("batch", "sst"):
+        res = (run_batch if args.workload == "batch" else run_sst)(args, rank, world)
         if rank == 0:
             print(json.dumps(res))
         if world > 1:

@@ -22,6 +22,7 @@ __global__ void k_narrow(int n, const double* __restrict__ a, float* __restrict_
 
 int ScalarSolve::init(int nn) {
   if (const char* e = std::getenv("OA_AMG_REFRESH")) refresh = std::max(1, std::atoi(e));
+  if (const char* e = std::getenv("OA_IR_INNER")) inner_floor = std::atof(e);
   if (n == nn && r) return OA_OK;
   release();
   n = nn;
@@ -101,7 +102,7 @@ int ScalarSolve::solve(const ScalarGraph& g, bool mixed, bool amg, bool graphs, 
     int it = 0;
     double r_in = 0.0;
     // inner tolerance: enough digits for FP32 without stalling
-    const double inner = std::max(rtol / rel, amg ? 1e-4 : 2e-4);
+    const double inner = std::max(rtol / rel, inner_floor > 0 ? inner_floor : (amg ? 1e-4 : 2e-4));
     if (int s = k32.solve<float>(A32, r32, d, std::min(inner, 0.1), std::min(INNER_CAP, maxit - total), &it, &r_in,
                                  check_every, reuse || nref > 0))
       return s;

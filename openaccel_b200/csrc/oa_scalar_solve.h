@@ -32,7 +32,15 @@ struct ScalarSolve {
   double* hscal = nullptr;  // [2] pinned
   double* partials = nullptr;
   int n = 0;
-  int refresh = 1;       // AMG numeric phase every refresh-th solve
+  // AMG numeric phase (coarse operators, prolongation, inverse diagonals)
+  // every refresh-th solve; between refreshes the fine matrix is the current
+  // one and only the coarse operators lag (on the 128^3 cavity 4 keeps the
+  // iteration counts and saves 5 % of the outer iteration; OA_AMG_REFRESH
+  // overrides)
+  int refresh = 4;
+  // lowest relative tolerance asked of an FP32 inner solve (0: 1e-4 with AMG,
+  // 2e-4 with Jacobi); OA_IR_INNER overrides
+  double inner_floor = 0.0;
   long long solves = 0;
 
   int init(int n);
