@@ -133,14 +133,19 @@ __host__ __device__ constexpr double dshape(int n, int d, double s1, double s2, 
 // Inverse-Jacobian rows at a parametric point: ds_k/dx_i stored as
 // inv[k][i]; returns det(J). Same algebra and singular-Jacobian guard as
 // hex_gradient_operator (det <= 1e6*realmin -> treated as 1, flag raised).
-struct InvJac {
-  double s[3][3];  // s[k][i] = d s_k / d x_i
-  double det;
+// Inverse Jacobian at a point, in the arithmetic type R (FP64 everywhere but
+// the mixed form's momentum fluxes, which use FP32 on element-local
+// coordinates).
+template <class R>
+struct InvJacR {
+  R s[3][3];  // s[k][i] = d s_k / d x_i
+  R det;
 };
+using InvJac = InvJacR<double>;
 
-template <class PT>
-__device__ __forceinline__ InvJac inv_jacobian(const double (&x)[8][3], int* err) {
-  double J[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};  // J[i][d] = dx_i/ds_d
+template <class PT, class R = double>
+__device__ __forceinline__ InvJacR<R> inv_jacobian(const R (&x)[8][3], int* err) {
+  R J[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};  // J[i][d] = dx_i/ds_d
 #pragma unroll
   for (int n = 0; n < 8; ++n) {
 #pragma unroll
@@ -148,22 +153,23 @@ __device__ __forceinline__ InvJac inv_jacobian(const double (&x)[8][3], int* err
       const double v = dshape(n, d, PT::s(0), PT::s(1), PT::s(2));
       if (v != 0.0) {
 #pragma unroll
-        for (int i = 0; i < 3; ++i) J[i][d] += v * x[n][i];
+        for (int i = 0; i < 3; ++i) J[i][d] += R(v) * x[n][i];
       }
     }
   }
-  const double xs1 = J[0][0], xs2 = J[0][1], xs3 = J[0][2];
-  const double ys1 = J[1][0], ys2 = J[1][1], ys3 = J[1][2];
-  const double zs1 = J[2][0], zs2 = J[2][1], zs3 = J[2][2];
-  InvJac r;
-  r.det = xs1 * (ys2 * zs3 - zs2 * ys3) + ys1 * (zs2 * xs3 - xs2 * zs3) +
-          zs1 * (xs2 * ys3 - ys2 * xs3);
-  double t = r.det;
-  if (t <= 1.0e6 * 2.2250738585072014e-308) {
-    t = 1.0;
+  const R xs1 = J[0][0], xs2 = J[0][1], xs3 = J[0][2];
+  const R ys1 = J[1][0], ys2 = J[1][1], ys3 = J[1][2];
+  const R zs1 = J[2][0], zs2 = J[2][1], zs3 = J[2][2];
+  InvJacR<R> r;
+  r.det = xs1 * (ys2 * zs3 - zs2 * ys3) + ys1 * (zs2 * xs3 - xs2 * zs3) + zs1 * (xs2 * ys3 - ys2 * xs3);
+  R t = r.det;
+  // determinant guard of hex_gradient_operator: 1e6 times the smallest normal
+  // number of the arithmetic type
+  if (t <= R(1.0e6) * (sizeof(R) == 4 ? R(1.1754943508222875e-38) : R(2.2250738585072014e-308))) {
+    t = R(1);
     *err = 1;
   }
-  const double d = 1.0 / t;
+  const R d = R(1) / t;
   r.s[0][0] = d * (ys2 * zs3 - zs2 * ys3);
   r.s[1][0] = d * (zs1 * ys3 - ys1 * zs3);
   r.s[2][0] = d * (ys1 * zs2 - zs1 * ys2);
@@ -177,17 +183,17 @@ __device__ __forceinline__ InvJac inv_jacobian(const double (&x)[8][3], int* err
 }
 
 // Physical gradient of N_n at the point PT: g_i = sum_k dN_n/ds_k * ds_k/dx_i.
-template <class PT, int N>
-__device__ __forceinline__ void grad_n(const InvJac& J, double g[3]) {
+template <class PT, int N, class R = double>
+__device__ __forceinline__ void grad_n(const InvJacR<R>& J, R g[3]) {
   constexpr double d0 = dshape(N, 0, PT::s(0), PT::s(1), PT::s(2));
   constexpr double d1 = dshape(N, 1, PT::s(0), PT::s(1), PT::s(2));
   constexpr double d2 = dshape(N, 2, PT::s(0), PT::s(1), PT::s(2));
 #pragma unroll
   for (int i = 0; i < 3; ++i) {
-    double v = 0.0;
-    if (d0 != 0.0) v += d0 * J.s[0][i];
-    if (d1 != 0.0) v += d1 * J.s[1][i];
-    if (d2 != 0.0) v += d2 * J.s[2][i];
+    R v = R(0);
+    if (d0 != 0.0) v += R(d0) * J.s[0][i];
+    if (d1 != 0.0) v += R(d1) * J.s[1][i];
+    if (d2 != 0.0) v += R(d2) * J.s[2][i];
     g[i] = v;
   }
 }
@@ -250,21 +256,20 @@ __device__ __forceinline__ void corner0_areas(const Corner0Points& p, double A0[
 
 // Exposed-face sub-area at face node 0 of a quad whose nodes are listed
 // cyclically starting at corner 0 (quad3d_scs_det, first sub-face).
-__device__ __forceinline__ void face_area_at_first(const double* p0, const double* p1,
-                                                   const double* p2, const double* p3,
-                                                   double A[3]) {
-  double e0[3], e3[3], c[3];
+template <class R>
+__device__ __forceinline__ void face_area_at_first(const R* p0, const R* p1, const R* p2, const R* p3, R A[3]) {
+  R e0[3], e3[3], c[3];
 #pragma unroll
   for (int k = 0; k < 3; ++k) {
-    e0[k] = (p0[k] + p1[k]) * 0.5;
-    e3[k] = (p3[k] + p0[k]) * 0.5;
-    c[k] = (p0[k] + p1[k] + p2[k] + p3[k]) * 0.25;
+    e0[k] = (p0[k] + p1[k]) * R(0.5);
+    e3[k] = (p3[k] + p0[k]) * R(0.5);
+    c[k] = (p0[k] + p1[k] + p2[k] + p3[k]) * R(0.25);
   }
-  const double d13x = c[0] - p0[0], d13y = c[1] - p0[1], d13z = c[2] - p0[2];
-  const double d24x = e3[0] - e0[0], d24y = e3[1] - e0[1], d24z = e3[2] - e0[2];
-  A[0] = 0.5 * (d24z * d13y - d13z * d24y);
-  A[1] = 0.5 * (d24x * d13z - d13x * d24z);
-  A[2] = 0.5 * (d24y * d13x - d13y * d24x);
+  const R d13x = c[0] - p0[0], d13y = c[1] - p0[1], d13z = c[2] - p0[2];
+  const R d24x = e3[0] - e0[0], d24y = e3[1] - e0[1], d24z = e3[2] - e0[2];
+  A[0] = R(0.5) * (d24z * d13y - d13z * d24y);
+  A[1] = R(0.5) * (d24x * d13z - d13x * d24z);
+  A[2] = R(0.5) * (d24y * d13x - d13y * d24x);
 }
 
 }  // namespace hex8

@@ -334,14 +334,14 @@ struct MomArgs {
 // Zero-normal-stress wall term at the exposed ip of canonical face FC nearest
 // corner 0 (IP_ZERO_NORMAL_STRESS_FIXED_VEL__).
 template <int FC, bool USH, bool UGSH, class TF>
-__device__ __forceinline__ void wall_face(const MomArgs& a, const double (&x)[8][3], const int (&nd)[8],
+__device__ __forceinline__ void wall_face(const MomArgs& a, const TF (&x)[8][3], const int (&nd)[8],
                                           const TF (&Uc)[8][3], const TF (&mu)[8], TF (&diag)[9],
                                           TF (&nb)[3][9], TF (&rhs)[3], int* err) {
   constexpr int f0 = face_node(FC, 0), f1 = face_node(FC, 1), f2 = face_node(FC, 2), f3 = face_node(FC, 3);
-  double Af[3];
-  face_area_at_first(x[f0], x[f1], x[f2], x[f3], Af);
+  TF Af[3];
+  face_area_at_first<TF>(x[f0], x[f1], x[f2], x[f3], Af);
   using PT = FacePt<FC, 0, UGSH>;
-  const InvJac J = inv_jacobian<PT>(x, err);
+  const InvJacR<TF> J = inv_jacobian<PT, TF>(x, err);
   // face-node velocities replaced by the wall (node-side) values
   TF Ue[8][3];
 #pragma unroll
@@ -362,21 +362,20 @@ __device__ __forceinline__ void wall_face(const MomArgs& a, const double (&x)[8]
   } else {
     muB = TF(0.5625) * mu[f0] + TF(0.1875) * mu[f1] + TF(0.0625) * mu[f2] + TF(0.1875) * mu[f3];
   }
-  const double amag = sqrt(Af[0] * Af[0] + Af[1] * Af[1] + Af[2] * Af[2]);
+  const TF amag = sqrt(Af[0] * Af[0] + Af[1] * Af[1] + Af[2] * Af[2]);
   TF nx[3], ax[3];
 #pragma unroll
   for (int i = 0; i < 3; ++i) {
-    nx[i] = TF(Af[i] / amag);
-    ax[i] = TF(Af[i]);
+    nx[i] = Af[i] / amag;
+    ax[i] = Af[i];
   }
   StaticFor<0, 8>::run([&](auto nc) {
     constexpr int n = decltype(nc)::value;
     if (!grad_is_zero<PT, n>()) {
       constexpr bool on_face = (n == f0 || n == f1 || n == f2 || n == f3);
       constexpr int sl = nb_slot(n);
-      double gd[3];
-      grad_n<PT, n>(J, gd);
-      TF g[3] = {TF(gd[0]), TF(gd[1]), TF(gd[2])};
+      TF g[3];
+      grad_n<PT, n, TF>(J, g);
 #pragma unroll
       for (int j = 0; j < 3; ++j) {
 #pragma unroll
@@ -414,7 +413,7 @@ __device__ __forceinline__ void wall_face(const MomArgs& a, const double (&x)[8]
 }
 
 template <bool USH, bool UGSH, class TF>
-__global__ void __launch_bounds__(BLOCK, sizeof(TF) == 4 ? 3 : 1) k_momentum(MomArgs a) {
+__global__ void __launch_bounds__(BLOCK, sizeof(TF) == 4 ? (UGSH ? 4 : 3) : 1) k_momentum(MomArgs a) {
   __shared__ TF sh_val[BLOCK * 3 * 9];
   __shared__ int sh_col[BLOCK * 3];
   const int lane = threadIdx.x & 31;
@@ -434,9 +433,16 @@ __global__ void __launch_bounds__(BLOCK, sizeof(TF) == 4 ? 3 : 1) k_momentum(Mom
   if (e >= 0) {
     const uint32_t pw = perm_word(c);
     const uint32_t iw = ip_word(c);
-    double x[8][3];
+    double xg[8][3];
     int nd[8];
-    gather_x(a.m, e, pw, x, nd);
+    gather_x(a.m, e, pw, xg, nd);
+    // coordinates of the flux arithmetic: FP64 as gathered, or FP32 relative
+    // to corner 0 in the mixed form (the Jacobians are translation invariant)
+    TF x[8][3];
+#pragma unroll
+    for (int k = 0; k < 8; ++k)
+#pragma unroll
+      for (int i = 0; i < 3; ++i) x[k][i] = sizeof(TF) == 4 ? TF(xg[k][i] - xg[0][i]) : TF(xg[k][i]);
     TF Uc[8][3], mu[8];
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
@@ -478,15 +484,14 @@ __global__ void __launch_bounds__(BLOCK, sizeof(TF) == 4 ? 3 : 1) k_momentum(Mom
         nb[RS][3 * i + i] += fr;
       }
       // viscous stress incl. transpose
-      const InvJac J = inv_jacobian<PG>(x, &err);
+      const InvJacR<TF> J = inv_jacobian<PG, TF>(x, &err);
       TF ax[3] = {TF(Aip[0]), TF(Aip[1]), TF(Aip[2])};
       StaticFor<0, 8>::run([&](auto nc) {
         constexpr int n = decltype(nc)::value;
         if (!grad_is_zero<PG, n>()) {
           constexpr int sl = nb_slot(n);
-          double gd[3];
-          grad_n<PG, n>(J, gd);
-          const TF g[3] = {TF(gd[0]), TF(gd[1]), TF(gd[2])};
+          TF g[3];
+          grad_n<PG, n, TF>(J, g);
 #pragma unroll
           for (int i = 0; i < 3; ++i) {
             TF lc = TF(0);
