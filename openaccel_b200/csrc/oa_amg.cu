@@ -66,7 +66,10 @@ int Amg<T>::setup(int n, const int* h_rp, const int* h_cols, const int* h_diag, 
   std::vector<int> rp(h_rp, h_rp + n + 1), cols(h_cols, h_cols + h_rp[n]), dg(h_diag, h_diag + n);
   int cur = n;
   for (int lev = 0;; ++lev) {
-    AmgLevel<T> lv;
+    // the level joins L before anything is allocated for it, so an error
+    // return leaves every allocation where release() finds it
+    L.emplace_back();
+    AmgLevel<T>& lv = L.back();
     lv.n = cur;
     lv.nnz = rp[cur];
     if (lev == 0) {
@@ -84,10 +87,7 @@ int Amg<T>::setup(int n, const int* h_rp, const int* h_cols, const int* h_diag, 
     if (lev > 0 && ((s = dalloc(&lv.x, cur)) || (s = dalloc(&lv.b, cur)))) return s;
     lv.lpr_a = lanes_for(double(lv.nnz) / std::max(1, cur), cur);
     const bool last = cur <= COARSE_MAX || lev >= 14;
-    if (last) {
-      L.push_back(lv);
-      break;
-    }
+    if (last) break;
     int nc = 0;
     std::vector<int> crp, ccols, cdg;
     if (smoothed) {
@@ -169,7 +169,6 @@ int Amg<T>::setup(int n, const int* h_rp, const int* h_cols, const int* h_diag, 
           (s = upload(&lv.gptr, gcnt)) || (s = upload(&lv.glist, glist)))
         return s;
     }
-    L.push_back(lv);
     rp.swap(crp);
     cols.swap(ccols);
     dg.swap(cdg);

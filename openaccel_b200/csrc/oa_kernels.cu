@@ -264,36 +264,45 @@ __global__ void __launch_bounds__(BLOCK, 4) k_pcorr(PcArgs a) {
           }
         }
       });
-      double g[8][3];
+      // grad p at the ip through the parametric gradient: dp = J^-T sum_n dN_n/ds p_n
+      double dps[3] = {0.0, 0.0, 0.0};
       StaticFor<0, 8>::run([&](auto nc) {
         constexpr int n = decltype(nc)::value;
-        grad_n<PG, n>(J, g[n]);
-        if (!grad_is_zero<PG, n>()) {
-#pragma unroll
-          for (int j = 0; j < 3; ++j) dp[j] += g[n][j] * pn[n];
-        }
+        constexpr double d0 = dshape(n, 0, PG::s(0), PG::s(1), PG::s(2));
+        constexpr double d1 = dshape(n, 1, PG::s(0), PG::s(1), PG::s(2));
+        constexpr double d2 = dshape(n, 2, PG::s(0), PG::s(1), PG::s(2));
+        if (d0 != 0.0) dps[0] += d0 * pn[n];
+        if (d1 != 0.0) dps[1] += d1 * pn[n];
+        if (d2 != 0.0) dps[2] += d2 * pn[n];
       });
+#pragma unroll
+      for (int i = 0; i < 3; ++i) dp[i] = J.s[0][i] * dps[0] + J.s[1][i] * dps[1] + J.s[2][i] * dps[2];
       const int pk = (iw >> (5 * q)) & 31;
       const double tm = (pk & 1) ? -__ldg(a.mDot + 12 * e + (pk >> 1)) : __ldg(a.mDot + 12 * e + (pk >> 1));
       const double rhoHR = tm > 0 ? rho0 : __ldg(a.rho + nd[R]);
-      // lhs: -rhoHR * D_ip . (grad N_n) A  (FP32 in the mixed form)
+      // lhs: -rhoHR * D_ip . (grad N_n) A (FP32 in the mixed form). Only the
+      // three edge neighbours keep their own columns; the diagonal takes every
+      // other column, which by the partition of unity (sum_n grad N_n = 0) is
+      // minus the sum of the neighbours' coefficients
       const TF rh = TF(rhoHR);
       TF dA[3];
 #pragma unroll
       for (int j = 0; j < 3; ++j) dA[j] = TF(duip[j]) * TF(Aq[q][j]);
-      StaticFor<0, 8>::run([&](auto nc) {
+      TF fsum = TF(0);
+      StaticFor<1, 5>::run([&](auto nc) {
         constexpr int n = decltype(nc)::value;
-        if (!grad_is_zero<PG, n>()) {
+        constexpr int sl = nb_slot(n);
+        if (sl >= 0 && !grad_is_zero<PG, n>()) {
+          double gd[3];
+          grad_n<PG, n>(J, gd);
           TF f = TF(0);
 #pragma unroll
-          for (int j = 0; j < 3; ++j) f += -rh * dA[j] * TF(g[n][j]);
-          constexpr int sl = nb_slot(n);
-          if (sl < 0)
-            diag[0] += f;
-          else
-            nb[sl][0] += f;
+          for (int j = 0; j < 3; ++j) f += -rh * dA[j] * TF(gd[j]);
+          nb[sl][0] += f;
+          fsum += f;
         }
       });
+      diag[0] -= fsum;
       double mm = 0.0;
 #pragma unroll
       for (int j = 0; j < 3; ++j) {
@@ -483,27 +492,52 @@ __global__ void __launch_bounds__(BLOCK, sizeof(TF) == 4 ? (UGSH ? 4 : 3) : 1) k
         diag[3 * i + i] += fl;
         nb[RS][3 * i + i] += fr;
       }
-      // viscous stress incl. transpose
+      // viscous stress incl. transpose. Block of column n:
+      //   -mu_ip (g_n . A) I - mu_ip A (x) g_n   (rows i, columns j: g_n,i A_j)
+      // Its defect contribution summed over the eight columns is
+      //   rhs += mu_ip (G A + G^T A), G = grad U at the ip,
+      // taken through the parametric gradient; only the three edge neighbours
+      // keep their own blocks, and the diagonal block, which takes every other
+      // column, is minus their sum (partition of unity: sum_n g_n = 0).
       const InvJacR<TF> J = inv_jacobian<PG, TF>(x, &err);
       TF ax[3] = {TF(Aip[0]), TF(Aip[1]), TF(Aip[2])};
+      TF Gs[3][3] = {{TF(0), TF(0), TF(0)}, {TF(0), TF(0), TF(0)}, {TF(0), TF(0), TF(0)}};
       StaticFor<0, 8>::run([&](auto nc) {
         constexpr int n = decltype(nc)::value;
-        if (!grad_is_zero<PG, n>()) {
-          constexpr int sl = nb_slot(n);
+        constexpr double d0 = dshape(n, 0, PG::s(0), PG::s(1), PG::s(2));
+        constexpr double d1 = dshape(n, 1, PG::s(0), PG::s(1), PG::s(2));
+        constexpr double d2 = dshape(n, 2, PG::s(0), PG::s(1), PG::s(2));
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+          if (d0 != 0.0) Gs[i][0] += TF(d0) * Uc[n][i];
+          if (d1 != 0.0) Gs[i][1] += TF(d1) * Uc[n][i];
+          if (d2 != 0.0) Gs[i][2] += TF(d2) * Uc[n][i];
+        }
+      });
+      TF G[3][3];
+#pragma unroll
+      for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) G[i][j] = Gs[i][0] * J.s[0][j] + Gs[i][1] * J.s[1][j] + Gs[i][2] * J.s[2][j];
+#pragma unroll
+      for (int i = 0; i < 3; ++i)
+        rhs[i] += muIp * (G[i][0] * ax[0] + G[i][1] * ax[1] + G[i][2] * ax[2] + G[0][i] * ax[0] + G[1][i] * ax[1] +
+                          G[2][i] * ax[2]);
+      StaticFor<1, 5>::run([&](auto nc) {
+        constexpr int n = decltype(nc)::value;
+        constexpr int sl = nb_slot(n);
+        if (sl >= 0 && !grad_is_zero<PG, n>()) {
           TF g[3];
           grad_n<PG, n, TF>(J, g);
+          const TF ga = g[0] * ax[0] + g[1] * ax[1] + g[2] * ax[2];
 #pragma unroll
           for (int i = 0; i < 3; ++i) {
-            TF lc = TF(0);
 #pragma unroll
             for (int j = 0; j < 3; ++j) {
-              lc += -muIp * g[j] * ax[j];
-              const TF fj = -muIp * g[i] * ax[j];
-              if (sl < 0) diag[3 * i + j] += fj; else nb[sl][3 * i + j] += fj;
-              rhs[i] -= fj * Uc[n][j];
+              const TF fj = -muIp * g[i] * ax[j] + (i == j ? -muIp * ga : TF(0));
+              nb[sl][3 * i + j] += fj;
+              diag[3 * i + j] -= fj;
             }
-            if (sl < 0) diag[3 * i + i] += lc; else nb[sl][3 * i + i] += lc;
-            rhs[i] -= lc * Uc[n][i];
           }
         }
       });
@@ -637,17 +671,12 @@ int launch_scs_area(DeviceMesh& m, cudaStream_t st) {
 // initializeMassFlowRateInterior_ (flowModel.cpp:3303-3470) when init != 0,
 // otherwise updateMassFlowRateInterior_ (flowModel.cpp:5272-5687).
 template <bool USH, bool PGSH>
-__global__ void __launch_bounds__(BLOCK, 3) k_mdot(MdotArgs a) {
+__global__ void __launch_bounds__(BLOCK, 4) k_mdot(MdotArgs a) {
   const int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= a.m.ne) return;
   double x[8][3];
   int nd[8];
   gather_x(a.m, e, perm_word(0), x, nd);
-  double A[12][3];
-#pragma unroll
-  for (int ip = 0; ip < 12; ++ip)
-#pragma unroll
-    for (int k = 0; k < 3; ++k) A[ip][k] = __ldg(a.m.scs_area + 36L * e + 3 * ip + k);
   double Gp[3] = {0.0, 0.0, 0.0}, pn[8];
   if (!a.init) {
 #pragma unroll
@@ -683,30 +712,37 @@ __global__ void __launch_bounds__(BLOCK, 3) k_mdot(MdotArgs a) {
         }
       }
     });
+    double Aip[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) Aip[k] = __ldg(a.m.scs_area + 36L * e + 3 * IP + k);
     double m = 0.0;
     if (a.init) {
 #pragma unroll
-      for (int j = 0; j < 3; ++j) m += rhoIp * u[j] * A[IP][j];
+      for (int j = 0; j < 3; ++j) m += rhoIp * u[j] * Aip[j];
       a.mDot[12 * e + IP] = m;
     } else {
       const InvJac J = inv_jacobian<PG>(x, &err);
-      double dp[3] = {0, 0, 0};
+      // grad p at the ip through the parametric gradient: dp = J^-T sum_n dN_n/ds p_n
+      double dps[3] = {0.0, 0.0, 0.0};
       StaticFor<0, 8>::run([&](auto nc) {
         constexpr int n = decltype(nc)::value;
-        if (!grad_is_zero<PG, n>()) {
-          double g[3];
-          grad_n<PG, n>(J, g);
-#pragma unroll
-          for (int j = 0; j < 3; ++j) dp[j] += g[j] * pn[n];
-        }
+        constexpr double d0 = dshape(n, 0, PG::s(0), PG::s(1), PG::s(2));
+        constexpr double d1 = dshape(n, 1, PG::s(0), PG::s(1), PG::s(2));
+        constexpr double d2 = dshape(n, 2, PG::s(0), PG::s(1), PG::s(2));
+        if (d0 != 0.0) dps[0] += d0 * pn[n];
+        if (d1 != 0.0) dps[1] += d1 * pn[n];
+        if (d2 != 0.0) dps[2] += d2 * pn[n];
       });
+      double dp[3];
+#pragma unroll
+      for (int i = 0; i < 3; ++i) dp[i] = J.s[0][i] * dps[0] + J.s[1][i] * dps[1] + J.s[2][i] * dps[2];
       const double old = a.mDot[12 * e + IP];
       const double tU = old / rhoIp;
       const double rhoUp = tU > 0 ? __ldg(a.rho + nd[lr(IP, 0)]) : __ldg(a.rho + nd[lr(IP, 1)]);
 #pragma unroll
       for (int j = 0; j < 3; ++j) {
-        m += rhoUp * u[j] * A[IP][j];
-        m -= rhoUp * duip[j] * (dp[j] - Gp[j]) * A[IP][j];
+        m += rhoUp * u[j] * Aip[j];
+        m -= rhoUp * duip[j] * (dp[j] - Gp[j]) * Aip[j];
       }
       a.mDot[12 * e + IP] = a.urf * m + (1.0 - a.urf) * old;
     }
