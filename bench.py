@@ -249,6 +249,8 @@ def run_ours(args, rank, world):
         "kernel_ms": {"momentum_mixed": t_mom, "pcorr_mixed": t_pc, "momentum_fp64": t_mom64,
                       "pcorr_fp64": t_pc64},
         "continuity_rms_last": {"mixed": st_mixed[-1]["continuity_rms"], "fp64": st_64[-1]["continuity_rms"]},
+        "phase_ms_per_step": {form: {k[3:]: float(np.mean([x[k] for x in st[-args.steps:]])) for k in rt.PHASES}
+                              for form, st in (("mixed", st_mixed), ("fp64", st_64))},
         "pc_iters_last": {"mixed": st_mixed[-1]["pc_iters"], "fp64": st_64[-1]["pc_iters"]},
         "roofline": {"bound": "hbm", "kernel": "k_momentum (mixed)", "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,

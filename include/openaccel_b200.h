@@ -60,6 +60,10 @@ typedef struct oa_iter_stats {
   int mom_iters, pc_iters, pc_refinements;
   double mom_res, pc_res;
   double continuity_rms;        /* RMS of the pressure-correction rhs before the solve */
+  /* device time of the iteration's phases in ms (CUDA events on the flow's
+   * stream), the counterpart of the reference's Profiler push/pop around
+   * assembly and solve (src/equation/linearSystem.h:452-454) */
+  double ms_momentum_assembly, ms_momentum_solve, ms_pcorr_assembly, ms_pcorr_solve, ms_corrections;
 } oa_iter_stats;
 
 /* Last error message of the calling thread ("" when none). */

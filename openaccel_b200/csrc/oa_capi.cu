@@ -11,6 +11,8 @@
 #include <string>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "oa_internal.h"
 #include "oa_krylov.h"
 #include "oa_scalar_solve.h"
@@ -521,27 +523,69 @@ int oa_simple_iterate(oa_flow* H, int n, oa_iter_stats* stats) {
   if (!H || n < 0) return fail(OA_ERR_ARG, "oa_simple_iterate: bad arguments");
   Flow& f = H->f;
   const bool mx = mixed(f);
-  for (int it = 0; it < n; ++it) {
+  // Phase boundaries (device time, recorded only when stats are asked for):
+  // momentum assembly | momentum solve | mass flow + pressure-correction
+  // assembly | pressure-correction solve | corrections and gradients. NVTX
+  // ranges name the same phases for profilers.
+  cudaEvent_t ev[6] = {};
+  if (stats)
+    for (auto& e : ev) OA_CUDA(cudaEventCreate(&e));
+  auto mark = [&](int k) {
+    if (stats) cudaEventRecord(ev[k], f.stream);
+  };
+  int s = OA_OK;
+  for (int it = 0; it < n && s == OA_OK; ++it) {
     oa_iter_stats st{};
-    int s;
+    nvtxRangePushA("oa_simple_iterate");
     // momentum predictor (navierStokesEquation::solve)
-    if ((s = launch_momentum(f, mx))) return s;
-    if ((s = solve_momentum(H, f.s.mom_rtol, f.s.mom_maxit, &st.mom_iters, &st.mom_res, true))) return s;
-    if ((s = launch_update_mdot(f))) return s;
+    mark(0);
+    nvtxRangePushA("momentum assembly");
+    s = launch_momentum(f, mx);
+    nvtxRangePop();
+    mark(1);
+    nvtxRangePushA("momentum solve");
+    if (!s) s = solve_momentum(H, f.s.mom_rtol, f.s.mom_maxit, &st.mom_iters, &st.mom_res, true);
+    nvtxRangePop();
+    mark(2);
     // pressure correction (pressureCorrectionEquation::solve)
-    if ((s = launch_pcorr(f, mx))) return s;
-    if ((s = continuity_rms(H, &st.continuity_rms))) return s;
-    if ((s = solve_pcorr(H, f.s.pc_rtol, f.s.pc_maxit, &st.pc_iters, &st.pc_res, &st.pc_refinements))) return s;
-    k_axpy<<<(f.mesh->nn + 255) / 256, 256, 0, f.stream>>>(f.mesh->nn, f.p, f.b.x_pc, f.s.urf_p);
-    count_launches(1);
+    nvtxRangePushA("mass flow and pressure-correction assembly");
+    if (!s) s = launch_update_mdot(f);
+    if (!s) s = launch_pcorr(f, mx);
+    if (!s) s = continuity_rms(H, &st.continuity_rms);
+    nvtxRangePop();
+    mark(3);
+    nvtxRangePushA("pressure-correction solve");
+    if (!s) s = solve_pcorr(H, f.s.pc_rtol, f.s.pc_maxit, &st.pc_iters, &st.pc_res, &st.pc_refinements);
+    nvtxRangePop();
+    mark(4);
     // corrections
-    if ((s = launch_update_mdot(f)) || (s = launch_div(f)) || (s = launch_axpy_du_gradp(f, +1.0)) ||
-        (s = launch_gradient(f, 0)) || (s = launch_axpy_du_gradp(f, -1.0)) || (s = launch_gradient(f, 1)))
-      return s;
-    if ((s = check_err_flag(f, "oa_simple_iterate"))) return s;
-    if (stats) stats[it] = st;
+    nvtxRangePushA("corrections and gradients");
+    if (!s) {
+      k_axpy<<<(f.mesh->nn + 255) / 256, 256, 0, f.stream>>>(f.mesh->nn, f.p, f.b.x_pc, f.s.urf_p);
+      count_launches(1);
+      if (!(s = launch_update_mdot(f)) && !(s = launch_div(f)) && !(s = launch_axpy_du_gradp(f, +1.0)) &&
+          !(s = launch_gradient(f, 0)) && !(s = launch_axpy_du_gradp(f, -1.0)))
+        s = launch_gradient(f, 1);
+    }
+    nvtxRangePop();
+    mark(5);
+    nvtxRangePop();
+    if (!s) s = check_err_flag(f, "oa_simple_iterate");  // synchronises the stream
+    if (!s && stats) {
+      float t[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
+      for (int k = 0; k < 5; ++k) cudaEventElapsedTime(&t[k], ev[k], ev[k + 1]);
+      st.ms_momentum_assembly = t[0];
+      st.ms_momentum_solve = t[1];
+      st.ms_pcorr_assembly = t[2];
+      st.ms_pcorr_solve = t[3];
+      st.ms_corrections = t[4];
+      stats[it] = st;
+    }
   }
-  return OA_OK;
+  if (stats)
+    for (auto& e : ev)
+      if (e) cudaEventDestroy(e);
+  return s;
 }
 
 int oa_flow_stream(oa_flow* H, void** stream) {

@@ -54,11 +54,14 @@ class FlowSettings(C.Structure):
     ]
 
 
+PHASES = ("ms_momentum_assembly", "ms_momentum_solve", "ms_pcorr_assembly", "ms_pcorr_solve", "ms_corrections")
+
+
 class IterStats(C.Structure):
     _fields_ = [
         ("mom_iters", C.c_int), ("pc_iters", C.c_int), ("pc_refinements", C.c_int),
         ("mom_res", C.c_double), ("pc_res", C.c_double), ("continuity_rms", C.c_double),
-    ]
+    ] + [(n, C.c_double) for n in PHASES]
 
 
 class DiffusionSettings(C.Structure):
@@ -302,7 +305,8 @@ class Flow:
         st = (IterStats * max(n, 1))()
         _check(lib().oa_simple_iterate(self.h, n, st))
         return [dict(mom_iters=s.mom_iters, pc_iters=s.pc_iters, pc_refinements=s.pc_refinements,
-                     mom_res=s.mom_res, pc_res=s.pc_res, continuity_rms=s.continuity_rms) for s in st[:n]]
+                     mom_res=s.mom_res, pc_res=s.pc_res, continuity_rms=s.continuity_rms,
+                     **{k: getattr(s, k) for k in PHASES}) for s in st[:n]]
 
     def sync(self):
         _check(lib().oa_flow_sync(self.h))
