@@ -13,6 +13,7 @@ namespace oa {
 
 constexpr int AB = 256;          // threads per block
 constexpr int COARSE_MAX = 256;  // coarsest level solved by a dense inverse
+constexpr int MAX_CHEB = 6;      // highest Chebyshev smoothing degree
 
 // Lanes per row of the row-parallel kernels (1, 4, 8 or 32): levels with many
 // rows keep one lane per row for short rows and take 8 for long ones (the
@@ -63,6 +64,12 @@ int Amg<T>::setup(int n, const int* h_rp, const int* h_cols, const int* h_diag, 
   if (const char* e = std::getenv("OA_AMG_OMEGA")) omega = std::atof(e);
   if (const char* e = std::getenv("OA_AMG_ALPHA")) alpha = std::atof(e);
   if (const char* e = std::getenv("OA_AMG_OMEGA_P")) omega_p = std::atof(e);
+  if (const char* e = std::getenv("OA_AMG_CHEB_DEGREE")) cheb_degree = std::atoi(e);
+  if (const char* e = std::getenv("OA_AMG_CHEB_ROWS")) cheb_rows = std::atoi(e);
+  if (const char* e = std::getenv("OA_AMG_CHEB_RATIO")) cheb_ratio = std::max(1.5, std::atof(e));
+  if (cheb_degree < 2 || !smoothed) cheb_degree = 0;
+  if (cheb_degree > MAX_CHEB) return fail(OA_ERR_ARG, "AMG: Chebyshev degree above the supported maximum");
+  cheb_launches = 0;
   std::vector<int> rp(h_rp, h_rp + n + 1), cols(h_cols, h_cols + h_rp[n]), dg(h_diag, h_diag + n);
   int cur = n;
   for (int lev = 0;; ++lev) {
@@ -88,6 +95,19 @@ int Amg<T>::setup(int n, const int* h_rp, const int* h_cols, const int* h_diag, 
     lv.lpr_a = lanes_for(double(lv.nnz) / std::max(1, cur), cur);
     const bool last = cur <= COARSE_MAX || lev >= 14;
     if (last) break;
+    // not on the finest level: its matrix is always the caller's current one,
+    // while the spectral estimate (like Dinv) is refreshed only with the
+    // hierarchy; a coarse level's matrix, Dinv and estimate come from the same
+    // numeric phase
+    if (cheb_degree >= 2 && lev > 0 && cur <= cheb_rows) {
+      lv.cheb = true;
+      if ((s = dalloc(&lv.cr, cur)) || (s = dalloc(&lv.cd0, cur)) || (s = dalloc(&lv.cd1, cur)) ||
+          (s = dalloc(&lv.lmax, 2)) || (s = dalloc(&lv.pw_a, (size_t)lv.nnz)) || (s = dalloc(&lv.pw_dinv, cur)) ||
+          (s = dalloc(&lv.pw_v, cur)) || (s = dalloc(&lv.pw_w, cur)) ||
+          (s = dalloc(&lv.pw_part, grid_for(cur, lv.lpr_a))))
+        return s;
+      cheb_launches += 2LL * (cheb_degree - 1);
+    }
     int nc = 0;
     std::vector<int> crp, ccols, cdg;
     if (smoothed) {
@@ -193,7 +213,8 @@ void Amg<T>::release() {
     if (v.own_A) cudaFree(v.A);
     void* p[] = {v.dinv,   v.agg,   v.mptr,   v.mlist, v.gptr,   v.glist, v.r,      v.t,    v.p_rp,
                  v.p_cols, v.p_diag, v.pg_ptr, v.pg_list, v.pv, v.ptv, v.pt_rp, v.pt_rows, v.pt_src, v.tv,
-                 v.tt_ptr, v.tt_a,   v.tt_p,   v.ct_ptr, v.ct_p, v.ct_t};
+                 v.tt_ptr, v.tt_a,   v.tt_p,   v.ct_ptr, v.ct_p, v.ct_t, v.cr,      v.cd0,  v.cd1,
+                 v.lmax,   v.pw_a,  v.pw_dinv, v.pw_v, v.pw_w,   v.pw_part};
     for (void* q : p)
       if (q) cudaFree(q);
     if (l > 0) {
@@ -217,6 +238,12 @@ __global__ void k_galerkin(int nnz_c, const int* __restrict__ gptr, const int* _
   double s = 0.0;
   for (int q = gptr[c]; q < gptr[c + 1]; ++q) s += double(Af[glist[q]]);
   Ac[c] = T(s);
+}
+
+template <class T>
+__global__ void k_widen(int n, const T* __restrict__ a, double* __restrict__ b) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) b[i] = double(a[i]);
 }
 
 template <class T>
@@ -427,6 +454,182 @@ __global__ void __launch_bounds__(AB) k_post_smooth(int n, const int* __restrict
   if (i < n && lane == 0) x[i] = T(double(t[i]) + w * double(dinv[i]) * (double(b[i]) - s));
 }
 
+// Chebyshev smoothing (Saad, Iterative Methods for Sparse Linear Systems,
+// 2nd ed., Algorithm 12.1, applied to Dinv A) over [lambda / ratio, lambda]:
+// with theta and delta the interval's centre and half width, sigma = theta /
+// delta and rho_0 = 1 / sigma, step k >= 1 takes rho_k = 1 / (2 sigma -
+// rho_{k-1}), r_k = r_{k-1} - Dinv A d_{k-1}, d_k = rho_k rho_{k-1} d_{k-1} +
+// (2 rho_k / delta) r_k and x += d_k, from r_0 = Dinv (b - A x), d_0 = r_0 /
+// theta. The step coefficients are formed from lambda by every thread.
+struct ChebStep {
+  double inv_theta, c1, c2;
+};
+
+__device__ __forceinline__ ChebStep cheb_step(double lmax, double ratio, int k) {
+  const double lmin = lmax / ratio, theta = 0.5 * (lmax + lmin), delta = 0.5 * (lmax - lmin);
+  const double sigma = theta / delta;
+  double rho = 1.0 / sigma, c1 = 0.0, c2 = 0.0;
+  for (int j = 1; j <= k; ++j) {
+    const double rho1 = 1.0 / (2.0 * sigma - rho);
+    c1 = rho1 * rho;
+    c2 = 2.0 * rho1 / delta;
+    rho = rho1;
+  }
+  return {1.0 / theta, c1, c2};
+}
+
+// Spectral radius of Dinv A by power iteration from a fixed pseudo-random
+// vector: POWER_STEPS products w = Dinv A (v / |v|), each followed by an
+// ordered reduction of |w|^2; the last |w|, times a safety factor of 1.1,
+// bounds the smoothing interval. State in est[]: est[0] = 1 / |v| of the
+// vector being multiplied, est[1] = the bound.
+constexpr int POWER_STEPS = 15;
+
+__global__ void k_power_init(int n, double* v, double* est) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) {
+    unsigned h = (unsigned)i * 2654435761u;
+    h ^= h >> 15;
+    h *= 2246822519u;
+    h ^= h >> 13;
+    v[i] = double(h) * (2.0 / 4294967296.0) - 1.0;
+  }
+  if (i == 0) est[0] = 1.0;
+}
+
+template <int LPR>
+__global__ void __launch_bounds__(AB) k_power_apply(int n, const int* __restrict__ rp, const int* __restrict__ cols,
+                                                    const double* __restrict__ Ad, const double* __restrict__ dinv,
+                                                    const double* __restrict__ v, const double* __restrict__ est,
+                                                    double* __restrict__ w, double* __restrict__ partials) {
+  __shared__ double sh[AB];
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = g / LPR, lane = g % LPR;
+  double s = 0.0;
+  if (i < n)
+    for (int k = rp[i] + lane; k < rp[i + 1]; k += LPR) s += Ad[k] * v[cols[k]];
+  s = group_sum<LPR>(s);
+  double q = 0.0;
+  if (i < n && lane == 0) {
+    const double wi = dinv[i] * s * est[0];
+    w[i] = wi;
+    q = wi * wi;
+  }
+  sh[threadIdx.x] = q;
+  __syncthreads();
+  for (int o = AB / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) partials[blockIdx.x] = sh[0];
+}
+
+__global__ void k_power_norm(int nb, const double* __restrict__ partials, double* est) {
+  __shared__ double sh[AB];
+  double s = 0.0;
+  for (int b = threadIdx.x; b < nb; b += AB) s += partials[b];
+  sh[threadIdx.x] = s;
+  __syncthreads();
+  for (int o = AB / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    const double nrm = sqrt(sh[0]);
+    est[0] = nrm > 0.0 ? 1.0 / nrm : 1.0;
+    est[1] = 1.1 * nrm;
+  }
+}
+
+// Pre-smoothing from a zero iterate, steps 0 and 1 together: d_0 = Dinv b /
+// theta (formed for the neighbours from b), r_1 = Dinv b - Dinv A d_0, d_1 and
+// x = d_0 + d_1.
+template <class T, int LPR>
+__global__ void __launch_bounds__(AB) k_cheb_first(int n, const int* __restrict__ rp, const int* __restrict__ cols,
+                                                   const T* __restrict__ A, const T* __restrict__ dinv,
+                                                   const T* __restrict__ b, const double* __restrict__ lmax,
+                                                   double ratio, T* __restrict__ cr, T* __restrict__ d1,
+                                                   T* __restrict__ x, const int* done) {
+  if (*done) return;
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = g / LPR, lane = g % LPR;
+  double s = 0.0;
+  if (i < n)
+    for (int k = rp[i] + lane; k < rp[i + 1]; k += LPR) s += double(A[k]) * (double(dinv[cols[k]]) * double(b[cols[k]]));
+  s = group_sum<LPR>(s);
+  if (i >= n || lane) return;
+  const ChebStep c = cheb_step(lmax[1], ratio, 1);
+  const double di = double(dinv[i]), db = di * double(b[i]);
+  const double r1 = db - di * s * c.inv_theta, d0 = db * c.inv_theta;
+  const double dn = c.c1 * d0 + c.c2 * r1;
+  cr[i] = T(r1);
+  d1[i] = T(dn);
+  x[i] = T(d0 + dn);
+}
+
+// Post-smoothing, step 0 from the iterate t: r_0 = Dinv (b - A t), d_0 = r_0 /
+// theta, x = t + d_0.
+template <class T, int LPR>
+__global__ void __launch_bounds__(AB) k_cheb_start(int n, const int* __restrict__ rp, const int* __restrict__ cols,
+                                                   const T* __restrict__ A, const T* __restrict__ dinv,
+                                                   const T* __restrict__ b, const T* __restrict__ t,
+                                                   const double* __restrict__ lmax, double ratio,
+                                                   T* __restrict__ cr, T* __restrict__ d0, T* __restrict__ x,
+                                                   const int* done) {
+  if (*done) return;
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = g / LPR, lane = g % LPR;
+  double s = 0.0;
+  if (i < n)
+    for (int k = rp[i] + lane; k < rp[i + 1]; k += LPR) s += double(A[k]) * double(t[cols[k]]);
+  s = group_sum<LPR>(s);
+  if (i >= n || lane) return;
+  const ChebStep c = cheb_step(lmax[1], ratio, 0);
+  const double r0 = double(dinv[i]) * (double(b[i]) - s), d = r0 * c.inv_theta;
+  cr[i] = T(r0);
+  d0[i] = T(d);
+  x[i] = T(double(t[i]) + d);
+}
+
+// Step k >= 1: r -= Dinv A d_in, d_out = c1 d_in + c2 r, x += d_out (each row
+// updates only its own r and x; the neighbours are read from d_in)
+template <class T, int LPR>
+__global__ void __launch_bounds__(AB) k_cheb_next(int n, const int* __restrict__ rp, const int* __restrict__ cols,
+                                                  const T* __restrict__ A, const T* __restrict__ dinv,
+                                                  const T* __restrict__ d_in, const double* __restrict__ lmax,
+                                                  double ratio, int step, T* __restrict__ cr, T* __restrict__ d_out,
+                                                  T* __restrict__ x, const int* done) {
+  if (*done) return;
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = g / LPR, lane = g % LPR;
+  double s = 0.0;
+  if (i < n)
+    for (int k = rp[i] + lane; k < rp[i + 1]; k += LPR) s += double(A[k]) * double(d_in[cols[k]]);
+  s = group_sum<LPR>(s);
+  if (i >= n || lane) return;
+  const ChebStep c = cheb_step(lmax[1], ratio, step);
+  const double r = double(cr[i]) - double(dinv[i]) * s;
+  const double dn = c.c1 * double(d_in[i]) + c.c2 * r;
+  cr[i] = T(r);
+  d_out[i] = T(dn);
+  x[i] = T(double(x[i]) + dn);
+}
+
+// residual r = b - A x
+template <class T, int LPR>
+__global__ void __launch_bounds__(AB) k_resid(int n, const int* __restrict__ rp, const int* __restrict__ cols,
+                                              const T* __restrict__ A, const T* __restrict__ b,
+                                              const T* __restrict__ x, T* __restrict__ r, const int* done) {
+  if (*done) return;
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = g / LPR, lane = g % LPR;
+  double s = 0.0;
+  if (i < n)
+    for (int k = rp[i] + lane; k < rp[i + 1]; k += LPR) s += double(A[k]) * double(x[cols[k]]);
+  s = group_sum<LPR>(s);
+  if (i < n && lane == 0) r[i] = T(double(b[i]) - s);
+}
+
 #define OA_LPR_LAUNCH(lpr, kernel, T, rows, st, ...)                                         \
   do {                                                                                        \
     if ((lpr) == 1)                                                                           \
@@ -448,6 +651,26 @@ int Amg<T>::numeric(const T* A_fine, cudaStream_t st) {
     AmgLevel<T>& v = L[l];
     k_dinv<T><<<(v.n + AB - 1) / AB, AB, 0, st>>>(v.n, v.rp, v.diag, v.A, v.dinv);
     count_launches(1);
+    if (v.cheb) {
+      // the estimate runs in FP64 on an FP64 copy of the level (small by
+      // construction: at most cheb_rows rows)
+      k_widen<T><<<(v.nnz + AB - 1) / AB, AB, 0, st>>>(v.nnz, v.A, v.pw_a);
+      k_widen<T><<<(v.n + AB - 1) / AB, AB, 0, st>>>(v.n, v.dinv, v.pw_dinv);
+      k_power_init<<<(v.n + AB - 1) / AB, AB, 0, st>>>(v.n, v.pw_v, v.lmax);
+      const int nb = (int)grid_for(v.n, v.lpr_a);
+      for (int it = 0; it < POWER_STEPS; ++it) {
+        const double* vin = (it & 1) ? v.pw_w : v.pw_v;
+        double* wout = (it & 1) ? v.pw_v : v.pw_w;
+        switch (v.lpr_a) {
+          case 1: k_power_apply<1><<<nb, AB, 0, st>>>(v.n, v.rp, v.cols, v.pw_a, v.pw_dinv, vin, v.lmax, wout, v.pw_part); break;
+          case 4: k_power_apply<4><<<nb, AB, 0, st>>>(v.n, v.rp, v.cols, v.pw_a, v.pw_dinv, vin, v.lmax, wout, v.pw_part); break;
+          case 8: k_power_apply<8><<<nb, AB, 0, st>>>(v.n, v.rp, v.cols, v.pw_a, v.pw_dinv, vin, v.lmax, wout, v.pw_part); break;
+          default: k_power_apply<32><<<nb, AB, 0, st>>>(v.n, v.rp, v.cols, v.pw_a, v.pw_dinv, vin, v.lmax, wout, v.pw_part);
+        }
+        k_power_norm<<<1, AB, 0, st>>>(nb, v.pw_part, v.lmax);
+      }
+      count_launches(3 + 2 * POWER_STEPS);
+    }
     if (l + 1 < L.size()) {
       AmgLevel<T>& c = L[l + 1];
       if (smoothed) {
@@ -484,8 +707,20 @@ int Amg<T>::apply(const T* v, T* z, const int* done, cudaStream_t st) {
       break;
     }
     AmgLevel<T>& c = L[l + 1];
-    OA_LPR_LAUNCH(lv.lpr_a, k_smooth_resid, T, lv.n, st, lv.n, lv.rp, lv.cols, lv.A, lv.dinv, b, lv.t, lv.r, omega,
-                  done);
+    if (lv.cheb) {
+      OA_LPR_LAUNCH(lv.lpr_a, k_cheb_first, T, lv.n, st, lv.n, lv.rp, lv.cols, lv.A, lv.dinv, b, lv.lmax, cheb_ratio,
+                    lv.cr, lv.cd1, lv.t, done);
+      for (int k = 2; k < cheb_degree; ++k) {
+        const T* din = (k & 1) ? lv.cd0 : lv.cd1;
+        T* dout = (k & 1) ? lv.cd1 : lv.cd0;
+        OA_LPR_LAUNCH(lv.lpr_a, k_cheb_next, T, lv.n, st, lv.n, lv.rp, lv.cols, lv.A, lv.dinv, din, lv.lmax,
+                      cheb_ratio, k, lv.cr, dout, lv.t, done);
+      }
+      OA_LPR_LAUNCH(lv.lpr_a, k_resid, T, lv.n, st, lv.n, lv.rp, lv.cols, lv.A, b, lv.t, lv.r, done);
+    } else {
+      OA_LPR_LAUNCH(lv.lpr_a, k_smooth_resid, T, lv.n, st, lv.n, lv.rp, lv.cols, lv.A, lv.dinv, b, lv.t, lv.r,
+                    omega, done);
+    }
     if (smoothed)
       OA_LPR_LAUNCH(lv.lpr_pt, k_sa_restrict, T, c.n, st, c.n, lv.pt_rp, lv.pt_rows, lv.ptv, lv.r, c.b, done);
     else
@@ -500,14 +735,25 @@ int Amg<T>::apply(const T* v, T* z, const int* done, cudaStream_t st) {
     if (smoothed) {
       OA_LPR_LAUNCH(lv.lpr_p, k_sa_prolong_add, T, lv.n, st, lv.n, lv.p_rp, lv.p_cols, lv.pv, L[l + 1].x, lv.t,
                     alpha, done);
-      OA_LPR_LAUNCH(lv.lpr_a, k_post_smooth, T, lv.n, st, lv.n, lv.rp, lv.cols, lv.A, lv.dinv, b, lv.t, x, omega,
-                    done);
+      if (lv.cheb) {
+        OA_LPR_LAUNCH(lv.lpr_a, k_cheb_start, T, lv.n, st, lv.n, lv.rp, lv.cols, lv.A, lv.dinv, b, lv.t, lv.lmax,
+                      cheb_ratio, lv.cr, lv.cd0, x, done);
+        for (int k = 1; k < cheb_degree; ++k) {
+          const T* din = (k & 1) ? lv.cd0 : lv.cd1;
+          T* dout = (k & 1) ? lv.cd1 : lv.cd0;
+          OA_LPR_LAUNCH(lv.lpr_a, k_cheb_next, T, lv.n, st, lv.n, lv.rp, lv.cols, lv.A, lv.dinv, din, lv.lmax,
+                        cheb_ratio, k, lv.cr, dout, x, done);
+        }
+      } else {
+        OA_LPR_LAUNCH(lv.lpr_a, k_post_smooth, T, lv.n, st, lv.n, lv.rp, lv.cols, lv.A, lv.dinv, b, lv.t, x, omega,
+                      done);
+      }
     } else {
       k_up<T><<<(lv.n + AB - 1) / AB, AB, 0, st>>>(lv.n, lv.rp, lv.cols, lv.A, lv.dinv, lv.agg, b, lv.t, L[l + 1].x,
                                                     x, omega, alpha, done);
     }
   }
-  count_launches((smoothed ? 4 : 3) * (long long)(nl - 1) + 1);
+  count_launches((smoothed ? 4 : 3) * (long long)(nl - 1) + 1 + cheb_launches);
   OA_CUDA(cudaGetLastError());
   return OA_OK;
 }

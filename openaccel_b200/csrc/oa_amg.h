@@ -48,6 +48,14 @@ struct AmgLevel {
   // cycle work vectors: x (output, levels > 0), b (input, levels > 0), r
   // (residual), t (pre-smoothed iterate)
   T *x = nullptr, *b = nullptr, *r = nullptr, *t = nullptr;
+  // Chebyshev smoother (small levels): preconditioned residual, two direction
+  // buffers; the power-iteration estimate of the spectral radius of Dinv A
+  // (lmax[1]) and its FP64 work arrays (matrix and Dinv copies, two vectors,
+  // block partials)
+  bool cheb = false;
+  T *cr = nullptr, *cd0 = nullptr, *cd1 = nullptr;
+  double* lmax = nullptr;
+  double *pw_a = nullptr, *pw_dinv = nullptr, *pw_v = nullptr, *pw_w = nullptr, *pw_part = nullptr;
   bool own_A = false;
 };
 
@@ -64,6 +72,14 @@ struct Amg {
                                   // prolongation, whose over-correction halves the Krylov
                                   // iterations on the 128^3 cavity)
   int pre = 1, post = 1;          // smoothing sweeps
+  // Chebyshev smoothing of the given degree (0: Jacobi everywhere) on every
+  // coarse level above the coarsest with at most cheb_rows rows, over the interval
+  // [lambda / cheb_ratio, lambda] of Dinv A, lambda 1.1 times its power
+  // iteration estimate
+  int cheb_degree = 3;
+  int cheb_rows = 50000;
+  double cheb_ratio = 30.0;
+  long long cheb_launches = 0;    // extra launches per V-cycle of the Chebyshev levels
   bool ready = false;
 
   // structure from the fine graph (host arrays); device pointers of the fine
