@@ -334,7 +334,8 @@ int oa_flow_create(oa_mesh* M, const oa_flow_settings* s, const double* bnd_velo
   int st = OA_OK;
   if ((st = dalloc(&f.U, 3 * nn)) || (st = dalloc(&f.p, nn)) || (st = dalloc(&f.gradU, 9 * nn)) ||
       (st = dalloc(&f.gradP, 3 * nn)) || (st = dalloc(&f.du, 3 * nn)) || (st = dalloc(&f.div, nn)) ||
-      (st = dalloc(&f.mDot, 12 * ne)) || (st = dalloc(&f.rho, nn)) || (st = dalloc(&f.mu, nn)) ||
+      (st = dalloc(&f.mDot, 12 * ne)) || (st = dalloc(&f.pc_flux, 12 * ne)) || (st = dalloc(&f.rho, nn)) ||
+      (st = dalloc(&f.mu, nn)) ||
       (st = dalloc(&f.sideU, 3 * nn)) || (st = dalloc(&f.b.b_pc, nn)) || (st = dalloc(&f.b.x_mom, 3 * nn)) ||
       (st = dalloc(&f.b.x_pc, nn)) || (st = dalloc(&f.err_dev, 1)) || (st = dalloc(&H->scal, 4)) ||
       (st = dalloc(&f.red, (size_t)partials_size())) || (st = dalloc(&f.ref_flag, nn))) {
@@ -394,8 +395,8 @@ int oa_flow_create(oa_mesh* M, const oa_flow_settings* s, const double* bnd_velo
 void oa_flow_destroy(oa_flow* H) {
   if (!H) return;
   Flow& f = H->f;
-  void* ptrs[] = {f.U, f.p, f.gradU, f.gradP, f.du, f.div, f.mDot, f.rho, f.mu, f.sideU, f.b.A_mom, f.b.b_mom,
-                  f.b.A_pc, f.b.b_pc, f.b.x_mom, f.b.x_pc, f.err_dev, H->scal, f.red,
+  void* ptrs[] = {f.U, f.p, f.gradU, f.gradP, f.du, f.div, f.mDot, f.pc_flux, f.rho, f.mu, f.sideU, f.b.A_mom,
+                  f.b.b_mom, f.b.A_pc, f.b.b_pc, f.b.x_mom, f.b.x_pc, f.err_dev, H->scal, f.red,
                   f.ref_flag};
   for (void* p : ptrs)
     if (p) cudaFree(p);
@@ -550,7 +551,7 @@ int oa_simple_iterate(oa_flow* H, int n, oa_iter_stats* stats) {
     // pressure correction (pressureCorrectionEquation::solve)
     nvtxRangePushA("mass flow and pressure-correction assembly");
     if (!s) s = launch_update_mdot(f);
-    if (!s) s = launch_pcorr(f, mx);
+    if (!s) s = launch_pcorr(f, mx, true);
     if (!s) s = continuity_rms(H, &st.continuity_rms);
     nvtxRangePop();
     mark(3);

@@ -64,6 +64,10 @@ struct Flow {
   // fields (FP64)
   double *U = nullptr, *p = nullptr, *gradU = nullptr, *gradP = nullptr, *du = nullptr,
          *div = nullptr, *mDot = nullptr, *rho = nullptr, *mu = nullptr, *sideU = nullptr;
+  // [ne][12] Rhie-Chow mass flux of each SCS ip with the pressure-correction
+  // equation's upwind density (its right-hand side), written by the mass-flow
+  // kernel and summed per row by the pressure-correction kernel
+  double* pc_flux = nullptr;
   Buffers b;
   // Krylov workspace (allocated on first solve)
   std::vector<void*> work;
@@ -102,7 +106,9 @@ int create_tet4_mesh(oa_mesh* M, const double* coords, int nn, const int* conn, 
 
 // kernels / launchers (oa_kernels.cu)
 int launch_geometry(DeviceMesh& m, cudaStream_t st);
-int launch_pcorr(Flow& f, bool mixed);
+// flux_fresh: pc_flux already holds this state's fluxes (the mass-flow update
+// ran last on the stream); otherwise a flux-only mass-flow pass runs first
+int launch_pcorr(Flow& f, bool mixed, bool flux_fresh = false);
 int launch_momentum(Flow& f, bool mixed);
 int launch_init_mdot(Flow& f);
 int launch_update_mdot(Flow& f);

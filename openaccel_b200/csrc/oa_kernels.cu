@@ -198,7 +198,8 @@ __device__ __forceinline__ void write_row(int row, bool rv, int c, int lane, con
 // frame; adjustMatrixForPressureReference, pressureCorrectionAssembler.cpp:19-63).
 struct PcArgs {
   MeshView m;
-  const double *U, *p, *gradP, *du, *mDot, *rho;
+  const double *du, *mDot, *rho;
+  const double* flux;  // [ne][12] Rhie-Chow ip mass fluxes with the upwind density
   void* A;
   double* b;
   const uint8_t* ref_flag;  // [nn] 1 on pressure-level rows
@@ -228,18 +229,6 @@ __global__ void __launch_bounds__(BLOCK, 4) k_pcorr(PcArgs a) {
     double Aq[3][3];
 #pragma unroll
     for (int q = 0; q < 3; ++q) load_area(a.m, e, (iw >> (5 * q)) & 31, Aq[q]);
-    // element-centre pressure gradient by SCV volume fractions
-    double Gp[3] = {0.0, 0.0, 0.0};
-    double pn[8];
-#pragma unroll
-    for (int k = 0; k < 8; ++k) {
-      const double w = __ldg(a.m.wscv + 8 * e + perm_at(pw, k));
-      double gp[3];
-      load3(a.gradP, nd[k], gp);
-#pragma unroll
-      for (int j = 0; j < 3; ++j) Gp[j] += w * gp[j];
-      pn[k] = __ldg(a.p + nd[k]);
-    }
     const double rho0 = __ldg(a.rho + nd[0]);
     int err = 0;
     StaticFor<0, 3>::run([&](auto qc) {
@@ -249,34 +238,17 @@ __global__ void __launch_bounds__(BLOCK, 4) k_pcorr(PcArgs a) {
       using PG = ScsPt<IP, PGSH>;
       using PV = ScsPt<IP, USH>;
       const InvJac J = inv_jacobian<PG>(x, &err);
-      double u[3] = {0, 0, 0}, duip[3] = {0, 0, 0}, dp[3] = {0, 0, 0};
+      double duip[3] = {0, 0, 0};
       StaticFor<0, 8>::run([&](auto nc) {
         constexpr int n = decltype(nc)::value;
         constexpr double N = shape_at<PV, n>();
         if (N != 0.0) {
-          double un[3], dn[3];
-          load3(a.U, nd[n], un);
+          double dn[3];
           load3(a.du, nd[n], dn);
 #pragma unroll
-          for (int j = 0; j < 3; ++j) {
-            u[j] += N * un[j];
-            duip[j] += N * dn[j];
-          }
+          for (int j = 0; j < 3; ++j) duip[j] += N * dn[j];
         }
       });
-      // grad p at the ip through the parametric gradient: dp = J^-T sum_n dN_n/ds p_n
-      double dps[3] = {0.0, 0.0, 0.0};
-      StaticFor<0, 8>::run([&](auto nc) {
-        constexpr int n = decltype(nc)::value;
-        constexpr double d0 = dshape(n, 0, PG::s(0), PG::s(1), PG::s(2));
-        constexpr double d1 = dshape(n, 1, PG::s(0), PG::s(1), PG::s(2));
-        constexpr double d2 = dshape(n, 2, PG::s(0), PG::s(1), PG::s(2));
-        if (d0 != 0.0) dps[0] += d0 * pn[n];
-        if (d1 != 0.0) dps[1] += d1 * pn[n];
-        if (d2 != 0.0) dps[2] += d2 * pn[n];
-      });
-#pragma unroll
-      for (int i = 0; i < 3; ++i) dp[i] = J.s[0][i] * dps[0] + J.s[1][i] * dps[1] + J.s[2][i] * dps[2];
       const int pk = (iw >> (5 * q)) & 31;
       const double tm = (pk & 1) ? -__ldg(a.mDot + 12 * e + (pk >> 1)) : __ldg(a.mDot + 12 * e + (pk >> 1));
       const double rhoHR = tm > 0 ? rho0 : __ldg(a.rho + nd[R]);
@@ -303,13 +275,10 @@ __global__ void __launch_bounds__(BLOCK, 4) k_pcorr(PcArgs a) {
         }
       });
       diag[0] -= fsum;
-      double mm = 0.0;
-#pragma unroll
-      for (int j = 0; j < 3; ++j) {
-        mm += rhoHR * u[j] * Aq[q][j];
-        mm -= rhoHR * duip[j] * (dp[j] - Gp[j]) * Aq[q][j];
-      }
-      rhs -= mm;
+      // rhs: the ip's Rhie-Chow mass flux, evaluated once per ip by the
+      // mass-flow kernel in the ip's canonical orientation
+      const double fl = __ldg(a.flux + 12 * e + (pk >> 1));
+      rhs -= (pk & 1) ? -fl : fl;
     });
     if (err) a.err[0] = 1;
     nbc[0] = nd[1];
@@ -600,8 +569,10 @@ struct MdotArgs {
   MeshView m;
   const double *U, *p, *gradP, *du, *rho;
   double* mDot;
+  double* flux;  // [ne][12] pressure-correction ip fluxes (update and flux-only modes)
   double urf;
-  int init;
+  int init;       // initial mass flow rho U.A (no Rhie-Chow term, no fluxes)
+  int flux_only;  // write the fluxes from the current mass flow, leave it unchanged
   int* err;
 };
 
@@ -737,14 +708,30 @@ __global__ void __launch_bounds__(BLOCK, 4) k_mdot(MdotArgs a) {
 #pragma unroll
       for (int i = 0; i < 3; ++i) dp[i] = J.s[0][i] * dps[0] + J.s[1][i] * dps[1] + J.s[2][i] * dps[2];
       const double old = a.mDot[12 * e + IP];
-      const double tU = old / rhoIp;
-      const double rhoUp = tU > 0 ? __ldg(a.rho + nd[lr(IP, 0)]) : __ldg(a.rho + nd[lr(IP, 1)]);
+      double now = old;
+      if (!a.flux_only) {
+        const double tU = old / rhoIp;
+        const double rhoUp = tU > 0 ? __ldg(a.rho + nd[lr(IP, 0)]) : __ldg(a.rho + nd[lr(IP, 1)]);
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+          m += rhoUp * u[j] * Aip[j];
+          m -= rhoUp * duip[j] * (dp[j] - Gp[j]) * Aip[j];
+        }
+        now = a.urf * m + (1.0 - a.urf) * old;
+        a.mDot[12 * e + IP] = now;
+      }
+      // the pressure-correction right-hand side's flux at this ip: the same
+      // Rhie-Chow velocity with the density upwinded by the new mass flow
+      // (pressureCorrectionAssemblerElemTerms.cpp:17-616, as the oracle's
+      // assemble_pcorr forms it per ip)
+      const double rhoHR = now > 0 ? __ldg(a.rho + nd[lr(IP, 0)]) : __ldg(a.rho + nd[lr(IP, 1)]);
+      double mm = 0.0;
 #pragma unroll
       for (int j = 0; j < 3; ++j) {
-        m += rhoUp * u[j] * Aip[j];
-        m -= rhoUp * duip[j] * (dp[j] - Gp[j]) * Aip[j];
+        mm += rhoHR * u[j] * Aip[j];
+        mm -= rhoHR * duip[j] * (dp[j] - Gp[j]) * Aip[j];
       }
-      a.mDot[12 * e + IP] = a.urf * m + (1.0 - a.urf) * old;
+      a.flux[12 * e + IP] = mm;
     }
   });
   if (err) a.err[0] = 1;
@@ -883,8 +870,12 @@ __global__ void k_vel_correct(int n3, double* U, const double* du, const double*
 // launchers
 static int grid_rows(int nn) { return (int)(((size_t)nn * 8 + BLOCK - 1) / BLOCK); }
 
-int launch_pcorr(Flow& f, bool mixed) {
-  PcArgs a{f.mesh->view(), f.U, f.p, f.gradP, f.du, f.mDot, f.rho, f.b.A_pc, f.b.b_pc, f.ref_flag, f.err_dev};
+static int launch_mdot_impl(Flow& f, int mode);
+
+int launch_pcorr(Flow& f, bool mixed, bool flux_fresh) {
+  if (!flux_fresh)
+    if (int s = launch_mdot_impl(f, 2)) return s;
+  PcArgs a{f.mesh->view(), f.du, f.mDot, f.rho, f.pc_flux, f.b.A_pc, f.b.b_pc, f.ref_flag, f.err_dev};
   const int g = grid_rows(f.mesh->nn);
   const bool us = f.s.u_shifted, ps = f.s.p_grad_shifted;
 #define OA_PC(US, PS, T)                                                                    \
@@ -918,8 +909,11 @@ int launch_momentum(Flow& f, bool mixed) {
   return OA_OK;
 }
 
-static int launch_mdot_impl(Flow& f, int init) {
-  MdotArgs a{f.mesh->view(), f.U, f.p, f.gradP, f.du, f.rho, f.mDot, f.s.mdot_urf, init, f.err_dev};
+// mode 0: update the mass flow and write the pressure-correction ip fluxes;
+// 1: initial mass flow; 2: ip fluxes only (mass flow unchanged)
+static int launch_mdot_impl(Flow& f, int mode) {
+  MdotArgs a{f.mesh->view(), f.U,          f.p,          f.gradP,   f.du,     f.rho, f.mDot, f.pc_flux,
+             f.s.mdot_urf,   mode == 1 ? 1 : 0, mode == 2 ? 1 : 0, f.err_dev};
   const int g = (f.mesh->ne + BLOCK - 1) / BLOCK;
   const bool us = f.s.u_shifted, ps = f.s.p_grad_shifted;
   if (us && ps) k_mdot<true, true><<<g, BLOCK, 0, f.stream>>>(a);
