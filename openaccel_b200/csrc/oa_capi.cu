@@ -343,11 +343,23 @@ int oa_flow_create(oa_mesh* M, const oa_flow_settings* s, const double* bnd_velo
     return st;
   }
   if (cudaMalloc(&f.b.A_mom, tm * 9 * nnz) != cudaSuccess || cudaMalloc(&f.b.b_mom, tm * 3 * nn) != cudaSuccess ||
-      cudaMalloc(&f.b.A_pc, tm * nnz) != cudaSuccess || cudaMallocHost(&H->hscal, 4 * sizeof(double)) != cudaSuccess) {
+      cudaMalloc(&f.b.A_pc, tm * nnz) != cudaSuccess || cudaMalloc(&f.pc_coef, tm * 24 * ne) != cudaSuccess ||
+      cudaMallocHost(&H->hscal, 4 * sizeof(double)) != cudaSuccess ||
+      (s->precision == OA_PREC_MIXED && (cudaMalloc(&f.xloc32, sizeof(float4) * 8 * ne) != cudaSuccess ||
+                                         cudaMalloc(&f.umu32, sizeof(float4) * nn) != cudaSuccess))) {
     oa_flow_destroy(H);
     return fail(OA_ERR_CUDA, "oa_flow_create: device allocation failed");
   }
   cudaStreamCreateWithFlags(&f.stream, cudaStreamNonBlocking);
+  if (f.xloc32) {
+    st = launch_xloc(f);
+    if (!st && cudaStreamSynchronize(f.stream) != cudaSuccess)
+      st = fail(OA_ERR_CUDA, "oa_flow_create: corner offsets failed");
+    if (st) {
+      oa_flow_destroy(H);
+      return st;
+    }
+  }
   // constant properties, zero fields
   std::vector<double> h(nn, s->rho);
   cudaMemcpy(f.rho, h.data(), sizeof(double) * nn, cudaMemcpyHostToDevice);
@@ -395,9 +407,9 @@ int oa_flow_create(oa_mesh* M, const oa_flow_settings* s, const double* bnd_velo
 void oa_flow_destroy(oa_flow* H) {
   if (!H) return;
   Flow& f = H->f;
-  void* ptrs[] = {f.U, f.p, f.gradU, f.gradP, f.du, f.div, f.mDot, f.pc_flux, f.rho, f.mu, f.sideU, f.b.A_mom,
-                  f.b.b_mom, f.b.A_pc, f.b.b_pc, f.b.x_mom, f.b.x_pc, f.err_dev, H->scal, f.red,
-                  f.ref_flag};
+  void* ptrs[] = {f.U,       f.p,       f.gradU,   f.gradP,   f.du,      f.div,    f.mDot,  f.pc_flux,
+                  f.pc_coef, f.xloc32,  f.umu32,   f.rho,     f.mu,      f.sideU,  f.b.A_mom, f.b.b_mom,
+                  f.b.A_pc,  f.b.b_pc,  f.b.x_mom, f.b.x_pc,  f.err_dev, H->scal,  f.red,   f.ref_flag};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (H->hscal) cudaFreeHost(H->hscal);
@@ -550,7 +562,7 @@ int oa_simple_iterate(oa_flow* H, int n, oa_iter_stats* stats) {
     mark(2);
     // pressure correction (pressureCorrectionEquation::solve)
     nvtxRangePushA("mass flow and pressure-correction assembly");
-    if (!s) s = launch_update_mdot(f);
+    if (!s) s = launch_update_mdot(f, true);
     if (!s) s = launch_pcorr(f, mx, true);
     if (!s) s = continuity_rms(H, &st.continuity_rms);
     nvtxRangePop();

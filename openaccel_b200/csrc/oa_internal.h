@@ -68,6 +68,13 @@ struct Flow {
   // equation's upwind density (its right-hand side), written by the mass-flow
   // kernel and summed per row by the pressure-correction kernel
   double* pc_flux = nullptr;
+  // [ne][8][3] pressure-correction lhs coefficients per element corner (edge
+  // neighbours in the row-slot order), matrix precision, staged the same way
+  void* pc_coef = nullptr;
+  // mixed form only: [ne][8] FP32 corner offsets from corner 0 (static) and
+  // the [nn] FP32 (U, mu) copy packed before each momentum assembly
+  float4* xloc32 = nullptr;
+  float4* umu32 = nullptr;
   Buffers b;
   // Krylov workspace (allocated on first solve)
   std::vector<void*> work;
@@ -111,7 +118,9 @@ int launch_geometry(DeviceMesh& m, cudaStream_t st);
 int launch_pcorr(Flow& f, bool mixed, bool flux_fresh = false);
 int launch_momentum(Flow& f, bool mixed);
 int launch_init_mdot(Flow& f);
-int launch_update_mdot(Flow& f);
+int launch_xloc(Flow& f);
+// stage: also write the pressure-correction ip fluxes and corner coefficients
+int launch_update_mdot(Flow& f, bool stage = false);
 int launch_div(Flow& f);
 int launch_gradient(Flow& f, int which);
 int launch_axpy_du_gradp(Flow& f, double sign);

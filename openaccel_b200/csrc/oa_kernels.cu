@@ -196,18 +196,33 @@ __device__ __forceinline__ void write_row(int row, bool rv, int c, int lane, con
 // Pressure-correction assembly
 // (pressureCorrectionAssemblerElemTerms.cpp:17-616, incompressible, stationary
 // frame; adjustMatrixForPressureReference, pressureCorrectionAssembler.cpp:19-63).
+//
+// Split in two: the element-owner mass-flow kernel (k_mdot below) evaluates
+// every SCS ip once and stages, per element corner, the lhs coefficients of
+// the corner's three edge neighbours summed over the corner's three ips
+// ([ne][8][3], in the order of edge_nbr) and, per ip, the Rhie-Chow flux of the
+// rhs ([ne][12]); this row kernel gathers its row's eight corner records and
+// writes the CSR row. The diagonal is minus the sum of the kept neighbour
+// coefficients (partition of unity, sum_n grad N_n = 0: every column outside
+// the edge stencil is lumped into it).
 struct PcArgs {
   MeshView m;
-  const double *du, *mDot, *rho;
+  const void* coef;    // [ne][8][3] staged lhs coefficients (TF)
   const double* flux;  // [ne][12] Rhie-Chow ip mass fluxes with the upwind density
   void* A;
   double* b;
   const uint8_t* ref_flag;  // [nn] 1 on pressure-level rows
-  int* err;
 };
 
-template <bool USH, bool PGSH, class TF>
-__global__ void __launch_bounds__(BLOCK, 4) k_pcorr(PcArgs a) {
+// Edge neighbours of corner c in the order of the row slots (canonical nodes
+// 1, 3, 4 of the rotation that maps c to corner 0).
+__host__ __device__ constexpr int edge_nbr(int c, int s) {
+  constexpr int T[8][3] = {{1, 3, 4}, {0, 5, 2}, {3, 1, 6}, {2, 7, 0}, {5, 0, 7}, {4, 6, 1}, {7, 2, 5}, {6, 4, 3}};
+  return T[c][s];
+}
+
+template <class TF>
+__global__ void __launch_bounds__(BLOCK) k_pcorr(PcArgs a) {
   __shared__ TF sh_val[BLOCK * 3];
   __shared__ int sh_col[BLOCK * 3];
   const int lane = threadIdx.x & 31;
@@ -221,69 +236,21 @@ __global__ void __launch_bounds__(BLOCK, 4) k_pcorr(PcArgs a) {
   int nbc[3] = {-1, -1, -1};
   double rhs = 0.0;
   if (e >= 0) {
+    const TF* cf = static_cast<const TF*>(a.coef) + 24 * (size_t)e + 3 * c;
     const uint32_t pw = perm_word(c);
+#pragma unroll
+    for (int s = 0; s < 3; ++s) {
+      nb[s][0] = __ldg(cf + s);
+      nbc[s] = __ldg(a.m.conn + 8 * e + perm_at(pw, s == 0 ? 1 : (s == 1 ? 3 : 4)));
+    }
+    diag[0] = -(nb[0][0] + nb[1][0] + nb[2][0]);
     const uint32_t iw = ip_word(c);
-    double x[8][3];
-    int nd[8];
-    gather_x(a.m, e, pw, x, nd);
-    double Aq[3][3];
 #pragma unroll
-    for (int q = 0; q < 3; ++q) load_area(a.m, e, (iw >> (5 * q)) & 31, Aq[q]);
-    const double rho0 = __ldg(a.rho + nd[0]);
-    int err = 0;
-    StaticFor<0, 3>::run([&](auto qc) {
-      constexpr int q = decltype(qc)::value;
-      constexpr int IP = q == 0 ? 0 : (q == 1 ? 3 : 8);
-      constexpr int R = q == 0 ? 1 : (q == 1 ? 3 : 4);
-      using PG = ScsPt<IP, PGSH>;
-      using PV = ScsPt<IP, USH>;
-      const InvJac J = inv_jacobian<PG>(x, &err);
-      double duip[3] = {0, 0, 0};
-      StaticFor<0, 8>::run([&](auto nc) {
-        constexpr int n = decltype(nc)::value;
-        constexpr double N = shape_at<PV, n>();
-        if (N != 0.0) {
-          double dn[3];
-          load3(a.du, nd[n], dn);
-#pragma unroll
-          for (int j = 0; j < 3; ++j) duip[j] += N * dn[j];
-        }
-      });
+    for (int q = 0; q < 3; ++q) {
       const int pk = (iw >> (5 * q)) & 31;
-      const double tm = (pk & 1) ? -__ldg(a.mDot + 12 * e + (pk >> 1)) : __ldg(a.mDot + 12 * e + (pk >> 1));
-      const double rhoHR = tm > 0 ? rho0 : __ldg(a.rho + nd[R]);
-      // lhs: -rhoHR * D_ip . (grad N_n) A (FP32 in the mixed form). Only the
-      // three edge neighbours keep their own columns; the diagonal takes every
-      // other column, which by the partition of unity (sum_n grad N_n = 0) is
-      // minus the sum of the neighbours' coefficients
-      const TF rh = TF(rhoHR);
-      TF dA[3];
-#pragma unroll
-      for (int j = 0; j < 3; ++j) dA[j] = TF(duip[j]) * TF(Aq[q][j]);
-      TF fsum = TF(0);
-      StaticFor<1, 5>::run([&](auto nc) {
-        constexpr int n = decltype(nc)::value;
-        constexpr int sl = nb_slot(n);
-        if (sl >= 0 && !grad_is_zero<PG, n>()) {
-          double gd[3];
-          grad_n<PG, n>(J, gd);
-          TF f = TF(0);
-#pragma unroll
-          for (int j = 0; j < 3; ++j) f += -rh * dA[j] * TF(gd[j]);
-          nb[sl][0] += f;
-          fsum += f;
-        }
-      });
-      diag[0] -= fsum;
-      // rhs: the ip's Rhie-Chow mass flux, evaluated once per ip by the
-      // mass-flow kernel in the ip's canonical orientation
       const double fl = __ldg(a.flux + 12 * e + (pk >> 1));
       rhs -= (pk & 1) ? -fl : fl;
-    });
-    if (err) a.err[0] = 1;
-    nbc[0] = nd[1];
-    nbc[1] = nd[3];
-    nbc[2] = nd[4];
+    }
   }
   diag[0] = rowsum8(diag[0]);
   rhs = rowsum8(rhs);
@@ -302,6 +269,8 @@ __global__ void __launch_bounds__(BLOCK, 4) k_pcorr(PcArgs a) {
 struct MomArgs {
   MeshView m;
   const double *U, *gradP, *div, *mDot, *rho, *mu, *sideU;
+  const float4* xloc;  // mixed form: [ne][8] FP32 corner offsets from corner 0
+  const float4* umu;   // mixed form: [nn] FP32 (U, mu)
   void* A;
   void* b;
   double* du;
@@ -411,25 +380,44 @@ __global__ void __launch_bounds__(BLOCK, sizeof(TF) == 4 ? (UGSH ? 4 : 3) : 1) k
   if (e >= 0) {
     const uint32_t pw = perm_word(c);
     const uint32_t iw = ip_word(c);
-    double xg[8][3];
     int nd[8];
-    gather_x(a.m, e, pw, xg, nd);
-    // coordinates of the flux arithmetic: FP64 as gathered, or FP32 relative
-    // to corner 0 in the mixed form (the Jacobians are translation invariant)
+    // coordinates of the flux arithmetic: FP64 as gathered, or, in the mixed
+    // form, the element's FP32 corner offsets from its corner 0 (the Jacobians
+    // are translation invariant), one 16-byte load per corner, with U and mu
+    // from the FP32 node copy (one 16-byte load per node)
     TF x[8][3];
-#pragma unroll
-    for (int k = 0; k < 8; ++k)
-#pragma unroll
-      for (int i = 0; i < 3; ++i) x[k][i] = sizeof(TF) == 4 ? TF(xg[k][i] - xg[0][i]) : TF(xg[k][i]);
     TF Uc[8][3], mu[8];
+    if constexpr (sizeof(TF) == 4) {
 #pragma unroll
-    for (int k = 0; k < 8; ++k) {
-      double u[3];
-      load3(a.U, nd[k], u);
-      Uc[k][0] = TF(u[0]);
-      Uc[k][1] = TF(u[1]);
-      Uc[k][2] = TF(u[2]);
-      mu[k] = TF(__ldg(a.mu + nd[k]));
+      for (int k = 0; k < 8; ++k) {
+        const int pk = perm_at(pw, k);
+        nd[k] = __ldg(a.m.conn + 8 * e + pk);
+        const float4 t = __ldg(a.xloc + 8 * (size_t)e + pk);
+        x[k][0] = t.x;
+        x[k][1] = t.y;
+        x[k][2] = t.z;
+        const float4 u = __ldg(a.umu + nd[k]);
+        Uc[k][0] = u.x;
+        Uc[k][1] = u.y;
+        Uc[k][2] = u.z;
+        mu[k] = u.w;
+      }
+    } else {
+      double xg[8][3];
+      gather_x(a.m, e, pw, xg, nd);
+#pragma unroll
+      for (int k = 0; k < 8; ++k)
+#pragma unroll
+        for (int i = 0; i < 3; ++i) x[k][i] = TF(xg[k][i]);
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        double u[3];
+        load3(a.U, nd[k], u);
+        Uc[k][0] = TF(u[0]);
+        Uc[k][1] = TF(u[1]);
+        Uc[k][2] = TF(u[2]);
+        mu[k] = TF(__ldg(a.mu + nd[k]));
+      }
     }
     int err = 0;
     StaticFor<0, 3>::run([&](auto qc) {
@@ -569,7 +557,8 @@ struct MdotArgs {
   MeshView m;
   const double *U, *p, *gradP, *du, *rho;
   double* mDot;
-  double* flux;  // [ne][12] pressure-correction ip fluxes (update and flux-only modes)
+  double* flux;  // [ne][12] pressure-correction ip fluxes (staging modes)
+  void* coef;    // [ne][8][3] pressure-correction lhs coefficients per corner (staging modes)
   double urf;
   int init;       // initial mass flow rho U.A (no Rhie-Chow term, no fluxes)
   int flux_only;  // write the fluxes from the current mass flow, leave it unchanged
@@ -641,8 +630,12 @@ int launch_scs_area(DeviceMesh& m, cudaStream_t st) {
 
 // initializeMassFlowRateInterior_ (flowModel.cpp:3303-3470) when init != 0,
 // otherwise updateMassFlowRateInterior_ (flowModel.cpp:5272-5687).
-template <bool USH, bool PGSH>
-__global__ void __launch_bounds__(BLOCK, 4) k_mdot(MdotArgs a) {
+//
+// STAGE: also write the pressure-correction ip fluxes and corner coefficients
+// (TC: the matrix precision); without it the kernel keeps the register budget
+// of four blocks per SM.
+template <bool USH, bool PGSH, class TC, bool STAGE>
+__global__ void __launch_bounds__(BLOCK, STAGE ? 3 : 4) k_mdot(MdotArgs a) {
   const int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= a.m.ne) return;
   double x[8][3];
@@ -661,6 +654,9 @@ __global__ void __launch_bounds__(BLOCK, 4) k_mdot(MdotArgs a) {
     }
   }
   int err = 0;
+  TC coef[8][3];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) coef[k][0] = coef[k][1] = coef[k][2] = TC(0);
   StaticFor<0, 12>::run([&](auto ic) {
     constexpr int IP = decltype(ic)::value;
     using PV = ScsPt<IP, USH>;
@@ -720,20 +716,48 @@ __global__ void __launch_bounds__(BLOCK, 4) k_mdot(MdotArgs a) {
         now = a.urf * m + (1.0 - a.urf) * old;
         a.mDot[12 * e + IP] = now;
       }
-      // the pressure-correction right-hand side's flux at this ip: the same
-      // Rhie-Chow velocity with the density upwinded by the new mass flow
-      // (pressureCorrectionAssemblerElemTerms.cpp:17-616, as the oracle's
-      // assemble_pcorr forms it per ip)
-      const double rhoHR = now > 0 ? __ldg(a.rho + nd[lr(IP, 0)]) : __ldg(a.rho + nd[lr(IP, 1)]);
-      double mm = 0.0;
+      if constexpr (STAGE) {
+        // the pressure-correction right-hand side's flux at this ip: the same
+        // Rhie-Chow velocity with the density upwinded by the new mass flow
+        // (pressureCorrectionAssemblerElemTerms.cpp:17-616, as the oracle's
+        // assemble_pcorr forms it per ip)
+        const double rhoHR = now > 0 ? __ldg(a.rho + nd[lr(IP, 0)]) : __ldg(a.rho + nd[lr(IP, 1)]);
+        double mm = 0.0;
 #pragma unroll
-      for (int j = 0; j < 3; ++j) {
-        mm += rhoHR * u[j] * Aip[j];
-        mm -= rhoHR * duip[j] * (dp[j] - Gp[j]) * Aip[j];
+        for (int j = 0; j < 3; ++j) {
+          mm += rhoHR * u[j] * Aip[j];
+          mm -= rhoHR * duip[j] * (dp[j] - Gp[j]) * Aip[j];
+        }
+        a.flux[12 * e + IP] = mm;
+        // lhs: the flux's dependence on the pressure correction, -rhoHR DU_ip
+        // A . grad N_n, for the edge neighbours of L (added to L's row) and of
+        // R (subtracted from R's row: the ip's area points away from L)
+        constexpr int L = lr(IP, 0), R = lr(IP, 1);
+        const double w[3] = {-rhoHR * duip[0] * Aip[0], -rhoHR * duip[1] * Aip[1], -rhoHR * duip[2] * Aip[2]};
+        StaticFor<0, 3>::run([&](auto sc) {
+          constexpr int sl = decltype(sc)::value;
+          constexpr int nl = edge_nbr(L, sl), nr = edge_nbr(R, sl);
+          if (!grad_is_zero<PG, nl>()) {
+            double g[3];
+            grad_n<PG, nl>(J, g);
+            coef[L][sl] += TC(w[0] * g[0] + w[1] * g[1] + w[2] * g[2]);
+          }
+          if (!grad_is_zero<PG, nr>()) {
+            double g[3];
+            grad_n<PG, nr>(J, g);
+            coef[R][sl] -= TC(w[0] * g[0] + w[1] * g[1] + w[2] * g[2]);
+          }
+        });
       }
-      a.flux[12 * e + IP] = mm;
     }
   });
+  if constexpr (STAGE) {
+    TC* out = static_cast<TC*>(a.coef) + 24 * (size_t)e;
+#pragma unroll
+    for (int k = 0; k < 8; ++k)
+#pragma unroll
+      for (int sl = 0; sl < 3; ++sl) out[3 * k + sl] = coef[k][sl];
+  }
   if (err) a.err[0] = 1;
 }
 
@@ -873,27 +897,56 @@ static int grid_rows(int nn) { return (int)(((size_t)nn * 8 + BLOCK - 1) / BLOCK
 static int launch_mdot_impl(Flow& f, int mode);
 
 int launch_pcorr(Flow& f, bool mixed, bool flux_fresh) {
+  // the staged coefficients are written in the flow's matrix precision
+  if (mixed != (f.s.precision == OA_PREC_MIXED))
+    return fail(OA_ERR_ARG, "pressure-correction assembly: precision differs from the flow's");
   if (!flux_fresh)
     if (int s = launch_mdot_impl(f, 2)) return s;
-  PcArgs a{f.mesh->view(), f.du, f.mDot, f.rho, f.pc_flux, f.b.A_pc, f.b.b_pc, f.ref_flag, f.err_dev};
+  PcArgs a{f.mesh->view(), f.pc_coef, f.pc_flux, f.b.A_pc, f.b.b_pc, f.ref_flag};
   const int g = grid_rows(f.mesh->nn);
-  const bool us = f.s.u_shifted, ps = f.s.p_grad_shifted;
-#define OA_PC(US, PS, T)                                                                    \
-  if (us == US && ps == PS) k_pcorr<US, PS, T><<<g, BLOCK, 0, f.stream>>>(a);
-  if (mixed) {
-    OA_PC(true, true, float) OA_PC(true, false, float) OA_PC(false, true, float) OA_PC(false, false, float)
-  } else {
-    OA_PC(true, true, double) OA_PC(true, false, double) OA_PC(false, true, double) OA_PC(false, false, double)
-  }
-#undef OA_PC
+  if (mixed)
+    k_pcorr<float><<<g, BLOCK, 0, f.stream>>>(a);
+  else
+    k_pcorr<double><<<g, BLOCK, 0, f.stream>>>(a);
+  count_launches(1);
+  OA_CUDA(cudaGetLastError());
+  return OA_OK;
+}
+
+// FP32 corner offsets of every element from its corner 0 (mixed form, once
+// per flow: the offsets are formed in FP64 and rounded once)
+__global__ void k_xloc(MeshView m, float4* xloc) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= 8LL * m.ne) return;
+  const int e = (int)(t >> 3);
+  const int n0 = m.conn[8 * e], nk = m.conn[t];
+  xloc[t] = make_float4(float(m.x[3 * nk] - m.x[3 * n0]), float(m.x[3 * nk + 1] - m.x[3 * n0 + 1]),
+                        float(m.x[3 * nk + 2] - m.x[3 * n0 + 2]), 0.f);
+}
+
+// FP32 node copy of (U, mu) for the mixed momentum kernel
+__global__ void k_pack_umu(int nn, const double* __restrict__ U, const double* __restrict__ mu, float4* umu) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < nn) umu[i] = make_float4(float(U[3 * i]), float(U[3 * i + 1]), float(U[3 * i + 2]), float(mu[i]));
+}
+
+int launch_xloc(Flow& f) {
+  const long long n = 8LL * f.mesh->ne;
+  k_xloc<<<(unsigned)((n + 255) / 256), 256, 0, f.stream>>>(f.mesh->view(), f.xloc32);
   count_launches(1);
   OA_CUDA(cudaGetLastError());
   return OA_OK;
 }
 
 int launch_momentum(Flow& f, bool mixed) {
-  MomArgs a{f.mesh->view(), f.U, f.gradP, f.div, f.mDot, f.rho, f.mu, f.sideU, f.b.A_mom, f.b.b_mom, f.du,
-            f.s.dt, 1.0 / f.s.urf_u, f.s.wall_rhs_relax, f.err_dev};
+  if (mixed) {
+    if (!f.xloc32 || !f.umu32) return fail(OA_ERR_ARG, "momentum assembly: mixed-form buffers missing");
+    k_pack_umu<<<(f.mesh->nn + 255) / 256, 256, 0, f.stream>>>(f.mesh->nn, f.U, f.mu, f.umu32);
+    count_launches(1);
+  }
+  MomArgs a{f.mesh->view(), f.U,       f.gradP, f.div,  f.mDot,          f.rho,
+            f.mu,           f.sideU,   f.xloc32, f.umu32, f.b.A_mom,     f.b.b_mom,
+            f.du,           f.s.dt,    1.0 / f.s.urf_u, f.s.wall_rhs_relax, f.err_dev};
   const int g = grid_rows(f.mesh->nn);
   const bool us = f.s.u_shifted, gs = f.s.u_grad_shifted;
 #define OA_MOM(US, GS, T)                                                                   \
@@ -909,23 +962,33 @@ int launch_momentum(Flow& f, bool mixed) {
   return OA_OK;
 }
 
-// mode 0: update the mass flow and write the pressure-correction ip fluxes;
-// 1: initial mass flow; 2: ip fluxes only (mass flow unchanged)
+// mode 0: update the mass flow; 1: initial mass flow; 2: pressure-correction
+// staging only (ip fluxes and corner coefficients from the current mass flow,
+// which stays unchanged); 3: update and staging
 static int launch_mdot_impl(Flow& f, int mode) {
   MdotArgs a{f.mesh->view(), f.U,          f.p,          f.gradP,   f.du,     f.rho, f.mDot, f.pc_flux,
-             f.s.mdot_urf,   mode == 1 ? 1 : 0, mode == 2 ? 1 : 0, f.err_dev};
+             f.pc_coef,      f.s.mdot_urf, mode == 1 ? 1 : 0, mode == 2 ? 1 : 0, f.err_dev};
   const int g = (f.mesh->ne + BLOCK - 1) / BLOCK;
   const bool us = f.s.u_shifted, ps = f.s.p_grad_shifted;
-  if (us && ps) k_mdot<true, true><<<g, BLOCK, 0, f.stream>>>(a);
-  else if (us && !ps) k_mdot<true, false><<<g, BLOCK, 0, f.stream>>>(a);
-  else if (!us && ps) k_mdot<false, true><<<g, BLOCK, 0, f.stream>>>(a);
-  else k_mdot<false, false><<<g, BLOCK, 0, f.stream>>>(a);
+#define OA_MD(T, ST)                                                            \
+  if (us && ps) k_mdot<true, true, T, ST><<<g, BLOCK, 0, f.stream>>>(a);        \
+  else if (us && !ps) k_mdot<true, false, T, ST><<<g, BLOCK, 0, f.stream>>>(a); \
+  else if (!us && ps) k_mdot<false, true, T, ST><<<g, BLOCK, 0, f.stream>>>(a); \
+  else k_mdot<false, false, T, ST><<<g, BLOCK, 0, f.stream>>>(a);
+  if (mode == 0 || mode == 1) {
+    OA_MD(double, false)
+  } else if (f.s.precision == OA_PREC_MIXED) {
+    OA_MD(float, true)
+  } else {
+    OA_MD(double, true)
+  }
+#undef OA_MD
   count_launches(1);
   OA_CUDA(cudaGetLastError());
   return OA_OK;
 }
 int launch_init_mdot(Flow& f) { return launch_mdot_impl(f, 1); }
-int launch_update_mdot(Flow& f) { return launch_mdot_impl(f, 0); }
+int launch_update_mdot(Flow& f, bool stage) { return launch_mdot_impl(f, stage ? 3 : 0); }
 
 int launch_div(Flow& f) {
   DivArgs a{f.mesh->view(), f.mDot, f.div};
