@@ -343,7 +343,10 @@ def run_conduction(args, rank, world):
         "kernel_ms": {"assembly_mixed": t_asm, "assembly_fp64": t_asm64},
         "krylov_iters": {"mixed": st_mixed[-1]["iters"], "fp64": st_64[-1]["iters"],
                          "refinements_mixed": st_mixed[-1]["refinements"]},
-        "roofline": {"bound": "hbm", "kernel": "k_diffusion (mixed)", "achieved": achieved, "peak": peak,
+        "roofline": {"bound": "hbm",
+                     "kernel": "tet4 diffusion assembly, all passes (k_tet_elem, k_tet_face, k_tet_gather, k_tet_rhs; "
+                               "mixed)",
+                     "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind, "algorithmic_bytes": alg,
                      "traffic": None},
         "gpu_launches": launches,

@@ -17,6 +17,7 @@
 #include <cstdint>
 #include <cstring>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "oa_internal.h"
@@ -27,20 +28,12 @@ namespace oa {
 
 namespace {
 
-constexpr int DWARPS = 4;          // rows per 128-thread block
-constexpr int DIFF_MAX_ROW = 64;   // columns per row the row-owner kernel holds
 
 template <class T>
 int dalloc(T** p, size_t n) {
   cudaError_t e = cudaMalloc(p, sizeof(T) * (n ? n : 1));
   if (e != cudaSuccess) return fail(OA_ERR_CUDA, std::string("cudaMalloc: ") + cudaGetErrorString(e));
   return OA_OK;
-}
-
-__device__ __forceinline__ double warp_sum(double v) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-  return v;
 }
 
 __device__ __forceinline__ void load3(const double* __restrict__ p, int n, double (&v)[3]) {
@@ -130,8 +123,6 @@ int create_tet4_mesh(oa_mesh* M, const double* coords, int nn, const int* conn, 
     tmp.push_back(i);
     std::sort(tmp.begin(), tmp.end());
     tmp.erase(std::unique(tmp.begin(), tmp.end()), tmp.end());
-    if ((int)tmp.size() > DIFF_MAX_ROW)
-      return fail(OA_ERR_MESH, "oa_mesh_create: a tet4 node has more than 63 neighbours");
     for (size_t k = 0; k < tmp.size(); ++k)
       if (tmp[k] == i) m.h_diag[i] = (int)k;
     m.h_cols.insert(m.h_cols.end(), tmp.begin(), tmp.end());
@@ -204,162 +195,151 @@ struct DiffView {
   double wall_relax;       // wall-node rhs factor
 };
 
-// Row-owner diffusion assembly. One warp per CSR row; lane l takes the l-th
-// incident item of the row (an element seen from one of its corners, or a
-// fixed-value boundary face seen from one of its side nodes), in 32-item
-// chunks. An element item adds the owner's share of the element's diffusion
-// operator,
-//   row(owner), col(k) += -dN_k/dx . S,   S = sum over the three SCS ips
-//   around the owner of Gamma_ip * A_ip (A pointing away from the owner),
-// with the defect rhs += grad(phi) . S. A face item adds the fixed-value flux
-// of its boundary ip: lhs on the off-face node only (the side nodes' columns
-// carry bcMultiplier 0) and rhs += Gamma_bip * grad(phi~) . A_bip with phi~ the
-// side values on the face nodes. The diagonal and rhs are warp sums; the
-// off-diagonal entries are a segmented sum by CSR slot (__match_any_sync
-// groups, each summed in ascending lane order), so every entry is written once
-// and the result does not depend on scheduling.
+// Diffusion assembly in three passes, deterministic and without atomics.
+//
+// 1. Element owner (k_tet_elem): one thread per tet evaluates, for each of
+//    its four corners a, what the corner's control volume receives from the
+//    element: with S_a = sum over the three SCS ips around a of Gamma_ip A_ip
+//    (A pointing away from a), the coefficients c_a[k] = -dN_k/dx . S_a of the
+//    four element nodes and the defect rhs -sum_k c_a[k] phi_k. The corner is
+//    evaluated in the frame of the even permutation that brings it to local
+//    node 0, with the same arithmetic the oracle's element loop uses per
+//    corner. Stored as lhs[16 e + 4 a + k] and rhs[4 e + a].
+// 2. Face owner (k_tet_face): one thread per boundary face; on a fixed-value
+//    face each side node k gets the flux of its boundary ip: lhs on the
+//    off-face node only (the side nodes' columns carry bcMultiplier 0) and
+//    rhs Gamma_bip grad(phi~) . A_bip with phi~ the side values on the face
+//    nodes. Stored after the element records; zero-flux faces store zeros.
+// 3. Gathers: every CSR entry sums its staged contributions in the fixed
+//    order of a precomputed list (k_tet_gather; the diagonal is then divided
+//    by the relaxation factor), and every row sums the rhs of its element and
+//    face items in n2e / n2f order (k_tet_rhs).
 template <bool SH, class TM>
-__global__ void __launch_bounds__(32 * DWARPS, 5) k_diffusion(MeshView m, DiffView d, TM* __restrict__ A,
-                                                             double* __restrict__ b, int* err) {
-  __shared__ double s_val[DWARPS][32];
-  __shared__ double s_part[DWARPS][3][DIFF_MAX_ROW];
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const int row = blockIdx.x * DWARPS + w;
-  if (row >= m.nn) return;  // whole warp
-  const int beg = __ldg(m.row_ptr + row), len = __ldg(m.row_ptr + row + 1) - beg, dslot = __ldg(m.diag + row);
-  const int colA = lane < len ? __ldg(m.cols + beg + lane) : -1;
-  const int colB = lane + 32 < len ? __ldg(m.cols + beg + lane + 32) : -1;
-  const int ea = __ldg(m.n2e_ptr + row), n_el = __ldg(m.n2e_ptr + row + 1) - ea;
-  const int fa = __ldg(m.n2f_ptr + row), n_fc = __ldg(m.n2f_ptr + row + 1) - fa;
-  const int nitems = n_el + n_fc;
-  // shape-function weights of Gamma at an SCS ip (edge nodes, other nodes) and
-  // at a tri3 boundary ip (own node, other nodes)
+__global__ void __launch_bounds__(128) k_tet_elem(MeshView m, DiffView d, TM* __restrict__ lhs,
+                                                  double* __restrict__ rhs, int* err) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= m.ne) return;
+  // shape-function weights of Gamma at an SCS ip (edge nodes, other nodes)
   const double wn = SH ? 0.5 : 13.0 / 36.0, wf = SH ? 0.0 : 5.0 / 36.0;
-  const double fo = SH ? 1.0 : 1.0 - 7.0 / 36.0 - 7.0 / 36.0, ff = SH ? 0.0 : 7.0 / 36.0;
-  double accA = 0.0, accB = 0.0, dsum = 0.0, rsum = 0.0;
-  bool bad = false;
-  for (int base = 0; base < nitems; base += 32) {
-    const int it = base + lane;
-    double vd = 0.0, r = 0.0, v[3] = {0.0, 0.0, 0.0};
-    int nb[3] = {-1, -1, -1};
-    if (it < n_el) {
-      const int code = __ldg(m.n2e + ea + it);
-      const int e = code >> 2, a = code & 3;
-      double x[4][3], ph[4], gm[4];
-      int nd[4];
+  double x[4][3], ph[4], gm[4];
 #pragma unroll
-      for (int k = 0; k < 4; ++k) {
-        nd[k] = __ldg(m.conn + 4 * e + tet4::perm_at(a, k));
-        load3(m.x, nd[k], x[k]);
-        ph[k] = __ldg(d.phi + nd[k]);
-        gm[k] = __ldg(d.gamma + nd[k]);
-      }
-      double Ar[3][3], g[4][3];
-      tet4::corner0_areas(x, Ar);
-      if (!tet4::grad_op(x, g)) bad = true;
-      // Gamma at the ips of edges 0-1, 0-2, 0-3
-      const double G1 = wn * (gm[0] + gm[1]) + wf * (gm[2] + gm[3]);
-      const double G2 = wn * (gm[0] + gm[2]) + wf * (gm[1] + gm[3]);
-      const double G3 = wn * (gm[0] + gm[3]) + wf * (gm[1] + gm[2]);
-      double S[3];
-#pragma unroll
-      for (int j = 0; j < 3; ++j) S[j] = G1 * Ar[0][j] + G2 * Ar[1][j] + G3 * Ar[2][j];
-      double c[4];
-#pragma unroll
-      for (int k = 0; k < 4; ++k) c[k] = -(g[k][0] * S[0] + g[k][1] * S[1] + g[k][2] * S[2]);
-      vd = c[0];
-      r = -(c[0] * ph[0] + c[1] * ph[1] + c[2] * ph[2] + c[3] * ph[3]);
-#pragma unroll
-      for (int q = 0; q < 3; ++q) {
-        v[q] = c[q + 1];
-        nb[q] = nd[q + 1];
-      }
-    } else if (it < nitems) {
-      const int code = __ldg(m.n2f + fa + (it - n_el));
-      const int f = code >> 2, k = code & 3;
-      const int bnd = __ldg(m.face_bnd + f);
-      if (bnd < d.nbnd && __ldg(d.bnd_kind + bnd) == OA_BND_FIXED_VALUE) {
-        const int e = __ldg(m.face_elem + f), o = __ldg(m.face_ord + f);
-        // element nodes as (opposite node, side nodes in side order): a
-        // positively oriented ordering with the face opposite local node 0
-        double x[4][3], g[4][3], p[3][3], Af[3];
-        int nd[4];
-        nd[0] = __ldg(m.conn + 4 * e + tet4::opposite_node(o));
-#pragma unroll
-        for (int q = 0; q < 3; ++q) nd[q + 1] = __ldg(m.conn + 4 * e + tet4::side_node(o, q));
-#pragma unroll
-        for (int q = 0; q < 4; ++q) load3(m.x, nd[q], x[q]);
-        if (!tet4::grad_op(x, g)) bad = true;
-        double gs[3], grad_t[3];
-        const double po = __ldg(d.phi + nd[0]);
-#pragma unroll
-        for (int j = 0; j < 3; ++j) grad_t[j] = po * g[0][j];
-#pragma unroll
-        for (int q = 0; q < 3; ++q) {
-#pragma unroll
-          for (int j = 0; j < 3; ++j) p[q][j] = x[q + 1][j];
-          gs[q] = __ldg(d.gamma + nd[q + 1]);
-          const double ps = __ldg(d.side + nd[q + 1]);
-#pragma unroll
-          for (int j = 0; j < 3; ++j) grad_t[j] += ps * g[q + 1][j];
-        }
-        double Aall[3][3];
-        tet4::tri_face_areas(p, Aall);
-#pragma unroll
-        for (int j = 0; j < 3; ++j) Af[j] = k == 0 ? Aall[0][j] : (k == 1 ? Aall[1][j] : Aall[2][j]);
-        const double gk = k == 0 ? gs[0] : (k == 1 ? gs[1] : gs[2]);
-        const double G = fo * gk + ff * (gs[0] + gs[1] + gs[2] - gk);
-        v[0] = -G * (g[0][0] * Af[0] + g[0][1] * Af[1] + g[0][2] * Af[2]);
-        nb[0] = nd[0];
-        r = G * (grad_t[0] * Af[0] + grad_t[1] * Af[1] + grad_t[2] * Af[2]);
-      }
-    }
-    dsum += warp_sum(vd);
-    rsum += warp_sum(r);
-    // CSR slots of the item's off-diagonal columns
-    int sl[3] = {-1, -1, -1};
-    for (int s = 0; s < len; ++s) {
-      const int cs = __shfl_sync(0xffffffffu, s < 32 ? colA : colB, s & 31);
-#pragma unroll
-      for (int q = 0; q < 3; ++q)
-        if (nb[q] == cs) sl[q] = s;
-    }
-    // segmented sum by CSR slot: lanes holding the same slot (for the same
-    // off-diagonal position q) are summed by the lowest of them in ascending
-    // lane order; the slot's owner lane then adds the three position partials
-#pragma unroll
-    for (int q = 0; q < 3; ++q) {
-      s_part[w][q][lane] = 0.0;
-      s_part[w][q][lane + 32] = 0.0;
-    }
-#pragma unroll
-    for (int q = 0; q < 3; ++q) {
-      if (nb[q] >= 0 && sl[q] < 0) sl[q] = dslot;  // column outside the stencil: lumped into the diagonal
-      s_val[w][lane] = v[q];
-      __syncwarp();
-      const unsigned peers = __match_any_sync(0xffffffffu, sl[q]);
-      if (sl[q] >= 0 && lane == __ffs(peers) - 1) {
-        double sum = 0.0;
-        for (unsigned mk = peers; mk; mk &= mk - 1) sum += s_val[w][__ffs(mk) - 1];
-        s_part[w][q][sl[q]] = sum;
-      }
-      __syncwarp();
-    }
-    accA += s_part[w][0][lane] + s_part[w][1][lane] + s_part[w][2][lane];
-    accB += s_part[w][0][lane + 32] + s_part[w][1][lane + 32] + s_part[w][2][lane + 32];
-    __syncwarp();
+  for (int k = 0; k < 4; ++k) {
+    const int n = __ldg(m.conn + 4 * e + k);
+    load3(m.x, n, x[k]);
+    ph[k] = __ldg(d.phi + n);
+    gm[k] = __ldg(d.gamma + n);
   }
-  // diagonal: element share, then relaxation (diag / urf)
-  if (dslot == lane) accA = (accA + dsum) * d.urf_inv;
-  else if (dslot == lane + 32) accB = (accB + dsum) * d.urf_inv;
-  if (lane < len) A[beg + lane] = TM(accA);
-  if (lane + 32 < len) A[beg + lane + 32] = TM(accB);
-  if (lane == 0) {
-    double bb = __ldg(d.src + row) * __ldg(m.vol + row) + rsum;
-    if (__ldg(m.wall_node + row)) bb *= d.wall_relax;
-    b[row] = bb;
+  bool bad = false;
+#pragma unroll
+  for (int a = 0; a < 4; ++a) {
+    double xa[4][3], pa[4], ga[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const int q = tet4::perm_at(a, k);
+#pragma unroll
+      for (int j = 0; j < 3; ++j) xa[k][j] = x[q][j];
+      pa[k] = ph[q];
+      ga[k] = gm[q];
+    }
+    double Ar[3][3], g[4][3];
+    tet4::corner0_areas(xa, Ar);
+    if (!tet4::grad_op(xa, g)) bad = true;
+    // Gamma at the ips of edges 0-1, 0-2, 0-3
+    const double G1 = wn * (ga[0] + ga[1]) + wf * (ga[2] + ga[3]);
+    const double G2 = wn * (ga[0] + ga[2]) + wf * (ga[1] + ga[3]);
+    const double G3 = wn * (ga[0] + ga[3]) + wf * (ga[1] + ga[2]);
+    double S[3];
+#pragma unroll
+    for (int j = 0; j < 3; ++j) S[j] = G1 * Ar[0][j] + G2 * Ar[1][j] + G3 * Ar[2][j];
+    double c[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) c[k] = -(g[k][0] * S[0] + g[k][1] * S[1] + g[k][2] * S[2]);
+    rhs[4 * (size_t)e + a] = -(c[0] * pa[0] + c[1] * pa[1] + c[2] * pa[2] + c[3] * pa[3]);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) lhs[16 * (size_t)e + 4 * a + tet4::perm_at(a, k)] = TM(c[k]);
   }
   if (bad) err[0] = 1;
+}
+
+template <bool SH, class TM>
+__global__ void __launch_bounds__(128) k_tet_face(MeshView m, DiffView d, TM* __restrict__ lhs,
+                                                  double* __restrict__ rhs, int* err) {
+  const int f = blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= m.nf) return;
+  const int bnd = __ldg(m.face_bnd + f);
+  if (!(bnd < d.nbnd && __ldg(d.bnd_kind + bnd) == OA_BND_FIXED_VALUE)) {
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      lhs[3 * (size_t)f + k] = TM(0);
+      rhs[3 * (size_t)f + k] = 0.0;
+    }
+    return;
+  }
+  // shape-function weights of Gamma at a tri3 boundary ip (own node, others)
+  const double fo = SH ? 1.0 : 1.0 - 7.0 / 36.0 - 7.0 / 36.0, ff = SH ? 0.0 : 7.0 / 36.0;
+  const int e = __ldg(m.face_elem + f), o = __ldg(m.face_ord + f);
+  // element nodes as (opposite node, side nodes in side order): a positively
+  // oriented ordering with the face opposite local node 0
+  double x[4][3], g[4][3], p[3][3];
+  int nd[4];
+  nd[0] = __ldg(m.conn + 4 * e + tet4::opposite_node(o));
+#pragma unroll
+  for (int q = 0; q < 3; ++q) nd[q + 1] = __ldg(m.conn + 4 * e + tet4::side_node(o, q));
+#pragma unroll
+  for (int q = 0; q < 4; ++q) load3(m.x, nd[q], x[q]);
+  if (!tet4::grad_op(x, g)) err[0] = 1;
+  double gs[3], grad_t[3];
+  const double po = __ldg(d.phi + nd[0]);
+#pragma unroll
+  for (int j = 0; j < 3; ++j) grad_t[j] = po * g[0][j];
+#pragma unroll
+  for (int q = 0; q < 3; ++q) {
+#pragma unroll
+    for (int j = 0; j < 3; ++j) p[q][j] = x[q + 1][j];
+    gs[q] = __ldg(d.gamma + nd[q + 1]);
+    const double ps = __ldg(d.side + nd[q + 1]);
+#pragma unroll
+    for (int j = 0; j < 3; ++j) grad_t[j] += ps * g[q + 1][j];
+  }
+  double Aall[3][3];
+  tet4::tri_face_areas(p, Aall);
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const double G = fo * gs[k] + ff * (gs[0] + gs[1] + gs[2] - gs[k]);
+    lhs[3 * (size_t)f + k] = TM(-G * (g[0][0] * Aall[k][0] + g[0][1] * Aall[k][1] + g[0][2] * Aall[k][2]));
+    rhs[3 * (size_t)f + k] = G * (grad_t[0] * Aall[k][0] + grad_t[1] * Aall[k][1] + grad_t[2] * Aall[k][2]);
+  }
+}
+
+// A[s] = sum of the staged contributions listed for entry s, in list order;
+// diagonal entries divided by the relaxation factor
+template <class TM>
+__global__ void __launch_bounds__(256) k_tet_gather(int nnz, const int* __restrict__ eptr,
+                                                    const int* __restrict__ eidx, const uint8_t* __restrict__ ediag,
+                                                    const TM* __restrict__ lhs, double urf_inv, TM* __restrict__ A) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nnz) return;
+  double acc = 0.0;
+  for (int q = __ldg(eptr + s); q < __ldg(eptr + s + 1); ++q) acc += double(__ldg(lhs + __ldg(eidx + q)));
+  if (__ldg(ediag + s)) acc *= urf_inv;
+  A[s] = TM(acc);
+}
+
+// b[row] = source * volume + the row's element and face rhs (n2e, then n2f
+// order), times the wall relaxation on wall nodes
+__global__ void __launch_bounds__(256) k_tet_rhs(MeshView m, DiffView d, const double* __restrict__ rhs_e,
+                                                 const double* __restrict__ rhs_f, double* __restrict__ b) {
+  const int row = blockIdx.x * blockDim.x + threadIdx.x;
+  if (row >= m.nn) return;
+  double r = 0.0;
+  for (int q = __ldg(m.n2e_ptr + row); q < __ldg(m.n2e_ptr + row + 1); ++q) r += __ldg(rhs_e + __ldg(m.n2e + q));
+  for (int q = __ldg(m.n2f_ptr + row); q < __ldg(m.n2f_ptr + row + 1); ++q) {
+    const int code = __ldg(m.n2f + q);
+    r += __ldg(rhs_f + 3 * (code >> 2) + (code & 3));
+  }
+  double bb = __ldg(d.src + row) * __ldg(m.vol + row) + r;
+  if (__ldg(m.wall_node + row)) bb *= d.wall_relax;
+  b[row] = bb;
 }
 
 // phi <- phi + x, clipped below (equation::correctField_ with CLIP,
@@ -397,11 +377,70 @@ struct oa_diffusion {
   int* err = nullptr;
   bool assembled = false;
   ScalarSolve solver;
+  // staged contributions: [16 ne] element lhs then [3 nf] face lhs (matrix
+  // precision), [4 ne] element rhs then [3 nf] face rhs (FP64)
+  void* lhs_st = nullptr;
+  double* rhs_st = nullptr;
+  // per CSR entry, the ordered list of staged lhs contributions, and a mark
+  // on the diagonal entries
+  int *eptr = nullptr, *eidx = nullptr;
+  uint8_t* ediag = nullptr;
 };
 
 namespace {
 
 bool dmixed(const oa_diffusion* H) { return H->s.precision == OA_PREC_MIXED; }
+
+// Contribution lists of the CSR entries (the element-to-CSR slot map, kept in
+// the entry-owner direction): corner a of element e adds its coefficient of
+// node k to entry (conn[a], conn[k]) as staged index 16 e + 4 a + k; side node
+// q of a fixed-value face f adds its coefficient of the face's opposite node
+// to entry (side node, opposite node) as staged index 16 ne + 3 f + q. Each
+// list is in ascending staged index (elements in order, then faces). A column
+// missing from its row, which a conforming mesh cannot produce (its graph holds
+// every element pair), is lumped into the row's diagonal.
+int build_entry_lists(const DeviceMesh& m, const int* bnd_kind, int nbnd, std::vector<int>& eptr,
+                      std::vector<int>& eidx, std::vector<uint8_t>& ediag) {
+  const long long ne = m.ne, nf = m.nf, nnz = m.nnz;
+  if (16 * ne + 3 * nf >= INT_MAX) return fail(OA_ERR_ARG, "oa_diffusion_create: mesh too large for 32-bit lists");
+  const int* cols = m.h_cols.data();
+  auto slot = [&](int row, int col) -> int {
+    const int *b = cols + m.h_row_ptr[row], *e = cols + m.h_row_ptr[row + 1];
+    const int* p = std::lower_bound(b, e, col);
+    return (p != e && *p == col) ? (int)(p - cols) : m.h_row_ptr[row] + m.h_diag[row];
+  };
+  // slot of every staged contribution (-1: a face that is not fixed-value)
+  std::vector<int> sl(16 * ne + 3 * nf, -1);
+  const int nt = std::max(1, std::min<int>(16, (int)std::thread::hardware_concurrency()));
+  auto work = [&](int t) {
+    const long long lo = ne * t / nt, hi = ne * (t + 1) / nt;
+    for (long long e = lo; e < hi; ++e)
+      for (int a = 0; a < 4; ++a)
+        for (int k = 0; k < 4; ++k) sl[16 * e + 4 * a + k] = slot(m.h_conn[4 * e + a], m.h_conn[4 * e + k]);
+  };
+  std::vector<std::thread> th;
+  for (int t = 0; t < nt; ++t) th.emplace_back(work, t);
+  for (auto& t : th) t.join();
+  for (long long f = 0; f < nf; ++f) {
+    const int bnd = m.h_face_bnd[f];
+    if (!(bnd < nbnd && bnd_kind[bnd] == OA_BND_FIXED_VALUE)) continue;
+    const long long e = m.h_face_elem[f];
+    const int o = m.h_face_ord[f];
+    const int opp = m.h_conn[4 * e + tet4::opposite_node(o)];
+    for (int q = 0; q < 3; ++q) sl[16 * ne + 3 * f + q] = slot(m.h_conn[4 * e + tet4::side_node(o, q)], opp);
+  }
+  eptr.assign(nnz + 1, 0);
+  for (const int s : sl)
+    if (s >= 0) ++eptr[s + 1];
+  for (long long s = 0; s < nnz; ++s) eptr[s + 1] += eptr[s];
+  eidx.assign(eptr[nnz], 0);
+  std::vector<int> pos(eptr.begin(), eptr.end() - 1);
+  for (size_t i = 0; i < sl.size(); ++i)
+    if (sl[i] >= 0) eidx[pos[sl[i]]++] = (int)i;
+  ediag.assign(nnz, 0);
+  for (int r = 0; r < m.nn; ++r) ediag[m.h_row_ptr[r] + m.h_diag[r]] = 1;
+  return OA_OK;
+}
 
 double* diff_field(oa_diffusion* H, const std::string& n) {
   if (n == "phi") return H->phi;
@@ -411,19 +450,30 @@ double* diff_field(oa_diffusion* H, const std::string& n) {
   return nullptr;
 }
 
-int launch_diffusion(oa_diffusion* H) {
+template <bool SH, class TM>
+void launch_diffusion_t(oa_diffusion* H, const DiffView& d) {
   DeviceMesh& m = *H->mesh;
+  TM* lhs = static_cast<TM*>(H->lhs_st);
+  double* rhs = H->rhs_st;
+  const size_t ne = m.ne;
+  k_tet_elem<SH, TM><<<(m.ne + 127) / 128, 128, 0, H->stream>>>(m.view(), d, lhs, rhs, H->err);
+  if (m.nf) k_tet_face<SH, TM><<<(m.nf + 127) / 128, 128, 0, H->stream>>>(m.view(), d, lhs + 16 * ne, rhs + 4 * ne, H->err);
+  k_tet_gather<TM><<<(m.nnz + 255) / 256, 256, 0, H->stream>>>(m.nnz, H->eptr, H->eidx, H->ediag, lhs, d.urf_inv,
+                                                                static_cast<TM*>(H->A));
+  k_tet_rhs<<<(m.nn + 255) / 256, 256, 0, H->stream>>>(m.view(), d, rhs, rhs + 4 * ne, H->b);
+  count_launches(m.nf ? 4 : 3);
+}
+
+int launch_diffusion(oa_diffusion* H) {
   DiffView d{H->phi, H->gamma, H->src, H->side, H->bnd_kind, H->nbnd, 1.0 / H->s.urf, H->s.wall_rhs_relax};
-  const int grid = (m.nn + DWARPS - 1) / DWARPS;
   const bool sh = H->s.shifted != 0;
   if (dmixed(H)) {
-    if (sh) k_diffusion<true, float><<<grid, 32 * DWARPS, 0, H->stream>>>(m.view(), d, (float*)H->A, H->b, H->err);
-    else k_diffusion<false, float><<<grid, 32 * DWARPS, 0, H->stream>>>(m.view(), d, (float*)H->A, H->b, H->err);
+    if (sh) launch_diffusion_t<true, float>(H, d);
+    else launch_diffusion_t<false, float>(H, d);
   } else {
-    if (sh) k_diffusion<true, double><<<grid, 32 * DWARPS, 0, H->stream>>>(m.view(), d, (double*)H->A, H->b, H->err);
-    else k_diffusion<false, double><<<grid, 32 * DWARPS, 0, H->stream>>>(m.view(), d, (double*)H->A, H->b, H->err);
+    if (sh) launch_diffusion_t<true, double>(H, d);
+    else launch_diffusion_t<false, double>(H, d);
   }
-  count_launches(1);
   OA_CUDA(cudaGetLastError());
   H->assembled = true;
   return OA_OK;
@@ -491,6 +541,24 @@ int oa_diffusion_create(oa_mesh* M, const oa_diffusion_settings* s, const int* b
     oa_diffusion_destroy(H);
     return fail(OA_ERR_CUDA, "oa_diffusion_create: device allocation failed");
   }
+  {
+    std::vector<int> eptr, eidx;
+    std::vector<uint8_t> ediag;
+    const size_t ne = m.ne, nf = m.nf;
+    if ((st = build_entry_lists(m, bnd_kind, nbnd, eptr, eidx, ediag)) || (st = dalloc(&H->eptr, eptr.size())) ||
+        (st = dalloc(&H->eidx, eidx.size())) || (st = dalloc(&H->ediag, ediag.size())) ||
+        (st = dalloc(&H->rhs_st, 4 * ne + 3 * nf))) {
+      oa_diffusion_destroy(H);
+      return st;
+    }
+    if (cudaMalloc(&H->lhs_st, tm * (16 * ne + 3 * nf + 1)) != cudaSuccess) {
+      oa_diffusion_destroy(H);
+      return fail(OA_ERR_CUDA, "oa_diffusion_create: device allocation failed");
+    }
+    cudaMemcpy(H->eptr, eptr.data(), sizeof(int) * eptr.size(), cudaMemcpyHostToDevice);
+    if (!eidx.empty()) cudaMemcpy(H->eidx, eidx.data(), sizeof(int) * eidx.size(), cudaMemcpyHostToDevice);
+    cudaMemcpy(H->ediag, ediag.data(), ediag.size(), cudaMemcpyHostToDevice);
+  }
   cudaStreamCreateWithFlags(&H->stream, cudaStreamNonBlocking);
   std::vector<double> h(nn, 0.0);
   // node-side values of the fixed-value boundaries, boundary by boundary in
@@ -524,7 +592,8 @@ int oa_diffusion_create(oa_mesh* M, const oa_diffusion_settings* s, const int* b
 
 void oa_diffusion_destroy(oa_diffusion* H) {
   if (!H) return;
-  void* ptrs[] = {H->phi, H->gamma, H->src, H->side, H->bnd_kind, H->A, H->b, H->x, H->err};
+  void* ptrs[] = {H->phi, H->gamma, H->src,   H->side, H->bnd_kind, H->A,    H->b,
+                  H->x,   H->err,   H->lhs_st, H->rhs_st, H->eptr,    H->eidx, H->ediag};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   H->solver.release();
