@@ -217,48 +217,62 @@ struct DiffView {
 template <bool SH, class TM>
 __global__ void __launch_bounds__(128) k_tet_elem(MeshView m, DiffView d, TM* __restrict__ lhs,
                                                   double* __restrict__ rhs, int* err) {
+  // the records are assembled in shared memory (rows padded against bank
+  // conflicts) and each warp stores its 32 elements' records as one
+  // contiguous, coalesced block
+  __shared__ TM s_lhs[128 * 17];
+  __shared__ double s_rhs[128 * 5];
   const int e = blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= m.ne) return;
-  // shape-function weights of Gamma at an SCS ip (edge nodes, other nodes)
-  const double wn = SH ? 0.5 : 13.0 / 36.0, wf = SH ? 0.0 : 5.0 / 36.0;
-  double x[4][3], ph[4], gm[4];
-#pragma unroll
-  for (int k = 0; k < 4; ++k) {
-    const int n = __ldg(m.conn + 4 * e + k);
-    load3(m.x, n, x[k]);
-    ph[k] = __ldg(d.phi + n);
-    gm[k] = __ldg(d.gamma + n);
-  }
-  bool bad = false;
-#pragma unroll
-  for (int a = 0; a < 4; ++a) {
-    double xa[4][3], pa[4], ga[4];
+  const int lane = threadIdx.x & 31, wbase = threadIdx.x & ~31;
+  const long long e0 = (long long)blockIdx.x * blockDim.x + wbase;
+  if (e0 >= m.ne) return;  // whole warp
+  const int nvalid = (int)min(32LL, (long long)m.ne - e0);
+  if (e < m.ne) {
+    // shape-function weights of Gamma at an SCS ip (edge nodes, other nodes)
+    const double wn = SH ? 0.5 : 13.0 / 36.0, wf = SH ? 0.0 : 5.0 / 36.0;
+    double x[4][3], ph[4], gm[4];
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
-      const int q = tet4::perm_at(a, k);
-#pragma unroll
-      for (int j = 0; j < 3; ++j) xa[k][j] = x[q][j];
-      pa[k] = ph[q];
-      ga[k] = gm[q];
+      const int n = __ldg(m.conn + 4 * e + k);
+      load3(m.x, n, x[k]);
+      ph[k] = __ldg(d.phi + n);
+      gm[k] = __ldg(d.gamma + n);
     }
-    double Ar[3][3], g[4][3];
-    tet4::corner0_areas(xa, Ar);
-    if (!tet4::grad_op(xa, g)) bad = true;
-    // Gamma at the ips of edges 0-1, 0-2, 0-3
-    const double G1 = wn * (ga[0] + ga[1]) + wf * (ga[2] + ga[3]);
-    const double G2 = wn * (ga[0] + ga[2]) + wf * (ga[1] + ga[3]);
-    const double G3 = wn * (ga[0] + ga[3]) + wf * (ga[1] + ga[2]);
-    double S[3];
+    // the element's six SCS areas and its gradient operator, once
+    double A6[6][3], g[4][3];
+    tet4::scs_areas6(x, A6);
+    const bool bad = !tet4::grad_op(x, g);
+    // Gamma at the ip of each edge: its two nodes with weight wn, the others wf
+    constexpr int EN[6][4] = {{0, 1, 2, 3}, {0, 2, 1, 3}, {0, 3, 1, 2}, {1, 3, 0, 2}, {1, 2, 0, 3}, {2, 3, 0, 1}};
+    double Ge[6];
 #pragma unroll
-    for (int j = 0; j < 3; ++j) S[j] = G1 * Ar[0][j] + G2 * Ar[1][j] + G3 * Ar[2][j];
-    double c[4];
+    for (int q = 0; q < 6; ++q) Ge[q] = wn * (gm[EN[q][0]] + gm[EN[q][1]]) + wf * (gm[EN[q][2]] + gm[EN[q][3]]);
 #pragma unroll
-    for (int k = 0; k < 4; ++k) c[k] = -(g[k][0] * S[0] + g[k][1] * S[1] + g[k][2] * S[2]);
-    rhs[4 * (size_t)e + a] = -(c[0] * pa[0] + c[1] * pa[1] + c[2] * pa[2] + c[3] * pa[3]);
+    for (int a = 0; a < 4; ++a) {
+      // S = sum over the corner's three ips of Gamma_ip A_ip, A away from a
+      double S[3] = {0.0, 0.0, 0.0};
 #pragma unroll
-    for (int k = 0; k < 4; ++k) lhs[16 * (size_t)e + 4 * a + tet4::perm_at(a, k)] = TM(c[k]);
+      for (int k = 1; k < 4; ++k) {
+        const int q = tet4::corner_edge(a, k);
+        const double w = tet4::corner_edge_sign(a, k) * Ge[q];
+#pragma unroll
+        for (int j = 0; j < 3; ++j) S[j] += w * A6[q][j];
+      }
+      double c[4], r = 0.0;
+#pragma unroll
+      for (int n = 0; n < 4; ++n) {
+        c[n] = -(g[n][0] * S[0] + g[n][1] * S[1] + g[n][2] * S[2]);
+        r -= c[n] * ph[n];
+      }
+      s_rhs[threadIdx.x * 5 + a] = r;
+#pragma unroll
+      for (int n = 0; n < 4; ++n) s_lhs[threadIdx.x * 17 + 4 * a + n] = TM(c[n]);
+    }
+    if (bad) err[0] = 1;
   }
-  if (bad) err[0] = 1;
+  __syncwarp();
+  for (int i = lane; i < 16 * nvalid; i += 32) lhs[16 * e0 + i] = s_lhs[(wbase + (i >> 4)) * 17 + (i & 15)];
+  for (int i = lane; i < 4 * nvalid; i += 32) rhs[4 * e0 + i] = s_rhs[(wbase + (i >> 2)) * 5 + (i & 3)];
 }
 
 template <bool SH, class TM>
@@ -319,8 +333,21 @@ __global__ void __launch_bounds__(256) k_tet_gather(int nnz, const int* __restri
                                                     const TM* __restrict__ lhs, double urf_inv, TM* __restrict__ A) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= nnz) return;
+  // four list items per pass with every load issued before the adds (items
+  // past the end clamped and dropped); the sum keeps list order
+  const int q0 = __ldg(eptr + s), q1 = __ldg(eptr + s + 1);
   double acc = 0.0;
-  for (int q = __ldg(eptr + s); q < __ldg(eptr + s + 1); ++q) acc += double(__ldg(lhs + __ldg(eidx + q)));
+  for (int q = q0; q < q1; q += 4) {
+    int id[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) id[u] = __ldg(eidx + min(q + u, q1 - 1));
+    double v[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) v[u] = double(__ldg(lhs + id[u]));
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+      if (q + u < q1) acc += v[u];
+  }
   if (__ldg(ediag + s)) acc *= urf_inv;
   A[s] = TM(acc);
 }
@@ -332,7 +359,18 @@ __global__ void __launch_bounds__(256) k_tet_rhs(MeshView m, DiffView d, const d
   const int row = blockIdx.x * blockDim.x + threadIdx.x;
   if (row >= m.nn) return;
   double r = 0.0;
-  for (int q = __ldg(m.n2e_ptr + row); q < __ldg(m.n2e_ptr + row + 1); ++q) r += __ldg(rhs_e + __ldg(m.n2e + q));
+  const int q0 = __ldg(m.n2e_ptr + row), q1 = __ldg(m.n2e_ptr + row + 1);
+  for (int q = q0; q < q1; q += 4) {  // as in k_tet_gather: four items in flight, order kept
+    int id[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) id[u] = __ldg(m.n2e + min(q + u, q1 - 1));
+    double v[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) v[u] = __ldg(rhs_e + id[u]);
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+      if (q + u < q1) r += v[u];
+  }
   for (int q = __ldg(m.n2f_ptr + row); q < __ldg(m.n2f_ptr + row + 1); ++q) {
     const int code = __ldg(m.n2f + q);
     r += __ldg(rhs_f + 3 * (code >> 2) + (code & 3));

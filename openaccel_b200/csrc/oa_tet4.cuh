@@ -57,6 +57,54 @@ __device__ __forceinline__ void corner0_areas(const double (&x)[4][3], double (&
   quad_area(m03, f013, c, f023, A[2]);
 }
 
+// Area vectors of all six sub-control surfaces of the element, one per edge,
+// in the order (0,1), (0,2), (0,3), (1,3), (1,2), (2,3), each pointing away
+// from the edge's first node. Each is the quad of corner0_areas seen from the
+// edge's first node in that node's even-permutation frame (corner 0: nodes
+// 0123, corner 1: 1032, corner 2: 2301); the surface seen from the other node
+// is the same quad in reverse order, i.e. the negated vector.
+__device__ __forceinline__ void scs_areas6(const double (&x)[4][3], double (&A)[6][3]) {
+  double m01[3], m02[3], m03[3], m12[3], m13[3], m23[3], f012[3], f013[3], f023[3], f123[3], c[3];
+  const double half = 0.5, third = 1.0 / 3.0;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const double x0 = x[0][k], x1 = x[1][k], x2 = x[2][k], x3 = x[3][k];
+    m01[k] = half * (x0 + x1);
+    m02[k] = half * (x2 + x0);
+    m03[k] = half * (x0 + x3);
+    m12[k] = half * (x1 + x2);
+    m13[k] = half * (x1 + x3);
+    m23[k] = half * (x2 + x3);
+    f012[k] = third * (x0 + x1 + x2);
+    f023[k] = third * (x0 + x2 + x3);
+    f013[k] = third * (x0 + x1 + x3);
+    f123[k] = third * (x1 + x2 + x3);
+    double s = 0.0;
+    s = s + 0.25 * x0;
+    s = s + 0.25 * x1;
+    s = s + 0.25 * x2;
+    s = s + 0.25 * x3;
+    c[k] = s;
+  }
+  quad_area(m01, f012, c, f013, A[0]);
+  quad_area(m02, f023, c, f012, A[1]);
+  quad_area(m03, f013, c, f023, A[2]);
+  quad_area(m13, f123, c, f013, A[3]);
+  quad_area(m12, f012, c, f123, A[4]);
+  quad_area(m23, f023, c, f123, A[5]);
+}
+
+// Edge of scs_areas6 joining corner a to node perm_at(a, k) (k = 1..3), with
+// the sign that makes its area point away from a.
+__host__ __device__ constexpr int corner_edge(int a, int k) {
+  constexpr int E[4][3] = {{0, 1, 2}, {0, 3, 4}, {5, 1, 4}, {5, 3, 2}};
+  return E[a][k - 1];
+}
+__host__ __device__ constexpr double corner_edge_sign(int a, int k) {
+  constexpr int S[4][3] = {{1, 1, 1}, {-1, 1, 1}, {1, -1, -1}, {-1, -1, -1}};
+  return S[a][k - 1];
+}
+
 // Constant dN/dx of the four nodes (tet_gradient_operator). Returns false when
 // the Jacobian determinant is <= 1e6 * DBL_MIN (the determinant is then 1).
 __device__ __forceinline__ bool grad_op(const double (&x)[4][3], double (&g)[4][3]) {
