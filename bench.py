@@ -348,7 +348,7 @@ def run_conduction(args, rank, world):
                                "mixed)",
                      "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind, "algorithmic_bytes": alg,
-                     "traffic": None},
+                     "traffic": traffic_from_profile("tet4_assembly_conduction96.md") if args.n == 96 else None},
         "gpu_launches": launches,
         "clocks": clk.summary(),
     }
