@@ -1,5 +1,6 @@
 // tet4 scalar-diffusion path of the B200 CVFEM engine: tet4 mesh set-up,
-// the row-owner diffusion assembly kernel, and the C-ABI of the diffusion
+// the diffusion assembly (element pass, face pass and CSR-entry gather over
+// contribution lists built at set-up), and the C-ABI of the diffusion
 // handle (a solid-domain energy equation: Gamma-diffusion with a volumetric
 // source, fixed-value and zero-flux walls).
 //

@@ -1,13 +1,14 @@
-// tet4 control-volume master element for the row-owner kernels (device).
+// tet4 control-volume master element (device).
 //
 // Tables restate external/nalu/src/master_element/Tet4CVFEM.C (lrscv_ :329-335,
 // intgLoc_ / intgLocShift_ :365-382, sideNodeOrdinals_ :416-421) and the
 // subdivision of MasterElementWork.F tet_scs_det (:608-752) / tet_scv_det
-// (:459-606). A row owner sees an element from one of its corners; the
-// element's nodes are reordered by an even permutation that brings that corner
-// to local node 0 (orientation is preserved), so the three sub-control
-// surfaces around the owner are always ips 0 (0->1), 2 (0->2) and 3 (0->3),
-// each with its area vector pointing away from the owner.
+// (:459-606). A corner of an element is seen through the even permutation of
+// the element's nodes that brings it to local node 0 (orientation is
+// preserved), so the three sub-control surfaces around it are always ips 0
+// (0->1), 2 (0->2) and 3 (0->3), each with its area vector pointing away from
+// the corner; scs_areas6 evaluates all six surfaces of an element once in
+// those frames.
 #pragma once
 #include <cstdint>
 
@@ -31,38 +32,15 @@ __host__ __device__ __forceinline__ int side_node(int f, int k) {
 }
 __host__ __device__ __forceinline__ int opposite_node(int f) { return (0x3102u >> (4 * f)) & 0xFu; }
 
-// Area vectors of the three sub-control surfaces around local node 0 (quads
-// 4-7-14-13, 6-12-14-7 and 11-13-14-12 of the 15-point subdivision).
-__device__ __forceinline__ void corner0_areas(const double (&x)[4][3], double (&A)[3][3]) {
-  double m01[3], m02[3], m03[3], f012[3], f023[3], f013[3], c[3];
-  const double half = 0.5, third = 1.0 / 3.0;
-#pragma unroll
-  for (int k = 0; k < 3; ++k) {
-    const double x0 = x[0][k], x1 = x[1][k], x2 = x[2][k], x3 = x[3][k];
-    m01[k] = half * (x0 + x1);
-    m02[k] = half * (x2 + x0);
-    m03[k] = half * (x0 + x3);
-    f012[k] = third * (x0 + x1 + x2);
-    f023[k] = third * (x0 + x2 + x3);
-    f013[k] = third * (x0 + x1 + x3);
-    double s = 0.0;
-    s = s + 0.25 * x0;
-    s = s + 0.25 * x1;
-    s = s + 0.25 * x2;
-    s = s + 0.25 * x3;
-    c[k] = s;
-  }
-  quad_area(m01, f012, c, f013, A[0]);
-  quad_area(m02, f023, c, f012, A[1]);
-  quad_area(m03, f013, c, f023, A[2]);
-}
-
 // Area vectors of all six sub-control surfaces of the element, one per edge,
 // in the order (0,1), (0,2), (0,3), (1,3), (1,2), (2,3), each pointing away
-// from the edge's first node. Each is the quad of corner0_areas seen from the
-// edge's first node in that node's even-permutation frame (corner 0: nodes
-// 0123, corner 1: 1032, corner 2: 2301); the surface seen from the other node
-// is the same quad in reverse order, i.e. the negated vector.
+// from the edge's first node. In the frame of a corner (nodes p0 p1 p2 p3,
+// p0 the corner) the surfaces around it are the quads (m01, f012, c, f013),
+// (m02, f023, c, f012) and (m03, f013, c, f023) of the 15-point subdivision
+// (edge midpoints m, face centroids f, element centroid c); each edge is
+// evaluated in the frame of its first node (corner 0: nodes 0123, corner 1:
+// 1032, corner 2: 2301), and the surface seen from the other node is the same
+// quad in reverse order, i.e. the negated vector.
 __device__ __forceinline__ void scs_areas6(const double (&x)[4][3], double (&A)[6][3]) {
   double m01[3], m02[3], m03[3], m12[3], m13[3], m23[3], f012[3], f013[3], f023[3], f123[3], c[3];
   const double half = 0.5, third = 1.0 / 3.0;
