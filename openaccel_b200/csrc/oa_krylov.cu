@@ -111,46 +111,48 @@ __global__ void __launch_bounds__(KB) k_spmv(int nn, const int* __restrict__ rp,
   if (ND > 0) block_reduce_store<ND>(reinterpret_cast<double(&)[ND]>(v), partials, MAX_PARTIALS);
 }
 
-// z = Minv v (point or 3x3 block Jacobi)
+// z = Minv v (point or 3x3 block Jacobi); the inverse is stored in the
+// precision of the Krylov vectors (FP32 in the mixed form's inner solves)
 template <int B, class TV>
-__global__ void k_prec(int nn, const double* __restrict__ Minv, const TV* __restrict__ v, TV* __restrict__ z,
+__global__ void k_prec(int nn, const TV* __restrict__ Minv, const TV* __restrict__ v, TV* __restrict__ z,
                        const KScal* sc) {
   if (sc->done) return;
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= nn * B) return;
   if (B == 1) {
-    z[t] = TV(Minv[t] * double(v[t]));
+    z[t] = TV(double(Minv[t]) * double(v[t]));
   } else {
     const int i = t / 3, m = t - 3 * i;
-    const double* M = Minv + 9 * (size_t)i + 3 * m;
-    z[t] = TV(M[0] * double(v[3 * i]) + M[1] * double(v[3 * i + 1]) + M[2] * double(v[3 * i + 2]));
+    const TV* M = Minv + 9 * (size_t)i + 3 * m;
+    z[t] = TV(double(M[0]) * double(v[3 * i]) + double(M[1]) * double(v[3 * i + 1]) +
+              double(M[2]) * double(v[3 * i + 2]));
   }
 }
 
-template <int B, class TM>
+template <int B, class TM, class TP>
 __global__ void k_build_minv(int nn, const int* __restrict__ rp, const int* __restrict__ dg, const TM* __restrict__ A,
-                             double* Minv) {
+                             TP* Minv) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nn) return;
   const TM* d = A + (size_t)(rp[i] + dg[i]) * B * B;
   if (B == 1) {
-    Minv[i] = 1.0 / double(d[0]);
+    Minv[i] = TP(1.0 / double(d[0]));
   } else {
     double a[9];
     for (int k = 0; k < 9; ++k) a[k] = double(d[k]);
     const double det = a[0] * (a[4] * a[8] - a[5] * a[7]) - a[1] * (a[3] * a[8] - a[5] * a[6]) +
                        a[2] * (a[3] * a[7] - a[4] * a[6]);
     const double id = 1.0 / det;
-    double* r = Minv + 9 * (size_t)i;
-    r[0] = (a[4] * a[8] - a[5] * a[7]) * id;
-    r[1] = (a[2] * a[7] - a[1] * a[8]) * id;
-    r[2] = (a[1] * a[5] - a[2] * a[4]) * id;
-    r[3] = (a[5] * a[6] - a[3] * a[8]) * id;
-    r[4] = (a[0] * a[8] - a[2] * a[6]) * id;
-    r[5] = (a[2] * a[3] - a[0] * a[5]) * id;
-    r[6] = (a[3] * a[7] - a[4] * a[6]) * id;
-    r[7] = (a[1] * a[6] - a[0] * a[7]) * id;
-    r[8] = (a[0] * a[4] - a[1] * a[3]) * id;
+    TP* r = Minv + 9 * (size_t)i;
+    r[0] = TP((a[4] * a[8] - a[5] * a[7]) * id);
+    r[1] = TP((a[2] * a[7] - a[1] * a[8]) * id);
+    r[2] = TP((a[1] * a[5] - a[2] * a[4]) * id);
+    r[3] = TP((a[5] * a[6] - a[3] * a[8]) * id);
+    r[4] = TP((a[0] * a[8] - a[2] * a[6]) * id);
+    r[5] = TP((a[2] * a[3] - a[0] * a[5]) * id);
+    r[6] = TP((a[3] * a[7] - a[4] * a[6]) * id);
+    r[7] = TP((a[1] * a[6] - a[0] * a[7]) * id);
+    r[8] = TP((a[0] * a[4] - a[1] * a[3]) * id);
   }
 }
 
@@ -368,7 +370,7 @@ int KrylovSolver<B, TM, TV>::solve(const TM* A, const TB* b, TV*& xout, double r
     if constexpr (kAmgOk) {
       if (amg) return amg->apply(reinterpret_cast<const TV*>(in), out, done_flag, st);
     }
-    k_prec<B, TV><<<gfull, KB, 0, st>>>(nn, Minv, in, out, sc);
+    k_prec<B, TV><<<gfull, KB, 0, st>>>(nn, reinterpret_cast<const TV*>(Minv), in, out, sc);
     count_launches(1);
     return OA_OK;
   };
@@ -386,7 +388,7 @@ int KrylovSolver<B, TM, TV>::solve(const TM* A, const TB* b, TV*& xout, double r
     }
   }
   if (dbg) cudaEventRecord(ev[1], st);
-  k_build_minv<B, TM><<<gr, KB, 0, st>>>(nn, rp, dg, A, Minv);
+  k_build_minv<B, TM, TV><<<gr, KB, 0, st>>>(nn, rp, dg, A, reinterpret_cast<TV*>(Minv));
   k_init<TV, TB><<<gv, KB, 0, st>>>(n, b, x, r, rh, p, v, partials);
   k_init_scalars<<<1, KB, 0, st>>>(sc, partials, gv, rtol, maxit);
   count_launches(3);

@@ -13,7 +13,7 @@ struct KrylovSolver {
   const int *rp = nullptr, *cols = nullptr, *dg = nullptr;
   cudaStream_t st = nullptr;
   void* vec[8] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
-  double* Minv = nullptr;
+  double* Minv = nullptr;  // Jacobi inverse, B*B*nn values stored as TV (room for FP64)
   double* partials = nullptr;
   void* scal = nullptr;
   void* hscal = nullptr;
