@@ -200,7 +200,11 @@ typedef struct oa_diffusion_settings {
 } oa_diffusion_settings;
 
 /* bnd_kind[nbnd] (OA_BND_*) and bnd_value[nbnd] (fixed values) by boundary
- * index; node-side values are applied boundary by boundary in index order. */
+ * index; node-side values are applied boundary by boundary in index order.
+ * Set-up builds, on the host, the assembly's contribution list of every CSR
+ * entry (4 bytes per element-corner-node triple, 64 bytes per element) and
+ * keeps it on the device with the staging buffers of the element pass
+ * (16 matrix values and 4 FP64 rhs values per element). */
 int oa_diffusion_create(oa_mesh* m, const oa_diffusion_settings* s, const int* bnd_kind, const double* bnd_value,
                         int nbnd, oa_diffusion** out);
 void oa_diffusion_destroy(oa_diffusion* d);
