@@ -24,6 +24,7 @@
 #include "oa_internal.h"
 #include "oa_scalar_solve.h"
 #include "oa_tet4.cuh"
+#include "oa_tet4_lists.h"
 
 namespace oa {
 
@@ -430,54 +431,32 @@ namespace {
 
 bool dmixed(const oa_diffusion* H) { return H->s.precision == OA_PREC_MIXED; }
 
-// Contribution lists of the CSR entries (the element-to-CSR slot map, kept in
-// the entry-owner direction): corner a of element e adds its coefficient of
-// node k to entry (conn[a], conn[k]) as staged index 16 e + 4 a + k; side node
-// q of a fixed-value face f adds its coefficient of the face's opposite node
-// to entry (side node, opposite node) as staged index 16 ne + 3 f + q. Each
-// list is in ascending staged index (elements in order, then faces). A column
-// missing from its row, which a conforming mesh cannot produce (its graph holds
-// every element pair), is lumped into the row's diagonal.
+// Contribution lists of the CSR entries (oa_tet4_lists.h) from the mesh's
+// host copies; the faces' side and opposite nodes come from the tet4 tables.
 int build_entry_lists(const DeviceMesh& m, const int* bnd_kind, int nbnd, std::vector<int>& eptr,
                       std::vector<int>& eidx, std::vector<uint8_t>& ediag) {
-  const long long ne = m.ne, nf = m.nf, nnz = m.nnz;
-  if (16 * ne + 3 * nf >= INT_MAX) return fail(OA_ERR_ARG, "oa_diffusion_create: mesh too large for 32-bit lists");
-  const int* cols = m.h_cols.data();
-  auto slot = [&](int row, int col) -> int {
-    const int *b = cols + m.h_row_ptr[row], *e = cols + m.h_row_ptr[row + 1];
-    const int* p = std::lower_bound(b, e, col);
-    return (p != e && *p == col) ? (int)(p - cols) : m.h_row_ptr[row] + m.h_diag[row];
-  };
-  // slot of every staged contribution (-1: a face that is not fixed-value)
-  std::vector<int> sl(16 * ne + 3 * nf, -1);
-  const int nt = std::max(1, std::min<int>(16, (int)std::thread::hardware_concurrency()));
-  auto work = [&](int t) {
-    const long long lo = ne * t / nt, hi = ne * (t + 1) / nt;
-    for (long long e = lo; e < hi; ++e)
-      for (int a = 0; a < 4; ++a)
-        for (int k = 0; k < 4; ++k) sl[16 * e + 4 * a + k] = slot(m.h_conn[4 * e + a], m.h_conn[4 * e + k]);
-  };
-  std::vector<std::thread> th;
-  for (int t = 0; t < nt; ++t) th.emplace_back(work, t);
-  for (auto& t : th) t.join();
-  for (long long f = 0; f < nf; ++f) {
-    const int bnd = m.h_face_bnd[f];
-    if (!(bnd < nbnd && bnd_kind[bnd] == OA_BND_FIXED_VALUE)) continue;
+  std::vector<int> side(3 * (size_t)m.nf), opp(m.nf);
+  std::vector<uint8_t> fixed(m.nf, 0);
+  for (int f = 0; f < m.nf; ++f) {
     const long long e = m.h_face_elem[f];
-    const int o = m.h_face_ord[f];
-    const int opp = m.h_conn[4 * e + tet4::opposite_node(o)];
-    for (int q = 0; q < 3; ++q) sl[16 * ne + 3 * f + q] = slot(m.h_conn[4 * e + tet4::side_node(o, q)], opp);
+    const int o = m.h_face_ord[f], bnd = m.h_face_bnd[f];
+    fixed[f] = (bnd < nbnd && bnd_kind[bnd] == OA_BND_FIXED_VALUE) ? 1 : 0;
+    opp[f] = m.h_conn[4 * e + tet4::opposite_node(o)];
+    for (int q = 0; q < 3; ++q) side[3 * f + q] = m.h_conn[4 * e + tet4::side_node(o, q)];
   }
-  eptr.assign(nnz + 1, 0);
-  for (const int s : sl)
-    if (s >= 0) ++eptr[s + 1];
-  for (long long s = 0; s < nnz; ++s) eptr[s + 1] += eptr[s];
-  eidx.assign(eptr[nnz], 0);
-  std::vector<int> pos(eptr.begin(), eptr.end() - 1);
-  for (size_t i = 0; i < sl.size(); ++i)
-    if (sl[i] >= 0) eidx[pos[sl[i]]++] = (int)i;
-  ediag.assign(nnz, 0);
-  for (int r = 0; r < m.nn; ++r) ediag[m.h_row_ptr[r] + m.h_diag[r]] = 1;
+  tet4lists::Input in;
+  in.nn = m.nn;
+  in.ne = m.ne;
+  in.nf = m.nf;
+  in.row_ptr = m.h_row_ptr.data();
+  in.cols = m.h_cols.data();
+  in.diag = m.h_diag.data();
+  in.conn = m.h_conn.data();
+  in.face_side = side.data();
+  in.face_opp = opp.data();
+  in.face_fixed = fixed.data();
+  if (!tet4lists::build(in, eptr, eidx, ediag))
+    return fail(OA_ERR_ARG, "oa_diffusion_create: mesh too large for 32-bit lists");
   return OA_OK;
 }
 
