@@ -543,6 +543,9 @@ int oa_diffusion_create(oa_mesh* M, const oa_diffusion_settings* s, const int* b
   for (int f = 0; f < m.nf; ++f)
     if (m.h_face_bnd[f] >= nbnd) return fail(OA_ERR_ARG, "oa_diffusion_create: a face names a boundary index >= nbnd");
   oa_diffusion* H = new oa_diffusion();
+  // BiCGStab by default: on the tet4 conduction GCR(2) needs as many V-cycles
+  // as BiCGStab (26 against 13 x 2 at 96^3 x 6) and is 7 % slower per step
+  H->solver.gcr = false;
   H->mesh = &M->m;
   H->s = *s;
   H->nbnd = nbnd;

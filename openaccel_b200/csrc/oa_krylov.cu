@@ -275,6 +275,123 @@ __global__ void __launch_bounds__(KB) k_end_iter(KScal* sc, const double* partia
 }
 
 // ---------------------------------------------------------------------------
+// GCR(2) for scalar systems with a variable-free right preconditioner (Eisenstat,
+// Elman and Schultz 1983, truncated to the two latest directions): z = M^-1 r,
+// q = A z, orthogonalised against the stored A-images Q0, Q1 (orthonormal)
+// with the same combination applied to z, normalised, then x += alpha P,
+// r -= alpha Q with alpha = r.Q. One preconditioner application and one SpMV
+// per iteration instead of BiCGStab's two of each; the residual norm is
+// monotone.
+
+// q = A z (scalar CSR); partial q.Q0, q.Q1
+template <class TM, class TV>
+__global__ void __launch_bounds__(KB) k_spmv_gcr(int nn, const int* __restrict__ rp, const int* __restrict__ cols,
+                                                  const TM* __restrict__ A, const TV* __restrict__ z,
+                                                  TV* __restrict__ q, const TV* __restrict__ Q0,
+                                                  const TV* __restrict__ Q1, double* partials, const KScal* sc) {
+  if (sc->done) return;
+  double v[2] = {0.0, 0.0};
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nn; i += gridDim.x * blockDim.x) {
+    double s = 0.0;
+    for (int k = __ldg(rp + i); k < __ldg(rp + i + 1); ++k) s += double(A[k]) * double(z[__ldg(cols + k)]);
+    const TV qs = TV(s);
+    q[i] = qs;
+    v[0] += double(qs) * double(Q0[i]);
+    v[1] += double(qs) * double(Q1[i]);
+  }
+  block_reduce_store<2>(v, partials, MAX_PARTIALS);
+}
+
+// beta_j = q.Q_j (d0, d1)
+__global__ void __launch_bounds__(KB) k_gcr_beta(KScal* sc, const double* partials, int nb) {
+  if (sc->done) return;
+  double o[2];
+  final_reduce<2>(partials, nb, o);
+  if (threadIdx.x == 0) {
+    sc->d0 = o[0];
+    sc->d1 = o[1];
+  }
+}
+
+// z -= beta0 P0 + beta1 P1, q -= beta0 Q0 + beta1 Q1; partial q.q, r.q
+template <class TV>
+__global__ void __launch_bounds__(KB) k_gcr_orth(int n, TV* z, TV* q, const TV* P0, const TV* P1, const TV* Q0,
+                                                  const TV* Q1, const TV* r, double* partials, const KScal* sc) {
+  if (sc->done) return;
+  const double b0 = sc->d0, b1 = sc->d1;
+  double v[2] = {0.0, 0.0};
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    z[i] = TV(double(z[i]) - b0 * double(P0[i]) - b1 * double(P1[i]));
+    const TV qn = TV(double(q[i]) - b0 * double(Q0[i]) - b1 * double(Q1[i]));
+    q[i] = qn;
+    v[0] += double(qn) * double(qn);
+    v[1] += double(r[i]) * double(qn);
+  }
+  block_reduce_store<2>(v, partials, MAX_PARTIALS);
+}
+
+// 1/|q| (omega) and alpha = r.q / |q|; a vanishing q is a breakdown
+__global__ void __launch_bounds__(KB) k_gcr_alpha(KScal* sc, const double* partials, int nb) {
+  if (sc->done) return;
+  double o[2];
+  final_reduce<2>(partials, nb, o);
+  if (threadIdx.x == 0) {
+    const double nq = sqrt(o[0]);
+    if (!(nq > 0.0) || !(nq < INFINITY)) {
+      sc->done = 1;
+      sc->status = nq < INFINITY ? 1 : 2;
+      return;
+    }
+    sc->omega = 1.0 / nq;
+    sc->alpha = o[1] / nq;
+  }
+}
+
+// P = z / |q|, Q = q / |q| into the oldest slot; x += alpha P, r -= alpha Q;
+// partial r.r
+template <class TV>
+__global__ void __launch_bounds__(KB) k_gcr_update(int n, TV* x, TV* r, const TV* z, const TV* q, TV* P, TV* Q,
+                                                    double* partials, const KScal* sc) {
+  if (sc->done) return;
+  const double inv = sc->omega, al = sc->alpha;
+  double v[1] = {0.0};
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const TV pi = TV(double(z[i]) * inv), qi = TV(double(q[i]) * inv);
+    P[i] = pi;
+    Q[i] = qi;
+    x[i] = TV(double(x[i]) + al * double(pi));
+    const TV rn = TV(double(r[i]) - al * double(qi));
+    r[i] = rn;
+    v[0] += double(rn) * double(rn);
+  }
+  block_reduce_store<1>(v, partials, MAX_PARTIALS);
+}
+
+// residual norm and convergence test; an iteration that leaves the residual
+// where it was (truncated GCR can stagnate when the preconditioned operator's
+// symmetric part is not definite) ends the solve with status 1, and the
+// caller falls back to BiCGStab
+__global__ void __launch_bounds__(KB) k_gcr_end(KScal* sc, const double* partials, int nb) {
+  if (sc->done) return;
+  double o[1];
+  final_reduce<1>(partials, nb, o);
+  if (threadIdx.x == 0) {
+    const double prev = sc->rnorm;
+    sc->rnorm = sqrt(o[0]);
+    sc->iters += 1;
+    if (!(sc->rnorm < INFINITY)) {
+      sc->done = 1;
+      sc->status = 2;
+    } else if (sc->rnorm <= sc->rtol * sc->bnorm || sc->iters >= sc->maxit) {
+      sc->done = 1;
+    } else if (sc->rnorm > 0.9999 * prev) {
+      sc->done = 1;
+      sc->status = 1;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
 template <int B, class TM, class TV>
 int KrylovSolver<B, TM, TV>::setup(int nn_, const int* rp_, const int* cols_, const int* dg_, cudaStream_t st_) {
   if (nn == nn_ && rp == rp_) return OA_OK;
@@ -393,11 +510,35 @@ int KrylovSolver<B, TM, TV>::solve(const TM* A, const TB* b, TV*& xout, double r
   k_init_scalars<<<1, KB, 0, st>>>(sc, partials, gv, rtol, maxit);
   count_launches(3);
   OA_CUDA(cudaGetLastError());
+  // GCR(2) work vectors in the same buffers: x r z q P0 P1 Q0 Q1; the
+  // direction slots start at zero (no stored directions yet)
+  const bool use_gcr = gcr && B == 1;
+  TV *gz = rh, *gq = p, *gP[2] = {v, ph}, *gQ[2] = {sh, t};
+  if (use_gcr) {
+    if (check_every % 2) return fail(OA_ERR_ARG, "GCR: iteration chunks must hold an even number of iterations");
+    for (int k = 4; k < 8; ++k) OA_CUDA(cudaMemsetAsync(vec[k], 0, sizeof(TV) * (size_t)n, st));
+  }
   // one chunk of check_every iterations; every kernel reads its scalars and
   // the tolerance from device memory, so the chunk can be captured once
   long long per_chunk = 0;
   auto chunk = [&]() -> int {
     const long long l0 = launch_total();
+    if (use_gcr) {
+      for (int it = 0; it < check_every; ++it) {
+        const int slot = it & 1;  // the older of the two stored directions
+        if (int s = precond(r, gz)) return s;
+        k_spmv_gcr<TM, TV><<<gv, KB, 0, st>>>(nn, rp, cols, A, gz, gq, gQ[0], gQ[1], partials, sc);
+        k_gcr_beta<<<1, KB, 0, st>>>(sc, partials, gv);
+        k_gcr_orth<TV><<<gv, KB, 0, st>>>(n, gz, gq, gP[0], gP[1], gQ[0], gQ[1], r, partials, sc);
+        k_gcr_alpha<<<1, KB, 0, st>>>(sc, partials, gv);
+        k_gcr_update<TV><<<gv, KB, 0, st>>>(n, x, r, gz, gq, gP[slot], gQ[slot], partials, sc);
+        k_gcr_end<<<1, KB, 0, st>>>(sc, partials, gv);
+      }
+      count_launches(6L * check_every);
+      per_chunk = launch_total() - l0;
+      OA_CUDA(cudaGetLastError());
+      return OA_OK;
+    }
     for (int it = 0; it < check_every; ++it) {
       k_p_update<TV><<<gfull, KB, 0, st>>>(n, p, r, v, sc);
       if (int s = precond(p, ph)) return s;
@@ -416,7 +557,7 @@ int KrylovSolver<B, TM, TV>::solve(const TM* A, const TB* b, TV*& xout, double r
     return OA_OK;
   };
   if (use_graph && (graph_exec == nullptr || graph_A != (const void*)A || graph_chunk != check_every ||
-                    graph_amg != (const void*)amg)) {
+                    graph_amg != (const void*)amg || graph_gcr != use_gcr)) {
     if (graph_exec) cudaGraphExecDestroy(graph_exec);
     graph_exec = nullptr;
     cudaGraph_t g;
@@ -430,6 +571,7 @@ int KrylovSolver<B, TM, TV>::solve(const TM* A, const TB* b, TV*& xout, double r
     graph_A = A;
     graph_amg = amg;
     graph_chunk = check_every;
+    graph_gcr = use_gcr;
     graph_launches = per_chunk;
     count_launches(-per_chunk);  // captured, not launched
   }
@@ -461,11 +603,11 @@ int KrylovSolver<B, TM, TV>::solve(const TM* A, const TB* b, TV*& xout, double r
     float t_setup = 0.f, t_all = 0.f;
     cudaEventElapsedTime(&t_setup, ev[0], ev[1]);
     cudaEventElapsedTime(&t_all, ev[0], ev[2]);
-    std::fprintf(stderr, "[oa] BiCGStab<%d,%s> n %d iters %d: precond set-up %.3f ms, solve %.3f ms\n", B,
-                 sizeof(TV) == 4 ? "f32" : "f64", nn, h->iters, t_setup, t_all);
+    std::fprintf(stderr, "[oa] %s<%d,%s> n %d iters %d: precond set-up %.3f ms, solve %.3f ms\n",
+                 use_gcr ? "GCR(2)" : "BiCGStab", B, sizeof(TV) == 4 ? "f32" : "f64", nn, h->iters, t_setup, t_all);
     for (auto& e : ev) cudaEventDestroy(e);
   }
-  if (h->status == 2) return fail(OA_ERR_SOLVER, "BiCGStab: non-finite residual");
+  if (h->status == 2) return fail(OA_ERR_SOLVER, use_gcr ? "GCR: non-finite residual" : "BiCGStab: non-finite residual");
   return OA_OK;
 }
 

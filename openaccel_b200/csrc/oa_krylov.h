@@ -20,12 +20,14 @@ struct KrylovSolver {
   int last_status = 0;  // 0 ok, 1 breakdown, 2 non-finite, 3 diverging
   // optional AMG preconditioner (scalar systems); null = point/block Jacobi
   Amg<TV>* amg = nullptr;
+  bool gcr = false;  // scalar systems: GCR(2) instead of BiCGStab (chunks of an even iteration count)
   // CUDA-graph replay of the iteration chunk (captured on first use)
   bool use_graph = false;
   cudaGraphExec_t graph_exec = nullptr;
   const void* graph_A = nullptr;
   const void* graph_amg = nullptr;
   int graph_chunk = 0;
+  bool graph_gcr = false;
   long long graph_launches = 0;
 
   // storage carved from caller memory instead of cudaMalloc (no allocation)

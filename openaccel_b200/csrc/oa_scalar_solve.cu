@@ -6,6 +6,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
+#include <cstring>
 #include <string>
 
 #include "oa_internal.h"
@@ -23,6 +24,7 @@ __global__ void k_narrow(int n, const double* __restrict__ a, float* __restrict_
 int ScalarSolve::init(int nn) {
   if (const char* e = std::getenv("OA_AMG_REFRESH")) refresh = std::max(1, std::atoi(e));
   if (const char* e = std::getenv("OA_IR_INNER")) inner_floor = std::atof(e);
+  if (const char* e = std::getenv("OA_KRYLOV")) gcr = std::strcmp(e, "bicgstab") != 0;
   if (n == nn && r) return OA_OK;
   release();
   n = nn;
@@ -71,7 +73,10 @@ int ScalarSolve::solve(const ScalarGraph& g, bool mixed, bool amg, bool graphs, 
     k32.amg = nullptr;
   }
   k64.use_graph = k32.use_graph = graphs;
-  const int check_every = amg ? 5 : 20;
+  // with the AMG: GCR(2), one V-cycle per iteration (chunks of 4); with point
+  // Jacobi: BiCGStab
+  k64.gcr = k32.gcr = amg && gcr;
+  int check_every = amg ? (gcr ? 4 : 5) : 20;
   // AMG numeric phase every refresh-th solve (the fine matrix is always the
   // current one; the coarse operators may lag by refresh - 1 assemblies)
   const bool reuse = amg && refresh > 1 && (solves++ % refresh) != 0;
@@ -80,6 +85,12 @@ int ScalarSolve::solve(const ScalarGraph& g, bool mixed, bool amg, bool graphs, 
     double* xs = nullptr;
     if (int s = k64.solve<double>(static_cast<const double*>(A), b, xs, rtol, maxit, iters, res, check_every, reuse))
       return s;
+    if (k64.gcr && k64.last_status == 1) {
+      // GCR stagnated or broke down: BiCGStab from now on, and for this system
+      gcr = false;
+      k64.gcr = false;
+      if (int s = k64.solve<double>(static_cast<const double*>(A), b, xs, rtol, maxit, iters, res, 5, true)) return s;
+    }
     OA_CUDA(cudaMemcpyAsync(x, xs, sizeof(double) * g.nn, cudaMemcpyDeviceToDevice, st));
     if (refinements) *refinements = 0;
     return OA_OK;
@@ -107,6 +118,15 @@ int ScalarSolve::solve(const ScalarGraph& g, bool mixed, bool amg, bool graphs, 
                                  check_every, reuse || nref > 0))
       return s;
     total += it;
+    if (k32.gcr && k32.last_status == 1 && r_in > 10.0 * std::min(inner, 0.1)) {
+      // GCR stagnated or broke down far from its target (its partial
+      // correction still reduced the residual): BiCGStab for the remaining
+      // passes and later solves. A stall within a decade of the target is the
+      // FP32 floor and only ends the pass.
+      gcr = false;
+      k32.gcr = false;
+      check_every = 5;
+    }
     // a diverged inner solve contributes nothing; the next pass restarts from
     // the FP64 residual
     if (k32.last_status != 3 && r_in < 1.0) add_correction<float>(g.nn, x, d, st);

@@ -41,6 +41,12 @@ struct ScalarSolve {
   // lowest relative tolerance asked of an FP32 inner solve (0: 1e-4 with AMG,
   // 2e-4 with Jacobi); OA_IR_INNER overrides
   double inner_floor = 0.0;
+  // Krylov method with the AMG: GCR(2) (one V-cycle per iteration; the
+  // pressure correction's default: 22 instead of 26 V-cycles per outer
+  // iteration on the 128^3 cavity) or BiCGStab (two per iteration). The
+  // OA_KRYLOV environment variable overrides ("bicgstab", else GCR); a GCR
+  // solve that stagnates switches this solver to BiCGStab for good.
+  bool gcr = true;
   long long solves = 0;
 
   int init(int n);
