@@ -1,6 +1,7 @@
 // Pressure-correction / momentum Krylov solve on the device: BiCGStab
 // (van der Vorst 1992) right-preconditioned by point or 3x3 block Jacobi, or
-// for scalar systems by the aggregation-AMG V-cycle of oa_amg.cu.
+// for scalar systems by the aggregation-AMG V-cycle of oa_amg.cu; for scalar
+// AMG-preconditioned systems also GCR(2), one V-cycle per iteration.
 //
 // The reference hands its systems to liblinsolve (PETSc / Trilinos / HYPRE,
 // src/equation/linearSystem.h:416-462), which is absent from the reference

@@ -41,3 +41,20 @@ def test_chebyshev_degree_out_of_range_is_rejected(monkeypatch):
     monkeypatch.setenv("OA_AMG_CHEB_DEGREE", "9")
     with pytest.raises(rt.OpenAccelError):
         _run(rt.OA_PREC_FP64, n_iter=1)
+
+
+@pytest.mark.parametrize("prec", [rt.OA_PREC_FP64, rt.OA_PREC_MIXED])
+def test_gcr_and_bicgstab_reach_the_same_fields(monkeypatch, prec):
+    # the pressure correction's default Krylov method (GCR(2), one V-cycle per
+    # iteration) against BiCGStab (two per iteration) on the same systems
+    monkeypatch.setenv("OA_KRYLOV", "bicgstab")
+    st_b, U_b, p_b = _run(prec)
+    monkeypatch.delenv("OA_KRYLOV")
+    st_g, U_g, p_g = _run(prec)
+    assert all(s["pc_res"] <= 1e-10 * 1.0001 for s in st_g)
+    vcycles_b = 2 * sum(s["pc_iters"] for s in st_b)
+    vcycles_g = sum(s["pc_iters"] for s in st_g)
+    assert vcycles_g <= vcycles_b, (vcycles_g, vcycles_b)
+    tol = 1e-7 if prec == rt.OA_PREC_FP64 else 1e-5
+    assert np.abs(U_g - U_b).max() <= tol * np.abs(U_b).max()
+    assert np.abs(p_g - p_b).max() <= tol * np.abs(p_b).max()
