@@ -52,7 +52,8 @@ typedef struct oa_flow_settings {
   int pc_maxit;
   double pc_rtol;
   int precision;                /* OA_PREC_FP64 or OA_PREC_MIXED */
-  int pc_amg;                   /* 1: aggregation-AMG preconditioned pressure solve, 0: Jacobi */
+  int pc_amg;                   /* 1: aggregation-AMG preconditioned GCR(2) pressure solve (BiCGStab
+                                   if GCR stagnates or OA_KRYLOV=bicgstab), 0: Jacobi BiCGStab */
   int use_graphs;               /* 1: replay Krylov iteration chunks as CUDA graphs */
 } oa_flow_settings;
 
@@ -135,7 +136,9 @@ int oa_update_div(oa_flow* f);
 int oa_update_gradient(oa_flow* f, int which);
 /* Linear solve of the last assembled system: linearSystem::solve()
  * (src/equation/linearSystem.h:416-462). sys = 0 momentum (x [nn][3]), 1
- * pressure correction (x [nn]); x may be NULL (result kept on the device). */
+ * pressure correction (x [nn]); x may be NULL (result kept on the device).
+ * iters counts Krylov iterations of the method in use (GCR(2): one
+ * preconditioner application each; BiCGStab: two). */
 int oa_solve(oa_flow* f, int sys, double rtol, int maxit, double* x, int* iters, double* res);
 /* n SIMPLE outer iterations: segregatedFlowEquations::solve
  * (src/equation/flow/segregatedFlowEquations.cpp:76-297). stats may be NULL. */
