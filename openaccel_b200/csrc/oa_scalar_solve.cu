@@ -25,6 +25,7 @@ int ScalarSolve::init(int nn) {
   if (const char* e = std::getenv("OA_AMG_REFRESH")) refresh = std::max(1, std::atoi(e));
   if (const char* e = std::getenv("OA_IR_INNER")) inner_floor = std::atof(e);
   if (const char* e = std::getenv("OA_KRYLOV")) gcr = std::strcmp(e, "bicgstab") != 0;
+  if (const char* e = std::getenv("OA_GCR_CHUNK")) gcr_chunk = std::max(2, std::atoi(e) / 2 * 2);
   if (n == nn && r) return OA_OK;
   release();
   n = nn;
@@ -76,7 +77,7 @@ int ScalarSolve::solve(const ScalarGraph& g, bool mixed, bool amg, bool graphs, 
   // with the AMG: GCR(2), one V-cycle per iteration (chunks of 4); with point
   // Jacobi: BiCGStab
   k64.gcr = k32.gcr = amg && gcr;
-  int check_every = amg ? (gcr ? 4 : 5) : 20;
+  int check_every = amg ? (gcr ? gcr_chunk : 5) : 20;
   // AMG numeric phase every refresh-th solve (the fine matrix is always the
   // current one; the coarse operators may lag by refresh - 1 assemblies)
   const bool reuse = amg && refresh > 1 && (solves++ % refresh) != 0;

@@ -32,12 +32,13 @@ struct ScalarSolve {
   double* hscal = nullptr;  // [2] pinned
   double* partials = nullptr;
   int n = 0;
-  // AMG numeric phase (coarse operators, prolongation, inverse diagonals)
-  // every refresh-th solve; between refreshes the fine matrix is the current
-  // one and only the coarse operators lag (on the 128^3 cavity 4 keeps the
-  // iteration counts and saves 5 % of the outer iteration; OA_AMG_REFRESH
-  // overrides)
-  int refresh = 4;
+  // AMG numeric phase (coarse operators, prolongation, inverse diagonals,
+  // Chebyshev bounds) every refresh-th solve; between refreshes the fine
+  // matrix is the current one and only the coarse operators lag. On the 128^3
+  // cavity 4 kept the iteration counts of 1 and saved 5 % of the outer
+  // iteration; with GCR(2) 8 still keeps them (22 per outer iteration) and
+  // saves another 2 % (OA_AMG_REFRESH overrides)
+  int refresh = 8;
   // lowest relative tolerance asked of an FP32 inner solve (0: 1e-4 with AMG,
   // 2e-4 with Jacobi); OA_IR_INNER overrides
   double inner_floor = 0.0;
@@ -47,6 +48,12 @@ struct ScalarSolve {
   // OA_KRYLOV environment variable overrides ("bicgstab", else GCR); a GCR
   // solve that stagnates switches this solver to BiCGStab for good.
   bool gcr = true;
+  // GCR iterations per device-resident chunk (even; OA_GCR_CHUNK): short
+  // chunks launch fewer iterations past convergence (each a V-cycle of early
+  // exits) at the price of more host checks; on the 128^3 cavity 2 beat 4, 6
+  // and 8 (with refresh 8: 68.1 against 65.6 outer iterations/s for 4 and
+  // refresh 4)
+  int gcr_chunk = 2;
   long long solves = 0;
 
   int init(int n);
