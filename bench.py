@@ -119,7 +119,7 @@ def workload(n):
 
 
 def algorithmic_bytes_momentum(nn, ne, nnz, mixed):
-    """SURVEY-defined algorithmic bytes of one momentum assembly: nodal inputs
+    """Algorithmic bytes of one momentum assembly: nodal inputs
     13 doubles (x3, U3, mu, rho, V, grad p3, div) = 104 B/node; element inputs
     32 B connectivity + 96 B mDot; outputs 3x3 blocks + rhs + DU."""
     val = 4 if mixed else 8
