@@ -252,6 +252,7 @@ def run_ours(args, rank, world):
         "phase_ms_per_step": {form: {k[3:]: float(np.mean([x[k] for x in st[-args.steps:]])) for k in rt.PHASES}
                               for form, st in (("mixed", st_mixed), ("fp64", st_64))},
         "pc_iters_last": {"mixed": st_mixed[-1]["pc_iters"], "fp64": st_64[-1]["pc_iters"]},
+        "pc_krylov": "GCR(2) with the AMG V-cycle (one V-cycle per iteration)",
         "roofline": {"bound": "hbm", "kernel": "k_momentum (mixed)", "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
                      "algorithmic_bytes": alg, "traffic": traffic},
