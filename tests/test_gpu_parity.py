@@ -81,6 +81,49 @@ def test_momentum_assembly_parity(oracle_mod, shift):
     assert rel(gf.get_field("du"), oc.field("du")) < TOL_ASM
 
 
+def _variable_properties(m, oc, gf, seed=9):
+    """Per-node density and viscosity, and mass flows of which one in ten is
+    exactly zero (the upwind choices at a zero flux must match the oracle's)."""
+    rng = np.random.default_rng(seed)
+    rho = rng.uniform(0.5, 2.0, m.nn)
+    mu = rng.uniform(0.5e-2, 2e-2, m.nn)
+    mdot = rng.normal(0, 0.01, 12 * m.ne)
+    mdot[rng.uniform(size=mdot.size) < 0.1] = 0.0
+    for k, v in (("rho", rho), ("mu", mu), ("mDot", mdot)):
+        oc.field(k)[:] = v
+        gf.set_field(k, v)
+
+
+@pytest.mark.parametrize("prec", [rt.OA_PREC_FP64, rt.OA_PREC_MIXED])
+def test_pcorr_assembly_parity_variable_density(oracle_mod, prec):
+    # the staged path: per-ip fluxes and corner coefficients from the mass-flow
+    # kernel, gathered by the row kernel (FP32 matrix in the mixed form, whose
+    # rhs stays FP64)
+    m, oc, gm, gf = make_pair(oracle_mod, n=7, prec=prec)
+    random_state(m, oc, gf)
+    _variable_properties(m, oc, gf)
+    A_o, b_o = oc.assemble_pcorr()
+    A_g, b_g = gf.assemble_pcorr()
+    assert rel(A_g, A_o) < (TOL_ASM if prec == rt.OA_PREC_FP64 else 1e-6)
+    assert rel(b_g, b_o) < TOL_ASM
+
+
+@pytest.mark.parametrize("prec", [rt.OA_PREC_FP64, rt.OA_PREC_MIXED])
+def test_momentum_assembly_parity_variable_properties(oracle_mod, prec):
+    # the mixed form's fluxes are FP32 arithmetic (Jacobians on FP32 corner
+    # offsets, U and mu from an FP32 copy): matrix, rhs and DU (from the FP32
+    # diagonal) within 1e-5 of the FP64 oracle, norm-wise
+    m, oc, gm, gf = make_pair(oracle_mod, n=7, prec=prec)
+    random_state(m, oc, gf)
+    _variable_properties(m, oc, gf)
+    A_o, b_o = oc.assemble_momentum()
+    A_g, b_g = gf.assemble_momentum()
+    tol = TOL_ASM if prec == rt.OA_PREC_FP64 else 1e-5
+    assert rel(A_g, A_o) < tol
+    assert rel(b_g, b_o) < tol
+    assert rel(gf.get_field("du"), oc.field("du")) < tol
+
+
 def test_mdot_div_gradient_parity(oracle_mod):
     m, oc, gm, gf = make_pair(oracle_mod, n=7)
     random_state(m, oc, gf)
