@@ -50,20 +50,6 @@ def measured_peaks():
     return HBM_FALLBACK, "fallback"
 
 
-def traffic_from_profile(name):
-    """Per-launch DRAM bytes recorded from an ncu capture in profiles/ (or None)."""
-    p = os.path.join(ROOT, "profiles", name)
-    if not os.path.exists(p):
-        return None
-    for line in open(p):
-        if line.strip().startswith("traffic_bytes_per_launch:"):
-            try:
-                return float(line.split(":", 1)[1].split()[0])
-            except ValueError:
-                return None
-    return None
-
-
 class ClockSampler:
     FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
               "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
@@ -137,11 +123,10 @@ def run_ours(args, rank, world):
     gm = rt.Mesh(m)
 
     def make(prec):
-        # the mixed form replays its Krylov chunks as CUDA graphs; the plain FP64
-        # form launches every kernel from the host
-        graphs = 1 if (prec == rt.OA_PREC_MIXED and not args.no_graphs) else 0
+        # both forms replay their Krylov chunks as CUDA graphs, so the ratio of
+        # the two measures precision, not launch overhead
         f = rt.Flow(gm, rt.default_settings(precision=prec, pc_rtol=args.pc_rtol, mom_rtol=args.mom_rtol,
-                                            mom_maxit=args.mom_maxit, use_graphs=graphs))
+                                            mom_maxit=args.mom_maxit, use_graphs=0 if args.no_graphs else 1))
         f.set_field("U", U0)
         f.initialize()
         return f
@@ -219,10 +204,11 @@ def run_ours(args, rank, world):
     ms_e2e = e0.elapsed_time(e1)
     ms_e2e = max_over_ranks(ms_e2e, dev, world)
 
+    conv = converge(args, gm, U0, dev, world) if args.converge_iters > 0 else None
+
     peak, peak_kind = measured_peaks()
     alg = algorithmic_bytes_momentum(m.nn, m.ne, gm.nnz, True)
     achieved = alg / (t_mom * 1e-3) / 1e9
-    traffic = traffic_from_profile("momentum_assembly_mixed_128.md")
     value = world * args.steps / (ms_mixed * 1e-3)
     value64 = world * args.steps / (ms_64 * 1e-3)
     res = {
@@ -243,6 +229,7 @@ def run_ours(args, rank, world):
                    "mom_rtol": args.mom_rtol, "mom_maxit": args.mom_maxit, "l2": "inputs larger than L2 (no flush)",
                    "parallelism": f"replicas x{world}"},
         "fp64_outer_iters_per_s": value64,
+        "graphs": "Krylov chunks replayed as CUDA graphs in both forms" if not args.no_graphs else "off",
         "mixed_over_fp64": value / value64,
         "assembled_elems_per_s": {"mixed": 2 * m.ne / ((t_mom + t_pc) * 1e-3),
                                   "fp64": 2 * m.ne / ((t_mom64 + t_pc64) * 1e-3)},
@@ -255,13 +242,72 @@ def run_ours(args, rank, world):
         "pc_krylov": "GCR(2) with the AMG V-cycle (one V-cycle per iteration)",
         "roofline": {"bound": "hbm", "kernel": "k_momentum (mixed)", "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
-                     "algorithmic_bytes": alg, "traffic": traffic},
+                     "algorithmic_bytes": alg, "traffic": None,
+                     "traffic_ncu": "not measured in this run; per-launch DRAM bytes of an ncu capture of the same "
+                                    "kernel are in profiles/"},
+        "converge": conv,
         "e2e": {"value": world * args.steps / (ms_e2e * 1e-3), "unit": "outer_iters/s",
                 "h2d_bytes_per_step": 32 * m.nn, "d2h_bytes_per_step": 32 * m.nn},
         "gpu_launches": launches,
         "clocks": clk.summary(),
     }
     return res
+
+
+def converge(args, gm, U0, dev, world):
+    """Both forms from the same initial state for up to --converge-iters SIMPLE
+    outer iterations (or until the continuity residual, RMS of the nodal mass
+    imbalance / (rho U_lid h^2), falls to --converge-target). Device time of
+    every iteration on the flow's stream (CUDA events). Reports the time each
+    form needs to reach the smallest residual both reach (the target when both
+    get there), their ratio, and the mixed form's field error against the FP64
+    form after the same number of iterations."""
+    import torch
+
+    from openaccel_b200 import runtime as rt
+
+    out = {}
+    fields = {}
+    for name, prec in (("mixed", rt.OA_PREC_MIXED), ("fp64", rt.OA_PREC_FP64)):
+        f = rt.Flow(gm, rt.default_settings(precision=prec, pc_rtol=args.pc_rtol, mom_rtol=args.mom_rtol,
+                                            mom_maxit=args.mom_maxit, use_graphs=0 if args.no_graphs else 1))
+        f.set_field("U", U0)
+        f.initialize()
+        stream = torch.cuda.ExternalStream(f.stream_handle(), device=dev)
+        res, t = [], []
+        for _ in range(args.converge_iters):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            st = f.simple_iterate(1)[0]
+            e1.record(stream)
+            e1.synchronize()
+            t.append(e0.elapsed_time(e1))
+            res.append(st["continuity_rms"])
+            if st["continuity_rms"] <= args.converge_target:
+                break
+        fields[name] = (f.get_field("U"), f.get_field("p"), len(res))
+        out[name] = {"iters": len(res), "residual_first": res[0], "residual_last": res[-1], "residual_min": min(res),
+                     "ms_total": float(np.sum(t)), "cum_ms": np.cumsum(t), "res": np.array(res)}
+        f.close()
+    target = max(args.converge_target, out["mixed"]["residual_min"], out["fp64"]["residual_min"])
+    summary = {"target": args.converge_target, "max_iters": args.converge_iters,
+               "residual_definition": "RMS over nodes of the pressure-correction rhs before the solve / (rho U_lid h^2), "
+                                      "h = mean element edge length",
+               "common_residual": target}
+    t_to = {}
+    for name, o in out.items():
+        k = int(np.argmax(o["res"] <= target))
+        t_to[name] = float(o["cum_ms"][k])
+        summary[name] = {"iters_run": o["iters"], "residual_first": o["residual_first"],
+                         "residual_last": o["residual_last"], "iters_to_common": k + 1, "ms_to_common": t_to[name],
+                         "ms_per_iter": o["ms_total"] / o["iters"]}
+    summary["time_to_residual_ratio_fp64_over_mixed"] = t_to["fp64"] / t_to["mixed"]
+    (Um, pm, nm), (Ud, pd, nd) = fields["mixed"], fields["fp64"]
+    if nm == nd:
+        summary["field_err_mixed_vs_fp64"] = {
+            "iters": nm, "U": float(np.abs(Um - Ud).max() / np.abs(Ud).max()),
+            "p": float(np.abs(pm - pd).max() / max(np.abs(pd).max(), 1e-300))}
+    return summary
 
 
 def algorithmic_bytes_diffusion(nn, ne, nnz, mixed):
@@ -349,7 +395,7 @@ def run_conduction(args, rank, world):
                                "mixed)",
                      "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind, "algorithmic_bytes": alg,
-                     "traffic": traffic_from_profile("tet4_assembly_conduction96.md") if args.n == 96 else None},
+                     "traffic": None},
         "gpu_launches": launches,
         "clocks": clk.summary(),
     }
@@ -479,7 +525,7 @@ def run_sst(args, rank, world):
                    "l2": "inputs larger than L2 (no flush)"},
         "roofline": {"bound": "hbm", "kernel": "k_sst_nodes", "achieved": alg / t / 1e9, "peak": peak, "unit": "GB/s",
                      "frac": alg / t / 1e9 / peak, "peak_kind": peak_kind, "algorithmic_bytes": alg,
-                     "traffic": traffic_from_profile("k_sst_nodes_channel256.md")},
+                     "traffic": None},
         "gpu_launches": rt.launch_count() - l0, "clocks": clk.summary(),
     }
 
@@ -531,6 +577,9 @@ def main():
                     help="cavity: the headline SIMPLE workload; conduction: the tet4 diffusion case (--n 96); "
                          "batch: 64 independent cavities, batched mixed form against a loop over the FP64 form")
     ap.add_argument("--batch-count", type=int, default=64)
+    ap.add_argument("--converge-iters", type=int, default=200,
+                    help="outer iterations of the time-to-residual comparison (0: skip it)")
+    ap.add_argument("--converge-target", type=float, default=1e-8)
     ap.add_argument("--diff-rtol", type=float, default=1e-10)
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", 0))

@@ -57,14 +57,48 @@ typedef struct oa_flow_settings {
   int use_graphs;               /* 1: replay Krylov iteration chunks as CUDA graphs */
 } oa_flow_settings;
 
+/* Convergence record of one linear solve: the ControlData that liblinsolve
+ * hands to linearSystem::convergenceReport_ (src/equation/linearSystem.h:464-571,
+ * fields read at :473-488). Component i is velocity component i for the
+ * momentum system and [0] for the scalar pressure correction (the other
+ * entries are 0). Residuals are RMS over the rows of the component:
+ *   solver_initial_res[i] = RMS_i(b - A x0), x0 = 0 (defect form), i.e. RMS_i(b);
+ *   solver_final_res[i]   = RMS_i of the solver's residual at exit (the FP64
+ *                           residual b - A x of the last refinement pass in
+ *                           the mixed pressure solve);
+ *   scaled_initial_res[i] = solver_initial_res[i] / flux scale, with the
+ *                           mass-flux scale rho U_ref h^2 (pressure correction:
+ *                           this is the continuity residual) and the
+ *                           momentum-flux scale rho U_ref^2 h^2 (momentum);
+ *                           rho = settings.rho, U_ref = the largest wall speed
+ *                           given to oa_flow_create (1 when every wall is at
+ *                           rest), h = the mean element edge length.
+ * The reference multiplies scaled_initial_res by its residual_scales
+ * (1 / field scale, navierStokesEquation.cpp:230-238,
+ * pressureCorrectionEquation.cpp:165-169) to form the control residual; the
+ * scale normalisation inside liblinsolve is not in the reference checkout, so
+ * the one above is this library's definition. */
+typedef struct oa_control_data {
+  int n_iterations;               /* Krylov iterations (GCR(2): V-cycles; BiCGStab: two per iteration) */
+  int fallback;                   /* 1 when a stagnated GCR(2) solve was finished by BiCGStab */
+  double solver_initial_res[3];
+  double solver_final_res[3];
+  double scaled_initial_res[3];
+} oa_control_data;
+
 typedef struct oa_iter_stats {
   int mom_iters, pc_iters, pc_refinements;
-  double mom_res, pc_res;
-  double continuity_rms;        /* RMS of the pressure-correction rhs before the solve */
+  double mom_res, pc_res;         /* relative residuals ||r|| / ||b|| at exit */
+  /* continuity residual: RMS over nodes of the pressure-correction rhs (the
+   * nodal mass imbalance) before the solve, divided by rho U_ref h^2 (see
+   * oa_control_data); continuity_rms_raw is the RMS itself */
+  double continuity_rms;
   /* device time of the iteration's phases in ms (CUDA events on the flow's
    * stream), the counterpart of the reference's Profiler push/pop around
    * assembly and solve (src/equation/linearSystem.h:452-454) */
   double ms_momentum_assembly, ms_momentum_solve, ms_pcorr_assembly, ms_pcorr_solve, ms_corrections;
+  double continuity_rms_raw;
+  oa_control_data mom, pc;        /* ControlData of the iteration's two solves */
 } oa_iter_stats;
 
 /* Last error message of the calling thread ("" when none). */
@@ -140,6 +174,14 @@ int oa_update_gradient(oa_flow* f, int which);
  * iters counts Krylov iterations of the method in use (GCR(2): one
  * preconditioner application each; BiCGStab: two). */
 int oa_solve(oa_flow* f, int sys, double rtol, int maxit, double* x, int* iters, double* res);
+/* ControlData of the last solve of system sys (0 momentum, 1 pressure
+ * correction) made by oa_solve or oa_simple_iterate: Context::getControlData()
+ * as linearSystem::convergenceReport_ reads it (src/equation/linearSystem.h:473-488).
+ * OA_ERR_NOT_READY before the first solve of that system. */
+int oa_flow_last_control(oa_flow* f, int sys, oa_control_data* out);
+/* Residual scales of the flow: U_ref, the mass-flux scale rho U_ref h^2 and the
+ * momentum-flux scale rho U_ref^2 h^2 (see oa_control_data); any pointer may be NULL. */
+int oa_flow_scales(oa_flow* f, double* u_ref, double* mass_scale, double* mom_scale);
 /* n SIMPLE outer iterations: segregatedFlowEquations::solve
  * (src/equation/flow/segregatedFlowEquations.cpp:76-297). stats may be NULL. */
 int oa_simple_iterate(oa_flow* f, int n, oa_iter_stats* stats);
@@ -157,19 +199,24 @@ int oa_launch_count(long long* count);
 int oa_time_kernel(oa_flow* f, int which, int reps, double* ms_per_launch);
 
 /* Allocation-free pressure-correction solve. No counterpart in the reference:
- * it exists for callers that cannot allocate device memory when they solve
- * (inside a CUDA stream capture, under an application that owns all device
- * memory, or in a plug-in that must not allocate). Everything is a device
- * pointer the caller owns: the CSR graph (row_ptr[nn+1], cols, diag = offset
- * of the diagonal within each row), A (FP64 values), b and the solution x
- * [nn]. BiCGStab with Jacobi preconditioning, FP64, to rtol relative to ||b||.
- * Its work vectors live in one file-scope device array sized for
+ * it exists for callers that cannot allocate device memory when they solve,
+ * such as a host application that reserves all device memory up front and
+ * hands out slices itself, or a solver plug-in called from a framework that
+ * forbids allocation on its hot path. Everything is a device pointer the
+ * caller owns: the CSR graph (row_ptr[nn+1], cols, diag = offset of the
+ * diagonal within each row), A (FP64 values), b and the solution x [nn].
+ * BiCGStab with Jacobi preconditioning, FP64, to rtol relative to ||b||. Its
+ * work vectors live in one file-scope device array sized for
  * OA_STATIC_SOLVE_MAX_ROWS rows (about 9.5 MB, held by every GPU that loads the
- * library until exit); larger systems are rejected with OA_ERR_ARG. All calls
- * on a device share that array, so calls that overlap on the GPU race: the
- * caller must serialise them. The first call on a device resolves the array's
- * device address and should not be made inside a stream capture. stream may be
- * NULL (default stream). */
+ * library until exit); larger systems are rejected with OA_ERR_ARG, and the
+ * call allocates nothing. All calls on a device share that array, so calls
+ * that overlap on the GPU race: the caller must serialise them. The first call
+ * on a device resolves the array's device address (cudaGetSymbolAddress) and
+ * caches it; make that first call before any stream capture. A breakdown, a
+ * diverging iteration or a solve that ends above rtol returns OA_ERR_SOLVER
+ * (oa_last_error names the status) with the last iterate in x. The call
+ * synchronises `stream` before it returns. stream may be NULL (default
+ * stream). */
 #define OA_STATIC_SOLVE_MAX_ROWS 131072
 int oa_pcorr_solve_static(int nn, const int* row_ptr, const int* cols, const int* diag, const double* A,
                           const double* b, double* x, double rtol, int maxit, int* iters, double* res,

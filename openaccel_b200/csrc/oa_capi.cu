@@ -52,7 +52,7 @@ struct oa_flow {
   KrylovSolver<3, double, double> mom64;
   KrylovSolver<3, float, float> mom32;
   ScalarSolve pc;           // pressure-correction solve
-  double* scal = nullptr;   // [4] device scalars
+  double* scal = nullptr;   // [8] device scalars
   double* hscal = nullptr;  // pinned
 };
 
@@ -111,37 +111,74 @@ double* field_ptr(Flow& f, const std::string& n, size_t* len) {
   return nullptr;
 }
 
+// Per-component RMS of the momentum rhs (initial residual, x0 = 0) and of the
+// solver's exit residual into the ControlData record.
+template <class T>
+int momentum_control(oa_flow* h, const T* b, const T* r, int iters) {
+  Flow& f = h->f;
+  const int nn = f.mesh->nn;
+  if (int s = device_comp_sumsq3<T>(nn, b, h->scal + 2, f.red, f.stream)) return s;
+  if (int s = device_comp_sumsq3<T>(nn, r, h->scal + 5, f.red, f.stream)) return s;
+  OA_CUDA(cudaMemcpyAsync(h->hscal + 2, h->scal + 2, 6 * sizeof(double), cudaMemcpyDeviceToHost, f.stream));
+  OA_CUDA(cudaStreamSynchronize(f.stream));
+  oa_control_data& cd = f.cd_mom;
+  cd = oa_control_data{};
+  cd.n_iterations = iters;
+  for (int k = 0; k < 3; ++k) {
+    cd.solver_initial_res[k] = std::sqrt(h->hscal[2 + k] / nn);
+    cd.solver_final_res[k] = std::sqrt(h->hscal[5 + k] / nn);
+    cd.scaled_initial_res[k] = cd.solver_initial_res[k] / f.mom_scale;
+  }
+  return OA_OK;
+}
+
 // Momentum solve: BiCGStab with 3x3 block Jacobi; U += x (correctField_ with
 // relaxation 1, navierStokesEquation.cpp:186-201).
 int solve_momentum(oa_flow* h, double rtol, int maxit, int* iters, double* res, bool apply) {
   Flow& f = h->f;
   DeviceMesh& m = *f.mesh;
   h->mom64.use_graph = h->mom32.use_graph = f.s.use_graphs != 0;
+  int it = 0;
   if (mixed(f)) {
     if (int s = h->mom32.setup(m.nn, m.row_ptr, m.cols, m.diag, f.stream)) return s;
     float* x = nullptr;
     if (int s = h->mom32.solve<float>(static_cast<const float*>(f.b.A_mom), static_cast<const float*>(f.b.b_mom), x,
-                                      rtol, maxit, iters, res, 10))
+                                      rtol, maxit, &it, res, 10))
       return s;
     k_to_double<float><<<(3 * m.nn + 255) / 256, 256, 0, f.stream>>>(3 * (size_t)m.nn, x, f.b.x_mom);
     count_launches(1);
+    if (int s = momentum_control<float>(h, static_cast<const float*>(f.b.b_mom), h->mom32.residual(), it)) return s;
   } else {
     if (int s = h->mom64.setup(m.nn, m.row_ptr, m.cols, m.diag, f.stream)) return s;
     double* x = nullptr;
     if (int s = h->mom64.solve<double>(static_cast<const double*>(f.b.A_mom),
-                                       static_cast<const double*>(f.b.b_mom), x, rtol, maxit, iters, res, 10))
+                                       static_cast<const double*>(f.b.b_mom), x, rtol, maxit, &it, res, 10))
       return s;
     OA_CUDA(cudaMemcpyAsync(f.b.x_mom, x, sizeof(double) * 3 * m.nn, cudaMemcpyDeviceToDevice, f.stream));
+    if (int s = momentum_control<double>(h, static_cast<const double*>(f.b.b_mom), h->mom64.residual(), it)) return s;
   }
+  if (iters) *iters = it;
   if (apply) k_axpy<<<(3 * m.nn + 255) / 256, 256, 0, f.stream>>>(3 * m.nn, f.U, f.b.x_mom, 1.0);
   count_launches(1);
   OA_CUDA(cudaGetLastError());
   return OA_OK;
 }
 
-// Pressure-correction solve into f.b.x_pc (ScalarSolve: FP64 BiCGStab, or
-// FP32 inner iterations under FP64 iterative refinement).
-int solve_pcorr(oa_flow* h, double rtol, int maxit, int* iters, double* res, int* refinements) {
+// RMS over nodes of the pressure-correction rhs (the nodal mass imbalance).
+int pc_rhs_rms(oa_flow* h, double* out) {
+  Flow& f = h->f;
+  if (int s = device_sumsq(f.mesh->nn, f.b.b_pc, h->scal + 2, f.red, f.stream)) return s;
+  OA_CUDA(cudaMemcpyAsync(h->hscal + 2, h->scal + 2, sizeof(double), cudaMemcpyDeviceToHost, f.stream));
+  OA_CUDA(cudaStreamSynchronize(f.stream));
+  *out = std::sqrt(h->hscal[2] / f.mesh->nn);
+  return OA_OK;
+}
+
+// Pressure-correction solve into f.b.x_pc (ScalarSolve: FP64 Krylov, or FP32
+// inner iterations under FP64 iterative refinement), with its ControlData
+// record. rhs_rms: RMS of the rhs when the caller has it already (< 0: formed
+// here).
+int solve_pcorr(oa_flow* h, double rtol, int maxit, int* iters, double* res, int* refinements, double rhs_rms = -1.0) {
   Flow& f = h->f;
   DeviceMesh& m = *f.mesh;
   ScalarGraph g;
@@ -152,16 +189,23 @@ int solve_pcorr(oa_flow* h, double rtol, int maxit, int* iters, double* res, int
   g.h_rp = m.h_row_ptr.data();
   g.h_cols = m.h_cols.data();
   g.h_diag = m.h_diag.data();
-  return h->pc.solve(g, mixed(f), f.s.pc_amg != 0, f.s.use_graphs != 0, f.b.A_pc, f.b.b_pc, f.b.x_pc, rtol, maxit,
-                     iters, res, refinements, f.stream, "pressure");
-}
-
-int continuity_rms(oa_flow* h, double* out) {
-  Flow& f = h->f;
-  if (int s = device_sumsq(f.mesh->nn, f.b.b_pc, h->scal + 2, f.red, f.stream)) return s;
-  OA_CUDA(cudaMemcpyAsync(h->hscal + 2, h->scal + 2, sizeof(double), cudaMemcpyDeviceToHost, f.stream));
-  OA_CUDA(cudaStreamSynchronize(f.stream));
-  *out = std::sqrt(h->hscal[2] / f.mesh->nn);
+  if (rhs_rms < 0)
+    if (int s = pc_rhs_rms(h, &rhs_rms)) return s;
+  const int fb0 = h->pc.fallbacks;
+  int it = 0;
+  double r = 0.0;
+  if (int s = h->pc.solve(g, mixed(f), f.s.pc_amg != 0, f.s.use_graphs != 0, f.b.A_pc, f.b.b_pc, f.b.x_pc, rtol,
+                          maxit, &it, &r, refinements, f.stream, "pressure"))
+    return s;
+  oa_control_data& cd = f.cd_pc;
+  cd = oa_control_data{};
+  cd.n_iterations = it;
+  cd.fallback = h->pc.fallbacks != fb0;
+  cd.solver_initial_res[0] = rhs_rms;
+  cd.solver_final_res[0] = r * rhs_rms;  // r = ||b - A x|| / ||b||, and x0 = 0
+  cd.scaled_initial_res[0] = rhs_rms / f.mass_scale;
+  if (iters) *iters = it;
+  if (res) *res = r;
   return OA_OK;
 }
 
@@ -244,6 +288,17 @@ int oa_mesh_create(const double* coords, int nn, const int* conn, int ne, int to
     m.h_row_ptr[i + 1] = (int)m.h_cols.size();
   }
   m.nnz = m.h_row_ptr[nn];
+  {
+    // mean element edge length (the 12 edges are the SCS L/R pairs)
+    double sum = 0.0;
+    for (int e = 0; e < ne; ++e)
+      for (int ip = 0; ip < 12; ++ip) {
+        const double* a = coords + 3L * conn[8L * e + LRt[ip][0]];
+        const double* b = coords + 3L * conn[8L * e + LRt[ip][1]];
+        sum += std::sqrt((a[0] - b[0]) * (a[0] - b[0]) + (a[1] - b[1]) * (a[1] - b[1]) + (a[2] - b[2]) * (a[2] - b[2]));
+      }
+    m.h_mean = sum / (12.0 * ne);
+  }
   m.h_conn.assign(conn, conn + 8L * ne);
   m.h_face_elem.assign(face_elem, face_elem + nf);
   m.h_face_ord.assign(face_ord, face_ord + nf);
@@ -329,6 +384,18 @@ int oa_flow_create(oa_mesh* M, const oa_flow_settings* s, const double* bnd_velo
   Flow& f = H->f;
   f.mesh = &M->m;
   f.s = *s;
+  {
+    double u = 0.0;
+    for (int k = 0; k < nbnd; ++k) {
+      const double* v = bnd_velocity + 3L * k;
+      u = std::max(u, std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]));
+    }
+    f.u_ref = u > 0.0 ? u : 1.0;
+    const double h2 = M->m.h_mean * M->m.h_mean;
+    f.mass_scale = s->rho * f.u_ref * h2;
+    f.mom_scale = s->rho * f.u_ref * f.u_ref * h2;
+    f.cd_mom.n_iterations = f.cd_pc.n_iterations = -1;  // no solve yet
+  }
   const size_t nn = M->m.nn, ne = M->m.ne, nnz = M->m.nnz;
   const size_t tm = s->precision == OA_PREC_MIXED ? sizeof(float) : sizeof(double);
   int st = OA_OK;
@@ -337,14 +404,14 @@ int oa_flow_create(oa_mesh* M, const oa_flow_settings* s, const double* bnd_velo
       (st = dalloc(&f.mDot, 12 * ne)) || (st = dalloc(&f.pc_flux, 12 * ne)) || (st = dalloc(&f.rho, nn)) ||
       (st = dalloc(&f.mu, nn)) ||
       (st = dalloc(&f.sideU, 3 * nn)) || (st = dalloc(&f.b.b_pc, nn)) || (st = dalloc(&f.b.x_mom, 3 * nn)) ||
-      (st = dalloc(&f.b.x_pc, nn)) || (st = dalloc(&f.err_dev, 1)) || (st = dalloc(&H->scal, 4)) ||
+      (st = dalloc(&f.b.x_pc, nn)) || (st = dalloc(&f.err_dev, 1)) || (st = dalloc(&H->scal, 8)) ||
       (st = dalloc(&f.red, (size_t)partials_size())) || (st = dalloc(&f.ref_flag, nn))) {
     oa_flow_destroy(H);
     return st;
   }
   if (cudaMalloc(&f.b.A_mom, tm * 9 * nnz) != cudaSuccess || cudaMalloc(&f.b.b_mom, tm * 3 * nn) != cudaSuccess ||
       cudaMalloc(&f.b.A_pc, tm * nnz) != cudaSuccess || cudaMalloc(&f.pc_coef, tm * 24 * ne) != cudaSuccess ||
-      cudaMallocHost(&H->hscal, 4 * sizeof(double)) != cudaSuccess ||
+      cudaMallocHost(&H->hscal, 8 * sizeof(double)) != cudaSuccess ||
       (s->precision == OA_PREC_MIXED && (cudaMalloc(&f.xloc32, sizeof(float4) * 8 * ne) != cudaSuccess ||
                                          cudaMalloc(&f.umu32, sizeof(float4) * nn) != cudaSuccess))) {
     oa_flow_destroy(H);
@@ -564,11 +631,14 @@ int oa_simple_iterate(oa_flow* H, int n, oa_iter_stats* stats) {
     nvtxRangePushA("mass flow and pressure-correction assembly");
     if (!s) s = launch_update_mdot(f, true);
     if (!s) s = launch_pcorr(f, mx, true);
-    if (!s) s = continuity_rms(H, &st.continuity_rms);
+    if (!s) s = pc_rhs_rms(H, &st.continuity_rms_raw);
+    st.continuity_rms = st.continuity_rms_raw / f.mass_scale;
     nvtxRangePop();
     mark(3);
     nvtxRangePushA("pressure-correction solve");
-    if (!s) s = solve_pcorr(H, f.s.pc_rtol, f.s.pc_maxit, &st.pc_iters, &st.pc_res, &st.pc_refinements);
+    if (!s)
+      s = solve_pcorr(H, f.s.pc_rtol, f.s.pc_maxit, &st.pc_iters, &st.pc_res, &st.pc_refinements,
+                      st.continuity_rms_raw);
     nvtxRangePop();
     mark(4);
     // corrections
@@ -592,6 +662,8 @@ int oa_simple_iterate(oa_flow* H, int n, oa_iter_stats* stats) {
       st.ms_pcorr_assembly = t[2];
       st.ms_pcorr_solve = t[3];
       st.ms_corrections = t[4];
+      st.mom = f.cd_mom;
+      st.pc = f.cd_pc;
       stats[it] = st;
     }
   }
@@ -599,6 +671,22 @@ int oa_simple_iterate(oa_flow* H, int n, oa_iter_stats* stats) {
     for (auto& e : ev)
       if (e) cudaEventDestroy(e);
   return s;
+}
+
+int oa_flow_last_control(oa_flow* H, int sys, oa_control_data* out) {
+  if (!H || !out || (sys != 0 && sys != 1)) return fail(OA_ERR_ARG, "oa_flow_last_control: bad arguments");
+  const oa_control_data& cd = sys == 0 ? H->f.cd_mom : H->f.cd_pc;
+  if (cd.n_iterations < 0) return fail(OA_ERR_NOT_READY, "oa_flow_last_control: no solve of this system yet");
+  *out = cd;
+  return OA_OK;
+}
+
+int oa_flow_scales(oa_flow* H, double* u_ref, double* mass_scale, double* mom_scale) {
+  if (!H) return fail(OA_ERR_ARG, "oa_flow_scales: null handle");
+  if (u_ref) *u_ref = H->f.u_ref;
+  if (mass_scale) *mass_scale = H->f.mass_scale;
+  if (mom_scale) *mom_scale = H->f.mom_scale;
+  return OA_OK;
 }
 
 int oa_flow_stream(oa_flow* H, void** stream) {

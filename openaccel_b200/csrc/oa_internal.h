@@ -41,6 +41,9 @@ struct MeshView {
 struct DeviceMesh : MeshView {
   int topo = OA_TOPO_HEX8;
   int geom_err = 0;
+  // mean element edge length (every element's 12 edges, summed in element
+  // order on the host): the h of the continuity-residual scale rho U_ref h^2
+  double h_mean = 0.0;
   // host copies needed for set-up and parity dumps
   std::vector<int> h_row_ptr, h_cols, h_diag;
   std::vector<int> h_conn, h_face_elem, h_face_ord, h_face_bnd;
@@ -82,8 +85,11 @@ struct Flow {
   double* red_host = nullptr;   // pinned
   int* err_dev = nullptr;       // device error flags
   uint8_t* ref_flag = nullptr;  // [nn] pressure-level rows (one per closed domain)
-  int last_mom_iters = 0, last_pc_iters = 0;
-  double last_mom_res = 0, last_pc_res = 0, last_cont = 0;
+  // residual scales: U_ref = largest wall speed (1 when all walls rest),
+  // mass-flux scale rho U_ref h^2, momentum-flux scale rho U_ref^2 h^2
+  double u_ref = 1.0, mass_scale = 1.0, mom_scale = 1.0;
+  // convergence record of the last momentum / pressure-correction solve
+  oa_control_data cd_mom{}, cd_pc{};
 };
 
 void set_error(const std::string& msg);

@@ -693,6 +693,39 @@ int device_sumsq(int n, const double* v, double* out, double* partials, cudaStre
 
 int partials_size() { return 3 * MAX_PARTIALS; }
 
+// per-component sums of squares of a [nn][3] vector (ordered two-stage tree)
+template <class T>
+__global__ void __launch_bounds__(KB) k_comp_sumsq3(int nn, const T* __restrict__ v, double* partials) {
+  double s[3] = {0.0, 0.0, 0.0};
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nn; i += gridDim.x * blockDim.x)
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const double a = double(v[3 * (size_t)i + k]);
+      s[k] += a * a;
+    }
+  block_reduce_store<3>(s, partials, MAX_PARTIALS);
+}
+
+__global__ void __launch_bounds__(KB) k_sum3_out(const double* partials, int nb, double* out) {
+  double o[3];
+  final_reduce<3>(partials, nb, o);
+  if (threadIdx.x == 0)
+    for (int k = 0; k < 3; ++k) out[k] = o[k];
+}
+
+template <class T>
+int device_comp_sumsq3(int nn, const T* v, double* out, double* partials, cudaStream_t st) {
+  const int gf = (nn + KB - 1) / KB;
+  const int g = gf < MAX_PARTIALS ? gf : MAX_PARTIALS;
+  k_comp_sumsq3<T><<<g, KB, 0, st>>>(nn, v, partials);
+  k_sum3_out<<<1, KB, 0, st>>>(partials, g, out);
+  count_launches(2);
+  OA_CUDA(cudaGetLastError());
+  return OA_OK;
+}
+template int device_comp_sumsq3<float>(int, const float*, double*, double*, cudaStream_t);
+template int device_comp_sumsq3<double>(int, const double*, double*, double*, cudaStream_t);
+
 template <class TV>
 int add_correction(int n, double* x, const TV* d, cudaStream_t st) {
   k_add_correction<TV><<<(n + KB - 1) / KB, KB, 0, st>>>(n, x, d);

@@ -34,6 +34,8 @@ struct KrylovSolver {
   bool external = false;
   alignas(16) unsigned char hbuf[128];  // host copy of the scalars when not pinned
 
+  // the solver's residual vector (b - A x, updated by recurrence) after solve()
+  const TV* residual() const { return static_cast<const TV*>(vec[1]); }
   int setup(int nn, const int* rp, const int* cols, const int* dg, cudaStream_t st);
   static size_t storage_bytes(int nn);
   int attach(int nn, const int* rp, const int* cols, const int* dg, cudaStream_t st, void* storage, size_t bytes);
@@ -57,6 +59,9 @@ int add_correction(int n, double* x, const TV* d, cudaStream_t st);
 // sum of squares of v into *out (device), ordered two-stage reduction;
 // partials must hold partials_size() doubles
 int device_sumsq(int n, const double* v, double* out, double* partials, cudaStream_t st);
+// per-component sums of squares of a [nn][3] vector into out[3] (device)
+template <class T>
+int device_comp_sumsq3(int nn, const T* v, double* out, double* partials, cudaStream_t st);
 int partials_size();
 
 }  // namespace oa

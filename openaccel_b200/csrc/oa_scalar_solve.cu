@@ -87,10 +87,14 @@ int ScalarSolve::solve(const ScalarGraph& g, bool mixed, bool amg, bool graphs, 
     if (int s = k64.solve<double>(static_cast<const double*>(A), b, xs, rtol, maxit, iters, res, check_every, reuse))
       return s;
     if (k64.gcr && k64.last_status == 1) {
-      // GCR stagnated or broke down: BiCGStab from now on, and for this system
+      // GCR stagnated or broke down: BiCGStab from now on, and for this system;
+      // the reported count includes the GCR iterations already spent
       gcr = false;
       k64.gcr = false;
+      const int spent = iters ? *iters : 0;
       if (int s = k64.solve<double>(static_cast<const double*>(A), b, xs, rtol, maxit, iters, res, 5, true)) return s;
+      if (iters) *iters += spent;
+      ++fallbacks;
     }
     OA_CUDA(cudaMemcpyAsync(x, xs, sizeof(double) * g.nn, cudaMemcpyDeviceToDevice, st));
     if (refinements) *refinements = 0;
@@ -103,6 +107,7 @@ int ScalarSolve::solve(const ScalarGraph& g, bool mixed, bool amg, bool graphs, 
   OA_CUDA(cudaMemcpyAsync(hscal, scal, sizeof(double), cudaMemcpyDeviceToHost, st));
   OA_CUDA(cudaStreamSynchronize(st));
   const double bnorm = std::sqrt(hscal[0]);
+  if (!(bnorm < INFINITY)) return fail(OA_ERR_SOLVER, std::string(what) + ": non-finite right-hand side");
   int total = 0, nref = 0;
   double rel = bnorm > 0 ? 1.0 : 0.0;
   OA_CUDA(cudaMemcpyAsync(r, b, sizeof(double) * g.nn, cudaMemcpyDeviceToDevice, st));
@@ -127,6 +132,7 @@ int ScalarSolve::solve(const ScalarGraph& g, bool mixed, bool amg, bool graphs, 
       gcr = false;
       k32.gcr = false;
       check_every = 5;
+      ++fallbacks;
     }
     // a diverged inner solve contributes nothing; the next pass restarts from
     // the FP64 residual

@@ -55,6 +55,9 @@ struct ScalarSolve {
   // refresh 4)
   int gcr_chunk = 2;
   long long solves = 0;
+  // GCR(2) solves that stagnated and were finished by BiCGStab (in either
+  // precision); reported so callers can see the switch happen
+  int fallbacks = 0;
 
   int init(int n);
   // A: const double* (mixed = false) or const float* (mixed = true); b and x

@@ -1,13 +1,15 @@
 // Allocation-free pressure-correction solve.
 //
 // Some callers cannot allocate device memory at the point where they need a
-// solve: code running inside a CUDA stream capture (cudaMalloc is not a
-// capturable operation), host applications that reserve the whole device up
-// front and hand out slices themselves, and solver plug-ins called from a
-// framework that forbids allocation on its hot path. oa_pcorr_solve_static
-// serves them: the caller passes the system and the solution in device memory
-// it already owns, and the BiCGStab work vectors live in one file-scope device
-// array of fixed size instead of cudaMalloc'd buffers.
+// solve: host applications that reserve the whole device up front and hand
+// out slices of it themselves (a cudaMalloc would fail or break their
+// accounting), and solver plug-ins called from a framework that forbids
+// allocation on its hot path (an allocation there can synchronise the device
+// or fragment the pool the framework manages). oa_pcorr_solve_static serves
+// them: the caller passes the system and the solution in device memory it
+// already owns, and the BiCGStab work vectors live in one file-scope device
+// array of fixed size instead of cudaMalloc'd buffers. Nothing here calls
+// cudaMalloc, cudaFree or an allocating library routine.
 //
 // Limits and sharing rules:
 //  - at most OA_STATIC_SOLVE_MAX_ROWS rows; larger systems are rejected;
@@ -16,11 +18,17 @@
 //  - every call on a device uses the same array, so calls whose work overlaps
 //    on the GPU (different streams or threads) race and corrupt each other;
 //    serialise them. The array keeps the previous call's contents; the solver
-//    overwrites every region it reads before reading it.
+//    overwrites every region it reads before reading it (the iterate and the
+//    search directions start from zero fills it issues itself);
 //  - the first call on a device looks up the array's device address
-//    (cudaGetSymbolAddress); make that first call outside any stream capture.
+//    (cudaGetSymbolAddress) and caches it; make that first call before any
+//    stream capture;
+//  - a breakdown, a diverging iteration or a solve that ends above rtol
+//    returns OA_ERR_SOLVER (the status is named in oa_last_error); x then
+//    holds the last iterate.
 #include <cuda_runtime.h>
 
+#include <cstdio>
 #include <mutex>
 
 #include "oa_internal.h"
@@ -74,11 +82,22 @@ extern "C" int oa_pcorr_solve_static(int nn, const int* row_ptr, const int* cols
   oa::KrylovSolver<1, double, double> ks;  // no storage of its own: attached below
   if (int s = ks.attach(nn, row_ptr, cols, diag, st, scratch, sizeof(double) * kScratchDoubles)) return s;
   double* xs = nullptr;
-  const int s = ks.solve<double>(A, b, xs, rtol, maxit, iters, res, 20);
+  double r = 0.0;
+  int s = ks.solve<double>(A, b, xs, rtol, maxit, iters, &r, 20);
+  if (res) *res = r;
   if (s == OA_OK) {
     cudaError_t e = cudaMemcpyAsync(x, xs, sizeof(double) * nn, cudaMemcpyDeviceToDevice, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-    if (e != cudaSuccess) return oa::fail(OA_ERR_CUDA, std::string("oa_pcorr_solve_static: ") + cudaGetErrorString(e));
+    if (e != cudaSuccess) s = oa::fail(OA_ERR_CUDA, std::string("oa_pcorr_solve_static: ") + cudaGetErrorString(e));
+  }
+  if (s == OA_OK && (ks.last_status == 1 || ks.last_status == 3 || !(r <= rtol))) {
+    const char* why = ks.last_status == 1 ? "breakdown (status 1)"
+                      : ks.last_status == 3 ? "diverging residual (status 3)"
+                                            : "not converged within maxit (status 0)";
+    char msg[160];
+    std::snprintf(msg, sizeof msg, "oa_pcorr_solve_static: BiCGStab %s, relative residual %.3e > rtol %.3e", why, r,
+                  rtol);
+    s = oa::fail(OA_ERR_SOLVER, msg);
   }
   ks.release();
   return s;

@@ -99,26 +99,28 @@ def block_faces(nx, ny, nz):
 
 
 def cavity(n, perturb=0.0, seed=12345, lid_velocity=(1.0, 0.0, 0.0)):
-    """Lid-driven cavity on the unit cube with n^3 hex8 elements.
+    """Lid-driven cavity on the unit cube with n^3 hex8 elements (or nx*ny*nz
+    when n is a triple).
 
     Boundary 0 is the lid (z = 1) moving with ``lid_velocity``; boundary 1 is
     the other five no-slip faces. Boundary 1 is applied last, so the lid's edge
     nodes carry zero wall velocity (the cavity example lists the lid first).
     ``perturb`` displaces interior nodes by U(-perturb*h, perturb*h) per
-    coordinate (numpy PCG64 stream ``seed``).
+    coordinate (numpy PCG64 stream ``seed``; h = 1/n, the x spacing of a box).
     """
-    coords, conn = hex_block(n, n, n)
+    nx, ny, nz = (n, n, n) if np.isscalar(n) else (int(v) for v in n)
+    coords, conn = hex_block(nx, ny, nz)
     if perturb > 0.0:
-        h = 1.0 / n
+        h = 1.0 / nx
         rng = np.random.Generator(np.random.PCG64(seed))
         noise = rng.uniform(-perturb * h, perturb * h, size=coords.shape)
         idx = np.arange(coords.shape[0])
-        i = idx % (n + 1)
-        j = (idx // (n + 1)) % (n + 1)
-        k = idx // ((n + 1) * (n + 1))
-        interior = (i > 0) & (i < n) & (j > 0) & (j < n) & (k > 0) & (k < n)
+        i = idx % (nx + 1)
+        j = (idx // (nx + 1)) % (ny + 1)
+        k = idx // ((nx + 1) * (ny + 1))
+        interior = (i > 0) & (i < nx) & (j > 0) & (j < ny) & (k > 0) & (k < nz)
         coords[interior] += noise[interior]
-    faces = block_faces(n, n, n)
+    faces = block_faces(nx, ny, nz)
     fe, fo, fb = [], [], []
     for side in ["z+"]:
         e, o = faces[side]
@@ -128,7 +130,7 @@ def cavity(n, perturb=0.0, seed=12345, lid_velocity=(1.0, 0.0, 0.0)):
         fe.append(e), fo.append(np.full_like(e, o)), fb.append(np.ones_like(e))
     bnd_velocity = np.array([list(lid_velocity), [0.0, 0.0, 0.0]], dtype=np.float64)
     return HexMesh(
-        n, n, n, coords, conn,
+        nx, ny, nz, coords, conn,
         np.concatenate(fe).astype(np.int32), np.concatenate(fo).astype(np.int32),
         np.concatenate(fb).astype(np.int32), bnd_velocity,
         meta={"kind": "cavity", "n": n, "perturb": perturb, "seed": seed},

@@ -31,6 +31,7 @@ EXPORTS = [
     "oa_diffusion_create", "oa_diffusion_destroy", "oa_diffusion_set_field", "oa_diffusion_get_field",
     "oa_diffusion_field_device_ptr", "oa_diffusion_assemble", "oa_diffusion_solve", "oa_diffusion_step",
     "oa_diffusion_stream", "oa_diffusion_time_assembly", "oa_sst_default_constants", "oa_sst_node_update",
+    "oa_flow_last_control", "oa_flow_scales",
 ]
 
 OA_BND_FIXED_VALUE = 0
@@ -57,11 +58,27 @@ class FlowSettings(C.Structure):
 PHASES = ("ms_momentum_assembly", "ms_momentum_solve", "ms_pcorr_assembly", "ms_pcorr_solve", "ms_corrections")
 
 
+class ControlData(C.Structure):
+    """oa_control_data: the ControlData of one linear solve
+    (src/equation/linearSystem.h:473-488)."""
+    _fields_ = [
+        ("n_iterations", C.c_int), ("fallback", C.c_int), ("solver_initial_res", C.c_double * 3),
+        ("solver_final_res", C.c_double * 3), ("scaled_initial_res", C.c_double * 3),
+    ]
+
+    def as_dict(self):
+        return dict(n_iterations=self.n_iterations, fallback=self.fallback,
+                    solver_initial_res=list(self.solver_initial_res), solver_final_res=list(self.solver_final_res),
+                    scaled_initial_res=list(self.scaled_initial_res))
+
+
 class IterStats(C.Structure):
     _fields_ = [
         ("mom_iters", C.c_int), ("pc_iters", C.c_int), ("pc_refinements", C.c_int),
         ("mom_res", C.c_double), ("pc_res", C.c_double), ("continuity_rms", C.c_double),
-    ] + [(n, C.c_double) for n in PHASES]
+    ] + [(n, C.c_double) for n in PHASES] + [
+        ("continuity_rms_raw", C.c_double), ("mom", ControlData), ("pc", ControlData),
+    ]
 
 
 class DiffusionSettings(C.Structure):
@@ -145,6 +162,8 @@ def lib():
         "oa_update_gradient": (C.c_int, [vp, C.c_int]),
         "oa_solve": (C.c_int, [vp, C.c_int, C.c_double, C.c_int, dp, ip, dp]),
         "oa_simple_iterate": (C.c_int, [vp, C.c_int, P(IterStats)]),
+        "oa_flow_last_control": (C.c_int, [vp, C.c_int, P(ControlData)]),
+        "oa_flow_scales": (C.c_int, [vp, dp, dp, dp]),
         "oa_flow_sync": (C.c_int, [vp]),
         "oa_flow_stream": (C.c_int, [vp, P(vp)]),
         "oa_launch_count": (C.c_int, [P(C.c_longlong)]),
@@ -306,7 +325,20 @@ class Flow:
         _check(lib().oa_simple_iterate(self.h, n, st))
         return [dict(mom_iters=s.mom_iters, pc_iters=s.pc_iters, pc_refinements=s.pc_refinements,
                      mom_res=s.mom_res, pc_res=s.pc_res, continuity_rms=s.continuity_rms,
+                     continuity_rms_raw=s.continuity_rms_raw, mom=s.mom.as_dict(), pc=s.pc.as_dict(),
                      **{k: getattr(s, k) for k in PHASES}) for s in st[:n]]
+
+    def last_control(self, sys):
+        """ControlData of the last solve of ``sys`` ("momentum"/0 or "pcorr"/1)."""
+        cd = ControlData()
+        _check(lib().oa_flow_last_control(self.h, 0 if sys in (0, "momentum") else 1, C.byref(cd)))
+        return cd.as_dict()
+
+    def scales(self):
+        """(U_ref, mass-flux scale rho U_ref h^2, momentum-flux scale rho U_ref^2 h^2)."""
+        u, m, mo = C.c_double(), C.c_double(), C.c_double()
+        _check(lib().oa_flow_scales(self.h, C.byref(u), C.byref(m), C.byref(mo)))
+        return u.value, m.value, mo.value
 
     def sync(self):
         _check(lib().oa_flow_sync(self.h))

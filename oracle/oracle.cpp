@@ -68,6 +68,9 @@ struct Case {
   std::vector<int> refNodes;
   // last assembled systems (for the solver inside simple_iteration)
   std::vector<double> Am, bm, xm, Ap, bp, xp;
+  // continuity-residual scale rho U_ref h^2 (the residual normalisation of
+  // the cavity benchmark; the reference's own lives in the absent liblinsolve)
+  double massScale = 1.0;
 };
 
 // Greedy element colouring over shared nodes (built once per case).
@@ -709,7 +712,8 @@ void simple_iteration(Case& c, orc_iter_stats* st) {
   if (st) {
     double s2 = 0.0;
     for (int i = 0; i < c.nn; ++i) s2 += c.bp[i] * c.bp[i];
-    st->continuity_rms = std::sqrt(s2 / c.nn);
+    st->continuity_raw = std::sqrt(s2 / c.nn);
+    st->continuity_rms = st->continuity_raw / c.massScale;
   }
   const int pi = bicgstab(c, 1, c.Ap.data(), c.bp.data(), c.xp.data(), c.s.pc_rtol, c.s.pc_maxit, &res);
   for (int i = 0; i < c.nn; ++i) c.p[i] += c.s.urf_p * c.xp[i];
@@ -773,6 +777,23 @@ void* orc_case_create(int nn, int ne, const double* x, const int* conn, int nf, 
   c->sideU.assign(3L * nn, 0.0);
   c->wallNode.assign(nn, 0.0);
   if (s->ref_node >= 0) c->refNodes.push_back(s->ref_node);
+  {
+    // mean element edge length over every element's 12 edges (element order)
+    // and the largest wall speed
+    double sum = 0.0;
+    for (int e = 0; e < ne; ++e)
+      for (int ip = 0; ip < 12; ++ip) {
+        const double* a = &c->x[3L * c->conn[8L * e + oracle::hex8::LR[ip][0]]];
+        const double* b = &c->x[3L * c->conn[8L * e + oracle::hex8::LR[ip][1]]];
+        sum += std::sqrt((a[0] - b[0]) * (a[0] - b[0]) + (a[1] - b[1]) * (a[1] - b[1]) + (a[2] - b[2]) * (a[2] - b[2]));
+      }
+    const double h = sum / (12.0 * ne);
+    double u = 0.0;
+    for (int k = 0; k < nbnd; ++k)
+      u = std::max(u, std::sqrt(bnd_velocity[3 * k] * bnd_velocity[3 * k] + bnd_velocity[3 * k + 1] * bnd_velocity[3 * k + 1] +
+                                bnd_velocity[3 * k + 2] * bnd_velocity[3 * k + 2]));
+    c->massScale = s->rho * (u > 0.0 ? u : 1.0) * h * h;
+  }
   // node side velocity: boundaries applied in order, later ones overwrite shared
   // nodes (nodeField::updateBoundarySideFieldSpecifiedValue, setToValue per part)
   for (int bnd = 0; bnd < nbnd; ++bnd)
@@ -788,6 +809,8 @@ void* orc_case_create(int nn, int ne, const double* x, const int* conn, int nf, 
 }
 
 void orc_case_destroy(void* h) { delete static_cast<Case*>(h); }
+
+double orc_case_mass_scale(void* h) { return static_cast<Case*>(h)->massScale; }
 
 void orc_set_ref_nodes(void* h, const int* nodes, int n) {
   Case* c = static_cast<Case*>(h);

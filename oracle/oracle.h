@@ -46,7 +46,8 @@ typedef struct orc_iter_stats {
   double mom_res;
   int pc_iters;
   double pc_res;
-  double continuity_rms; /* RMS of the PC rhs before the solve */
+  double continuity_rms; /* RMS of the PC rhs before the solve / (rho U_ref h^2) */
+  double continuity_raw; /* the RMS itself */
 } orc_iter_stats;
 
 /* ---- stateless geometry kernels (per element) ---- */
@@ -66,6 +67,9 @@ void orc_set_ref_nodes(void* h, const int* nodes, int n);
  * receives the number of doubles. */
 double* orc_case_field(void* h, const char* name, long* len);
 int orc_case_nnz(void* h);
+/* continuity-residual scale rho U_ref h^2: rho = settings.rho, U_ref = largest
+ * wall speed (1 when every wall is at rest), h = mean element edge length */
+double orc_case_mass_scale(void* h);
 void orc_case_graph(void* h, int* row_ptr /*nn+1*/, int* cols /*nnz*/);
 
 /* initialisation: mDot from U, gradients, divergence */

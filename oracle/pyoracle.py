@@ -46,6 +46,7 @@ class IterStats(C.Structure):
         ("pc_iters", C.c_int),
         ("pc_res", C.c_double),
         ("continuity_rms", C.c_double),
+        ("continuity_raw", C.c_double),
     ]
 
 
@@ -118,6 +119,8 @@ def lib():
         L.orc_case_field.argtypes = [C.c_void_p, C.c_char_p, P(C.c_long)]
         L.orc_case_nnz.restype = C.c_int
         L.orc_case_nnz.argtypes = [C.c_void_p]
+        L.orc_case_mass_scale.restype = C.c_double
+        L.orc_case_mass_scale.argtypes = [C.c_void_p]
         L.orc_case_graph.argtypes = [C.c_void_p, ip, ip]
         for name in ["orc_initialize", "orc_update_mdot", "orc_update_div", "orc_update_grad_p",
                      "orc_update_grad_u"]:
@@ -262,7 +265,11 @@ class FlowCase:
         st = IterStats()
         lib().orc_simple_iteration(self.h, C.byref(st))
         return dict(mom_iters=st.mom_iters[0], mom_res=st.mom_res, pc_iters=st.pc_iters,
-                    pc_res=st.pc_res, continuity_rms=st.continuity_rms)
+                    pc_res=st.pc_res, continuity_rms=st.continuity_rms, continuity_raw=st.continuity_raw)
+
+    def mass_scale(self):
+        """Continuity-residual scale rho U_ref h^2 of the case."""
+        return lib().orc_case_mass_scale(self.h)
 
 
 def hex8_scs_areav(x):

@@ -1,0 +1,91 @@
+"""Failure paths of the C-ABI, driven by inputs made on the host (no device
+fault is provoked): each bad input must come back as its status code with a
+message, and the handle must stay usable where the reference's errorMsg
+convention would let a caller continue.
+
+- a non-finite value in the field state reaches the solvers as a non-finite
+  right-hand side -> OA_ERR_SOLVER (Krylov status 2), in both precisions;
+- a hex whose nodes are moved so that it turns inside out -> OA_ERR_GEOMETRY
+  (non-positive sub-control volume, the Jacobian determinant check of
+  hex_scv_det / hex_gradient_operator);
+- an oversize or non-converging allocation-free solve -> its status codes.
+"""
+import ctypes as C
+import dataclasses
+
+import numpy as np
+import pytest
+
+from openaccel_b200 import meshgen
+from openaccel_b200 import runtime as rt
+
+pytestmark = pytest.mark.gpu
+
+OA_ERR_MESH, OA_ERR_GEOMETRY, OA_ERR_SOLVER = 2, 3, 5
+
+
+@pytest.mark.parametrize("prec", [rt.OA_PREC_FP64, rt.OA_PREC_MIXED])
+def test_nan_state_is_a_solver_error(prec):
+    m = meshgen.cavity(5, perturb=0.2, seed=3)
+    gf = rt.Flow(rt.Mesh(m), rt.default_settings(precision=prec))
+    gf.initialize()
+    gf.simple_iterate(1)
+    p = gf.get_field("p")
+    p[17] = np.nan  # enters the Rhie-Chow fluxes of the pressure-correction rhs
+    gf.set_field("p", p)
+    gf.assemble_pcorr()
+    with pytest.raises(rt.OpenAccelError) as ei:
+        gf.solve("pcorr", 1e-8, 100)
+    assert ei.value.status == OA_ERR_SOLVER
+    assert "non-finite" in str(ei.value)
+    U = gf.get_field("U")
+    U[3 * 40] = np.inf
+    gf.set_field("U", U)
+    with pytest.raises(rt.OpenAccelError) as ei:
+        gf.simple_iterate(1)
+    assert ei.value.status == OA_ERR_SOLVER
+
+
+def test_inverted_hex_is_a_geometry_error():
+    m = meshgen.cavity(4)
+    x = m.coords.copy()
+    # push an interior node through the opposite faces of its elements
+    i = 2 + 5 * (2 + 5 * 2)
+    x[i] += np.array([0.9, 0.0, 0.0])
+    bad = dataclasses.replace(m, coords=x)
+    with pytest.raises(rt.OpenAccelError) as ei:
+        rt.Mesh(bad)
+    assert ei.value.status == OA_ERR_GEOMETRY
+    # a valid mesh is still accepted afterwards (no sticky error state)
+    rt.Mesh(m)
+
+
+def test_static_solve_reports_non_convergence():
+    import torch
+
+    m = meshgen.cavity(6, perturb=0.2, seed=21)
+    gm = rt.Mesh(m)
+    gf = rt.Flow(gm, rt.default_settings())
+    gf.initialize()
+    gf.simple_iterate(1)
+    A, b = gf.assemble_pcorr()
+    rp, cols = gm.graph()
+    diag = np.array([np.searchsorted(cols[rp[i]:rp[i + 1]], i) for i in range(m.nn)], dtype=np.int32)
+    d = {k: torch.from_numpy(v).to("cuda") for k, v in (("rp", rp), ("cols", cols), ("diag", diag), ("A", A),
+                                                          ("b", b))}
+    x = torch.zeros(m.nn, dtype=torch.float64, device="cuda")
+    L = rt.lib()
+    it, res = C.c_int(), C.c_double()
+    # two iterations cannot reach 1e-12: the call must say so
+    st = L.oa_pcorr_solve_static(m.nn, d["rp"].data_ptr(), d["cols"].data_ptr(), d["diag"].data_ptr(),
+                                 d["A"].data_ptr(), d["b"].data_ptr(), x.data_ptr(), 1e-12, 2, C.byref(it),
+                                 C.byref(res), None)
+    assert st == OA_ERR_SOLVER
+    assert b"not converged" in L.oa_last_error()
+    assert res.value > 1e-12
+    # a non-finite right-hand side is reported as such
+    d["b"][5] = float("nan")
+    st = L.oa_pcorr_solve_static(m.nn, d["rp"].data_ptr(), d["cols"].data_ptr(), d["diag"].data_ptr(),
+                                 d["A"].data_ptr(), d["b"].data_ptr(), x.data_ptr(), 1e-8, 50, C.byref(it),
+                                 C.byref(res), None)
+    assert st == OA_ERR_SOLVER

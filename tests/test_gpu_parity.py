@@ -221,3 +221,38 @@ def test_solver_parity(oracle_mod):
     x_g, it, res = gf.solve("pcorr", 1e-13, 5000)
     assert res < 1e-12
     assert rel(x_g, x_o) < 1e-10
+
+
+def test_scaled_continuity_and_control_data(oracle_mod):
+    """The continuity residual (RMS of the nodal mass imbalance / rho U_lid h^2)
+    matches the oracle's over three SIMPLE iterations, and the ControlData
+    records of the solves carry the reference's fields: the initial residual is
+    the RMS of the rhs (x0 = 0), the scaled one is that over the flux scale,
+    the final one is the solver's exit residual."""
+    m, oc, gm, gf = make_pair(oracle_mod, n=6, mom_rtol=1e-13, pc_rtol=1e-13)
+    oc.initialize()
+    gf.initialize()
+    u_ref, mass_scale, mom_scale = gf.scales()
+    assert u_ref == 1.0
+    assert mass_scale == pytest.approx(oc.mass_scale(), rel=1e-15)
+    assert mom_scale == pytest.approx(oc.mass_scale(), rel=1e-15)  # U_lid = 1
+    for _ in range(3):
+        so = oc.simple_iteration()
+        sg = gf.simple_iterate(1)[0]
+        assert sg["continuity_rms"] == pytest.approx(so["continuity_rms"], rel=1e-6)
+        assert sg["continuity_rms_raw"] == pytest.approx(so["continuity_raw"], rel=1e-6)
+    pc, mom = sg["pc"], sg["mom"]
+    assert pc["solver_initial_res"][0] == pytest.approx(sg["continuity_rms_raw"], rel=1e-14)
+    assert pc["scaled_initial_res"][0] == pytest.approx(sg["continuity_rms"], rel=1e-14)
+    assert pc["solver_final_res"][0] <= 1e-12 * pc["solver_initial_res"][0]
+    assert pc["n_iterations"] == sg["pc_iters"] and pc["fallback"] in (0, 1)
+    assert mom["n_iterations"] == sg["mom_iters"]
+    assert gf.last_control("pcorr") == pc
+    # momentum: initial residual per component = RMS of that component of b
+    A, b = gf.assemble_momentum()
+    gf.solve("momentum", 1e-10, 500)
+    cd = gf.last_control("momentum")
+    rms = np.sqrt(np.mean(b.reshape(-1, 3) ** 2, axis=0))
+    np.testing.assert_allclose(cd["solver_initial_res"], rms, rtol=1e-13)
+    np.testing.assert_allclose(cd["scaled_initial_res"], rms / mom_scale, rtol=1e-13)
+    assert np.linalg.norm(cd["solver_final_res"]) <= 1e-10 * np.linalg.norm(rms) * 1.0001

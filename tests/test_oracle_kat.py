@@ -144,3 +144,23 @@ def test_golden_fixture_regenerates(oracle_mod):
     cur = generate(oracle_mod)
     for k in g.files:
         np.testing.assert_array_equal(cur[k], g[k], err_msg=k)
+
+
+def test_continuity_scale_is_rho_ulid_h2(oracle_mod):
+    """The continuity residual is the RMS of the nodal mass imbalance divided by
+    rho U_lid h^2 (h = mean element edge length): exactly (1/n)^2 on the unit
+    cavity with a unit lid, and the numpy mean edge length on a skewed one."""
+    from openaccel_b200 import meshgen
+
+    m = meshgen.cavity(4)
+    c = oracle_mod.FlowCase(m, oracle_mod.default_settings(rho=1.0))
+    assert c.mass_scale() == pytest.approx(1.0 / 16.0, rel=1e-15)
+    m = meshgen.cavity(5, perturb=0.2, seed=9, lid_velocity=(0.0, 2.0, 0.0))
+    c = oracle_mod.FlowCase(m, oracle_mod.default_settings(rho=1.5))
+    lr = [(0, 1), (1, 2), (2, 3), (0, 3), (4, 5), (5, 6), (6, 7), (4, 7), (0, 4), (1, 5), (2, 6), (3, 7)]
+    x = m.coords[m.conn]
+    h = np.mean([np.linalg.norm(x[:, a] - x[:, b], axis=1) for a, b in lr])
+    assert c.mass_scale() == pytest.approx(1.5 * 2.0 * h * h, rel=1e-12)
+    c.initialize()
+    st = c.simple_iteration()
+    assert st["continuity_rms"] == pytest.approx(st["continuity_raw"] / c.mass_scale(), rel=1e-15)

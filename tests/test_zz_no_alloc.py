@@ -1,13 +1,16 @@
 """The allocation-free pressure-correction solve, oa_pcorr_solve_static.
 
-It is for callers that cannot allocate device memory when they solve (inside a
-stream capture, under an application that owns all device memory, in a
-plug-in that must not allocate): its work vectors live in a fixed file-scope
-device array instead of cudaMalloc'd buffers. These tests call it through the
-C-ABI on device buffers the test owns and check it against the regular
-entry point (oa_solve on the same assembled system), on two calls in a row
-with two different systems, so state left in the shared array by the first
-call cannot leak into the second. This file is collected last on purpose.
+It is for callers that cannot allocate device memory when they solve (an
+application that owns all device memory and hands out slices itself, a
+solver plug-in whose host framework forbids allocation on its hot path): its
+work vectors live in a fixed file-scope device array instead of cudaMalloc'd
+buffers. These tests call it through the C-ABI on device buffers the test
+owns and check it against the regular entry point (oa_solve on the same
+assembled system), on two calls in a row with two different systems, so state
+left in the shared array by the first call cannot leak into the second; once
+at a small size and once at exactly the row limit, where the carve-up of the
+static array is tightest, and at a row count that is not a multiple of 32.
+This file is collected last on purpose.
 """
 import ctypes as C
 
@@ -54,10 +57,14 @@ def _static_solve(dev, A, b):
     return x.cpu().numpy(), it.value, res.value
 
 
-def test_static_solve_matches_regular_solve_twice():
+@pytest.mark.parametrize("n", [24, 49, (63, 63, 31)])
+def test_static_solve_matches_regular_solve_twice(n):
     import torch
 
-    m = meshgen.cavity(24, perturb=0.2, seed=21)
+    m = meshgen.cavity(n, perturb=0.2, seed=21)
+    assert m.nn <= rt.OA_STATIC_SOLVE_MAX_ROWS
+    if not np.isscalar(n):
+        assert m.nn == rt.OA_STATIC_SOLVE_MAX_ROWS
     gm = rt.Mesh(m)
     gf = rt.Flow(gm, rt.default_settings())
     rp, cols = gm.graph()
