@@ -20,6 +20,7 @@
 #include <vector>
 
 #include "hex8_master.hpp"
+#include "pool.hpp"
 
 namespace {
 
@@ -30,22 +31,20 @@ constexpr double SMALL = 2.220446049250313e-16;  // src/basic/types.h:179
 
 int g_threads = 1;
 
+// Static-chunked parallel loop on the persistent pool (serial below 4096
+// items or with one thread).
 template <class F>
 void parallel_for(long n, F f) {
   if (g_threads <= 1 || n < 4096) {
     for (long i = 0; i < n; ++i) f(i);
     return;
   }
-  std::vector<std::thread> th;
-  const long chunk = (n + g_threads - 1) / g_threads;
-  for (int t = 0; t < g_threads; ++t) {
-    const long a = t * chunk, b = std::min(n, a + chunk);
-    if (a >= b) break;
-    th.emplace_back([=, &f] {
-      for (long i = a; i < b; ++i) f(i);
-    });
-  }
-  for (auto& x : th) x.join();
+  oracle::Pool& P = oracle::Pool::get();
+  P.run([&](int t) {
+    long lo, hi;
+    oracle::chunk_range(n, P.size(), t, &lo, &hi);
+    for (long i = lo; i < hi; ++i) f(i);
+  });
 }
 
 struct Case {
@@ -71,6 +70,9 @@ struct Case {
   // continuity-residual scale rho U_ref h^2 (the residual normalisation of
   // the cavity benchmark; the reference's own lives in the absent liblinsolve)
   double massScale = 1.0;
+  // linear solvers of simple_iteration: 0 Jacobi-BiCGStab (the parity
+  // reference), 1 the reference example's configuration (GMRES + block ILU(0))
+  int solverKind = 0;
 };
 
 // Greedy element colouring over shared nodes (built once per case).
@@ -110,17 +112,15 @@ double pdot(long n, const double* a, const double* b) {
     for (long i = 0; i < n; ++i) s += a[i] * b[i];
     return s;
   }
-  std::vector<double> part(g_threads, 0.0);
-  std::vector<std::thread> th;
-  const long chunk = (n + g_threads - 1) / g_threads;
-  for (int t = 0; t < g_threads; ++t)
-    th.emplace_back([&, t] {
-      const long lo = t * chunk, hi = std::min(n, lo + chunk);
-      double s = 0.0;
-      for (long i = lo; i < hi; ++i) s += a[i] * b[i];
-      part[t] = s;
-    });
-  for (auto& x : th) x.join();
+  oracle::Pool& P = oracle::Pool::get();
+  std::vector<double> part(P.size(), 0.0);
+  P.run([&](int t) {
+    long lo, hi;
+    oracle::chunk_range(n, P.size(), t, &lo, &hi);
+    double s = 0.0;
+    for (long i = lo; i < hi; ++i) s += a[i] * b[i];
+    part[t] = s;
+  });
   double s = 0.0;
   for (double v : part) s += v;
   return s;
@@ -620,28 +620,11 @@ void invert3(const double* a, double* r) {
 
 double dot(long n, const double* a, const double* b) { return pdot(n, a, b); }
 
-int bicgstab(const Case& c, int bs, const double* A, const double* b, double* x, double rtol,
-             int maxit, double* res) {
+// BiCGStab core with a right preconditioner prec(v, z): z = M^-1 v.
+template <class Prec>
+int bicgstab_core(const Case& c, int bs, const double* A, const double* b, double* x, double rtol, int maxit,
+                  double* res, Prec prec) {
   const long n = (long)bs * c.nn;
-  std::vector<double> Minv((long)bs * bs * c.nn);
-  for (int i = 0; i < c.nn; ++i) {
-    const double* d = &A[(long)bs * bs * (c.rowPtr[i] + c.diagOff[i])];
-    if (bs == 1)
-      Minv[i] = 1.0 / d[0];
-    else
-      invert3(d, &Minv[9L * i]);
-  }
-  auto prec = [&](const double* v, double* z) {
-    parallel_for(c.nn, [&](long i) {
-      if (bs == 1) {
-        z[i] = Minv[i] * v[i];
-      } else {
-        for (int m = 0; m < 3; ++m)
-          z[3 * i + m] = Minv[9L * i + 3 * m] * v[3 * i] + Minv[9L * i + 3 * m + 1] * v[3 * i + 1] +
-                         Minv[9L * i + 3 * m + 2] * v[3 * i + 2];
-      }
-    });
-  };
   std::vector<double> r(n), rh(n), pv(n, 0.0), v(n, 0.0), s(n), t(n), ph(n), sh(n);
   std::fill(x, x + n, 0.0);
   for (long i = 0; i < n; ++i) r[i] = b[i];
@@ -683,6 +666,238 @@ int bicgstab(const Case& c, int bs, const double* A, const double* b, double* x,
   return it;
 }
 
+// Jacobi (bs 1) or 3x3 block-Jacobi (bs 3) preconditioned BiCGStab.
+int bicgstab(const Case& c, int bs, const double* A, const double* b, double* x, double rtol, int maxit,
+             double* res) {
+  std::vector<double> Minv((long)bs * bs * c.nn);
+  for (int i = 0; i < c.nn; ++i) {
+    const double* d = &A[(long)bs * bs * (c.rowPtr[i] + c.diagOff[i])];
+    if (bs == 1)
+      Minv[i] = 1.0 / d[0];
+    else
+      invert3(d, &Minv[9L * i]);
+  }
+  auto prec = [&](const double* v, double* z) {
+    parallel_for(c.nn, [&](long i) {
+      if (bs == 1) {
+        z[i] = Minv[i] * v[i];
+      } else {
+        for (int m = 0; m < 3; ++m)
+          z[3 * i + m] = Minv[9L * i + 3 * m] * v[3 * i] + Minv[9L * i + 3 * m + 1] * v[3 * i + 1] +
+                         Minv[9L * i + 3 * m + 2] * v[3 * i + 2];
+      }
+    });
+  };
+  return bicgstab_core(c, bs, A, b, x, rtol, maxit, res, prec);
+}
+
+// ---------------------------------------------------------------------------
+// The reference cavity example's solver configuration
+// (examples/cavity/input.i:61-77): momentum by PETSc fgmres with bjacobi
+// (block Jacobi, ILU(0) on each block: PETSc's sub-solver default), pressure
+// correction by Trilinos Belos GMRES with Ifpack2 ILU (one ILU(0) block per
+// MPI rank). Restated from the published algorithms (Saad, Iterative Methods
+// for Sparse Linear Systems, 2nd ed.: ILU(0) Alg. 10.4 in its IKJ form,
+// restarted GMRES Alg. 6.9 with right preconditioning and Givens rotations):
+// one block of contiguous rows per thread, as one block per rank; couplings
+// to rows outside the block are dropped from the factors (block Jacobi);
+// block ILU(0) on the 3x3 blocks of the momentum BSR matrix.
+template <int B>
+struct BlockIlu0 {
+  const Case* c = nullptr;
+  int nblk = 1;
+  std::vector<double> lu;    // factors in the CSR layout of A (B*B per entry)
+  std::vector<double> dinv;  // inverse of each row's factored diagonal block
+
+  static void mul(const double* a, const double* b, double* out) {  // out = a b
+    for (int i = 0; i < B; ++i)
+      for (int j = 0; j < B; ++j) {
+        double s = 0.0;
+        for (int k = 0; k < B; ++k) s += a[B * i + k] * b[B * k + j];
+        out[B * i + j] = s;
+      }
+  }
+  static void inv(const double* a, double* r) {
+    if (B == 1)
+      r[0] = 1.0 / a[0];
+    else
+      invert3(a, r);
+  }
+
+  void factor(const Case& cs, const double* A, int blocks) {
+    c = &cs;
+    nblk = std::max(1, std::min(blocks, oracle::Pool::get().size()));
+    const long nnz = cs.rowPtr[cs.nn];
+    lu.assign(A, A + (long)B * B * nnz);
+    dinv.assign((long)B * B * cs.nn, 0.0);
+    auto body = [&](int t) {
+      long r0, r1;
+      oracle::chunk_range(cs.nn, nblk, t, &r0, &r1);
+      std::vector<int> w(std::max<long>(r1 - r0, 1), -1);
+      double tmp[B * B], upd[B * B];
+      for (long i = r0; i < r1; ++i) {
+        const int a = cs.rowPtr[i], e = cs.rowPtr[i + 1];
+        for (int k = a; k < e; ++k)
+          if (cs.cols[k] >= r0 && cs.cols[k] < r1) w[cs.cols[k] - r0] = k;
+        for (int k = a; k < e; ++k) {
+          const int j = cs.cols[k];
+          if (j >= i) break;
+          if (j < r0) continue;
+          // L_ij = A_ij U_jj^-1, then A_il -= L_ij U_jl for the kept l > j
+          mul(&lu[(long)B * B * k], &dinv[(long)B * B * j], tmp);
+          std::copy(tmp, tmp + B * B, &lu[(long)B * B * k]);
+          for (int kk = cs.rowPtr[j]; kk < cs.rowPtr[j + 1]; ++kk) {
+            const int cc = cs.cols[kk];
+            if (cc <= j || cc >= r1) continue;
+            const int pos = w[cc - r0];
+            if (pos < 0) continue;
+            mul(&lu[(long)B * B * k], &lu[(long)B * B * kk], upd);
+            for (int q = 0; q < B * B; ++q) lu[(long)B * B * pos + q] -= upd[q];
+          }
+        }
+        inv(&lu[(long)B * B * (a + cs.diagOff[i])], &dinv[(long)B * B * i]);
+        for (int k = a; k < e; ++k)
+          if (cs.cols[k] >= r0 && cs.cols[k] < r1) w[cs.cols[k] - r0] = -1;
+      }
+    };
+    if (nblk == 1)
+      body(0);
+    else
+      oracle::Pool::get().run([&](int t) {
+        if (t < nblk) body(t);
+      });
+  }
+
+  // z = (LU)^-1 v, each block on its own
+  void apply(const double* v, double* z) const {
+    const Case& cs = *c;
+    auto body = [&](int t) {
+      long r0, r1;
+      oracle::chunk_range(cs.nn, nblk, t, &r0, &r1);
+      for (long i = r0; i < r1; ++i) {  // L y = v (unit lower)
+        double y[B];
+        for (int m = 0; m < B; ++m) y[m] = v[B * i + m];
+        for (int k = cs.rowPtr[i]; k < cs.rowPtr[i + 1]; ++k) {
+          const int j = cs.cols[k];
+          if (j >= i) break;
+          if (j < r0) continue;
+          const double* L = &lu[(long)B * B * k];
+          for (int m = 0; m < B; ++m)
+            for (int q = 0; q < B; ++q) y[m] -= L[B * m + q] * z[B * j + q];
+        }
+        for (int m = 0; m < B; ++m) z[B * i + m] = y[m];
+      }
+      for (long i = r1 - 1; i >= r0; --i) {  // U x = y
+        double y[B];
+        for (int m = 0; m < B; ++m) y[m] = z[B * i + m];
+        for (int k = cs.rowPtr[i] + cs.diagOff[i] + 1; k < cs.rowPtr[i + 1]; ++k) {
+          const int j = cs.cols[k];
+          if (j >= r1) break;
+          const double* U = &lu[(long)B * B * k];
+          for (int m = 0; m < B; ++m)
+            for (int q = 0; q < B; ++q) y[m] -= U[B * m + q] * z[B * j + q];
+        }
+        const double* D = &dinv[(long)B * B * i];
+        for (int m = 0; m < B; ++m) {
+          double s = 0.0;
+          for (int q = 0; q < B; ++q) s += D[B * m + q] * y[q];
+          z[B * i + m] = s;
+        }
+      }
+    };
+    if (nblk == 1)
+      body(0);
+    else
+      oracle::Pool::get().run([&](int t) {
+        if (t < nblk) body(t);
+      });
+  }
+};
+
+// Restarted GMRES(m), right-preconditioned by block ILU(0); x0 = 0. Returns
+// the iteration count; *res = ||b - A x|| / ||b|| at exit.
+template <int B>
+int gmres_ilu(const Case& c, const double* A, const double* b, double* x, double rtol, int maxit, int m,
+              double* res) {
+  const long n = (long)B * c.nn;
+  BlockIlu0<B> M;
+  M.factor(c, A, g_threads);
+  std::fill(x, x + n, 0.0);
+  const double bn = std::sqrt(dot(n, b, b));
+  if (bn == 0.0) {
+    *res = 0.0;
+    return 0;
+  }
+  std::vector<double> V((long)(m + 1) * n), z(n), w(n), r(b, b + n);
+  std::vector<double> H((long)(m + 1) * m, 0.0), cs(m), sn(m), g(m + 1);
+  double beta = bn;
+  int it = 0;
+  while (true) {
+    for (int k = 0; k <= m; ++k) g[k] = 0.0;
+    g[0] = beta;
+    parallel_for(n, [&](long i) { V[i] = r[i] / beta; });
+    int j = 0;
+    for (; j < m && it < maxit;) {
+      M.apply(&V[(long)j * n], z.data());
+      spmv(c, B, A, z.data(), w.data());
+      for (int i = 0; i <= j; ++i) {  // modified Gram-Schmidt
+        const double* vi = &V[(long)i * n];
+        const double h = dot(n, w.data(), vi);
+        H[(long)i * m + j] = h;
+        parallel_for(n, [&](long q) { w[q] -= h * vi[q]; });
+      }
+      const double hn = std::sqrt(dot(n, w.data(), w.data()));
+      if (hn > 0.0) {
+        double* vj = &V[(long)(j + 1) * n];
+        parallel_for(n, [&](long q) { vj[q] = w[q] / hn; });
+      }
+      for (int i = 0; i < j; ++i) {  // earlier rotations on the new column
+        const double a = H[(long)i * m + j], bb = H[(long)(i + 1) * m + j];
+        H[(long)i * m + j] = cs[i] * a + sn[i] * bb;
+        H[(long)(i + 1) * m + j] = -sn[i] * a + cs[i] * bb;
+      }
+      const double a = H[(long)j * m + j];
+      const double d = std::sqrt(a * a + hn * hn);
+      cs[j] = d > 0.0 ? a / d : 1.0;
+      sn[j] = d > 0.0 ? hn / d : 0.0;
+      H[(long)j * m + j] = d;
+      g[j + 1] = -sn[j] * g[j];
+      g[j] = cs[j] * g[j];
+      ++it;
+      ++j;
+      if (std::fabs(g[j]) <= rtol * bn || hn == 0.0) break;
+    }
+    // y = H^-1 g (upper triangular j x j); x += M^-1 (V y)
+    std::vector<double> y(j, 0.0);
+    for (int i = j - 1; i >= 0; --i) {
+      double s = g[i];
+      for (int k = i + 1; k < j; ++k) s -= H[(long)i * m + k] * y[k];
+      y[i] = s / H[(long)i * m + i];
+    }
+    parallel_for(n, [&](long q) {
+      double s = 0.0;
+      for (int k = 0; k < j; ++k) s += y[k] * V[(long)k * n + q];
+      w[q] = s;
+    });
+    M.apply(w.data(), z.data());
+    parallel_for(n, [&](long q) { x[q] += z[q]; });
+    spmv(c, B, A, x, w.data());
+    parallel_for(n, [&](long q) { r[q] = b[q] - w[q]; });
+    beta = std::sqrt(dot(n, r.data(), r.data()));
+    if (beta <= rtol * bn || it >= maxit || !(beta < INFINITY)) break;
+  }
+  *res = beta / bn;
+  return it;
+}
+
+// BiCGStab right-preconditioned by block-Jacobi ILU(0) (one block per thread).
+template <int B>
+int bicgstab_ilu(const Case& c, const double* A, const double* b, double* x, double rtol, int maxit, double* res) {
+  BlockIlu0<B> M;
+  M.factor(c, A, g_threads);
+  return bicgstab_core(c, B, A, b, x, rtol, maxit, res, [&](const double* v, double* z) { M.apply(v, z); });
+}
+
 // ---------------------------------------------------------------------------
 // One SIMPLE outer iteration: segregatedFlowEquations::solve
 // (src/equation/flow/segregatedFlowEquations.cpp:76-297) with
@@ -700,7 +915,10 @@ void simple_iteration(Case& c, orc_iter_stats* st) {
   // momentum predictor
   assemble_momentum(c, c.Am.data(), c.bm.data());
   double res = 0.0;
-  const int mi = bicgstab(c, 3, c.Am.data(), c.bm.data(), c.xm.data(), c.s.mom_rtol, c.s.mom_maxit, &res);
+  const int mi =
+      c.solverKind == 1   ? gmres_ilu<3>(c, c.Am.data(), c.bm.data(), c.xm.data(), c.s.mom_rtol, c.s.mom_maxit, 30, &res)
+      : c.solverKind == 2 ? bicgstab_ilu<3>(c, c.Am.data(), c.bm.data(), c.xm.data(), c.s.mom_rtol, c.s.mom_maxit, &res)
+                          : bicgstab(c, 3, c.Am.data(), c.bm.data(), c.xm.data(), c.s.mom_rtol, c.s.mom_maxit, &res);
   for (long i = 0; i < 3L * c.nn; ++i) c.U[i] += c.xm[i];
   update_mdot(c);
   if (st) {
@@ -715,7 +933,10 @@ void simple_iteration(Case& c, orc_iter_stats* st) {
     st->continuity_raw = std::sqrt(s2 / c.nn);
     st->continuity_rms = st->continuity_raw / c.massScale;
   }
-  const int pi = bicgstab(c, 1, c.Ap.data(), c.bp.data(), c.xp.data(), c.s.pc_rtol, c.s.pc_maxit, &res);
+  const int pi =
+      c.solverKind == 1   ? gmres_ilu<1>(c, c.Ap.data(), c.bp.data(), c.xp.data(), c.s.pc_rtol, c.s.pc_maxit, 50, &res)
+      : c.solverKind == 2 ? bicgstab_ilu<1>(c, c.Ap.data(), c.bp.data(), c.xp.data(), c.s.pc_rtol, c.s.pc_maxit, &res)
+                          : bicgstab(c, 1, c.Ap.data(), c.bp.data(), c.xp.data(), c.s.pc_rtol, c.s.pc_maxit, &res);
   for (int i = 0; i < c.nn; ++i) c.p[i] += c.s.urf_p * c.xp[i];
   if (st) {
     st->pc_iters = pi;
@@ -734,7 +955,10 @@ void simple_iteration(Case& c, orc_iter_stats* st) {
 
 extern "C" {
 
-void orc_set_threads(int n) { g_threads = n < 1 ? 1 : n; }
+void orc_set_threads(int n) {
+  g_threads = n < 1 ? 1 : n;
+  oracle::Pool::get().resize(g_threads);
+}
 int orc_get_threads(void) { return g_threads; }
 
 void orc_hex8_scs_areav(const double* x, double* areav) { oracle::hex8::scs_areav(x, areav); }
@@ -886,5 +1110,14 @@ int orc_bicgstab(void* h, int bs, const double* A, const double* b, double* x, d
   return bicgstab(*static_cast<Case*>(h), bs, A, b, x, rtol, maxit, res);
 }
 void orc_simple_iteration(void* h, orc_iter_stats* st) { simple_iteration(*static_cast<Case*>(h), st); }
+
+void orc_set_solver(void* h, int kind) { static_cast<Case*>(h)->solverKind = (kind == 1 || kind == 2) ? kind : 0; }
+
+int orc_gmres_ilu(void* h, int bs, const double* A, const double* b, double* x, double rtol, int maxit, int restart,
+                  double* res) {
+  const Case& c = *static_cast<Case*>(h);
+  return bs == 3 ? gmres_ilu<3>(c, A, b, x, rtol, maxit, restart, res)
+                 : gmres_ilu<1>(c, A, b, x, rtol, maxit, restart, res);
+}
 
 }  // extern "C"

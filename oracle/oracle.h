@@ -89,6 +89,15 @@ int orc_bicgstab(void* h, int bs, const double* A, const double* b, double* x,
                  double rtol, int maxit, double* res);
 /* one SIMPLE outer iteration (segregatedFlowEquations::solve) */
 void orc_simple_iteration(void* h, orc_iter_stats* st);
+/* linear solvers of orc_simple_iteration: 0 = Jacobi-preconditioned BiCGStab
+ * (default, the parity reference), 1 = the reference cavity example's
+ * configuration (examples/cavity/input.i:61-77): momentum FGMRES(30) and
+ * pressure correction GMRES(50), both right-preconditioned by block-Jacobi
+ * ILU(0) with one block of contiguous rows per thread */
+void orc_set_solver(void* h, int kind);
+/* restarted GMRES with block-Jacobi ILU(0) on the case's graph (bs 1 or 3) */
+int orc_gmres_ilu(void* h, int bs, const double* A, const double* b, double* x, double rtol, int maxit,
+                  int restart, double* res);
 /* thread count used by the element loops and SpMV (1 = serial) */
 void orc_set_threads(int n);
 int orc_get_threads(void);

@@ -121,6 +121,11 @@ def lib():
         L.orc_case_nnz.argtypes = [C.c_void_p]
         L.orc_case_mass_scale.restype = C.c_double
         L.orc_case_mass_scale.argtypes = [C.c_void_p]
+        L.orc_set_solver.restype = None
+        L.orc_set_solver.argtypes = [C.c_void_p, C.c_int]
+        L.orc_gmres_ilu.restype = C.c_int
+        L.orc_gmres_ilu.argtypes = [C.c_void_p, C.c_int, P(C.c_double), P(C.c_double), P(C.c_double), C.c_double,
+                                    C.c_int, C.c_int, P(C.c_double)]
         L.orc_case_graph.argtypes = [C.c_void_p, ip, ip]
         for name in ["orc_initialize", "orc_update_mdot", "orc_update_div", "orc_update_grad_p",
                      "orc_update_grad_u"]:
@@ -266,6 +271,17 @@ class FlowCase:
         lib().orc_simple_iteration(self.h, C.byref(st))
         return dict(mom_iters=st.mom_iters[0], mom_res=st.mom_res, pc_iters=st.pc_iters,
                     pc_res=st.pc_res, continuity_rms=st.continuity_rms, continuity_raw=st.continuity_raw)
+
+    def set_solver(self, kind):
+        """0: Jacobi-BiCGStab (parity reference); 1 or "reference": the cavity
+        example's GMRES + block-Jacobi ILU(0) configuration."""
+        lib().orc_set_solver(self.h, {"reference": 1, "ilu-bicgstab": 2}.get(kind, kind))
+
+    def gmres_ilu(self, bs, A, b, rtol=1e-12, maxit=2000, restart=50):
+        x = np.zeros_like(b)
+        res = C.c_double(0)
+        it = lib().orc_gmres_ilu(self.h, bs, _dp(A), _dp(b), _dp(x), rtol, maxit, restart, C.byref(res))
+        return x, it, res.value
 
     def mass_scale(self):
         """Continuity-residual scale rho U_ref h^2 of the case."""

@@ -28,13 +28,14 @@ def rel(a, b):
 
 
 def _system(gf, seed):
-    """Assemble a pressure-correction system from a random (but valid) state."""
-    rng = np.random.default_rng(seed)
-    m = gf.mesh
-    gf.set_field("p", rng.normal(0, 1, m.nn))
-    gf.set_field("gradP", rng.normal(0, 1, 3 * m.nn))
-    gf.set_field("du", rng.uniform(0.1, 1.0, 3 * m.nn))
-    gf.set_field("mDot", rng.normal(0, 0.01, 12 * m.ne))
+    """Assemble the pressure-correction system of a flow state: a seeded
+    Gaussian initial velocity, one SIMPLE outer iteration, then the assembly
+    the next iteration would solve."""
+    m = gf.mesh.src
+    gf.set_field("U", meshgen.initial_velocity(m, sigma=0.1, seed=seed))
+    gf.set_field("p", np.zeros(m.nn))
+    gf.initialize()
+    gf.simple_iterate(1)
     A, b = gf.assemble_pcorr()
     x_ref, _, res_ref = gf.solve("pcorr", 1e-13, 5000)
     assert res_ref < 1e-12
