@@ -255,10 +255,11 @@ def converge(args, gm, U0, dev, world):
     """Both forms from the same initial state for up to --converge-iters SIMPLE
     outer iterations (or until the continuity residual, RMS of the nodal mass
     imbalance / (rho U_lid h^2), falls to --converge-target). Device time of
-    every iteration on the flow's stream (CUDA events). Reports the time each
-    form needs to reach the smallest residual both reach (the target when both
-    get there), their ratio, and the mixed form's field error against the FP64
-    form after the same number of iterations."""
+    every iteration on the flow's stream (CUDA events); the first iteration,
+    which also builds the AMG hierarchy on the host, is run untimed. Reports
+    the time each form needs to reach the smallest residual both reach (the
+    target when both get there), their ratio, and the mixed form's field error
+    against the FP64 form after the same number of iterations."""
     import torch
 
     from openaccel_b200 import runtime as rt
@@ -271,8 +272,11 @@ def converge(args, gm, U0, dev, world):
         f.set_field("U", U0)
         f.initialize()
         stream = torch.cuda.ExternalStream(f.stream_handle(), device=dev)
-        res, t = [], []
-        for _ in range(args.converge_iters):
+        # iteration 1 builds the pressure solve's AMG hierarchy on the host
+        # (about 1.8 s at 128^3, the same in both forms): run it untimed
+        st = f.simple_iterate(1)[0]
+        res, t = [st["continuity_rms"]], [0.0]
+        for _ in range(args.converge_iters - 1):
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(stream)
             st = f.simple_iterate(1)[0]
@@ -290,14 +294,14 @@ def converge(args, gm, U0, dev, world):
     summary = {"target": args.converge_target, "max_iters": args.converge_iters,
                "residual_definition": "RMS over nodes of the pressure-correction rhs before the solve / (rho U_lid h^2), "
                                       "h = mean element edge length",
-               "common_residual": target}
+               "common_residual": target, "timed_from_iteration": 2}
     t_to = {}
     for name, o in out.items():
         k = int(np.argmax(o["res"] <= target))
         t_to[name] = float(o["cum_ms"][k])
         summary[name] = {"iters_run": o["iters"], "residual_first": o["residual_first"],
                          "residual_last": o["residual_last"], "iters_to_common": k + 1, "ms_to_common": t_to[name],
-                         "ms_per_iter": o["ms_total"] / o["iters"]}
+                         "ms_per_iter": o["ms_total"] / max(o["iters"] - 1, 1)}
     summary["time_to_residual_ratio_fp64_over_mixed"] = t_to["fp64"] / t_to["mixed"]
     (Um, pm, nm), (Ud, pd, nd) = fields["mixed"], fields["fp64"]
     if nm == nd:
