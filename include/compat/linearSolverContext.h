@@ -91,6 +91,38 @@ class Vector {
   std::vector<double> v_;
 };
 
+/* Coefficient scaling the linear system applies before a solve when asked
+ * (linearSystem::solveSystem_, src/equation/linearSystem.h:416-462: normalize,
+ * diagonalScale). The absent library's own definitions are not in the
+ * reference checkout; this reconstruction scales every equation (row i, dof
+ * m) of A and b by the inverse of its diagonal coefficient, so the diagonal
+ * becomes 1 and the solution is unchanged, for both calls. */
+template <std::size_t N>
+class Coefficients {
+ public:
+  Coefficients(Matrix<N>& A, Vector<N>& b) : A_(A), b_(b) {}
+  void normalize() { scale_rows(); }
+  void diagonalScale() { scale_rows(); }
+
+ private:
+  void scale_rows() {
+    for (int i = 0; i < A_.nRows(); ++i) {
+      const auto vals = A_.rowVals(i);
+      const std::size_t len = vals.size() / (N * N);
+      for (std::size_t m = 0; m < N; ++m) {
+        const double d = A_.dofDiag(i, static_cast<int>(m));
+        if (d == 0.0) continue;
+        const double inv = 1.0 / d;
+        for (std::size_t k = 0; k < len; ++k)
+          for (std::size_t q = 0; q < N; ++q) vals[N * N * k + N * m + q] *= inv;
+        b_[N * static_cast<std::size_t>(i) + m] *= inv;
+      }
+    }
+  }
+  Matrix<N>& A_;
+  Vector<N>& b_;
+};
+
 template <std::size_t N>
 struct ControlData {
   int n_iterations = 0;
@@ -104,6 +136,7 @@ class Context {
   using Matrix = linearSolver::Matrix<N>;
   using Vector = linearSolver::Vector<N>;
   using Array = std::array<double, N>;
+  using Index = int;  // column id type of rowCols (32-bit ids: one rank, local = global order)
 
   Context(std::string name, const CRSNodeGraph* g)
       : name_(std::move(name)), A_(g), b_(g->nRows()), x_(g->nRows()), r_(g->nRows()) {
@@ -119,6 +152,7 @@ class Context {
     x_.zero();
     r_.zero();
   }
+  Coefficients<N> getCoefficients() { return Coefficients<N>(A_, b_); }
   ControlData<N>& getControlData() { return cdata_; }
   Array& getResidualScales() { return scales_; }
   Array& getControlResidual() { return control_; }

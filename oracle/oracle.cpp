@@ -1111,6 +1111,16 @@ int orc_bicgstab(void* h, int bs, const double* A, const double* b, double* x, d
 }
 void orc_simple_iteration(void* h, orc_iter_stats* st) { simple_iteration(*static_cast<Case*>(h), st); }
 
+void orc_apply_coeff(void* h, int bs, double* A, double* b, const int* nodes, int n, const double* rhs,
+                     const double* lhs) {
+  Case& c = *static_cast<Case*>(h);
+  if (n < 1 || n > 8) return;  // hex8 / tet4 elements
+  if (bs == 3)
+    apply_coeff<3>(c, A, b, nodes, n, rhs, lhs);
+  else
+    apply_coeff<1>(c, A, b, nodes, n, rhs, lhs);
+}
+
 void orc_set_solver(void* h, int kind) { static_cast<Case*>(h)->solverKind = (kind == 1 || kind == 2) ? kind : 0; }
 
 int orc_gmres_ilu(void* h, int bs, const double* A, const double* b, double* x, double rtol, int maxit, int restart,

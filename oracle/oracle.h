@@ -87,6 +87,11 @@ void orc_update_grad_u(void* h);
  * relative residual. bs = 1 or 3. */
 int orc_bicgstab(void* h, int bs, const double* A, const double* b, double* x,
                  double rtol, int maxit, double* res);
+/* the oracle's applyCoeff_ restatement on the case's graph: adds an element's
+ * lhs [(n*bs)^2] and rhs [n*bs] (node-major, assembler.h layout) into A (BSR,
+ * bs = 1 or 3) and b; columns missing from a row go to the diagonal block */
+void orc_apply_coeff(void* h, int bs, double* A, double* b, const int* nodes, int n, const double* rhs,
+                     const double* lhs);
 /* one SIMPLE outer iteration (segregatedFlowEquations::solve) */
 void orc_simple_iteration(void* h, orc_iter_stats* st);
 /* linear solvers of orc_simple_iteration: 0 = Jacobi-preconditioned BiCGStab

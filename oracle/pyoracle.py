@@ -121,6 +121,9 @@ def lib():
         L.orc_case_nnz.argtypes = [C.c_void_p]
         L.orc_case_mass_scale.restype = C.c_double
         L.orc_case_mass_scale.argtypes = [C.c_void_p]
+        L.orc_apply_coeff.restype = None
+        L.orc_apply_coeff.argtypes = [C.c_void_p, C.c_int, P(C.c_double), P(C.c_double), P(C.c_int), C.c_int,
+                                      P(C.c_double), P(C.c_double)]
         L.orc_set_solver.restype = None
         L.orc_set_solver.argtypes = [C.c_void_p, C.c_int]
         L.orc_gmres_ilu.restype = C.c_int
@@ -271,6 +274,12 @@ class FlowCase:
         lib().orc_simple_iteration(self.h, C.byref(st))
         return dict(mom_iters=st.mom_iters[0], mom_res=st.mom_res, pc_iters=st.pc_iters,
                     pc_res=st.pc_res, continuity_rms=st.continuity_rms, continuity_raw=st.continuity_raw)
+
+    def apply_coeff(self, bs, A, b, nodes, rhs, lhs):
+        """The oracle's applyCoeff_ restatement: adds an element system into A, b in place."""
+        nodes = np.ascontiguousarray(nodes, np.int32)
+        lib().orc_apply_coeff(self.h, bs, _dp(A), _dp(b), nodes.ctypes.data_as(C.POINTER(C.c_int)), int(nodes.size),
+                              _dp(np.ascontiguousarray(rhs, np.float64)), _dp(np.ascontiguousarray(lhs, np.float64)))
 
     def set_solver(self, kind):
         """0: Jacobi-BiCGStab (parity reference); 1 or "reference": the cavity

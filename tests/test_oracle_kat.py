@@ -164,3 +164,39 @@ def test_continuity_scale_is_rho_ulid_h2(oracle_mod):
     c.initialize()
     st = c.simple_iteration()
     assert st["continuity_rms"] == pytest.approx(st["continuity_raw"] / c.mass_scale(), rel=1e-15)
+
+
+REF_ASM_LIB = os.path.join(ROOT, "oracle", "_ref", "libref_assembler.so")
+
+
+@pytest.mark.skipif(not os.path.exists(REF_ASM_LIB),
+                    reason="reference assembler library not built (needs the reference tree)")
+@pytest.mark.parametrize("bs", [1, 3])
+def test_oracle_scatter_matches_reference_apply_coeff(oracle_mod, bs):
+    """Pin the oracle's scatter against the reference's own
+    assembler<N>::applyCoeff_ (src/assemble/assembler.h:311-453, compiled from
+    the reference tree): random element matrices of hex8 elements, in random
+    node orders, added into the reduced-stencil block-CSR system, where the
+    face- and body-diagonal columns the stencil lacks are lumped into the
+    diagonal block. Bitwise equal."""
+    L = C.CDLL(REF_ASM_LIB)
+    m = meshgen.cavity(4, perturb=0.2, seed=3)
+    c = oracle_mod.FlowCase(m, oracle_mod.default_settings())
+    rp, cols = c.graph()
+    diag = np.array([np.searchsorted(cols[rp[i]:rp[i + 1]], i) for i in range(m.nn)], dtype=np.int32)
+    rng = np.random.default_rng(11 + bs)
+    A_o = np.zeros(bs * bs * cols.size)
+    b_o = np.zeros(bs * m.nn)
+    A_r, b_r = A_o.copy(), b_o.copy()
+    ptr = lambda a: a.ctypes.data_as(C.c_void_p)
+    for e in rng.permutation(m.ne):
+        nodes = np.ascontiguousarray(rng.permutation(m.conn[e]), np.int32)
+        n = nodes.size
+        lhs = rng.normal(size=(n * bs) ** 2)
+        rhs = rng.normal(size=n * bs)
+        c.apply_coeff(bs, A_o, b_o, nodes, rhs, lhs)
+        L.ref_apply_coeff(bs, m.nn, ptr(rp), ptr(cols), ptr(diag), ptr(A_r), ptr(b_r), ptr(nodes), n, ptr(rhs),
+                          ptr(lhs), 1)
+    np.testing.assert_array_equal(A_o, A_r)
+    np.testing.assert_array_equal(b_o, b_r)
+    assert np.abs(A_o).sum() > 0
