@@ -288,11 +288,6 @@ int oa_mesh_create(const double* coords, int nn, const int* conn, int ne, int to
     m.h_row_ptr[i + 1] = (int)m.h_cols.size();
   }
   m.nnz = m.h_row_ptr[nn];
-  if (!hex_axes_consistent(conn, nn, n2e.data(), m.h_row_ptr.data())) {
-    delete M;
-    return fail(OA_ERR_MESH,
-                "oa_mesh_create: the elements around a node do not form a consistently oriented 2x2x2 block");
-  }
   {
     // mean element edge length (the 12 edges are the SCS L/R pairs)
     double sum = 0.0;
@@ -418,7 +413,7 @@ int oa_flow_create(oa_mesh* M, const oa_flow_settings* s, const double* bnd_velo
       cudaMalloc(&f.b.A_pc, tm * nnz) != cudaSuccess || cudaMalloc(&f.pc_coef, tm * 24 * ne) != cudaSuccess ||
       cudaMallocHost(&H->hscal, 8 * sizeof(double)) != cudaSuccess ||
       (s->precision == OA_PREC_MIXED && (cudaMalloc(&f.xloc32, sizeof(float4) * 8 * ne) != cudaSuccess ||
-                                         cudaMalloc(&f.umu32, sizeof(float4) * 8 * ne) != cudaSuccess))) {
+                                         cudaMalloc(&f.umu32, sizeof(float4) * nn) != cudaSuccess))) {
     oa_flow_destroy(H);
     return fail(OA_ERR_CUDA, "oa_flow_create: device allocation failed");
   }

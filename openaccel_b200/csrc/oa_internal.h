@@ -75,9 +75,7 @@ struct Flow {
   // neighbours in the row-slot order), matrix precision, staged the same way
   void* pc_coef = nullptr;
   // mixed form only: [ne][8] FP32 corner offsets from corner 0 (static) and
-  // the [ne][8] element-major FP32 (U, mu) copy packed before each momentum
-  // assembly (one contiguous 128-byte record per element, read without the
-  // node-id indirection)
+  // the [nn] FP32 (U, mu) copy packed before each momentum assembly
   float4* xloc32 = nullptr;
   float4* umu32 = nullptr;
   Buffers b;
@@ -120,9 +118,6 @@ int create_tet4_mesh(oa_mesh* M, const double* coords, int nn, const int* conn, 
                      const int* face_ord, const int* face_bnd, int nf);
 
 // kernels / launchers (oa_kernels.cu)
-// hex8 row kernels' precondition: every node's elements form the 2x2x2
-// arrangement of a consistently oriented block (n2e [nn][8], CSR row_ptr)
-bool hex_axes_consistent(const int* conn, int nn, const int* n2e, const int* row_ptr);
 int launch_geometry(DeviceMesh& m, cudaStream_t st);
 // flux_fresh: pc_flux already holds this state's fluxes (the mass-flow update
 // ran last on the stream); otherwise a flux-only mass-flow pass runs first

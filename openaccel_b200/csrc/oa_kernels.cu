@@ -144,55 +144,52 @@ int launch_geometry(DeviceMesh& m, cudaStream_t st) {
 }
 
 // ---------------------------------------------------------------------------
-// CSR row write-out by element axes, for meshes whose elements around every
-// node sit in the 2x2x2 arrangement of a consistently oriented hex block (the
-// mesh set-up checks this). The four lanes whose elements share the row's
-// neighbour across one element axis hold that neighbour in the edge slot of
-// that axis (axis_slot_word); two xor-shuffle steps sum their blocks, and the
-// lowest-numbered of them with an element writes the sum into the neighbour's
-// CSR slot. Lane 0 writes the diagonal block, already reduced in every lane.
-// Every entry is written exactly once, in a fixed summation order; no shared
-// memory, no atomics. offdiag_zero: write zeros off the diagonal (the
-// pressure-level row).
+// CSR row write-out shared by the assembly kernels. Each lane publishes its
+// three edge-neighbour blocks with their column ids; lane s of the row then
+// emits CSR slot s (s, s+8, ...), summing the matching contributions in lane
+// order. The diagonal block is already reduced in every lane.
 template <int B, class TM>
-__device__ __forceinline__ void write_row_axes(int row, bool rv, int c, int lane, bool valid, const TM (&diag)[B],
-                                               const TM (&nb)[3][B], const int (&nbc)[3], const MeshView& m,
-                                               TM* __restrict__ A, bool offdiag_zero) {
-  const unsigned vmask = (__ballot_sync(FULL_MASK, valid) >> (lane & 24)) & 0xffu;
-  const uint32_t aw = axis_slot_word(c);
-  int rp = 0, len = 0;
+__device__ __forceinline__ void write_row(int row, bool rv, int c, int lane, const TM (&diag)[B],
+                                          const TM (&nb)[3][B], const int (&nbc)[3],
+                                          const MeshView& m, TM* __restrict__ A, TM* sh_val,
+                                          int* sh_col, bool offdiag_zero) {
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    sh_col[lane * 3 + k] = nbc[k];
+#pragma unroll
+    for (int b = 0; b < B; ++b) sh_val[(lane * 3 + k) * B + b] = nb[k][b];
+  }
+  __syncwarp();
   if (rv) {
-    rp = __ldg(m.row_ptr + row);
-    len = __ldg(m.row_ptr + row + 1) - rp;
-  }
-  StaticFor<0, 3>::run([&](auto axc) {
-    constexpr int ax = decltype(axc)::value;
-    constexpr int f1 = axis_flip((ax + 1) % 3), f2 = axis_flip((ax + 2) % 3);
-    const int k = (aw >> (2 * ax)) & 3;
-    TM v[B];
-#pragma unroll
-    for (int b = 0; b < B; ++b) v[b] = k == 0 ? nb[0][b] : (k == 1 ? nb[1][b] : nb[2][b]);
-    const int col = k == 0 ? nbc[0] : (k == 1 ? nbc[1] : nbc[2]);
-#pragma unroll
-    for (int b = 0; b < B; ++b) v[b] += __shfl_xor_sync(FULL_MASK, v[b], f1);
-#pragma unroll
-    for (int b = 0; b < B; ++b) v[b] += __shfl_xor_sync(FULL_MASK, v[b], f2);
-    auto lower_valid = [&](int g) { return g < c && ((vmask >> g) & 1u); };
-    const bool writer = valid && !lower_valid(c ^ f1) && !lower_valid(c ^ f2) && !lower_valid(c ^ f1 ^ f2);
-    if (rv && writer) {
-      int s = 0;
-      while (s < len && __ldg(m.cols + rp + s) != col) ++s;
-      if (s < len) {
-#pragma unroll
-        for (int b = 0; b < B; ++b) A[(size_t)(rp + s) * B + b] = offdiag_zero ? TM(0) : v[b];
-      }
-    }
-  });
-  if (rv && c == 0) {
+    const int rp = __ldg(m.row_ptr + row);
+    const int len = __ldg(m.row_ptr + row + 1) - rp;
     const int dof = __ldg(m.diag + row);
+    const int base = lane & ~7;
+    for (int s = c; s < len; s += 8) {
+      TM out[B];
+      if (s == dof) {
 #pragma unroll
-    for (int b = 0; b < B; ++b) A[(size_t)(rp + dof) * B + b] = diag[b];
+        for (int b = 0; b < B; ++b) out[b] = diag[b];
+      } else {
+#pragma unroll
+        for (int b = 0; b < B; ++b) out[b] = TM(0);
+        if (!offdiag_zero) {
+          const int col = __ldg(m.cols + rp + s);
+#pragma unroll
+          for (int c2 = 0; c2 < 8; ++c2)
+#pragma unroll
+            for (int k = 0; k < 3; ++k)
+              if (sh_col[(base + c2) * 3 + k] == col) {
+#pragma unroll
+                for (int b = 0; b < B; ++b) out[b] += sh_val[((base + c2) * 3 + k) * B + b];
+              }
+        }
+      }
+#pragma unroll
+      for (int b = 0; b < B; ++b) A[(size_t)(rp + s) * B + b] = out[b];
+    }
   }
+  __syncwarp();
 }
 
 // ---------------------------------------------------------------------------
@@ -226,7 +223,10 @@ __host__ __device__ constexpr int edge_nbr(int c, int s) {
 
 template <class TF>
 __global__ void __launch_bounds__(BLOCK) k_pcorr(PcArgs a) {
+  __shared__ TF sh_val[BLOCK * 3];
+  __shared__ int sh_col[BLOCK * 3];
   const int lane = threadIdx.x & 31;
+  const int warp_base = threadIdx.x & ~31;
   const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 3;
   const int c = threadIdx.x & 7;
   const bool rv = row < a.m.nn;
@@ -255,7 +255,8 @@ __global__ void __launch_bounds__(BLOCK) k_pcorr(PcArgs a) {
   diag[0] = rowsum8(diag[0]);
   rhs = rowsum8(rhs);
   const bool refrow = rv && __ldg(a.ref_flag + row) != 0;
-  write_row_axes<1, TF>(row, rv, c, lane, e >= 0, diag, nb, nbc, a.m, static_cast<TF*>(a.A), refrow);
+  write_row<1, TF>(row, rv, c, lane, diag, nb, nbc, a.m, static_cast<TF*>(a.A),
+                   sh_val + warp_base * 3, sh_col + warp_base * 3, refrow);
   if (rv && c == 0) a.b[row] = refrow ? 0.0 : rhs;
 }
 
@@ -269,7 +270,7 @@ struct MomArgs {
   MeshView m;
   const double *U, *gradP, *div, *mDot, *rho, *mu, *sideU;
   const float4* xloc;  // mixed form: [ne][8] FP32 corner offsets from corner 0
-  const float4* umu;   // mixed form: [ne][8] element-major FP32 (U, mu)
+  const float4* umu;   // mixed form: [nn] FP32 (U, mu)
   void* A;
   void* b;
   double* du;
@@ -280,7 +281,7 @@ struct MomArgs {
 // Zero-normal-stress wall term at the exposed ip of canonical face FC nearest
 // corner 0 (IP_ZERO_NORMAL_STRESS_FIXED_VEL__).
 template <int FC, bool USH, bool UGSH, class TF>
-__device__ __forceinline__ void wall_face(const MomArgs& a, const TF (&x)[8][3], int e, uint32_t pw,
+__device__ __forceinline__ void wall_face(const MomArgs& a, const TF (&x)[8][3], const int (&nd)[8],
                                           const TF (&Uc)[8][3], const TF (&mu)[8], TF (&diag)[9],
                                           TF (&nb)[3][9], TF (&rhs)[3], int* err) {
   constexpr int f0 = face_node(FC, 0), f1 = face_node(FC, 1), f2 = face_node(FC, 2), f3 = face_node(FC, 3);
@@ -297,7 +298,7 @@ __device__ __forceinline__ void wall_face(const MomArgs& a, const TF (&x)[8][3],
   StaticFor<0, 4>::run([&](auto kc) {
     constexpr int fn = face_node(FC, decltype(kc)::value);
     double s[3];
-    load3(a.sideU, __ldg(a.m.conn + 8 * e + perm_at(pw, fn)), s);
+    load3(a.sideU, nd[fn], s);
 #pragma unroll
     for (int k = 0; k < 3; ++k) Ue[fn][k] = TF(s[k]);
   });
@@ -360,16 +361,15 @@ __device__ __forceinline__ void wall_face(const MomArgs& a, const TF (&x)[8][3],
 
 template <bool USH, bool UGSH, class TF>
 __global__ void __launch_bounds__(BLOCK, sizeof(TF) == 4 ? (UGSH ? 4 : 3) : 1) k_momentum(MomArgs a) {
+  __shared__ TF sh_val[BLOCK * 3 * 9];
+  __shared__ int sh_col[BLOCK * 3];
   const int lane = threadIdx.x & 31;
+  const int warp_base = threadIdx.x & ~31;
   const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 3;
   const int c = threadIdx.x & 7;
   const bool rv = row < a.m.nn;
   const int e = rv ? __ldg(a.m.n2e + 8 * row + c) : -1;
-  // nb: the viscous neighbour blocks (the diagonal block is formed from them
-  // once after the ip loop), then wall terms, then the advective neighbour
-  // coefficients fr on their diagonals
   TF diag[9], nb[3][9], rhs[3];
-  TF fl_sum = TF(0), fr[3] = {TF(0), TF(0), TF(0)};
 #pragma unroll
   for (int k = 0; k < 9; ++k) {
     diag[k] = TF(0);
@@ -384,23 +384,19 @@ __global__ void __launch_bounds__(BLOCK, sizeof(TF) == 4 ? (UGSH ? 4 : 3) : 1) k
     // coordinates of the flux arithmetic: FP64 as gathered, or, in the mixed
     // form, the element's FP32 corner offsets from its corner 0 (the Jacobians
     // are translation invariant), one 16-byte load per corner, with U and mu
-    // from the element-major FP32 copy (one 16-byte load per corner, from the
-    // same 128-byte record: no node-id indirection); only the three edge
-    // neighbours' ids are read (wall faces read theirs when present)
+    // from the FP32 node copy (one 16-byte load per node)
     TF x[8][3];
     TF Uc[8][3], mu[8];
     if constexpr (sizeof(TF) == 4) {
-      nd[1] = __ldg(a.m.conn + 8 * e + perm_at(pw, 1));
-      nd[3] = __ldg(a.m.conn + 8 * e + perm_at(pw, 3));
-      nd[4] = __ldg(a.m.conn + 8 * e + perm_at(pw, 4));
 #pragma unroll
       for (int k = 0; k < 8; ++k) {
         const int pk = perm_at(pw, k);
+        nd[k] = __ldg(a.m.conn + 8 * e + pk);
         const float4 t = __ldg(a.xloc + 8 * (size_t)e + pk);
         x[k][0] = t.x;
         x[k][1] = t.y;
         x[k][2] = t.z;
-        const float4 u = __ldg(a.umu + 8 * (size_t)e + pk);
+        const float4 u = __ldg(a.umu + nd[k]);
         Uc[k][0] = u.x;
         Uc[k][1] = u.y;
         Uc[k][2] = u.z;
@@ -444,12 +440,14 @@ __global__ void __launch_bounds__(BLOCK, sizeof(TF) == 4 ? (UGSH ? 4 : 3) : 1) k
         if (N != 0.0) muIp += TF(N) * mu[n];
       });
       // upwind advection (row L = corner 0)
-      fl_sum += TF(0.5) * (tm + fabs(tm));
-      fr[RS] += TF(0.5) * (tm - fabs(tm));
+      const TF fl = TF(0.5) * (tm + fabs(tm));
+      const TF fr = TF(0.5) * (tm - fabs(tm));
 #pragma unroll
       for (int i = 0; i < 3; ++i) {
         const TF up = tmd > 0 ? Uc[0][i] : Uc[R][i];
         rhs[i] -= tm * up;
+        diag[3 * i + i] += fl;
+        nb[RS][3 * i + i] += fr;
       }
       // viscous stress incl. transpose. Block of column n:
       //   -mu_ip (g_n . A) I - mu_ip A (x) g_n   (rows i, columns j: g_n,i A_j)
@@ -492,35 +490,27 @@ __global__ void __launch_bounds__(BLOCK, sizeof(TF) == 4 ? (UGSH ? 4 : 3) : 1) k
 #pragma unroll
           for (int i = 0; i < 3; ++i) {
 #pragma unroll
-            for (int j = 0; j < 3; ++j) nb[sl][3 * i + j] += -muIp * g[i] * ax[j] + (i == j ? -muIp * ga : TF(0));
+            for (int j = 0; j < 3; ++j) {
+              const TF fj = -muIp * g[i] * ax[j] + (i == j ? -muIp * ga : TF(0));
+              nb[sl][3 * i + j] += fj;
+              diag[3 * i + j] -= fj;
+            }
           }
         }
       });
     });
-    // the viscous diagonal block takes every column but the three kept
-    // neighbours (partition of unity); the wall terms below are added as they
-    // are (their face nodes carry no lhs)
-#pragma unroll
-    for (int k = 0; k < 9; ++k) diag[k] -= nb[0][k] + nb[1][k] + nb[2][k];
     // no-slip wall faces touching this corner
     const uint8_t fm = __ldg(a.m.face_mask + e);
     if (fm) {
       const uint32_t fw = face_word(c);
-      if (fm & (1u << ((fw >> 0) & 7))) wall_face<0, USH, UGSH, TF>(a, x, e, pw, Uc, mu, diag, nb, rhs, &err);
-      if (fm & (1u << ((fw >> 3) & 7))) wall_face<3, USH, UGSH, TF>(a, x, e, pw, Uc, mu, diag, nb, rhs, &err);
-      if (fm & (1u << ((fw >> 6) & 7))) wall_face<4, USH, UGSH, TF>(a, x, e, pw, Uc, mu, diag, nb, rhs, &err);
+      if (fm & (1u << ((fw >> 0) & 7))) wall_face<0, USH, UGSH, TF>(a, x, nd, Uc, mu, diag, nb, rhs, &err);
+      if (fm & (1u << ((fw >> 3) & 7))) wall_face<3, USH, UGSH, TF>(a, x, nd, Uc, mu, diag, nb, rhs, &err);
+      if (fm & (1u << ((fw >> 6) & 7))) wall_face<4, USH, UGSH, TF>(a, x, nd, Uc, mu, diag, nb, rhs, &err);
     }
     if (err) a.err[0] = 1;
     nbc[0] = nd[1];
     nbc[1] = nd[3];
     nbc[2] = nd[4];
-  }
-  // advective coefficients
-#pragma unroll
-  for (int i = 0; i < 3; ++i) {
-    diag[4 * i] += fl_sum;
-#pragma unroll
-    for (int s = 0; s < 3; ++s) nb[s][4 * i] += fr[s];
   }
 #pragma unroll
   for (int k = 0; k < 9; ++k) diag[k] = rowsum8(diag[k]);
@@ -557,7 +547,8 @@ __global__ void __launch_bounds__(BLOCK, sizeof(TF) == 4 ? (UGSH ? 4 : 3) : 1) k
       }
     }
   }
-  write_row_axes<9, TF>(row, rv, c, lane, e >= 0, diag, nb, nbc, a.m, static_cast<TF*>(a.A), false);
+  write_row<9, TF>(row, rv, c, lane, diag, nb, nbc, a.m, static_cast<TF*>(a.A),
+                   sh_val + warp_base * 3 * 9, sh_col + warp_base * 3, false);
 }
 
 // ---------------------------------------------------------------------------
@@ -900,34 +891,6 @@ __global__ void k_vel_correct(int n3, double* U, const double* du, const double*
 }
 
 // ---------------------------------------------------------------------------
-// Host check behind write_row_axes: around every node, the lanes whose
-// elements share an element axis and a side name the same neighbour node
-// there, and the row's CSR length is one plus the number of such neighbours.
-bool hex_axes_consistent(const int* conn, int nn, const int* n2e, const int* row_ptr) {
-  for (int n = 0; n < nn; ++n) {
-    int nbr[3][2] = {{-1, -1}, {-1, -1}, {-1, -1}};
-    for (int c = 0; c < 8; ++c) {
-      const int e = n2e[8L * n + c];
-      if (e < 0) continue;
-      const uint32_t w = axis_slot_word_ce(c);
-      for (int ax = 0; ax < 3; ++ax) {
-        const int k = (w >> (2 * ax)) & 3;
-        const int j = conn[8L * e + rot_perm(c, slot_node(k))];
-        int& slot = nbr[ax][corner_side(c, ax) < 0 ? 1 : 0];
-        if (slot == -1)
-          slot = j;
-        else if (slot != j)
-          return false;
-      }
-    }
-    int count = 1;
-    for (int ax = 0; ax < 3; ++ax) count += (nbr[ax][0] >= 0) + (nbr[ax][1] >= 0);
-    if (count != row_ptr[n + 1] - row_ptr[n]) return false;
-  }
-  return true;
-}
-
-// ---------------------------------------------------------------------------
 // launchers
 static int grid_rows(int nn) { return (int)(((size_t)nn * 8 + BLOCK - 1) / BLOCK); }
 
@@ -961,15 +924,10 @@ __global__ void k_xloc(MeshView m, float4* xloc) {
                         float(m.x[3 * nk + 2] - m.x[3 * n0 + 2]), 0.f);
 }
 
-// Element-major FP32 copy of (U, mu) for the mixed momentum kernel: record
-// [e][k] holds node conn[e][k], so a lane reads its element's eight nodes from
-// one 128-byte line without the node-id indirection
-__global__ void k_pack_umu(MeshView m, const double* __restrict__ U, const double* __restrict__ mu, float4* umu) {
-  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= 8LL * m.ne) return;
-  const int n = __ldg(m.conn + t);
-  umu[t] = make_float4(float(__ldg(U + 3 * n)), float(__ldg(U + 3 * n + 1)), float(__ldg(U + 3 * n + 2)),
-                       float(__ldg(mu + n)));
+// FP32 node copy of (U, mu) for the mixed momentum kernel
+__global__ void k_pack_umu(int nn, const double* __restrict__ U, const double* __restrict__ mu, float4* umu) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < nn) umu[i] = make_float4(float(U[3 * i]), float(U[3 * i + 1]), float(U[3 * i + 2]), float(mu[i]));
 }
 
 int launch_xloc(Flow& f) {
@@ -983,7 +941,7 @@ int launch_xloc(Flow& f) {
 int launch_momentum(Flow& f, bool mixed) {
   if (mixed) {
     if (!f.xloc32 || !f.umu32) return fail(OA_ERR_ARG, "momentum assembly: mixed-form buffers missing");
-    k_pack_umu<<<(unsigned)((8LL * f.mesh->ne + 255) / 256), 256, 0, f.stream>>>(f.mesh->view(), f.U, f.mu, f.umu32);
+    k_pack_umu<<<(f.mesh->nn + 255) / 256, 256, 0, f.stream>>>(f.mesh->nn, f.U, f.mu, f.umu32);
     count_launches(1);
   }
   MomArgs a{f.mesh->view(), f.U,       f.gradP, f.div,  f.mDot,          f.rho,

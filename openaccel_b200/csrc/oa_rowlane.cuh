@@ -67,53 +67,6 @@ __device__ __forceinline__ T rowsum8(T v) {
   return v;
 }
 
-// ROT_PERM of oa_hex8.cuh as a constant expression (host and device).
-__host__ __device__ constexpr int rot_perm(int c, int k) {
-  constexpr int T[8][8] = {{0, 1, 2, 3, 4, 5, 6, 7}, {1, 0, 4, 5, 2, 3, 7, 6}, {2, 3, 0, 1, 6, 7, 4, 5},
-                           {3, 2, 6, 7, 0, 1, 5, 4}, {4, 5, 1, 0, 7, 6, 2, 3}, {5, 4, 7, 6, 1, 0, 3, 2},
-                           {6, 7, 3, 2, 5, 4, 0, 1}, {7, 6, 5, 4, 3, 2, 1, 0}};
-  return T[c][k];
-}
-
-// Element axis (0, 1, 2 for s1, s2, s3) along which edge-neighbour corners a
-// and b of the hex8 element differ, and the side of corner a on an axis
-// (-1 or +1; Nalu corner order 0 (-,-,-), 1 (+,-,-), 2 (+,+,-), 3 (-,+,-),
-// then 4..7 the same at s3 = +).
-__host__ __device__ constexpr int corner_side(int a, int ax) {
-  constexpr int S[8][3] = {{-1, -1, -1}, {1, -1, -1}, {1, 1, -1}, {-1, 1, -1},
-                           {-1, -1, 1},  {1, -1, 1},  {1, 1, 1},  {-1, 1, 1}};
-  return S[a][ax];
-}
-__host__ __device__ constexpr int edge_axis(int a, int b) {
-  return corner_side(a, 0) != corner_side(b, 0) ? 0 : (corner_side(a, 1) != corner_side(b, 1) ? 1 : 2);
-}
-// Canonical nodes 1, 3, 4 are the edge slots 0, 1, 2 of a lane.
-__host__ __device__ constexpr int slot_node(int k) { return k == 0 ? 1 : (k == 1 ? 3 : 4); }
-// Element axis of lane c's edge slot k.
-__host__ __device__ constexpr int slot_axis(int c, int k) { return edge_axis(c, rot_perm(c, slot_node(k))); }
-// Lane xor that moves a corner to its neighbour across element axis ax.
-__host__ __device__ constexpr int axis_flip(int ax) { return ax == 0 ? 1 : (ax == 1 ? 3 : 4); }
-// 2 bits per element axis: the edge slot of lane c along that axis.
-__host__ __device__ constexpr uint32_t axis_slot_word_ce(int c) {
-  uint32_t w = 0;
-  for (int ax = 0; ax < 3; ++ax)
-    for (int k = 0; k < 3; ++k)
-      if (slot_axis(c, k) == ax) w |= uint32_t(k) << (2 * ax);
-  return w;
-}
-__device__ __forceinline__ uint32_t axis_slot_word(int c) {
-  switch (c) {
-    case 0: return axis_slot_word_ce(0);
-    case 1: return axis_slot_word_ce(1);
-    case 2: return axis_slot_word_ce(2);
-    case 3: return axis_slot_word_ce(3);
-    case 4: return axis_slot_word_ce(4);
-    case 5: return axis_slot_word_ce(5);
-    case 6: return axis_slot_word_ce(6);
-    default: return axis_slot_word_ce(7);
-  }
-}
-
 // Canonical target of element column a for the row at canonical corner 0 in
 // the reduced (edge) stencil: 1, 3, 4 are edge neighbours (slots 0, 1, 2);
 // 0 is the row itself and 2, 5, 6, 7 (face/body diagonals) are lumped into the

@@ -17,6 +17,7 @@
 #include <cstdio>
 #include <cstring>
 #include <fstream>
+#include <iomanip>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -163,8 +164,10 @@ static int gpu_checks(const std::string& dir) {
   write_file(dir + "/A.f64", ctx.getAMatrix().data(), ctx.getAMatrix().size());
   write_file(dir + "/b.f64", ctx.getBVector().data(), ctx.getBVector().size());
   write_file(dir + "/x.f64", ctx.getXVector().data(), ctx.getXVector().size());
-  std::ofstream(dir + "/control.txt") << cd.n_iterations << " " << cd.solver_initial_res[0] << " "
-                                      << cd.solver_final_res[0] << " " << cd.scaled_initial_res[0] << "\n";
+  std::ofstream ctl(dir + "/control.txt");
+  ctl << std::setprecision(17) << cd.n_iterations << " " << cd.solver_initial_res[0] << " " << cd.solver_final_res[0]
+      << " " << cd.scaled_initial_res[0] << "\n";
+  ctl.close();
   oa_flow_destroy(flow);
   oa_mesh_destroy(mesh);
   std::printf("compat gpu ok\n");
