@@ -55,6 +55,9 @@ typedef struct oa_flow_settings {
   int pc_amg;                   /* 1: aggregation-AMG preconditioned GCR(2) pressure solve (BiCGStab
                                    if GCR stagnates or OA_KRYLOV=bicgstab), 0: Jacobi BiCGStab */
   int use_graphs;               /* 1: replay Krylov iteration chunks as CUDA graphs */
+  int hr;                       /* advection: 0 upwind, 1 high resolution (advectionSchemeType::highResolution:
+                                   blended deferred correction, nodeField::updateBlendingFactorField) */
+  double beta_max;              /* upper limit of the blending factor (nodeField.h:150, default 1) */
 } oa_flow_settings;
 
 /* Convergence record of one linear solve: the ControlData that liblinsolve
@@ -130,7 +133,9 @@ int oa_flow_create(oa_mesh* m, const oa_flow_settings* s, const double* bnd_velo
 void oa_flow_destroy(oa_flow* f);
 /* Host <-> device copies of a named field: "U" [nn][3], "p" [nn], "gradU"
  * [nn][9], "gradP" [nn][3], "du" [nn][3], "div" [nn], "mDot" [ne][12],
- * "sideU" [nn][3]. n is the number of doubles. */
+ * "sideU" [nn][3], "rho" [nn], "mu" [nn]; with settings.hr also the velocity
+ * blending factor "betaU" and its extrema fields "minU", "maxU" [nn][3].
+ * n is the number of doubles. */
 int oa_flow_set_field(oa_flow* f, const char* name, const double* host, long n);
 int oa_flow_get_field(oa_flow* f, const char* name, double* host, long n);
 /* Device pointer of a named field (for callers that keep data resident). */

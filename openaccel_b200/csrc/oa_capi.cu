@@ -107,6 +107,9 @@ double* field_ptr(Flow& f, const std::string& n, size_t* len) {
   if (n == "sideU") { *len = 3 * nn; return f.sideU; }
   if (n == "rho") { *len = nn; return f.rho; }
   if (n == "mu") { *len = nn; return f.mu; }
+  if (f.betaU && n == "betaU") { *len = 3 * nn; return f.betaU; }
+  if (f.minU && n == "minU") { *len = 3 * nn; return f.minU; }
+  if (f.maxU && n == "maxU") { *len = 3 * nn; return f.maxU; }
   *len = 0;
   return nullptr;
 }
@@ -377,6 +380,8 @@ int oa_flow_create(oa_mesh* M, const oa_flow_settings* s, const double* bnd_velo
   if (!M || !s || !out || nbnd < 0 || (nbnd > 0 && !bnd_velocity)) return fail(OA_ERR_ARG, "oa_flow_create: bad arguments");
   if (s->urf_u <= 0 || s->urf_p <= 0 || s->dt <= 0) return fail(OA_ERR_ARG, "oa_flow_create: relaxation/timescale must be > 0");
   if (s->precision != OA_PREC_FP64 && s->precision != OA_PREC_MIXED) return fail(OA_ERR_ARG, "oa_flow_create: unknown precision");
+  if (s->hr != 0 && s->hr != 1) return fail(OA_ERR_ARG, "oa_flow_create: advection scheme must be 0 (upwind) or 1 (high resolution)");
+  if (s->hr && !(s->beta_max > 0)) return fail(OA_ERR_ARG, "oa_flow_create: beta_max must be > 0 for high resolution");
   if (s->ref_node >= M->m.nn) return fail(OA_ERR_ARG, "oa_flow_create: ref_node out of range");
   if (M->m.topo != OA_TOPO_HEX8) return fail(OA_ERR_MESH, "oa_flow_create: the flow path needs a hex8 mesh");
   *out = nullptr;
@@ -405,7 +410,9 @@ int oa_flow_create(oa_mesh* M, const oa_flow_settings* s, const double* bnd_velo
       (st = dalloc(&f.mu, nn)) ||
       (st = dalloc(&f.sideU, 3 * nn)) || (st = dalloc(&f.b.b_pc, nn)) || (st = dalloc(&f.b.x_mom, 3 * nn)) ||
       (st = dalloc(&f.b.x_pc, nn)) || (st = dalloc(&f.err_dev, 1)) || (st = dalloc(&H->scal, 8)) ||
-      (st = dalloc(&f.red, (size_t)partials_size())) || (st = dalloc(&f.ref_flag, nn))) {
+      (st = dalloc(&f.red, (size_t)partials_size())) || (st = dalloc(&f.ref_flag, nn)) ||
+      (s->hr && ((st = dalloc(&f.betaU, 3 * nn)) || (st = dalloc(&f.minU, 3 * nn)) ||
+                 (st = dalloc(&f.maxU, 3 * nn))))) {
     oa_flow_destroy(H);
     return st;
   }
@@ -440,6 +447,13 @@ int oa_flow_create(oa_mesh* M, const oa_flow_settings* s, const double* bnd_velo
   cudaMemset(f.div, 0, sizeof(double) * nn);
   cudaMemset(f.mDot, 0, sizeof(double) * 12 * ne);
   cudaMemset(f.err_dev, 0, sizeof(int));
+  if (f.betaU) {
+    // setupBlendingFactorField starts the blending factor at zero
+    // (src/field/nodeField/nodeField.hpp:733-745)
+    cudaMemset(f.betaU, 0, sizeof(double) * 3 * nn);
+    cudaMemset(f.minU, 0, sizeof(double) * 3 * nn);
+    cudaMemset(f.maxU, 0, sizeof(double) * 3 * nn);
+  }
   cudaMemset(f.ref_flag, 0, nn);
   if (s->ref_node >= 0) {
     const uint8_t one = 1;
@@ -476,7 +490,8 @@ void oa_flow_destroy(oa_flow* H) {
   Flow& f = H->f;
   void* ptrs[] = {f.U,       f.p,       f.gradU,   f.gradP,   f.du,      f.div,    f.mDot,  f.pc_flux,
                   f.pc_coef, f.xloc32,  f.umu32,   f.rho,     f.mu,      f.sideU,  f.b.A_mom, f.b.b_mom,
-                  f.b.A_pc,  f.b.b_pc,  f.b.x_mom, f.b.x_pc,  f.err_dev, H->scal,  f.red,   f.ref_flag};
+                  f.b.A_pc,  f.b.b_pc,  f.b.x_mom, f.b.x_pc,  f.err_dev, H->scal,  f.red,   f.ref_flag,
+                  f.betaU,   f.minU,    f.maxU};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (H->hscal) cudaFreeHost(H->hscal);
@@ -534,7 +549,10 @@ int oa_flow_initialize(oa_flow* H) {
   if (!H) return fail(OA_ERR_ARG, "oa_flow_initialize: null handle");
   Flow& f = H->f;
   int s;
-  if ((s = launch_gradient(f, 1)) || (s = launch_init_mdot(f)) || (s = launch_div(f)) || (s = launch_gradient(f, 0)))
+  // navierStokesEquation::initialize: velocity gradient, then (high
+  // resolution) the blending factor
+  if ((s = launch_gradient(f, 1)) || (f.s.hr && (s = launch_blend_u(f))) || (s = launch_init_mdot(f)) ||
+      (s = launch_div(f)) || (s = launch_gradient(f, 0)))
     return s;
   return check_err_flag(f, "oa_flow_initialize");
 }
@@ -647,8 +665,9 @@ int oa_simple_iterate(oa_flow* H, int n, oa_iter_stats* stats) {
       k_axpy<<<(f.mesh->nn + 255) / 256, 256, 0, f.stream>>>(f.mesh->nn, f.p, f.b.x_pc, f.s.urf_p);
       count_launches(1);
       if (!(s = launch_update_mdot(f)) && !(s = launch_div(f)) && !(s = launch_axpy_du_gradp(f, +1.0)) &&
-          !(s = launch_gradient(f, 0)) && !(s = launch_axpy_du_gradp(f, -1.0)))
-        s = launch_gradient(f, 1);
+          !(s = launch_gradient(f, 0)) && !(s = launch_axpy_du_gradp(f, -1.0)) && !(s = launch_gradient(f, 1)) &&
+          f.s.hr)
+        s = launch_blend_u(f);  // segregatedFlowEquations.cpp:287-288
     }
     nvtxRangePop();
     mark(5);

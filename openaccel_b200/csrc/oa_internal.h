@@ -67,6 +67,9 @@ struct Flow {
   // fields (FP64)
   double *U = nullptr, *p = nullptr, *gradU = nullptr, *gradP = nullptr, *du = nullptr,
          *div = nullptr, *mDot = nullptr, *rho = nullptr, *mu = nullptr, *sideU = nullptr;
+  // high-resolution advection (settings.hr): velocity blending factor and the
+  // extrema it is limited by, [nn][3] each
+  double *betaU = nullptr, *minU = nullptr, *maxU = nullptr;
   // [ne][12] Rhie-Chow mass flux of each SCS ip with the pressure-correction
   // equation's upwind density (its right-hand side), written by the mass-flow
   // kernel and summed per row by the pressure-correction kernel
@@ -130,5 +133,7 @@ int launch_update_mdot(Flow& f, bool stage = false);
 int launch_div(Flow& f);
 int launch_gradient(Flow& f, int which);
 int launch_axpy_du_gradp(Flow& f, double sign);
+// velocity extrema and blending factor of the high-resolution scheme
+int launch_blend_u(Flow& f);
 
 }  // namespace oa

@@ -269,6 +269,9 @@ __global__ void __launch_bounds__(BLOCK) k_pcorr(PcArgs a) {
 struct MomArgs {
   MeshView m;
   const double *U, *gradP, *div, *mDot, *rho, *mu, *sideU;
+  // high-resolution advection: velocity blending factor [nn][3] and nodal
+  // velocity gradient [nn][9] of the deferred correction
+  const double *betaU, *gradU;
   const float4* xloc;  // mixed form: [ne][8] FP32 corner offsets from corner 0
   const float4* umu;   // mixed form: [nn] FP32 (U, mu)
   void* A;
@@ -359,7 +362,7 @@ __device__ __forceinline__ void wall_face(const MomArgs& a, const TF (&x)[8][3],
   });
 }
 
-template <bool USH, bool UGSH, class TF>
+template <bool USH, bool UGSH, class TF, bool HR = false>
 __global__ void __launch_bounds__(BLOCK, sizeof(TF) == 4 ? (UGSH ? 4 : 3) : 1) k_momentum(MomArgs a) {
   __shared__ TF sh_val[BLOCK * 3 * 9];
   __shared__ int sh_col[BLOCK * 3];
@@ -442,10 +445,38 @@ __global__ void __launch_bounds__(BLOCK, sizeof(TF) == 4 ? (UGSH ? 4 : 3) : 1) k
       // upwind advection (row L = corner 0)
       const TF fl = TF(0.5) * (tm + fabs(tm));
       const TF fr = TF(0.5) * (tm - fabs(tm));
+      // high resolution: deferred correction beta_up,i (x_ip - x_up) . grad
+      // u_i,up on the rhs (navierStokesAssemblerElemTerms.cpp:287-330), x_ip
+      // from the standard trilinear coordinate shape functions
+      TF dcorr[3] = {TF(0), TF(0), TF(0)};
+      if constexpr (HR) {
+        using PC = ScsPt<IP, false>;
+        TF dx[3];
+        const int ku = tmd > 0 ? 0 : R;
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+          TF xi = TF(0);
+          StaticFor<0, 8>::run([&](auto nc) {
+            constexpr int n = decltype(nc)::value;
+            constexpr double N = shape_at<PC, n>();
+            if (N != 0.0) xi += TF(N) * x[n][j];
+          });
+          dx[j] = xi - (tmd > 0 ? x[0][j] : x[R][j]);
+        }
+        const int nu = ku == 0 ? row : __ldg(a.m.conn + 8 * e + perm_at(pw, R));
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+          const TF bu = TF(__ldg(a.betaU + 3 * nu + i));
+          TF g = TF(0);
+#pragma unroll
+          for (int j = 0; j < 3; ++j) g += TF(__ldg(a.gradU + 9 * nu + 3 * i + j)) * dx[j];
+          dcorr[i] = bu * g;
+        }
+      }
 #pragma unroll
       for (int i = 0; i < 3; ++i) {
         const TF up = tmd > 0 ? Uc[0][i] : Uc[R][i];
-        rhs[i] -= tm * up;
+        rhs[i] -= tm * (up + dcorr[i]);
         diag[3 * i + i] += fl;
         nb[RS][3 * i + i] += fr;
       }
@@ -884,6 +915,142 @@ __global__ void __launch_bounds__(BLOCK) k_gradient(GradArgs a) {
   }
 }
 
+// ---------------------------------------------------------------------------
+// High-resolution advection: velocity blending factor
+// (nodeField::updateMinMaxFields, src/field/nodeField/nodeField.hpp:1843-2066,
+// and nodeField::updateBlendingFactorField, :2069-2410 and the relaxation
+// after it), row-owner like the assembly: lane c looks at the incident
+// element where the row node is corner c.
+struct BlendArgs {
+  MeshView m;
+  const double *U, *gradU;
+  double *minU, *maxU, *beta;
+  double beta_max;
+};
+
+// extrema of every velocity component over the row node and its edge
+// neighbours (each SCS ip gives its L node the R value and vice versa)
+__global__ void __launch_bounds__(BLOCK) k_minmax_u(BlendArgs a) {
+  const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 3;
+  const int c = threadIdx.x & 7;
+  const bool rv = row < a.m.nn;
+  const int e = rv ? __ldg(a.m.n2e + 8 * row + c) : -1;
+  double lo[3], hi[3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) lo[i] = hi[i] = rv ? __ldg(a.U + 3 * row + i) : 0.0;
+  if (e >= 0) {
+    const uint32_t pw = perm_word(c);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const int nd = __ldg(a.m.conn + 8 * e + perm_at(pw, k == 0 ? 1 : (k == 1 ? 3 : 4)));
+#pragma unroll
+      for (int i = 0; i < 3; ++i) {
+        const double v = __ldg(a.U + 3 * nd + i);
+        lo[i] = fmin(lo[i], v);
+        hi[i] = fmax(hi[i], v);
+      }
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int o = 1; o < 8; o <<= 1) {
+      lo[i] = fmin(lo[i], __shfl_xor_sync(FULL_MASK, lo[i], o));
+      hi[i] = fmax(hi[i], __shfl_xor_sync(FULL_MASK, hi[i], o));
+    }
+  if (rv && c == 0)
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      a.minU[3 * row + i] = lo[i];
+      a.maxU[3 * row + i] = hi[i];
+    }
+}
+
+// limiter of the row node for the point at dx from it (the reference's
+// formulas: SMALL-stabilised projected increment, the two-sided ratio, the
+// smooth Venkatakrishnan-type map when beta_max < 2)
+__device__ __forceinline__ void blend_limit(const BlendArgs& a, const double (&phi)[3], const double (&lo)[3],
+                                            const double (&hi)[3], const double (&G)[9], const double (&dx)[3],
+                                            double (&beta)[3]) {
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    double rgrad = G[3 * i] * dx[0] + G[3 * i + 1] * dx[1] + G[3 * i + 2] * dx[2];
+    rgrad = rgrad > 0 ? rgrad + SMALL : rgrad - SMALL;
+    const double dmax = hi[i] - phi[i], dmin = lo[i] - phi[i];
+    const double bl = fmax(dmax / rgrad, dmin / rgrad);
+    const double bl12 = fmax(-dmax / rgrad, -dmin / rgrad);
+    double y = fmin(bl, bl12);
+    if (a.beta_max < 2.0 - SMALL) y = (y * y + 2.0 * y) / (y * y + y + 2.0);
+    if (rgrad > 100 * SMALL || rgrad < -100 * SMALL) beta[i] = fmin(beta[i], y);
+  }
+}
+
+__global__ void __launch_bounds__(BLOCK) k_blend_u(BlendArgs a) {
+  const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 3;
+  const int c = threadIdx.x & 7;
+  const bool rv = row < a.m.nn;
+  const int e = rv ? __ldg(a.m.n2e + 8 * row + c) : -1;
+  double beta[3] = {a.beta_max, a.beta_max, a.beta_max};
+  if (e >= 0) {
+    double phi[3], lo[3], hi[3], G[9];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      phi[i] = __ldg(a.U + 3 * row + i);
+      lo[i] = __ldg(a.minU + 3 * row + i);
+      hi[i] = __ldg(a.maxU + 3 * row + i);
+    }
+#pragma unroll
+    for (int k = 0; k < 9; ++k) G[k] = __ldg(a.gradU + 9 * row + k);
+    double x[8][3];
+    int nd[8];
+    gather_x(a.m, e, perm_word(c), x, nd);
+    // interior SCS ips touching the row node (canonical ips 0, 3, 8)
+    StaticFor<0, 3>::run([&](auto qc) {
+      constexpr int IP = decltype(qc)::value == 0 ? 0 : (decltype(qc)::value == 1 ? 3 : 8);
+      using PC = ScsPt<IP, false>;
+      double dx[3];
+#pragma unroll
+      for (int j = 0; j < 3; ++j) {
+        double xi = 0.0;
+        StaticFor<0, 8>::run([&](auto nc) {
+          constexpr int n = decltype(nc)::value;
+          constexpr double N = shape_at<PC, n>();
+          if (N != 0.0) xi += N * x[n][j];
+        });
+        dx[j] = xi - x[0][j];
+      }
+      blend_limit(a, phi, lo, hi, G, dx, beta);
+    });
+    // boundary faces at the row node: the face ip nearest to it (standard
+    // bilinear face shape functions: 9/16, 3/16, 1/16, 3/16)
+    const uint8_t fm = __ldg(a.m.face_mask + e);
+    if (fm) {
+      const uint32_t fw = face_word(c);
+      StaticFor<0, 3>::run([&](auto qc) {
+        constexpr int q = decltype(qc)::value;
+        constexpr int FC = q == 0 ? 0 : (q == 1 ? 3 : 4);
+        if (fm & (1u << ((fw >> (3 * q)) & 7))) {
+          constexpr int f1 = face_node(FC, 1), f2 = face_node(FC, 2), f3 = face_node(FC, 3);
+          double dx[3];
+#pragma unroll
+          for (int j = 0; j < 3; ++j) {
+            const double xi = 0.5625 * x[0][j] + 0.1875 * x[f1][j] + 0.0625 * x[f2][j] + 0.1875 * x[f3][j];
+            dx[j] = xi - x[0][j];
+          }
+          blend_limit(a, phi, lo, hi, G, dx, beta);
+        }
+      });
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int o = 1; o < 8; o <<= 1) beta[i] = fmin(beta[i], __shfl_xor_sync(FULL_MASK, beta[i], o));
+  if (rv && c == 0)
+#pragma unroll
+    for (int i = 0; i < 3; ++i) a.beta[3 * row + i] = 0.75 * a.beta[3 * row + i] + 0.25 * beta[i];
+}
+
 // U += sign * du * gradP / urf_p on all nodes (segregatedFlowEquations.cpp:134-278)
 __global__ void k_vel_correct(int n3, double* U, const double* du, const double* gradP, double f) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -945,12 +1112,17 @@ int launch_momentum(Flow& f, bool mixed) {
     count_launches(1);
   }
   MomArgs a{f.mesh->view(), f.U,       f.gradP, f.div,  f.mDot,          f.rho,
-            f.mu,           f.sideU,   f.xloc32, f.umu32, f.b.A_mom,     f.b.b_mom,
+            f.mu,           f.sideU,   f.betaU, f.gradU, f.xloc32, f.umu32, f.b.A_mom, f.b.b_mom,
             f.du,           f.s.dt,    1.0 / f.s.urf_u, f.s.wall_rhs_relax, f.err_dev};
   const int g = grid_rows(f.mesh->nn);
-  const bool us = f.s.u_shifted, gs = f.s.u_grad_shifted;
+  const bool us = f.s.u_shifted, gs = f.s.u_grad_shifted, hr = f.s.hr != 0;
 #define OA_MOM(US, GS, T)                                                                   \
-  if (us == US && gs == GS) k_momentum<US, GS, T><<<g, BLOCK, 0, f.stream>>>(a);
+  if (us == US && gs == GS) {                                                               \
+    if (hr)                                                                                 \
+      k_momentum<US, GS, T, true><<<g, BLOCK, 0, f.stream>>>(a);                            \
+    else                                                                                    \
+      k_momentum<US, GS, T, false><<<g, BLOCK, 0, f.stream>>>(a);                           \
+  }
   if (mixed) {
     OA_MOM(true, true, float) OA_MOM(true, false, float) OA_MOM(false, true, float) OA_MOM(false, false, float)
   } else {
@@ -1010,6 +1182,16 @@ int launch_gradient(Flow& f, int which) {
     else k_gradient<3, false><<<g, BLOCK, 0, f.stream>>>(a);
   }
   count_launches(1);
+  OA_CUDA(cudaGetLastError());
+  return OA_OK;
+}
+
+int launch_blend_u(Flow& f) {
+  BlendArgs a{f.mesh->view(), f.U, f.gradU, f.minU, f.maxU, f.betaU, f.s.beta_max};
+  const int g = grid_rows(f.mesh->nn);
+  k_minmax_u<<<g, BLOCK, 0, f.stream>>>(a);
+  k_blend_u<<<g, BLOCK, 0, f.stream>>>(a);
+  count_launches(2);
   OA_CUDA(cudaGetLastError());
   return OA_OK;
 }

@@ -60,6 +60,9 @@ struct Case {
   std::vector<int> rowPtr, cols, diagOff;
   // fields
   std::vector<double> U, p, gradU, gradP, du, div, mDot, rho, mu, sideU, wallNode;
+  // high-resolution advection: velocity blending factor and its extrema
+  // fields, [nn][3] each (nodeField blendingFactor / minValue / maxValue)
+  std::vector<double> betaU, minU, maxU;
   // element colours (no two elements of a colour share a node), for the
   // threaded CPU-baseline path
   std::vector<std::vector<int>> colors;
@@ -359,6 +362,80 @@ void update_gradient(Case& c, const std::vector<double>& phi, std::vector<double
 // stationary frame; adjustMatrixForPressureReference
 // (pressureCorrectionAssembler.cpp:19-63). No-slip wall faces add rho*U_bc.A
 // with U_bc tangential to the flat walls, i.e. exact zeros, so they are omitted.
+// Velocity blending factor of the high-resolution scheme:
+// nodeField::updateMinMaxFields (src/field/nodeField/nodeField.hpp:1843-2066,
+// defaults: no extrema expansion, no smoothing) followed by
+// nodeField::updateBlendingFactorField (:2069-2410 interior and boundary ips,
+// then the relaxation beta = 0.75 beta_prev + 0.25 beta, :2410+). Interior
+// ips: the extrema over the edge neighbours, then the limiter at both ends of
+// every SCS ip with dx = x_ip - x_node (x_ip from the standard trilinear
+// coordinate shape functions); boundary faces: the limiter at each face ip's
+// nearest node (standard face shape functions for x_ip).
+void update_blending_u(Case& c) {
+  const long n3 = 3L * c.nn;
+  c.minU.assign(c.U.begin(), c.U.end());
+  c.maxU.assign(c.U.begin(), c.U.end());
+  for (int e = 0; e < c.ne; ++e) {
+    const int* en = &c.conn[8 * e];
+    for (int ip = 0; ip < NSCS; ++ip) {
+      const int L = en[LR[ip][0]], R = en[LR[ip][1]];
+      for (int i = 0; i < 3; ++i) {
+        c.minU[3 * L + i] = std::min(c.minU[3 * L + i], c.U[3 * R + i]);
+        c.maxU[3 * L + i] = std::max(c.maxU[3 * L + i], c.U[3 * R + i]);
+        c.minU[3 * R + i] = std::min(c.minU[3 * R + i], c.U[3 * L + i]);
+        c.maxU[3 * R + i] = std::max(c.maxU[3 * R + i], c.U[3 * L + i]);
+      }
+    }
+  }
+  const std::vector<double> prev = c.betaU;
+  std::vector<double> beta(n3, c.s.beta_max);
+  // limiter at node nd for the point xip (reference formulas, both loops)
+  auto limit = [&](int nd, const double* xip) {
+    double dx[3];
+    for (int j = 0; j < 3; ++j) dx[j] = xip[j] - c.x[3 * nd + j];
+    for (int i = 0; i < 3; ++i) {
+      double rgrad = 0.0;
+      for (int j = 0; j < 3; ++j) rgrad += c.gradU[9 * nd + 3 * i + j] * dx[j];
+      if (rgrad > 0)
+        rgrad = rgrad + SMALL;
+      else
+        rgrad = rgrad - SMALL;
+      const double dmax = c.maxU[3 * nd + i] - c.U[3 * nd + i];
+      const double dmin = c.minU[3 * nd + i] - c.U[3 * nd + i];
+      const double betaLocal = std::max(dmax / rgrad, dmin / rgrad);
+      const double beta12Local = std::max(-dmax / rgrad, -dmin / rgrad);
+      double y = std::min(betaLocal, beta12Local);
+      if (c.s.beta_max < 2.0 - SMALL) y = ((y * y + 2.0 * y) / (y * y + y + 2.0));
+      if ((rgrad > 100 * SMALL) || (rgrad < -100 * SMALL)) beta[3 * nd + i] = std::min(beta[3 * nd + i], y);
+    }
+  };
+  double Nc[96];
+  oracle::hex8::scs_shape(Nc, false);
+  for (int e = 0; e < c.ne; ++e) {
+    const int* en = &c.conn[8 * e];
+    for (int ip = 0; ip < NSCS; ++ip) {
+      double xip[3] = {0.0, 0.0, 0.0};
+      for (int a = 0; a < 8; ++a)
+        for (int j = 0; j < 3; ++j) xip[j] += Nc[8 * ip + a] * c.x[3 * en[a] + j];
+      limit(en[LR[ip][0]], xip);
+      limit(en[LR[ip][1]], xip);
+    }
+  }
+  double Nf[16];
+  oracle::hex8::face_shape(Nf, false);
+  for (int f = 0; f < c.nf; ++f) {
+    const int* en = &c.conn[8 * c.fElem[f]];
+    const int o = c.fOrd[f];
+    for (int ip = 0; ip < 4; ++ip) {
+      double xip[3] = {0.0, 0.0, 0.0};
+      for (int k = 0; k < 4; ++k)
+        for (int j = 0; j < 3; ++j) xip[j] += Nf[4 * ip + k] * c.x[3 * en[oracle::hex8::FACE_NODES[o][k]] + j];
+      limit(en[oracle::hex8::FACE_NODES[o][ip]], xip);
+    }
+  }
+  for (long k = 0; k < n3; ++k) c.betaU[k] = 0.75 * prev[k] + 0.25 * beta[k];
+}
+
 void assemble_pcorr(Case& c, double* A, double* b) {
   const int nnz = c.rowPtr[c.nn];
   std::fill(A, A + nnz, 0.0);
@@ -466,9 +543,23 @@ void assemble_momentum(Case& c, double* A, double* b) {
       const double tm = c.mDot[12 * e + ip];
       double muIp = 0.0;
       for (int a = 0; a < 8; ++a) muIp += Nv[8 * ip + a] * mue[a];
+      // high resolution: deferred correction beta_up,i (x_ip - x_up) . grad u_i,up
+      // (navierStokesAssemblerElemTerms.cpp:287-330), x_ip from the standard
+      // coordinate shape functions
+      double xip[3] = {0.0, 0.0, 0.0};
+      if (c.s.hr)
+        for (int a = 0; a < 8; ++a)
+          for (int j = 0; j < 3; ++j) xip[j] += Nc[8 * ip + a] * xe[3 * a + j];
       for (int i = 0; i < 3; ++i) {
         const double up = tm > 0 ? Ue[3 * il + i] : Ue[3 * ir + i];
-        const double af = tm * up;
+        double dcorr = 0.0;
+        if (c.s.hr) {
+          const int iu = tm > 0 ? il : ir;
+          const int nu = en[iu];
+          for (int j = 0; j < 3; ++j)
+            dcorr += c.betaU[3 * nu + i] * (xip[j] - xe[3 * iu + j]) * c.gradU[9 * nu + 3 * i + j];
+        }
+        const double af = tm * (up + dcorr);
         const int iL = 3 * il + i, iR = 3 * ir + i;
         const int rowL = iL * 24, rowR = iR * 24;
         rhs[iL] -= af;
@@ -949,6 +1040,7 @@ void simple_iteration(Case& c, orc_iter_stats* st) {
   update_gradient<1>(c, c.p, c.gradP, c.s.p_shifted);
   for (long i = 0; i < 3L * c.nn; ++i) c.U[i] -= iu * c.du[i] * c.gradP[i];
   update_gradient<3>(c, c.U, c.gradU, c.s.u_shifted);
+  if (c.s.hr) update_blending_u(c);  // segregatedFlowEquations.cpp:287-288
 }
 
 }  // namespace
@@ -1000,6 +1092,9 @@ void* orc_case_create(int nn, int ne, const double* x, const int* conn, int nf, 
   c->mu.assign(nn, s->mu);
   c->sideU.assign(3L * nn, 0.0);
   c->wallNode.assign(nn, 0.0);
+  c->betaU.assign(3L * nn, 0.0);  // setupBlendingFactorField: zero (nodeField.hpp:733-745)
+  c->minU.assign(3L * nn, 0.0);
+  c->maxU.assign(3L * nn, 0.0);
   if (s->ref_node >= 0) c->refNodes.push_back(s->ref_node);
   {
     // mean element edge length over every element's 12 edges (element order)
@@ -1059,6 +1154,9 @@ double* orc_case_field(void* h, const char* name, long* len) {
   else if (n == "sideU") v = &c->sideU;
   else if (n == "wallNode") v = &c->wallNode;
   else if (n == "x") v = &c->x;
+  else if (n == "betaU") v = &c->betaU;
+  else if (n == "minU") v = &c->minU;
+  else if (n == "maxU") v = &c->maxU;
   if (!v) {
     *len = 0;
     return nullptr;
@@ -1084,6 +1182,7 @@ void orc_case_graph(void* h, int* row_ptr, int* cols) {
 void orc_initialize(void* h) {
   Case* c = static_cast<Case*>(h);
   update_gradient<3>(*c, c->U, c->gradU, c->s.u_shifted);
+  if (c->s.hr) update_blending_u(*c);  // navierStokesEquation::initialize
   init_mdot(*c);
   update_div(*c);
   update_gradient<1>(*c, c->p, c->gradP, c->s.p_shifted);
@@ -1101,6 +1200,8 @@ void orc_update_grad_p(void* h) {
   Case* c = static_cast<Case*>(h);
   update_gradient<1>(*c, c->p, c->gradP, c->s.p_shifted);
 }
+void orc_update_blending_u(void* h) { update_blending_u(*static_cast<Case*>(h)); }
+
 void orc_update_grad_u(void* h) {
   Case* c = static_cast<Case*>(h);
   update_gradient<3>(*c, c->U, c->gradU, c->s.u_shifted);

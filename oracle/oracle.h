@@ -39,6 +39,8 @@ typedef struct orc_settings {
   double mom_rtol;
   int pc_maxit;
   double pc_rtol;
+  int hr;              /* advection scheme: 0 upwind, 1 high resolution (Barth-Jespersen blended deferred correction) */
+  double beta_max;     /* upper limit of the blending factor (nodeField.h:150) */
 } orc_settings;
 
 typedef struct orc_iter_stats {
@@ -83,6 +85,9 @@ void orc_update_mdot(void* h);
 void orc_update_div(void* h);
 void orc_update_grad_p(void* h);
 void orc_update_grad_u(void* h);
+/* high-resolution velocity blending factor (min/max fields, limiter,
+ * relaxation) from the current U and grad U: field "betaU" */
+void orc_update_blending_u(void* h);
 /* BiCGStab with (block-)Jacobi preconditioning; returns iterations, res = final
  * relative residual. bs = 1 or 3. */
 int orc_bicgstab(void* h, int bs, const double* A, const double* b, double* x,

@@ -36,6 +36,8 @@ class Settings(C.Structure):
         ("mom_rtol", C.c_double),
         ("pc_maxit", C.c_int),
         ("pc_rtol", C.c_double),
+        ("hr", C.c_int),
+        ("beta_max", C.c_double),
     ]
 
 
@@ -55,7 +57,7 @@ def default_settings(**kw) -> Settings:
     linear_linear velocity interpolation and the controls.h defaults."""
     d = dict(rho=1.0, mu=0.01, urf_u=0.9, urf_p=0.1, dt=1.0, grad_urf=0.5625, mdot_urf=1.0,
              wall_rhs_relax=0.75, u_shifted=1, u_grad_shifted=1, p_shifted=1, p_grad_shifted=1,
-             ref_node=0, mom_maxit=200, mom_rtol=1e-12, pc_maxit=5000, pc_rtol=1e-12)
+             ref_node=0, mom_maxit=200, mom_rtol=1e-12, pc_maxit=5000, pc_rtol=1e-12, hr=0, beta_max=1.0)
     d.update(kw)
     return Settings(**d)
 
@@ -131,7 +133,7 @@ def lib():
                                     C.c_int, C.c_int, P(C.c_double)]
         L.orc_case_graph.argtypes = [C.c_void_p, ip, ip]
         for name in ["orc_initialize", "orc_update_mdot", "orc_update_div", "orc_update_grad_p",
-                     "orc_update_grad_u"]:
+                     "orc_update_grad_u", "orc_update_blending_u"]:
             getattr(L, name).argtypes = [C.c_void_p]
         L.orc_assemble_momentum.argtypes = [C.c_void_p, dp, dp]
         L.orc_assemble_pcorr.argtypes = [C.c_void_p, dp, dp]
@@ -262,6 +264,9 @@ class FlowCase:
 
     def update_grad_u(self):
         lib().orc_update_grad_u(self.h)
+
+    def update_blending_u(self):
+        lib().orc_update_blending_u(self.h)
 
     def bicgstab(self, bs, A, b, rtol=1e-12, maxit=2000):
         x = np.zeros_like(b)

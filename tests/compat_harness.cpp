@@ -146,6 +146,8 @@ static int gpu_checks(const std::string& dir) {
   s.precision = OA_PREC_FP64;
   s.pc_amg = 1;
   s.use_graphs = 0;
+  s.hr = 0;
+  s.beta_max = 1.0;
   oa_flow* flow = nullptr;
   openaccel_b200::check(oa_flow_create(mesh, &s, bnd.data(), nb, &flow));
   openaccel_b200::check(oa_flow_initialize(flow));

@@ -200,3 +200,33 @@ def test_oracle_scatter_matches_reference_apply_coeff(oracle_mod, bs):
     np.testing.assert_array_equal(A_o, A_r)
     np.testing.assert_array_equal(b_o, b_r)
     assert np.abs(A_o).sum() > 0
+
+
+def test_blending_factor_known_answers(oracle_mod):
+    """High-resolution limiter (nodeField::updateBlendingFactorField) on a
+    uniform 4^3 mesh with U = (x, 0, 0): along x the projected increment to an
+    SCS ip is h/2 against an extremum h away, ratio 2, which the smooth map
+    sends to 1 = beta_max; components with zero gradient are not limited; on
+    the x = 0 and x = 1 faces one extremum is the node's own value, so
+    beta_x = 0. After the first update the relaxation 0.75 * 0 + 0.25 * beta
+    leaves 0.25 inside and 0 on those faces; a constant field stays at
+    0.25 * beta_max."""
+    m = meshgen.cavity(4)
+    c = oracle_mod.FlowCase(m, oracle_mod.default_settings(hr=1, beta_max=1.0))
+    x = m.coords
+    U = np.zeros((m.nn, 3))
+    U[:, 0] = x[:, 0]
+    c.field("U")[:] = U.ravel()
+    for _ in range(60):  # the gradient under-relaxation (0.5625) converges to the exact gradient
+        c.update_grad_u()
+    c.update_blending_u()
+    beta = c.field("betaU").reshape(-1, 3)
+    xb = (np.isclose(x[:, 0], 0.0)) | (np.isclose(x[:, 0], 1.0))
+    np.testing.assert_allclose(beta[~xb, 0], 0.25, atol=1e-12)
+    np.testing.assert_allclose(beta[xb, 0], 0.0, atol=1e-12)
+    np.testing.assert_allclose(beta[:, 1:], 0.25, atol=1e-12)
+    c2 = oracle_mod.FlowCase(m, oracle_mod.default_settings(hr=1, beta_max=0.8))
+    c2.field("U")[:] = 1.0
+    c2.update_grad_u()
+    c2.update_blending_u()
+    np.testing.assert_allclose(c2.field("betaU"), 0.2, atol=1e-15)
