@@ -58,6 +58,10 @@ typedef struct oa_flow_settings {
   int hr;                       /* advection: 0 upwind, 1 high resolution (advectionSchemeType::highResolution:
                                    blended deferred correction, nodeField::updateBlendingFactorField) */
   double beta_max;              /* upper limit of the blending factor (nodeField.h:150, default 1) */
+  int du_mode;                  /* pressure-velocity coupling coefficient (computeDUCoefficients,
+                                   navierStokesAssembler.cpp:84-232): 0 SIMPLE D = V/a_ii, 1 SIMPLEC (consistent_:
+                                   D~ = V/(a_ii + sum of off-diagonals) on the pressure-correction lhs and in the
+                                   velocity correction), 2 fractional step D = dt/rho */
 } oa_flow_settings;
 
 /* Convergence record of one linear solve: the ControlData that liblinsolve
@@ -134,7 +138,8 @@ void oa_flow_destroy(oa_flow* f);
 /* Host <-> device copies of a named field: "U" [nn][3], "p" [nn], "gradU"
  * [nn][9], "gradP" [nn][3], "du" [nn][3], "div" [nn], "mDot" [ne][12],
  * "sideU" [nn][3], "rho" [nn], "mu" [nn]; with settings.hr also the velocity
- * blending factor "betaU" and its extrema fields "minU", "maxU" [nn][3].
+ * blending factor "betaU" and its extrema fields "minU", "maxU" [nn][3]; with
+ * SIMPLEC (du_mode 1) "duTilde" [nn][3].
  * n is the number of doubles. */
 int oa_flow_set_field(oa_flow* f, const char* name, const double* host, long n);
 int oa_flow_get_field(oa_flow* f, const char* name, double* host, long n);

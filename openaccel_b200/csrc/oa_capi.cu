@@ -110,6 +110,7 @@ double* field_ptr(Flow& f, const std::string& n, size_t* len) {
   if (f.betaU && n == "betaU") { *len = 3 * nn; return f.betaU; }
   if (f.minU && n == "minU") { *len = 3 * nn; return f.minU; }
   if (f.maxU && n == "maxU") { *len = 3 * nn; return f.maxU; }
+  if (f.duT && n == "duTilde") { *len = 3 * nn; return f.duT; }
   *len = 0;
   return nullptr;
 }
@@ -382,6 +383,8 @@ int oa_flow_create(oa_mesh* M, const oa_flow_settings* s, const double* bnd_velo
   if (s->precision != OA_PREC_FP64 && s->precision != OA_PREC_MIXED) return fail(OA_ERR_ARG, "oa_flow_create: unknown precision");
   if (s->hr != 0 && s->hr != 1) return fail(OA_ERR_ARG, "oa_flow_create: advection scheme must be 0 (upwind) or 1 (high resolution)");
   if (s->hr && !(s->beta_max > 0)) return fail(OA_ERR_ARG, "oa_flow_create: beta_max must be > 0 for high resolution");
+  if (s->du_mode < 0 || s->du_mode > 2)
+    return fail(OA_ERR_ARG, "oa_flow_create: du_mode must be 0 (SIMPLE), 1 (SIMPLEC) or 2 (fractional step)");
   if (s->ref_node >= M->m.nn) return fail(OA_ERR_ARG, "oa_flow_create: ref_node out of range");
   if (M->m.topo != OA_TOPO_HEX8) return fail(OA_ERR_MESH, "oa_flow_create: the flow path needs a hex8 mesh");
   *out = nullptr;
@@ -412,7 +415,8 @@ int oa_flow_create(oa_mesh* M, const oa_flow_settings* s, const double* bnd_velo
       (st = dalloc(&f.b.x_pc, nn)) || (st = dalloc(&f.err_dev, 1)) || (st = dalloc(&H->scal, 8)) ||
       (st = dalloc(&f.red, (size_t)partials_size())) || (st = dalloc(&f.ref_flag, nn)) ||
       (s->hr && ((st = dalloc(&f.betaU, 3 * nn)) || (st = dalloc(&f.minU, 3 * nn)) ||
-                 (st = dalloc(&f.maxU, 3 * nn))))) {
+                 (st = dalloc(&f.maxU, 3 * nn)))) ||
+      (s->du_mode == 1 && (st = dalloc(&f.duT, 3 * nn)))) {
     oa_flow_destroy(H);
     return st;
   }
@@ -447,6 +451,7 @@ int oa_flow_create(oa_mesh* M, const oa_flow_settings* s, const double* bnd_velo
   cudaMemset(f.div, 0, sizeof(double) * nn);
   cudaMemset(f.mDot, 0, sizeof(double) * 12 * ne);
   cudaMemset(f.err_dev, 0, sizeof(int));
+  if (f.duT) cudaMemset(f.duT, 0, sizeof(double) * 3 * nn);
   if (f.betaU) {
     // setupBlendingFactorField starts the blending factor at zero
     // (src/field/nodeField/nodeField.hpp:733-745)
@@ -491,7 +496,7 @@ void oa_flow_destroy(oa_flow* H) {
   void* ptrs[] = {f.U,       f.p,       f.gradU,   f.gradP,   f.du,      f.div,    f.mDot,  f.pc_flux,
                   f.pc_coef, f.xloc32,  f.umu32,   f.rho,     f.mu,      f.sideU,  f.b.A_mom, f.b.b_mom,
                   f.b.A_pc,  f.b.b_pc,  f.b.x_mom, f.b.x_pc,  f.err_dev, H->scal,  f.red,   f.ref_flag,
-                  f.betaU,   f.minU,    f.maxU};
+                  f.betaU,   f.minU,    f.maxU,    f.duT};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (H->hscal) cudaFreeHost(H->hscal);

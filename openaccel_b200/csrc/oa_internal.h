@@ -70,6 +70,8 @@ struct Flow {
   // high-resolution advection (settings.hr): velocity blending factor and the
   // extrema it is limited by, [nn][3] each
   double *betaU = nullptr, *minU = nullptr, *maxU = nullptr;
+  // SIMPLEC (settings.du_mode == 1): the consistent coefficient D~ [nn][3]
+  double* duT = nullptr;
   // [ne][12] Rhie-Chow mass flux of each SCS ip with the pressure-correction
   // equation's upwind density (its right-hand side), written by the mass-flow
   // kernel and summed per row by the pressure-correction kernel

@@ -277,7 +277,9 @@ struct MomArgs {
   void* A;
   void* b;
   double* du;
+  double* duT;   // SIMPLEC: D~ [nn][3]
   double dt, urf_inv, wall_relax;
+  int du_mode;   // 0 SIMPLE, 1 SIMPLEC, 2 fractional step
   int* err;
 };
 
@@ -547,6 +549,12 @@ __global__ void __launch_bounds__(BLOCK, sizeof(TF) == 4 ? (UGSH ? 4 : 3) : 1) k
   for (int k = 0; k < 9; ++k) diag[k] = rowsum8(diag[k]);
 #pragma unroll
   for (int k = 0; k < 3; ++k) rhs[k] = rowsum8(rhs[k]);
+  // SIMPLEC: sum of the row's off-diagonal (i, i) coefficients (the CSR
+  // off-diagonal entries are the lanes' neighbour blocks summed)
+  double off[3] = {0.0, 0.0, 0.0};
+  if (a.du_mode == 1)
+#pragma unroll
+    for (int k = 0; k < 3; ++k) off[k] = double(rowsum8(TF(nb[0][4 * k] + nb[1][4 * k] + nb[2][4 * k])));
   if (rv) {
     // node terms, relaxation, wall rhs relaxation, DU
     const double vol = __ldg(a.m.vol + row);
@@ -571,9 +579,13 @@ __global__ void __launch_bounds__(BLOCK, sizeof(TF) == 4 ? (UGSH ? 4 : 3) : 1) k
       rhs[k] = TF(r);
     }
     if (c == 0) {
+      // computeDUCoefficients (navierStokesAssembler.cpp:84-232): V / (a_ii +
+      // SMALL), or dt / rho (fractional step, steady gamma1 = 1); SIMPLEC also
+      // D~ = V / (a_ii + off-diagonal sum + SMALL)
 #pragma unroll
       for (int k = 0; k < 3; ++k) {
-        a.du[3 * row + k] = vol / (double(diag[4 * k]) + SMALL);
+        a.du[3 * row + k] = a.du_mode == 2 ? a.dt / rho : vol / (double(diag[4 * k]) + SMALL);
+        if (a.du_mode == 1) a.duT[3 * row + k] = vol / (double(diag[4 * k]) + off[k] + SMALL);
         static_cast<TF*>(a.b)[3 * row + k] = rhs[k];
       }
     }
@@ -587,6 +599,7 @@ __global__ void __launch_bounds__(BLOCK, sizeof(TF) == 4 ? (UGSH ? 4 : 3) : 1) k
 struct MdotArgs {
   MeshView m;
   const double *U, *p, *gradP, *du, *rho;
+  const double* du_lhs;  // diffusivity of the pressure-correction lhs: D, or D~ with SIMPLEC
   double* mDot;
   double* flux;  // [ne][12] pressure-correction ip fluxes (staging modes)
   void* coef;    // [ne][8][3] pressure-correction lhs coefficients per corner (staging modes)
@@ -665,7 +678,9 @@ int launch_scs_area(DeviceMesh& m, cudaStream_t st) {
 // STAGE: also write the pressure-correction ip fluxes and corner coefficients
 // (TC: the matrix precision); without it the kernel keeps the register budget
 // of four blocks per SM.
-template <bool USH, bool PGSH, class TC, bool STAGE>
+// SC (staging with SIMPLEC): the staged lhs coefficients take D~ (du_lhs)
+// while the fluxes keep D.
+template <bool USH, bool PGSH, class TC, bool STAGE, bool SC = false>
 __global__ void __launch_bounds__(BLOCK, STAGE ? 3 : 4) k_mdot(MdotArgs a) {
   const int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= a.m.ne) return;
@@ -692,7 +707,8 @@ __global__ void __launch_bounds__(BLOCK, STAGE ? 3 : 4) k_mdot(MdotArgs a) {
     constexpr int IP = decltype(ic)::value;
     using PV = ScsPt<IP, USH>;
     using PG = ScsPt<IP, PGSH>;
-    double u[3] = {0, 0, 0}, duip[3] = {0, 0, 0}, rhoIp = 0.0;
+    double u[3] = {0, 0, 0}, duip[3] = {0, 0, 0}, dulip[3] = {0, 0, 0}, rhoIp = 0.0;
+    constexpr bool simplec = STAGE && SC;
     StaticFor<0, 8>::run([&](auto nc) {
       constexpr int n = decltype(nc)::value;
       constexpr double N = shape_at<PV, n>();
@@ -707,9 +723,17 @@ __global__ void __launch_bounds__(BLOCK, STAGE ? 3 : 4) k_mdot(MdotArgs a) {
           load3(a.du, nd[n], dn);
 #pragma unroll
           for (int j = 0; j < 3; ++j) duip[j] += N * dn[j];
+          if (simplec) {
+            load3(a.du_lhs, nd[n], dn);
+#pragma unroll
+            for (int j = 0; j < 3; ++j) dulip[j] += N * dn[j];
+          }
         }
       }
     });
+    if (!simplec)
+#pragma unroll
+      for (int j = 0; j < 3; ++j) dulip[j] = duip[j];
     double Aip[3];
 #pragma unroll
     for (int k = 0; k < 3; ++k) Aip[k] = __ldg(a.m.scs_area + 36L * e + 3 * IP + k);
@@ -764,7 +788,7 @@ __global__ void __launch_bounds__(BLOCK, STAGE ? 3 : 4) k_mdot(MdotArgs a) {
         // A . grad N_n, for the edge neighbours of L (added to L's row) and of
         // R (subtracted from R's row: the ip's area points away from L)
         constexpr int L = lr(IP, 0), R = lr(IP, 1);
-        const double w[3] = {-rhoHR * duip[0] * Aip[0], -rhoHR * duip[1] * Aip[1], -rhoHR * duip[2] * Aip[2]};
+        const double w[3] = {-rhoHR * dulip[0] * Aip[0], -rhoHR * dulip[1] * Aip[1], -rhoHR * dulip[2] * Aip[2]};
         StaticFor<0, 3>::run([&](auto sc) {
           constexpr int sl = decltype(sc)::value;
           constexpr int nl = edge_nbr(L, sl), nr = edge_nbr(R, sl);
@@ -1113,7 +1137,7 @@ int launch_momentum(Flow& f, bool mixed) {
   }
   MomArgs a{f.mesh->view(), f.U,       f.gradP, f.div,  f.mDot,          f.rho,
             f.mu,           f.sideU,   f.betaU, f.gradU, f.xloc32, f.umu32, f.b.A_mom, f.b.b_mom,
-            f.du,           f.s.dt,    1.0 / f.s.urf_u, f.s.wall_rhs_relax, f.err_dev};
+            f.du,           f.duT,     f.s.dt,  1.0 / f.s.urf_u, f.s.wall_rhs_relax, f.s.du_mode, f.err_dev};
   const int g = grid_rows(f.mesh->nn);
   const bool us = f.s.u_shifted, gs = f.s.u_grad_shifted, hr = f.s.hr != 0;
 #define OA_MOM(US, GS, T)                                                                   \
@@ -1138,21 +1162,31 @@ int launch_momentum(Flow& f, bool mixed) {
 // staging only (ip fluxes and corner coefficients from the current mass flow,
 // which stays unchanged); 3: update and staging
 static int launch_mdot_impl(Flow& f, int mode) {
-  MdotArgs a{f.mesh->view(), f.U,          f.p,          f.gradP,   f.du,     f.rho, f.mDot, f.pc_flux,
+  MdotArgs a{f.mesh->view(), f.U,          f.p,          f.gradP,   f.du,     f.rho,
+             f.s.du_mode == 1 ? f.duT : f.du, f.mDot, f.pc_flux,
              f.pc_coef,      f.s.mdot_urf, mode == 1 ? 1 : 0, mode == 2 ? 1 : 0, f.err_dev};
   const int g = (f.mesh->ne + BLOCK - 1) / BLOCK;
   const bool us = f.s.u_shifted, ps = f.s.p_grad_shifted;
-#define OA_MD(T, ST)                                                            \
-  if (us && ps) k_mdot<true, true, T, ST><<<g, BLOCK, 0, f.stream>>>(a);        \
-  else if (us && !ps) k_mdot<true, false, T, ST><<<g, BLOCK, 0, f.stream>>>(a); \
-  else if (!us && ps) k_mdot<false, true, T, ST><<<g, BLOCK, 0, f.stream>>>(a); \
-  else k_mdot<false, false, T, ST><<<g, BLOCK, 0, f.stream>>>(a);
+#define OA_MD(T, ST, SC)                                                                \
+  if (us && ps) k_mdot<true, true, T, ST, SC><<<g, BLOCK, 0, f.stream>>>(a);            \
+  else if (us && !ps) k_mdot<true, false, T, ST, SC><<<g, BLOCK, 0, f.stream>>>(a);     \
+  else if (!us && ps) k_mdot<false, true, T, ST, SC><<<g, BLOCK, 0, f.stream>>>(a);     \
+  else k_mdot<false, false, T, ST, SC><<<g, BLOCK, 0, f.stream>>>(a);
+  const bool sc = f.s.du_mode == 1;
   if (mode == 0 || mode == 1) {
-    OA_MD(double, false)
+    OA_MD(double, false, false)
   } else if (f.s.precision == OA_PREC_MIXED) {
-    OA_MD(float, true)
+    if (sc) {
+      OA_MD(float, true, true)
+    } else {
+      OA_MD(float, true, false)
+    }
   } else {
-    OA_MD(double, true)
+    if (sc) {
+      OA_MD(double, true, true)
+    } else {
+      OA_MD(double, true, false)
+    }
   }
 #undef OA_MD
   count_launches(1);
@@ -1198,7 +1232,9 @@ int launch_blend_u(Flow& f) {
 
 int launch_axpy_du_gradp(Flow& f, double sign) {
   const int n3 = 3 * f.mesh->nn;
-  k_vel_correct<<<(n3 + 255) / 256, 256, 0, f.stream>>>(n3, f.U, f.du, f.gradP, sign / f.s.urf_p);
+  // D, or D~ with SIMPLEC (segregatedFlowEquations.cpp:134-278)
+  k_vel_correct<<<(n3 + 255) / 256, 256, 0, f.stream>>>(n3, f.U, f.s.du_mode == 1 ? f.duT : f.du, f.gradP,
+                                                         sign / f.s.urf_p);
   count_launches(1);
   OA_CUDA(cudaGetLastError());
   return OA_OK;

@@ -52,7 +52,7 @@ class FlowSettings(C.Structure):
         ("p_shifted", C.c_int), ("p_grad_shifted", C.c_int), ("ref_node", C.c_int),
         ("mom_maxit", C.c_int), ("mom_rtol", C.c_double), ("pc_maxit", C.c_int), ("pc_rtol", C.c_double),
         ("precision", C.c_int), ("pc_amg", C.c_int), ("use_graphs", C.c_int), ("hr", C.c_int),
-        ("beta_max", C.c_double),
+        ("beta_max", C.c_double), ("du_mode", C.c_int),
     ]
 
 
@@ -123,7 +123,7 @@ def default_settings(**kw) -> FlowSettings:
     d = dict(rho=1.0, mu=0.01, urf_u=0.9, urf_p=0.1, dt=1.0, grad_urf=0.5625, mdot_urf=1.0,
              wall_rhs_relax=0.75, u_shifted=1, u_grad_shifted=1, p_shifted=1, p_grad_shifted=1,
              ref_node=0, mom_maxit=200, mom_rtol=1e-6, pc_maxit=5000, pc_rtol=1e-8,
-             precision=OA_PREC_FP64, pc_amg=1, use_graphs=0, hr=0, beta_max=1.0)
+             precision=OA_PREC_FP64, pc_amg=1, use_graphs=0, hr=0, beta_max=1.0, du_mode=0)
     d.update(kw)
     return FlowSettings(**d)
 
@@ -257,7 +257,7 @@ class Flow:
     """Segregated laminar flow state on the device (oa_flow_create)."""
 
     FIELD_SHAPES = {"U": 3, "p": 1, "gradU": 9, "gradP": 3, "du": 3, "div": 1, "sideU": 3, "rho": 1, "mu": 1,
-                    "betaU": 3, "minU": 3, "maxU": 3}
+                    "betaU": 3, "minU": 3, "maxU": 3, "duTilde": 3}
 
     def __init__(self, mesh: Mesh, settings: FlowSettings | None = None):
         self.mesh = mesh

@@ -63,6 +63,8 @@ struct Case {
   // high-resolution advection: velocity blending factor and its extrema
   // fields, [nn][3] each (nodeField blendingFactor / minValue / maxValue)
   std::vector<double> betaU, minU, maxU;
+  // SIMPLEC: the consistent coefficient D~ [nn][3] (flowModel duTilde)
+  std::vector<double> duT;
   // element colours (no two elements of a colour share a node), for the
   // threaded CPU-baseline path
   std::vector<std::vector<int>> colors;
@@ -460,12 +462,16 @@ void assemble_pcorr(Case& c, double* A, double* b) {
     for (int ip = 0; ip < NSCS; ++ip) {
       const int il = LR[ip][0], ir = LR[ip][1];
       const double tm = c.mDot[12 * e + ip];
-      double u[3] = {0, 0, 0}, du[3] = {0, 0, 0}, dp[3] = {0, 0, 0}, Gp[3] = {0, 0, 0};
+      // the lhs diffusivity is D~ with SIMPLEC, the rhs keeps D
+      // (pressureCorrectionAssemblerElemTerms.cpp:126-134)
+      const std::vector<double>& dl = c.s.du_mode == 1 ? c.duT : c.du;
+      double u[3] = {0, 0, 0}, du[3] = {0, 0, 0}, dul[3] = {0, 0, 0}, dp[3] = {0, 0, 0}, Gp[3] = {0, 0, 0};
       for (int a = 0; a < 8; ++a) {
         const double r = Nv[8 * ip + a];
         for (int j = 0; j < 3; ++j) {
           u[j] += r * c.U[3 * en[a] + j];
           du[j] += r * c.du[3 * en[a] + j];
+          dul[j] += r * dl[3 * en[a] + j];
           dp[j] += g[24 * ip + 3 * a + j] * c.p[en[a]];
           Gp[j] += w[a] * c.gradP[3 * en[a] + j];
         }
@@ -473,7 +479,7 @@ void assemble_pcorr(Case& c, double* A, double* b) {
       const double rhoHR = tm > 0 ? c.rho[en[il]] : c.rho[en[ir]];
       for (int a = 0; a < 8; ++a) {
         double f = 0.0;
-        for (int j = 0; j < 3; ++j) f += -rhoHR * du[j] * g[24 * ip + 3 * a + j] * Ar[3 * ip + j];
+        for (int j = 0; j < 3; ++j) f += -rhoHR * dul[j] * g[24 * ip + 3 * a + j] * Ar[3 * ip + j];
         lhs[8 * il + a] += f;
         lhs[8 * ir + a] -= f;
       }
@@ -670,10 +676,22 @@ void assemble_momentum(Case& c, double* A, double* b) {
   for (int i = 0; i < c.nn; ++i)
     if (c.wallNode[i] != 0.0)
       for (int k = 0; k < 3; ++k) b[3 * i + k] *= c.s.wall_rhs_relax;
-  // DU coefficients
+  // DU coefficients: navierStokesAssembler::computeDUCoefficients
+  // (src/assemble/flow/segregatedFlow/navierStokesAssembler/navierStokesAssembler.cpp:84-232):
+  // D = V / (a_ii + SMALL), or dt / rho for the fractional-step method (steady:
+  // gamma1 = 1, dt the physical timescale); SIMPLEC also D~ = V / (a_ii + sum
+  // of the row's off-diagonal (i, i) coefficients + SMALL)
   for (int i = 0; i < c.nn; ++i) {
     const double* d = &A[9L * (c.rowPtr[i] + c.diagOff[i])];
-    for (int k = 0; k < 3; ++k) c.du[3 * i + k] = c.vol[i] / (d[4 * k] + SMALL);
+    for (int k = 0; k < 3; ++k)
+      c.du[3 * i + k] = c.s.du_mode == 2 ? c.s.dt / c.rho[i] : c.vol[i] / (d[4 * k] + SMALL);
+    if (c.s.du_mode == 1)
+      for (int k = 0; k < 3; ++k) {
+        double off = 0.0;
+        for (int q = c.rowPtr[i]; q < c.rowPtr[i + 1]; ++q)
+          if (q - c.rowPtr[i] != c.diagOff[i]) off += A[9L * q + 4 * k];
+        c.duT[3 * i + k] = c.vol[i] / (d[4 * k] + off + SMALL);
+      }
   }
 }
 
@@ -1035,10 +1053,12 @@ void simple_iteration(Case& c, orc_iter_stats* st) {
   }
   update_mdot(c);
   update_div(c);
+  // velocity correction with D, or D~ with SIMPLEC (segregatedFlowEquations.cpp:134-278)
   const double iu = 1.0 / c.s.urf_p;
-  for (long i = 0; i < 3L * c.nn; ++i) c.U[i] += iu * c.du[i] * c.gradP[i];
+  const std::vector<double>& dc = c.s.du_mode == 1 ? c.duT : c.du;
+  for (long i = 0; i < 3L * c.nn; ++i) c.U[i] += iu * dc[i] * c.gradP[i];
   update_gradient<1>(c, c.p, c.gradP, c.s.p_shifted);
-  for (long i = 0; i < 3L * c.nn; ++i) c.U[i] -= iu * c.du[i] * c.gradP[i];
+  for (long i = 0; i < 3L * c.nn; ++i) c.U[i] -= iu * dc[i] * c.gradP[i];
   update_gradient<3>(c, c.U, c.gradU, c.s.u_shifted);
   if (c.s.hr) update_blending_u(c);  // segregatedFlowEquations.cpp:287-288
 }
@@ -1092,6 +1112,7 @@ void* orc_case_create(int nn, int ne, const double* x, const int* conn, int nf, 
   c->mu.assign(nn, s->mu);
   c->sideU.assign(3L * nn, 0.0);
   c->wallNode.assign(nn, 0.0);
+  c->duT.assign(3L * nn, 0.0);
   c->betaU.assign(3L * nn, 0.0);  // setupBlendingFactorField: zero (nodeField.hpp:733-745)
   c->minU.assign(3L * nn, 0.0);
   c->maxU.assign(3L * nn, 0.0);
@@ -1155,6 +1176,7 @@ double* orc_case_field(void* h, const char* name, long* len) {
   else if (n == "wallNode") v = &c->wallNode;
   else if (n == "x") v = &c->x;
   else if (n == "betaU") v = &c->betaU;
+  else if (n == "duTilde") v = &c->duT;
   else if (n == "minU") v = &c->minU;
   else if (n == "maxU") v = &c->maxU;
   if (!v) {

@@ -41,6 +41,7 @@ typedef struct orc_settings {
   double pc_rtol;
   int hr;              /* advection scheme: 0 upwind, 1 high resolution (Barth-Jespersen blended deferred correction) */
   double beta_max;     /* upper limit of the blending factor (nodeField.h:150) */
+  int du_mode;         /* pressure-velocity coupling: 0 SIMPLE, 1 SIMPLEC (consistent_), 2 fractional step */
 } orc_settings;
 
 typedef struct orc_iter_stats {

@@ -38,6 +38,7 @@ class Settings(C.Structure):
         ("pc_rtol", C.c_double),
         ("hr", C.c_int),
         ("beta_max", C.c_double),
+        ("du_mode", C.c_int),
     ]
 
 
@@ -57,7 +58,7 @@ def default_settings(**kw) -> Settings:
     linear_linear velocity interpolation and the controls.h defaults."""
     d = dict(rho=1.0, mu=0.01, urf_u=0.9, urf_p=0.1, dt=1.0, grad_urf=0.5625, mdot_urf=1.0,
              wall_rhs_relax=0.75, u_shifted=1, u_grad_shifted=1, p_shifted=1, p_grad_shifted=1,
-             ref_node=0, mom_maxit=200, mom_rtol=1e-12, pc_maxit=5000, pc_rtol=1e-12, hr=0, beta_max=1.0)
+             ref_node=0, mom_maxit=200, mom_rtol=1e-12, pc_maxit=5000, pc_rtol=1e-12, hr=0, beta_max=1.0, du_mode=0)
     d.update(kw)
     return Settings(**d)
 

@@ -148,6 +148,7 @@ static int gpu_checks(const std::string& dir) {
   s.use_graphs = 0;
   s.hr = 0;
   s.beta_max = 1.0;
+  s.du_mode = 0;
   oa_flow* flow = nullptr;
   openaccel_b200::check(oa_flow_create(mesh, &s, bnd.data(), nb, &flow));
   openaccel_b200::check(oa_flow_initialize(flow));
