@@ -184,6 +184,19 @@ int oa_update_gradient(oa_flow* f, int which);
  * iters counts Krylov iterations of the method in use (GCR(2): one
  * preconditioner application each; BiCGStab: two). */
 int oa_solve(oa_flow* f, int sys, double rtol, int maxit, double* x, int* iters, double* res);
+/* Transient runs: start a time step of size dt (simulation::runTransient's
+ * preWork and time advance, src/simulation/simulation.cpp:222-312): the
+ * velocity moves to the old time level (old to old-old), and the following
+ * oa_simple_iterate calls (the step's coefficient iterations) assemble the
+ * BDF1 or BDF2 momentum node terms
+ * (src/assemble/flow/segregatedFlow/navierStokesAssembler/navierStokesAssemblerNodeTerms.cpp:151-427)
+ * and the transient part of the mass divergence (src/model/flow/flowModel.cpp:13556-13700)
+ * instead of the steady false transient; BDF2 uses variable-step
+ * coefficients (src/basic/types.cpp:398-410) and BDF1 on its first step.
+ * The density is constant in time (incompressible). Fields "Uold",
+ * "Uoldold" become readable. */
+enum { OA_TIME_BDF1 = 1, OA_TIME_BDF2 = 2 };
+int oa_flow_advance_time(oa_flow* f, int scheme, double dt);
 /* ControlData of the last solve of system sys (0 momentum, 1 pressure
  * correction) made by oa_solve or oa_simple_iterate: Context::getControlData()
  * as linearSystem::convergenceReport_ reads it (src/equation/linearSystem.h:473-488).

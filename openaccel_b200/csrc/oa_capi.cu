@@ -111,6 +111,8 @@ double* field_ptr(Flow& f, const std::string& n, size_t* len) {
   if (f.minU && n == "minU") { *len = 3 * nn; return f.minU; }
   if (f.maxU && n == "maxU") { *len = 3 * nn; return f.maxU; }
   if (f.duT && n == "duTilde") { *len = 3 * nn; return f.duT; }
+  if (f.Uold && n == "Uold") { *len = 3 * nn; return f.Uold; }
+  if (f.Uoldold && n == "Uoldold") { *len = 3 * nn; return f.Uoldold; }
   *len = 0;
   return nullptr;
 }
@@ -496,7 +498,7 @@ void oa_flow_destroy(oa_flow* H) {
   void* ptrs[] = {f.U,       f.p,       f.gradU,   f.gradP,   f.du,      f.div,    f.mDot,  f.pc_flux,
                   f.pc_coef, f.xloc32,  f.umu32,   f.rho,     f.mu,      f.sideU,  f.b.A_mom, f.b.b_mom,
                   f.b.A_pc,  f.b.b_pc,  f.b.x_mom, f.b.x_pc,  f.err_dev, H->scal,  f.red,   f.ref_flag,
-                  f.betaU,   f.minU,    f.maxU,    f.duT};
+                  f.betaU,   f.minU,    f.maxU,    f.duT,     f.Uold,    f.Uoldold};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (H->hscal) cudaFreeHost(H->hscal);
@@ -695,6 +697,41 @@ int oa_simple_iterate(oa_flow* H, int n, oa_iter_stats* stats) {
     for (auto& e : ev)
       if (e) cudaEventDestroy(e);
   return s;
+}
+
+int oa_flow_advance_time(oa_flow* H, int scheme, double dt) {
+  if (!H || (scheme != OA_TIME_BDF1 && scheme != OA_TIME_BDF2) || !(dt > 0))
+    return fail(OA_ERR_ARG, "oa_flow_advance_time: scheme must be OA_TIME_BDF1 or OA_TIME_BDF2 and dt > 0");
+  Flow& f = H->f;
+  const size_t n3 = 3 * (size_t)f.mesh->nn;
+  if (!f.Uold) {
+    if (int s = dalloc(&f.Uold, n3)) return s;
+    if (int s = dalloc(&f.Uoldold, n3)) return s;
+    OA_CUDA(cudaMemsetAsync(f.Uold, 0, sizeof(double) * n3, f.stream));
+  }
+  // time levels: old -> old-old, current -> old (the reference's preWork)
+  OA_CUDA(cudaMemcpyAsync(f.Uoldold, f.Uold, sizeof(double) * n3, cudaMemcpyDeviceToDevice, f.stream));
+  OA_CUDA(cudaMemcpyAsync(f.Uold, f.U, sizeof(double) * n3, cudaMemcpyDeviceToDevice, f.stream));
+  f.dt_prev = f.time_steps ? f.dt_step : dt;
+  f.dt_step = dt;
+  f.time_scheme = scheme;
+  ++f.time_steps;
+  // BDF1 {1, -1} (src/basic/types.cpp:392-396); BDF2 with w = dt / dt_prev
+  // (:398-410), BDF1 on the first step
+  if (scheme == OA_TIME_BDF2 && f.time_steps >= 2) {
+    const double w = f.dt_step / f.dt_prev;
+    f.tk[0] = (1.0 + 2.0 * w) / (1.0 + w);
+    f.tk[1] = -(1.0 + w);
+    f.tk[2] = w * w / (1.0 + w);
+    f.time_order = 2;
+  } else {
+    f.tk[0] = 1.0;
+    f.tk[1] = -1.0;
+    f.tk[2] = 0.0;
+    f.time_order = 1;
+  }
+  OA_CUDA(cudaStreamSynchronize(f.stream));
+  return OA_OK;
 }
 
 int oa_flow_last_control(oa_flow* H, int sys, oa_control_data* out) {

@@ -72,6 +72,13 @@ struct Flow {
   double *betaU = nullptr, *minU = nullptr, *maxU = nullptr;
   // SIMPLEC (settings.du_mode == 1): the consistent coefficient D~ [nn][3]
   double* duT = nullptr;
+  // transient runs (oa_flow_advance_time): scheme (0 steady, 1 BDF1, 2 BDF2),
+  // time steps taken, the order and coefficients of the current step, its
+  // size and the previous one, velocity at the two previous time levels
+  int time_scheme = 0, time_steps = 0, time_order = 0;
+  double tk[3] = {0.0, 0.0, 0.0};
+  double dt_step = 0.0, dt_prev = 0.0;
+  double *Uold = nullptr, *Uoldold = nullptr;
   // [ne][12] Rhie-Chow mass flux of each SCS ip with the pressure-correction
   // equation's upwind density (its right-hand side), written by the mass-flow
   // kernel and summed per row by the pressure-correction kernel

@@ -280,6 +280,11 @@ struct MomArgs {
   double* duT;   // SIMPLEC: D~ [nn][3]
   double dt, urf_inv, wall_relax;
   int du_mode;   // 0 SIMPLE, 1 SIMPLEC, 2 fractional step
+  // transient runs: BDF order (0 steady: dt is the false-transient physical
+  // timescale; 1, 2: dt is the time step), coefficients, old velocity levels
+  int order;
+  double tk0, tk1, tk2;
+  const double *Uold, *Uoldold;
   int* err;
 };
 
@@ -561,18 +566,30 @@ __global__ void __launch_bounds__(BLOCK, sizeof(TF) == 4 ? (UGSH ? 4 : 3) : 1) k
     const double dv = __ldg(a.div + row);
     const double rho = __ldg(a.rho + row);
     const double lf = rho * vol / a.dt;
-    double un[3], gp[3];
+    double un[3], gp[3], uo[3] = {0.0, 0.0, 0.0}, uoo[3] = {0.0, 0.0, 0.0};
     load3(a.U, row, un);
     load3(a.gradP, row, gp);
+    if (a.order >= 1) load3(a.Uold, row, uo);
+    if (a.order == 2) load3(a.Uoldold, row, uoo);
     const bool wall = __ldg(a.m.wall_node + row) != 0;
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
       double d = double(diag[4 * k]);
-      if (dv < 0) d += -dv;
-      d += lf;
+      double r = double(rhs[k]);
+      if (a.order == 0) {
+        // steady: false transient with the physical timescale
+        if (dv < 0) d += -dv;
+        d += lf;
+      } else {
+        // BDF1 / BDF2 node terms (navierStokesAssemblerNodeTerms.cpp:151-427),
+        // density constant in time
+        const double f0 = a.tk0 * lf, f1 = a.tk1 * lf, f2 = a.tk2 * lf;
+        d += f0;
+        r -= a.order == 1 ? (f0 * un[k] + f1 * uo[k]) : (f0 * un[k] + f1 * uo[k] + f2 * uoo[k]);
+        if (dv < 0) d += -dv;
+      }
       d *= a.urf_inv;
       diag[4 * k] = TF(d);
-      double r = double(rhs[k]);
       r -= -dv * un[k];
       r -= gp[k] * vol;
       if (wall) r *= a.wall_relax;
@@ -584,7 +601,8 @@ __global__ void __launch_bounds__(BLOCK, sizeof(TF) == 4 ? (UGSH ? 4 : 3) : 1) k
       // D~ = V / (a_ii + off-diagonal sum + SMALL)
 #pragma unroll
       for (int k = 0; k < 3; ++k) {
-        a.du[3 * row + k] = a.du_mode == 2 ? a.dt / rho : vol / (double(diag[4 * k]) + SMALL);
+        a.du[3 * row + k] = a.du_mode == 2 ? (a.order ? a.dt / a.tk0 / rho : a.dt / rho)
+                                           : vol / (double(diag[4 * k]) + SMALL);
         if (a.du_mode == 1) a.duT[3 * row + k] = vol / (double(diag[4 * k]) + off[k] + SMALL);
         static_cast<TF*>(a.b)[3 * row + k] = rhs[k];
       }
@@ -823,6 +841,11 @@ struct DivArgs {
   MeshView m;
   const double* mDot;
   double* div;
+  // transient contribution (flowModel.cpp:13556-13700, fixed mesh, density
+  // constant in time): (tk0 + tk1 [+ tk2]) rho V / dt
+  const double* rho;
+  int order;
+  double tk0, tk1, tk2, dt;
 };
 
 __global__ void __launch_bounds__(BLOCK) k_div(DivArgs a) {
@@ -841,7 +864,13 @@ __global__ void __launch_bounds__(BLOCK) k_div(DivArgs a) {
     }
   }
   s = rowsum8(s);
-  if (rv && c == 0) a.div[row] = s;
+  if (rv && c == 0) {
+    if (a.order) {
+      const double rho = __ldg(a.rho + row), vol = __ldg(a.m.vol + row);
+      s += (a.order == 1 ? (a.tk0 * rho + a.tk1 * rho) : (a.tk0 * rho + a.tk1 * rho + a.tk2 * rho)) * vol / a.dt;
+    }
+    a.div[row] = s;
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -1137,7 +1166,8 @@ int launch_momentum(Flow& f, bool mixed) {
   }
   MomArgs a{f.mesh->view(), f.U,       f.gradP, f.div,  f.mDot,          f.rho,
             f.mu,           f.sideU,   f.betaU, f.gradU, f.xloc32, f.umu32, f.b.A_mom, f.b.b_mom,
-            f.du,           f.duT,     f.s.dt,  1.0 / f.s.urf_u, f.s.wall_rhs_relax, f.s.du_mode, f.err_dev};
+            f.du,           f.duT,     f.time_order ? f.dt_step : f.s.dt,  1.0 / f.s.urf_u, f.s.wall_rhs_relax,
+            f.s.du_mode,    f.time_order, f.tk[0], f.tk[1], f.tk[2], f.Uold, f.Uoldold, f.err_dev};
   const int g = grid_rows(f.mesh->nn);
   const bool us = f.s.u_shifted, gs = f.s.u_grad_shifted, hr = f.s.hr != 0;
 #define OA_MOM(US, GS, T)                                                                   \
@@ -1197,7 +1227,7 @@ int launch_init_mdot(Flow& f) { return launch_mdot_impl(f, 1); }
 int launch_update_mdot(Flow& f, bool stage) { return launch_mdot_impl(f, stage ? 3 : 0); }
 
 int launch_div(Flow& f) {
-  DivArgs a{f.mesh->view(), f.mDot, f.div};
+  DivArgs a{f.mesh->view(), f.mDot, f.div, f.rho, f.time_order, f.tk[0], f.tk[1], f.tk[2], f.dt_step};
   k_div<<<grid_rows(f.mesh->nn), BLOCK, 0, f.stream>>>(a);
   count_launches(1);
   OA_CUDA(cudaGetLastError());

@@ -31,7 +31,7 @@ EXPORTS = [
     "oa_diffusion_create", "oa_diffusion_destroy", "oa_diffusion_set_field", "oa_diffusion_get_field",
     "oa_diffusion_field_device_ptr", "oa_diffusion_assemble", "oa_diffusion_solve", "oa_diffusion_step",
     "oa_diffusion_stream", "oa_diffusion_time_assembly", "oa_sst_default_constants", "oa_sst_node_update",
-    "oa_flow_last_control", "oa_flow_scales",
+    "oa_flow_last_control", "oa_flow_scales", "oa_flow_advance_time",
 ]
 
 OA_BND_FIXED_VALUE = 0
@@ -165,6 +165,7 @@ def lib():
         "oa_simple_iterate": (C.c_int, [vp, C.c_int, P(IterStats)]),
         "oa_flow_last_control": (C.c_int, [vp, C.c_int, P(ControlData)]),
         "oa_flow_scales": (C.c_int, [vp, dp, dp, dp]),
+        "oa_flow_advance_time": (C.c_int, [vp, C.c_int, C.c_double]),
         "oa_flow_sync": (C.c_int, [vp]),
         "oa_flow_stream": (C.c_int, [vp, P(vp)]),
         "oa_launch_count": (C.c_int, [P(C.c_longlong)]),
@@ -257,7 +258,7 @@ class Flow:
     """Segregated laminar flow state on the device (oa_flow_create)."""
 
     FIELD_SHAPES = {"U": 3, "p": 1, "gradU": 9, "gradP": 3, "du": 3, "div": 1, "sideU": 3, "rho": 1, "mu": 1,
-                    "betaU": 3, "minU": 3, "maxU": 3, "duTilde": 3}
+                    "betaU": 3, "minU": 3, "maxU": 3, "duTilde": 3, "Uold": 3, "Uoldold": 3}
 
     def __init__(self, mesh: Mesh, settings: FlowSettings | None = None):
         self.mesh = mesh
@@ -329,6 +330,10 @@ class Flow:
                      mom_res=s.mom_res, pc_res=s.pc_res, continuity_rms=s.continuity_rms,
                      continuity_rms_raw=s.continuity_rms_raw, mom=s.mom.as_dict(), pc=s.pc.as_dict(),
                      **{k: getattr(s, k) for k in PHASES}) for s in st[:n]]
+
+    def advance_time(self, scheme, dt):
+        """Start a time step of size dt: scheme 1 BDF1, 2 BDF2."""
+        _check(lib().oa_flow_advance_time(self.h, int(scheme), float(dt)))
 
     def last_control(self, sys):
         """ControlData of the last solve of ``sys`` ("momentum"/0 or "pcorr"/1)."""

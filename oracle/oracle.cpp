@@ -65,6 +65,11 @@ struct Case {
   std::vector<double> betaU, minU, maxU;
   // SIMPLEC: the consistent coefficient D~ [nn][3] (flowModel duTilde)
   std::vector<double> duT;
+  // transient runs: scheme (0 steady, 1 BDF1, 2 BDF2), time steps taken, the
+  // current and previous step sizes, velocity at the two previous time levels
+  int timeScheme = 0, timeSteps = 0;
+  double dtStep = 0.0, dtPrev = 0.0;
+  std::vector<double> Uold, Uoldold;
   // element colours (no two elements of a colour share a node), for the
   // threaded CPU-baseline path
   std::vector<std::vector<int>> colors;
@@ -201,6 +206,24 @@ void gather_coords(const Case& c, int e, double* xe) {
     for (int k = 0; k < 3; ++k) xe[3 * a + k] = c.x[3 * c.conn[8 * e + a] + k];
 }
 
+// Time-integration coefficients of the current step: BDF1 {1, -1}
+// (src/basic/types.cpp:392-396), BDF2 {(1 + 2w)/(1 + w), -(1 + w), w^2/(1 + w)}
+// with w = dt / dt_prev (:398-410); BDF2 takes BDF1 on the first step, when no
+// second old level exists.
+int time_coeffs(const Case& c, double* k) {
+  if (c.timeScheme == 2 && c.timeSteps >= 2) {
+    const double w = c.dtStep / c.dtPrev;
+    k[0] = (1.0 + 2.0 * w) / (1.0 + w);
+    k[1] = -(1.0 + w);
+    k[2] = w * w / (1.0 + w);
+    return 2;
+  }
+  k[0] = 1.0;
+  k[1] = -1.0;
+  k[2] = 0.0;
+  return 1;
+}
+
 // mesh::updateDualNodalVolumeField_ (src/mesh/meshGeometry.cpp:1277-1345)
 void dual_volume(Case& c) {
   c.vol.assign(c.nn, 0.0);
@@ -307,6 +330,19 @@ void update_div(Case& c) {
       c.div[en[LR[ip][1]]] -= m;
     }
   });
+  // transient contribution (flowModel.cpp:13556-13700, fixed mesh): the
+  // density at every time level is the current one (constant density)
+  if (c.timeScheme) {
+    double k[3];
+    const int order = time_coeffs(c, k);
+    for (int i = 0; i < c.nn; ++i) {
+      const double rho = c.rho[i];
+      if (order == 1)
+        c.div[i] += (k[0] * rho + k[1] * rho) * c.vol[i] / c.dtStep;
+      else
+        c.div[i] += (k[0] * rho + k[1] * rho + k[2] * rho) * c.vol[i] / c.dtStep;
+    }
+  }
 }
 
 // nodeField::updateGradientField (src/field/nodeField/nodeField.hpp:3253-3445
@@ -517,15 +553,35 @@ void assemble_momentum(Case& c, double* A, double* b) {
   std::fill(A, A + 9L * nnz, 0.0);
   std::fill(b, b + 3L * c.nn, 0.0);
   // node terms, one applyCoeff_ per node
+  double tk[3];
+  const int order = c.timeScheme ? time_coeffs(c, tk) : 0;
   for (int i = 0; i < c.nn; ++i) {
     double lhs[9] = {0}, rhs[3] = {0};
     const double rho = c.rho[i], vol = c.vol[i], dv = c.div[i];
-    const double lf = rho * vol / c.s.dt;
-    for (int k = 0; k < 3; ++k) {
-      if (dv < 0) lhs[4 * k] += -dv;
-      rhs[k] -= -dv * c.U[3 * i + k];
-      rhs[k] -= c.gradP[3 * i + k] * vol;
-      lhs[4 * k] += lf;
+    if (order == 0) {
+      // steady: false transient with the physical timescale (...NodeTerms.cpp:16-149)
+      const double lf = rho * vol / c.s.dt;
+      for (int k = 0; k < 3; ++k) {
+        if (dv < 0) lhs[4 * k] += -dv;
+        rhs[k] -= -dv * c.U[3 * i + k];
+        rhs[k] -= c.gradP[3 * i + k] * vol;
+        lhs[4 * k] += lf;
+      }
+    } else {
+      // BDF1 / BDF2 (...NodeTerms.cpp:151-427); density constant in time
+      const double lhsfac = tk[0] * rho * vol / c.dtStep;
+      const double lhsfacOld = tk[1] * rho * vol / c.dtStep;
+      const double lhsfacOldOld = tk[2] * rho * vol / c.dtStep;
+      for (int k = 0; k < 3; ++k) {
+        lhs[4 * k] += lhsfac;
+        if (order == 1)
+          rhs[k] -= (lhsfac * c.U[3 * i + k] + lhsfacOld * c.Uold[3 * i + k]);
+        else
+          rhs[k] -= (lhsfac * c.U[3 * i + k] + lhsfacOld * c.Uold[3 * i + k] + lhsfacOldOld * c.Uoldold[3 * i + k]);
+        if (dv < 0) lhs[4 * k] += -dv;
+        rhs[k] -= -dv * c.U[3 * i + k];
+        rhs[k] -= c.gradP[3 * i + k] * vol;
+      }
     }
     apply_coeff<3>(c, A, b, &i, 1, rhs, lhs);
   }
@@ -684,7 +740,8 @@ void assemble_momentum(Case& c, double* A, double* b) {
   for (int i = 0; i < c.nn; ++i) {
     const double* d = &A[9L * (c.rowPtr[i] + c.diagOff[i])];
     for (int k = 0; k < 3; ++k)
-      c.du[3 * i + k] = c.s.du_mode == 2 ? c.s.dt / c.rho[i] : c.vol[i] / (d[4 * k] + SMALL);
+      c.du[3 * i + k] = c.s.du_mode == 2 ? (order ? c.dtStep / tk[0] / c.rho[i] : c.s.dt / c.rho[i])
+                                          : c.vol[i] / (d[4 * k] + SMALL);
     if (c.s.du_mode == 1)
       for (int k = 0; k < 3; ++k) {
         double off = 0.0;
@@ -1242,6 +1299,20 @@ void orc_apply_coeff(void* h, int bs, double* A, double* b, const int* nodes, in
     apply_coeff<3>(c, A, b, nodes, n, rhs, lhs);
   else
     apply_coeff<1>(c, A, b, nodes, n, rhs, lhs);
+}
+
+void orc_advance_time(void* h, int scheme, double dt) {
+  Case& c = *static_cast<Case*>(h);
+  if (c.Uold.empty()) {
+    c.Uold.assign(3L * c.nn, 0.0);
+    c.Uoldold.assign(3L * c.nn, 0.0);
+  }
+  c.Uoldold = c.Uold;
+  c.Uold = c.U;
+  c.dtPrev = c.timeSteps ? c.dtStep : dt;
+  c.dtStep = dt;
+  c.timeScheme = scheme == 2 ? 2 : 1;
+  ++c.timeSteps;
 }
 
 void orc_set_solver(void* h, int kind) { static_cast<Case*>(h)->solverKind = (kind == 1 || kind == 2) ? kind : 0; }

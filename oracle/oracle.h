@@ -100,6 +100,10 @@ void orc_apply_coeff(void* h, int bs, double* A, double* b, const int* nodes, in
                      const double* lhs);
 /* one SIMPLE outer iteration (segregatedFlowEquations::solve) */
 void orc_simple_iteration(void* h, orc_iter_stats* st);
+/* start a time step (simulation::runTransient preWork): the velocity moves to
+ * the old level (old to old-old), the step is dt, scheme 1 = BDF1, 2 = BDF2
+ * (BDF1 on the first step); later iterations use the transient node terms */
+void orc_advance_time(void* h, int scheme, double dt);
 /* linear solvers of orc_simple_iteration: 0 = Jacobi-preconditioned BiCGStab
  * (default, the parity reference), 1 = the reference cavity example's
  * configuration (examples/cavity/input.i:61-77): momentum FGMRES(30) and

@@ -127,6 +127,8 @@ def lib():
         L.orc_apply_coeff.restype = None
         L.orc_apply_coeff.argtypes = [C.c_void_p, C.c_int, P(C.c_double), P(C.c_double), P(C.c_int), C.c_int,
                                       P(C.c_double), P(C.c_double)]
+        L.orc_advance_time.restype = None
+        L.orc_advance_time.argtypes = [C.c_void_p, C.c_int, C.c_double]
         L.orc_set_solver.restype = None
         L.orc_set_solver.argtypes = [C.c_void_p, C.c_int]
         L.orc_gmres_ilu.restype = C.c_int
@@ -286,6 +288,10 @@ class FlowCase:
         nodes = np.ascontiguousarray(nodes, np.int32)
         lib().orc_apply_coeff(self.h, bs, _dp(A), _dp(b), nodes.ctypes.data_as(C.POINTER(C.c_int)), int(nodes.size),
                               _dp(np.ascontiguousarray(rhs, np.float64)), _dp(np.ascontiguousarray(lhs, np.float64)))
+
+    def advance_time(self, scheme, dt):
+        """Start a time step: scheme 1 BDF1, 2 BDF2."""
+        lib().orc_advance_time(self.h, scheme, dt)
 
     def set_solver(self, kind):
         """0: Jacobi-BiCGStab (parity reference); 1 or "reference": the cavity
