@@ -117,7 +117,14 @@ const char* oa_version(void);
  * updateExposedAreaVectorField_ (src/mesh/meshGeometry.cpp:1277-1527) and the
  * reduced-stencil CSR graph of nodeGraph::buildGraph_
  * (src/mesh/graph/nodeGraph.cpp:29-469). coords[nn][3], conn[ne][8] (Nalu hex8
- * ordering), boundary faces as (element, face ordinal, boundary index). */
+ * ordering), boundary faces as (element, face ordinal, boundary index).
+ * hex8: elements whose corner numbering starts at another corner or axis than
+ * their neighbours' are relabelled by a proper cube rotation (the geometry and
+ * Jacobian sign do not change) so that the mesh is a consistently oriented
+ * block; a hex mesh that admits no such labelling (not block-structured, e.g.
+ * three or five elements around an interior edge) is rejected with
+ * OA_ERR_MESH. Element fields ("mDot") are exchanged in the caller's
+ * labelling. */
 int oa_mesh_create(const double* coords, int nn, const int* conn, int ne, int topo,
                    const int* face_elem, const int* face_ord, const int* face_bnd, int nf,
                    oa_mesh** out);
@@ -143,7 +150,8 @@ void oa_flow_destroy(oa_flow* f);
  * n is the number of doubles. */
 int oa_flow_set_field(oa_flow* f, const char* name, const double* host, long n);
 int oa_flow_get_field(oa_flow* f, const char* name, double* host, long n);
-/* Device pointer of a named field (for callers that keep data resident). */
+/* Device pointer of a named field (for callers that keep data resident;
+ * "mDot" of a relabelled mesh is stored in the relabelled ip order). */
 int oa_flow_field_device_ptr(oa_flow* f, const char* name, double** dev);
 /* Pressure-level rows: replaces settings.ref_node with a list, one row per
  * closed domain of a batched (disjoint-union) mesh. Mirrors

@@ -19,7 +19,7 @@ LIB = os.path.join(LIBDIR, "libopenaccel_b200.so")
 SOURCES = ["oa_kernels.cu", "oa_krylov.cu", "oa_amg.cu", "oa_capi.cu", "oa_static_solve.cu", "oa_scalar_solve.cu",
            "oa_diffusion.cu", "oa_sst.cu"]
 HEADERS = ["oa_geom.cuh", "oa_hex8.cuh", "oa_tet4.cuh", "oa_rowlane.cuh", "oa_internal.h", "oa_krylov.h", "oa_amg.h",
-           "oa_amg_symbolic.h", "oa_tet4_lists.h",
+           "oa_amg_symbolic.h", "oa_tet4_lists.h", "oa_hex_orient.h",
            "oa_scalar_solve.h"]
 
 NVCC = os.environ.get("NVCC", "nvcc")

@@ -13,6 +13,7 @@
 
 #include <nvtx3/nvToolsExt.h>
 
+#include "oa_hex_orient.h"
 #include "oa_internal.h"
 #include "oa_krylov.h"
 #include "oa_scalar_solve.h"
@@ -244,8 +245,33 @@ int oa_mesh_create(const double* coords, int nn, const int* conn, int ne, int to
   static const int LRt[12][2] = {{0, 1}, {1, 2}, {2, 3}, {0, 3}, {4, 5}, {5, 6},
                                  {6, 7}, {4, 7}, {0, 4}, {1, 5}, {2, 6}, {3, 7}};
   static const int FN[6][4] = {{0, 1, 5, 4}, {1, 2, 6, 5}, {2, 3, 7, 6}, {0, 4, 7, 3}, {0, 3, 2, 1}, {4, 5, 6, 7}};
+  // relabel elements whose corner numbering starts elsewhere (one of the 24
+  // proper cube rotations each) so the mesh is a consistently oriented block;
+  // boundary-face ordinals follow their element
+  std::vector<int> oconn;
+  std::vector<uint8_t> rot;
+  std::vector<int> oface(face_ord, face_ord + nf);
+  bool consistent = true;
+  {
+    std::vector<uint8_t> seen(8L * nn, 0);
+    for (long k = 0; k < 8L * ne && consistent; ++k) {
+      uint8_t& v = seen[8L * conn[k] + (k & 7)];
+      if (v) consistent = false;
+      v = 1;
+    }
+  }
+  if (!consistent) {  // only meshes that need it pay for the face walk
+    std::string why;
+    if (!hexorient::orient(nn, ne, conn, oconn, rot, &why))
+      return fail(OA_ERR_MESH, "oa_mesh_create: the hex mesh is not a block-structured mesh the row kernels accept (" +
+                                   why + ")");
+    for (int f = 0; f < nf; ++f) oface[f] = hexorient::face_map(rot[face_elem[f]], face_ord[f]);
+    conn = oconn.data();
+    face_ord = oface.data();
+  }
   oa_mesh* M = new oa_mesh();
   DeviceMesh& m = M->m;
+  if (std::any_of(rot.begin(), rot.end(), [](uint8_t r) { return r != 0; })) m.h_rot.swap(rot);
   m.nn = nn;
   m.ne = ne;
   m.nf = nf;
@@ -509,12 +535,38 @@ void oa_flow_destroy(oa_flow* H) {
   delete H;
 }
 
+// Mass flows of relabelled elements: the device keeps them in the element's
+// new ip order; the caller sees its own (ip q of the new labelling is old ip
+// o, with the sign of the L -> R direction).
+static void mdot_to_device_order(const DeviceMesh& m, const double* in, double* out) {
+  for (int e = 0; e < m.ne; ++e)
+    for (int q = 0; q < 12; ++q) {
+      int o = q, sg = 1;
+      if (m.h_rot[e]) hexorient::ip_map(m.h_rot[e], q, &o, &sg);
+      out[12L * e + q] = sg * in[12L * e + o];
+    }
+}
+static void mdot_to_caller_order(const DeviceMesh& m, const double* in, double* out) {
+  for (int e = 0; e < m.ne; ++e)
+    for (int q = 0; q < 12; ++q) {
+      int o = q, sg = 1;
+      if (m.h_rot[e]) hexorient::ip_map(m.h_rot[e], q, &o, &sg);
+      out[12L * e + o] = sg * in[12L * e + q];
+    }
+}
+
 int oa_flow_set_field(oa_flow* H, const char* name, const double* host, long n) {
   if (!H || !name || !host) return fail(OA_ERR_ARG, "oa_flow_set_field: null argument");
   size_t len = 0;
   double* d = field_ptr(H->f, name, &len);
   if (!d) return fail(OA_ERR_ARG, std::string("oa_flow_set_field: unknown field ") + name);
   if ((size_t)n != len) return fail(OA_ERR_ARG, std::string("oa_flow_set_field: size mismatch for ") + name);
+  std::vector<double> tmp;
+  if (!H->f.mesh->h_rot.empty() && std::string(name) == "mDot") {
+    tmp.resize(len);
+    mdot_to_device_order(*H->f.mesh, host, tmp.data());
+    host = tmp.data();
+  }
   OA_CUDA(cudaMemcpyAsync(d, host, sizeof(double) * len, cudaMemcpyHostToDevice, H->f.stream));
   OA_CUDA(cudaStreamSynchronize(H->f.stream));
   return OA_OK;
@@ -528,6 +580,10 @@ int oa_flow_get_field(oa_flow* H, const char* name, double* host, long n) {
   if ((size_t)n != len) return fail(OA_ERR_ARG, std::string("oa_flow_get_field: size mismatch for ") + name);
   OA_CUDA(cudaMemcpyAsync(host, d, sizeof(double) * len, cudaMemcpyDeviceToHost, H->f.stream));
   OA_CUDA(cudaStreamSynchronize(H->f.stream));
+  if (!H->f.mesh->h_rot.empty() && std::string(name) == "mDot") {
+    std::vector<double> tmp(host, host + len);
+    mdot_to_caller_order(*H->f.mesh, tmp.data(), host);
+  }
   return OA_OK;
 }
 

@@ -44,6 +44,9 @@ struct DeviceMesh : MeshView {
   // mean element edge length (every element's 12 edges, summed in element
   // order on the host): the h of the continuity-residual scale rho U_ref h^2
   double h_mean = 0.0;
+  // hex8 elements relabelled into a consistently oriented block: the cube
+  // rotation applied to each (empty when none was needed)
+  std::vector<uint8_t> h_rot;
   // host copies needed for set-up and parity dumps
   std::vector<int> h_row_ptr, h_cols, h_diag;
   std::vector<int> h_conn, h_face_elem, h_face_ord, h_face_bnd;
