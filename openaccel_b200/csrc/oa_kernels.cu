@@ -280,6 +280,7 @@ struct MomArgs {
   double* duT;   // SIMPLEC: D~ [nn][3]
   double dt, urf_inv, wall_relax;
   int du_mode;   // 0 SIMPLE, 1 SIMPLEC, 2 fractional step
+  int hr;        // high-resolution deferred correction
   // transient runs: BDF order (0 steady: dt is the false-transient physical
   // timescale; 1, 2: dt is the time step), coefficients, old velocity levels
   int order;
@@ -369,7 +370,11 @@ __device__ __forceinline__ void wall_face(const MomArgs& a, const TF (&x)[8][3],
   });
 }
 
-template <bool USH, bool UGSH, class TF, bool HR = false>
+// EXT: the variant with the optional terms (high-resolution deferred
+// correction, transient node terms, SIMPLEC / fractional-step coefficients),
+// each switched at run time; without it the kernel is the steady upwind SIMPLE
+// assembly with nothing else in its register budget.
+template <bool USH, bool UGSH, class TF, bool EXT = false>
 __global__ void __launch_bounds__(BLOCK, sizeof(TF) == 4 ? (UGSH ? 4 : 3) : 1) k_momentum(MomArgs a) {
   __shared__ TF sh_val[BLOCK * 3 * 9];
   __shared__ int sh_col[BLOCK * 3];
@@ -456,7 +461,7 @@ __global__ void __launch_bounds__(BLOCK, sizeof(TF) == 4 ? (UGSH ? 4 : 3) : 1) k
       // u_i,up on the rhs (navierStokesAssemblerElemTerms.cpp:287-330), x_ip
       // from the standard trilinear coordinate shape functions
       TF dcorr[3] = {TF(0), TF(0), TF(0)};
-      if constexpr (HR) {
+      if (EXT && a.hr) {
         using PC = ScsPt<IP, false>;
         TF dx[3];
         const int ku = tmd > 0 ? 0 : R;
@@ -557,7 +562,7 @@ __global__ void __launch_bounds__(BLOCK, sizeof(TF) == 4 ? (UGSH ? 4 : 3) : 1) k
   // SIMPLEC: sum of the row's off-diagonal (i, i) coefficients (the CSR
   // off-diagonal entries are the lanes' neighbour blocks summed)
   double off[3] = {0.0, 0.0, 0.0};
-  if (a.du_mode == 1)
+  if (EXT && a.du_mode == 1)
 #pragma unroll
     for (int k = 0; k < 3; ++k) off[k] = double(rowsum8(TF(nb[0][4 * k] + nb[1][4 * k] + nb[2][4 * k])));
   if (rv) {
@@ -569,14 +574,15 @@ __global__ void __launch_bounds__(BLOCK, sizeof(TF) == 4 ? (UGSH ? 4 : 3) : 1) k
     double un[3], gp[3], uo[3] = {0.0, 0.0, 0.0}, uoo[3] = {0.0, 0.0, 0.0};
     load3(a.U, row, un);
     load3(a.gradP, row, gp);
-    if (a.order >= 1) load3(a.Uold, row, uo);
-    if (a.order == 2) load3(a.Uoldold, row, uoo);
+    const int order = EXT ? a.order : 0;
+    if (order >= 1) load3(a.Uold, row, uo);
+    if (order == 2) load3(a.Uoldold, row, uoo);
     const bool wall = __ldg(a.m.wall_node + row) != 0;
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
       double d = double(diag[4 * k]);
       double r = double(rhs[k]);
-      if (a.order == 0) {
+      if (order == 0) {
         // steady: false transient with the physical timescale
         if (dv < 0) d += -dv;
         d += lf;
@@ -585,7 +591,7 @@ __global__ void __launch_bounds__(BLOCK, sizeof(TF) == 4 ? (UGSH ? 4 : 3) : 1) k
         // density constant in time
         const double f0 = a.tk0 * lf, f1 = a.tk1 * lf, f2 = a.tk2 * lf;
         d += f0;
-        r -= a.order == 1 ? (f0 * un[k] + f1 * uo[k]) : (f0 * un[k] + f1 * uo[k] + f2 * uoo[k]);
+        r -= order == 1 ? (f0 * un[k] + f1 * uo[k]) : (f0 * un[k] + f1 * uo[k] + f2 * uoo[k]);
         if (dv < 0) d += -dv;
       }
       d *= a.urf_inv;
@@ -601,9 +607,10 @@ __global__ void __launch_bounds__(BLOCK, sizeof(TF) == 4 ? (UGSH ? 4 : 3) : 1) k
       // D~ = V / (a_ii + off-diagonal sum + SMALL)
 #pragma unroll
       for (int k = 0; k < 3; ++k) {
-        a.du[3 * row + k] = a.du_mode == 2 ? (a.order ? a.dt / a.tk0 / rho : a.dt / rho)
-                                           : vol / (double(diag[4 * k]) + SMALL);
-        if (a.du_mode == 1) a.duT[3 * row + k] = vol / (double(diag[4 * k]) + off[k] + SMALL);
+        const int du_mode = EXT ? a.du_mode : 0;
+        a.du[3 * row + k] = du_mode == 2 ? (order ? a.dt / a.tk0 / rho : a.dt / rho)
+                                         : vol / (double(diag[4 * k]) + SMALL);
+        if (du_mode == 1) a.duT[3 * row + k] = vol / (double(diag[4 * k]) + off[k] + SMALL);
         static_cast<TF*>(a.b)[3 * row + k] = rhs[k];
       }
     }
@@ -1167,9 +1174,10 @@ int launch_momentum(Flow& f, bool mixed) {
   MomArgs a{f.mesh->view(), f.U,       f.gradP, f.div,  f.mDot,          f.rho,
             f.mu,           f.sideU,   f.betaU, f.gradU, f.xloc32, f.umu32, f.b.A_mom, f.b.b_mom,
             f.du,           f.duT,     f.time_order ? f.dt_step : f.s.dt,  1.0 / f.s.urf_u, f.s.wall_rhs_relax,
-            f.s.du_mode,    f.time_order, f.tk[0], f.tk[1], f.tk[2], f.Uold, f.Uoldold, f.err_dev};
+            f.s.du_mode,    f.s.hr,    f.time_order, f.tk[0], f.tk[1], f.tk[2], f.Uold, f.Uoldold, f.err_dev};
   const int g = grid_rows(f.mesh->nn);
-  const bool us = f.s.u_shifted, gs = f.s.u_grad_shifted, hr = f.s.hr != 0;
+  const bool us = f.s.u_shifted, gs = f.s.u_grad_shifted;
+  const bool hr = f.s.hr != 0 || f.time_order != 0 || f.s.du_mode != 0;  // the EXT variant
 #define OA_MOM(US, GS, T)                                                                   \
   if (us == US && gs == GS) {                                                               \
     if (hr)                                                                                 \
