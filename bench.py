@@ -129,7 +129,12 @@ def run_ours(args, rank, world):
                                             mom_maxit=args.mom_maxit, use_graphs=0 if args.no_graphs else 1))
         f.set_field("U", U0)
         f.initialize()
+        if not args.no_autotune:
+            # set-up, not timed: the flow's state is restored afterwards
+            tuning[prec] = f.autotune(iters=2)
         return f
+
+    tuning = {}
 
     def timed(f, steps, warmup):
         stream = torch.cuda.ExternalStream(f.stream_handle(), device=dev)
@@ -204,7 +209,7 @@ def run_ours(args, rank, world):
     ms_e2e = e0.elapsed_time(e1)
     ms_e2e = max_over_ranks(ms_e2e, dev, world)
 
-    conv = converge(args, gm, U0, dev, world) if args.converge_iters > 0 else None
+    conv = converge(args, gm, U0, dev, world, tuning) if args.converge_iters > 0 else None
 
     peak, peak_kind = measured_peaks()
     alg = algorithmic_bytes_momentum(m.nn, m.ne, gm.nnz, True)
@@ -227,6 +232,7 @@ def run_ours(args, rank, world):
         "config": cavity_config(args, args.n, m.ne, m.nn, gm.nnz, world),
         "fp64_outer_iters_per_s": value64,
         "graphs": "Krylov chunks replayed as CUDA graphs in both forms" if not args.no_graphs else "off",
+        "autotune": {("mixed" if k == rt.OA_PREC_MIXED else "fp64"): v for k, v in tuning.items()} or "off",
         "mixed_over_fp64": value / value64,
         "assembled_elems_per_s": {"mixed": 2 * m.ne / ((t_mom + t_pc) * 1e-3),
                                   "fp64": 2 * m.ne / ((t_mom64 + t_pc64) * 1e-3)},
@@ -251,7 +257,7 @@ def run_ours(args, rank, world):
     return res
 
 
-def converge(args, gm, U0, dev, world):
+def converge(args, gm, U0, dev, world, tuning=None):
     """Both forms from the same initial state for up to --converge-iters SIMPLE
     outer iterations (or until the continuity residual, RMS of the nodal mass
     imbalance / (rho U_lid h^2), falls to --converge-target). Device time of
@@ -271,6 +277,8 @@ def converge(args, gm, U0, dev, world):
                                             mom_maxit=args.mom_maxit, use_graphs=0 if args.no_graphs else 1))
         f.set_field("U", U0)
         f.initialize()
+        if tuning and prec in tuning:  # the timed legs' tuning
+            f.set_tuning(**tuning[prec])
         stream = torch.cuda.ExternalStream(f.stream_handle(), device=dev)
         # iteration 1 builds the pressure solve's AMG hierarchy on the host
         # (about 1.8 s at 128^3, the same in both forms): run it untimed
@@ -623,6 +631,7 @@ def main():
     ap.add_argument("--mom-maxit", type=int, default=20)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-graphs", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true", help="skip the launch-shape / solve-schedule autotuning")
     ap.add_argument("--only-mixed", action="store_true", help="time the mixed form only (profiling)")
     ap.add_argument("--workload", default="cavity", choices=["cavity", "conduction", "batch", "sst"],
                     help="cavity: the headline SIMPLE workload; conduction: the tet4 diffusion case (--n 96); "

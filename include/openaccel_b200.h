@@ -205,6 +205,25 @@ int oa_solve(oa_flow* f, int sys, double rtol, int maxit, double* x, int* iters,
  * "Uoldold" become readable. */
 enum { OA_TIME_BDF1 = 1, OA_TIME_BDF2 = 2 };
 int oa_flow_advance_time(oa_flow* f, int scheme, double dt);
+/* Autotuning of the flow's launch shapes and pressure-solve schedule (no
+ * counterpart in the reference, which has no device). Coordinate descent over
+ * the threads per block of the row kernels without shared memory (gradients,
+ * divergence, blending factor), of the element-owner mass-flow kernel and of
+ * the assembly row kernels (each 32, 64 or 128), the GCR(2) iterations per
+ * device-resident chunk (2 or 4) and the AMG numeric refresh interval (4, 8 or
+ * 16 solves), each candidate timed over `iters` SIMPLE outer iterations (CUDA
+ * events on the flow's stream, after one untimed iteration) from the same
+ * saved state; the flow's fields are restored afterwards and the next
+ * pressure solve rebuilds the AMG numeric phase. Block sizes do not change
+ * results; the solve schedule changes iterates within the solve tolerance. */
+typedef struct oa_tuning {
+  int block_rows, block_elements, block_assembly;  /* threads per block */
+  int gcr_chunk, amg_refresh;
+  double ms_per_iteration_before, ms_per_iteration_after;
+} oa_tuning;
+int oa_flow_autotune(oa_flow* f, int iters, oa_tuning* out);
+/* Apply a tuning found earlier (ms fields ignored). */
+int oa_flow_set_tuning(oa_flow* f, const oa_tuning* t);
 /* ControlData of the last solve of system sys (0 momentum, 1 pressure
  * correction) made by oa_solve or oa_simple_iterate: Context::getControlData()
  * as linearSystem::convergenceReport_ reads it (src/equation/linearSystem.h:473-488).

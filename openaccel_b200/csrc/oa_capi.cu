@@ -755,6 +755,111 @@ int oa_simple_iterate(oa_flow* H, int n, oa_iter_stats* stats) {
   return s;
 }
 
+int oa_flow_set_tuning(oa_flow* H, const oa_tuning* t) {
+  if (!H || !t) return fail(OA_ERR_ARG, "oa_flow_set_tuning: null argument");
+  auto ok_bs = [](int b) { return b == 32 || b == 64 || b == 128; };
+  if (!ok_bs(t->block_rows) || !ok_bs(t->block_elements) || !ok_bs(t->block_assembly) || t->gcr_chunk < 2 ||
+      t->gcr_chunk % 2 || t->amg_refresh < 1)
+    return fail(OA_ERR_ARG, "oa_flow_set_tuning: block sizes 32/64/128, even GCR chunk >= 2, AMG refresh >= 1");
+  Flow& f = H->f;
+  f.bs_rows = t->block_rows;
+  f.bs_elems = t->block_elements;
+  f.bs_asm = t->block_assembly;
+  H->pc.gcr_chunk = t->gcr_chunk;
+  H->pc.refresh = t->amg_refresh;
+  return OA_OK;
+}
+
+int oa_flow_autotune(oa_flow* H, int iters, oa_tuning* out) {
+  if (!H || iters < 1) return fail(OA_ERR_ARG, "oa_flow_autotune: bad arguments");
+  Flow& f = H->f;
+  const size_t nn = f.mesh->nn, ne = f.mesh->ne;
+  // the state the trials start from, restored after each and at the end
+  struct Saved {
+    double* dev;
+    double* copy;
+    size_t n;
+  };
+  std::vector<Saved> saved;
+  double* fields[] = {f.U, f.p, f.gradU, f.gradP, f.du, f.div, f.mDot, f.betaU, f.minU, f.maxU, f.duT};
+  const size_t sizes[] = {3 * nn, nn, 9 * nn, 3 * nn, 3 * nn, nn, 12 * ne, 3 * nn, 3 * nn, 3 * nn, 3 * nn};
+  int st = OA_OK;
+  for (int k = 0; k < 11 && !st; ++k) {
+    if (!fields[k]) continue;
+    Saved sv{fields[k], nullptr, sizes[k]};
+    if (cudaMalloc(&sv.copy, sizeof(double) * sv.n) != cudaSuccess) {
+      st = fail(OA_ERR_CUDA, "oa_flow_autotune: could not save the state");
+      break;
+    }
+    saved.push_back(sv);
+    if (cudaMemcpyAsync(sv.copy, sv.dev, sizeof(double) * sv.n, cudaMemcpyDeviceToDevice, f.stream) != cudaSuccess)
+      st = fail(OA_ERR_CUDA, "oa_flow_autotune: state copy failed");
+  }
+  auto restore = [&]() -> int {
+    for (auto& sv : saved)
+      OA_CUDA(cudaMemcpyAsync(sv.dev, sv.copy, sizeof(double) * sv.n, cudaMemcpyDeviceToDevice, f.stream));
+    return OA_OK;
+  };
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (!st && (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess))
+    st = fail(OA_ERR_CUDA, "oa_flow_autotune: event creation failed");
+  const long long solves0 = H->pc.solves;
+  // one trial: restore, one untimed iteration, `iters` timed ones
+  auto trial = [&](double* ms) -> int {
+    if (int s = restore()) return s;
+    H->pc.solves = 0;  // the first solve of a trial refreshes the AMG numeric phase
+    if (int s = oa_simple_iterate(H, 1, nullptr)) return s;
+    OA_CUDA(cudaEventRecord(e0, f.stream));
+    if (int s = oa_simple_iterate(H, iters, nullptr)) return s;
+    OA_CUDA(cudaEventRecord(e1, f.stream));
+    OA_CUDA(cudaEventSynchronize(e1));
+    float t = 0.f;
+    OA_CUDA(cudaEventElapsedTime(&t, e0, e1));
+    *ms = t / iters;
+    return OA_OK;
+  };
+  oa_tuning best{f.bs_rows, f.bs_elems, f.bs_asm, H->pc.gcr_chunk, H->pc.refresh, 0.0, 0.0};
+  double best_ms = 0.0;
+  if (!st) st = trial(&best_ms);
+  const double before = best_ms;
+  // coordinate descent, one knob at a time
+  const int bss[3] = {32, 64, 128};
+  const int chunks[2] = {2, 4};
+  const int refreshes[3] = {4, 8, 16};
+  for (int knob = 0; knob < 5 && !st; ++knob) {
+    const int* cand = knob < 3 ? bss : (knob == 3 ? chunks : refreshes);
+    const int nc = knob == 3 ? 2 : 3;
+    for (int c = 0; c < nc && !st; ++c) {
+      oa_tuning t = best;
+      int* slot = knob == 0 ? &t.block_rows
+                            : knob == 1 ? &t.block_elements
+                                        : knob == 2 ? &t.block_assembly : knob == 3 ? &t.gcr_chunk : &t.amg_refresh;
+      if (*slot == cand[c]) continue;
+      *slot = cand[c];
+      if ((st = oa_flow_set_tuning(H, &t))) break;
+      double ms = 0.0;
+      if ((st = trial(&ms))) break;
+      if (ms < best_ms) {
+        best_ms = ms;
+        best = t;
+      }
+    }
+    if (!st) st = oa_flow_set_tuning(H, &best);
+  }
+  if (!st) st = restore();
+  if (!st && cudaStreamSynchronize(f.stream) != cudaSuccess) st = fail(OA_ERR_CUDA, "oa_flow_autotune: sync failed");
+  H->pc.solves = 0;
+  (void)solves0;
+  for (auto& sv : saved) cudaFree(sv.copy);
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  if (st) return st;
+  best.ms_per_iteration_before = before;
+  best.ms_per_iteration_after = best_ms;
+  if (out) *out = best;
+  return OA_OK;
+}
+
 int oa_flow_advance_time(oa_flow* H, int scheme, double dt) {
   if (!H || (scheme != OA_TIME_BDF1 && scheme != OA_TIME_BDF2) || !(dt > 0))
     return fail(OA_ERR_ARG, "oa_flow_advance_time: scheme must be OA_TIME_BDF1 or OA_TIME_BDF2 and dt > 0");

@@ -82,6 +82,11 @@ struct Flow {
   double tk[3] = {0.0, 0.0, 0.0};
   double dt_step = 0.0, dt_prev = 0.0;
   double *Uold = nullptr, *Uoldold = nullptr;
+  // launch shapes chosen by oa_flow_autotune (threads per block; multiples
+  // of 32 up to the kernels' compiled 128): row kernels without shared
+  // memory (gradients, divergence, blending), the element-owner mass-flow
+  // kernel, the assembly row kernels (momentum, pressure correction)
+  int bs_rows = 128, bs_elems = 128, bs_asm = 128;
   // [ne][12] Rhie-Chow mass flux of each SCS ip with the pressure-correction
   // equation's upwind density (its right-hand side), written by the mass-flow
   // kernel and summed per row by the pressure-correction kernel

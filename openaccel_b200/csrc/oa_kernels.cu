@@ -1119,7 +1119,9 @@ __global__ void k_vel_correct(int n3, double* U, const double* du, const double*
 
 // ---------------------------------------------------------------------------
 // launchers
-static int grid_rows(int nn) { return (int)(((size_t)nn * 8 + BLOCK - 1) / BLOCK); }
+// grids: 8 lanes per row, bs threads per block (a multiple of 32, at most the
+// BLOCK the kernels are compiled for)
+static int grid_rows(int nn, int bs = BLOCK) { return (int)(((size_t)nn * 8 + bs - 1) / bs); }
 
 static int launch_mdot_impl(Flow& f, int mode);
 
@@ -1130,11 +1132,12 @@ int launch_pcorr(Flow& f, bool mixed, bool flux_fresh) {
   if (!flux_fresh)
     if (int s = launch_mdot_impl(f, 2)) return s;
   PcArgs a{f.mesh->view(), f.pc_coef, f.pc_flux, f.b.A_pc, f.b.b_pc, f.ref_flag};
-  const int g = grid_rows(f.mesh->nn);
+  const int bs = f.bs_asm;
+  const int g = grid_rows(f.mesh->nn, bs);
   if (mixed)
-    k_pcorr<float><<<g, BLOCK, 0, f.stream>>>(a);
+    k_pcorr<float><<<g, bs, 0, f.stream>>>(a);
   else
-    k_pcorr<double><<<g, BLOCK, 0, f.stream>>>(a);
+    k_pcorr<double><<<g, bs, 0, f.stream>>>(a);
   count_launches(1);
   OA_CUDA(cudaGetLastError());
   return OA_OK;
@@ -1175,15 +1178,16 @@ int launch_momentum(Flow& f, bool mixed) {
             f.mu,           f.sideU,   f.betaU, f.gradU, f.xloc32, f.umu32, f.b.A_mom, f.b.b_mom,
             f.du,           f.duT,     f.time_order ? f.dt_step : f.s.dt,  1.0 / f.s.urf_u, f.s.wall_rhs_relax,
             f.s.du_mode,    f.s.hr,    f.time_order, f.tk[0], f.tk[1], f.tk[2], f.Uold, f.Uoldold, f.err_dev};
-  const int g = grid_rows(f.mesh->nn);
+  const int bs = f.bs_asm;
+  const int g = grid_rows(f.mesh->nn, bs);
   const bool us = f.s.u_shifted, gs = f.s.u_grad_shifted;
   const bool hr = f.s.hr != 0 || f.time_order != 0 || f.s.du_mode != 0;  // the EXT variant
 #define OA_MOM(US, GS, T)                                                                   \
   if (us == US && gs == GS) {                                                               \
     if (hr)                                                                                 \
-      k_momentum<US, GS, T, true><<<g, BLOCK, 0, f.stream>>>(a);                            \
+      k_momentum<US, GS, T, true><<<g, bs, 0, f.stream>>>(a);                               \
     else                                                                                    \
-      k_momentum<US, GS, T, false><<<g, BLOCK, 0, f.stream>>>(a);                           \
+      k_momentum<US, GS, T, false><<<g, bs, 0, f.stream>>>(a);                              \
   }
   if (mixed) {
     OA_MOM(true, true, float) OA_MOM(true, false, float) OA_MOM(false, true, float) OA_MOM(false, false, float)
@@ -1203,13 +1207,14 @@ static int launch_mdot_impl(Flow& f, int mode) {
   MdotArgs a{f.mesh->view(), f.U,          f.p,          f.gradP,   f.du,     f.rho,
              f.s.du_mode == 1 ? f.duT : f.du, f.mDot, f.pc_flux,
              f.pc_coef,      f.s.mdot_urf, mode == 1 ? 1 : 0, mode == 2 ? 1 : 0, f.err_dev};
-  const int g = (f.mesh->ne + BLOCK - 1) / BLOCK;
+  const int bs = f.bs_elems;
+  const int g = (f.mesh->ne + bs - 1) / bs;
   const bool us = f.s.u_shifted, ps = f.s.p_grad_shifted;
 #define OA_MD(T, ST, SC)                                                                \
-  if (us && ps) k_mdot<true, true, T, ST, SC><<<g, BLOCK, 0, f.stream>>>(a);            \
-  else if (us && !ps) k_mdot<true, false, T, ST, SC><<<g, BLOCK, 0, f.stream>>>(a);     \
-  else if (!us && ps) k_mdot<false, true, T, ST, SC><<<g, BLOCK, 0, f.stream>>>(a);     \
-  else k_mdot<false, false, T, ST, SC><<<g, BLOCK, 0, f.stream>>>(a);
+  if (us && ps) k_mdot<true, true, T, ST, SC><<<g, bs, 0, f.stream>>>(a);            \
+  else if (us && !ps) k_mdot<true, false, T, ST, SC><<<g, bs, 0, f.stream>>>(a);     \
+  else if (!us && ps) k_mdot<false, true, T, ST, SC><<<g, bs, 0, f.stream>>>(a);     \
+  else k_mdot<false, false, T, ST, SC><<<g, bs, 0, f.stream>>>(a);
   const bool sc = f.s.du_mode == 1;
   if (mode == 0 || mode == 1) {
     OA_MD(double, false, false)
@@ -1236,22 +1241,23 @@ int launch_update_mdot(Flow& f, bool stage) { return launch_mdot_impl(f, stage ?
 
 int launch_div(Flow& f) {
   DivArgs a{f.mesh->view(), f.mDot, f.div, f.rho, f.time_order, f.tk[0], f.tk[1], f.tk[2], f.dt_step};
-  k_div<<<grid_rows(f.mesh->nn), BLOCK, 0, f.stream>>>(a);
+  k_div<<<grid_rows(f.mesh->nn, f.bs_rows), f.bs_rows, 0, f.stream>>>(a);
   count_launches(1);
   OA_CUDA(cudaGetLastError());
   return OA_OK;
 }
 
 int launch_gradient(Flow& f, int which) {
-  const int g = grid_rows(f.mesh->nn);
+  const int bs = f.bs_rows;
+  const int g = grid_rows(f.mesh->nn, bs);
   if (which == 0) {
     GradArgs a{f.mesh->view(), f.p, f.gradP, f.s.grad_urf};
-    if (f.s.p_shifted) k_gradient<1, true><<<g, BLOCK, 0, f.stream>>>(a);
-    else k_gradient<1, false><<<g, BLOCK, 0, f.stream>>>(a);
+    if (f.s.p_shifted) k_gradient<1, true><<<g, bs, 0, f.stream>>>(a);
+    else k_gradient<1, false><<<g, bs, 0, f.stream>>>(a);
   } else {
     GradArgs a{f.mesh->view(), f.U, f.gradU, f.s.grad_urf};
-    if (f.s.u_shifted) k_gradient<3, true><<<g, BLOCK, 0, f.stream>>>(a);
-    else k_gradient<3, false><<<g, BLOCK, 0, f.stream>>>(a);
+    if (f.s.u_shifted) k_gradient<3, true><<<g, bs, 0, f.stream>>>(a);
+    else k_gradient<3, false><<<g, bs, 0, f.stream>>>(a);
   }
   count_launches(1);
   OA_CUDA(cudaGetLastError());
@@ -1260,9 +1266,9 @@ int launch_gradient(Flow& f, int which) {
 
 int launch_blend_u(Flow& f) {
   BlendArgs a{f.mesh->view(), f.U, f.gradU, f.minU, f.maxU, f.betaU, f.s.beta_max};
-  const int g = grid_rows(f.mesh->nn);
-  k_minmax_u<<<g, BLOCK, 0, f.stream>>>(a);
-  k_blend_u<<<g, BLOCK, 0, f.stream>>>(a);
+  const int g = grid_rows(f.mesh->nn, f.bs_rows);
+  k_minmax_u<<<g, f.bs_rows, 0, f.stream>>>(a);
+  k_blend_u<<<g, f.bs_rows, 0, f.stream>>>(a);
   count_launches(2);
   OA_CUDA(cudaGetLastError());
   return OA_OK;

@@ -31,7 +31,7 @@ EXPORTS = [
     "oa_diffusion_create", "oa_diffusion_destroy", "oa_diffusion_set_field", "oa_diffusion_get_field",
     "oa_diffusion_field_device_ptr", "oa_diffusion_assemble", "oa_diffusion_solve", "oa_diffusion_step",
     "oa_diffusion_stream", "oa_diffusion_time_assembly", "oa_sst_default_constants", "oa_sst_node_update",
-    "oa_flow_last_control", "oa_flow_scales", "oa_flow_advance_time",
+    "oa_flow_last_control", "oa_flow_scales", "oa_flow_advance_time", "oa_flow_autotune", "oa_flow_set_tuning",
 ]
 
 OA_BND_FIXED_VALUE = 0
@@ -71,6 +71,16 @@ class ControlData(C.Structure):
         return dict(n_iterations=self.n_iterations, fallback=self.fallback,
                     solver_initial_res=list(self.solver_initial_res), solver_final_res=list(self.solver_final_res),
                     scaled_initial_res=list(self.scaled_initial_res))
+
+
+class Tuning(C.Structure):
+    """oa_tuning: launch shapes and pressure-solve schedule chosen by oa_flow_autotune."""
+    _fields_ = [("block_rows", C.c_int), ("block_elements", C.c_int), ("block_assembly", C.c_int),
+                ("gcr_chunk", C.c_int), ("amg_refresh", C.c_int), ("ms_per_iteration_before", C.c_double),
+                ("ms_per_iteration_after", C.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
 
 
 class IterStats(C.Structure):
@@ -166,6 +176,8 @@ def lib():
         "oa_flow_last_control": (C.c_int, [vp, C.c_int, P(ControlData)]),
         "oa_flow_scales": (C.c_int, [vp, dp, dp, dp]),
         "oa_flow_advance_time": (C.c_int, [vp, C.c_int, C.c_double]),
+        "oa_flow_autotune": (C.c_int, [vp, C.c_int, P(Tuning)]),
+        "oa_flow_set_tuning": (C.c_int, [vp, P(Tuning)]),
         "oa_flow_sync": (C.c_int, [vp]),
         "oa_flow_stream": (C.c_int, [vp, P(vp)]),
         "oa_launch_count": (C.c_int, [P(C.c_longlong)]),
@@ -334,6 +346,17 @@ class Flow:
     def advance_time(self, scheme, dt):
         """Start a time step of size dt: scheme 1 BDF1, 2 BDF2."""
         _check(lib().oa_flow_advance_time(self.h, int(scheme), float(dt)))
+
+    def autotune(self, iters=3):
+        """Tune launch shapes and the pressure-solve schedule; the flow state is
+        restored afterwards. Returns the chosen tuning as a dict."""
+        t = Tuning()
+        _check(lib().oa_flow_autotune(self.h, int(iters), C.byref(t)))
+        return t.as_dict()
+
+    def set_tuning(self, **kw):
+        t = Tuning(**{k: kw[k] for k, _ in Tuning._fields_ if k in kw})
+        _check(lib().oa_flow_set_tuning(self.h, C.byref(t)))
 
     def last_control(self, sys):
         """ControlData of the last solve of ``sys`` ("momentum"/0 or "pcorr"/1)."""
