@@ -16,6 +16,7 @@
 #include "oa_hex_orient.h"
 #include "oa_internal.h"
 #include "oa_krylov.h"
+#include "oa_rowlane.cuh"
 #include "oa_scalar_solve.h"
 
 namespace oa {
@@ -320,6 +321,27 @@ int oa_mesh_create(const double* coords, int nn, const int* conn, int ne, int to
     m.h_row_ptr[i + 1] = (int)m.h_cols.size();
   }
   m.nnz = m.h_row_ptr[nn];
+  // slot maps of the row write-out: which corner-lane neighbour blocks sum
+  // into each off-diagonal CSR entry (a row's lanes then add them in bit
+  // order, the same ascending (lane, neighbour) order as a search would)
+  std::vector<uint32_t> smask(m.nnz, 0u);
+  for (int i = 0; i < nn; ++i) {
+    const int* rb = m.h_cols.data() + m.h_row_ptr[i];
+    const int* re = m.h_cols.data() + m.h_row_ptr[i + 1];
+    for (int c = 0; c < 8; ++c) {
+      const int e = n2e[8L * i + c];
+      if (e < 0) continue;
+      for (int k = 0; k < 3; ++k) {
+        const int j = conn[8L * e + edge_nbr(c, k)];
+        const int* q = std::lower_bound(rb, re, j);
+        if (q == re || *q != j) {
+          delete M;
+          return fail(OA_ERR_MESH, "oa_mesh_create: an element edge is missing from the stencil graph");
+        }
+        smask[q - m.h_cols.data()] |= 1u << (3 * c + k);
+      }
+    }
+  }
   {
     // mean element edge length (the 12 edges are the SCS L/R pairs)
     double sum = 0.0;
@@ -345,6 +367,7 @@ int oa_mesh_create(const double* coords, int nn, const int* conn, int ne, int to
   int st = OA_OK;
   if ((st = dalloc(&m.x, 3L * nn)) || (st = dalloc(&m.conn, 8L * ne)) || (st = dalloc(&m.n2e, 8L * nn)) ||
       (st = dalloc(&m.row_ptr, nn + 1L)) || (st = dalloc(&m.cols, (size_t)m.nnz)) || (st = dalloc(&m.diag, (size_t)nn)) ||
+      (st = dalloc(&m.slot_mask, (size_t)m.nnz)) ||
       (st = dalloc(&m.face_mask, (size_t)ne)) || (st = dalloc(&m.vol, (size_t)nn)) || (st = dalloc(&m.wscv, 8L * ne)) ||
       (st = dalloc(&m.scs_area, 36L * ne)) ||
       (st = dalloc(&m.wall_node, (size_t)nn))) {
@@ -358,6 +381,7 @@ int oa_mesh_create(const double* coords, int nn, const int* conn, int ne, int to
   cudaMemcpy(m.row_ptr, m.h_row_ptr.data(), sizeof(int) * (nn + 1), cudaMemcpyHostToDevice);
   cudaMemcpy(m.cols, m.h_cols.data(), sizeof(int) * m.nnz, cudaMemcpyHostToDevice);
   cudaMemcpy(m.diag, m.h_diag.data(), sizeof(int) * nn, cudaMemcpyHostToDevice);
+  cudaMemcpy(m.slot_mask, smask.data(), sizeof(uint32_t) * m.nnz, cudaMemcpyHostToDevice);
   cudaMemcpy(m.face_mask, fmask.data(), ne, cudaMemcpyHostToDevice);
   cudaMemcpy(m.wall_node, wall.data(), sizeof(int) * nn, cudaMemcpyHostToDevice);
   cudaError_t ce = cudaDeviceSynchronize();
@@ -379,7 +403,7 @@ void oa_mesh_destroy(oa_mesh* M) {
   DeviceMesh& m = M->m;
   void* ptrs[] = {m.x,       m.conn,      m.n2e,      m.n2e_ptr,  m.n2f,       m.n2f_ptr, m.face_elem, m.face_ord,
                   m.face_bnd, m.row_ptr, m.cols,     m.diag,     m.face_mask, m.vol,     m.wscv,      m.wall_node,
-                  m.scs_area};
+                  m.scs_area, m.slot_mask};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (M->st) cudaStreamDestroy(M->st);

@@ -31,6 +31,9 @@ struct MeshView {
   int* row_ptr = nullptr;      // [nn+1]
   int* cols = nullptr;         // [nnz]
   int* diag = nullptr;         // [nn] offset of the diagonal within the row
+  // hex8: per off-diagonal CSR entry, the row's corner-lane contributions that
+  // land in it: bit 3c + k is lane c's edge neighbour k (edge_nbr order)
+  uint32_t* slot_mask = nullptr;  // [nnz]
   uint8_t* face_mask = nullptr;  // [ne] bit f: face f is a no-slip wall face
   double* vol = nullptr;       // [nn] dual nodal volume
   double* wscv = nullptr;      // [ne][8] SCV volume fractions (hex8)

@@ -145,26 +145,23 @@ int launch_geometry(DeviceMesh& m, cudaStream_t st) {
 
 // ---------------------------------------------------------------------------
 // CSR row write-out shared by the assembly kernels. Each lane publishes its
-// three edge-neighbour blocks with their column ids; lane s of the row then
-// emits CSR slot s (s, s+8, ...), summing the matching contributions in lane
-// order. The diagonal block is already reduced in every lane.
+// three edge-neighbour blocks; lane s of the row then emits CSR slot s (s,
+// s+8, ...), summing the blocks its precomputed slot mask names in ascending
+// (lane, neighbour) order. The diagonal block is already reduced in every lane.
 template <int B, class TM>
 __device__ __forceinline__ void write_row(int row, bool rv, int c, int lane, const TM (&diag)[B],
-                                          const TM (&nb)[3][B], const int (&nbc)[3],
-                                          const MeshView& m, TM* __restrict__ A, TM* sh_val,
-                                          int* sh_col, bool offdiag_zero) {
+                                          const TM (&nb)[3][B], const MeshView& m, TM* __restrict__ A,
+                                          TM* sh_val, bool offdiag_zero) {
 #pragma unroll
-  for (int k = 0; k < 3; ++k) {
-    sh_col[lane * 3 + k] = nbc[k];
+  for (int k = 0; k < 3; ++k)
 #pragma unroll
     for (int b = 0; b < B; ++b) sh_val[(lane * 3 + k) * B + b] = nb[k][b];
-  }
   __syncwarp();
   if (rv) {
     const int rp = __ldg(m.row_ptr + row);
     const int len = __ldg(m.row_ptr + row + 1) - rp;
     const int dof = __ldg(m.diag + row);
-    const int base = lane & ~7;
+    const TM* row_vals = sh_val + (lane & ~7) * 3 * B;
     for (int s = c; s < len; s += 8) {
       TM out[B];
       if (s == dof) {
@@ -173,16 +170,12 @@ __device__ __forceinline__ void write_row(int row, bool rv, int c, int lane, con
       } else {
 #pragma unroll
         for (int b = 0; b < B; ++b) out[b] = TM(0);
-        if (!offdiag_zero) {
-          const int col = __ldg(m.cols + rp + s);
+        uint32_t mk = offdiag_zero ? 0u : __ldg(m.slot_mask + rp + s);
+        while (mk) {
+          const TM* v = row_vals + (__ffs(mk) - 1) * B;
+          mk &= mk - 1;
 #pragma unroll
-          for (int c2 = 0; c2 < 8; ++c2)
-#pragma unroll
-            for (int k = 0; k < 3; ++k)
-              if (sh_col[(base + c2) * 3 + k] == col) {
-#pragma unroll
-                for (int b = 0; b < B; ++b) out[b] += sh_val[((base + c2) * 3 + k) * B + b];
-              }
+          for (int b = 0; b < B; ++b) out[b] += v[b];
         }
       }
 #pragma unroll
@@ -214,17 +207,9 @@ struct PcArgs {
   const uint8_t* ref_flag;  // [nn] 1 on pressure-level rows
 };
 
-// Edge neighbours of corner c in the order of the row slots (canonical nodes
-// 1, 3, 4 of the rotation that maps c to corner 0).
-__host__ __device__ constexpr int edge_nbr(int c, int s) {
-  constexpr int T[8][3] = {{1, 3, 4}, {0, 5, 2}, {3, 1, 6}, {2, 7, 0}, {5, 0, 7}, {4, 6, 1}, {7, 2, 5}, {6, 4, 3}};
-  return T[c][s];
-}
-
 template <class TF>
 __global__ void __launch_bounds__(BLOCK) k_pcorr(PcArgs a) {
   __shared__ TF sh_val[BLOCK * 3];
-  __shared__ int sh_col[BLOCK * 3];
   const int lane = threadIdx.x & 31;
   const int warp_base = threadIdx.x & ~31;
   const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 3;
@@ -233,16 +218,11 @@ __global__ void __launch_bounds__(BLOCK) k_pcorr(PcArgs a) {
   const int e = rv ? __ldg(a.m.n2e + 8 * row + c) : -1;
   TF diag[1] = {TF(0)};
   TF nb[3][1] = {{TF(0)}, {TF(0)}, {TF(0)}};
-  int nbc[3] = {-1, -1, -1};
   double rhs = 0.0;
   if (e >= 0) {
     const TF* cf = static_cast<const TF*>(a.coef) + 24 * (size_t)e + 3 * c;
-    const uint32_t pw = perm_word(c);
 #pragma unroll
-    for (int s = 0; s < 3; ++s) {
-      nb[s][0] = __ldg(cf + s);
-      nbc[s] = __ldg(a.m.conn + 8 * e + perm_at(pw, s == 0 ? 1 : (s == 1 ? 3 : 4)));
-    }
+    for (int s = 0; s < 3; ++s) nb[s][0] = __ldg(cf + s);
     diag[0] = -(nb[0][0] + nb[1][0] + nb[2][0]);
     const uint32_t iw = ip_word(c);
 #pragma unroll
@@ -255,8 +235,7 @@ __global__ void __launch_bounds__(BLOCK) k_pcorr(PcArgs a) {
   diag[0] = rowsum8(diag[0]);
   rhs = rowsum8(rhs);
   const bool refrow = rv && __ldg(a.ref_flag + row) != 0;
-  write_row<1, TF>(row, rv, c, lane, diag, nb, nbc, a.m, static_cast<TF*>(a.A),
-                   sh_val + warp_base * 3, sh_col + warp_base * 3, refrow);
+  write_row<1, TF>(row, rv, c, lane, diag, nb, a.m, static_cast<TF*>(a.A), sh_val + warp_base * 3, refrow);
   if (rv && c == 0) a.b[row] = refrow ? 0.0 : rhs;
 }
 
@@ -377,7 +356,6 @@ __device__ __forceinline__ void wall_face(const MomArgs& a, const TF (&x)[8][3],
 template <bool USH, bool UGSH, class TF, bool EXT = false>
 __global__ void __launch_bounds__(BLOCK, sizeof(TF) == 4 ? (UGSH ? 4 : 3) : 1) k_momentum(MomArgs a) {
   __shared__ TF sh_val[BLOCK * 3 * 9];
-  __shared__ int sh_col[BLOCK * 3];
   const int lane = threadIdx.x & 31;
   const int warp_base = threadIdx.x & ~31;
   const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 3;
@@ -391,7 +369,6 @@ __global__ void __launch_bounds__(BLOCK, sizeof(TF) == 4 ? (UGSH ? 4 : 3) : 1) k
     nb[0][k] = nb[1][k] = nb[2][k] = TF(0);
   }
   rhs[0] = rhs[1] = rhs[2] = TF(0);
-  int nbc[3] = {-1, -1, -1};
   if (e >= 0) {
     const uint32_t pw = perm_word(c);
     const uint32_t iw = ip_word(c);
@@ -551,9 +528,6 @@ __global__ void __launch_bounds__(BLOCK, sizeof(TF) == 4 ? (UGSH ? 4 : 3) : 1) k
       if (fm & (1u << ((fw >> 6) & 7))) wall_face<4, USH, UGSH, TF>(a, x, nd, Uc, mu, diag, nb, rhs, &err);
     }
     if (err) a.err[0] = 1;
-    nbc[0] = nd[1];
-    nbc[1] = nd[3];
-    nbc[2] = nd[4];
   }
 #pragma unroll
   for (int k = 0; k < 9; ++k) diag[k] = rowsum8(diag[k]);
@@ -615,8 +589,7 @@ __global__ void __launch_bounds__(BLOCK, sizeof(TF) == 4 ? (UGSH ? 4 : 3) : 1) k
       }
     }
   }
-  write_row<9, TF>(row, rv, c, lane, diag, nb, nbc, a.m, static_cast<TF*>(a.A),
-                   sh_val + warp_base * 3 * 9, sh_col + warp_base * 3, false);
+  write_row<9, TF>(row, rv, c, lane, diag, nb, a.m, static_cast<TF*>(a.A), sh_val + warp_base * 3 * 9, false);
 }
 
 // ---------------------------------------------------------------------------

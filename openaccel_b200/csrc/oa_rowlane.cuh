@@ -73,4 +73,11 @@ __device__ __forceinline__ T rowsum8(T v) {
 // diagonal block, as applyCoeff_'s deductUnfound does (assembler.h:423-445).
 __host__ __device__ constexpr int nb_slot(int a) { return a == 1 ? 0 : (a == 3 ? 1 : (a == 4 ? 2 : -1)); }
 
+// Edge neighbours of corner c in the order of a lane's neighbour slots
+// (canonical nodes 1, 3, 4 of the rotation that maps c to corner 0).
+__host__ __device__ constexpr int edge_nbr(int c, int s) {
+  constexpr int T[8][3] = {{1, 3, 4}, {0, 5, 2}, {3, 1, 6}, {2, 7, 0}, {5, 0, 7}, {4, 6, 1}, {7, 2, 5}, {6, 4, 3}};
+  return T[c][s];
+}
+
 }  // namespace oa

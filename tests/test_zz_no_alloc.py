@@ -27,6 +27,23 @@ def rel(a, b):
     return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)
 
 
+def host_residual(rp, cols, A, b, x):
+    """||b - A x|| / ||b|| in FP64 on the host, independent of either solver's
+    report; its own rounding (||A|| ||x|| eps / ||b||) is of order 1e-12 here,
+    so it is held to 1e-11 while the solvers report below 1e-12."""
+    import scipy.sparse as sp
+
+    M = sp.csr_matrix((A, cols, rp), shape=(b.size, b.size))
+    return np.linalg.norm(b - M @ x) / np.linalg.norm(b)
+
+
+# Both solves stop at a relative residual below 1e-12; the solutions then agree
+# to about cond(A) times that. The pressure-correction operator of these
+# meshes has a condition number of order 1e4, so 1e-8 leaves a margin while
+# staying five decades below the gap between the two systems (> 1e-3).
+X_TOL = 1e-8
+
+
 def _system(gf, seed):
     """Assemble the pressure-correction system of a flow state: a seeded
     Gaussian initial velocity, one SIMPLE outer iteration, then the assembly
@@ -76,12 +93,14 @@ def test_static_solve_matches_regular_solve_twice(n):
     A1, b1, x1_ref = _system(gf, seed=1)
     x1, it1, res1 = _static_solve(dev, A1, b1)
     assert res1 < 1e-12 and it1 > 0
-    assert rel(x1, x1_ref) < 1e-10
+    assert host_residual(rp, cols, A1, b1, x1) < 1e-11
+    assert rel(x1, x1_ref) < X_TOL
     # second call, different system: the shared array must not carry state over
     A2, b2, x2_ref = _system(gf, seed=2)
     x2, it2, res2 = _static_solve(dev, A2, b2)
     assert res2 < 1e-12
-    assert rel(x2, x2_ref) < 1e-10
+    assert host_residual(rp, cols, A2, b2, x2) < 1e-11
+    assert rel(x2, x2_ref) < X_TOL
     assert rel(x2, x1) > 1e-3  # genuinely a different system
 
 
