@@ -123,10 +123,11 @@ def run_ours(args, rank, world):
     gm = rt.Mesh(m)
 
     def make(prec):
-        # both forms replay their Krylov chunks as CUDA graphs, so the ratio of
-        # the two measures precision, not launch overhead
+        # both forms run the same graph mode (default: each outer iteration as
+        # one CUDA graph), so the ratio of the two measures precision, not
+        # launch overhead
         f = rt.Flow(gm, rt.default_settings(precision=prec, pc_rtol=args.pc_rtol, mom_rtol=args.mom_rtol,
-                                            mom_maxit=args.mom_maxit, use_graphs=0 if args.no_graphs else 1))
+                                            mom_maxit=args.mom_maxit, use_graphs=graph_mode(args)))
         f.set_field("U", U0)
         f.initialize()
         if not args.no_autotune:
@@ -231,7 +232,7 @@ def run_ours(args, rank, world):
         "data": "synthetic",
         "config": cavity_config(args, args.n, m.ne, m.nn, gm.nnz, world),
         "fp64_outer_iters_per_s": value64,
-        "graphs": "Krylov chunks replayed as CUDA graphs in both forms" if not args.no_graphs else "off",
+        "graphs": GRAPH_MODES[graph_mode(args)],
         "autotune": {("mixed" if k == rt.OA_PREC_MIXED else "fp64"): v for k, v in tuning.items()} or "off",
         "mixed_over_fp64": value / value64,
         "assembled_elems_per_s": {"mixed": 2 * m.ne / ((t_mom + t_pc) * 1e-3),
@@ -274,7 +275,7 @@ def converge(args, gm, U0, dev, world, tuning=None):
     fields = {}
     for name, prec in (("mixed", rt.OA_PREC_MIXED), ("fp64", rt.OA_PREC_FP64)):
         f = rt.Flow(gm, rt.default_settings(precision=prec, pc_rtol=args.pc_rtol, mom_rtol=args.mom_rtol,
-                                            mom_maxit=args.mom_maxit, use_graphs=0 if args.no_graphs else 1))
+                                            mom_maxit=args.mom_maxit, use_graphs=graph_mode(args)))
         f.set_field("U", U0)
         f.initialize()
         if tuning and prec in tuning:  # the timed legs' tuning
@@ -343,7 +344,7 @@ def run_conduction(args, rank, world):
 
     def make(prec):
         d = rt.Diffusion(gm, rt.default_diffusion_settings(precision=prec, rtol=args.diff_rtol,
-                                                           use_graphs=0 if args.no_graphs else 1))
+                                                           use_graphs=graph_mode(args)))
         d.set_field("gamma", gam)
         d.set_field("src", src)
         return d
@@ -428,7 +429,7 @@ def run_batch(args, rank, world):
     kw = dict(pc_rtol=args.pc_rtol, mom_rtol=args.mom_rtol, mom_maxit=args.mom_maxit)
     gm = rt.Mesh(bt.mesh)
     fb = rt.Flow(gm, rt.default_settings(precision=rt.OA_PREC_MIXED, ref_node=-1,
-                                         use_graphs=0 if args.no_graphs else 1, **kw))
+                                         use_graphs=graph_mode(args), **kw))
     fb.set_field("mu", bt.mu)
     fb.set_reference_nodes(bt.ref_nodes)
     fb.initialize()
@@ -616,6 +617,17 @@ def cpu_sample(args, threads, warmup, steps, budget_s):
     }
 
 
+GRAPH_MODES = {0: "off", 1: "Krylov chunks replayed as CUDA graphs in both forms",
+               2: "each outer iteration after the first replayed as one CUDA graph (solver loops as device-side "
+                  "conditional nodes) in both forms"}
+
+
+def graph_mode(args):
+    if args.graphs is not None:
+        return args.graphs
+    return 0 if args.no_graphs else 2
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -631,6 +643,8 @@ def main():
     ap.add_argument("--mom-maxit", type=int, default=20)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-graphs", action="store_true")
+    ap.add_argument("--graphs", type=int, default=None, choices=[0, 1, 2],
+                    help="0 none, 1 Krylov chunks as CUDA graphs, 2 each outer iteration as one CUDA graph")
     ap.add_argument("--no-autotune", action="store_true", help="skip the launch-shape / solve-schedule autotuning")
     ap.add_argument("--only-mixed", action="store_true", help="time the mixed form only (profiling)")
     ap.add_argument("--workload", default="cavity", choices=["cavity", "conduction", "batch", "sst"],

@@ -54,7 +54,11 @@ typedef struct oa_flow_settings {
   int precision;                /* OA_PREC_FP64 or OA_PREC_MIXED */
   int pc_amg;                   /* 1: aggregation-AMG preconditioned GCR(2) pressure solve (BiCGStab
                                    if GCR stagnates or OA_KRYLOV=bicgstab), 0: Jacobi BiCGStab */
-  int use_graphs;               /* 1: replay Krylov iteration chunks as CUDA graphs */
+  int use_graphs;               /* 1: replay Krylov iteration chunks as CUDA graphs; 2: run each
+                                   outer iteration of oa_simple_iterate after the first as one CUDA
+                                   graph whose solver loops are device-side conditional nodes (no
+                                   host round trip inside the iteration; recaptured when tuning,
+                                   time step or solver fallback change what it holds) */
   int hr;                       /* advection: 0 upwind, 1 high resolution (advectionSchemeType::highResolution:
                                    blended deferred correction, nodeField::updateBlendingFactorField) */
   double beta_max;              /* upper limit of the blending factor (nodeField.h:150, default 1) */

@@ -20,7 +20,7 @@ SOURCES = ["oa_kernels.cu", "oa_krylov.cu", "oa_amg.cu", "oa_capi.cu", "oa_stati
            "oa_diffusion.cu", "oa_sst.cu"]
 HEADERS = ["oa_geom.cuh", "oa_hex8.cuh", "oa_tet4.cuh", "oa_rowlane.cuh", "oa_internal.h", "oa_krylov.h", "oa_amg.h",
            "oa_amg_symbolic.h", "oa_tet4_lists.h", "oa_hex_orient.h",
-           "oa_scalar_solve.h"]
+           "oa_scalar_solve.h", "oa_graph.h"]
 
 NVCC = os.environ.get("NVCC", "nvcc")
 FLAGS = [

@@ -49,6 +49,57 @@ __global__ void k_from_double(size_t n, const double* a, T* b) {
 
 using namespace oa;
 
+// What a captured outer-iteration graph baked into its kernel arguments and
+// node structure; a change of any of it means a new capture.
+struct IterGraphKey {
+  oa_flow_settings s;
+  int bs_rows, bs_elems, bs_asm;
+  int time_order;
+  double tk[3], dt_step;
+  int pc_gcr, pc_chunk, pc_refresh;
+  double pc_floor;
+  bool operator==(const IterGraphKey& o) const { return std::memcmp(this, &o, sizeof(*this)) == 0; }
+};
+
+// The whole SIMPLE outer iteration as one CUDA graph (settings.use_graphs =
+// 2): assembly kernels, the momentum and pressure-correction solves with
+// their convergence loops as conditional device-side nodes, the corrections,
+// and copies of every scalar the host reports into one pinned block.
+struct IterGraph {
+  cudaGraphExec_t exec = nullptr;
+  GraphBuild gb;
+  IterGraphKey key;
+  BodyCounters* ctr = nullptr;       // device
+  BodyCounters* ctr_host = nullptr;  // pinned
+  double* dsum = nullptr;            // device [8]: momentum |b|^2, |r|^2 per component, |b_pc|^2
+  double* hsum = nullptr;            // pinned [8]
+  KScal* mom_host = nullptr;         // pinned copy of the momentum solver's scalars
+  int* herr = nullptr;               // pinned copy of the flow's error flag
+  cudaEvent_t ev[6] = {};            // phase boundaries (event nodes)
+  void drop() {
+    if (exec) cudaGraphExecDestroy(exec);
+    exec = nullptr;
+  }
+  void release() {
+    drop();
+    if (ctr) cudaFree(ctr);
+    if (dsum) cudaFree(dsum);
+    if (ctr_host) cudaFreeHost(ctr_host);
+    if (hsum) cudaFreeHost(hsum);
+    if (mom_host) cudaFreeHost(mom_host);
+    if (herr) cudaFreeHost(herr);
+    for (auto& e : ev)
+      if (e) cudaEventDestroy(e);
+    ctr = nullptr;
+    dsum = nullptr;
+    ctr_host = nullptr;
+    hsum = nullptr;
+    mom_host = nullptr;
+    herr = nullptr;
+    for (auto& e : ev) e = nullptr;
+  }
+};
+
 struct oa_flow {
   Flow f;
   KrylovSolver<3, double, double> mom64;
@@ -56,6 +107,8 @@ struct oa_flow {
   ScalarSolve pc;           // pressure-correction solve
   double* scal = nullptr;   // [8] device scalars
   double* hscal = nullptr;  // pinned
+  IterGraph ig;
+  int eager_iters = 0;      // outer iterations run without the whole-iteration graph
 };
 
 namespace {
@@ -186,9 +239,7 @@ int pc_rhs_rms(oa_flow* h, double* out) {
 // inner iterations under FP64 iterative refinement), with its ControlData
 // record. rhs_rms: RMS of the rhs when the caller has it already (< 0: formed
 // here).
-int solve_pcorr(oa_flow* h, double rtol, int maxit, int* iters, double* res, int* refinements, double rhs_rms = -1.0) {
-  Flow& f = h->f;
-  DeviceMesh& m = *f.mesh;
+ScalarGraph pc_graph(const DeviceMesh& m) {
   ScalarGraph g;
   g.nn = m.nn;
   g.rp = m.row_ptr;
@@ -197,6 +248,12 @@ int solve_pcorr(oa_flow* h, double rtol, int maxit, int* iters, double* res, int
   g.h_rp = m.h_row_ptr.data();
   g.h_cols = m.h_cols.data();
   g.h_diag = m.h_diag.data();
+  return g;
+}
+
+int solve_pcorr(oa_flow* h, double rtol, int maxit, int* iters, double* res, int* refinements, double rhs_rms = -1.0) {
+  Flow& f = h->f;
+  const ScalarGraph g = pc_graph(*f.mesh);
   if (rhs_rms < 0)
     if (int s = pc_rhs_rms(h, &rhs_rms)) return s;
   const int fb0 = h->pc.fallbacks;
@@ -214,6 +271,208 @@ int solve_pcorr(oa_flow* h, double rtol, int maxit, int* iters, double* res, int
   cd.scaled_initial_res[0] = rhs_rms / f.mass_scale;
   if (iters) *iters = it;
   if (res) *res = r;
+  return OA_OK;
+}
+
+IterGraphKey iter_graph_key(oa_flow* h) {
+  IterGraphKey k;
+  std::memset(&k, 0, sizeof(k));
+  const Flow& f = h->f;
+  k.s = f.s;
+  k.bs_rows = f.bs_rows;
+  k.bs_elems = f.bs_elems;
+  k.bs_asm = f.bs_asm;
+  k.time_order = f.time_order;
+  for (int i = 0; i < 3; ++i) k.tk[i] = f.tk[i];
+  k.dt_step = f.dt_step;
+  k.pc_gcr = h->pc.gcr ? 1 : 0;
+  k.pc_chunk = h->pc.gcr_chunk;
+  k.pc_refresh = h->pc.refresh;
+  k.pc_floor = h->pc.inner_floor;
+  return k;
+}
+
+// Capture one outer iteration (the steps of oa_simple_iterate, in its order)
+// into a graph with device-side loops; the solvers were set up by an eager
+// iteration before.
+int build_iteration_graph(oa_flow* h) {
+  Flow& f = h->f;
+  DeviceMesh& m = *f.mesh;
+  IterGraph& G = h->ig;
+  const bool mx = mixed(f);
+  if (!G.ctr) {
+    if (cudaMalloc(&G.ctr, sizeof(BodyCounters)) != cudaSuccess || cudaMalloc(&G.dsum, 8 * sizeof(double)) != cudaSuccess ||
+        cudaMallocHost(&G.ctr_host, sizeof(BodyCounters)) != cudaSuccess ||
+        cudaMallocHost(&G.hsum, 8 * sizeof(double)) != cudaSuccess ||
+        cudaMallocHost(&G.mom_host, sizeof(KScal)) != cudaSuccess || cudaMallocHost(&G.herr, sizeof(int)) != cudaSuccess)
+      return fail(OA_ERR_CUDA, "iteration graph: allocation failed");
+    for (auto& e : G.ev) OA_CUDA(cudaEventCreate(&e));
+  }
+  G.drop();
+  G.gb = GraphBuild{};
+  G.gb.st = f.stream;
+  G.gb.ctr = G.ctr;
+  GraphBuild& gb = G.gb;
+  cudaGraph_t g = nullptr;
+  OA_CUDA(cudaGraphCreate(&g, 0));
+  struct GraphGuard {
+    cudaGraph_t g;
+    ~GraphGuard() {
+      if (g) cudaGraphDestroy(g);
+    }
+  } guard{g};
+  Deps d;
+  auto mark = [&](int k) -> int {
+    OA_CUDA(cudaEventRecordWithFlags(G.ev[k], f.stream, cudaEventRecordExternal));
+    return OA_OK;
+  };
+  const int n3 = 3 * m.nn;
+  // momentum predictor: assembly, then the solve as a device-side loop
+  if (int s = gb.seg(g, d, -1, [&]() -> int {
+        if (int s2 = launch_counters_reset(gb)) return s2;
+        if (int s2 = mark(0)) return s2;
+        if (int s2 = launch_momentum(f, mx)) return s2;
+        return mark(1);
+      }))
+    return s;
+  constexpr int MOM_CHUNK = 2;  // device-side checks are cheap: short chunks
+  if (mx) {
+    h->mom32.amg = nullptr;
+    if (int s = h->mom32.setup(m.nn, m.row_ptr, m.cols, m.diag, f.stream)) return s;
+    if (int s = h->mom32.emit<float>(gb, g, d, -1, static_cast<const float*>(f.b.A_mom),
+                                     static_cast<const float*>(f.b.b_mom), f.s.mom_rtol, f.s.mom_maxit, nullptr,
+                                     nullptr, f.s.mom_maxit, MOM_CHUNK, false, -1))
+      return s;
+  } else {
+    h->mom64.amg = nullptr;
+    if (int s = h->mom64.setup(m.nn, m.row_ptr, m.cols, m.diag, f.stream)) return s;
+    if (int s = h->mom64.emit<double>(gb, g, d, -1, static_cast<const double*>(f.b.A_mom),
+                                      static_cast<const double*>(f.b.b_mom), f.s.mom_rtol, f.s.mom_maxit, nullptr,
+                                      nullptr, f.s.mom_maxit, MOM_CHUNK, false, -1))
+      return s;
+  }
+  // U += x, the momentum ControlData sums; mass flow and pressure-correction
+  // assembly with the rhs norm
+  if (int s = gb.seg(g, d, -1, [&]() -> int {
+        if (mx) {
+          k_to_double<float><<<(n3 + 255) / 256, 256, 0, f.stream>>>((size_t)n3, h->mom32.solution(), f.b.x_mom);
+          count_launches(1);
+          if (int s2 = device_comp_sumsq3<float>(m.nn, static_cast<const float*>(f.b.b_mom), G.dsum, f.red, f.stream))
+            return s2;
+          if (int s2 = device_comp_sumsq3<float>(m.nn, h->mom32.residual(), G.dsum + 3, f.red, f.stream)) return s2;
+          OA_CUDA(cudaMemcpyAsync(G.mom_host, h->mom32.scalars(), sizeof(KScal), cudaMemcpyDeviceToHost, f.stream));
+        } else {
+          OA_CUDA(cudaMemcpyAsync(f.b.x_mom, h->mom64.solution(), sizeof(double) * n3, cudaMemcpyDeviceToDevice,
+                                  f.stream));
+          if (int s2 = device_comp_sumsq3<double>(m.nn, static_cast<const double*>(f.b.b_mom), G.dsum, f.red,
+                                                  f.stream))
+            return s2;
+          if (int s2 = device_comp_sumsq3<double>(m.nn, h->mom64.residual(), G.dsum + 3, f.red, f.stream)) return s2;
+          OA_CUDA(cudaMemcpyAsync(G.mom_host, h->mom64.scalars(), sizeof(KScal), cudaMemcpyDeviceToHost, f.stream));
+        }
+        k_axpy<<<(n3 + 255) / 256, 256, 0, f.stream>>>(n3, f.U, f.b.x_mom, 1.0);
+        count_launches(1);
+        if (int s2 = mark(2)) return s2;
+        if (int s2 = launch_update_mdot(f, true)) return s2;
+        if (int s2 = launch_pcorr(f, mx, true)) return s2;
+        if (int s2 = device_sumsq(m.nn, f.b.b_pc, G.dsum + 6, f.red, f.stream)) return s2;
+        return mark(3);
+      }))
+    return s;
+  // pressure-correction solve
+  const ScalarGraph pg = pc_graph(m);
+  if (int s = h->pc.emit(gb, g, d, pg, mx, f.s.pc_amg != 0, f.b.A_pc, f.b.b_pc, f.b.x_pc, f.s.pc_rtol, f.s.pc_maxit,
+                         f.stream))
+    return s;
+  // corrections and gradients; the scalars the host reads
+  if (int s = gb.seg(g, d, -1, [&]() -> int {
+        if (int s2 = mark(4)) return s2;
+        k_axpy<<<(m.nn + 255) / 256, 256, 0, f.stream>>>(m.nn, f.p, f.b.x_pc, f.s.urf_p);
+        count_launches(1);
+        if (int s2 = launch_update_mdot(f)) return s2;
+        if (int s2 = launch_div(f)) return s2;
+        if (int s2 = launch_axpy_du_gradp(f, +1.0)) return s2;
+        if (int s2 = launch_gradient(f, 0)) return s2;
+        if (int s2 = launch_axpy_du_gradp(f, -1.0)) return s2;
+        if (int s2 = launch_gradient(f, 1)) return s2;
+        if (f.s.hr)
+          if (int s2 = launch_blend_u(f)) return s2;
+        if (int s2 = mark(5)) return s2;
+        OA_CUDA(cudaMemcpyAsync(G.hsum, G.dsum, 8 * sizeof(double), cudaMemcpyDeviceToHost, f.stream));
+        OA_CUDA(cudaMemcpyAsync(G.herr, f.err_dev, sizeof(int), cudaMemcpyDeviceToHost, f.stream));
+        OA_CUDA(cudaMemcpyAsync(G.ctr_host, G.ctr, sizeof(BodyCounters), cudaMemcpyDeviceToHost, f.stream));
+        return OA_OK;
+      }))
+    return s;
+  const cudaError_t ie = cudaGraphInstantiate(&G.exec, g, 0);
+  if (ie != cudaSuccess) {
+    G.exec = nullptr;
+    return fail(OA_ERR_CUDA, std::string("iteration graph instantiate: ") + cudaGetErrorString(ie));
+  }
+  G.key = iter_graph_key(h);
+  return OA_OK;
+}
+
+// One outer iteration by the graph; the same statistics and ControlData as
+// the eager path, from the pinned copies the graph wrote.
+int iterate_graph(oa_flow* h, oa_iter_stats* out) {
+  Flow& f = h->f;
+  IterGraph& G = h->ig;
+  const int nn = f.mesh->nn;
+  if (G.exec && !(iter_graph_key(h) == G.key)) G.drop();
+  if (!G.exec)
+    if (int s = build_iteration_graph(h)) {
+      G.drop();
+      return s;
+    }
+  if (int s = h->pc.graph_prepare(f.stream)) return s;
+  OA_CUDA(cudaGraphLaunch(G.exec, f.stream));
+  OA_CUDA(cudaStreamSynchronize(f.stream));
+  count_launches(G.gb.launches(*G.ctr_host));
+  if (*G.herr) {
+    OA_CUDA(cudaMemsetAsync(f.err_dev, 0, sizeof(int), f.stream));
+    OA_CUDA(cudaStreamSynchronize(f.stream));
+    return fail(OA_ERR_GEOMETRY, "oa_simple_iterate: singular Jacobian (det <= 1e6*realmin)");
+  }
+  oa_iter_stats st{};
+  const KScal& K = *G.mom_host;
+  if (K.status == 2) return fail(OA_ERR_SOLVER, "BiCGStab: non-finite residual");
+  st.mom_iters = K.iters;
+  st.mom_res = K.bnorm > 0 ? K.rnorm / K.bnorm : 0.0;
+  oa_control_data& cm = f.cd_mom;
+  cm = oa_control_data{};
+  cm.n_iterations = K.iters;
+  for (int k = 0; k < 3; ++k) {
+    cm.solver_initial_res[k] = std::sqrt(G.hsum[k] / nn);
+    cm.solver_final_res[k] = std::sqrt(G.hsum[3 + k] / nn);
+    cm.scaled_initial_res[k] = cm.solver_initial_res[k] / f.mom_scale;
+  }
+  st.continuity_rms_raw = std::sqrt(G.hsum[6] / nn);
+  st.continuity_rms = st.continuity_rms_raw / f.mass_scale;
+  bool recapture = false;
+  const int fb0 = h->pc.fallbacks;
+  const int ps = h->pc.graph_result(mixed(f), &st.pc_iters, &st.pc_res, &st.pc_refinements, &recapture, "pressure");
+  if (recapture) G.drop();
+  if (ps) return ps;
+  oa_control_data& cp = f.cd_pc;
+  cp = oa_control_data{};
+  cp.n_iterations = st.pc_iters;
+  cp.fallback = h->pc.fallbacks != fb0;
+  cp.solver_initial_res[0] = st.continuity_rms_raw;
+  cp.solver_final_res[0] = st.pc_res * st.continuity_rms_raw;
+  cp.scaled_initial_res[0] = st.continuity_rms_raw / f.mass_scale;
+  if (out) {
+    float t[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
+    for (int k = 0; k < 5; ++k) cudaEventElapsedTime(&t[k], G.ev[k], G.ev[k + 1]);
+    st.ms_momentum_assembly = t[0];
+    st.ms_momentum_solve = t[1];
+    st.ms_pcorr_assembly = t[2];
+    st.ms_pcorr_solve = t[3];
+    st.ms_corrections = t[4];
+    st.mom = f.cd_mom;
+    st.pc = f.cd_pc;
+    *out = st;
+  }
   return OA_OK;
 }
 
@@ -433,6 +692,7 @@ int oa_flow_create(oa_mesh* M, const oa_flow_settings* s, const double* bnd_velo
   if (!M || !s || !out || nbnd < 0 || (nbnd > 0 && !bnd_velocity)) return fail(OA_ERR_ARG, "oa_flow_create: bad arguments");
   if (s->urf_u <= 0 || s->urf_p <= 0 || s->dt <= 0) return fail(OA_ERR_ARG, "oa_flow_create: relaxation/timescale must be > 0");
   if (s->precision != OA_PREC_FP64 && s->precision != OA_PREC_MIXED) return fail(OA_ERR_ARG, "oa_flow_create: unknown precision");
+  if (s->use_graphs < 0 || s->use_graphs > 2) return fail(OA_ERR_ARG, "oa_flow_create: use_graphs must be 0, 1 or 2");
   if (s->hr != 0 && s->hr != 1) return fail(OA_ERR_ARG, "oa_flow_create: advection scheme must be 0 (upwind) or 1 (high resolution)");
   if (s->hr && !(s->beta_max > 0)) return fail(OA_ERR_ARG, "oa_flow_create: beta_max must be > 0 for high resolution");
   if (s->du_mode < 0 || s->du_mode > 2)
@@ -552,6 +812,7 @@ void oa_flow_destroy(oa_flow* H) {
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (H->hscal) cudaFreeHost(H->hscal);
+  H->ig.release();
   H->pc.release();
   H->mom64.release();
   H->mom32.release();
@@ -720,6 +981,14 @@ int oa_simple_iterate(oa_flow* H, int n, oa_iter_stats* stats) {
   };
   int s = OA_OK;
   for (int it = 0; it < n && s == OA_OK; ++it) {
+    if (f.s.use_graphs == 2 && H->eager_iters > 0) {
+      // the whole outer iteration as one graph (the first iteration ran eagerly
+      // and set up the solvers and the AMG hierarchy)
+      nvtxRangePushA("oa_simple_iterate (graph)");
+      s = iterate_graph(H, stats ? stats + it : nullptr);
+      nvtxRangePop();
+      continue;
+    }
     oa_iter_stats st{};
     nvtxRangePushA("oa_simple_iterate");
     // momentum predictor (navierStokesEquation::solve)
@@ -760,6 +1029,7 @@ int oa_simple_iterate(oa_flow* H, int n, oa_iter_stats* stats) {
     mark(5);
     nvtxRangePop();
     if (!s) s = check_err_flag(f, "oa_simple_iterate");  // synchronises the stream
+    if (!s) ++H->eager_iters;
     if (!s && stats) {
       float t[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
       for (int k = 0; k < 5; ++k) cudaEventElapsedTime(&t[k], ev[k], ev[k + 1]);

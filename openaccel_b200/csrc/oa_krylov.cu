@@ -26,14 +26,6 @@ namespace oa {
 constexpr int KB = 256;        // threads per block for vector kernels
 constexpr int MAX_PARTIALS = 2048;
 
-struct KScal {
-  double rho, alpha, omega, bnorm, rnorm;
-  double d0, d1, d2;  // reduced dots of the current phase
-  double rtol;
-  int maxit;
-  int done, iters, status;
-};
-
 template <class T>
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
@@ -174,13 +166,15 @@ __global__ void __launch_bounds__(KB) k_init(int n, const TB* __restrict__ b, TV
   block_reduce_store<1>(s, partials, MAX_PARTIALS);
 }
 
+// rtol_dev / maxit_dev (when not null) replace rtol / maxit: the inner solves
+// of a graph-captured iterative refinement take them from the refinement state
 __global__ void __launch_bounds__(KB) k_init_scalars(KScal* sc, const double* partials, int nb, double rtol,
-                                                      int maxit) {
+                                                      int maxit, const double* rtol_dev, const int* maxit_dev) {
   double o[1];
   final_reduce<1>(partials, nb, o);
   if (threadIdx.x == 0) {
-    sc->rtol = rtol;
-    sc->maxit = maxit;
+    sc->rtol = rtol_dev ? *rtol_dev : rtol;
+    sc->maxit = maxit_dev ? *maxit_dev : maxit;
     sc->bnorm = sqrt(o[0]);
     sc->rnorm = sc->bnorm;
     sc->rho = sc->alpha = sc->omega = 1.0;
@@ -470,28 +464,94 @@ void KrylovSolver<B, TM, TV>::release() {
 }
 
 template <int B, class TM, class TV>
+int KrylovSolver<B, TM, TV>::precond(const TV* in, TV* out) {
+  constexpr bool kAmgOk = (B == 1) && std::is_same<TM, TV>::value;
+  KScal* sc = static_cast<KScal*>(scal);
+  if constexpr (kAmgOk) {
+    if (amg) return amg->apply(reinterpret_cast<const TV*>(in), out, &sc->done, st);
+  }
+  const int gfull = (B * nn + KB - 1) / KB;
+  k_prec<B, TV><<<gfull, KB, 0, st>>>(nn, reinterpret_cast<const TV*>(Minv), in, out, sc);
+  count_launches(1);
+  return OA_OK;
+}
+
+// x = 0, r = rh = b, p = v = 0, inverse (block) diagonal, device scalars; the
+// GCR(2) direction slots start at zero (no stored directions yet)
+template <int B, class TM, class TV>
 template <class TB>
-int KrylovSolver<B, TM, TV>::solve(const TM* A, const TB* b, TV*& xout, double rtol, int maxit, int* iters,
-                                   double* res, int check_every, bool reuse_precond) {
+int KrylovSolver<B, TM, TV>::prologue(const TM* A, const TB* b, double rtol, int maxit, const double* rtol_dev,
+                                      const int* maxit_dev, bool use_gcr) {
   const int n = B * nn;
-  // work vectors: x r rh p v ph sh t
+  TV *x = static_cast<TV*>(vec[0]), *r = static_cast<TV*>(vec[1]), *rh = static_cast<TV*>(vec[2]),
+     *p = static_cast<TV*>(vec[3]), *v = static_cast<TV*>(vec[4]);
+  KScal* sc = static_cast<KScal*>(scal);
+  const int gfull = (n + KB - 1) / KB;
+  const int gv = gfull < MAX_PARTIALS ? gfull : MAX_PARTIALS;
+  const int gr = (nn + KB - 1) / KB;
+  k_build_minv<B, TM, TV><<<gr, KB, 0, st>>>(nn, rp, dg, A, reinterpret_cast<TV*>(Minv));
+  k_init<TV, TB><<<gv, KB, 0, st>>>(n, b, x, r, rh, p, v, partials);
+  k_init_scalars<<<1, KB, 0, st>>>(sc, partials, gv, rtol, maxit, rtol_dev, maxit_dev);
+  count_launches(3);
+  OA_CUDA(cudaGetLastError());
+  if (use_gcr)
+    for (int k = 4; k < 8; ++k) OA_CUDA(cudaMemsetAsync(vec[k], 0, sizeof(TV) * (size_t)n, st));
+  return OA_OK;
+}
+
+// one chunk of check_every iterations; every kernel reads its scalars and the
+// tolerance from device memory, so a chunk can be captured once and replayed
+template <int B, class TM, class TV>
+int KrylovSolver<B, TM, TV>::chunk(const TM* A, int check_every, bool use_gcr) {
+  const int n = B * nn;
   TV *x = static_cast<TV*>(vec[0]), *r = static_cast<TV*>(vec[1]), *rh = static_cast<TV*>(vec[2]),
      *p = static_cast<TV*>(vec[3]), *v = static_cast<TV*>(vec[4]), *ph = static_cast<TV*>(vec[5]),
      *sh = static_cast<TV*>(vec[6]), *t = static_cast<TV*>(vec[7]);
   KScal* sc = static_cast<KScal*>(scal);
-  const int gfull = (n + KB - 1) / KB;                 // element-wise kernels
-  const int gv = gfull < MAX_PARTIALS ? gfull : MAX_PARTIALS;  // reducing kernels (grid-stride)
-  const int gr = (nn + KB - 1) / KB;
-  constexpr bool kAmgOk = (B == 1) && std::is_same<TM, TV>::value;
-  const int* done_flag = &sc->done;
-  auto precond = [&](const TV* in, TV* out) -> int {
-    if constexpr (kAmgOk) {
-      if (amg) return amg->apply(reinterpret_cast<const TV*>(in), out, done_flag, st);
+  const int gfull = (n + KB - 1) / KB;
+  const int gv = gfull < MAX_PARTIALS ? gfull : MAX_PARTIALS;
+  if (use_gcr) {
+    // GCR(2) work vectors in the same buffers: x r z q P0 P1 Q0 Q1
+    TV *gz = rh, *gq = p, *gP[2] = {v, ph}, *gQ[2] = {sh, t};
+    for (int it = 0; it < check_every; ++it) {
+      const int slot = it & 1;  // the older of the two stored directions
+      if (int s = precond(r, gz)) return s;
+      k_spmv_gcr<TM, TV><<<gv, KB, 0, st>>>(nn, rp, cols, A, gz, gq, gQ[0], gQ[1], partials, sc);
+      k_gcr_beta<<<1, KB, 0, st>>>(sc, partials, gv);
+      k_gcr_orth<TV><<<gv, KB, 0, st>>>(n, gz, gq, gP[0], gP[1], gQ[0], gQ[1], r, partials, sc);
+      k_gcr_alpha<<<1, KB, 0, st>>>(sc, partials, gv);
+      k_gcr_update<TV><<<gv, KB, 0, st>>>(n, x, r, gz, gq, gP[slot], gQ[slot], partials, sc);
+      k_gcr_end<<<1, KB, 0, st>>>(sc, partials, gv);
     }
-    k_prec<B, TV><<<gfull, KB, 0, st>>>(nn, reinterpret_cast<const TV*>(Minv), in, out, sc);
-    count_launches(1);
+    count_launches(6L * check_every);
+    OA_CUDA(cudaGetLastError());
     return OA_OK;
-  };
+  }
+  for (int it = 0; it < check_every; ++it) {
+    k_p_update<TV><<<gfull, KB, 0, st>>>(n, p, r, v, sc);
+    if (int s = precond(p, ph)) return s;
+    k_spmv<B, TM, TV, 1><<<gv, KB, 0, st>>>(nn, rp, cols, A, ph, v, rh, nullptr, partials, sc);
+    k_alpha<<<1, KB, 0, st>>>(sc, partials, gv);
+    k_s_update<TV><<<gfull, KB, 0, st>>>(n, r, v, sc);
+    if (int s = precond(r, sh)) return s;
+    k_spmv<B, TM, TV, 2><<<gv, KB, 0, st>>>(nn, rp, cols, A, sh, t, r, nullptr, partials, sc);
+    k_omega<<<1, KB, 0, st>>>(sc, partials, gv);
+    k_x_update<TV><<<gv, KB, 0, st>>>(n, x, r, ph, sh, t, rh, partials, sc);
+    k_end_iter<<<1, KB, 0, st>>>(sc, partials, gv);
+  }
+  count_launches(8L * check_every);
+  OA_CUDA(cudaGetLastError());
+  return OA_OK;
+}
+
+template <int B, class TM, class TV>
+template <class TB>
+int KrylovSolver<B, TM, TV>::solve(const TM* A, const TB* b, TV*& xout, double rtol, int maxit, int* iters,
+                                   double* res, int check_every, bool reuse_precond) {
+  constexpr bool kAmgOk = (B == 1) && std::is_same<TM, TV>::value;
+  KScal* sc = static_cast<KScal*>(scal);
+  const bool use_gcr = gcr && B == 1;
+  if (use_gcr && check_every % 2) return fail(OA_ERR_ARG, "GCR: iteration chunks must hold an even number of iterations");
   // OA_DEBUG: device time of the preconditioner set-up and of the whole solve
   const bool dbg = std::getenv("OA_DEBUG") != nullptr;
   cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
@@ -506,64 +566,16 @@ int KrylovSolver<B, TM, TV>::solve(const TM* A, const TB* b, TV*& xout, double r
     }
   }
   if (dbg) cudaEventRecord(ev[1], st);
-  k_build_minv<B, TM, TV><<<gr, KB, 0, st>>>(nn, rp, dg, A, reinterpret_cast<TV*>(Minv));
-  k_init<TV, TB><<<gv, KB, 0, st>>>(n, b, x, r, rh, p, v, partials);
-  k_init_scalars<<<1, KB, 0, st>>>(sc, partials, gv, rtol, maxit);
-  count_launches(3);
-  OA_CUDA(cudaGetLastError());
-  // GCR(2) work vectors in the same buffers: x r z q P0 P1 Q0 Q1; the
-  // direction slots start at zero (no stored directions yet)
-  const bool use_gcr = gcr && B == 1;
-  TV *gz = rh, *gq = p, *gP[2] = {v, ph}, *gQ[2] = {sh, t};
-  if (use_gcr) {
-    if (check_every % 2) return fail(OA_ERR_ARG, "GCR: iteration chunks must hold an even number of iterations");
-    for (int k = 4; k < 8; ++k) OA_CUDA(cudaMemsetAsync(vec[k], 0, sizeof(TV) * (size_t)n, st));
-  }
-  // one chunk of check_every iterations; every kernel reads its scalars and
-  // the tolerance from device memory, so the chunk can be captured once
-  long long per_chunk = 0;
-  auto chunk = [&]() -> int {
-    const long long l0 = launch_total();
-    if (use_gcr) {
-      for (int it = 0; it < check_every; ++it) {
-        const int slot = it & 1;  // the older of the two stored directions
-        if (int s = precond(r, gz)) return s;
-        k_spmv_gcr<TM, TV><<<gv, KB, 0, st>>>(nn, rp, cols, A, gz, gq, gQ[0], gQ[1], partials, sc);
-        k_gcr_beta<<<1, KB, 0, st>>>(sc, partials, gv);
-        k_gcr_orth<TV><<<gv, KB, 0, st>>>(n, gz, gq, gP[0], gP[1], gQ[0], gQ[1], r, partials, sc);
-        k_gcr_alpha<<<1, KB, 0, st>>>(sc, partials, gv);
-        k_gcr_update<TV><<<gv, KB, 0, st>>>(n, x, r, gz, gq, gP[slot], gQ[slot], partials, sc);
-        k_gcr_end<<<1, KB, 0, st>>>(sc, partials, gv);
-      }
-      count_launches(6L * check_every);
-      per_chunk = launch_total() - l0;
-      OA_CUDA(cudaGetLastError());
-      return OA_OK;
-    }
-    for (int it = 0; it < check_every; ++it) {
-      k_p_update<TV><<<gfull, KB, 0, st>>>(n, p, r, v, sc);
-      if (int s = precond(p, ph)) return s;
-      k_spmv<B, TM, TV, 1><<<gv, KB, 0, st>>>(nn, rp, cols, A, ph, v, rh, nullptr, partials, sc);
-      k_alpha<<<1, KB, 0, st>>>(sc, partials, gv);
-      k_s_update<TV><<<gfull, KB, 0, st>>>(n, r, v, sc);
-      if (int s = precond(r, sh)) return s;
-      k_spmv<B, TM, TV, 2><<<gv, KB, 0, st>>>(nn, rp, cols, A, sh, t, r, nullptr, partials, sc);
-      k_omega<<<1, KB, 0, st>>>(sc, partials, gv);
-      k_x_update<TV><<<gv, KB, 0, st>>>(n, x, r, ph, sh, t, rh, partials, sc);
-      k_end_iter<<<1, KB, 0, st>>>(sc, partials, gv);
-    }
-    count_launches(8L * check_every);
-    per_chunk = launch_total() - l0;
-    OA_CUDA(cudaGetLastError());
-    return OA_OK;
-  };
+  if (int s = prologue<TB>(A, b, rtol, maxit, nullptr, nullptr, use_gcr)) return s;
   if (use_graph && (graph_exec == nullptr || graph_A != (const void*)A || graph_chunk != check_every ||
                     graph_amg != (const void*)amg || graph_gcr != use_gcr)) {
     if (graph_exec) cudaGraphExecDestroy(graph_exec);
     graph_exec = nullptr;
     cudaGraph_t g;
     OA_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-    const int cs = chunk();
+    const long long l0 = launch_total();
+    const int cs = chunk(A, check_every, use_gcr);
+    const long long per_chunk = launch_total() - l0;
     const cudaError_t ce = cudaStreamEndCapture(st, &g);
     if (cs) return cs;
     if (ce != cudaSuccess) return fail(OA_ERR_CUDA, std::string("Krylov chunk capture: ") + cudaGetErrorString(ce));
@@ -581,7 +593,7 @@ int KrylovSolver<B, TM, TV>::solve(const TM* A, const TB* b, TV*& xout, double r
     if (use_graph) {
       OA_CUDA(cudaGraphLaunch(graph_exec, st));
       count_launches(graph_launches);
-    } else if (int s = chunk()) {
+    } else if (int s = chunk(A, check_every, use_gcr)) {
       return s;
     }
     done_iters += check_every;
@@ -596,7 +608,7 @@ int KrylovSolver<B, TM, TV>::solve(const TM* A, const TB* b, TV*& xout, double r
   static_assert(sizeof(KScal) <= sizeof(hbuf), "host staging buffer too small");
   if (iters) *iters = h->iters;
   if (res) *res = h->bnorm > 0 ? h->rnorm / h->bnorm : 0.0;
-  xout = x;
+  xout = static_cast<TV*>(vec[0]);
   last_status = h->status;
   if (dbg) {
     cudaEventRecord(ev[2], st);
@@ -612,6 +624,33 @@ int KrylovSolver<B, TM, TV>::solve(const TM* A, const TB* b, TV*& xout, double r
   return OA_OK;
 }
 
+template <int B, class TM, class TV>
+template <class TB>
+int KrylovSolver<B, TM, TV>::emit(GraphBuild& gb, cudaGraph_t g, Deps& d, int body, const TM* A, const TB* b,
+                                  double rtol, int maxit, const double* rtol_dev, const int* maxit_dev, int maxit_cap,
+                                  int check_every, bool gcr_mode, int branch_body) {
+  const bool use_gcr = gcr_mode && B == 1;
+  if (use_gcr && check_every % 2) return fail(OA_ERR_ARG, "GCR: iteration chunks must hold an even number of iterations");
+  if (st != gb.st) return fail(OA_ERR_ARG, "Krylov graph: the solver's stream is not the capturing stream");
+  const int lb = gb.new_body();
+  if (lb < 0) return fail(OA_ERR_ARG, "Krylov graph: too many conditional bodies");
+  cudaGraphConditionalHandle h;
+  if (int s = gb.handle(g, &h)) return s;
+  if (int s = gb.seg(g, d, body, [&]() -> int {
+        if (int s2 = prologue<TB>(A, b, rtol, maxit, rtol_dev, maxit_dev, use_gcr)) return s2;
+        return launch_loop_enter(gb, h, scal, lb, branch_body);
+      }))
+    return s;
+  cudaGraph_t wb = nullptr;
+  if (int s = gb.cond(g, d, h, cudaGraphCondTypeWhile, 1, &wb)) return s;
+  Deps bd;
+  const int cap = (maxit_cap + check_every - 1) / check_every + 2;
+  return gb.seg(wb, bd, lb, [&]() -> int {
+    if (int s2 = chunk(A, check_every, use_gcr)) return s2;
+    return launch_loop_next(gb, h, scal, lb, cap);
+  });
+}
+
 template struct KrylovSolver<1, double, double>;
 template struct KrylovSolver<3, double, double>;
 template struct KrylovSolver<1, float, float>;
@@ -621,6 +660,14 @@ template int KrylovSolver<3, double, double>::solve<double>(const double*, const
 template int KrylovSolver<1, float, float>::solve<double>(const float*, const double*, float*&, double, int, int*, double*, int, bool);
 template int KrylovSolver<1, float, float>::solve<float>(const float*, const float*, float*&, double, int, int*, double*, int, bool);
 template int KrylovSolver<3, float, float>::solve<float>(const float*, const float*, float*&, double, int, int*, double*, int, bool);
+#define OA_EMIT(B, TM, TV, TB)                                                                                   \
+  template int KrylovSolver<B, TM, TV>::emit<TB>(GraphBuild&, cudaGraph_t, Deps&, int, const TM*, const TB*, double, \
+                                                 int, const double*, const int*, int, int, bool, int);
+OA_EMIT(1, double, double, double)
+OA_EMIT(3, double, double, double)
+OA_EMIT(1, float, float, float)
+OA_EMIT(3, float, float, float)
+#undef OA_EMIT
 
 // ---------------------------------------------------------------------------
 // FP64 residual for iterative refinement: r = b - A x (A in its stored
@@ -735,5 +782,56 @@ int add_correction(int n, double* x, const TV* d, cudaStream_t st) {
 }
 template int add_correction<float>(int, double*, const float*, cudaStream_t);
 template int add_correction<double>(int, double*, const double*, cudaStream_t);
+
+// ---------------------------------------------------------------------------
+// Control kernels of the conditional nodes of whole-iteration graphs (one
+// thread each; the condition is set by the graph that holds the node, or by
+// the node's own body).
+namespace {
+__global__ void k_set_if(cudaGraphConditionalHandle h, const int* flag, int negate) {
+  cudaGraphSetConditional(h, ((*flag != 0) != (negate != 0)) ? 1u : 0u);
+}
+__global__ void k_count_body(BodyCounters* c, int body) { c->total[body] += 1; }
+__global__ void k_loop_enter(cudaGraphConditionalHandle h, const KScal* sc, BodyCounters* c, int body,
+                             int branch_body) {
+  c->cur[body] = 0;
+  if (branch_body >= 0) c->total[branch_body] += 1;
+  cudaGraphSetConditional(h, sc->done ? 0u : 1u);
+}
+__global__ void k_loop_next(cudaGraphConditionalHandle h, const KScal* sc, BodyCounters* c, int body, int cap) {
+  const int n = ++c->cur[body];
+  c->total[body] += 1;
+  cudaGraphSetConditional(h, (!sc->done && n < cap) ? 1u : 0u);
+}
+}  // namespace
+
+int launch_set_if(GraphBuild& gb, cudaGraphConditionalHandle h, const int* flag, bool negate) {
+  k_set_if<<<1, 1, 0, gb.st>>>(h, flag, negate ? 1 : 0);
+  count_launches(1);
+  OA_CUDA(cudaGetLastError());
+  return OA_OK;
+}
+int launch_count_body(GraphBuild& gb, int body) {
+  k_count_body<<<1, 1, 0, gb.st>>>(gb.ctr, body);
+  count_launches(1);
+  OA_CUDA(cudaGetLastError());
+  return OA_OK;
+}
+int launch_loop_enter(GraphBuild& gb, cudaGraphConditionalHandle h, const void* kscal, int body, int branch_body) {
+  k_loop_enter<<<1, 1, 0, gb.st>>>(h, static_cast<const KScal*>(kscal), gb.ctr, body, branch_body);
+  count_launches(1);
+  OA_CUDA(cudaGetLastError());
+  return OA_OK;
+}
+int launch_loop_next(GraphBuild& gb, cudaGraphConditionalHandle h, const void* kscal, int body, int cap) {
+  k_loop_next<<<1, 1, 0, gb.st>>>(h, static_cast<const KScal*>(kscal), gb.ctr, body, cap);
+  count_launches(1);
+  OA_CUDA(cudaGetLastError());
+  return OA_OK;
+}
+int launch_counters_reset(GraphBuild& gb) {
+  OA_CUDA(cudaMemsetAsync(gb.ctr, 0, sizeof(BodyCounters), gb.st));
+  return OA_OK;
+}
 
 }  // namespace oa

@@ -3,8 +3,18 @@
 #include <cuda_runtime.h>
 
 #include "oa_amg.h"
+#include "oa_graph.h"
 
 namespace oa {
+
+// Device scalars of one Krylov solve (read by every iteration kernel).
+struct KScal {
+  double rho, alpha, omega, bnorm, rnorm;
+  double d0, d1, d2;  // reduced dots of the current phase
+  double rtol;
+  int maxit;
+  int done, iters, status;
+};
 
 // BiCGStab on a BSR matrix with BxB blocks; matrix values TM, vectors TV.
 template <int B, class TM, class TV>
@@ -47,6 +57,27 @@ struct KrylovSolver {
   // previous call (iterative-refinement passes)
   int solve(const TM* A, const TB* b, TV*& xout, double rtol, int maxit, int* iters, double* res,
             int check_every, bool reuse_precond = false);
+
+  // Graph form of solve() (whole-iteration graphs): its prologue (x = 0,
+  // r = b, device scalars; rtol and maxit read on the device when rtol_dev /
+  // maxit_dev are given) and a WHILE node over chunks of check_every
+  // iterations, captured into g after d. The preconditioner's numeric phase is
+  // left to the caller. gcr_mode: GCR(2) (scalar AMG systems) or BiCGStab.
+  // The loop is capped at maxit_cap / check_every + 2 passes on the device.
+  // branch_body >= 0: g is that IF body, counted once per execution here.
+  template <class TB>
+  int emit(GraphBuild& gb, cudaGraph_t g, Deps& d, int body, const TM* A, const TB* b, double rtol, int maxit,
+           const double* rtol_dev, const int* maxit_dev, int maxit_cap, int check_every, bool gcr_mode,
+           int branch_body);
+  const KScal* scalars() const { return static_cast<const KScal*>(scal); }
+  TV* solution() const { return static_cast<TV*>(vec[0]); }
+
+ private:
+  int precond(const TV* in, TV* out);
+  template <class TB>
+  int prologue(const TM* A, const TB* b, double rtol, int maxit, const double* rtol_dev, const int* maxit_dev,
+               bool use_gcr);
+  int chunk(const TM* A, int check_every, bool use_gcr);
 };
 
 // r = b - A x in FP64 arithmetic (A scalar CSR in its stored precision);

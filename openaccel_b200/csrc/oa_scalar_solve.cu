@@ -14,10 +14,92 @@
 
 namespace oa {
 
+constexpr int INNER_CAP = 300;  // FP32 Krylov iterations per refinement pass
+
 namespace {
 __global__ void k_narrow(int n, const double* __restrict__ a, float* __restrict__ b) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) b[i] = float(a[i]);
+}
+
+// ---- graph form: the host decisions of solve() as one-thread kernels ----
+
+// AMG numeric phase on every refresh-th solve (the counter persists across
+// graph launches)
+__global__ void k_refresh_if(cudaGraphConditionalHandle h, ScalarGraphState* S, int refresh) {
+  const int go = refresh <= 1 || (S->refresh_ctr % refresh) == 0;
+  S->refresh_ctr += 1;
+  cudaGraphSetConditional(h, go ? 1u : 0u);
+}
+
+// FP64: a GCR(2) solve that stagnated or broke down is redone by BiCGStab
+__global__ void k_fallback_if(cudaGraphConditionalHandle h, const KScal* sc, ScalarGraphState* S) {
+  const int fb = sc->status == 1;
+  S->fallback = fb;
+  S->spent = fb ? sc->iters : 0;
+  cudaGraphSetConditional(h, fb ? 1u : 0u);
+}
+
+// mixed: entry of the refinement loop (||b|| from the reduction before it)
+__global__ void k_ir_begin(cudaGraphConditionalHandle h, ScalarGraphState* S, double rtol, int maxit, double floor,
+                           int use_gcr) {
+  const double bn = sqrt(S->bsq);
+  S->bnorm = bn;
+  S->rtol = rtol;
+  S->maxit = maxit;
+  S->floor = floor;
+  S->use_gcr = use_gcr;
+  S->total = 0;
+  S->nref = 0;
+  S->fallback = 0;
+  S->it_last = 0;
+  S->apply = 0;
+  S->spent = 0;
+  S->status = bn < INFINITY ? 0 : 3;  // 3: non-finite right-hand side
+  S->rel = bn > 0 ? 1.0 : 0.0;
+  cudaGraphSetConditional(h, (S->status == 0 && S->rel > rtol && maxit > 0) ? 1u : 0u);
+}
+
+// inner tolerance and iteration budget of a pass; selects GCR(2) or BiCGStab
+__global__ void k_ir_params(cudaGraphConditionalHandle hsel, ScalarGraphState* S) {
+  const double inner = fmax(S->rtol / S->rel, S->floor);
+  S->inner_rtol = fmin(inner, 0.1);
+  S->inner_maxit = min(INNER_CAP, S->maxit - S->total);
+  cudaGraphSetConditional(hsel, S->use_gcr ? 1u : 0u);
+}
+
+// after the inner solve: iteration count, the switch to BiCGStab for a GCR(2)
+// stall far from its target, and whether the correction is applied
+__global__ void k_ir_after(ScalarGraphState* S, const KScal* sc) {
+  const int it = sc->iters;
+  const double r_in = sc->bnorm > 0 ? sc->rnorm / sc->bnorm : 0.0;
+  S->it_last = it;
+  S->r_in = r_in;
+  S->total += it;
+  if (S->use_gcr && sc->status == 1 && r_in > 10.0 * S->inner_rtol) {
+    S->use_gcr = 0;
+    S->fallback += 1;
+  }
+  if (sc->status == 2 && S->status == 0) S->status = 4;  // 4: non-finite inner residual
+  S->apply = (sc->status != 3 && r_in < 1.0) ? 1 : 0;
+}
+
+template <class TV>
+__global__ void k_add_correction_if(int n, double* x, const TV* d, const ScalarGraphState* S) {
+  if (!S->apply) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) x[i] += double(d[i]);
+}
+
+// end of a pass: relative FP64 residual, loop condition
+__global__ void k_ir_next(cudaGraphConditionalHandle h, ScalarGraphState* S, BodyCounters* c, int body) {
+  c->total[body] += 1;
+  const double rel = S->bnorm > 0 ? S->rnorm_out / S->bnorm : 0.0;
+  S->rel = rel;
+  S->nref += 1;
+  if (!(rel < INFINITY) && S->status == 0) S->status = 2;
+  const bool go = S->status == 0 && rel > S->rtol && S->total < S->maxit && S->nref < 40 && S->it_last != 0;
+  cudaGraphSetConditional(h, go ? 1u : 0u);
 }
 }  // namespace
 
@@ -41,6 +123,12 @@ int ScalarSolve::init(int nn) {
 }
 
 void ScalarSolve::release() {
+  if (gs) cudaFree(gs);
+  if (gs_host) cudaFreeHost(gs_host);
+  if (k_host) cudaFreeHost(k_host);
+  gs = nullptr;
+  gs_host = nullptr;
+  k_host = nullptr;
   if (r) cudaFree(r);
   if (r32) cudaFree(r32);
   if (scal) cudaFree(scal);
@@ -111,7 +199,6 @@ int ScalarSolve::solve(const ScalarGraph& g, bool mixed, bool amg, bool graphs, 
   int total = 0, nref = 0;
   double rel = bnorm > 0 ? 1.0 : 0.0;
   OA_CUDA(cudaMemcpyAsync(r, b, sizeof(double) * g.nn, cudaMemcpyDeviceToDevice, st));
-  constexpr int INNER_CAP = 300;  // FP32 Krylov iterations per refinement
   while (rel > rtol && total < maxit && nref < 40) {
     k_narrow<<<(g.nn + 255) / 256, 256, 0, st>>>(g.nn, r, r32);
     count_launches(1);
@@ -151,6 +238,186 @@ int ScalarSolve::solve(const ScalarGraph& g, bool mixed, bool amg, bool graphs, 
   if (iters) *iters = total;
   if (res) *res = rel;
   if (refinements) *refinements = nref;
+  return OA_OK;
+}
+
+int ScalarSolve::emit(GraphBuild& gb, cudaGraph_t g, Deps& d, const ScalarGraph& gr, bool mixed, bool amg,
+                      const void* A, const double* b, double* x, double rtol, int maxit, cudaStream_t st) {
+  if (int s = init(gr.nn)) return s;
+  if (amg && !(mixed ? amg32.ready : amg64.ready))
+    return fail(OA_ERR_NOT_READY, "scalar solve graph: the preconditioner is set up by a first eager solve");
+  if (!gs) {
+    if (cudaMalloc(&gs, sizeof(ScalarGraphState)) != cudaSuccess ||
+        cudaMallocHost(&gs_host, sizeof(ScalarGraphState)) != cudaSuccess ||
+        cudaMallocHost(&k_host, sizeof(KScal)) != cudaSuccess)
+      return fail(OA_ERR_CUDA, "scalar solve graph: allocation failed");
+    OA_CUDA(cudaMemsetAsync(gs, 0, sizeof(ScalarGraphState), st));
+  }
+  k64.amg = amg && !mixed ? &amg64 : nullptr;
+  k32.amg = amg && mixed ? &amg32 : nullptr;
+  if (mixed) {
+    if (int s = k32.setup(gr.nn, gr.rp, gr.cols, gr.diag, st)) return s;
+  } else if (int s = k64.setup(gr.nn, gr.rp, gr.cols, gr.diag, st)) {
+    return s;
+  }
+  const bool use_gcr = amg && gcr;
+  const int chunk_gcr = gcr_chunk;
+  // AMG numeric phase under the refresh IF
+  if (amg) {
+    cudaGraphConditionalHandle hn;
+    if (int s = gb.handle(g, &hn)) return s;
+    if (int s = gb.seg(g, d, -1, [&]() -> int {
+          k_refresh_if<<<1, 1, 0, st>>>(hn, gs, refresh);
+          count_launches(1);
+          return OA_OK;
+        }))
+      return s;
+    cudaGraph_t nb = nullptr;
+    if (int s = gb.cond(g, d, hn, cudaGraphCondTypeIf, 1, &nb)) return s;
+    const int bid = gb.new_body();
+    if (bid < 0) return fail(OA_ERR_ARG, "scalar solve graph: too many conditional bodies");
+    Deps nd;
+    if (int s = gb.seg(nb, nd, bid, [&]() -> int {
+          if (int s2 = launch_count_body(gb, bid)) return s2;
+          return mixed ? amg32.numeric(static_cast<const float*>(A), st)
+                       : amg64.numeric(static_cast<const double*>(A), st);
+        }))
+      return s;
+  }
+  if (!mixed) {
+    const double* A64 = static_cast<const double*>(A);
+    if (int s = k64.emit<double>(gb, g, d, -1, A64, b, rtol, maxit, nullptr, nullptr, maxit,
+                                 use_gcr ? chunk_gcr : (amg ? 5 : 20), use_gcr, -1))
+      return s;
+    if (use_gcr) {
+      // the BiCGStab fallback of a stagnated GCR(2) solve
+      cudaGraphConditionalHandle hf;
+      if (int s = gb.handle(g, &hf)) return s;
+      if (int s = gb.seg(g, d, -1, [&]() -> int {
+            k_fallback_if<<<1, 1, 0, st>>>(hf, k64.scalars(), gs);
+            count_launches(1);
+            return OA_OK;
+          }))
+        return s;
+      cudaGraph_t fb = nullptr;
+      if (int s = gb.cond(g, d, hf, cudaGraphCondTypeIf, 1, &fb)) return s;
+      const int bid = gb.new_body();
+      if (bid < 0) return fail(OA_ERR_ARG, "scalar solve graph: too many conditional bodies");
+      Deps fd;
+      if (int s = k64.emit<double>(gb, fb, fd, bid, A64, b, rtol, maxit, nullptr, nullptr, maxit, 5, false, bid))
+        return s;
+    } else {
+      if (int s = gb.seg(g, d, -1, [&]() -> int {
+            OA_CUDA(cudaMemsetAsync(&gs->fallback, 0, sizeof(int), st));
+            OA_CUDA(cudaMemsetAsync(&gs->spent, 0, sizeof(int), st));
+            return OA_OK;
+          }))
+        return s;
+    }
+    return gb.seg(g, d, -1, [&]() -> int {
+      OA_CUDA(cudaMemcpyAsync(x, k64.solution(), sizeof(double) * gr.nn, cudaMemcpyDeviceToDevice, st));
+      OA_CUDA(cudaMemcpyAsync(k_host, k64.scalars(), sizeof(KScal), cudaMemcpyDeviceToHost, st));
+      OA_CUDA(cudaMemcpyAsync(gs_host, gs, sizeof(ScalarGraphState), cudaMemcpyDeviceToHost, st));
+      return OA_OK;
+    });
+  }
+  // mixed: FP64 iterative refinement around FP32 inner solves
+  const float* A32 = static_cast<const float*>(A);
+  const double floor = inner_floor > 0 ? inner_floor : (amg ? 1e-4 : 2e-4);
+  cudaGraphConditionalHandle hir;
+  if (int s = gb.handle(g, &hir)) return s;
+  if (int s = gb.seg(g, d, -1, [&]() -> int {
+        OA_CUDA(cudaMemsetAsync(x, 0, sizeof(double) * gr.nn, st));
+        if (int s2 = device_sumsq(gr.nn, b, &gs->bsq, partials, st)) return s2;
+        OA_CUDA(cudaMemcpyAsync(r, b, sizeof(double) * gr.nn, cudaMemcpyDeviceToDevice, st));
+        k_ir_begin<<<1, 1, 0, st>>>(hir, gs, rtol, maxit, floor, use_gcr ? 1 : 0);
+        count_launches(1);
+        return OA_OK;
+      }))
+    return s;
+  cudaGraph_t irb = nullptr;
+  if (int s = gb.cond(g, d, hir, cudaGraphCondTypeWhile, 1, &irb)) return s;
+  const int ir_body = gb.new_body();
+  if (ir_body < 0) return fail(OA_ERR_ARG, "scalar solve graph: too many conditional bodies");
+  Deps bd;
+  cudaGraphConditionalHandle hsel;
+  if (int s = gb.handle(irb, &hsel)) return s;
+  if (int s = gb.seg(irb, bd, ir_body, [&]() -> int {
+        k_narrow<<<(gr.nn + 255) / 256, 256, 0, st>>>(gr.nn, r, r32);
+        k_ir_params<<<1, 1, 0, st>>>(hsel, gs);
+        count_launches(2);
+        return OA_OK;
+      }))
+    return s;
+  // GCR(2) while the solve has not fallen back, else BiCGStab
+  cudaGraph_t sel[2] = {nullptr, nullptr};
+  if (int s = gb.cond(irb, bd, hsel, cudaGraphCondTypeIf, 2, sel)) return s;
+  const int b_gcr = gb.new_body(), b_bicg = gb.new_body();
+  if (b_gcr < 0 || b_bicg < 0) return fail(OA_ERR_ARG, "scalar solve graph: too many conditional bodies");
+  {
+    Deps d0, d1;
+    if (int s = k32.emit<float>(gb, sel[0], d0, b_gcr, A32, r32, 0.0, 0, &gs->inner_rtol, &gs->inner_maxit, INNER_CAP,
+                                chunk_gcr, true, b_gcr))
+      return s;
+    if (int s = k32.emit<float>(gb, sel[1], d1, b_bicg, A32, r32, 0.0, 0, &gs->inner_rtol, &gs->inner_maxit,
+                                INNER_CAP, 5, false, b_bicg))
+      return s;
+  }
+  if (int s = gb.seg(irb, bd, ir_body, [&]() -> int {
+        k_ir_after<<<1, 1, 0, st>>>(gs, k32.scalars());
+        k_add_correction_if<float><<<(gr.nn + 255) / 256, 256, 0, st>>>(gr.nn, x, k32.solution(), gs);
+        count_launches(2);
+        if (int s2 = fp64_residual<float>(gr.nn, gr.rp, gr.cols, A32, x, b, r, k32.partials, &gs->rnorm_out, st))
+          return s2;
+        k_ir_next<<<1, 1, 0, st>>>(hir, gs, gb.ctr, ir_body);
+        count_launches(1);
+        return OA_OK;
+      }))
+    return s;
+  return gb.seg(g, d, -1, [&]() -> int {
+    OA_CUDA(cudaMemcpyAsync(gs_host, gs, sizeof(ScalarGraphState), cudaMemcpyDeviceToHost, st));
+    return OA_OK;
+  });
+}
+
+int ScalarSolve::graph_prepare(cudaStream_t st) {
+  if (!gs) return fail(OA_ERR_NOT_READY, "scalar solve graph: not captured");
+  gs_host->refresh_ctr = (int)solves;
+  OA_CUDA(cudaMemcpyAsync(&gs->refresh_ctr, &gs_host->refresh_ctr, sizeof(int), cudaMemcpyHostToDevice, st));
+  return OA_OK;
+}
+
+int ScalarSolve::graph_result(bool mixed, int* iters, double* res, int* refinements, bool* recapture,
+                              const char* what) {
+  const ScalarGraphState& S = *gs_host;
+  ++solves;  // the device refresh counter advanced once
+  if (recapture) *recapture = false;
+  if (mixed) {
+    if (S.fallback) {
+      gcr = false;
+      k32.gcr = false;
+      fallbacks += S.fallback;
+      if (recapture) *recapture = true;
+    }
+    if (S.status == 3) return fail(OA_ERR_SOLVER, std::string(what) + ": non-finite right-hand side");
+    if (S.status == 2) return fail(OA_ERR_SOLVER, std::string(what) + " refinement: non-finite residual");
+    if (S.status == 4) return fail(OA_ERR_SOLVER, std::string(what) + ": non-finite residual in an inner solve");
+    if (iters) *iters = S.total;
+    if (res) *res = S.rel;
+    if (refinements) *refinements = S.nref;
+    return OA_OK;
+  }
+  const KScal& K = *k_host;
+  if (S.fallback) {
+    gcr = false;
+    k64.gcr = false;
+    ++fallbacks;
+    if (recapture) *recapture = true;
+  }
+  if (K.status == 2) return fail(OA_ERR_SOLVER, std::string(what) + ": non-finite residual");
+  if (iters) *iters = K.iters + S.spent;
+  if (res) *res = K.bnorm > 0 ? K.rnorm / K.bnorm : 0.0;
+  if (refinements) *refinements = 0;
   return OA_OK;
 }
 

@@ -16,6 +16,14 @@ struct ScalarGraph {
   const int *h_rp = nullptr, *h_cols = nullptr, *h_diag = nullptr;
 };
 
+// Device state of a graph-captured scalar solve: the refinement loop of the
+// mixed form, the AMG refresh counter and the fallback bookkeeping.
+struct ScalarGraphState {
+  double bsq, bnorm, rel, rtol, floor, inner_rtol, r_in, rnorm_out;
+  int maxit, total, nref, inner_maxit, use_gcr, fallback, status, it_last, apply;
+  int refresh_ctr, refresh, spent;
+};
+
 // FP64: BiCGStab (AMG- or Jacobi-preconditioned) to rtol. Mixed: iterative
 // refinement with the FP64 residual r = b - A x (A in its stored FP32 values),
 // FP32 BiCGStab on A d = r to a loose inner tolerance, x += d, until
@@ -59,11 +67,28 @@ struct ScalarSolve {
   // precision); reported so callers can see the switch happen
   int fallbacks = 0;
 
+  // graph form (whole-iteration graphs)
+  ScalarGraphState* gs = nullptr;       // device
+  ScalarGraphState* gs_host = nullptr;  // pinned mirror, written by the graph's last nodes
+  KScal* k_host = nullptr;              // pinned mirror of the FP64 solver's scalars
+
   int init(int n);
   // A: const double* (mixed = false) or const float* (mixed = true); b and x
   // FP64 device vectors of g.nn; x is overwritten. refinements may be null.
   int solve(const ScalarGraph& g, bool mixed, bool amg, bool graphs, const void* A, const double* b, double* x,
             double rtol, int maxit, int* iters, double* res, int* refinements, cudaStream_t st, const char* what);
+  // Graph form of solve(): the same steps with every host decision moved to
+  // the device (refresh IF, Krylov WHILE loops, the BiCGStab fallback IF, the
+  // refinement WHILE loop), captured into g after d on the stream st. The
+  // preconditioner must have been set up by an earlier solve(). After the
+  // graph ran, graph_result() reads the outcome from the pinned mirrors;
+  // *recapture is set when the solve switched to BiCGStab for good.
+  int emit(GraphBuild& gb, cudaGraph_t g, Deps& d, const ScalarGraph& gr, bool mixed, bool amg, const void* A,
+           const double* b, double* x, double rtol, int maxit, cudaStream_t st);
+  int graph_result(bool mixed, int* iters, double* res, int* refinements, bool* recapture, const char* what);
+  // before each launch of a graph holding emit()'s nodes: the device refresh
+  // counter takes the host's solve count (which a caller may have reset)
+  int graph_prepare(cudaStream_t st);
   void release();
   ~ScalarSolve() { release(); }
 };

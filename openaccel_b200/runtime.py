@@ -19,6 +19,8 @@ OA_TOPO_HEX8 = 8
 OA_TOPO_TET4 = 4
 OA_PREC_FP64 = 0
 OA_PREC_MIXED = 1
+OA_TIME_BDF1 = 1
+OA_TIME_BDF2 = 2
 OA_STATIC_SOLVE_MAX_ROWS = 131072
 
 # every symbol the header declares; checked by tests on CPU
