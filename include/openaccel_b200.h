@@ -125,10 +125,12 @@ const char* oa_version(void);
  * hex8: elements whose corner numbering starts at another corner or axis than
  * their neighbours' are relabelled by a proper cube rotation (the geometry and
  * Jacobian sign do not change) so that the mesh is a consistently oriented
- * block; a hex mesh that admits no such labelling (not block-structured, e.g.
- * three or five elements around an interior edge) is rejected with
- * OA_ERR_MESH. Element fields ("mDot") are exchanged in the caller's
- * labelling. */
+ * block. A hex mesh that admits no such labelling (three or five elements
+ * around an interior edge, as where blocks of a multi-block mesh meet) keeps
+ * the caller's labelling and its row kernels take each node's incident
+ * elements from a list (up to 16 per node; more is OA_ERR_MESH, as is a face
+ * shared by three elements). Element fields ("mDot") are exchanged in the
+ * caller's labelling. */
 int oa_mesh_create(const double* coords, int nn, const int* conn, int ne, int topo,
                    const int* face_elem, const int* face_ord, const int* face_bnd, int nf,
                    oa_mesh** out);

@@ -512,6 +512,8 @@ int oa_mesh_create(const double* coords, int nn, const int* conn, int ne, int to
   std::vector<uint8_t> rot;
   std::vector<int> oface(face_ord, face_ord + nf);
   bool consistent = true;
+  bool general = false;  // not a consistently oriented block: incident-list lanes
+  if (ne > (1 << 28)) return fail(OA_ERR_MESH, "oa_mesh_create: more than 2^28 elements");
   {
     std::vector<uint8_t> seen(8L * nn, 0);
     for (long k = 0; k < 8L * ne && consistent; ++k) {
@@ -522,12 +524,17 @@ int oa_mesh_create(const double* coords, int nn, const int* conn, int ne, int to
   }
   if (!consistent) {  // only meshes that need it pay for the face walk
     std::string why;
-    if (!hexorient::orient(nn, ne, conn, oconn, rot, &why))
-      return fail(OA_ERR_MESH, "oa_mesh_create: the hex mesh is not a block-structured mesh the row kernels accept (" +
-                                   why + ")");
-    for (int f = 0; f < nf; ++f) oface[f] = hexorient::face_map(rot[face_elem[f]], face_ord[f]);
-    conn = oconn.data();
-    face_ord = oface.data();
+    bool invalid = false;
+    if (hexorient::orient(nn, ne, conn, oconn, rot, &why, &invalid)) {
+      for (int f = 0; f < nf; ++f) oface[f] = hexorient::face_map(rot[face_elem[f]], face_ord[f]);
+      conn = oconn.data();
+      face_ord = oface.data();
+    } else if (invalid) {
+      return fail(OA_ERR_MESH, "oa_mesh_create: invalid hex mesh (" + why + ")");
+    } else {
+      general = true;  // the caller's labelling, incident-list lanes
+      rot.clear();
+    }
   }
   oa_mesh* M = new oa_mesh();
   DeviceMesh& m = M->m;
@@ -535,19 +542,40 @@ int oa_mesh_create(const double* coords, int nn, const int* conn, int ne, int to
   m.nn = nn;
   m.ne = ne;
   m.nf = nf;
-  // node -> element-by-corner table
-  std::vector<int> n2e(8L * nn, -1);
-  for (int e = 0; e < ne; ++e)
-    for (int a = 0; a < 8; ++a) {
-      int& slot = n2e[8L * conn[8L * e + a] + a];
-      if (slot != -1) {
-        delete M;
-        return fail(OA_ERR_MESH,
-                    "oa_mesh_create: a node is the same local corner of two elements; the row-owner kernels "
-                    "need a consistently oriented hex block");
+  // node -> incident (element, corner) table, lpr entries per node:
+  // entry c = the element where the node is corner c on a block mesh, the
+  // incident elements in element order otherwise
+  int lpr = 8;
+  std::vector<int> n2e;
+  if (!general) {
+    n2e.assign(8L * nn, -1);
+    for (int e = 0; e < ne; ++e)
+      for (int a = 0; a < 8; ++a) {
+        int& slot = n2e[8L * conn[8L * e + a] + a];
+        if (slot != -1) {
+          delete M;
+          return fail(OA_ERR_MESH, "oa_mesh_create: a node is the same local corner of two elements");
+        }
+        slot = 8 * e + a;
       }
-      slot = e;
+  } else {
+    std::vector<int> inc(nn, 0);
+    int most = 0;
+    for (long k = 0; k < 8L * ne; ++k) most = std::max(most, ++inc[conn[k]]);
+    if (most > 16) {
+      delete M;
+      return fail(OA_ERR_MESH, "oa_mesh_create: a node with more than 16 incident hex elements");
     }
+    lpr = most <= 8 ? 8 : 16;
+    n2e.assign((size_t)lpr * nn, -1);
+    std::fill(inc.begin(), inc.end(), 0);
+    for (int e = 0; e < ne; ++e)
+      for (int a = 0; a < 8; ++a) {
+        const int nd = conn[8L * e + a];
+        n2e[(size_t)lpr * nd + inc[nd]++] = 8 * e + a;
+      }
+  }
+  m.lpr = lpr;
   // reduced-stencil graph: row i = {i} U {j : (i,j) is an SCS L/R pair}
   std::vector<int> cnt(nn + 1, 0);
   for (int e = 0; e < ne; ++e)
@@ -583,13 +611,14 @@ int oa_mesh_create(const double* coords, int nn, const int* conn, int ne, int to
   // slot maps of the row write-out: which corner-lane neighbour blocks sum
   // into each off-diagonal CSR entry (a row's lanes then add them in bit
   // order, the same ascending (lane, neighbour) order as a search would)
-  std::vector<uint32_t> smask(m.nnz, 0u);
+  std::vector<unsigned long long> smask(m.nnz, 0ull);
   for (int i = 0; i < nn; ++i) {
     const int* rb = m.h_cols.data() + m.h_row_ptr[i];
     const int* re = m.h_cols.data() + m.h_row_ptr[i + 1];
-    for (int c = 0; c < 8; ++c) {
-      const int e = n2e[8L * i + c];
-      if (e < 0) continue;
+    for (int l = 0; l < lpr; ++l) {
+      const int ec = n2e[(size_t)lpr * i + l];
+      if (ec < 0) continue;
+      const int e = ec >> 3, c = ec & 7;
       for (int k = 0; k < 3; ++k) {
         const int j = conn[8L * e + edge_nbr(c, k)];
         const int* q = std::lower_bound(rb, re, j);
@@ -597,10 +626,12 @@ int oa_mesh_create(const double* coords, int nn, const int* conn, int ne, int to
           delete M;
           return fail(OA_ERR_MESH, "oa_mesh_create: an element edge is missing from the stencil graph");
         }
-        smask[q - m.h_cols.data()] |= 1u << (3 * c + k);
+        smask[q - m.h_cols.data()] |= 1ull << (3 * l + k);
       }
     }
   }
+  std::vector<uint32_t> smask32;
+  if (lpr == 8) smask32.assign(smask.begin(), smask.end());
   {
     // mean element edge length (the 12 edges are the SCS L/R pairs)
     double sum = 0.0;
@@ -624,9 +655,9 @@ int oa_mesh_create(const double* coords, int nn, const int* conn, int ne, int to
     for (int k = 0; k < 4; ++k) wall[conn[8L * face_elem[f] + FN[face_ord[f]][k]]] = 1;
   }
   int st = OA_OK;
-  if ((st = dalloc(&m.x, 3L * nn)) || (st = dalloc(&m.conn, 8L * ne)) || (st = dalloc(&m.n2e, 8L * nn)) ||
+  if ((st = dalloc(&m.x, 3L * nn)) || (st = dalloc(&m.conn, 8L * ne)) || (st = dalloc(&m.n2e, (size_t)lpr * nn)) ||
       (st = dalloc(&m.row_ptr, nn + 1L)) || (st = dalloc(&m.cols, (size_t)m.nnz)) || (st = dalloc(&m.diag, (size_t)nn)) ||
-      (st = dalloc(&m.slot_mask, (size_t)m.nnz)) ||
+      (lpr == 8 ? (st = dalloc(&m.slot_mask, (size_t)m.nnz)) : (st = dalloc(&m.slot_mask64, (size_t)m.nnz))) ||
       (st = dalloc(&m.face_mask, (size_t)ne)) || (st = dalloc(&m.vol, (size_t)nn)) || (st = dalloc(&m.wscv, 8L * ne)) ||
       (st = dalloc(&m.scs_area, 36L * ne)) ||
       (st = dalloc(&m.wall_node, (size_t)nn))) {
@@ -636,11 +667,12 @@ int oa_mesh_create(const double* coords, int nn, const int* conn, int ne, int to
   cudaStreamCreateWithFlags(&M->st, cudaStreamNonBlocking);
   cudaMemcpy(m.x, coords, sizeof(double) * 3 * nn, cudaMemcpyHostToDevice);
   cudaMemcpy(m.conn, conn, sizeof(int) * 8 * ne, cudaMemcpyHostToDevice);
-  cudaMemcpy(m.n2e, n2e.data(), sizeof(int) * 8 * nn, cudaMemcpyHostToDevice);
+  cudaMemcpy(m.n2e, n2e.data(), sizeof(int) * n2e.size(), cudaMemcpyHostToDevice);
   cudaMemcpy(m.row_ptr, m.h_row_ptr.data(), sizeof(int) * (nn + 1), cudaMemcpyHostToDevice);
   cudaMemcpy(m.cols, m.h_cols.data(), sizeof(int) * m.nnz, cudaMemcpyHostToDevice);
   cudaMemcpy(m.diag, m.h_diag.data(), sizeof(int) * nn, cudaMemcpyHostToDevice);
-  cudaMemcpy(m.slot_mask, smask.data(), sizeof(uint32_t) * m.nnz, cudaMemcpyHostToDevice);
+  if (lpr == 8) cudaMemcpy(m.slot_mask, smask32.data(), sizeof(uint32_t) * m.nnz, cudaMemcpyHostToDevice);
+  else cudaMemcpy(m.slot_mask64, smask.data(), sizeof(unsigned long long) * m.nnz, cudaMemcpyHostToDevice);
   cudaMemcpy(m.face_mask, fmask.data(), ne, cudaMemcpyHostToDevice);
   cudaMemcpy(m.wall_node, wall.data(), sizeof(int) * nn, cudaMemcpyHostToDevice);
   cudaError_t ce = cudaDeviceSynchronize();
@@ -662,7 +694,7 @@ void oa_mesh_destroy(oa_mesh* M) {
   DeviceMesh& m = M->m;
   void* ptrs[] = {m.x,       m.conn,      m.n2e,      m.n2e_ptr,  m.n2f,       m.n2f_ptr, m.face_elem, m.face_ord,
                   m.face_bnd, m.row_ptr, m.cols,     m.diag,     m.face_mask, m.vol,     m.wscv,      m.wall_node,
-                  m.scs_area, m.slot_mask};
+                  m.scs_area, m.slot_mask, m.slot_mask64};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (M->st) cudaStreamDestroy(M->st);

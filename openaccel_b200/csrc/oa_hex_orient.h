@@ -12,8 +12,8 @@
 // shared faces fixes the rotation of each element from an already oriented
 // neighbour, whose face is the opposite face of the neighbour's (same
 // positions in the other two axes). A mesh where two walks disagree is not a
-// block (for instance a node where 3 or 5 elements meet around an edge) and
-// is rejected.
+// block (for instance a node where 3 or 5 elements meet around an edge): the
+// row kernels then run with 16 lanes per row on the caller's labelling.
 #pragma once
 #include <algorithm>
 #include <array>
@@ -109,9 +109,12 @@ inline int face_map(int r, int f) {
 
 // Orient every element. conn [ne][8] in, out_conn / rot [ne] out (rot = index
 // into rotations(), 0 = unchanged). Returns false with a reason when the mesh
-// is not a consistently orientable block.
+// is not a consistently orientable block; *invalid (when given) is then set if
+// the mesh is not a valid hex mesh at all (a face shared by three elements)
+// rather than only not a block.
 inline bool orient(int nn, int ne, const int* conn, std::vector<int>& out_conn, std::vector<uint8_t>& rot,
-                   std::string* why) {
+                   std::string* why, bool* invalid = nullptr) {
+  if (invalid) *invalid = false;
   const auto& R = rotations();
   out_conn.assign(conn, conn + 8L * ne);
   rot.assign(ne, 0);
@@ -128,6 +131,7 @@ inline bool orient(int nn, int ne, const int* conn, std::vector<int>& out_conn, 
   for (auto& kv : faces)
     if (kv.second.size() > 2) {
       if (why) *why = "a face is shared by more than two elements";
+      if (invalid) *invalid = true;
       return false;
     }
   std::vector<int> queue;

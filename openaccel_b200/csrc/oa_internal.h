@@ -13,7 +13,9 @@ namespace oa {
 // Device-resident mesh: connectivity, node -> incident-element table,
 // reduced-stencil CSR graph, wall faces and static FP64 geometry.
 // POD view of the device arrays, passed to kernels by value.
-//   hex8: n2e is [nn][8], the element where the node is corner c (or -1).
+//   hex8: n2e is [nn][lpr]: element * 8 + corner of the node's incident
+//         elements (or -1); on block meshes entry c is the element where the
+//         node is corner c.
 //   tet4: n2e[n2e_ptr[i] .. n2e_ptr[i+1]) lists 4*element + corner for every
 //         element incident to node i, by ascending element; n2f likewise
 //         lists 4*face + k for every boundary face whose side node k is i.
@@ -34,6 +36,11 @@ struct MeshView {
   // hex8: per off-diagonal CSR entry, the row's corner-lane contributions that
   // land in it: bit 3c + k is lane c's edge neighbour k (edge_nbr order)
   uint32_t* slot_mask = nullptr;  // [nnz]
+  // the same with 16 lanes per row (meshes that are not consistently
+  // oriented blocks; bit 3 lane + neighbour)
+  unsigned long long* slot_mask64 = nullptr;  // [nnz]
+  // hex8 lanes per row: 8 (block mesh, lane = corner) or 16 (general)
+  int lpr = 8;
   uint8_t* face_mask = nullptr;  // [ne] bit f: face f is a no-slip wall face
   double* vol = nullptr;       // [nn] dual nodal volume
   double* wscv = nullptr;      // [ne][8] SCV volume fractions (hex8)

@@ -112,14 +112,12 @@ __global__ void __launch_bounds__(BLOCK) k_scv(GeoArgs a) {
 
 // Row kernel: dual nodal volume = sum of incident SCV volumes
 // (mesh::updateDualNodalVolumeField_).
+template <int LPR>
 __global__ void __launch_bounds__(BLOCK) k_dual_volume(GeoArgs a) {
-  const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 3;
-  const int c = threadIdx.x & 7;
-  const bool rv = row < a.m.nn;
-  const int e = rv ? a.m.n2e[8 * row + c] : -1;
-  double v = (e >= 0) ? a.scv[8 * e + c] : 0.0;
-  v = rowsum8(v);
-  if (rv && c == 0) a.m.vol[row] = v;
+  const RowLane<LPR> rl = row_lane<LPR>(a.m);
+  double v = (rl.e >= 0) ? a.scv[8 * rl.e + rl.c] : 0.0;
+  v = rowsum<LPR>(v);
+  if (rl.rv && rl.li == 0) a.m.vol[rl.row] = v;
 }
 
 int launch_scs_area(DeviceMesh& m, cudaStream_t st);
@@ -131,7 +129,9 @@ int launch_geometry(DeviceMesh& m, cudaStream_t st) {
   OA_CUDA(cudaMallocAsync(&a.err, sizeof(int), st));
   OA_CUDA(cudaMemsetAsync(a.err, 0, sizeof(int), st));
   k_scv<<<(m.ne + BLOCK - 1) / BLOCK, BLOCK, 0, st>>>(a);
-  k_dual_volume<<<(int)(((size_t)m.nn * 8 + BLOCK - 1) / BLOCK), BLOCK, 0, st>>>(a);
+  const unsigned gdv = (unsigned)(((size_t)m.nn * m.lpr + BLOCK - 1) / BLOCK);
+  if (m.lpr == 16) k_dual_volume<16><<<gdv, BLOCK, 0, st>>>(a);
+  else k_dual_volume<8><<<gdv, BLOCK, 0, st>>>(a);
   OA_CUDA(cudaGetLastError());
   int herr = 0;
   OA_CUDA(cudaMemcpyAsync(&herr, a.err, sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -148,8 +148,8 @@ int launch_geometry(DeviceMesh& m, cudaStream_t st) {
 // three edge-neighbour blocks; lane s of the row then emits CSR slot s (s,
 // s+8, ...), summing the blocks its precomputed slot mask names in ascending
 // (lane, neighbour) order. The diagonal block is already reduced in every lane.
-template <int B, class TM>
-__device__ __forceinline__ void write_row(int row, bool rv, int c, int lane, const TM (&diag)[B],
+template <int B, class TM, int LPR>
+__device__ __forceinline__ void write_row(int row, bool rv, int li, int lane, const TM (&diag)[B],
                                           const TM (&nb)[3][B], const MeshView& m, TM* __restrict__ A,
                                           TM* sh_val, bool offdiag_zero) {
 #pragma unroll
@@ -161,8 +161,8 @@ __device__ __forceinline__ void write_row(int row, bool rv, int c, int lane, con
     const int rp = __ldg(m.row_ptr + row);
     const int len = __ldg(m.row_ptr + row + 1) - rp;
     const int dof = __ldg(m.diag + row);
-    const TM* row_vals = sh_val + (lane & ~7) * 3 * B;
-    for (int s = c; s < len; s += 8) {
+    const TM* row_vals = sh_val + (lane & ~(LPR - 1)) * 3 * B;
+    for (int s = li; s < len; s += LPR) {
       TM out[B];
       if (s == dof) {
 #pragma unroll
@@ -170,9 +170,10 @@ __device__ __forceinline__ void write_row(int row, bool rv, int c, int lane, con
       } else {
 #pragma unroll
         for (int b = 0; b < B; ++b) out[b] = TM(0);
-        uint32_t mk = offdiag_zero ? 0u : __ldg(m.slot_mask + rp + s);
+        unsigned long long mk = 0ull;
+        if (!offdiag_zero) mk = LPR == 8 ? __ldg(m.slot_mask + rp + s) : __ldg(m.slot_mask64 + rp + s);
         while (mk) {
-          const TM* v = row_vals + (__ffs(mk) - 1) * B;
+          const TM* v = row_vals + (__ffsll(mk) - 1) * B;
           mk &= mk - 1;
 #pragma unroll
           for (int b = 0; b < B; ++b) out[b] += v[b];
@@ -207,15 +208,14 @@ struct PcArgs {
   const uint8_t* ref_flag;  // [nn] 1 on pressure-level rows
 };
 
-template <class TF>
+template <int LPR, class TF>
 __global__ void __launch_bounds__(BLOCK) k_pcorr(PcArgs a) {
   __shared__ TF sh_val[BLOCK * 3];
   const int lane = threadIdx.x & 31;
   const int warp_base = threadIdx.x & ~31;
-  const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 3;
-  const int c = threadIdx.x & 7;
-  const bool rv = row < a.m.nn;
-  const int e = rv ? __ldg(a.m.n2e + 8 * row + c) : -1;
+  const RowLane<LPR> rl = row_lane<LPR>(a.m);
+  const int row = rl.row, li = rl.li, e = rl.e, c = rl.c;
+  const bool rv = rl.rv;
   TF diag[1] = {TF(0)};
   TF nb[3][1] = {{TF(0)}, {TF(0)}, {TF(0)}};
   double rhs = 0.0;
@@ -232,11 +232,11 @@ __global__ void __launch_bounds__(BLOCK) k_pcorr(PcArgs a) {
       rhs -= (pk & 1) ? -fl : fl;
     }
   }
-  diag[0] = rowsum8(diag[0]);
-  rhs = rowsum8(rhs);
+  diag[0] = rowsum<LPR>(diag[0]);
+  rhs = rowsum<LPR>(rhs);
   const bool refrow = rv && __ldg(a.ref_flag + row) != 0;
-  write_row<1, TF>(row, rv, c, lane, diag, nb, a.m, static_cast<TF*>(a.A), sh_val + warp_base * 3, refrow);
-  if (rv && c == 0) a.b[row] = refrow ? 0.0 : rhs;
+  write_row<1, TF, LPR>(row, rv, li, lane, diag, nb, a.m, static_cast<TF*>(a.A), sh_val + warp_base * 3, refrow);
+  if (rv && li == 0) a.b[row] = refrow ? 0.0 : rhs;
 }
 
 // ---------------------------------------------------------------------------
@@ -353,15 +353,14 @@ __device__ __forceinline__ void wall_face(const MomArgs& a, const TF (&x)[8][3],
 // correction, transient node terms, SIMPLEC / fractional-step coefficients),
 // each switched at run time; without it the kernel is the steady upwind SIMPLE
 // assembly with nothing else in its register budget.
-template <bool USH, bool UGSH, class TF, bool EXT = false>
+template <int LPR, bool USH, bool UGSH, class TF, bool EXT = false>
 __global__ void __launch_bounds__(BLOCK, sizeof(TF) == 4 ? (UGSH ? 4 : 3) : 1) k_momentum(MomArgs a) {
   __shared__ TF sh_val[BLOCK * 3 * 9];
   const int lane = threadIdx.x & 31;
   const int warp_base = threadIdx.x & ~31;
-  const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 3;
-  const int c = threadIdx.x & 7;
-  const bool rv = row < a.m.nn;
-  const int e = rv ? __ldg(a.m.n2e + 8 * row + c) : -1;
+  const RowLane<LPR> rl = row_lane<LPR>(a.m);
+  const int row = rl.row, li = rl.li, e = rl.e, c = rl.c;
+  const bool rv = rl.rv;
   TF diag[9], nb[3][9], rhs[3];
 #pragma unroll
   for (int k = 0; k < 9; ++k) {
@@ -530,15 +529,15 @@ __global__ void __launch_bounds__(BLOCK, sizeof(TF) == 4 ? (UGSH ? 4 : 3) : 1) k
     if (err) a.err[0] = 1;
   }
 #pragma unroll
-  for (int k = 0; k < 9; ++k) diag[k] = rowsum8(diag[k]);
+  for (int k = 0; k < 9; ++k) diag[k] = rowsum<LPR>(diag[k]);
 #pragma unroll
-  for (int k = 0; k < 3; ++k) rhs[k] = rowsum8(rhs[k]);
+  for (int k = 0; k < 3; ++k) rhs[k] = rowsum<LPR>(rhs[k]);
   // SIMPLEC: sum of the row's off-diagonal (i, i) coefficients (the CSR
   // off-diagonal entries are the lanes' neighbour blocks summed)
   double off[3] = {0.0, 0.0, 0.0};
   if (EXT && a.du_mode == 1)
 #pragma unroll
-    for (int k = 0; k < 3; ++k) off[k] = double(rowsum8(TF(nb[0][4 * k] + nb[1][4 * k] + nb[2][4 * k])));
+    for (int k = 0; k < 3; ++k) off[k] = double(rowsum<LPR>(TF(nb[0][4 * k] + nb[1][4 * k] + nb[2][4 * k])));
   if (rv) {
     // node terms, relaxation, wall rhs relaxation, DU
     const double vol = __ldg(a.m.vol + row);
@@ -575,7 +574,7 @@ __global__ void __launch_bounds__(BLOCK, sizeof(TF) == 4 ? (UGSH ? 4 : 3) : 1) k
       if (wall) r *= a.wall_relax;
       rhs[k] = TF(r);
     }
-    if (c == 0) {
+    if (li == 0) {
       // computeDUCoefficients (navierStokesAssembler.cpp:84-232): V / (a_ii +
       // SMALL), or dt / rho (fractional step, steady gamma1 = 1); SIMPLEC also
       // D~ = V / (a_ii + off-diagonal sum + SMALL)
@@ -589,7 +588,7 @@ __global__ void __launch_bounds__(BLOCK, sizeof(TF) == 4 ? (UGSH ? 4 : 3) : 1) k
       }
     }
   }
-  write_row<9, TF>(row, rv, c, lane, diag, nb, a.m, static_cast<TF*>(a.A), sh_val + warp_base * 3 * 9, false);
+  write_row<9, TF, LPR>(row, rv, li, lane, diag, nb, a.m, static_cast<TF*>(a.A), sh_val + warp_base * 3 * 9, false);
 }
 
 // ---------------------------------------------------------------------------
@@ -828,11 +827,11 @@ struct DivArgs {
   double tk0, tk1, tk2, dt;
 };
 
+template <int LPR>
 __global__ void __launch_bounds__(BLOCK) k_div(DivArgs a) {
-  const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 3;
-  const int c = threadIdx.x & 7;
-  const bool rv = row < a.m.nn;
-  const int e = rv ? __ldg(a.m.n2e + 8 * row + c) : -1;
+  const RowLane<LPR> rl = row_lane<LPR>(a.m);
+  const int row = rl.row, li = rl.li, e = rl.e, c = rl.c;
+  const bool rv = rl.rv;
   double s = 0.0;
   if (e >= 0) {
     const uint32_t iw = ip_word(c);
@@ -843,8 +842,8 @@ __global__ void __launch_bounds__(BLOCK) k_div(DivArgs a) {
       s += (pk & 1) ? -m : m;
     }
   }
-  s = rowsum8(s);
-  if (rv && c == 0) {
+  s = rowsum<LPR>(s);
+  if (rv && li == 0) {
     if (a.order) {
       const double rho = __ldg(a.rho + row), vol = __ldg(a.m.vol + row);
       s += (a.order == 1 ? (a.tk0 * rho + a.tk1 * rho) : (a.tk0 * rho + a.tk1 * rho + a.tk2 * rho)) * vol / a.dt;
@@ -864,12 +863,11 @@ struct GradArgs {
   double gurf;
 };
 
-template <int NC, bool SH>
+template <int LPR, int NC, bool SH>
 __global__ void __launch_bounds__(BLOCK) k_gradient(GradArgs a) {
-  const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 3;
-  const int c = threadIdx.x & 7;
-  const bool rv = row < a.m.nn;
-  const int e = rv ? __ldg(a.m.n2e + 8 * row + c) : -1;
+  const RowLane<LPR> rl = row_lane<LPR>(a.m);
+  const int row = rl.row, li = rl.li, e = rl.e, c = rl.c;
+  const bool rv = rl.rv;
   double acc[NC][3];
 #pragma unroll
   for (int i = 0; i < NC; ++i) acc[i][0] = acc[i][1] = acc[i][2] = 0.0;
@@ -935,8 +933,8 @@ __global__ void __launch_bounds__(BLOCK) k_gradient(GradArgs a) {
 #pragma unroll
   for (int i = 0; i < NC; ++i)
 #pragma unroll
-    for (int j = 0; j < 3; ++j) acc[i][j] = rowsum8(acc[i][j]);
-  if (rv && c == 0) {
+    for (int j = 0; j < 3; ++j) acc[i][j] = rowsum<LPR>(acc[i][j]);
+  if (rv && li == 0) {
     const double iv = 1.0 / __ldg(a.m.vol + row);
 #pragma unroll
     for (int i = 0; i < NC; ++i)
@@ -963,11 +961,11 @@ struct BlendArgs {
 
 // extrema of every velocity component over the row node and its edge
 // neighbours (each SCS ip gives its L node the R value and vice versa)
+template <int LPR>
 __global__ void __launch_bounds__(BLOCK) k_minmax_u(BlendArgs a) {
-  const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 3;
-  const int c = threadIdx.x & 7;
-  const bool rv = row < a.m.nn;
-  const int e = rv ? __ldg(a.m.n2e + 8 * row + c) : -1;
+  const RowLane<LPR> rl = row_lane<LPR>(a.m);
+  const int row = rl.row, li = rl.li, e = rl.e, c = rl.c;
+  const bool rv = rl.rv;
   double lo[3], hi[3];
 #pragma unroll
   for (int i = 0; i < 3; ++i) lo[i] = hi[i] = rv ? __ldg(a.U + 3 * row + i) : 0.0;
@@ -987,11 +985,11 @@ __global__ void __launch_bounds__(BLOCK) k_minmax_u(BlendArgs a) {
 #pragma unroll
   for (int i = 0; i < 3; ++i)
 #pragma unroll
-    for (int o = 1; o < 8; o <<= 1) {
+    for (int o = 1; o < LPR; o <<= 1) {
       lo[i] = fmin(lo[i], __shfl_xor_sync(FULL_MASK, lo[i], o));
       hi[i] = fmax(hi[i], __shfl_xor_sync(FULL_MASK, hi[i], o));
     }
-  if (rv && c == 0)
+  if (rv && li == 0)
 #pragma unroll
     for (int i = 0; i < 3; ++i) {
       a.minU[3 * row + i] = lo[i];
@@ -1018,11 +1016,11 @@ __device__ __forceinline__ void blend_limit(const BlendArgs& a, const double (&p
   }
 }
 
+template <int LPR>
 __global__ void __launch_bounds__(BLOCK) k_blend_u(BlendArgs a) {
-  const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 3;
-  const int c = threadIdx.x & 7;
-  const bool rv = row < a.m.nn;
-  const int e = rv ? __ldg(a.m.n2e + 8 * row + c) : -1;
+  const RowLane<LPR> rl = row_lane<LPR>(a.m);
+  const int row = rl.row, li = rl.li, e = rl.e, c = rl.c;
+  const bool rv = rl.rv;
   double beta[3] = {a.beta_max, a.beta_max, a.beta_max};
   if (e >= 0) {
     double phi[3], lo[3], hi[3], G[9];
@@ -1078,8 +1076,8 @@ __global__ void __launch_bounds__(BLOCK) k_blend_u(BlendArgs a) {
 #pragma unroll
   for (int i = 0; i < 3; ++i)
 #pragma unroll
-    for (int o = 1; o < 8; o <<= 1) beta[i] = fmin(beta[i], __shfl_xor_sync(FULL_MASK, beta[i], o));
-  if (rv && c == 0)
+    for (int o = 1; o < LPR; o <<= 1) beta[i] = fmin(beta[i], __shfl_xor_sync(FULL_MASK, beta[i], o));
+  if (rv && li == 0)
 #pragma unroll
     for (int i = 0; i < 3; ++i) a.beta[3 * row + i] = 0.75 * a.beta[3 * row + i] + 0.25 * beta[i];
 }
@@ -1094,7 +1092,7 @@ __global__ void k_vel_correct(int n3, double* U, const double* du, const double*
 // launchers
 // grids: 8 lanes per row, bs threads per block (a multiple of 32, at most the
 // BLOCK the kernels are compiled for)
-static int grid_rows(int nn, int bs = BLOCK) { return (int)(((size_t)nn * 8 + bs - 1) / bs); }
+static int grid_rows(const DeviceMesh& m, int bs = BLOCK) { return (int)(((size_t)m.nn * m.lpr + bs - 1) / bs); }
 
 static int launch_mdot_impl(Flow& f, int mode);
 
@@ -1106,11 +1104,13 @@ int launch_pcorr(Flow& f, bool mixed, bool flux_fresh) {
     if (int s = launch_mdot_impl(f, 2)) return s;
   PcArgs a{f.mesh->view(), f.pc_coef, f.pc_flux, f.b.A_pc, f.b.b_pc, f.ref_flag};
   const int bs = f.bs_asm;
-  const int g = grid_rows(f.mesh->nn, bs);
+  const int g = grid_rows(*f.mesh, bs);
   if (mixed)
-    k_pcorr<float><<<g, bs, 0, f.stream>>>(a);
+    if (f.mesh->lpr == 16) k_pcorr<16, float><<<g, bs, 0, f.stream>>>(a);
+    else k_pcorr<8, float><<<g, bs, 0, f.stream>>>(a);
   else
-    k_pcorr<double><<<g, bs, 0, f.stream>>>(a);
+    if (f.mesh->lpr == 16) k_pcorr<16, double><<<g, bs, 0, f.stream>>>(a);
+    else k_pcorr<8, double><<<g, bs, 0, f.stream>>>(a);
   count_launches(1);
   OA_CUDA(cudaGetLastError());
   return OA_OK;
@@ -1152,22 +1152,27 @@ int launch_momentum(Flow& f, bool mixed) {
             f.du,           f.duT,     f.time_order ? f.dt_step : f.s.dt,  1.0 / f.s.urf_u, f.s.wall_rhs_relax,
             f.s.du_mode,    f.s.hr,    f.time_order, f.tk[0], f.tk[1], f.tk[2], f.Uold, f.Uoldold, f.err_dev};
   const int bs = f.bs_asm;
-  const int g = grid_rows(f.mesh->nn, bs);
+  const int g = grid_rows(*f.mesh, bs);
   const bool us = f.s.u_shifted, gs = f.s.u_grad_shifted;
   const bool hr = f.s.hr != 0 || f.time_order != 0 || f.s.du_mode != 0;  // the EXT variant
+  auto go = [&](auto lanes) {
+    constexpr int L = decltype(lanes)::value;
 #define OA_MOM(US, GS, T)                                                                   \
   if (us == US && gs == GS) {                                                               \
     if (hr)                                                                                 \
-      k_momentum<US, GS, T, true><<<g, bs, 0, f.stream>>>(a);                               \
+      k_momentum<L, US, GS, T, true><<<g, bs, 0, f.stream>>>(a);                            \
     else                                                                                    \
-      k_momentum<US, GS, T, false><<<g, bs, 0, f.stream>>>(a);                              \
+      k_momentum<L, US, GS, T, false><<<g, bs, 0, f.stream>>>(a);                           \
   }
-  if (mixed) {
-    OA_MOM(true, true, float) OA_MOM(true, false, float) OA_MOM(false, true, float) OA_MOM(false, false, float)
-  } else {
-    OA_MOM(true, true, double) OA_MOM(true, false, double) OA_MOM(false, true, double) OA_MOM(false, false, double)
-  }
+    if (mixed) {
+      OA_MOM(true, true, float) OA_MOM(true, false, float) OA_MOM(false, true, float) OA_MOM(false, false, float)
+    } else {
+      OA_MOM(true, true, double) OA_MOM(true, false, double) OA_MOM(false, true, double) OA_MOM(false, false, double)
+    }
 #undef OA_MOM
+  };
+  if (f.mesh->lpr == 16) go(std::integral_constant<int, 16>{});
+  else go(std::integral_constant<int, 8>{});
   count_launches(1);
   OA_CUDA(cudaGetLastError());
   return OA_OK;
@@ -1214,7 +1219,8 @@ int launch_update_mdot(Flow& f, bool stage) { return launch_mdot_impl(f, stage ?
 
 int launch_div(Flow& f) {
   DivArgs a{f.mesh->view(), f.mDot, f.div, f.rho, f.time_order, f.tk[0], f.tk[1], f.tk[2], f.dt_step};
-  k_div<<<grid_rows(f.mesh->nn, f.bs_rows), f.bs_rows, 0, f.stream>>>(a);
+  if (f.mesh->lpr == 16) k_div<16><<<grid_rows(*f.mesh, f.bs_rows), f.bs_rows, 0, f.stream>>>(a);
+  else k_div<8><<<grid_rows(*f.mesh, f.bs_rows), f.bs_rows, 0, f.stream>>>(a);
   count_launches(1);
   OA_CUDA(cudaGetLastError());
   return OA_OK;
@@ -1222,15 +1228,25 @@ int launch_div(Flow& f) {
 
 int launch_gradient(Flow& f, int which) {
   const int bs = f.bs_rows;
-  const int g = grid_rows(f.mesh->nn, bs);
+  const int g = grid_rows(*f.mesh, bs);
   if (which == 0) {
     GradArgs a{f.mesh->view(), f.p, f.gradP, f.s.grad_urf};
-    if (f.s.p_shifted) k_gradient<1, true><<<g, bs, 0, f.stream>>>(a);
-    else k_gradient<1, false><<<g, bs, 0, f.stream>>>(a);
+    if (f.mesh->lpr == 16) {
+      if (f.s.p_shifted) k_gradient<16, 1, true><<<g, bs, 0, f.stream>>>(a);
+      else k_gradient<16, 1, false><<<g, bs, 0, f.stream>>>(a);
+    } else {
+      if (f.s.p_shifted) k_gradient<8, 1, true><<<g, bs, 0, f.stream>>>(a);
+      else k_gradient<8, 1, false><<<g, bs, 0, f.stream>>>(a);
+    }
   } else {
     GradArgs a{f.mesh->view(), f.U, f.gradU, f.s.grad_urf};
-    if (f.s.u_shifted) k_gradient<3, true><<<g, bs, 0, f.stream>>>(a);
-    else k_gradient<3, false><<<g, bs, 0, f.stream>>>(a);
+    if (f.mesh->lpr == 16) {
+      if (f.s.u_shifted) k_gradient<16, 3, true><<<g, bs, 0, f.stream>>>(a);
+      else k_gradient<16, 3, false><<<g, bs, 0, f.stream>>>(a);
+    } else {
+      if (f.s.u_shifted) k_gradient<8, 3, true><<<g, bs, 0, f.stream>>>(a);
+      else k_gradient<8, 3, false><<<g, bs, 0, f.stream>>>(a);
+    }
   }
   count_launches(1);
   OA_CUDA(cudaGetLastError());
@@ -1239,9 +1255,14 @@ int launch_gradient(Flow& f, int which) {
 
 int launch_blend_u(Flow& f) {
   BlendArgs a{f.mesh->view(), f.U, f.gradU, f.minU, f.maxU, f.betaU, f.s.beta_max};
-  const int g = grid_rows(f.mesh->nn, f.bs_rows);
-  k_minmax_u<<<g, f.bs_rows, 0, f.stream>>>(a);
-  k_blend_u<<<g, f.bs_rows, 0, f.stream>>>(a);
+  const int g = grid_rows(*f.mesh, f.bs_rows);
+  if (f.mesh->lpr == 16) {
+    k_minmax_u<16><<<g, f.bs_rows, 0, f.stream>>>(a);
+    k_blend_u<16><<<g, f.bs_rows, 0, f.stream>>>(a);
+  } else {
+    k_minmax_u<8><<<g, f.bs_rows, 0, f.stream>>>(a);
+    k_blend_u<8><<<g, f.bs_rows, 0, f.stream>>>(a);
+  }
   count_launches(2);
   OA_CUDA(cudaGetLastError());
   return OA_OK;

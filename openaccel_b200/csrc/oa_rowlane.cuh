@@ -1,8 +1,8 @@
 // Row-owner ("corner-lane") execution model shared by the hex8 kernels.
 //
-// Eight consecutive lanes own one CSR row (mesh node). Lane c handles the
-// incident element in which the node is element corner c (n2e table), in the
-// canonical frame of oa_hex8.cuh. Per-lane partial sums are combined in a fixed
+// Eight (or sixteen) consecutive lanes own one CSR row (mesh node). Each lane
+// handles one incident element, in the canonical frame of oa_hex8.cuh that
+// puts the row node at corner 0. Per-lane partial sums are combined in a fixed
 // order — xor-butterflies for the diagonal block and the rhs, and an ordered
 // shared-memory gather for off-diagonal slots — so every CSR entry is written
 // exactly once, deterministically, without atomics and without a zero fill.
@@ -10,10 +10,36 @@
 #include <cstdint>
 
 #include "oa_hex8.cuh"
+#include "oa_internal.h"
 
 namespace oa {
 
 constexpr unsigned FULL_MASK = 0xffffffffu;
+
+// Lanes per row: 8 on consistently oriented block meshes, where lane c takes
+// the element in which the node is corner c, and 16 on other hex meshes
+// (3, 5, ... elements around an edge), where the lanes take the node's
+// incident (element, corner) pairs in element order. n2e holds LPR entries per
+// node, element * 8 + corner, or -1.
+template <int LPR>
+struct RowLane {
+  int row, li, e, c;
+  bool rv;
+};
+
+template <int LPR>
+__device__ __forceinline__ RowLane<LPR> row_lane(const MeshView& m) {
+  static_assert(LPR == 8 || LPR == 16, "8 or 16 lanes per row");
+  RowLane<LPR> r;
+  const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  r.row = (int)(t / LPR);
+  r.li = threadIdx.x & (LPR - 1);
+  r.rv = r.row < m.nn;
+  const int ec = r.rv ? __ldg(m.n2e + (size_t)LPR * r.row + r.li) : -1;
+  r.e = ec >= 0 ? (ec >> 3) : -1;
+  r.c = ec >= 0 ? (ec & 7) : 0;
+  return r;
+}
 
 // ROT_PERM / ROT_IP / ROT_FACE rows packed into one word so a lane can select
 // its row without an indexed constant load (8 distinct addresses per warp).
@@ -59,11 +85,13 @@ __device__ __forceinline__ uint32_t face_word(int c) {
 
 __device__ __forceinline__ int perm_at(uint32_t w, int k) { return (w >> (3 * k)) & 7; }
 
-template <class T>
-__device__ __forceinline__ T rowsum8(T v) {
+// sum over a row's lanes (xor butterflies: every lane gets the same value)
+template <int LPR, class T>
+__device__ __forceinline__ T rowsum(T v) {
   v += __shfl_xor_sync(FULL_MASK, v, 1);
   v += __shfl_xor_sync(FULL_MASK, v, 2);
   v += __shfl_xor_sync(FULL_MASK, v, 4);
+  if (LPR == 16) v += __shfl_xor_sync(FULL_MASK, v, 8);
   return v;
 }
 

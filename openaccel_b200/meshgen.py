@@ -143,14 +143,85 @@ def initial_velocity(mesh: HexMesh, sigma=0.0, seed=12345):
     if sigma > 0.0:
         rng = np.random.Generator(np.random.PCG64(seed + 1))
         g = rng.normal(0.0, sigma, size=U.shape)
-        nx, ny, nz = mesh.nx, mesh.ny, mesh.nz
-        idx = np.arange(mesh.nn)
-        i = idx % (nx + 1)
-        j = (idx // (nx + 1)) % (ny + 1)
-        k = idx // ((nx + 1) * (ny + 1))
-        interior = (i > 0) & (i < nx) & (j > 0) & (j < ny) & (k > 0) & (k < nz)
+        if mesh.meta.get("kind") == "star":
+            interior = np.ones(mesh.nn, dtype=bool)
+            fn = mesh.conn[mesh.face_elem[:, None], HEX_FACE_NODES[mesh.face_ord]]
+            interior[fn.ravel()] = False
+        else:
+            nx, ny, nz = mesh.nx, mesh.ny, mesh.nz
+            idx = np.arange(mesh.nn)
+            i = idx % (nx + 1)
+            j = (idx // (nx + 1)) % (ny + 1)
+            k = idx // ((nx + 1) * (ny + 1))
+            interior = (i > 0) & (i < nx) & (j > 0) & (j < ny) & (k > 0) & (k < nz)
         U[interior] = g[interior]
     return U
+
+
+def star_prism(blocks=3, n=6, nz=6, radius=1.0, height=1.0, perturb=0.0, seed=7, lid_velocity=(1.0, 0.0, 0.0)):
+    """A hex mesh that is not one block: a regular polygon with 2*blocks
+    corners split into ``blocks`` quadrilaterals that meet at its centre, each
+    meshed n x n (bilinear), extruded into nz layers. Along the centre line
+    ``blocks`` elements meet around every edge (3 or 5 instead of 4), so no
+    consistent corner labelling exists; nodes there have 2*blocks incident
+    elements (10 for 5 blocks). Lid (z = height) is boundary 0 moving with
+    ``lid_velocity``, the side and bottom walls boundary 1 (applied last).
+    ``perturb`` displaces nodes off every boundary by U(-perturb h, perturb h)
+    per coordinate, h = radius / n."""
+    nb = int(blocks)
+    th = np.pi * np.arange(2 * nb) / nb
+    V = radius * np.stack([np.cos(th), np.sin(th)], axis=1)
+    C = np.zeros(2)
+    s1 = np.linspace(0.0, 1.0, n + 1)
+    # 2D nodes of every block, merged along the shared edges
+    keys, pts, ids = {}, [], []
+    for b in range(nb):
+        q10, q11, q01 = V[(2 * b) % (2 * nb)], V[(2 * b + 1) % (2 * nb)], V[(2 * b + 2) % (2 * nb)]
+        bid = np.empty((n + 1, n + 1), dtype=np.int64)
+        for j, t in enumerate(s1):
+            for i, sv in enumerate(s1):
+                X = (1 - sv) * (1 - t) * C + sv * (1 - t) * q10 + sv * t * q11 + (1 - sv) * t * q01
+                key = (round(X[0] * 1e9), round(X[1] * 1e9))
+                if key not in keys:
+                    keys[key] = len(pts)
+                    pts.append(X)
+                bid[i, j] = keys[key]
+        ids.append(bid)
+    P = np.array(pts)
+    n2 = P.shape[0]
+    z = np.linspace(0.0, height, nz + 1)
+    coords = np.concatenate([np.column_stack([P, np.full(n2, zk)]) for zk in z]).astype(np.float64)
+    conn, fe, fo, fb = [], [], [], []
+    for b in range(nb):
+        bid = ids[b]
+        for k in range(nz):
+            for j in range(n):
+                for i in range(n):
+                    q = [bid[i, j], bid[i + 1, j], bid[i + 1, j + 1], bid[i, j + 1]]
+                    e = len(conn)
+                    conn.append([v + k * n2 for v in q] + [v + (k + 1) * n2 for v in q])
+                    if k == nz - 1:
+                        fe.append(e), fo.append(5), fb.append(0)
+                    if k == 0:
+                        fe.append(e), fo.append(4), fb.append(1)
+                    if i == n - 1:
+                        fe.append(e), fo.append(1), fb.append(1)
+                    if j == n - 1:
+                        fe.append(e), fo.append(2), fb.append(1)
+    conn = np.array(conn, dtype=np.int32)
+    fe, fo, fb = (np.array(v, dtype=np.int32) for v in (fe, fo, fb))
+    # lid faces first, then the walls (node-side values: the later boundary wins)
+    order = np.argsort(fb, kind="stable")
+    fe, fo, fb = fe[order], fo[order], fb[order]
+    if perturb > 0.0:
+        on_bnd = np.zeros(coords.shape[0], dtype=bool)
+        on_bnd[conn[fe[:, None], HEX_FACE_NODES[fo]].ravel()] = True
+        rng = np.random.Generator(np.random.PCG64(seed))
+        noise = rng.uniform(-perturb * radius / n, perturb * radius / n, size=coords.shape)
+        coords[~on_bnd] += noise[~on_bnd]
+    bnd_velocity = np.array([list(lid_velocity), [0.0, 0.0, 0.0]], dtype=np.float64)
+    return HexMesh(n, n, nz, coords, conn, fe, fo, fb, bnd_velocity,
+                   meta={"kind": "star", "blocks": nb, "n": n, "nz": nz, "perturb": perturb, "seed": seed})
 
 
 @dataclass

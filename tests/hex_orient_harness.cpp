@@ -6,11 +6,14 @@
 #include "../openaccel_b200/csrc/oa_hex_orient.h"
 
 extern "C" {
+// 0: oriented; 1: not a block (the row kernels take the incident-list lanes);
+// 2: not a valid hex mesh
 int ho_orient(int nn, int ne, const int* conn, int* out_conn, unsigned char* rot) {
   std::vector<int> oc;
   std::vector<uint8_t> r;
   std::string why;
-  if (!oa::hexorient::orient(nn, ne, conn, oc, r, &why)) return 1;
+  bool invalid = false;
+  if (!oa::hexorient::orient(nn, ne, conn, oc, r, &why, &invalid)) return invalid ? 2 : 1;
   for (size_t i = 0; i < oc.size(); ++i) out_conn[i] = oc[i];
   for (size_t i = 0; i < r.size(); ++i) rot[i] = r[i];
   return 0;

@@ -4,7 +4,8 @@ numbering at different corners or axes, such as the reference's own cavity
 example mesh: the 24 rotations are proper (positive Jacobian kept); after
 orientation no node is the same local corner of two elements; every element
 keeps its node set; the ip and face maps are consistent with the
-permutation; a mesh that is not a block is rejected."""
+permutation; a mesh that is not a block is told apart (the row kernels then
+run on incident-element lists) from one that is not a valid hex mesh."""
 import ctypes as C
 import os
 import subprocess
@@ -123,3 +124,22 @@ def test_non_block_mesh_is_rejected(H):
     conn = np.array([[a, b, c, d, a + top, b + top, c + top, d + top] for a, b, c, d in quads])
     st, out, rot = orient(H, coords.shape[0], conn)
     assert st == 1
+
+
+@pytest.mark.parametrize("blocks,expect", [(3, 1), (4, 0), (5, 1)])
+def test_star_prisms(H, blocks, expect):
+    """Polygon split into 3, 4 or 5 blocks around its centre: only 4 (four
+    elements around every edge) is a consistently orientable block."""
+    m = meshgen.star_prism(blocks, 3, 2)
+    st, out, rot = orient(H, m.nn, m.conn)
+    assert st == expect
+    if st == 0:
+        assert corner_conflicts(m.nn, out) == 0
+        assert corner_conflicts(m.nn, m.conn) > 0  # it did need the relabelling
+
+
+def test_face_shared_by_three_elements_is_invalid(H):
+    m = meshgen.cavity(2)
+    conn = np.concatenate([m.conn, m.conn[:1]])  # a duplicated element
+    st, out, rot = orient(H, m.nn, np.ascontiguousarray(conn[::-1]))
+    assert st == 2

@@ -89,6 +89,29 @@ def test_dual_volume_and_graph(oracle_mod):
         assert np.all(np.diff(row) > 0) and i in row
 
 
+@pytest.mark.parametrize("blocks", [3, 5])
+def test_star_prism_volume_graph_and_row_sums(oracle_mod, blocks):
+    """A hex mesh that is not one block (3 or 5 elements around the centre
+    line's edges): dual volumes add up to the prism (polygon area x height),
+    the centre-line nodes have blocks + 2 stencil neighbours (+ self), and
+    the pressure-correction rows still sum to zero."""
+    m = meshgen.star_prism(blocks, 4, 3, radius=1.0, height=0.5)
+    c = oracle_mod.FlowCase(m, U0=np.random.default_rng(1).normal(0, 0.1, (m.nn, 3)))
+    k = 2 * blocks
+    area = 0.5 * k * np.sin(2 * np.pi / k)
+    np.testing.assert_allclose(c.field("vol").sum(), 0.5 * area, rtol=1e-13)
+    rp, cols = c.graph()
+    centre = np.where(np.linalg.norm(m.coords[:, :2], axis=1) < 1e-12)[0]
+    interior_centre = centre[(m.coords[centre, 2] > 0) & (m.coords[centre, 2] < 0.5)]
+    assert np.all(np.diff(rp)[interior_centre] == blocks + 3)
+    c.initialize()
+    c.field("du")[:] = np.random.default_rng(2).uniform(0.5, 1.5, 3 * m.nn)
+    A, b = c.assemble_pcorr()
+    rows = np.add.reduceat(A, rp[:-1])
+    rows[0] = 0.0
+    assert np.abs(rows).max() < 1e-13 * np.abs(A).max()
+
+
 def test_pcorr_row_sums_vanish(oracle_mod):
     """Rhie-Chow Laplacian: sum_n dN_n/dx = 0, so every row of the
     pressure-correction matrix sums to zero (lumping keeps row sums)."""
