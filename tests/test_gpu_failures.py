@@ -5,6 +5,7 @@ convention would let a caller continue.
 
 - a non-finite value in the field state reaches the solvers as a non-finite
   right-hand side -> OA_ERR_SOLVER (Krylov status 2), in both precisions;
+- a hex mesh with a face shared by three elements -> OA_ERR_MESH;
 - a hex whose nodes are moved so that it turns inside out -> OA_ERR_GEOMETRY
   (non-positive sub-control volume, the Jacobian determinant check of
   hex_scv_det / hex_gradient_operator);
@@ -44,6 +45,14 @@ def test_nan_state_is_a_solver_error(prec):
     with pytest.raises(rt.OpenAccelError) as ei:
         gf.simple_iterate(1)
     assert ei.value.status == OA_ERR_SOLVER
+
+
+def test_face_shared_by_three_elements_is_a_mesh_error():
+    m = meshgen.cavity(3)
+    bad = dataclasses.replace(m, conn=np.ascontiguousarray(np.concatenate([m.conn, m.conn[4:5]])[::-1]))
+    with pytest.raises(rt.OpenAccelError) as ei:
+        rt.Mesh(bad)
+    assert ei.value.status == OA_ERR_MESH and "invalid hex mesh" in str(ei.value)
 
 
 def test_inverted_hex_is_a_geometry_error():
