@@ -368,6 +368,29 @@ void oa_sst_default_constants(oa_sst_constants* c);
 int oa_sst_node_update(int nn, const oa_sst_constants* c, double dt, double mut_urf, const oa_sst_fields* f,
                        void* stream);
 
+/* Fused u/v/w/k/omega assembly. After this call every momentum assembly of the
+ * flow (oa_assemble_momentum, oa_simple_iterate) assembles in the same launch
+ * the k and omega transport systems of the SST equations' element terms
+ * (phiAssembler<1>::assembleElemTermsInterior_,
+ * src/assemble/phiAssembler/phiAssemblerElemTerms.hpp:11-413: upwind advection
+ * with the flow's mass flows, diffusion with the nodal diffusivities
+ * "gammaK" / "gammaOmega" interpolated to the ips on the velocity's shape
+ * functions and gradient operator), reusing the momentum kernel's ip geometry.
+ * Walls are zero-gradient for both fields
+ * (turbulent*SSTAssemblerElemBoundaryConditions.cpp), so they add no element
+ * terms. The node terms are the flow fields "srcDiagK" / "srcRhsK" /
+ * "srcDiagOmega" / "srcRhsOmega" (for instance the k_diag / k_rhs / w_diag /
+ * w_rhs outputs of oa_sst_node_update written to their device pointers); the
+ * diagonal is then relaxed by 1/urf (phiAssembler.h:967-1006). k and omega are
+ * the fields "k" and "omega". Creates these fields (zero); steady upwind SIMPLE
+ * flows only (no high resolution, SIMPLEC, fractional step or time stepping:
+ * OA_ERR_ARG). */
+int oa_flow_enable_turbulence(oa_flow* f, double urf_k, double urf_omega);
+/* Host copies of the k and omega systems of the last momentum assembly (same
+ * CSR layout as the pressure correction); any pointer may be NULL.
+ * OA_ERR_NOT_READY before oa_flow_enable_turbulence. */
+int oa_flow_turbulence_systems(oa_flow* f, double* A_k, double* b_k, double* A_omega, double* b_omega);
+
 #ifdef __cplusplus
 }
 #endif

@@ -168,6 +168,17 @@ double* field_ptr(Flow& f, const std::string& n, size_t* len) {
   if (f.duT && n == "duTilde") { *len = 3 * nn; return f.duT; }
   if (f.Uold && n == "Uold") { *len = 3 * nn; return f.Uold; }
   if (f.Uoldold && n == "Uoldold") { *len = 3 * nn; return f.Uoldold; }
+  if (f.turb) {
+    *len = nn;
+    if (n == "k") return f.kf;
+    if (n == "omega") return f.wf;
+    if (n == "gammaK") return f.gkf;
+    if (n == "gammaOmega") return f.gwf;
+    if (n == "srcDiagK") return f.sdk;
+    if (n == "srcRhsK") return f.srk;
+    if (n == "srcDiagOmega") return f.sdw;
+    if (n == "srcRhsOmega") return f.srw;
+  }
   *len = 0;
   return nullptr;
 }
@@ -840,7 +851,9 @@ void oa_flow_destroy(oa_flow* H) {
   void* ptrs[] = {f.U,       f.p,       f.gradU,   f.gradP,   f.du,      f.div,    f.mDot,  f.pc_flux,
                   f.pc_coef, f.xloc32,  f.umu32,   f.rho,     f.mu,      f.sideU,  f.b.A_mom, f.b.b_mom,
                   f.b.A_pc,  f.b.b_pc,  f.b.x_mom, f.b.x_pc,  f.err_dev, H->scal,  f.red,   f.ref_flag,
-                  f.betaU,   f.minU,    f.maxU,    f.duT,     f.Uold,    f.Uoldold};
+                  f.betaU,   f.minU,    f.maxU,    f.duT,     f.Uold,    f.Uoldold, f.kf,      f.wf,
+                  f.gkf,     f.gwf,     f.sdk,     f.srk,     f.sdw,     f.srw,     f.A_k,     f.b_k,
+                  f.A_w,     f.b_w};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (H->hscal) cudaFreeHost(H->hscal);
@@ -1081,6 +1094,42 @@ int oa_simple_iterate(oa_flow* H, int n, oa_iter_stats* stats) {
   return s;
 }
 
+int oa_flow_enable_turbulence(oa_flow* H, double urf_k, double urf_omega) {
+  if (!H || !(urf_k > 0 && urf_k <= 1) || !(urf_omega > 0 && urf_omega <= 1))
+    return fail(OA_ERR_ARG, "oa_flow_enable_turbulence: relaxation factors must be in (0, 1]");
+  Flow& f = H->f;
+  if (f.s.hr || f.s.du_mode || f.time_scheme)
+    return fail(OA_ERR_ARG, "oa_flow_enable_turbulence: the fused transport variant is steady upwind SIMPLE only");
+  f.urf_k = urf_k;
+  f.urf_w = urf_omega;
+  if (f.turb) return OA_OK;
+  const size_t nn = f.mesh->nn, nnz = f.mesh->nnz;
+  const size_t ws = mixed(f) ? sizeof(float) : sizeof(double);
+  double** fields[] = {&f.kf, &f.wf, &f.gkf, &f.gwf, &f.sdk, &f.srk, &f.sdw, &f.srw};
+  for (double** p : fields) {
+    if (int s = dalloc(p, nn)) return s;
+    OA_CUDA(cudaMemset(*p, 0, sizeof(double) * nn));
+  }
+  void** sys[] = {&f.A_k, &f.A_w};
+  for (void** p : sys) OA_CUDA(cudaMalloc(p, ws * (nnz ? nnz : 1)));
+  void** rhs[] = {&f.b_k, &f.b_w};
+  for (void** p : rhs) OA_CUDA(cudaMalloc(p, ws * (nn ? nn : 1)));
+  f.turb = true;
+  H->ig.drop();
+  return OA_OK;
+}
+
+int oa_flow_turbulence_systems(oa_flow* H, double* A_k, double* b_k, double* A_omega, double* b_omega) {
+  if (!H) return fail(OA_ERR_ARG, "oa_flow_turbulence_systems: null handle");
+  Flow& f = H->f;
+  if (!f.turb) return fail(OA_ERR_NOT_READY, "oa_flow_turbulence_systems: turbulence transport not enabled");
+  const size_t nn = f.mesh->nn, nnz = f.mesh->nnz;
+  if (int s = copy_out_matrix(f, f.A_k, nnz, A_k)) return s;
+  if (int s = copy_out_matrix(f, f.b_k, nn, b_k)) return s;
+  if (int s = copy_out_matrix(f, f.A_w, nnz, A_omega)) return s;
+  return copy_out_matrix(f, f.b_w, nn, b_omega);
+}
+
 int oa_flow_set_tuning(oa_flow* H, const oa_tuning* t) {
   if (!H || !t) return fail(OA_ERR_ARG, "oa_flow_set_tuning: null argument");
   auto ok_bs = [](int b) { return b == 32 || b == 64 || b == 128; };
@@ -1190,6 +1239,7 @@ int oa_flow_advance_time(oa_flow* H, int scheme, double dt) {
   if (!H || (scheme != OA_TIME_BDF1 && scheme != OA_TIME_BDF2) || !(dt > 0))
     return fail(OA_ERR_ARG, "oa_flow_advance_time: scheme must be OA_TIME_BDF1 or OA_TIME_BDF2 and dt > 0");
   Flow& f = H->f;
+  if (f.turb) return fail(OA_ERR_ARG, "oa_flow_advance_time: the fused turbulence transport is steady only");
   const size_t n3 = 3 * (size_t)f.mesh->nn;
   if (!f.Uold) {
     if (int s = dalloc(&f.Uold, n3)) return s;

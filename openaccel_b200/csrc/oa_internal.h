@@ -97,6 +97,14 @@ struct Flow {
   // memory (gradients, divergence, blending), the element-owner mass-flow
   // kernel, the assembly row kernels (momentum, pressure correction)
   int bs_rows = 128, bs_elems = 128, bs_asm = 128;
+  // k-omega transport assembled in the momentum launch (oa_flow_enable_turbulence):
+  // k, omega, their nodal diffusivities and node source terms ([nn] FP64), the
+  // two systems in the matrix precision, their relaxation factors
+  bool turb = false;
+  double *kf = nullptr, *wf = nullptr, *gkf = nullptr, *gwf = nullptr;
+  double *sdk = nullptr, *srk = nullptr, *sdw = nullptr, *srw = nullptr;
+  void *A_k = nullptr, *b_k = nullptr, *A_w = nullptr, *b_w = nullptr;
+  double urf_k = 1.0, urf_w = 1.0;
   // [ne][12] Rhie-Chow mass flux of each SCS ip with the pressure-correction
   // equation's upwind density (its right-hand side), written by the mass-flow
   // kernel and summed per row by the pressure-correction kernel

@@ -266,6 +266,11 @@ struct MomArgs {
   double tk0, tk1, tk2;
   const double *Uold, *Uoldold;
   int* err;
+  // fused turbulence transport (VAR 2): k, omega, their nodal diffusivities
+  // and node source terms; systems in the matrix precision
+  const double *kf, *wf, *gkf, *gwf, *sdk, *srk, *sdw, *srw;
+  void *Ak, *bk, *Aw, *bw;
+  double urf_k_inv, urf_w_inv;
 };
 
 // Zero-normal-stress wall term at the exposed ip of canonical face FC nearest
@@ -349,12 +354,19 @@ __device__ __forceinline__ void wall_face(const MomArgs& a, const TF (&x)[8][3],
   });
 }
 
-// EXT: the variant with the optional terms (high-resolution deferred
+// VAR 1: the variant with the optional terms (high-resolution deferred
 // correction, transient node terms, SIMPLEC / fractional-step coefficients),
-// each switched at run time; without it the kernel is the steady upwind SIMPLE
-// assembly with nothing else in its register budget.
-template <int LPR, bool USH, bool UGSH, class TF, bool EXT = false>
-__global__ void __launch_bounds__(BLOCK, sizeof(TF) == 4 ? (UGSH ? 4 : 3) : 1) k_momentum(MomArgs a) {
+// each switched at run time; VAR 2: the fused u/v/w/k/omega variant, which
+// also assembles the two turbulence transport equations from the same ip
+// geometry (upwind advection with the same mass flows, diffusion with the
+// nodal diffusivities at the ips: phiAssemblerElemTerms.hpp:11-413, N = 1);
+// VAR 0 is the steady upwind SIMPLE assembly with nothing else in its
+// register budget.
+template <int LPR, bool USH, bool UGSH, class TF, int VAR = 0>
+__global__ void __launch_bounds__(BLOCK, sizeof(TF) == 4 ? (VAR == 2 ? 2 : (UGSH ? 4 : 3)) : 1)
+    k_momentum(MomArgs a) {
+  constexpr bool EXT = VAR == 1;
+  constexpr bool TURB = VAR == 2;
   __shared__ TF sh_val[BLOCK * 3 * 9];
   const int lane = threadIdx.x & 31;
   const int warp_base = threadIdx.x & ~31;
@@ -368,6 +380,8 @@ __global__ void __launch_bounds__(BLOCK, sizeof(TF) == 4 ? (UGSH ? 4 : 3) : 1) k
     nb[0][k] = nb[1][k] = nb[2][k] = TF(0);
   }
   rhs[0] = rhs[1] = rhs[2] = TF(0);
+  // turbulence transport (TURB): [0] k, [1] omega
+  TF tdiag[2] = {TF(0), TF(0)}, tnb[2][3] = {{TF(0), TF(0), TF(0)}, {TF(0), TF(0), TF(0)}}, trhs[2] = {TF(0), TF(0)};
   if (e >= 0) {
     const uint32_t pw = perm_word(c);
     const uint32_t iw = ip_word(c);
@@ -408,6 +422,17 @@ __global__ void __launch_bounds__(BLOCK, sizeof(TF) == 4 ? (UGSH ? 4 : 3) : 1) k
         Uc[k][1] = TF(u[1]);
         Uc[k][2] = TF(u[2]);
         mu[k] = TF(__ldg(a.mu + nd[k]));
+      }
+    }
+    // k, omega and their diffusivities at the element's nodes
+    TF tph[2][8], tgam[2][8];
+    if constexpr (TURB) {
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        tph[0][k] = TF(__ldg(a.kf + nd[k]));
+        tph[1][k] = TF(__ldg(a.wf + nd[k]));
+        tgam[0][k] = TF(__ldg(a.gkf + nd[k]));
+        tgam[1][k] = TF(__ldg(a.gwf + nd[k]));
       }
     }
     int err = 0;
@@ -468,6 +493,22 @@ __global__ void __launch_bounds__(BLOCK, sizeof(TF) == 4 ? (UGSH ? 4 : 3) : 1) k
         diag[3 * i + i] += fl;
         nb[RS][3 * i + i] += fr;
       }
+      // turbulence transport: the same upwind advection; diffusivities at the
+      // ip with the velocity's shape functions
+      [[maybe_unused]] TF tgIp[2] = {TF(0), TF(0)};
+      if constexpr (TURB) {
+#pragma unroll
+        for (int t = 0; t < 2; ++t) {
+          StaticFor<0, 8>::run([&](auto nc) {
+            constexpr int n = decltype(nc)::value;
+            constexpr double N = shape_at<PV, n>();
+            if (N != 0.0) tgIp[t] += TF(N) * tgam[t][n];
+          });
+          trhs[t] -= tm * (tmd > 0 ? tph[t][0] : tph[t][R]);
+          tdiag[t] += fl;
+          tnb[t][RS] += fr;
+        }
+      }
       // viscous stress incl. transpose. Block of column n:
       //   -mu_ip (g_n . A) I - mu_ip A (x) g_n   (rows i, columns j: g_n,i A_j)
       // Its defect contribution summed over the eight columns is
@@ -499,6 +540,26 @@ __global__ void __launch_bounds__(BLOCK, sizeof(TF) == 4 ? (UGSH ? 4 : 3) : 1) k
       for (int i = 0; i < 3; ++i)
         rhs[i] += muIp * (G[i][0] * ax[0] + G[i][1] * ax[1] + G[i][2] * ax[2] + G[0][i] * ax[0] + G[1][i] * ax[1] +
                           G[2][i] * ax[2]);
+      if constexpr (TURB) {
+        // diffusion defect: rhs += Gamma_ip grad(phi)_ip . A
+#pragma unroll
+        for (int t = 0; t < 2; ++t) {
+          TF Gp[3] = {TF(0), TF(0), TF(0)};
+          StaticFor<0, 8>::run([&](auto nc) {
+            constexpr int n = decltype(nc)::value;
+            constexpr double d0 = dshape(n, 0, PG::s(0), PG::s(1), PG::s(2));
+            constexpr double d1 = dshape(n, 1, PG::s(0), PG::s(1), PG::s(2));
+            constexpr double d2 = dshape(n, 2, PG::s(0), PG::s(1), PG::s(2));
+            if (d0 != 0.0) Gp[0] += TF(d0) * tph[t][n];
+            if (d1 != 0.0) Gp[1] += TF(d1) * tph[t][n];
+            if (d2 != 0.0) Gp[2] += TF(d2) * tph[t][n];
+          });
+          TF gax = TF(0);
+#pragma unroll
+          for (int j = 0; j < 3; ++j) gax += (Gp[0] * J.s[0][j] + Gp[1] * J.s[1][j] + Gp[2] * J.s[2][j]) * ax[j];
+          trhs[t] += tgIp[t] * gax;
+        }
+      }
       StaticFor<1, 5>::run([&](auto nc) {
         constexpr int n = decltype(nc)::value;
         constexpr int sl = nb_slot(n);
@@ -513,6 +574,14 @@ __global__ void __launch_bounds__(BLOCK, sizeof(TF) == 4 ? (UGSH ? 4 : 3) : 1) k
               const TF fj = -muIp * g[i] * ax[j] + (i == j ? -muIp * ga : TF(0));
               nb[sl][3 * i + j] += fj;
               diag[3 * i + j] -= fj;
+            }
+          }
+          if constexpr (TURB) {
+#pragma unroll
+            for (int t = 0; t < 2; ++t) {
+              const TF ft = -tgIp[t] * ga;
+              tnb[t][sl] += ft;
+              tdiag[t] -= ft;
             }
           }
         }
@@ -589,6 +658,24 @@ __global__ void __launch_bounds__(BLOCK, sizeof(TF) == 4 ? (UGSH ? 4 : 3) : 1) k
     }
   }
   write_row<9, TF, LPR>(row, rv, li, lane, diag, nb, a.m, static_cast<TF*>(a.A), sh_val + warp_base * 3 * 9, false);
+  if constexpr (TURB) {
+    // k and omega rows: node source terms (the SST node update's diagonal and
+    // rhs), relaxation of the diagonal (phiAssembler.h:967-1006)
+#pragma unroll
+    for (int t = 0; t < 2; ++t) {
+      TF td[1] = {rowsum<LPR>(tdiag[t])};
+      TF tr = rowsum<LPR>(trhs[t]);
+      if (rv) {
+        const double d = (double(td[0]) + __ldg((t ? a.sdw : a.sdk) + row)) * (t ? a.urf_w_inv : a.urf_k_inv);
+        td[0] = TF(d);
+        tr = TF(double(tr) + __ldg((t ? a.srw : a.srk) + row));
+        if (li == 0) static_cast<TF*>(t ? a.bw : a.bk)[row] = tr;
+      }
+      TF tnbt[3][1] = {{tnb[t][0]}, {tnb[t][1]}, {tnb[t][2]}};
+      write_row<1, TF, LPR>(row, rv, li, lane, td, tnbt, a.m, static_cast<TF*>(t ? a.Aw : a.Ak),
+                            sh_val + warp_base * 3 * 9, false);
+    }
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -1154,15 +1241,35 @@ int launch_momentum(Flow& f, bool mixed) {
   const int bs = f.bs_asm;
   const int g = grid_rows(*f.mesh, bs);
   const bool us = f.s.u_shifted, gs = f.s.u_grad_shifted;
-  const bool hr = f.s.hr != 0 || f.time_order != 0 || f.s.du_mode != 0;  // the EXT variant
+  const bool hr = f.s.hr != 0 || f.time_order != 0 || f.s.du_mode != 0;  // the optional-terms variant
+  if (f.turb) {
+    if (hr) return fail(OA_ERR_ARG, "momentum assembly: the fused turbulence variant is steady upwind SIMPLE only");
+    a.kf = f.kf;
+    a.wf = f.wf;
+    a.gkf = f.gkf;
+    a.gwf = f.gwf;
+    a.sdk = f.sdk;
+    a.srk = f.srk;
+    a.sdw = f.sdw;
+    a.srw = f.srw;
+    a.Ak = f.A_k;
+    a.bk = f.b_k;
+    a.Aw = f.A_w;
+    a.bw = f.b_w;
+    a.urf_k_inv = 1.0 / f.urf_k;
+    a.urf_w_inv = 1.0 / f.urf_w;
+  }
+  const int var = f.turb ? 2 : (hr ? 1 : 0);
   auto go = [&](auto lanes) {
     constexpr int L = decltype(lanes)::value;
 #define OA_MOM(US, GS, T)                                                                   \
   if (us == US && gs == GS) {                                                               \
-    if (hr)                                                                                 \
-      k_momentum<L, US, GS, T, true><<<g, bs, 0, f.stream>>>(a);                            \
+    if (var == 1)                                                                           \
+      k_momentum<L, US, GS, T, 1><<<g, bs, 0, f.stream>>>(a);                               \
+    else if (var == 2)                                                                      \
+      k_momentum<L, US, GS, T, 2><<<g, bs, 0, f.stream>>>(a);                               \
     else                                                                                    \
-      k_momentum<L, US, GS, T, false><<<g, bs, 0, f.stream>>>(a);                           \
+      k_momentum<L, US, GS, T, 0><<<g, bs, 0, f.stream>>>(a);                               \
   }
     if (mixed) {
       OA_MOM(true, true, float) OA_MOM(true, false, float) OA_MOM(false, true, float) OA_MOM(false, false, float)

@@ -34,6 +34,7 @@ EXPORTS = [
     "oa_diffusion_field_device_ptr", "oa_diffusion_assemble", "oa_diffusion_solve", "oa_diffusion_step",
     "oa_diffusion_stream", "oa_diffusion_time_assembly", "oa_sst_default_constants", "oa_sst_node_update",
     "oa_flow_last_control", "oa_flow_scales", "oa_flow_advance_time", "oa_flow_autotune", "oa_flow_set_tuning",
+    "oa_flow_enable_turbulence", "oa_flow_turbulence_systems",
 ]
 
 OA_BND_FIXED_VALUE = 0
@@ -180,6 +181,8 @@ def lib():
         "oa_flow_advance_time": (C.c_int, [vp, C.c_int, C.c_double]),
         "oa_flow_autotune": (C.c_int, [vp, C.c_int, P(Tuning)]),
         "oa_flow_set_tuning": (C.c_int, [vp, P(Tuning)]),
+        "oa_flow_enable_turbulence": (C.c_int, [vp, C.c_double, C.c_double]),
+        "oa_flow_turbulence_systems": (C.c_int, [vp, dp, dp, dp, dp]),
         "oa_flow_sync": (C.c_int, [vp]),
         "oa_flow_stream": (C.c_int, [vp, P(vp)]),
         "oa_launch_count": (C.c_int, [P(C.c_longlong)]),
@@ -272,7 +275,9 @@ class Flow:
     """Segregated laminar flow state on the device (oa_flow_create)."""
 
     FIELD_SHAPES = {"U": 3, "p": 1, "gradU": 9, "gradP": 3, "du": 3, "div": 1, "sideU": 3, "rho": 1, "mu": 1,
-                    "betaU": 3, "minU": 3, "maxU": 3, "duTilde": 3, "Uold": 3, "Uoldold": 3}
+                    "betaU": 3, "minU": 3, "maxU": 3, "duTilde": 3, "Uold": 3, "Uoldold": 3,
+                    "k": 1, "omega": 1, "gammaK": 1, "gammaOmega": 1, "srcDiagK": 1, "srcRhsK": 1,
+                    "srcDiagOmega": 1, "srcRhsOmega": 1}
 
     def __init__(self, mesh: Mesh, settings: FlowSettings | None = None):
         self.mesh = mesh
@@ -348,6 +353,17 @@ class Flow:
     def advance_time(self, scheme, dt):
         """Start a time step of size dt: scheme 1 BDF1, 2 BDF2."""
         _check(lib().oa_flow_advance_time(self.h, int(scheme), float(dt)))
+
+    def enable_turbulence(self, urf_k=1.0, urf_omega=1.0):
+        """Assemble the k and omega transport systems in the momentum launch."""
+        _check(lib().oa_flow_enable_turbulence(self.h, float(urf_k), float(urf_omega)))
+
+    def turbulence_systems(self):
+        """(A_k, b_k, A_omega, b_omega) of the last momentum assembly."""
+        nn, nnz = self.mesh.nn, self.mesh.nnz
+        out = [np.zeros(nnz), np.zeros(nn), np.zeros(nnz), np.zeros(nn)]
+        _check(lib().oa_flow_turbulence_systems(self.h, *[_dp(a) for a in out]))
+        return tuple(out)
 
     def autotune(self, iters=3):
         """Tune launch shapes and the pressure-solve schedule; the flow state is

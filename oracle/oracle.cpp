@@ -753,6 +753,70 @@ void assemble_momentum(Case& c, double* A, double* b) {
 }
 
 // ---------------------------------------------------------------------------
+// Scalar transport of a turbulence field (k or omega of the SST model):
+// phiAssembler<1>::assembleElemTermsInterior_
+// (src/assemble/phiAssembler/phiAssemblerElemTerms.hpp:11-413) with upwind
+// advection (the blending factor of both fields is zero) and diffusion with the
+// nodal diffusivity interpolated to the ip, on the velocity's shape functions
+// and gradient operator. Walls are zero-gradient for k and omega
+// (turbulent*SSTAssemblerElemBoundaryConditions.cpp: no boundary element
+// terms). Node terms are given per node (sdiag, srhs: the SST node update's
+// sources), added by one applyCoeff_ per node before the elements; then the
+// diagonal is relaxed by 1/urf (phiAssembler.h:967-1006).
+void assemble_scalar_transport(Case& c, const double* phi, const double* gam, const double* sdiag,
+                               const double* srhs, double urf, double* A, double* b) {
+  const int nnz = c.rowPtr[c.nn];
+  std::fill(A, A + nnz, 0.0);
+  std::fill(b, b + c.nn, 0.0);
+  for (int i = 0; i < c.nn; ++i) {
+    double lhs[1] = {sdiag[i]}, rhs[1] = {srhs[i]};
+    apply_coeff<1>(c, A, b, &i, 1, rhs, lhs);
+  }
+  double Nv[96];
+  oracle::hex8::scs_shape(Nv, c.s.u_shifted);
+  for_elements(c, [&](int e) {
+    const int* en = &c.conn[8 * e];
+    double lhs[64] = {0.0}, rhs[8] = {0.0};
+    double xe[24], Ar[36], g[288], pe[8], ge[8];
+    gather_coords(c, e, xe);
+    for (int a = 0; a < 8; ++a) {
+      pe[a] = phi[en[a]];
+      ge[a] = gam[en[a]];
+    }
+    oracle::hex8::scs_areav(xe, Ar);
+    oracle::hex8::grad_op(xe, g, c.s.u_grad_shifted);
+    for (int ip = 0; ip < NSCS; ++ip) {
+      const int il = LR[ip][0], ir = LR[ip][1];
+      const double tm = c.mDot[12 * e + ip];
+      double gIp = 0.0;
+      for (int a = 0; a < 8; ++a) gIp += Nv[8 * ip + a] * ge[a];
+      // advection, upwind
+      const double af = tm * (tm > 0 ? pe[il] : pe[ir]);
+      rhs[il] -= af;
+      rhs[ir] += af;
+      const double fl = 0.5 * (tm + std::fabs(tm));
+      lhs[8 * il + il] += fl;
+      lhs[8 * ir + il] -= fl;
+      const double fr = 0.5 * (tm - std::fabs(tm));
+      lhs[8 * ir + ir] -= fr;
+      lhs[8 * il + ir] += fr;
+      // diffusion: -Gamma_ip dN_ic/dx_j A_j
+      for (int a = 0; a < 8; ++a) {
+        double lc = 0.0;
+        for (int j = 0; j < 3; ++j) lc += -gIp * g[24 * ip + 3 * a + j] * Ar[3 * ip + j];
+        lhs[8 * il + a] += lc;
+        lhs[8 * ir + a] -= lc;
+        rhs[il] -= lc * pe[a];
+        rhs[ir] += lc * pe[a];
+      }
+    }
+    apply_coeff<1>(c, A, b, en, 8, rhs, lhs);
+  });
+  const double ui = 1.0 / urf;
+  for (int i = 0; i < c.nn; ++i) A[c.rowPtr[i] + c.diagOff[i]] *= ui;
+}
+
+// ---------------------------------------------------------------------------
 // Krylov: BiCGStab, right-preconditioned by (block-)Jacobi. The reference's
 // solver library (liblinsolve over PETSc/Trilinos/HYPRE) is absent; this is the
 // published van der Vorst algorithm.
@@ -1272,6 +1336,10 @@ void orc_assemble_momentum(void* h, double* A, double* b) {
 }
 void orc_assemble_pcorr(void* h, double* A, double* b) {
   assemble_pcorr(*static_cast<Case*>(h), A, b);
+}
+void orc_assemble_scalar_transport(void* h, const double* phi, const double* gam, const double* sdiag,
+                                   const double* srhs, double urf, double* A, double* b) {
+  assemble_scalar_transport(*static_cast<Case*>(h), phi, gam, sdiag, srhs, urf, A, b);
 }
 void orc_update_mdot(void* h) { update_mdot(*static_cast<Case*>(h)); }
 void orc_update_div(void* h) { update_div(*static_cast<Case*>(h)); }

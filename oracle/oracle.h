@@ -82,6 +82,10 @@ void orc_initialize(void* h);
 void orc_assemble_momentum(void* h, double* A, double* b);
 /* pressure-correction system incl. reference-pressure row */
 void orc_assemble_pcorr(void* h, double* A, double* b);
+/* k / omega transport system (phiAssemblerElemTerms.hpp:11-413, upwind,
+ * zero-gradient walls) with per-node source terms and relaxation 1/urf. */
+void orc_assemble_scalar_transport(void* h, const double* phi, const double* gam, const double* sdiag,
+                                   const double* srhs, double urf, double* A, double* b);
 void orc_update_mdot(void* h);
 void orc_update_div(void* h);
 void orc_update_grad_p(void* h);

@@ -140,6 +140,8 @@ def lib():
             getattr(L, name).argtypes = [C.c_void_p]
         L.orc_assemble_momentum.argtypes = [C.c_void_p, dp, dp]
         L.orc_assemble_pcorr.argtypes = [C.c_void_p, dp, dp]
+        L.orc_assemble_scalar_transport.restype = None
+        L.orc_assemble_scalar_transport.argtypes = [C.c_void_p, dp, dp, dp, dp, C.c_double, dp, dp]
         L.orc_bicgstab.restype = C.c_int
         L.orc_bicgstab.argtypes = [C.c_void_p, C.c_int, dp, dp, dp, C.c_double, C.c_int, dp]
         L.orc_simple_iteration.argtypes = [C.c_void_p, P(IterStats)]
@@ -254,6 +256,15 @@ class FlowCase:
         A = np.zeros(self.nnz)
         b = np.zeros(self.mesh.nn)
         lib().orc_assemble_pcorr(self.h, _dp(A), _dp(b))
+        return A, b
+
+    def assemble_transport(self, phi, gamma, src_diag, src_rhs, urf):
+        """k / omega transport system of a nodal field phi with nodal diffusivity
+        gamma, per-node source terms and diagonal relaxation 1/urf."""
+        arrs = [np.ascontiguousarray(a, np.float64) for a in (phi, gamma, src_diag, src_rhs)]
+        A = np.zeros(self.nnz)
+        b = np.zeros(self.mesh.nn)
+        lib().orc_assemble_scalar_transport(self.h, *[_dp(a) for a in arrs], float(urf), _dp(A), _dp(b))
         return A, b
 
     def update_mdot(self):

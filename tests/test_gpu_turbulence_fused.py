@@ -1,0 +1,102 @@
+"""Fused u/v/w/k/omega assembly (oa_flow_enable_turbulence): one launch of
+the momentum kernel assembles the momentum system and the k and omega
+transport systems from the same ip geometry. Parity against the oracle's
+restatement of phiAssemblerElemTerms.hpp (upwind, nodal diffusivities at the
+ips, zero-gradient walls) plus the node source terms and the relaxation of the
+diagonal: 1e-12 in FP64, 1e-5 in the mixed form; the momentum system is the
+one the plain kernel assembles."""
+import numpy as np
+import pytest
+
+from openaccel_b200 import meshgen
+from openaccel_b200 import runtime as rt
+
+pytestmark = pytest.mark.gpu
+
+
+def rel(a, b):
+    d = np.linalg.norm(np.asarray(a) - np.asarray(b))
+    n = np.linalg.norm(np.asarray(b))
+    return d / n if n > 0 else d
+
+
+def setup(oracle_mod, m, prec, seed=4, **kw):
+    U0 = meshgen.initial_velocity(m, sigma=0.1, seed=seed)
+    oc = oracle_mod.FlowCase(m, oracle_mod.default_settings(**kw), U0=U0)
+    gf = rt.Flow(rt.Mesh(m), rt.default_settings(precision=prec, **kw))
+    gf.set_field("U", U0)
+    rng = np.random.default_rng(seed)
+    state = {"p": rng.normal(0, 1, m.nn), "gradP": rng.normal(0, 1, 3 * m.nn),
+             "du": rng.uniform(0.1, 1.0, 3 * m.nn), "mDot": rng.normal(0, 0.01, 12 * m.ne),
+             "div": rng.normal(0, 1e-3, m.nn)}
+    for k, v in state.items():
+        oc.field(k)[:] = v
+        gf.set_field(k, v)
+    turb = {"k": rng.uniform(1e-4, 1e-2, m.nn), "omega": rng.uniform(10.0, 1e3, m.nn),
+            "gammaK": rng.uniform(1e-3, 2e-2, m.nn), "gammaOmega": rng.uniform(1e-3, 2e-2, m.nn),
+            "srcDiagK": rng.uniform(0.0, 1e-3, m.nn), "srcRhsK": rng.normal(0, 1e-5, m.nn),
+            "srcDiagOmega": rng.uniform(0.0, 1e-2, m.nn), "srcRhsOmega": rng.normal(0, 1e-2, m.nn)}
+    return oc, gf, turb
+
+
+@pytest.mark.parametrize("prec,mesh", [(rt.OA_PREC_FP64, "cavity"), (rt.OA_PREC_MIXED, "cavity"),
+                                       (rt.OA_PREC_FP64, "star5")])
+def test_fused_assembly_parity(oracle_mod, prec, mesh):
+    m = meshgen.cavity(7, perturb=0.2, seed=8) if mesh == "cavity" else meshgen.star_prism(5, 4, 3, perturb=0.2)
+    oc, gf, turb = setup(oracle_mod, m, prec)
+    A_plain, b_plain = gf.assemble_momentum()
+    urf_k, urf_w = 0.8, 0.7
+    gf.enable_turbulence(urf_k, urf_w)
+    for k, v in turb.items():
+        gf.set_field(k, v)
+    A_m, b_m = gf.assemble_momentum()
+    # the momentum system is unchanged by the fusion
+    np.testing.assert_array_equal(A_m, A_plain)
+    np.testing.assert_array_equal(b_m, b_plain)
+    A_k, b_k, A_w, b_w = gf.turbulence_systems()
+    Ak_o, bk_o = oc.assemble_transport(turb["k"], turb["gammaK"], turb["srcDiagK"], turb["srcRhsK"], urf_k)
+    Aw_o, bw_o = oc.assemble_transport(turb["omega"], turb["gammaOmega"], turb["srcDiagOmega"],
+                                       turb["srcRhsOmega"], urf_w)
+    tol = 1e-12 if prec == rt.OA_PREC_FP64 else 1e-5
+    assert rel(A_k, Ak_o) < tol and rel(b_k, bk_o) < tol
+    assert rel(A_w, Aw_o) < tol and rel(b_w, bw_o) < tol
+
+
+def test_fused_assembly_inside_simple_iterations(oracle_mod):
+    # the systems follow the flow's state: after iterations (graph mode), the
+    # fused launch's k/omega systems match the oracle on the flow's mass flows
+    m = meshgen.cavity(6, perturb=0.2, seed=2)
+    oc, gf, turb = setup(oracle_mod, m, rt.OA_PREC_FP64)
+    gf2 = rt.Flow(rt.Mesh(m), rt.default_settings(use_graphs=2))
+    gf2.set_field("U", meshgen.initial_velocity(m, sigma=0.1, seed=4))
+    gf2.initialize()
+    gf2.enable_turbulence(0.9, 0.9)
+    for k, v in turb.items():
+        gf2.set_field(k, v)
+    gf2.simple_iterate(3)
+    A_k, b_k, _, _ = gf2.turbulence_systems()
+    # the last assembly used the mass flow of the start of iteration 3; redo it
+    # on the current state and compare with the oracle on the same state
+    gf2.assemble_momentum()
+    A_k, b_k, A_w, b_w = gf2.turbulence_systems()
+    oc.field("mDot")[:] = gf2.get_field("mDot")
+    Ak_o, bk_o = oc.assemble_transport(turb["k"], turb["gammaK"], turb["srcDiagK"], turb["srcRhsK"], 0.9)
+    assert rel(A_k, Ak_o) < 1e-12 and rel(b_k, bk_o) < 1e-12
+
+
+def test_fused_assembly_errors():
+    m = meshgen.cavity(4)
+    f = rt.Flow(rt.Mesh(m), rt.default_settings())
+    with pytest.raises(rt.OpenAccelError) as ei:
+        f.turbulence_systems()
+    assert ei.value.status == 6
+    with pytest.raises(rt.OpenAccelError):
+        f.enable_turbulence(0.0, 0.5)
+    f.enable_turbulence(0.8, 0.8)
+    with pytest.raises(rt.OpenAccelError) as ei:
+        f.advance_time(rt.OA_TIME_BDF1, 0.1)
+    assert ei.value.status == 1
+    h = rt.Flow(rt.Mesh(m), rt.default_settings(hr=1))
+    with pytest.raises(rt.OpenAccelError) as ei:
+        h.enable_turbulence(0.8, 0.8)
+    assert ei.value.status == 1

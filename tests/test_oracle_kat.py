@@ -253,3 +253,26 @@ def test_blending_factor_known_answers(oracle_mod):
     c2.update_grad_u()
     c2.update_blending_u()
     np.testing.assert_allclose(c2.field("betaU"), 0.2, atol=1e-15)
+
+
+def test_transport_assembly_known_answers(oracle_mod):
+    """k / omega transport restatement: a constant field gives a zero rhs and
+    zero row sums before the node terms; the node terms then sit on the
+    diagonal and the rhs; relaxation divides the diagonal only."""
+    m = meshgen.cavity(4, perturb=0.2, seed=6)
+    c = oracle_mod.FlowCase(m, U0=meshgen.initial_velocity(m, sigma=0.1, seed=6))
+    c.initialize()
+    rng = np.random.default_rng(3)
+    gam = rng.uniform(0.01, 0.02, m.nn)
+    zero = np.zeros(m.nn)
+    A, b = c.assemble_transport(np.full(m.nn, 2.5), gam, zero, zero, 1.0)
+    rp, cols = c.graph()
+    scale = np.abs(A).max()
+    # advection of a constant: the rhs is -phi * (net outflow) = -phi * div
+    np.testing.assert_allclose(b, -2.5 * c.field("div"), atol=1e-14 * scale)
+    diag = np.array([A[rp[i] + np.searchsorted(cols[rp[i]:rp[i + 1]], i)] for i in range(m.nn)])
+    sd, sr = rng.uniform(0, 1e-3, m.nn), rng.normal(0, 1e-3, m.nn)
+    A2, b2 = c.assemble_transport(np.full(m.nn, 2.5), gam, sd, sr, 0.5)
+    diag2 = np.array([A2[rp[i] + np.searchsorted(cols[rp[i]:rp[i + 1]], i)] for i in range(m.nn)])
+    np.testing.assert_allclose(diag2, (diag + sd) / 0.5, rtol=1e-13)
+    np.testing.assert_allclose(b2, b + sr, atol=1e-14 * scale)
