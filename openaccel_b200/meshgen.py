@@ -158,6 +158,36 @@ def initial_velocity(mesh: HexMesh, sigma=0.0, seed=12345):
     return U
 
 
+def stretched_1d(n, ratio, length=1.0):
+    """n cells on [0, length], geometric growth `ratio` from both ends to the
+    middle (symmetric wall-normal stretching)."""
+    half = n // 2
+    w = ratio ** np.arange(half)
+    w = np.concatenate([w, w[::-1]]) if n % 2 == 0 else np.concatenate([w, [ratio ** half], w[::-1]])
+    x = np.concatenate([[0.0], np.cumsum(w)])
+    return length * x / x[-1]
+
+
+def channel(nx=256, ny=96, nz=96, ratio=1.05, length=(4.0, 1.0, 1.0), perturb=0.0, seed=3):
+    """Channel-shaped hex block: nx x ny x nz elements, x streamwise, y
+    wall-normal with geometric stretching `ratio` from both walls, z spanwise.
+    The engine's boundaries are no-slip walls (boundary 0 the y walls, boundary
+    1 the other four faces); the configuration's inlet / outlet / symmetry
+    conditions are not modelled, so this stands in for the channel's mesh and
+    sizes, not its boundary conditions."""
+    coords, conn = hex_block(nx, ny, nz, np.linspace(0.0, length[0], nx + 1), stretched_1d(ny, ratio, length[1]),
+                             np.linspace(0.0, length[2], nz + 1))
+    faces = block_faces(nx, ny, nz)
+    fe, fo, fb = [], [], []
+    for side, bnd in (("y-", 0), ("y+", 0), ("x-", 1), ("x+", 1), ("z-", 1), ("z+", 1)):
+        e, o = faces[side]
+        fe.append(e), fo.append(np.full_like(e, o)), fb.append(np.full_like(e, bnd))
+    bnd_velocity = np.zeros((2, 3), dtype=np.float64)
+    return HexMesh(nx, ny, nz, coords, conn, np.concatenate(fe).astype(np.int32),
+                   np.concatenate(fo).astype(np.int32), np.concatenate(fb).astype(np.int32), bnd_velocity,
+                   meta={"kind": "channel", "ratio": ratio})
+
+
 def star_prism(blocks=3, n=6, nz=6, radius=1.0, height=1.0, perturb=0.0, seed=7, lid_velocity=(1.0, 0.0, 0.0)):
     """A hex mesh that is not one block: a regular polygon with 2*blocks
     corners split into ``blocks`` quadrilaterals that meet at its centre, each
