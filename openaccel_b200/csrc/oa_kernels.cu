@@ -363,7 +363,7 @@ __device__ __forceinline__ void wall_face(const MomArgs& a, const TF (&x)[8][3],
 // VAR 0 is the steady upwind SIMPLE assembly with nothing else in its
 // register budget.
 template <int LPR, bool USH, bool UGSH, class TF, int VAR = 0>
-__global__ void __launch_bounds__(BLOCK, sizeof(TF) == 4 ? (VAR == 2 ? 2 : (UGSH ? 4 : 3)) : 1)
+__global__ void __launch_bounds__(BLOCK, sizeof(TF) == 4 ? (UGSH ? 4 : 3) : 1)
     k_momentum(MomArgs a) {
   constexpr bool EXT = VAR == 1;
   constexpr bool TURB = VAR == 2;
@@ -380,17 +380,17 @@ __global__ void __launch_bounds__(BLOCK, sizeof(TF) == 4 ? (VAR == 2 ? 2 : (UGSH
     nb[0][k] = nb[1][k] = nb[2][k] = TF(0);
   }
   rhs[0] = rhs[1] = rhs[2] = TF(0);
-  // turbulence transport (TURB): [0] k, [1] omega
-  TF tdiag[2] = {TF(0), TF(0)}, tnb[2][3] = {{TF(0), TF(0), TF(0)}, {TF(0), TF(0), TF(0)}}, trhs[2] = {TF(0), TF(0)};
+  // element corner nodes and coordinates in the lane's canonical frame (kept
+  // for the turbulence pass of the fused variant)
+  int nd[8];
+  TF x[8][3];
   if (e >= 0) {
     const uint32_t pw = perm_word(c);
     const uint32_t iw = ip_word(c);
-    int nd[8];
     // coordinates of the flux arithmetic: FP64 as gathered, or, in the mixed
     // form, the element's FP32 corner offsets from its corner 0 (the Jacobians
     // are translation invariant), one 16-byte load per corner, with U and mu
     // from the FP32 node copy (one 16-byte load per node)
-    TF x[8][3];
     TF Uc[8][3], mu[8];
     if constexpr (sizeof(TF) == 4) {
 #pragma unroll
@@ -422,17 +422,6 @@ __global__ void __launch_bounds__(BLOCK, sizeof(TF) == 4 ? (VAR == 2 ? 2 : (UGSH
         Uc[k][1] = TF(u[1]);
         Uc[k][2] = TF(u[2]);
         mu[k] = TF(__ldg(a.mu + nd[k]));
-      }
-    }
-    // k, omega and their diffusivities at the element's nodes
-    TF tph[2][8], tgam[2][8];
-    if constexpr (TURB) {
-#pragma unroll
-      for (int k = 0; k < 8; ++k) {
-        tph[0][k] = TF(__ldg(a.kf + nd[k]));
-        tph[1][k] = TF(__ldg(a.wf + nd[k]));
-        tgam[0][k] = TF(__ldg(a.gkf + nd[k]));
-        tgam[1][k] = TF(__ldg(a.gwf + nd[k]));
       }
     }
     int err = 0;
@@ -493,22 +482,6 @@ __global__ void __launch_bounds__(BLOCK, sizeof(TF) == 4 ? (VAR == 2 ? 2 : (UGSH
         diag[3 * i + i] += fl;
         nb[RS][3 * i + i] += fr;
       }
-      // turbulence transport: the same upwind advection; diffusivities at the
-      // ip with the velocity's shape functions
-      [[maybe_unused]] TF tgIp[2] = {TF(0), TF(0)};
-      if constexpr (TURB) {
-#pragma unroll
-        for (int t = 0; t < 2; ++t) {
-          StaticFor<0, 8>::run([&](auto nc) {
-            constexpr int n = decltype(nc)::value;
-            constexpr double N = shape_at<PV, n>();
-            if (N != 0.0) tgIp[t] += TF(N) * tgam[t][n];
-          });
-          trhs[t] -= tm * (tmd > 0 ? tph[t][0] : tph[t][R]);
-          tdiag[t] += fl;
-          tnb[t][RS] += fr;
-        }
-      }
       // viscous stress incl. transpose. Block of column n:
       //   -mu_ip (g_n . A) I - mu_ip A (x) g_n   (rows i, columns j: g_n,i A_j)
       // Its defect contribution summed over the eight columns is
@@ -540,26 +513,6 @@ __global__ void __launch_bounds__(BLOCK, sizeof(TF) == 4 ? (VAR == 2 ? 2 : (UGSH
       for (int i = 0; i < 3; ++i)
         rhs[i] += muIp * (G[i][0] * ax[0] + G[i][1] * ax[1] + G[i][2] * ax[2] + G[0][i] * ax[0] + G[1][i] * ax[1] +
                           G[2][i] * ax[2]);
-      if constexpr (TURB) {
-        // diffusion defect: rhs += Gamma_ip grad(phi)_ip . A
-#pragma unroll
-        for (int t = 0; t < 2; ++t) {
-          TF Gp[3] = {TF(0), TF(0), TF(0)};
-          StaticFor<0, 8>::run([&](auto nc) {
-            constexpr int n = decltype(nc)::value;
-            constexpr double d0 = dshape(n, 0, PG::s(0), PG::s(1), PG::s(2));
-            constexpr double d1 = dshape(n, 1, PG::s(0), PG::s(1), PG::s(2));
-            constexpr double d2 = dshape(n, 2, PG::s(0), PG::s(1), PG::s(2));
-            if (d0 != 0.0) Gp[0] += TF(d0) * tph[t][n];
-            if (d1 != 0.0) Gp[1] += TF(d1) * tph[t][n];
-            if (d2 != 0.0) Gp[2] += TF(d2) * tph[t][n];
-          });
-          TF gax = TF(0);
-#pragma unroll
-          for (int j = 0; j < 3; ++j) gax += (Gp[0] * J.s[0][j] + Gp[1] * J.s[1][j] + Gp[2] * J.s[2][j]) * ax[j];
-          trhs[t] += tgIp[t] * gax;
-        }
-      }
       StaticFor<1, 5>::run([&](auto nc) {
         constexpr int n = decltype(nc)::value;
         constexpr int sl = nb_slot(n);
@@ -574,14 +527,6 @@ __global__ void __launch_bounds__(BLOCK, sizeof(TF) == 4 ? (VAR == 2 ? 2 : (UGSH
               const TF fj = -muIp * g[i] * ax[j] + (i == j ? -muIp * ga : TF(0));
               nb[sl][3 * i + j] += fj;
               diag[3 * i + j] -= fj;
-            }
-          }
-          if constexpr (TURB) {
-#pragma unroll
-            for (int t = 0; t < 2; ++t) {
-              const TF ft = -tgIp[t] * ga;
-              tnb[t][sl] += ft;
-              tdiag[t] -= ft;
             }
           }
         }
@@ -659,6 +604,92 @@ __global__ void __launch_bounds__(BLOCK, sizeof(TF) == 4 ? (VAR == 2 ? 2 : (UGSH
   }
   write_row<9, TF, LPR>(row, rv, li, lane, diag, nb, a.m, static_cast<TF*>(a.A), sh_val + warp_base * 3 * 9, false);
   if constexpr (TURB) {
+    // Second pass over the lane's three ips for k and omega, after the momentum
+    // row is written (its accumulators are dead, so the pass fits the same
+    // register budget): the inverse Jacobian is formed again from the corner
+    // coordinates still held, the mass flow and area come back from L1/L2.
+    // Upwind advection with the momentum's mass flows; diffusion -Gamma_ip
+    // grad N . A with the diffusivities at the ip on the velocity's shape
+    // functions; [0] k, [1] omega.
+    TF tdiag[2] = {TF(0), TF(0)}, tnb[2][3] = {{TF(0), TF(0), TF(0)}, {TF(0), TF(0), TF(0)}};
+    TF trhs[2] = {TF(0), TF(0)};
+    if (e >= 0) {
+      const uint32_t iw = ip_word(c);
+      TF tph[2][8], tgam[2][8];
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        tph[0][k] = TF(__ldg(a.kf + nd[k]));
+        tph[1][k] = TF(__ldg(a.wf + nd[k]));
+        tgam[0][k] = TF(__ldg(a.gkf + nd[k]));
+        tgam[1][k] = TF(__ldg(a.gwf + nd[k]));
+      }
+      int err = 0;
+      StaticFor<0, 3>::run([&](auto qc) {
+        constexpr int q = decltype(qc)::value;
+        constexpr int IP = q == 0 ? 0 : (q == 1 ? 3 : 8);
+        constexpr int R = q == 0 ? 1 : (q == 1 ? 3 : 4);
+        constexpr int RS = nb_slot(R);
+        using PG = ScsPt<IP, UGSH>;
+        using PV = ScsPt<IP, USH>;
+        double Aip[3];
+        load_area(a.m, e, (iw >> (5 * q)) & 31, Aip);
+        const TF ax[3] = {TF(Aip[0]), TF(Aip[1]), TF(Aip[2])};
+        const int pk = (iw >> (5 * q)) & 31;
+        const double tmd = (pk & 1) ? -__ldg(a.mDot + 12 * e + (pk >> 1)) : __ldg(a.mDot + 12 * e + (pk >> 1));
+        const TF tm = TF(tmd);
+        const TF fl = TF(0.5) * (tm + fabs(tm));
+        const TF fr = TF(0.5) * (tm - fabs(tm));
+        const InvJacR<TF> J = inv_jacobian<PG, TF>(x, &err);
+        TF tgIp[2] = {TF(0), TF(0)};
+#pragma unroll
+        for (int t = 0; t < 2; ++t) {
+          StaticFor<0, 8>::run([&](auto nc) {
+            constexpr int n = decltype(nc)::value;
+            constexpr double N = shape_at<PV, n>();
+            if (N != 0.0) tgIp[t] += TF(N) * tgam[t][n];
+          });
+          trhs[t] -= tm * (tmd > 0 ? tph[t][0] : tph[t][R]);
+          tdiag[t] += fl;
+          tnb[t][RS] += fr;
+        }
+        {
+          // diffusion defect: rhs += Gamma_ip grad(phi)_ip . A
+#pragma unroll
+          for (int t = 0; t < 2; ++t) {
+            TF Gp[3] = {TF(0), TF(0), TF(0)};
+            StaticFor<0, 8>::run([&](auto nc) {
+              constexpr int n = decltype(nc)::value;
+              constexpr double d0 = dshape(n, 0, PG::s(0), PG::s(1), PG::s(2));
+              constexpr double d1 = dshape(n, 1, PG::s(0), PG::s(1), PG::s(2));
+              constexpr double d2 = dshape(n, 2, PG::s(0), PG::s(1), PG::s(2));
+              if (d0 != 0.0) Gp[0] += TF(d0) * tph[t][n];
+              if (d1 != 0.0) Gp[1] += TF(d1) * tph[t][n];
+              if (d2 != 0.0) Gp[2] += TF(d2) * tph[t][n];
+            });
+            TF gax = TF(0);
+#pragma unroll
+            for (int j = 0; j < 3; ++j) gax += (Gp[0] * J.s[0][j] + Gp[1] * J.s[1][j] + Gp[2] * J.s[2][j]) * ax[j];
+            trhs[t] += tgIp[t] * gax;
+          }
+        }
+        StaticFor<1, 5>::run([&](auto nc) {
+          constexpr int n = decltype(nc)::value;
+          constexpr int sl = nb_slot(n);
+          if (sl >= 0 && !grad_is_zero<PG, n>()) {
+            TF g[3];
+            grad_n<PG, n, TF>(J, g);
+            const TF ga = g[0] * ax[0] + g[1] * ax[1] + g[2] * ax[2];
+#pragma unroll
+            for (int t = 0; t < 2; ++t) {
+              const TF ft = -tgIp[t] * ga;
+              tnb[t][sl] += ft;
+              tdiag[t] -= ft;
+            }
+          }
+        });
+      });
+      if (err) a.err[0] = 1;
+    }
     // k and omega rows: node source terms (the SST node update's diagonal and
     // rhs), relaxation of the diagonal (phiAssembler.h:967-1006)
 #pragma unroll
