@@ -390,6 +390,13 @@ int oa_flow_enable_turbulence(oa_flow* f, double urf_k, double urf_omega);
  * CSR layout as the pressure correction); any pointer may be NULL.
  * OA_ERR_NOT_READY before oa_flow_enable_turbulence. */
 int oa_flow_turbulence_systems(oa_flow* f, double* A_k, double* b_k, double* A_omega, double* b_omega);
+/* Solve the k and omega systems of the last fused assembly to rtol (BiCGStab
+ * with Jacobi; FP32 inner iterations under FP64 refinement in the mixed form)
+ * and correct the fields as turbulentKineticEnergySSTEquation::solve /
+ * turbulentEddyFrequencySSTEquation::solve do (correctField_ with relaxation 1
+ * and the lower clip SMALL, src/equation/equation.h:204-286). Iteration counts
+ * may be NULL. OA_ERR_NOT_READY before oa_flow_enable_turbulence. */
+int oa_flow_solve_turbulence(oa_flow* f, double rtol, int maxit, int* iters_k, int* iters_omega);
 
 #ifdef __cplusplus
 }

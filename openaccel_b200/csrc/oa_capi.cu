@@ -31,6 +31,17 @@ int fail(int code, const std::string& msg) {
   return code;
 }
 
+// correctField_ with CLIP, relaxation 1 and no upper bound (src/equation/equation.h:204-286):
+// phi += x, and a value below lo becomes phi + (lo - phi)
+__global__ void k_correct_clip(int n, double* phi, const double* x, double lo) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double o = phi[i];
+  double v = o + 1.0 * x[i];
+  if (v < lo) v = o + 1.0 * (lo - o);
+  phi[i] = v;
+}
+
 __global__ void k_axpy(int n, double* y, const double* x, double a) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) y[i] += a * x[i];
@@ -109,6 +120,11 @@ struct oa_flow {
   double* hscal = nullptr;  // pinned
   IterGraph ig;
   int eager_iters = 0;      // outer iterations run without the whole-iteration graph
+  // k / omega solves of the fused turbulence assembly: Jacobi BiCGStab (FP32
+  // inner iterations under FP64 refinement in the mixed form), FP64 rhs and
+  // solution scratch
+  ScalarSolve tsolve;
+  double *t_b64 = nullptr, *t_x = nullptr;
 };
 
 namespace {
@@ -858,6 +874,9 @@ void oa_flow_destroy(oa_flow* H) {
     if (p) cudaFree(p);
   if (H->hscal) cudaFreeHost(H->hscal);
   H->ig.release();
+  H->tsolve.release();
+  if (H->t_b64) cudaFree(H->t_b64);
+  if (H->t_x) cudaFree(H->t_x);
   H->pc.release();
   H->mom64.release();
   H->mom32.release();
@@ -1128,6 +1147,40 @@ int oa_flow_turbulence_systems(oa_flow* H, double* A_k, double* b_k, double* A_o
   if (int s = copy_out_matrix(f, f.b_k, nn, b_k)) return s;
   if (int s = copy_out_matrix(f, f.A_w, nnz, A_omega)) return s;
   return copy_out_matrix(f, f.b_w, nn, b_omega);
+}
+
+int oa_flow_solve_turbulence(oa_flow* H, double rtol, int maxit, int* iters_k, int* iters_omega) {
+  if (!H || !(rtol > 0) || maxit <= 0) return fail(OA_ERR_ARG, "oa_flow_solve_turbulence: bad arguments");
+  Flow& f = H->f;
+  if (!f.turb) return fail(OA_ERR_NOT_READY, "oa_flow_solve_turbulence: turbulence transport not enabled");
+  const int nn = f.mesh->nn;
+  if (!H->t_b64) {
+    if (int s = dalloc(&H->t_b64, (size_t)nn)) return s;
+    if (int s = dalloc(&H->t_x, (size_t)nn)) return s;
+  }
+  const ScalarGraph g = pc_graph(*f.mesh);
+  constexpr double CLIP_LO = 2.220446049250313e-16;  // accel::SMALL, the reference's lower clip value
+  for (int t = 0; t < 2; ++t) {
+    const void* bt = t ? f.b_w : f.b_k;
+    if (mixed(f)) {
+      k_to_double<float><<<(nn + 255) / 256, 256, 0, f.stream>>>((size_t)nn, static_cast<const float*>(bt), H->t_b64);
+      count_launches(1);
+    } else {
+      OA_CUDA(cudaMemcpyAsync(H->t_b64, bt, sizeof(double) * nn, cudaMemcpyDeviceToDevice, f.stream));
+    }
+    int it = 0;
+    double res = 0.0;
+    if (int s = H->tsolve.solve(g, mixed(f), false, f.s.use_graphs != 0, t ? f.A_w : f.A_k, H->t_b64, H->t_x, rtol,
+                                maxit, &it, &res, nullptr, f.stream, t ? "omega" : "k"))
+      return s;
+    k_correct_clip<<<(nn + 255) / 256, 256, 0, f.stream>>>(nn, t ? f.wf : f.kf, H->t_x, CLIP_LO);
+    count_launches(1);
+    if (t == 0 && iters_k) *iters_k = it;
+    if (t == 1 && iters_omega) *iters_omega = it;
+  }
+  OA_CUDA(cudaGetLastError());
+  OA_CUDA(cudaStreamSynchronize(f.stream));
+  return OA_OK;
 }
 
 int oa_flow_set_tuning(oa_flow* H, const oa_tuning* t) {

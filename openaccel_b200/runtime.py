@@ -34,7 +34,7 @@ EXPORTS = [
     "oa_diffusion_field_device_ptr", "oa_diffusion_assemble", "oa_diffusion_solve", "oa_diffusion_step",
     "oa_diffusion_stream", "oa_diffusion_time_assembly", "oa_sst_default_constants", "oa_sst_node_update",
     "oa_flow_last_control", "oa_flow_scales", "oa_flow_advance_time", "oa_flow_autotune", "oa_flow_set_tuning",
-    "oa_flow_enable_turbulence", "oa_flow_turbulence_systems",
+    "oa_flow_enable_turbulence", "oa_flow_turbulence_systems", "oa_flow_solve_turbulence",
 ]
 
 OA_BND_FIXED_VALUE = 0
@@ -183,6 +183,7 @@ def lib():
         "oa_flow_set_tuning": (C.c_int, [vp, P(Tuning)]),
         "oa_flow_enable_turbulence": (C.c_int, [vp, C.c_double, C.c_double]),
         "oa_flow_turbulence_systems": (C.c_int, [vp, dp, dp, dp, dp]),
+        "oa_flow_solve_turbulence": (C.c_int, [vp, C.c_double, C.c_int, ip, ip]),
         "oa_flow_sync": (C.c_int, [vp]),
         "oa_flow_stream": (C.c_int, [vp, P(vp)]),
         "oa_launch_count": (C.c_int, [P(C.c_longlong)]),
@@ -364,6 +365,12 @@ class Flow:
         out = [np.zeros(nnz), np.zeros(nn), np.zeros(nnz), np.zeros(nn)]
         _check(lib().oa_flow_turbulence_systems(self.h, *[_dp(a) for a in out]))
         return tuple(out)
+
+    def solve_turbulence(self, rtol=1e-8, maxit=500):
+        """Solve the k and omega systems of the last assembly and correct the fields."""
+        ik, iw = C.c_int(), C.c_int()
+        _check(lib().oa_flow_solve_turbulence(self.h, float(rtol), int(maxit), C.byref(ik), C.byref(iw)))
+        return ik.value, iw.value
 
     def autotune(self, iters=3):
         """Tune launch shapes and the pressure-solve schedule; the flow state is

@@ -100,3 +100,32 @@ def test_fused_assembly_errors():
     with pytest.raises(rt.OpenAccelError) as ei:
         h.enable_turbulence(0.8, 0.8)
     assert ei.value.status == 1
+
+
+@pytest.mark.parametrize("prec", [rt.OA_PREC_FP64, rt.OA_PREC_MIXED])
+def test_turbulence_solve_and_clipped_correction(oracle_mod, prec):
+    # the k and omega systems solved tightly and the corrections applied with
+    # the reference's lower clip: new = old + x, or old + (SMALL - old) below it
+    m = meshgen.cavity(7, perturb=0.2, seed=5)
+    oc, gf, turb = setup(oracle_mod, m, prec, seed=5)
+    turb["srcRhsK"] = turb["srcRhsK"] - 1e-3  # drive some k below zero
+    gf.enable_turbulence(0.8, 0.7)
+    for k, v in turb.items():
+        gf.set_field(k, v)
+    gf.assemble_momentum()
+    ik, iw = gf.solve_turbulence(1e-12 if prec == rt.OA_PREC_FP64 else 1e-10, 2000)
+    assert ik > 0 and iw > 0
+    small = np.finfo(float).eps
+    for name, g, sd, sr, urf in (("k", "gammaK", "srcDiagK", "srcRhsK", 0.8),
+                                 ("omega", "gammaOmega", "srcDiagOmega", "srcRhsOmega", 0.7)):
+        A, b = oc.assemble_transport(turb[name], turb[g], turb[sd], turb[sr], urf)
+        x, _, res = oc.bicgstab(1, A, b, rtol=1e-13, maxit=5000)
+        old = turb[name]
+        new = old + x
+        low = new < small
+        new[low] = old[low] + (small - old[low])
+        got = gf.get_field(name)
+        tol = 1e-9 if prec == rt.OA_PREC_FP64 else 1e-5
+        assert rel(got, new) < tol, name
+        if name == "k":
+            assert low.any() and np.all(got[low] == pytest.approx(small, abs=1e-18))
