@@ -199,6 +199,7 @@ int ScalarSolve::solve(const ScalarGraph& g, bool mixed, bool amg, bool graphs, 
   int total = 0, nref = 0;
   double rel = bnorm > 0 ? 1.0 : 0.0;
   OA_CUDA(cudaMemcpyAsync(r, b, sizeof(double) * g.nn, cudaMemcpyDeviceToDevice, st));
+  const double floor0 = floor_default(amg);  // fixed for the whole solve, as in the graph form
   while (rel > rtol && total < maxit && nref < 40) {
     k_narrow<<<(g.nn + 255) / 256, 256, 0, st>>>(g.nn, r, r32);
     count_launches(1);
@@ -206,7 +207,7 @@ int ScalarSolve::solve(const ScalarGraph& g, bool mixed, bool amg, bool graphs, 
     int it = 0;
     double r_in = 0.0;
     // inner tolerance: enough digits for FP32 without stalling
-    const double inner = std::max(rtol / rel, inner_floor > 0 ? inner_floor : (amg ? 1e-4 : 2e-4));
+    const double inner = std::max(rtol / rel, floor0);
     if (int s = k32.solve<float>(A32, r32, d, std::min(inner, 0.1), std::min(INNER_CAP, maxit - total), &it, &r_in,
                                  check_every, reuse || nref > 0))
       return s;
@@ -323,7 +324,7 @@ int ScalarSolve::emit(GraphBuild& gb, cudaGraph_t g, Deps& d, const ScalarGraph&
   }
   // mixed: FP64 iterative refinement around FP32 inner solves
   const float* A32 = static_cast<const float*>(A);
-  const double floor = inner_floor > 0 ? inner_floor : (amg ? 1e-4 : 2e-4);
+  const double floor = floor_default(amg);
   cudaGraphConditionalHandle hir;
   if (int s = gb.handle(g, &hir)) return s;
   if (int s = gb.seg(g, d, -1, [&]() -> int {
