@@ -129,3 +129,44 @@ def test_turbulence_solve_and_clipped_correction(oracle_mod, prec):
         assert rel(got, new) < tol, name
         if name == "k":
             assert low.any() and np.all(got[low] == pytest.approx(small, abs=1e-18))
+
+
+def test_sst_node_update_feeds_the_fused_assembly(oracle_mod):
+    # the SST node kernel writes the k and omega node terms straight into the
+    # flow's source fields (device pointers), reading k and omega from the
+    # flow's own fields; the next fused assembly carries them
+    import torch
+
+    m = meshgen.cavity(6, perturb=0.2, seed=9)
+    oc, gf, turb = setup(oracle_mod, m, rt.OA_PREC_FP64, seed=9)
+    gf.enable_turbulence(0.9, 0.9)
+    for k in ("k", "omega", "gammaK", "gammaOmega"):
+        gf.set_field(k, turb[k])
+    rng = np.random.default_rng(2)
+    dev = torch.device("cuda")
+    t = {"k_prev": torch.from_numpy(turb["k"]).to(dev), "rho": torch.ones(m.nn, dtype=torch.float64, device=dev),
+         "mu": torch.full((m.nn,), 1e-2, dtype=torch.float64, device=dev),
+         "ymin": torch.from_numpy(rng.uniform(1e-3, 0.5, m.nn)).to(dev),
+         "gradU": torch.from_numpy(rng.normal(0, 1, 9 * m.nn)).to(dev),
+         "gradK": torch.from_numpy(rng.normal(0, 1e-3, 3 * m.nn)).to(dev),
+         "gradW": torch.from_numpy(rng.normal(0, 10, 3 * m.nn)).to(dev),
+         "div": torch.zeros(m.nn, dtype=torch.float64, device=dev),
+         "vol": torch.full((m.nn,), 1.0 / m.nn, dtype=torch.float64, device=dev),
+         "mut_old": torch.zeros(m.nn, dtype=torch.float64, device=dev),
+         "wall_node": torch.zeros(m.nn, dtype=torch.int32, device=dev)}
+    for n in ("mut", "F1", "Pk"):
+        t[n] = torch.empty(m.nn, dtype=torch.float64, device=dev)
+    ptrs = {n: v.data_ptr() for n, v in t.items()}
+    ptrs.update(k=gf.device_ptr("k"), omega=gf.device_ptr("omega"), k_diag=gf.device_ptr("srcDiagK"),
+                k_rhs=gf.device_ptr("srcRhsK"), w_diag=gf.device_ptr("srcDiagOmega"),
+                w_rhs=gf.device_ptr("srcRhsOmega"))
+    rt.sst_node_update(m.nn, ptrs)
+    torch.cuda.synchronize()
+    src = {n: gf.get_field(n) for n in ("srcDiagK", "srcRhsK", "srcDiagOmega", "srcRhsOmega")}
+    assert np.all(src["srcDiagK"] > 0) and np.any(src["srcRhsK"] != 0)
+    gf.assemble_momentum()
+    A_k, b_k, A_w, b_w = gf.turbulence_systems()
+    Ak_o, bk_o = oc.assemble_transport(turb["k"], turb["gammaK"], src["srcDiagK"], src["srcRhsK"], 0.9)
+    Aw_o, bw_o = oc.assemble_transport(turb["omega"], turb["gammaOmega"], src["srcDiagOmega"], src["srcRhsOmega"], 0.9)
+    assert rel(A_k, Ak_o) < 1e-12 and rel(b_k, bk_o) < 1e-12
+    assert rel(A_w, Aw_o) < 1e-12 and rel(b_w, bw_o) < 1e-12
