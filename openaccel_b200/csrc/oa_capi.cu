@@ -954,6 +954,34 @@ int oa_flow_set_reference_nodes(oa_flow* H, const int* nodes, int count) {
   }
   OA_CUDA(cudaMemcpyAsync(f.ref_flag, flag.data(), f.mesh->nn, cudaMemcpyHostToDevice, f.stream));
   OA_CUDA(cudaStreamSynchronize(f.stream));
+  // closed domains of a batched (disjoint-union) mesh: the connected
+  // components of the stencil graph, numbered by their first node; the
+  // pressure-correction solve then converges when each of them does
+  const DeviceMesh& m = *f.mesh;
+  std::vector<int> comp(m.nn, -1), order;
+  order.reserve(m.nn);
+  std::vector<int> ptr(1, 0);
+  for (int r0 = 0; r0 < m.nn; ++r0) {
+    if (comp[r0] >= 0) continue;
+    const int c = (int)ptr.size() - 1;
+    const size_t first = order.size();
+    comp[r0] = c;
+    order.push_back(r0);
+    for (size_t q = first; q < order.size(); ++q) {
+      const int i = order[q];
+      for (int k = m.h_row_ptr[i]; k < m.h_row_ptr[i + 1]; ++k) {
+        const int j = m.h_cols[k];
+        if (comp[j] < 0) {
+          comp[j] = c;
+          order.push_back(j);
+        }
+      }
+    }
+    std::sort(order.begin() + first, order.end());
+    ptr.push_back((int)order.size());
+  }
+  if (int s = H->pc.set_segments(ptr, order)) return s;
+  H->ig.drop();  // the captured solve loops carry the segment tests
   return OA_OK;
 }
 

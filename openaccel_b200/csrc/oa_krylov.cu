@@ -244,12 +244,61 @@ __global__ void __launch_bounds__(KB) k_x_update(int n, TV* x, TV* r, const TV* 
   block_reduce_store<2>(v, partials, MAX_PARTIALS);
 }
 
-// rho <- rho1; rho1 <- rh.r; convergence test
-__global__ void __launch_bounds__(KB) k_end_iter(KScal* sc, const double* partials, int nb) {
+// Largest sqrt(r2[s] / b2[s]) over the segments (0 where b2 = 0), by the
+// whole block; 0 when nseg <= 1.
+__device__ __forceinline__ double block_seg_max(const double* r2, const double* b2, int nseg) {
+  __shared__ double sm[KB];
+  double m = 0.0;
+  if (nseg > 1)
+    for (int q = threadIdx.x; q < nseg; q += KB) {
+      const double b = b2[q];
+      if (b > 0.0) m = fmax(m, sqrt(r2[q] / b));
+    }
+  sm[threadIdx.x] = m;
+  __syncthreads();
+  for (int st = KB / 2; st > 0; st >>= 1) {
+    if (threadIdx.x < st) sm[threadIdx.x] = fmax(sm[threadIdx.x], sm[threadIdx.x + st]);
+    __syncthreads();
+  }
+  return sm[0];
+}
+
+// per-segment sums of squares, one block per segment, fixed-order tree
+template <class T>
+__global__ void __launch_bounds__(KB) k_seg_sumsq(const int* __restrict__ ptr, const int* __restrict__ rows,
+                                                   const T* __restrict__ v, double* out, const int* done) {
+  if (done && *done) return;
+  __shared__ double sm[KB];
+  const int sg = blockIdx.x;
+  double a = 0.0;
+  for (int q = ptr[sg] + threadIdx.x; q < ptr[sg + 1]; q += KB) {
+    const double x = double(v[rows[q]]);
+    a += x * x;
+  }
+  sm[threadIdx.x] = a;
+  __syncthreads();
+  for (int st = KB / 2; st > 0; st >>= 1) {
+    if (threadIdx.x < st) sm[threadIdx.x] += sm[threadIdx.x + st];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[sg] = sm[0];
+}
+
+__global__ void __launch_bounds__(KB) k_seg_max_ratio(const double* r2, const double* b2, int nseg, double* out) {
+  const double m = block_seg_max(r2, b2, nseg);
+  if (threadIdx.x == 0) *out = m;
+}
+
+// rho <- rho1; rho1 <- rh.r; convergence test (per segment for batched systems)
+__global__ void __launch_bounds__(KB) k_end_iter(KScal* sc, const double* partials, int nb, const double* seg_r2,
+                                                  const double* seg_b2, int nseg) {
   if (sc->done) return;
   double o[2];
   final_reduce<2>(partials, nb, o);
+  const double segmax = block_seg_max(seg_r2, seg_b2, nseg);
   if (threadIdx.x == 0) {
+    sc->seg_rel = segmax;
+    const bool conv = nseg > 1 ? segmax <= sc->rtol : false;
     sc->rho = sc->d0;
     sc->d0 = o[1];
     sc->rnorm = sqrt(o[0]);
@@ -260,7 +309,7 @@ __global__ void __launch_bounds__(KB) k_end_iter(KScal* sc, const double* partia
     } else if (sc->rnorm > 1e3 * sc->bnorm) {
       sc->done = 1;  // diverging (seen with FP32 vectors on stiff systems)
       sc->status = 3;
-    } else if (sc->rnorm <= sc->rtol * sc->bnorm || sc->iters >= sc->maxit) {
+    } else if ((nseg > 1 ? conv : sc->rnorm <= sc->rtol * sc->bnorm) || sc->iters >= sc->maxit) {
       sc->done = 1;
     } else if (sc->omega == 0.0 || sc->d0 == 0.0) {
       sc->done = 1;
@@ -366,18 +415,21 @@ __global__ void __launch_bounds__(KB) k_gcr_update(int n, TV* x, TV* r, const TV
 // where it was (truncated GCR can stagnate when the preconditioned operator's
 // symmetric part is not definite) ends the solve with status 1, and the
 // caller falls back to BiCGStab
-__global__ void __launch_bounds__(KB) k_gcr_end(KScal* sc, const double* partials, int nb) {
+__global__ void __launch_bounds__(KB) k_gcr_end(KScal* sc, const double* partials, int nb, const double* seg_r2,
+                                                 const double* seg_b2, int nseg) {
   if (sc->done) return;
   double o[1];
   final_reduce<1>(partials, nb, o);
+  const double segmax = block_seg_max(seg_r2, seg_b2, nseg);
   if (threadIdx.x == 0) {
+    sc->seg_rel = segmax;
     const double prev = sc->rnorm;
     sc->rnorm = sqrt(o[0]);
     sc->iters += 1;
     if (!(sc->rnorm < INFINITY)) {
       sc->done = 1;
       sc->status = 2;
-    } else if (sc->rnorm <= sc->rtol * sc->bnorm || sc->iters >= sc->maxit) {
+    } else if ((nseg > 1 ? segmax <= sc->rtol : sc->rnorm <= sc->rtol * sc->bnorm) || sc->iters >= sc->maxit) {
       sc->done = 1;
     } else if (sc->rnorm > 0.9999 * prev) {
       sc->done = 1;
@@ -493,6 +545,10 @@ int KrylovSolver<B, TM, TV>::prologue(const TM* A, const TB* b, double rtol, int
   k_init<TV, TB><<<gv, KB, 0, st>>>(n, b, x, r, rh, p, v, partials);
   k_init_scalars<<<1, KB, 0, st>>>(sc, partials, gv, rtol, maxit, rtol_dev, maxit_dev);
   count_launches(3);
+  if (seg.on()) {
+    k_seg_sumsq<TB><<<seg.nseg, KB, 0, st>>>(seg.ptr, seg.rows, b, seg.b2, nullptr);
+    count_launches(1);
+  }
   OA_CUDA(cudaGetLastError());
   if (use_gcr)
     for (int k = 4; k < 8; ++k) OA_CUDA(cudaMemsetAsync(vec[k], 0, sizeof(TV) * (size_t)n, st));
@@ -521,7 +577,11 @@ int KrylovSolver<B, TM, TV>::chunk(const TM* A, int check_every, bool use_gcr) {
       k_gcr_orth<TV><<<gv, KB, 0, st>>>(n, gz, gq, gP[0], gP[1], gQ[0], gQ[1], r, partials, sc);
       k_gcr_alpha<<<1, KB, 0, st>>>(sc, partials, gv);
       k_gcr_update<TV><<<gv, KB, 0, st>>>(n, x, r, gz, gq, gP[slot], gQ[slot], partials, sc);
-      k_gcr_end<<<1, KB, 0, st>>>(sc, partials, gv);
+      if (seg.on()) {
+        k_seg_sumsq<TV><<<seg.nseg, KB, 0, st>>>(seg.ptr, seg.rows, r, seg.r2, &sc->done);
+        count_launches(1);
+      }
+      k_gcr_end<<<1, KB, 0, st>>>(sc, partials, gv, seg.r2, seg.b2, seg.on() ? seg.nseg : 0);
     }
     count_launches(6L * check_every);
     OA_CUDA(cudaGetLastError());
@@ -537,7 +597,11 @@ int KrylovSolver<B, TM, TV>::chunk(const TM* A, int check_every, bool use_gcr) {
     k_spmv<B, TM, TV, 2><<<gv, KB, 0, st>>>(nn, rp, cols, A, sh, t, r, nullptr, partials, sc);
     k_omega<<<1, KB, 0, st>>>(sc, partials, gv);
     k_x_update<TV><<<gv, KB, 0, st>>>(n, x, r, ph, sh, t, rh, partials, sc);
-    k_end_iter<<<1, KB, 0, st>>>(sc, partials, gv);
+    if (seg.on()) {
+      k_seg_sumsq<TV><<<seg.nseg, KB, 0, st>>>(seg.ptr, seg.rows, r, seg.r2, &sc->done);
+      count_launches(1);
+    }
+    k_end_iter<<<1, KB, 0, st>>>(sc, partials, gv, seg.r2, seg.b2, seg.on() ? seg.nseg : 0);
   }
   count_launches(8L * check_every);
   OA_CUDA(cudaGetLastError());
@@ -607,7 +671,7 @@ int KrylovSolver<B, TM, TV>::solve(const TM* A, const TB* b, TV*& xout, double r
   const KScal* h = static_cast<const KScal*>(hscal ? hscal : static_cast<void*>(hbuf));
   static_assert(sizeof(KScal) <= sizeof(hbuf), "host staging buffer too small");
   if (iters) *iters = h->iters;
-  if (res) *res = h->bnorm > 0 ? h->rnorm / h->bnorm : 0.0;
+  if (res) *res = seg.on() ? h->seg_rel : (h->bnorm > 0 ? h->rnorm / h->bnorm : 0.0);
   xout = static_cast<TV*>(vec[0]);
   last_status = h->status;
   if (dbg) {
@@ -782,6 +846,24 @@ int add_correction(int n, double* x, const TV* d, cudaStream_t st) {
 }
 template int add_correction<float>(int, double*, const float*, cudaStream_t);
 template int add_correction<double>(int, double*, const double*, cudaStream_t);
+
+template <class T>
+int segment_sumsq(const Segments& sg, const T* v, double* out, cudaStream_t st) {
+  if (!sg.on()) return OA_OK;
+  k_seg_sumsq<T><<<sg.nseg, KB, 0, st>>>(sg.ptr, sg.rows, v, out, nullptr);
+  count_launches(1);
+  OA_CUDA(cudaGetLastError());
+  return OA_OK;
+}
+template int segment_sumsq<float>(const Segments&, const float*, double*, cudaStream_t);
+template int segment_sumsq<double>(const Segments&, const double*, double*, cudaStream_t);
+
+int segment_max_ratio(const Segments& sg, double* out, cudaStream_t st) {
+  k_seg_max_ratio<<<1, KB, 0, st>>>(sg.r2, sg.b2, sg.nseg, out);
+  count_launches(1);
+  OA_CUDA(cudaGetLastError());
+  return OA_OK;
+}
 
 // ---------------------------------------------------------------------------
 // Control kernels of the conditional nodes of whole-iteration graphs (one

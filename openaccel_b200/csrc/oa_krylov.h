@@ -14,7 +14,28 @@ struct KScal {
   double rtol;
   int maxit;
   int done, iters, status;
+  double seg_rel;  // segmented solves: largest per-segment ||r|| / ||b|| at the last test
 };
+
+// Independent systems solved as one (a batch of disjoint meshes): the rows of
+// each segment (seg_rows[seg_ptr[s] .. seg_ptr[s+1])) and scratch for the
+// per-segment sums of squares of b and r. With nseg > 1 a solve has converged
+// when every segment's ||r_s|| <= rtol ||b_s||, not when the whole batch's
+// norm is.
+struct Segments {
+  int nseg = 0;
+  const int* ptr = nullptr;
+  const int* rows = nullptr;
+  double* b2 = nullptr;  // [nseg]
+  double* r2 = nullptr;  // [nseg]
+  bool on() const { return nseg > 1; }
+};
+// per-segment sums of squares of v into out[nseg] (one block per segment,
+// fixed order)
+template <class T>
+int segment_sumsq(const Segments& sg, const T* v, double* out, cudaStream_t st);
+// largest sqrt(r2[s] / b2[s]) over segments (0 where b2 = 0) into *out
+int segment_max_ratio(const Segments& sg, double* out, cudaStream_t st);
 
 // BiCGStab on a BSR matrix with BxB blocks; matrix values TM, vectors TV.
 template <int B, class TM, class TV>
@@ -40,6 +61,8 @@ struct KrylovSolver {
   bool graph_gcr = false;
   long long graph_launches = 0;
 
+  // per-segment convergence (batched disjoint systems); off by default
+  Segments seg;
   // storage carved from caller memory instead of cudaMalloc (no allocation)
   bool external = false;
   alignas(16) unsigned char hbuf[128];  // host copy of the scalars when not pinned

@@ -42,8 +42,9 @@ __global__ void k_fallback_if(cudaGraphConditionalHandle h, const KScal* sc, Sca
 
 // mixed: entry of the refinement loop (||b|| from the reduction before it)
 __global__ void k_ir_begin(cudaGraphConditionalHandle h, ScalarGraphState* S, double rtol, int maxit, double floor,
-                           int use_gcr) {
+                           int use_gcr, int seg) {
   const double bn = sqrt(S->bsq);
+  S->seg = seg;
   S->bnorm = bn;
   S->rtol = rtol;
   S->maxit = maxit;
@@ -94,7 +95,8 @@ __global__ void k_add_correction_if(int n, double* x, const TV* d, const ScalarG
 // end of a pass: relative FP64 residual, loop condition
 __global__ void k_ir_next(cudaGraphConditionalHandle h, ScalarGraphState* S, BodyCounters* c, int body) {
   c->total[body] += 1;
-  const double rel = S->bnorm > 0 ? S->rnorm_out / S->bnorm : 0.0;
+  double rel = S->bnorm > 0 ? S->rnorm_out / S->bnorm : 0.0;
+  if (S->seg && rel < INFINITY) rel = S->rel_seg;  // the worst segment of a batch
   S->rel = rel;
   S->nref += 1;
   if (!(rel < INFINITY) && S->status == 0) S->status = 2;
@@ -120,6 +122,41 @@ int ScalarSolve::init(int nn) {
     return fail(OA_ERR_CUDA, "scalar solve: device allocation failed");
   }
   return OA_OK;
+}
+
+int ScalarSolve::set_segments(const std::vector<int>& ptr, const std::vector<int>& rows) {
+  release_segments();
+  const int nseg = (int)ptr.size() - 1;
+  if (nseg <= 1) return OA_OK;
+  if (cudaMalloc(&seg_dev, sizeof(int) * (ptr.size() + rows.size())) != cudaSuccess ||
+      cudaMalloc(&seg_buf, sizeof(double) * 4 * nseg) != cudaSuccess ||
+      cudaMalloc(&seg_rel, sizeof(double)) != cudaSuccess) {
+    release_segments();
+    return fail(OA_ERR_CUDA, "scalar solve: segment allocation failed");
+  }
+  OA_CUDA(cudaMemcpy(seg_dev, ptr.data(), sizeof(int) * ptr.size(), cudaMemcpyHostToDevice));
+  OA_CUDA(cudaMemcpy(seg_dev + ptr.size(), rows.data(), sizeof(int) * rows.size(), cudaMemcpyHostToDevice));
+  seg_in.nseg = seg_out.nseg = nseg;
+  seg_in.ptr = seg_out.ptr = seg_dev;
+  seg_in.rows = seg_out.rows = seg_dev + ptr.size();
+  seg_in.b2 = seg_buf;
+  seg_in.r2 = seg_buf + nseg;
+  seg_out.b2 = seg_buf + 2 * nseg;
+  seg_out.r2 = seg_buf + 3 * nseg;
+  return OA_OK;
+}
+
+void ScalarSolve::release_segments() {
+  if (seg_dev) cudaFree(seg_dev);
+  if (seg_buf) cudaFree(seg_buf);
+  if (seg_rel) cudaFree(seg_rel);
+  seg_dev = nullptr;
+  seg_buf = nullptr;
+  seg_rel = nullptr;
+  seg_in = Segments{};
+  seg_out = Segments{};
+  k64.seg = Segments{};
+  k32.seg = Segments{};
 }
 
 void ScalarSolve::release() {
@@ -162,6 +199,7 @@ int ScalarSolve::solve(const ScalarGraph& g, bool mixed, bool amg, bool graphs, 
     k32.amg = nullptr;
   }
   k64.use_graph = k32.use_graph = graphs;
+  k64.seg = k32.seg = seg_in;
   // with the AMG: GCR(2), one V-cycle per iteration (chunks of 4); with point
   // Jacobi: BiCGStab
   k64.gcr = k32.gcr = amg && gcr;
@@ -199,6 +237,8 @@ int ScalarSolve::solve(const ScalarGraph& g, bool mixed, bool amg, bool graphs, 
   int total = 0, nref = 0;
   double rel = bnorm > 0 ? 1.0 : 0.0;
   OA_CUDA(cudaMemcpyAsync(r, b, sizeof(double) * g.nn, cudaMemcpyDeviceToDevice, st));
+  if (seg_out.on())
+    if (int s = segment_sumsq<double>(seg_out, b, seg_out.b2, st)) return s;
   const double floor0 = floor_default(amg);  // fixed for the whole solve, as in the graph form
   while (rel > rtol && total < maxit && nref < 40) {
     k_narrow<<<(g.nn + 255) / 256, 256, 0, st>>>(g.nn, r, r32);
@@ -227,8 +267,15 @@ int ScalarSolve::solve(const ScalarGraph& g, bool mixed, bool amg, bool graphs, 
     if (k32.last_status != 3 && r_in < 1.0) add_correction<float>(g.nn, x, d, st);
     if (int s = fp64_residual<float>(g.nn, g.rp, g.cols, A32, x, b, r, k32.partials, scal + 1, st)) return s;
     OA_CUDA(cudaMemcpyAsync(hscal + 1, scal + 1, sizeof(double), cudaMemcpyDeviceToHost, st));
+    if (seg_out.on()) {
+      // batched disjoint systems: the worst segment's relative residual
+      if (int s = segment_sumsq<double>(seg_out, r, seg_out.r2, st)) return s;
+      if (int s = segment_max_ratio(seg_out, seg_rel, st)) return s;
+      OA_CUDA(cudaMemcpyAsync(hscal, seg_rel, sizeof(double), cudaMemcpyDeviceToHost, st));
+    }
     OA_CUDA(cudaStreamSynchronize(st));
-    rel = bnorm > 0 ? hscal[1] / bnorm : 0.0;
+    rel = seg_out.on() ? hscal[0] : (bnorm > 0 ? hscal[1] / bnorm : 0.0);
+    if (!(hscal[1] < INFINITY)) rel = hscal[1];
     if (std::getenv("OA_DEBUG"))
       std::fprintf(stderr, "[oa] %s refinement %d: inner iters %d inner res %.3e |b| %.3e rel %.3e\n", what, nref, it,
                    r_in, bnorm, rel);
@@ -256,6 +303,7 @@ int ScalarSolve::emit(GraphBuild& gb, cudaGraph_t g, Deps& d, const ScalarGraph&
   }
   k64.amg = amg && !mixed ? &amg64 : nullptr;
   k32.amg = amg && mixed ? &amg32 : nullptr;
+  k64.seg = k32.seg = seg_in;
   if (mixed) {
     if (int s = k32.setup(gr.nn, gr.rp, gr.cols, gr.diag, st)) return s;
   } else if (int s = k64.setup(gr.nn, gr.rp, gr.cols, gr.diag, st)) {
@@ -331,7 +379,9 @@ int ScalarSolve::emit(GraphBuild& gb, cudaGraph_t g, Deps& d, const ScalarGraph&
         OA_CUDA(cudaMemsetAsync(x, 0, sizeof(double) * gr.nn, st));
         if (int s2 = device_sumsq(gr.nn, b, &gs->bsq, partials, st)) return s2;
         OA_CUDA(cudaMemcpyAsync(r, b, sizeof(double) * gr.nn, cudaMemcpyDeviceToDevice, st));
-        k_ir_begin<<<1, 1, 0, st>>>(hir, gs, rtol, maxit, floor, use_gcr ? 1 : 0);
+        if (seg_out.on())
+          if (int s2 = segment_sumsq<double>(seg_out, b, seg_out.b2, st)) return s2;
+        k_ir_begin<<<1, 1, 0, st>>>(hir, gs, rtol, maxit, floor, use_gcr ? 1 : 0, seg_out.on() ? 1 : 0);
         count_launches(1);
         return OA_OK;
       }))
@@ -370,6 +420,10 @@ int ScalarSolve::emit(GraphBuild& gb, cudaGraph_t g, Deps& d, const ScalarGraph&
         count_launches(2);
         if (int s2 = fp64_residual<float>(gr.nn, gr.rp, gr.cols, A32, x, b, r, k32.partials, &gs->rnorm_out, st))
           return s2;
+        if (seg_out.on()) {
+          if (int s2 = segment_sumsq<double>(seg_out, r, seg_out.r2, st)) return s2;
+          if (int s2 = segment_max_ratio(seg_out, &gs->rel_seg, st)) return s2;
+        }
         k_ir_next<<<1, 1, 0, st>>>(hir, gs, gb.ctr, ir_body);
         count_launches(1);
         return OA_OK;
@@ -417,7 +471,7 @@ int ScalarSolve::graph_result(bool mixed, int* iters, double* res, int* refineme
   }
   if (K.status == 2) return fail(OA_ERR_SOLVER, std::string(what) + ": non-finite residual");
   if (iters) *iters = K.iters + S.spent;
-  if (res) *res = K.bnorm > 0 ? K.rnorm / K.bnorm : 0.0;
+  if (res) *res = seg_in.on() ? K.seg_rel : (K.bnorm > 0 ? K.rnorm / K.bnorm : 0.0);
   if (refinements) *refinements = 0;
   return OA_OK;
 }

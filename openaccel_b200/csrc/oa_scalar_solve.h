@@ -3,6 +3,8 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <vector>
+
 #include "oa_amg.h"
 #include "oa_krylov.h"
 
@@ -22,6 +24,8 @@ struct ScalarGraphState {
   double bsq, bnorm, rel, rtol, floor, inner_rtol, r_in, rnorm_out;
   int maxit, total, nref, inner_maxit, use_gcr, fallback, status, it_last, apply;
   int refresh_ctr, refresh, spent;
+  int seg;         // per-segment convergence (batched disjoint systems)
+  double rel_seg;  // largest per-segment ||r|| / ||b|| of the FP64 residual
 };
 
 // FP64: BiCGStab (AMG- or Jacobi-preconditioned) to rtol. Mixed: iterative
@@ -80,6 +84,15 @@ struct ScalarSolve {
   ScalarGraphState* gs_host = nullptr;  // pinned mirror, written by the graph's last nodes
   KScal* k_host = nullptr;              // pinned mirror of the FP64 solver's scalars
 
+  // disjoint systems solved as one: a solve converges when every segment
+  // does (inner Krylov tests on seg_in, the refinement test on seg_out)
+  Segments seg_in, seg_out;
+  int* seg_dev = nullptr;      // [nseg + 1 + nn] row pointers and rows
+  double* seg_buf = nullptr;   // [4 nseg] sums of squares
+  double* seg_rel = nullptr;   // device scalar: refinement's largest segment ratio
+  int set_segments(const std::vector<int>& ptr, const std::vector<int>& rows);
+  void release_segments();
+
   int init(int n);
   // A: const double* (mixed = false) or const float* (mixed = true); b and x
   // FP64 device vectors of g.nn; x is overwritten. refinements may be null.
@@ -98,7 +111,10 @@ struct ScalarSolve {
   // counter takes the host's solve count (which a caller may have reset)
   int graph_prepare(cudaStream_t st);
   void release();
-  ~ScalarSolve() { release(); }
+  ~ScalarSolve() {
+    release();
+    release_segments();
+  }
 };
 
 }  // namespace oa
