@@ -1153,14 +1153,18 @@ int oa_flow_enable_turbulence(oa_flow* H, double urf_k, double urf_omega) {
   const size_t nn = f.mesh->nn, nnz = f.mesh->nnz;
   const size_t ws = mixed(f) ? sizeof(float) : sizeof(double);
   double** fields[] = {&f.kf, &f.wf, &f.gkf, &f.gwf, &f.sdk, &f.srk, &f.sdw, &f.srw};
+  // a retry after a failed allocation keeps what the first attempt got
   for (double** p : fields) {
+    if (*p) continue;
     if (int s = dalloc(p, nn)) return s;
     OA_CUDA(cudaMemset(*p, 0, sizeof(double) * nn));
   }
   void** sys[] = {&f.A_k, &f.A_w};
-  for (void** p : sys) OA_CUDA(cudaMalloc(p, ws * (nnz ? nnz : 1)));
+  for (void** p : sys)
+    if (!*p) OA_CUDA(cudaMalloc(p, ws * (nnz ? nnz : 1)));
   void** rhs[] = {&f.b_k, &f.b_w};
-  for (void** p : rhs) OA_CUDA(cudaMalloc(p, ws * (nn ? nn : 1)));
+  for (void** p : rhs)
+    if (!*p) OA_CUDA(cudaMalloc(p, ws * (nn ? nn : 1)));
   f.turb = true;
   H->ig.drop();
   return OA_OK;
