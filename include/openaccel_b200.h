@@ -216,8 +216,10 @@ int oa_flow_advance_time(oa_flow* f, int scheme, double dt);
  * the threads per block of the row kernels without shared memory (gradients,
  * divergence, blending factor), of the element-owner mass-flow kernel and of
  * the assembly row kernels (each 32, 64 or 128), the GCR(2) iterations per
- * device-resident chunk (2 or 4) and the AMG numeric refresh interval (4, 8 or
- * 16 solves), each candidate timed over `iters` SIMPLE outer iterations (CUDA
+ * device-resident chunk (2 or 4), the AMG numeric refresh interval (4, 8 or
+ * 16 solves), the degree of the AMG's coarse-level Chebyshev smoother (3 or 4)
+ * and its prolongation damping (0.74 or 0.85), each candidate timed over
+ * `iters` SIMPLE outer iterations (CUDA
  * events on the flow's stream, after one untimed iteration) from the same
  * saved state; the flow's fields are restored afterwards and the next
  * pressure solve rebuilds the AMG numeric phase. Block sizes do not change
@@ -226,6 +228,8 @@ typedef struct oa_tuning {
   int block_rows, block_elements, block_assembly;  /* threads per block */
   int gcr_chunk, amg_refresh;
   double ms_per_iteration_before, ms_per_iteration_after;
+  int amg_cheb_degree;            /* 2..6; 0 in oa_flow_set_tuning: keep the current one */
+  double amg_prolong_damping;     /* (0, 1.5); 0 in oa_flow_set_tuning: keep the current one */
 } oa_tuning;
 int oa_flow_autotune(oa_flow* f, int iters, oa_tuning* out);
 /* Apply a tuning found earlier (ms fields ignored). */

@@ -758,6 +758,19 @@ int Amg<T>::apply(const T* v, T* z, const int* done, cudaStream_t st) {
   return OA_OK;
 }
 
+template <class T>
+int Amg<T>::set_smoothing(int degree, double prolongation_damping) {
+  if (degree < 2 || degree > MAX_CHEB || !(prolongation_damping > 0.0 && prolongation_damping < 1.5))
+    return fail(OA_ERR_ARG, "AMG: Chebyshev degree 2..6 and prolongation damping in (0, 1.5)");
+  omega_p = prolongation_damping;
+  if (!smoothed) return OA_OK;
+  cheb_degree = degree;
+  cheb_launches = 0;
+  for (const AmgLevel<T>& lv : L)
+    if (lv.cheb) cheb_launches += 2LL * (cheb_degree - 1);
+  return OA_OK;
+}
+
 template struct Amg<double>;
 template struct Amg<float>;
 

@@ -89,6 +89,10 @@ struct Amg {
   int numeric(const T* A_fine, cudaStream_t st);
   // z = M^-1 v (one V-cycle from zero initial guess); kernels return early when *done
   int apply(const T* v, T* z, const int* done, cudaStream_t st);
+  // Chebyshev degree of the coarse-level smoother and prolongation damping;
+  // before set-up they shape it, after it they take effect with the next
+  // numeric phase (degree) and apply (launch count)
+  int set_smoothing(int degree, double prolongation_damping);
   void release();
   ~Amg() { release(); }
 };

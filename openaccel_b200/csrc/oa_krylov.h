@@ -93,6 +93,11 @@ struct KrylovSolver {
            const double* rtol_dev, const int* maxit_dev, int maxit_cap, int check_every, bool gcr_mode,
            int branch_body);
   const KScal* scalars() const { return static_cast<const KScal*>(scal); }
+  // forget the captured chunk (its preconditioner launches changed)
+  void drop_graph() {
+    if (graph_exec) cudaGraphExecDestroy(graph_exec);
+    graph_exec = nullptr;
+  }
   TV* solution() const { return static_cast<TV*>(vec[0]); }
 
  private:

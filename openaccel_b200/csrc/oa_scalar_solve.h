@@ -93,6 +93,16 @@ struct ScalarSolve {
   int set_segments(const std::vector<int>& ptr, const std::vector<int>& rows);
   void release_segments();
 
+  // coarse-level Chebyshev degree and prolongation damping of both
+  // precisions' hierarchies (autotuned; defaults 3 and 0.74)
+  int set_smoothing(int degree, double prolongation_damping) {
+    if (int s = amg64.set_smoothing(degree, prolongation_damping)) return s;
+    if (int s = amg32.set_smoothing(degree, prolongation_damping)) return s;
+    k64.drop_graph();
+    k32.drop_graph();
+    return 0;
+  }
+
   int init(int n);
   // A: const double* (mixed = false) or const float* (mixed = true); b and x
   // FP64 device vectors of g.nn; x is overwritten. refinements may be null.

@@ -80,7 +80,8 @@ class Tuning(C.Structure):
     """oa_tuning: launch shapes and pressure-solve schedule chosen by oa_flow_autotune."""
     _fields_ = [("block_rows", C.c_int), ("block_elements", C.c_int), ("block_assembly", C.c_int),
                 ("gcr_chunk", C.c_int), ("amg_refresh", C.c_int), ("ms_per_iteration_before", C.c_double),
-                ("ms_per_iteration_after", C.c_double)]
+                ("ms_per_iteration_after", C.c_double), ("amg_cheb_degree", C.c_int),
+                ("amg_prolong_damping", C.c_double)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

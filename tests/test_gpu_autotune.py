@@ -27,6 +27,7 @@ def test_autotune_choices_and_state_restored():
     t = f.autotune(iters=2)
     assert t["block_rows"] in (32, 64, 128) and t["block_elements"] in (32, 64, 128)
     assert t["block_assembly"] in (32, 64, 128) and t["gcr_chunk"] in (2, 4) and t["amg_refresh"] in (4, 8, 16)
+    assert t["amg_cheb_degree"] in (3, 4) and t["amg_prolong_damping"] in (0.74, 0.85)
     assert 0 < t["ms_per_iteration_after"] <= t["ms_per_iteration_before"] * 1.0000001
     for k, v in before.items():
         np.testing.assert_array_equal(f.get_field(k), v)
@@ -44,3 +45,24 @@ def test_block_sizes_do_not_change_results():
     b.simple_iterate(3)
     for k in ("U", "p", "mDot"):
         np.testing.assert_array_equal(a.get_field(k), b.get_field(k))
+
+
+def test_amg_smoothing_tuning_changes_schedule_not_answers():
+    # a different Chebyshev degree / prolongation damping changes the V-cycle,
+    # hence the iterates within the solve tolerance, but not the converged
+    # answer; bad values are rejected
+    m = meshgen.cavity(12, perturb=0.2, seed=7)
+    U0 = meshgen.initial_velocity(m, sigma=0.1, seed=7)
+    kw = dict(mom_rtol=1e-12, pc_rtol=1e-12)
+    a = flow(m, U0, **kw)
+    b = flow(m, U0, **kw)
+    b.set_tuning(block_rows=128, block_elements=128, block_assembly=128, gcr_chunk=2, amg_refresh=8,
+                 amg_cheb_degree=4, amg_prolong_damping=0.85)
+    a.simple_iterate(3)
+    b.simple_iterate(3)
+    for k in ("U", "p"):
+        va, vb = a.get_field(k), b.get_field(k)
+        assert np.linalg.norm(va - vb) <= 1e-9 * np.linalg.norm(va)
+    with pytest.raises(rt.OpenAccelError):
+        b.set_tuning(block_rows=128, block_elements=128, block_assembly=128, gcr_chunk=2, amg_refresh=8,
+                     amg_cheb_degree=9)
