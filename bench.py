@@ -132,7 +132,7 @@ def run_ours(args, rank, world):
         f.initialize()
         if not args.no_autotune:
             # set-up, not timed: the flow's state is restored afterwards
-            tuning[prec] = f.autotune(iters=2)
+            tuning[prec] = f.autotune(iters=3)
         return f
 
     tuning = {}
