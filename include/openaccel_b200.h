@@ -163,7 +163,10 @@ int oa_flow_field_device_ptr(oa_flow* f, const char* name, double** dev);
  * closed domain of a batched (disjoint-union) mesh. Mirrors
  * domain::pressureLevelNodeId / adjustMatrixForPressureReference
  * (src/assemble/flow/segregatedFlow/pressureCorrectionAssembler/pressureCorrectionAssembler.cpp:19-63)
- * applied per domain. count = 0 removes all reference rows. */
+ * applied per domain. count = 0 removes all reference rows. The connected
+ * components of the stencil graph become segments of the pressure-correction
+ * solve: with more than one, a solve converges only when each component's
+ * ||r|| <= rtol ||b|| (its reported residual is the worst component's). */
 int oa_flow_set_reference_nodes(oa_flow* f, const int* nodes, int count);
 
 /* navierStokesEquation::initialize / postInitialize and
