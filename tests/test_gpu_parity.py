@@ -256,3 +256,25 @@ def test_scaled_continuity_and_control_data(oracle_mod):
     np.testing.assert_allclose(cd["solver_initial_res"], rms, rtol=1e-13)
     np.testing.assert_allclose(cd["scaled_initial_res"], rms / mom_scale, rtol=1e-13)
     assert np.linalg.norm(cd["solver_final_res"]) <= 1e-10 * np.linalg.norm(rms) * 1.0001
+
+
+@pytest.mark.parametrize("shape", [(1, 1, 1), (2, 1, 1), (3, 2, 1)])
+def test_smallest_meshes(oracle_mod, shape):
+    # every node a boundary node, rows with 1 to 4 elements: assembly and two
+    # SIMPLE iterations against the oracle
+    kw = dict(mom_rtol=1e-13, pc_rtol=1e-13, mom_maxit=500, pc_maxit=5000)
+    m = meshgen.cavity(shape, perturb=0.0)
+    U0 = np.zeros((m.nn, 3))
+    oc = oracle_mod.FlowCase(m, oracle_mod.default_settings(**kw), U0=U0)
+    gf = rt.Flow(rt.Mesh(m), rt.default_settings(**kw))
+    gf.set_field("U", U0)
+    oc.initialize()
+    gf.initialize()
+    A_o, b_o = oc.assemble_momentum()
+    A_g, b_g = gf.assemble_momentum()
+    assert rel(A_g, A_o) < TOL_ASM and rel(b_g, b_o) < TOL_ASM
+    for _ in range(2):
+        oc.simple_iteration()
+    gf.simple_iterate(2)
+    for k in ["U", "p"]:
+        assert np.abs(gf.get_field(k) - oc.field(k)).max() <= 1e-10 * max(1.0, np.abs(oc.field(k)).max()), k
