@@ -107,3 +107,14 @@ def test_graph_counts_its_launches():
     # pressure iteration, and far fewer than a launch per row
     assert n > 20 + st["pc_iters"] * 5
     assert n < 20000
+
+
+@pytest.mark.parametrize("precision", [rt.OA_PREC_FP64, rt.OA_PREC_MIXED])
+def test_graph_with_bicgstab_pressure_solves(monkeypatch, precision):
+    # the pressure solve's BiCGStab loops (the fallback branch of the graph)
+    # taken from the start: graph and eager still agree bit for bit
+    monkeypatch.setenv("OA_KRYLOV", "bicgstab")
+    m = meshgen.cavity(12, perturb=0.2, seed=13)
+    U0 = meshgen.initial_velocity(m, sigma=0.1, seed=13)
+    eager, graph, se, sg = run_both(m, U0, 4, precision=precision)
+    assert_same(eager, graph, se, sg)
