@@ -169,6 +169,26 @@ int oa_flow_field_device_ptr(oa_flow* f, const char* name, double** dev);
  * ||r|| <= rtol ||b|| (its reported residual is the worst component's). */
 int oa_flow_set_reference_nodes(oa_flow* f, const int* nodes, int count);
 
+/* Boundary physical types by boundary index (types[nbnd], nbnd as given to
+ * oa_flow_create): a no-slip wall (the default) or a symmetry plane
+ * (boundaryPhysicalType::wall / ::symmetry, zone/boundary/boundary.h). A
+ * symmetry face carries no mass flow and no gradient contribution
+ * (nodeField.hpp:4764), and its momentum term is the full viscous stress of the
+ * element's velocities (navierStokesAssemblerElemBoundaryConditions.cpp:2082-2375);
+ * after each momentum assembly a symmetry node's rhs loses its component along
+ * the assembled symmetry normal (navierStokesAssembler::applySymmetryConditions_,
+ * navierStokesAssembler.cpp:387-471) and its diagonal block D gains 0.25 D n n^T
+ * (assembleNormalRelaxation, :473-699). The symmetry boundary's row of
+ * bnd_velocity is ignored: the node side velocity is set again from the wall
+ * boundaries alone, in index order. In transient runs only wall-face nodes get
+ * the boundary rhs relaxation (assembleBoundaryRelaxation_, :241-385).
+ * correct_gradients = 1 is the solver's correctGradients_ expert switch: the
+ * velocity and pressure gradients at symmetry nodes lose their normal part
+ * (node{Scalar,Vector}Field::correctGradientField_). hex8 flows. Drops a
+ * captured iteration graph. */
+enum { OA_BTYPE_WALL = 0, OA_BTYPE_SYMMETRY = 1 };
+int oa_flow_set_boundary_types(oa_flow* f, const int* types, int nbnd, int correct_gradients);
+
 /* navierStokesEquation::initialize / postInitialize and
  * pressureCorrectionEquation::initialize
  * (src/equation/flow/navierStokes/navierStokesEquation.cpp:86-133,

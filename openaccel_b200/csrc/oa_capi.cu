@@ -765,6 +765,8 @@ int oa_flow_create(oa_mesh* M, const oa_flow_settings* s, const double* bnd_velo
   Flow& f = H->f;
   f.mesh = &M->m;
   f.s = *s;
+  f.h_bnd_velocity.assign(bnd_velocity, bnd_velocity + 3L * nbnd);
+  f.h_bnd_type.assign(nbnd, OA_BTYPE_WALL);
   {
     double u = 0.0;
     for (int k = 0; k < nbnd; ++k) {
@@ -871,7 +873,7 @@ void oa_flow_destroy(oa_flow* H) {
                   f.b.A_pc,  f.b.b_pc,  f.b.x_mom, f.b.x_pc,  f.err_dev, H->scal,  f.red,   f.ref_flag,
                   f.betaU,   f.minU,    f.maxU,    f.duT,     f.Uold,    f.Uoldold, f.kf,      f.wf,
                   f.gkf,     f.gwf,     f.sdk,     f.srk,     f.sdw,     f.srw,     f.A_k,     f.b_k,
-                  f.A_w,     f.b_w};
+                  f.A_w,     f.b_w,     f.sym_mask, f.sym_nodes, f.sym_area, f.wall_face_node};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (H->hscal) cudaFreeHost(H->hscal);
@@ -984,6 +986,87 @@ int oa_flow_set_reference_nodes(oa_flow* H, const int* nodes, int count) {
   }
   if (int s = H->pc.set_segments(ptr, order)) return s;
   H->ig.drop();  // the captured solve loops carry the segment tests
+  return OA_OK;
+}
+
+int oa_flow_set_boundary_types(oa_flow* H, const int* types, int nbnd, int correct_gradients) {
+  if (!H || nbnd < 0 || (nbnd > 0 && !types)) return fail(OA_ERR_ARG, "oa_flow_set_boundary_types: bad arguments");
+  Flow& f = H->f;
+  if (nbnd != (int)f.h_bnd_type.size())
+    return fail(OA_ERR_ARG, "oa_flow_set_boundary_types: one type per boundary index of oa_flow_create");
+  for (int k = 0; k < nbnd; ++k)
+    if (types[k] != OA_BTYPE_WALL && types[k] != OA_BTYPE_SYMMETRY)
+      return fail(OA_ERR_ARG, "oa_flow_set_boundary_types: a type is neither OA_BTYPE_WALL nor OA_BTYPE_SYMMETRY");
+  const DeviceMesh& m = *f.mesh;
+  static const int FN[6][4] = {{0, 1, 5, 4}, {1, 2, 6, 5}, {2, 3, 7, 6}, {0, 4, 7, 3}, {0, 3, 2, 1}, {4, 5, 6, 7}};
+  // element masks of the symmetry faces, the symmetry nodes, the wall-face
+  // nodes; the node side velocity again from the wall boundaries alone, in
+  // index order (nodeField::updateBoundarySideField leaves symmetry parts
+  // untouched, nodeField.hpp:1128)
+  std::vector<uint8_t> smask(m.ne, 0);
+  std::vector<int> wallf(m.nn, 0), sym_nodes;
+  std::vector<char> sym(m.nn, 0);
+  std::vector<double> side(3L * m.nn, 0.0);
+  for (int fc = 0; fc < m.nf; ++fc) {
+    const bool sf = types[m.h_face_bnd[fc]] == OA_BTYPE_SYMMETRY;
+    if (sf) smask[m.h_face_elem[fc]] |= (uint8_t)(1u << m.h_face_ord[fc]);
+    for (int k = 0; k < 4; ++k) {
+      const int nd = m.h_conn[8L * m.h_face_elem[fc] + FN[m.h_face_ord[fc]][k]];
+      if (sf) sym[nd] = 1;
+      else wallf[nd] = 1;
+    }
+  }
+  for (int bnd = 0; bnd < nbnd; ++bnd) {
+    if (types[bnd] == OA_BTYPE_SYMMETRY) continue;
+    for (int fc = 0; fc < m.nf; ++fc) {
+      if (m.h_face_bnd[fc] != bnd) continue;
+      for (int k = 0; k < 4; ++k) {
+        const int nd = m.h_conn[8L * m.h_face_elem[fc] + FN[m.h_face_ord[fc]][k]];
+        for (int d = 0; d < 3; ++d) side[3L * nd + d] = f.h_bnd_velocity[3L * bnd + d];
+      }
+    }
+  }
+  for (int i = 0; i < m.nn; ++i)
+    if (sym[i]) sym_nodes.push_back(i);
+  // drop the old symmetry state (and the captured iteration, which holds its
+  // launches), then upload the new one
+  OA_CUDA(cudaStreamSynchronize(f.stream));
+  H->ig.drop();
+  for (void** p : {(void**)&f.sym_mask, (void**)&f.sym_nodes, (void**)&f.sym_area, (void**)&f.wall_face_node}) {
+    if (*p) cudaFree(*p);
+    *p = nullptr;
+  }
+  f.nsym = 0;
+  f.h_bnd_type.assign(types, types + nbnd);
+  f.correct_grad = correct_gradients != 0;
+  OA_CUDA(cudaMemcpyAsync(f.sideU, side.data(), sizeof(double) * side.size(), cudaMemcpyHostToDevice, f.stream));
+  if (!sym_nodes.empty()) {
+    const int ns = (int)sym_nodes.size();
+    double* area_nn = nullptr;
+    int st = OA_OK;
+    if ((st = dalloc(&f.sym_mask, (size_t)m.ne)) || (st = dalloc(&f.sym_nodes, (size_t)ns)) ||
+        (st = dalloc(&f.sym_area, 3L * ns)) || (st = dalloc(&f.wall_face_node, (size_t)m.nn)) ||
+        (st = dalloc(&area_nn, 3L * m.nn))) {
+      if (area_nn) cudaFree(area_nn);
+      return st;
+    }
+    OA_CUDA(cudaMemcpyAsync(f.sym_mask, smask.data(), m.ne, cudaMemcpyHostToDevice, f.stream));
+    OA_CUDA(cudaMemcpyAsync(f.sym_nodes, sym_nodes.data(), sizeof(int) * ns, cudaMemcpyHostToDevice, f.stream));
+    OA_CUDA(cudaMemcpyAsync(f.wall_face_node, wallf.data(), sizeof(int) * m.nn, cudaMemcpyHostToDevice, f.stream));
+    if ((st = launch_sym_area(f, area_nn))) {
+      cudaFree(area_nn);
+      return st;
+    }
+    std::vector<double> all(3L * m.nn), cmp(3L * ns);
+    OA_CUDA(cudaMemcpyAsync(all.data(), area_nn, sizeof(double) * all.size(), cudaMemcpyDeviceToHost, f.stream));
+    OA_CUDA(cudaStreamSynchronize(f.stream));
+    cudaFree(area_nn);
+    for (int k = 0; k < ns; ++k)
+      for (int d = 0; d < 3; ++d) cmp[3L * k + d] = all[3L * sym_nodes[k] + d];
+    OA_CUDA(cudaMemcpyAsync(f.sym_area, cmp.data(), sizeof(double) * cmp.size(), cudaMemcpyHostToDevice, f.stream));
+    f.nsym = ns;
+  }
+  OA_CUDA(cudaStreamSynchronize(f.stream));
   return OA_OK;
 }
 

@@ -41,7 +41,10 @@ struct MeshView {
   unsigned long long* slot_mask64 = nullptr;  // [nnz]
   // hex8 lanes per row: 8 (block mesh, lane = corner) or 16 (general)
   int lpr = 8;
-  uint8_t* face_mask = nullptr;  // [ne] bit f: face f is a no-slip wall face
+  uint8_t* face_mask = nullptr;  // [ne] bit f: face f is a boundary face
+  // [ne] bit f: face f is on a symmetry plane (a flow's boundary types; null
+  // when it has none). The no-slip wall faces are face_mask & ~sym_mask.
+  uint8_t* sym_mask = nullptr;
   double* vol = nullptr;       // [nn] dual nodal volume
   double* wscv = nullptr;      // [ne][8] SCV volume fractions (hex8)
   double* scs_area = nullptr;  // [ne][12][3] SCS area vectors, L -> R (hex8)
@@ -128,6 +131,28 @@ struct Flow {
   double u_ref = 1.0, mass_scale = 1.0, mom_scale = 1.0;
   // convergence record of the last momentum / pressure-correction solve
   oa_control_data cd_mom{}, cd_pc{};
+  // boundary physical types (oa_flow_set_boundary_types): per boundary index,
+  // the wall velocities given at creation; with symmetry planes, the element
+  // face mask of the symmetry faces, the symmetry nodes and their assembled
+  // symmetry area vectors [nsym][3], the nodes on a wall face [nn] (the
+  // boundary rhs relaxation of transient runs), the gradient-correction switch
+  std::vector<int> h_bnd_type;
+  std::vector<double> h_bnd_velocity;
+  uint8_t* sym_mask = nullptr;
+  int nsym = 0;
+  int* sym_nodes = nullptr;
+  double* sym_area = nullptr;
+  int* wall_face_node = nullptr;
+  bool correct_grad = false;
+  // the mesh view of this flow's kernels: the mesh's, with the symmetry face
+  // mask, and in transient runs with symmetry planes the wall-face nodes as the
+  // relaxed boundary rows
+  MeshView view() const {
+    MeshView v = mesh->view();
+    v.sym_mask = nsym ? sym_mask : nullptr;
+    if (nsym && time_order) v.wall_node = wall_face_node;
+    return v;
+  }
 };
 
 void set_error(const std::string& msg);
@@ -170,5 +195,7 @@ int launch_gradient(Flow& f, int which);
 int launch_axpy_du_gradp(Flow& f, double sign);
 // velocity extrema and blending factor of the high-resolution scheme
 int launch_blend_u(Flow& f);
+// assembled symmetry area [nn][3] of every node (zero off the symmetry planes)
+int launch_sym_area(Flow& f, double* area_nn);
 
 }  // namespace oa

@@ -354,6 +354,45 @@ __device__ __forceinline__ void wall_face(const MomArgs& a, const TF (&x)[8][3],
   });
 }
 
+// Symmetry-plane term at the exposed ip of canonical face FC nearest corner 0
+// (navierStokesAssemblerElemBoundaryConditions.cpp:2082-2375 with
+// IP_FULL_STRESS__, :295-344): the full viscous stress of the element's own
+// velocities, -mu (dU_i/dx_j + dU_j/dx_i) A_j, every node's coefficient in
+// the row (the bulk term vanishes for the incompressible fluid).
+template <int FC, bool USH, bool UGSH, class TF>
+__device__ __forceinline__ void sym_face(const TF (&x)[8][3], const TF (&Uc)[8][3], const TF (&mu)[8],
+                                         TF (&diag)[9], TF (&nb)[3][9], TF (&rhs)[3], int* err) {
+  constexpr int f0 = face_node(FC, 0), f1 = face_node(FC, 1), f2 = face_node(FC, 2), f3 = face_node(FC, 3);
+  TF Af[3];
+  face_area_at_first<TF>(x[f0], x[f1], x[f2], x[f3], Af);
+  using PT = FacePt<FC, 0, UGSH>;
+  const InvJacR<TF> J = inv_jacobian<PT, TF>(x, err);
+  TF muB;
+  if (USH) {
+    muB = mu[f0];
+  } else {
+    muB = TF(0.5625) * mu[f0] + TF(0.1875) * mu[f1] + TF(0.0625) * mu[f2] + TF(0.1875) * mu[f3];
+  }
+  StaticFor<0, 8>::run([&](auto nc) {
+    constexpr int n = decltype(nc)::value;
+    if (!grad_is_zero<PT, n>()) {
+      constexpr int sl = nb_slot(n);
+      TF g[3];
+      grad_n<PT, n, TF>(J, g);
+      const TF ga = g[0] * Af[0] + g[1] * Af[1] + g[2] * Af[2];
+#pragma unroll
+      for (int i = 0; i < 3; ++i) {
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+          const TF lf = -muB * g[i] * Af[j] + (i == j ? -muB * ga : TF(0));
+          if (sl < 0) diag[3 * i + j] += lf; else nb[sl][3 * i + j] += lf;
+          rhs[i] -= lf * Uc[n][j];
+        }
+      }
+    }
+  });
+}
+
 // VAR 1: the variant with the optional terms (high-resolution deferred
 // correction, transient node terms, SIMPLEC / fractional-step coefficients),
 // each switched at run time; VAR 2: the fused u/v/w/k/omega variant, which
@@ -532,13 +571,20 @@ __global__ void __launch_bounds__(BLOCK, sizeof(TF) == 4 ? (UGSH ? 4 : 3) : 1)
         }
       });
     });
-    // no-slip wall faces touching this corner
-    const uint8_t fm = __ldg(a.m.face_mask + e);
+    // no-slip wall faces and symmetry faces touching this corner
+    const uint8_t sm = a.m.sym_mask ? __ldg(a.m.sym_mask + e) : uint8_t(0);
+    const uint8_t fm = __ldg(a.m.face_mask + e) & uint8_t(~sm);
     if (fm) {
       const uint32_t fw = face_word(c);
       if (fm & (1u << ((fw >> 0) & 7))) wall_face<0, USH, UGSH, TF>(a, x, nd, Uc, mu, diag, nb, rhs, &err);
       if (fm & (1u << ((fw >> 3) & 7))) wall_face<3, USH, UGSH, TF>(a, x, nd, Uc, mu, diag, nb, rhs, &err);
       if (fm & (1u << ((fw >> 6) & 7))) wall_face<4, USH, UGSH, TF>(a, x, nd, Uc, mu, diag, nb, rhs, &err);
+    }
+    if (sm) {
+      const uint32_t fw = face_word(c);
+      if (sm & (1u << ((fw >> 0) & 7))) sym_face<0, USH, UGSH, TF>(x, Uc, mu, diag, nb, rhs, &err);
+      if (sm & (1u << ((fw >> 3) & 7))) sym_face<3, USH, UGSH, TF>(x, Uc, mu, diag, nb, rhs, &err);
+      if (sm & (1u << ((fw >> 6) & 7))) sym_face<4, USH, UGSH, TF>(x, Uc, mu, diag, nb, rhs, &err);
     }
     if (err) a.err[0] = 1;
   }
@@ -1024,8 +1070,9 @@ __global__ void __launch_bounds__(BLOCK) k_gradient(GradArgs a) {
         for (int j = 0; j < 3; ++j) acc[i][j] += (pip[i] - ph[0][i]) * Aq[q][j];
     });
     if (!SH) {
-      // boundary faces: bilinear face value at the face ip nearest the node
-      const uint8_t fm = __ldg(a.m.face_mask + e);
+      // boundary faces: bilinear face value at the face ip nearest the node;
+      // symmetry faces add nothing (nodeField.hpp:4764)
+      const uint8_t fm = __ldg(a.m.face_mask + e) & uint8_t(a.m.sym_mask ? ~__ldg(a.m.sym_mask + e) : 0xff);
       if (fm) {
         const uint32_t fw = face_word(c);
         StaticFor<0, 3>::run([&](auto qc) {
@@ -1210,6 +1257,125 @@ __global__ void k_vel_correct(int n3, double* U, const double* du, const double*
 // launchers
 // grids: 8 lanes per row, bs threads per block (a multiple of 32, at most the
 // BLOCK the kernels are compiled for)
+// ---------------------------------------------------------------------------
+// Symmetry planes.
+//
+// Assembled symmetry area of each row node (mesh::updateAssembledSymmetryAreaField_,
+// src/mesh/meshGeometry.cpp:1787-1880): the exposed-area vectors of the
+// symmetry face ips nearest the node, summed over its incident elements (each
+// lane its element's symmetry faces at its corner). Set-up only.
+template <int LPR>
+__global__ void __launch_bounds__(BLOCK) k_sym_area(MeshView m, double* area) {
+  const RowLane<LPR> rl = row_lane<LPR>(m);
+  double A[3] = {0.0, 0.0, 0.0};
+  if (rl.e >= 0 && m.sym_mask) {
+    const uint8_t sm = __ldg(m.sym_mask + rl.e);
+    if (sm) {
+      const uint32_t fw = face_word(rl.c);
+      double x[8][3];
+      int nd[8];
+      gather_x(m, rl.e, perm_word(rl.c), x, nd);
+      StaticFor<0, 3>::run([&](auto qc) {
+        constexpr int q = decltype(qc)::value;
+        constexpr int FC = q == 0 ? 0 : (q == 1 ? 3 : 4);
+        if (sm & (1u << ((fw >> (3 * q)) & 7))) {
+          double Af[3];
+          face_area_at_first<double>(x[face_node(FC, 0)], x[face_node(FC, 1)], x[face_node(FC, 2)],
+                                     x[face_node(FC, 3)], Af);
+#pragma unroll
+          for (int k = 0; k < 3; ++k) A[k] += Af[k];
+        }
+      });
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < 3; ++k) A[k] = rowsum<LPR>(A[k]);
+  if (rl.rv && rl.li == 0)
+#pragma unroll
+    for (int k = 0; k < 3; ++k) area[3L * rl.row + k] = A[k];
+}
+
+__device__ __forceinline__ void sym_unit(const double* a, double (&n)[3]) {
+  const double amag = sqrt(a[0] * a[0] + a[1] * a[1] + a[2] * a[2]);
+#pragma unroll
+  for (int k = 0; k < 3; ++k) n[k] = a[k] / amag;
+}
+
+// Symmetry rows after the momentum assembly, one thread per symmetry node:
+// applySymmetryConditions_ (navierStokesAssembler.cpp:387-471) removes the rhs
+// component along the assembled symmetry normal n; assembleNormalRelaxation
+// (:473-699, urf 0.75 from navierStokesEquation.cpp:169, after the DU
+// coefficients) adds (1 - urf) D n n^T to the diagonal block D.
+template <class TF>
+__global__ void __launch_bounds__(BLOCK) k_sym_rows(int nsym, const int* __restrict__ nodes,
+                                                    const double* __restrict__ area, const int* __restrict__ row_ptr,
+                                                    const int* __restrict__ diag, TF* A, TF* b) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nsym) return;
+  const int i = nodes[k];
+  double n[3];
+  sym_unit(area + 3L * k, n);
+  TF* bb = b + 3L * i;
+  const double r[3] = {double(bb[0]), double(bb[1]), double(bb[2])};
+  const double dot = r[0] * n[0] + r[1] * n[1] + r[2] * n[2];
+#pragma unroll
+  for (int q = 0; q < 3; ++q) bb[q] = TF(r[q] - dot * n[q]);
+  TF* D = A + 9L * (row_ptr[i] + diag[i]);
+  double d[9];
+#pragma unroll
+  for (int q = 0; q < 9; ++q) d[q] = double(D[q]);
+#pragma unroll
+  for (int a = 0; a < 3; ++a)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      double m = 0.0;
+#pragma unroll
+      for (int q = 0; q < 3; ++q) m += d[3 * a + q] * (n[q] * n[c]);
+      D[3 * a + c] = TF(d[3 * a + c] + (1.0 - 0.75) * m);
+    }
+}
+
+// Gradient at a symmetry node without its normal part (the correctGradients_
+// switch, end of nodeField::updateGradientField, nodeField.hpp:4939-4943): a
+// scalar's G - (G.n) n (nodeScalarField.cpp:44-112), a vector's
+// G - (G n) n^T - n (n^T G) + 2 (n^T G n) n n^T (nodeVectorField.cpp:44-148).
+template <int NC>
+__global__ void __launch_bounds__(BLOCK) k_sym_grad(int nsym, const int* __restrict__ nodes,
+                                                    const double* __restrict__ area, double* grad) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nsym) return;
+  double n[3];
+  sym_unit(area + 3L * k, n);
+  double* G = grad + 3L * NC * nodes[k];
+  if (NC == 1) {
+    const double dot = G[0] * n[0] + G[1] * n[1] + G[2] * n[2];
+#pragma unroll
+    for (int j = 0; j < 3; ++j) G[j] -= dot * n[j];
+    return;
+  }
+  double g[9], Gn[3] = {0.0, 0.0, 0.0}, nG[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+  for (int q = 0; q < 9; ++q) g[q] = G[q];
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      Gn[i] += g[3 * i + j] * n[j];
+      nG[j] += g[3 * i + j] * n[i];
+    }
+  const double nGn = nG[0] * n[0] + nG[1] * n[1] + nG[2] * n[2];
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      double v = g[3 * i + j];
+      v -= Gn[i] * n[j];
+      v -= n[i] * nG[j];
+      v += 2.0 * n[i] * n[j] * nGn;
+      G[3 * i + j] = v;
+    }
+}
+
 static int grid_rows(const DeviceMesh& m, int bs = BLOCK) { return (int)(((size_t)m.nn * m.lpr + bs - 1) / bs); }
 
 static int launch_mdot_impl(Flow& f, int mode);
@@ -1265,7 +1431,7 @@ int launch_momentum(Flow& f, bool mixed) {
     k_pack_umu<<<(f.mesh->nn + 255) / 256, 256, 0, f.stream>>>(f.mesh->nn, f.U, f.mu, f.umu32);
     count_launches(1);
   }
-  MomArgs a{f.mesh->view(), f.U,       f.gradP, f.div,  f.mDot,          f.rho,
+  MomArgs a{f.view(),       f.U,       f.gradP, f.div,  f.mDot,          f.rho,
             f.mu,           f.sideU,   f.betaU, f.gradU, f.xloc32, f.umu32, f.b.A_mom, f.b.b_mom,
             f.du,           f.duT,     f.time_order ? f.dt_step : f.s.dt,  1.0 / f.s.urf_u, f.s.wall_rhs_relax,
             f.s.du_mode,    f.s.hr,    f.time_order, f.tk[0], f.tk[1], f.tk[2], f.Uold, f.Uoldold, f.err_dev};
@@ -1313,6 +1479,18 @@ int launch_momentum(Flow& f, bool mixed) {
   else go(std::integral_constant<int, 8>{});
   count_launches(1);
   OA_CUDA(cudaGetLastError());
+  if (f.nsym) {
+    const unsigned gs = (unsigned)((f.nsym + BLOCK - 1) / BLOCK);
+    const DeviceMesh& m = *f.mesh;
+    if (mixed)
+      k_sym_rows<float><<<gs, BLOCK, 0, f.stream>>>(f.nsym, f.sym_nodes, f.sym_area, m.row_ptr, m.diag,
+                                                     static_cast<float*>(f.b.A_mom), static_cast<float*>(f.b.b_mom));
+    else
+      k_sym_rows<double><<<gs, BLOCK, 0, f.stream>>>(f.nsym, f.sym_nodes, f.sym_area, m.row_ptr, m.diag,
+                                                      static_cast<double*>(f.b.A_mom), static_cast<double*>(f.b.b_mom));
+    count_launches(1);
+    OA_CUDA(cudaGetLastError());
+  }
   return OA_OK;
 }
 
@@ -1364,11 +1542,34 @@ int launch_div(Flow& f) {
   return OA_OK;
 }
 
+int launch_sym_area(Flow& f, double* area_nn) {
+  // the mesh view with the flow's symmetry mask, which f.view() exposes only
+  // once the symmetry nodes are set up
+  if (!f.sym_mask) return fail(OA_ERR_ARG, "symmetry area: no symmetry face mask");
+  MeshView v = f.mesh->view();
+  v.sym_mask = f.sym_mask;
+  const unsigned g = (unsigned)(((size_t)f.mesh->nn * f.mesh->lpr + BLOCK - 1) / BLOCK);
+  if (f.mesh->lpr == 16) k_sym_area<16><<<g, BLOCK, 0, f.stream>>>(v, area_nn);
+  else k_sym_area<8><<<g, BLOCK, 0, f.stream>>>(v, area_nn);
+  OA_CUDA(cudaGetLastError());
+  return OA_OK;
+}
+
+static int launch_sym_grad(Flow& f, int which) {
+  if (!f.nsym || !f.correct_grad) return OA_OK;
+  const unsigned g = (unsigned)((f.nsym + BLOCK - 1) / BLOCK);
+  if (which == 0) k_sym_grad<1><<<g, BLOCK, 0, f.stream>>>(f.nsym, f.sym_nodes, f.sym_area, f.gradP);
+  else k_sym_grad<3><<<g, BLOCK, 0, f.stream>>>(f.nsym, f.sym_nodes, f.sym_area, f.gradU);
+  count_launches(1);
+  OA_CUDA(cudaGetLastError());
+  return OA_OK;
+}
+
 int launch_gradient(Flow& f, int which) {
   const int bs = f.bs_rows;
   const int g = grid_rows(*f.mesh, bs);
   if (which == 0) {
-    GradArgs a{f.mesh->view(), f.p, f.gradP, f.s.grad_urf};
+    GradArgs a{f.view(), f.p, f.gradP, f.s.grad_urf};
     if (f.mesh->lpr == 16) {
       if (f.s.p_shifted) k_gradient<16, 1, true><<<g, bs, 0, f.stream>>>(a);
       else k_gradient<16, 1, false><<<g, bs, 0, f.stream>>>(a);
@@ -1377,7 +1578,7 @@ int launch_gradient(Flow& f, int which) {
       else k_gradient<8, 1, false><<<g, bs, 0, f.stream>>>(a);
     }
   } else {
-    GradArgs a{f.mesh->view(), f.U, f.gradU, f.s.grad_urf};
+    GradArgs a{f.view(), f.U, f.gradU, f.s.grad_urf};
     if (f.mesh->lpr == 16) {
       if (f.s.u_shifted) k_gradient<16, 3, true><<<g, bs, 0, f.stream>>>(a);
       else k_gradient<16, 3, false><<<g, bs, 0, f.stream>>>(a);
@@ -1388,7 +1589,7 @@ int launch_gradient(Flow& f, int which) {
   }
   count_launches(1);
   OA_CUDA(cudaGetLastError());
-  return OA_OK;
+  return launch_sym_grad(f, which);
 }
 
 int launch_blend_u(Flow& f) {

@@ -137,6 +137,24 @@ def cavity(n, perturb=0.0, seed=12345, lid_velocity=(1.0, 0.0, 0.0)):
     )
 
 
+def symmetry_box(n, perturb=0.0, seed=12345, lid_velocity=(1.0, 0.0, 0.0)):
+    """The cavity box with its two y faces as separate boundaries, for
+    symmetry planes: boundary 0 the lid (z = 1), 1 the x faces and the floor
+    (no-slip), 2 the face y = 0, 3 the face y = 1. Node layout and
+    ``perturb`` as in :func:`cavity` (interior nodes only, so the y faces stay
+    planes)."""
+    c = cavity(n, perturb=perturb, seed=seed, lid_velocity=lid_velocity)
+    faces = block_faces(c.nx, c.ny, c.nz)
+    fe, fo, fb = [], [], []
+    for side, bnd in (("z+", 0), ("x-", 1), ("x+", 1), ("z-", 1), ("y-", 2), ("y+", 3)):
+        e, o = faces[side]
+        fe.append(e), fo.append(np.full_like(e, o)), fb.append(np.full_like(e, bnd))
+    bnd_velocity = np.array([list(lid_velocity), [0.0] * 3, [0.0] * 3, [0.0] * 3], dtype=np.float64)
+    meta = dict(c.meta, kind="symmetry_box")
+    return HexMesh(c.nx, c.ny, c.nz, c.coords, c.conn, np.concatenate(fe).astype(np.int32),
+                   np.concatenate(fo).astype(np.int32), np.concatenate(fb).astype(np.int32), bnd_velocity, meta=meta)
+
+
 def initial_velocity(mesh: HexMesh, sigma=0.0, seed=12345):
     """Zero, or seeded Gaussian N(0, sigma^2) on interior nodes (walls keep 0)."""
     U = np.zeros((mesh.nn, 3), dtype=np.float64)
@@ -171,18 +189,17 @@ def stretched_1d(n, ratio, length=1.0):
 def channel(nx=256, ny=96, nz=96, ratio=1.05, length=(4.0, 1.0, 1.0), perturb=0.0, seed=3):
     """Channel-shaped hex block: nx x ny x nz elements, x streamwise, y
     wall-normal with geometric stretching `ratio` from both walls, z spanwise.
-    The engine's boundaries are no-slip walls (boundary 0 the y walls, boundary
-    1 the other four faces); the configuration's inlet / outlet / symmetry
-    conditions are not modelled, so this stands in for the channel's mesh and
-    sizes, not its boundary conditions."""
+    Boundary 0 is the y walls, 1 the x faces (the inlet and outlet planes,
+    no-slip walls here: inlet and outlet conditions are not modelled) and 2
+    the z faces (the spanwise planes, meant as symmetry planes)."""
     coords, conn = hex_block(nx, ny, nz, np.linspace(0.0, length[0], nx + 1), stretched_1d(ny, ratio, length[1]),
                              np.linspace(0.0, length[2], nz + 1))
     faces = block_faces(nx, ny, nz)
     fe, fo, fb = [], [], []
-    for side, bnd in (("y-", 0), ("y+", 0), ("x-", 1), ("x+", 1), ("z-", 1), ("z+", 1)):
+    for side, bnd in (("y-", 0), ("y+", 0), ("x-", 1), ("x+", 1), ("z-", 2), ("z+", 2)):
         e, o = faces[side]
         fe.append(e), fo.append(np.full_like(e, o)), fb.append(np.full_like(e, bnd))
-    bnd_velocity = np.zeros((2, 3), dtype=np.float64)
+    bnd_velocity = np.zeros((3, 3), dtype=np.float64)
     return HexMesh(nx, ny, nz, coords, conn, np.concatenate(fe).astype(np.int32),
                    np.concatenate(fo).astype(np.int32), np.concatenate(fb).astype(np.int32), bnd_velocity,
                    meta={"kind": "channel", "ratio": ratio})

@@ -19,6 +19,8 @@ OA_TOPO_HEX8 = 8
 OA_TOPO_TET4 = 4
 OA_PREC_FP64 = 0
 OA_PREC_MIXED = 1
+OA_BTYPE_WALL = 0
+OA_BTYPE_SYMMETRY = 1
 OA_TIME_BDF1 = 1
 OA_TIME_BDF2 = 2
 OA_STATIC_SOLVE_MAX_ROWS = 131072
@@ -27,7 +29,7 @@ OA_STATIC_SOLVE_MAX_ROWS = 131072
 EXPORTS = [
     "oa_last_error", "oa_version", "oa_mesh_create", "oa_mesh_destroy", "oa_mesh_nnz", "oa_mesh_graph",
     "oa_mesh_dual_volume", "oa_flow_create", "oa_flow_destroy", "oa_flow_set_field", "oa_flow_get_field",
-    "oa_flow_field_device_ptr", "oa_flow_set_reference_nodes", "oa_flow_initialize", "oa_assemble_momentum", "oa_assemble_pcorr",
+    "oa_flow_field_device_ptr", "oa_flow_set_reference_nodes", "oa_flow_set_boundary_types", "oa_flow_initialize", "oa_assemble_momentum", "oa_assemble_pcorr",
     "oa_update_mdot", "oa_update_div", "oa_update_gradient", "oa_solve", "oa_simple_iterate", "oa_flow_sync",
     "oa_flow_stream", "oa_launch_count", "oa_time_kernel", "oa_pcorr_solve_static",
     "oa_diffusion_create", "oa_diffusion_destroy", "oa_diffusion_set_field", "oa_diffusion_get_field",
@@ -74,6 +76,47 @@ class ControlData(C.Structure):
         return dict(n_iterations=self.n_iterations, fallback=self.fallback,
                     solver_initial_res=list(self.solver_initial_res), solver_final_res=list(self.solver_final_res),
                     scaled_initial_res=list(self.scaled_initial_res))
+
+
+class ResidualHistory:
+    """Per-outer-iteration convergence record, the counterpart of the
+    reference's convergence report (linearSystem::convergenceReport_,
+    src/equation/linearSystem.h:464-571: per equation and component the
+    solver's initial and final residuals, the scaled initial residual and the
+    iteration count), kept in memory and, with ``path``, appended to a CSV
+    file one row per outer iteration as the iterations are reported."""
+
+    COLUMNS = (("iteration", "continuity_rms", "continuity_rms_raw", "mom_iters", "mom_res", "mom_fallback")
+               + tuple(f"mom_{q}_{c}" for q in ("initial", "final", "scaled") for c in "uvw")
+               + ("pc_iters", "pc_res", "pc_refinements", "pc_fallback", "pc_initial", "pc_final", "pc_scaled")
+               + PHASES)
+
+    def __init__(self, path=None):
+        self.rows = []
+        self.path = path
+        if path is not None:
+            with open(path, "w") as fh:
+                fh.write(",".join(self.COLUMNS) + "\n")
+
+    def add(self, stats):
+        """Append the dicts Flow.simple_iterate returns (one per iteration)."""
+        for st in stats:
+            mom, pc = st["mom"], st["pc"]
+            row = [len(self.rows) + 1, st["continuity_rms"], st["continuity_rms_raw"], st["mom_iters"],
+                   st["mom_res"], mom["fallback"]]
+            for q in ("solver_initial_res", "solver_final_res", "scaled_initial_res"):
+                row += list(mom[q])
+            row += [st["pc_iters"], st["pc_res"], st["pc_refinements"], pc["fallback"], pc["solver_initial_res"][0],
+                    pc["solver_final_res"][0], pc["scaled_initial_res"][0]]
+            row += [st[k] for k in PHASES]
+            self.rows.append(row)
+            if self.path is not None:
+                with open(self.path, "a") as fh:
+                    fh.write(",".join(repr(v) if isinstance(v, float) else str(v) for v in row) + "\n")
+
+    def column(self, name):
+        i = self.COLUMNS.index(name)
+        return [r[i] for r in self.rows]
 
 
 class Tuning(C.Structure):
@@ -169,6 +212,7 @@ def lib():
         "oa_flow_get_field": (C.c_int, [vp, C.c_char_p, dp, C.c_long]),
         "oa_flow_field_device_ptr": (C.c_int, [vp, C.c_char_p, P(dp)]),
         "oa_flow_set_reference_nodes": (C.c_int, [vp, ip, C.c_int]),
+        "oa_flow_set_boundary_types": (C.c_int, [vp, ip, C.c_int, C.c_int]),
         "oa_flow_initialize": (C.c_int, [vp]),
         "oa_assemble_momentum": (C.c_int, [vp, dp, dp]),
         "oa_assemble_pcorr": (C.c_int, [vp, dp, dp]),
@@ -312,6 +356,12 @@ class Flow:
         n = np.ascontiguousarray(nodes, np.int32)
         _check(lib().oa_flow_set_reference_nodes(self.h, _ip(n), int(n.size)))
 
+    def set_boundary_types(self, types, correct_gradients=False):
+        """Boundary physical types by boundary index (OA_BTYPE_WALL,
+        OA_BTYPE_SYMMETRY); see oa_flow_set_boundary_types."""
+        t = np.ascontiguousarray(types, np.int32)
+        _check(lib().oa_flow_set_boundary_types(self.h, _ip(t), int(t.size), int(bool(correct_gradients))))
+
     def initialize(self):
         _check(lib().oa_flow_initialize(self.h))
 
@@ -344,13 +394,18 @@ class Flow:
                               C.byref(res)))
         return x, it.value, res.value
 
-    def simple_iterate(self, n=1):
+    def simple_iterate(self, n=1, history=None):
+        """n SIMPLE outer iterations; one stats dict each, also added to
+        ``history`` (a ResidualHistory) when given."""
         st = (IterStats * max(n, 1))()
         _check(lib().oa_simple_iterate(self.h, n, st))
-        return [dict(mom_iters=s.mom_iters, pc_iters=s.pc_iters, pc_refinements=s.pc_refinements,
-                     mom_res=s.mom_res, pc_res=s.pc_res, continuity_rms=s.continuity_rms,
-                     continuity_rms_raw=s.continuity_rms_raw, mom=s.mom.as_dict(), pc=s.pc.as_dict(),
-                     **{k: getattr(s, k) for k in PHASES}) for s in st[:n]]
+        out = [dict(mom_iters=s.mom_iters, pc_iters=s.pc_iters, pc_refinements=s.pc_refinements,
+                    mom_res=s.mom_res, pc_res=s.pc_res, continuity_rms=s.continuity_rms,
+                    continuity_rms_raw=s.continuity_rms_raw, mom=s.mom.as_dict(), pc=s.pc.as_dict(),
+                    **{k: getattr(s, k) for k in PHASES}) for s in st[:n]]
+        if history is not None:
+            history.add(out)
+        return out
 
     def advance_time(self, scheme, dt):
         """Start a time step of size dt: scheme 1 BDF1, 2 BDF2."""

@@ -75,6 +75,19 @@ struct Case {
   std::vector<std::vector<int>> colors;
   // pressure-level rows (settings.ref_node, or a list for batched meshes)
   std::vector<int> refNodes;
+  // boundary physical type by boundary index (ORC_BTYPE_WALL no-slip wall,
+  // ORC_BTYPE_SYMMETRY symmetry plane); all walls until set
+  std::vector<int> bndType;
+  // symmetry planes: the nodes on a symmetry face, the assembled symmetry
+  // area vector [nn][3] (sum of the exposed-area vectors of the face ips
+  // nearest each node, mesh::updateAssembledSymmetryAreaField_,
+  // src/mesh/meshGeometry.cpp:1787-1880) and the nodes on a wall face
+  std::vector<int> symNodes;
+  std::vector<double> symArea;
+  std::vector<char> wallFaceNode;
+  // expertParameters_.correctGradients_ (default off): gradients at symmetry
+  // nodes lose their normal part (node*Field::correctGradientField_)
+  bool correctGrad = false;
   // last assembled systems (for the solver inside simple_iteration)
   std::vector<double> Am, bm, xm, Ap, bp, xp;
   // continuity-residual scale rho U_ref h^2 (the residual normalisation of
@@ -199,6 +212,17 @@ void apply_coeff(Case& c, double* A, double* b, const int* nodes, int n, const d
     }
     for (int k = 0; k < N; ++k) b[N * row + k] += rr[k];
   }
+}
+
+bool is_symmetry_face(const Case& c, int f) {
+  return !c.bndType.empty() && c.bndType[c.fBnd[f]] == ORC_BTYPE_SYMMETRY;
+}
+
+// unit vector of node i's assembled symmetry area (amag from the vector itself)
+void sym_normal(const Case& c, int i, double* n) {
+  const double* a = &c.symArea[3L * i];
+  const double amag = std::sqrt(a[0] * a[0] + a[1] * a[1] + a[2] * a[2]);
+  for (int k = 0; k < 3; ++k) n[k] = a[k] / amag;
 }
 
 void gather_coords(const Case& c, int e, double* xe) {
@@ -345,6 +369,34 @@ void update_div(Case& c) {
   }
 }
 
+// Gradient at a symmetry node without its normal part, at the end of
+// updateGradientField (nodeField.hpp:4939-4943): a scalar's G - (G.n) n
+// (nodeScalarField.cpp:44-112); a vector's G - (G n) n^T - n (n^T G)
+// + 2 (n^T G n) n n^T (nodeVectorField.cpp:44-148).
+template <int NC>
+void correct_gradient(const Case& c, int node, double* G) {
+  double n[3];
+  sym_normal(c, node, n);
+  if (NC == 1) {
+    const double dot = G[0] * n[0] + G[1] * n[1] + G[2] * n[2];
+    for (int j = 0; j < 3; ++j) G[j] -= dot * n[j];
+    return;
+  }
+  double Gn[3] = {0, 0, 0}, nG[3] = {0, 0, 0};
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) {
+      Gn[i] += G[3 * i + j] * n[j];
+      nG[j] += G[3 * i + j] * n[i];
+    }
+  const double nGn = nG[0] * n[0] + nG[1] * n[1] + nG[2] * n[2];
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) {
+      G[3 * i + j] -= Gn[i] * n[j];
+      G[3 * i + j] -= n[i] * nG[j];
+      G[3 * i + j] += 2.0 * n[i] * n[j] * nGn;
+    }
+}
+
 // nodeField::updateGradientField (src/field/nodeField/nodeField.hpp:3253-3445
 // interior, :4732-4930 boundary, :6362-6398 relax). NC = field components.
 template <int NC>
@@ -375,6 +427,8 @@ void update_gradient(Case& c, const std::vector<double>& phi, std::vector<double
   double Nf[16];
   oracle::hex8::face_shape(Nf, shifted);
   for (int f = 0; f < c.nf; ++f) {
+    // symmetry faces add nothing (nodeField.hpp:4764)
+    if (is_symmetry_face(c, f)) continue;
     const int e = c.fElem[f], o = c.fOrd[f];
     int fn[4];
     for (int k = 0; k < 4; ++k) fn[k] = c.conn[8 * e + oracle::hex8::FACE_NODES[o][k]];
@@ -391,6 +445,8 @@ void update_gradient(Case& c, const std::vector<double>& phi, std::vector<double
               g * (pip[i] - phi[NC * nn + i]) * c.faceArea[12 * f + 3 * ip + j] * iv;
     }
   }
+  if (c.correctGrad)
+    for (int i : c.symNodes) correct_gradient<NC>(c, i, &grad[3L * NC * i]);
 }
 
 // ---------------------------------------------------------------------------
@@ -548,6 +604,43 @@ void assemble_pcorr(Case& c, double* A, double* b) {
 //  post         phiAssembler.h:748-753 + :967-1006 (diag / urf),
 //               navierStokesAssembler.cpp:234-385 (wall-node rhs * 0.75)
 //  DU           navierStokesAssembler.cpp:84-232 (SIMPLE, steady)
+// navierStokesAssembler::assembleElemTermsBoundarySymmetry_
+// (src/assemble/flow/segregatedFlow/navierStokesAssembler/
+//  navierStokesAssemblerElemBoundaryConditions.cpp:2082-2375): at each face
+// ip, the full viscous stress -mu (dU_i/dx_j + dU_j/dx_i) A_j of the element's
+// own velocities (IP_FULL_STRESS__, :295-344; the bulk term vanishes for the
+// incompressible fluid), mu at the ip by the face shape functions.
+void symmetry_face(const Case& c, int f, const double* Nf, double* lhs, double* rhs) {
+  const int e = c.fElem[f], o = c.fOrd[f];
+  const int* en = &c.conn[8 * e];
+  double xe[24], g[96], muf[4];
+  gather_coords(c, e, xe);
+  for (int k = 0; k < 4; ++k) muf[k] = c.mu[en[oracle::hex8::FACE_NODES[o][k]]];
+  oracle::hex8::face_grad_op(o, xe, g, c.s.u_grad_shifted);
+  const double* av = &c.faceArea[12 * f];
+  for (int ip = 0; ip < 4; ++ip) {
+    const int nn = oracle::hex8::FACE_NODES[o][ip];
+    double muB = 0.0;
+    for (int k = 0; k < 4; ++k) muB += Nf[4 * ip + k] * muf[k];
+    for (int a = 0; a < 8; ++a) {
+      const double* ga = &g[24 * ip + 3 * a];
+      const double* Ua = &c.U[3L * en[a]];
+      for (int i = 0; i < 3; ++i) {
+        const int iR = 3 * nn + i, rowR = iR * 24;
+        for (int j = 0; j < 3; ++j) {
+          const double Aj = av[3 * ip + j];
+          double lf = -muB * ga[j] * Aj;
+          lhs[rowR + 3 * a + i] += lf;
+          rhs[iR] -= lf * Ua[i];
+          lf = -muB * ga[i] * Aj;
+          lhs[rowR + 3 * a + j] += lf;
+          rhs[iR] -= lf * Ua[j];
+        }
+      }
+    }
+  }
+}
+
 void assemble_momentum(Case& c, double* A, double* b) {
   const int nnz = c.rowPtr[c.nn];
   std::fill(A, A + 9L * nnz, 0.0);
@@ -667,6 +760,11 @@ void assemble_momentum(Case& c, double* A, double* b) {
     const int* en = &c.conn[8 * e];
     std::fill(lhs.begin(), lhs.end(), 0.0);
     std::fill(rhs.begin(), rhs.end(), 0.0);
+    if (is_symmetry_face(c, f)) {
+      symmetry_face(c, f, Nf, lhs.data(), rhs.data());
+      apply_coeff<3>(c, A, b, en, 8, rhs.data(), lhs.data());
+      continue;
+    }
     double xe[24], g[96], Ue[24], bcm[8], muf[4];
     gather_coords(c, e, xe);
     for (int a = 0; a < 8; ++a) {
@@ -729,9 +827,21 @@ void assemble_momentum(Case& c, double* A, double* b) {
     double* d = &A[9L * (c.rowPtr[i] + c.diagOff[i])];
     for (int k = 0; k < 3; ++k) d[4 * k] *= ui;
   }
+  // navierStokesAssembler::assembleBoundaryRelaxation_ (navierStokesAssembler.cpp:241-385):
+  // every boundary node in steady runs, the no-slip wall nodes alone in
+  // transient ones
+  const bool wall_only = c.timeScheme != 0 && !c.symNodes.empty();
   for (int i = 0; i < c.nn; ++i)
-    if (c.wallNode[i] != 0.0)
+    if (wall_only ? c.wallFaceNode[i] != 0 : c.wallNode[i] != 0.0)
       for (int k = 0; k < 3; ++k) b[3 * i + k] *= c.s.wall_rhs_relax;
+  // applySymmetryConditions_ (navierStokesAssembler.cpp:387-471): the rhs of a
+  // symmetry node loses its component along the assembled symmetry normal
+  for (int i : c.symNodes) {
+    double n[3];
+    sym_normal(c, i, n);
+    const double dot = b[3 * i] * n[0] + b[3 * i + 1] * n[1] + b[3 * i + 2] * n[2];
+    for (int k = 0; k < 3; ++k) b[3 * i + k] -= dot * n[k];
+  }
   // DU coefficients: navierStokesAssembler::computeDUCoefficients
   // (src/assemble/flow/segregatedFlow/navierStokesAssembler/navierStokesAssembler.cpp:84-232):
   // D = V / (a_ii + SMALL), or dt / rho for the fractional-step method (steady:
@@ -749,6 +859,22 @@ void assemble_momentum(Case& c, double* A, double* b) {
           if (q - c.rowPtr[i] != c.diagOff[i]) off += A[9L * q + 4 * k];
         c.duT[3 * i + k] = c.vol[i] / (d[4 * k] + off + SMALL);
       }
+  }
+  // assembleNormalRelaxation (navierStokesAssembler.cpp:473-699, urf 0.75 from
+  // navierStokesEquation.cpp:169), after the DU coefficients: the diagonal
+  // block D of a symmetry node gains (1 - urf) D n n^T
+  for (int i : c.symNodes) {
+    double n[3], T[9], M[9];
+    sym_normal(c, i, n);
+    for (int a = 0; a < 3; ++a)
+      for (int q = 0; q < 3; ++q) T[3 * a + q] = n[a] * n[q];
+    double* d = &A[9L * (c.rowPtr[i] + c.diagOff[i])];
+    for (int a = 0; a < 3; ++a)
+      for (int q = 0; q < 3; ++q) {
+        M[3 * a + q] = 0.0;
+        for (int k = 0; k < 3; ++k) M[3 * a + q] += d[3 * a + k] * T[3 * k + q];
+      }
+    for (int k = 0; k < 9; ++k) d[k] += (1.0 - 0.75) * M[k];
   }
 }
 
@@ -1269,6 +1395,48 @@ void* orc_case_create(int nn, int ne, const double* x, const int* conn, int nf, 
   return c;
 }
 
+int orc_set_boundary_types(void* h, const int* types, int nbnd, int correct_gradients) {
+  Case& c = *static_cast<Case*>(h);
+  c.correctGrad = correct_gradients != 0;
+  if (nbnd != c.nbnd) return 1;
+  for (int k = 0; k < nbnd; ++k)
+    if (types[k] != ORC_BTYPE_WALL && types[k] != ORC_BTYPE_SYMMETRY) return 1;
+  c.bndType.assign(types, types + nbnd);
+  c.symArea.assign(3L * c.nn, 0.0);
+  c.wallFaceNode.assign(c.nn, 0);
+  std::vector<char> sym(c.nn, 0);
+  for (int f = 0; f < c.nf; ++f) {
+    const int* en = &c.conn[8 * c.fElem[f]];
+    const bool s = is_symmetry_face(c, f);
+    for (int ip = 0; ip < 4; ++ip) {
+      const int nd = en[oracle::hex8::FACE_NODES[c.fOrd[f]][ip]];
+      if (s) {
+        sym[nd] = 1;
+        for (int d = 0; d < 3; ++d) c.symArea[3L * nd + d] += c.faceArea[12 * f + 3 * ip + d];
+      } else {
+        c.wallFaceNode[nd] = 1;
+      }
+    }
+  }
+  c.symNodes.clear();
+  for (int i = 0; i < c.nn; ++i)
+    if (sym[i]) c.symNodes.push_back(i);
+  // side velocity from the wall boundaries alone (nodeField::updateBoundarySideField
+  // leaves symmetry parts untouched, nodeField.hpp:1128)
+  std::fill(c.sideU.begin(), c.sideU.end(), 0.0);
+  for (int bnd = 0; bnd < c.nbnd; ++bnd) {
+    if (c.bndType[bnd] == ORC_BTYPE_SYMMETRY) continue;
+    for (int f = 0; f < c.nf; ++f) {
+      if (c.fBnd[f] != bnd) continue;
+      for (int k = 0; k < 4; ++k) {
+        const int nd = c.conn[8 * c.fElem[f] + oracle::hex8::FACE_NODES[c.fOrd[f]][k]];
+        for (int d = 0; d < 3; ++d) c.sideU[3 * nd + d] = c.bndU[3 * bnd + d];
+      }
+    }
+  }
+  return 0;
+}
+
 void orc_case_destroy(void* h) { delete static_cast<Case*>(h); }
 
 double orc_case_mass_scale(void* h) { return static_cast<Case*>(h)->massScale; }
@@ -1295,6 +1463,7 @@ double* orc_case_field(void* h, const char* name, long* len) {
   else if (n == "faceArea") v = &c->faceArea;
   else if (n == "sideU") v = &c->sideU;
   else if (n == "wallNode") v = &c->wallNode;
+  else if (n == "symArea") v = &c->symArea;
   else if (n == "x") v = &c->x;
   else if (n == "betaU") v = &c->betaU;
   else if (n == "duTilde") v = &c->duT;

@@ -66,6 +66,14 @@ void* orc_case_create(int nn, int ne, const double* x, const int* conn, int nf,
 void orc_case_destroy(void* h);
 /* pressure-level rows (replaces settings.ref_node; one per closed domain) */
 void orc_set_ref_nodes(void* h, const int* nodes, int n);
+/* boundary physical types by boundary index (types[nbnd]): no-slip wall or
+ * symmetry plane (boundaryPhysicalType::wall / ::symmetry). A symmetry
+ * boundary's velocity row is ignored; the node side velocity is set again
+ * from the wall boundaries alone, in index order. correct_gradients: the
+ * solver's correctGradients_ expert switch (gradients at symmetry nodes lose
+ * their normal part). Returns nonzero on a bad type or count. */
+enum { ORC_BTYPE_WALL = 0, ORC_BTYPE_SYMMETRY = 1 };
+int orc_set_boundary_types(void* h, const int* types, int nbnd, int correct_gradients);
 /* Pointer to a named field of the case (see oracle.cpp for the list); *len
  * receives the number of doubles. */
 double* orc_case_field(void* h, const char* name, long* len);

@@ -118,6 +118,8 @@ def lib():
                                       P(Settings)]
         L.orc_case_destroy.argtypes = [C.c_void_p]
         L.orc_set_ref_nodes.argtypes = [C.c_void_p, ip, C.c_int]
+        L.orc_set_boundary_types.argtypes = [C.c_void_p, ip, C.c_int, C.c_int]
+        L.orc_set_boundary_types.restype = C.c_int
         L.orc_case_field.restype = dp
         L.orc_case_field.argtypes = [C.c_void_p, C.c_char_p, P(C.c_long)]
         L.orc_case_nnz.restype = C.c_int
@@ -242,6 +244,12 @@ class FlowCase:
         n = np.ascontiguousarray(nodes, np.int32)
         self._keep.append(n)
         lib().orc_set_ref_nodes(self.h, _ip(n), int(n.size))
+
+    def set_boundary_types(self, types, correct_gradients=False):
+        """Boundary physical types by boundary index: 0 no-slip wall, 1 symmetry."""
+        t = np.ascontiguousarray(types, np.int32)
+        if lib().orc_set_boundary_types(self.h, _ip(t), int(t.size), int(bool(correct_gradients))) != 0:
+            raise ValueError("orc_set_boundary_types: one type per boundary, 0 or 1")
 
     def initialize(self):
         lib().orc_initialize(self.h)

@@ -50,3 +50,30 @@ def test_meshgen_conventions():
     # right-handed elements
     x = m.coords[m.conn[0]]
     assert (x[1] - x[0])[0] > 0 and (x[3] - x[0])[1] > 0 and (x[4] - x[0])[2] > 0
+
+
+def test_residual_history_csv(tmp_path):
+    import csv
+
+    from openaccel_b200 import runtime as rt
+
+    def stats(i):
+        cd = lambda r: dict(n_iterations=3, fallback=0, solver_initial_res=[r, 2 * r, 3 * r],
+                            solver_final_res=[r / 10, r / 20, r / 30], scaled_initial_res=[r, r, r])
+        d = dict(mom_iters=3 + i, pc_iters=20 + i, pc_refinements=2, mom_res=1e-3, pc_res=1e-5,
+                 continuity_rms=10.0 ** -i, continuity_rms_raw=2.0 * 10.0 ** -i, mom=cd(0.5), pc=cd(0.25))
+        d.update({k: 0.1 * (j + 1) for j, k in enumerate(rt.PHASES)})
+        return d
+
+    path = tmp_path / "history.csv"
+    h = rt.ResidualHistory(str(path))
+    h.add([stats(1), stats(2)])
+    h.add([stats(3)])
+    with open(path) as fh:
+        rows = list(csv.DictReader(fh))
+    assert [int(r["iteration"]) for r in rows] == [1, 2, 3]
+    assert [float(r["continuity_rms"]) for r in rows] == [0.1, 0.01, 0.001]
+    assert float(rows[0]["mom_initial_v"]) == 1.0 and float(rows[2]["mom_final_w"]) == 0.5 / 30
+    assert float(rows[1]["pc_initial"]) == 0.25 and int(rows[2]["pc_iters"]) == 23
+    assert float(rows[0]["ms_pcorr_solve"]) == 0.4
+    assert h.column("mom_iters") == [4, 5, 6] and len(rt.ResidualHistory.COLUMNS) == len(rows[0])

@@ -276,3 +276,75 @@ def test_transport_assembly_known_answers(oracle_mod):
     diag2 = np.array([A2[rp[i] + np.searchsorted(cols[rp[i]:rp[i + 1]], i)] for i in range(m.nn)])
     np.testing.assert_allclose(diag2, (diag + sd) / 0.5, rtol=1e-13)
     np.testing.assert_allclose(b2, b + sr, atol=1e-14 * scale)
+
+
+def _linear_state(oc, m, G):
+    oc.field("U")[:] = (m.coords @ G.T).ravel()
+    for k in ("p", "gradP", "mDot", "div"):
+        oc.field(k)[:] = 0.0
+
+
+def test_symmetry_planes_close_every_control_volume(oracle_mod):
+    # a linear velocity field with uniform mu, no pressure and no mass flow: the
+    # interior viscous fluxes of a control volume cancel except where its surface
+    # meets the boundary; the symmetry term (the full stress at the face ip)
+    # closes it, so with every face a symmetry plane the momentum residual
+    # vanishes at every node, while a no-slip wall leaves its zero-normal-stress
+    # projection behind
+    m = meshgen.symmetry_box(4, perturb=0.25, seed=3)
+    G = np.random.default_rng(1).normal(size=(3, 3))
+    res = {}
+    for name, types in (("sym", [1, 1, 1, 1]), ("mixed", [0, 0, 1, 1]), ("wall", [0, 0, 0, 0])):
+        oc = oracle_mod.FlowCase(m, oracle_mod.default_settings())
+        oc.set_boundary_types(types)
+        _linear_state(oc, m, G)
+        _, b = oc.assemble_momentum()
+        res[name] = np.abs(b).max()
+    assert res["sym"] < 1e-15
+    assert res["mixed"] > 1e-4 and res["wall"] > 1e-4
+
+
+def test_symmetry_area_and_side_velocity(oracle_mod):
+    m = meshgen.symmetry_box((4, 3, 5), perturb=0.2, seed=4, lid_velocity=(1.0, 0.0, 0.0))
+    oc = oracle_mod.FlowCase(m, oracle_mod.default_settings())
+    oc.set_boundary_types([0, 0, 1, 1])
+    area = oc.field("symArea").reshape(-1, 3)
+    y = m.coords[:, 1]
+    on0, on1 = np.isclose(y, 0.0), np.isclose(y, 1.0)
+    # the planes are flat: every assembled area is along -y (y = 0) or +y (y = 1),
+    # and each plane's areas add up to the plane's area (1)
+    assert np.abs(area[:, [0, 2]]).max() < 1e-15
+    assert abs(area[on0, 1].sum() + 1.0) < 1e-14 and abs(area[on1, 1].sum() - 1.0) < 1e-14
+    assert np.all(area[~(on0 | on1)] == 0.0)
+    # the lid's velocity reaches the lid nodes on the symmetry planes (the
+    # symmetry boundaries no longer overwrite them), the walls win at their edges
+    side = oc.field("sideU").reshape(-1, 3)
+    x, z = m.coords[:, 0], m.coords[:, 2]
+    lid_sym = np.isclose(z, 1.0) & (on0 | on1) & ~np.isclose(x, 0.0) & ~np.isclose(x, 1.0)
+    assert lid_sym.any() and np.all(side[lid_sym, 0] == 1.0)
+    with pytest.raises(ValueError):
+        oc.set_boundary_types([0, 0, 2, 1])
+    with pytest.raises(ValueError):
+        oc.set_boundary_types([0, 1])
+
+
+def test_symmetry_gradient_correction(oracle_mod):
+    # with correctGradients_ the pressure gradient at a symmetry node has no
+    # normal (y) part and the velocity gradient keeps only its in-plane
+    # components and the normal-normal one
+    m = meshgen.symmetry_box(4, perturb=0.2, seed=6)
+    rng = np.random.default_rng(6)
+    oc = oracle_mod.FlowCase(m, oracle_mod.default_settings())
+    oc.set_boundary_types([0, 0, 1, 1], correct_gradients=True)
+    oc.field("p")[:] = rng.normal(size=m.nn)
+    oc.field("U")[:] = rng.normal(size=3 * m.nn)
+    oc.update_grad_p()
+    oc.update_grad_u()
+    y = m.coords[:, 1]
+    sym = np.isclose(y, 0.0) | np.isclose(y, 1.0)
+    gp = oc.field("gradP").reshape(-1, 3)
+    gu = oc.field("gradU").reshape(-1, 3, 3)
+    assert np.abs(gp[sym, 1]).max() < 1e-13 and np.abs(gp[~sym, 1]).max() > 1e-3
+    # G_iy = 0 for i != y and G_yj = 0 for j != y
+    assert np.abs(gu[sym][:, [0, 2], 1]).max() < 1e-13 and np.abs(gu[sym][:, 1, [0, 2]]).max() < 1e-13
+    assert np.abs(gu[sym][:, 1, 1]).max() > 1e-3
