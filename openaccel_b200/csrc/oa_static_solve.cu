@@ -21,8 +21,7 @@
 //    overwrites every region it reads before reading it (the iterate and the
 //    search directions start from zero fills it issues itself);
 //  - the first call on a device looks up the array's device address
-//    (cudaGetSymbolAddress) and caches it; make that first call before any
-//    stream capture;
+//    (cudaGetSymbolAddress) and caches it;
 //  - a breakdown, a diverging iteration or a solve that ends above rtol
 //    returns OA_ERR_SOLVER (the status is named in oa_last_error); x then
 //    holds the last iterate.
