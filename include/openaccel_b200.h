@@ -213,7 +213,11 @@ int oa_update_mdot(oa_flow* f);
 /* flowModel::updateMassDivergenceField_ (flowModel.cpp:13541-14948, interior). */
 int oa_update_div(oa_flow* f);
 /* nodeField::updateGradientField (src/field/nodeField/nodeField.hpp:3253-4948);
- * which = 0: pressure, 1: velocity. */
+ * which = 0: pressure, 1: velocity, 2: k, 3: omega (fields "gradK",
+ * "gradOmega" [nn][3] after oa_flow_enable_turbulence, else OA_ERR_NOT_READY;
+ * the SST driver's updateTurbulent{KineticEnergy,EddyFrequency}GradientField,
+ * segregatedShearStressTransportEquations.cpp:96-98, with the turbulence
+ * fields' default linear_linear interpolation, controls.h:97-102). */
 int oa_update_gradient(oa_flow* f, int which);
 /* Linear solve of the last assembled system: linearSystem::solve()
  * (src/equation/linearSystem.h:416-462). sys = 0 momentum (x [nn][3]), 1
@@ -394,6 +398,18 @@ void oa_sst_default_constants(oa_sst_constants* c);
 /* Launch on `stream` (NULL: default stream); asynchronous. */
 int oa_sst_node_update(int nn, const oa_sst_constants* c, double dt, double mut_urf, const oa_sst_fields* f,
                        void* stream);
+/* The SST driver's viscosity updates (segregatedShearStressTransportEquations
+ * preSolve and the k / omega equations' diffusivity setup): mu_eff = mu + mu_t
+ * (turbulenceModel::updateEffectiveDynamicViscosity,
+ * src/model/turbulence/turbulenceModel.cpp:121-150) and the diffusivities
+ * gamma_k = mu + mu_t (F1 sigma_k1 + (1 - F1) sigma_k2), gamma_w likewise with
+ * sigma_w1 / sigma_w2 (turbulentKineticEnergySSTEquation.cpp:55-75,
+ * turbulentEddyFrequencySSTEquation.cpp:55-75). mu is the laminar viscosity.
+ * Device pointers [nn]; outputs may be a flow's "mu", "gammaK" and
+ * "gammaOmega" fields (oa_flow_field_device_ptr), but not alias the inputs.
+ * Launch on `stream` (NULL: default stream); asynchronous. */
+int oa_sst_diffusivities(int nn, const oa_sst_constants* c, const double* mu, const double* mut, const double* F1,
+                         double* mu_eff, double* gamma_k, double* gamma_w, void* stream);
 
 /* Fused u/v/w/k/omega assembly. After this call every momentum assembly of the
  * flow (oa_assemble_momentum, oa_simple_iterate) assembles in the same launch
@@ -409,7 +425,9 @@ int oa_sst_node_update(int nn, const oa_sst_constants* c, double dt, double mut_
  * "srcDiagOmega" / "srcRhsOmega" (for instance the k_diag / k_rhs / w_diag /
  * w_rhs outputs of oa_sst_node_update written to their device pointers); the
  * diagonal is then relaxed by 1/urf (phiAssembler.h:967-1006). k and omega are
- * the fields "k" and "omega". Creates these fields (zero); steady upwind SIMPLE
+ * the fields "k" and "omega", their gradients "gradK" / "gradOmega" [nn][3]
+ * (oa_update_gradient 2 / 3, the SST node update's gradK / gradW inputs).
+ * Creates these fields (zero); steady upwind SIMPLE
  * flows only (no high resolution, SIMPLEC, fractional step or time stepping:
  * OA_ERR_ARG). */
 int oa_flow_enable_turbulence(oa_flow* f, double urf_k, double urf_omega);

@@ -184,6 +184,10 @@ double* field_ptr(Flow& f, const std::string& n, size_t* len) {
   if (f.duT && n == "duTilde") { *len = 3 * nn; return f.duT; }
   if (f.Uold && n == "Uold") { *len = 3 * nn; return f.Uold; }
   if (f.Uoldold && n == "Uoldold") { *len = 3 * nn; return f.Uoldold; }
+  if (f.turb && (n == "gradK" || n == "gradOmega")) {
+    *len = 3 * nn;
+    return n == "gradK" ? f.gradK : f.gradW;
+  }
   if (f.turb) {
     *len = nn;
     if (n == "k") return f.kf;
@@ -873,7 +877,8 @@ void oa_flow_destroy(oa_flow* H) {
                   f.b.A_pc,  f.b.b_pc,  f.b.x_mom, f.b.x_pc,  f.err_dev, H->scal,  f.red,   f.ref_flag,
                   f.betaU,   f.minU,    f.maxU,    f.duT,     f.Uold,    f.Uoldold, f.kf,      f.wf,
                   f.gkf,     f.gwf,     f.sdk,     f.srk,     f.sdw,     f.srw,     f.A_k,     f.b_k,
-                  f.A_w,     f.b_w,     f.sym_mask, f.sym_nodes, f.sym_area, f.wall_face_node};
+                  f.A_w,     f.b_w,     f.sym_mask, f.sym_nodes, f.sym_area, f.wall_face_node,
+                  f.gradK,   f.gradW};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (H->hscal) cudaFreeHost(H->hscal);
@@ -1116,7 +1121,9 @@ int oa_update_div(oa_flow* H) {
 }
 
 int oa_update_gradient(oa_flow* H, int which) {
-  if (!H || (which != 0 && which != 1)) return fail(OA_ERR_ARG, "oa_update_gradient: bad arguments");
+  if (!H || which < 0 || which > 3) return fail(OA_ERR_ARG, "oa_update_gradient: bad arguments");
+  if (which >= 2 && !H->f.turb)
+    return fail(OA_ERR_NOT_READY, "oa_update_gradient: k / omega gradients need oa_flow_enable_turbulence");
   return launch_gradient(H->f, which);
 }
 
@@ -1243,6 +1250,11 @@ int oa_flow_enable_turbulence(oa_flow* H, double urf_k, double urf_omega) {
     if (*p) continue;
     if (int s = dalloc(p, nn)) return s;
     OA_CUDA(cudaMemset(*p, 0, sizeof(double) * nn));
+  }
+  for (double** p : {&f.gradK, &f.gradW}) {
+    if (*p) continue;
+    if (int s = dalloc(p, 3 * nn)) return s;
+    OA_CUDA(cudaMemset(*p, 0, sizeof(double) * 3 * nn));
   }
   void** sys[] = {&f.A_k, &f.A_w};
   for (void** p : sys)

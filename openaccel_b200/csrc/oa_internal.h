@@ -107,6 +107,8 @@ struct Flow {
   double *kf = nullptr, *wf = nullptr, *gkf = nullptr, *gwf = nullptr;
   double *sdk = nullptr, *srk = nullptr, *sdw = nullptr, *srw = nullptr;
   void *A_k = nullptr, *b_k = nullptr, *A_w = nullptr, *b_w = nullptr;
+  // gradients of k and omega [nn][3] (oa_update_gradient 2 and 3)
+  double *gradK = nullptr, *gradW = nullptr;
   double urf_k = 1.0, urf_w = 1.0;
   // [ne][12] Rhie-Chow mass flux of each SCS ip with the pressure-correction
   // equation's upwind density (its right-hand side), written by the mass-flow

@@ -1558,8 +1558,10 @@ int launch_sym_area(Flow& f, double* area_nn) {
 static int launch_sym_grad(Flow& f, int which) {
   if (!f.nsym || !f.correct_grad) return OA_OK;
   const unsigned g = (unsigned)((f.nsym + BLOCK - 1) / BLOCK);
-  if (which == 0) k_sym_grad<1><<<g, BLOCK, 0, f.stream>>>(f.nsym, f.sym_nodes, f.sym_area, f.gradP);
-  else k_sym_grad<3><<<g, BLOCK, 0, f.stream>>>(f.nsym, f.sym_nodes, f.sym_area, f.gradU);
+  if (which == 1) k_sym_grad<3><<<g, BLOCK, 0, f.stream>>>(f.nsym, f.sym_nodes, f.sym_area, f.gradU);
+  else
+    k_sym_grad<1><<<g, BLOCK, 0, f.stream>>>(f.nsym, f.sym_nodes, f.sym_area,
+                                             which == 0 ? f.gradP : (which == 2 ? f.gradK : f.gradW));
   count_launches(1);
   OA_CUDA(cudaGetLastError());
   return OA_OK;
@@ -1568,7 +1570,14 @@ static int launch_sym_grad(Flow& f, int which) {
 int launch_gradient(Flow& f, int which) {
   const int bs = f.bs_rows;
   const int g = grid_rows(*f.mesh, bs);
-  if (which == 0) {
+  if (which >= 2) {
+    // k (2) and omega (3): the turbulence fields' default interpolation is
+    // linear_linear (controls.h:97-102), the shifted gradient operator
+    if (!f.turb) return fail(OA_ERR_NOT_READY, "gradient of k / omega: turbulence transport not enabled");
+    GradArgs a{f.view(), which == 2 ? f.kf : f.wf, which == 2 ? f.gradK : f.gradW, f.s.grad_urf};
+    if (f.mesh->lpr == 16) k_gradient<16, 1, true><<<g, bs, 0, f.stream>>>(a);
+    else k_gradient<8, 1, true><<<g, bs, 0, f.stream>>>(a);
+  } else if (which == 0) {
     GradArgs a{f.view(), f.p, f.gradP, f.s.grad_urf};
     if (f.mesh->lpr == 16) {
       if (f.s.p_shifted) k_gradient<16, 1, true><<<g, bs, 0, f.stream>>>(a);

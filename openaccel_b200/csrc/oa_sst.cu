@@ -122,6 +122,25 @@ __global__ void __launch_bounds__(256) k_sst_nodes(SstArgs a) {
   }
 }
 
+// The driver's viscosity updates after the node update, one thread per node:
+// mu_eff = mu + mu_t (turbulenceModel::updateEffectiveDynamicViscosity,
+// src/model/turbulence/turbulenceModel.cpp:121-150) and the k and omega
+// diffusivities mu + mu_t (F1 sigma_1 + (1 - F1) sigma_2)
+// (turbulentKineticEnergySSTEquation.cpp:55-75,
+// turbulentEddyFrequencySSTEquation.cpp:55-75).
+__global__ void k_sst_diffusivities(int nn, double sk1, double sk2, double sw1, double sw2,
+                                    const double* __restrict__ mu, const double* __restrict__ mut,
+                                    const double* __restrict__ F1, double* mu_eff, double* gk, double* gw) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nn) return;
+  const double m = mu[i], t = mut[i], f1 = F1[i];
+  const double ck = f1 * sk1 + (1.0 - f1) * sk2;
+  const double cw = f1 * sw1 + (1.0 - f1) * sw2;
+  gk[i] = m + t * ck;
+  gw[i] = m + t * cw;
+  mu_eff[i] = m + t;
+}
+
 }  // namespace
 }  // namespace oa
 
@@ -156,6 +175,18 @@ int oa_sst_node_update(int nn, const oa_sst_constants* c, double dt, double mut_
   if (nn == 0) return OA_OK;
   SstArgs a{*c, *f, dt, mut_urf, nn};
   k_sst_nodes<<<(nn + 255) / 256, 256, 0, static_cast<cudaStream_t>(stream)>>>(a);
+  count_launches(1);
+  OA_CUDA(cudaGetLastError());
+  return OA_OK;
+}
+
+int oa_sst_diffusivities(int nn, const oa_sst_constants* c, const double* mu, const double* mut, const double* F1,
+                         double* mu_eff, double* gamma_k, double* gamma_w, void* stream) {
+  if (nn < 0 || !c || !mu || !mut || !F1 || !mu_eff || !gamma_k || !gamma_w)
+    return fail(OA_ERR_ARG, "oa_sst_diffusivities: bad arguments");
+  if (nn == 0) return OA_OK;
+  k_sst_diffusivities<<<(nn + 255) / 256, 256, 0, static_cast<cudaStream_t>(stream)>>>(
+      nn, c->sigma_k1, c->sigma_k2, c->sigma_w1, c->sigma_w2, mu, mut, F1, mu_eff, gamma_k, gamma_w);
   count_launches(1);
   OA_CUDA(cudaGetLastError());
   return OA_OK;

@@ -34,7 +34,7 @@ EXPORTS = [
     "oa_flow_stream", "oa_launch_count", "oa_time_kernel", "oa_pcorr_solve_static",
     "oa_diffusion_create", "oa_diffusion_destroy", "oa_diffusion_set_field", "oa_diffusion_get_field",
     "oa_diffusion_field_device_ptr", "oa_diffusion_assemble", "oa_diffusion_solve", "oa_diffusion_step",
-    "oa_diffusion_stream", "oa_diffusion_time_assembly", "oa_sst_default_constants", "oa_sst_node_update",
+    "oa_diffusion_stream", "oa_diffusion_time_assembly", "oa_sst_default_constants", "oa_sst_node_update", "oa_sst_diffusivities",
     "oa_flow_last_control", "oa_flow_scales", "oa_flow_advance_time", "oa_flow_autotune", "oa_flow_set_tuning",
     "oa_flow_enable_turbulence", "oa_flow_turbulence_systems", "oa_flow_solve_turbulence",
 ]
@@ -246,6 +246,7 @@ def lib():
         "oa_diffusion_time_assembly": (C.c_int, [vp, C.c_int, dp]),
         "oa_sst_default_constants": (None, [P(SstConstants)]),
         "oa_sst_node_update": (C.c_int, [C.c_int, P(SstConstants), C.c_double, C.c_double, P(SstFields), vp]),
+        "oa_sst_diffusivities": (C.c_int, [C.c_int, P(SstConstants), vp, vp, vp, vp, vp, vp, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -323,7 +324,7 @@ class Flow:
     FIELD_SHAPES = {"U": 3, "p": 1, "gradU": 9, "gradP": 3, "du": 3, "div": 1, "sideU": 3, "rho": 1, "mu": 1,
                     "betaU": 3, "minU": 3, "maxU": 3, "duTilde": 3, "Uold": 3, "Uoldold": 3,
                     "k": 1, "omega": 1, "gammaK": 1, "gammaOmega": 1, "srcDiagK": 1, "srcRhsK": 1,
-                    "srcDiagOmega": 1, "srcRhsOmega": 1}
+                    "srcDiagOmega": 1, "srcRhsOmega": 1, "gradK": 3, "gradOmega": 3}
 
     def __init__(self, mesh: Mesh, settings: FlowSettings | None = None):
         self.mesh = mesh
@@ -384,7 +385,7 @@ class Flow:
         _check(lib().oa_update_div(self.h))
 
     def update_gradient(self, which):
-        _check(lib().oa_update_gradient(self.h, {"p": 0, "U": 1}.get(which, which)))
+        _check(lib().oa_update_gradient(self.h, {"p": 0, "U": 1, "k": 2, "omega": 3}.get(which, which)))
 
     def solve(self, sys, rtol, maxit):
         n = 3 * self.mesh.nn if sys in (0, "momentum") else self.mesh.nn
@@ -553,6 +554,15 @@ def sst_constants() -> SstConstants:
     c = SstConstants()
     lib().oa_sst_default_constants(C.byref(c))
     return c
+
+
+def sst_diffusivities(nn: int, mu, mut, F1, mu_eff, gamma_k, gamma_w, constants: SstConstants | None = None,
+                      stream=0):
+    """mu_eff = mu + mu_t and the F1-blended k / omega diffusivities on device
+    pointers (ints); asynchronous on ``stream``."""
+    c = constants or sst_constants()
+    args = [C.c_void_p(int(p)) for p in (mu, mut, F1, mu_eff, gamma_k, gamma_w)]
+    _check(lib().oa_sst_diffusivities(int(nn), C.byref(c), *args, C.c_void_p(stream or None)))
 
 
 def sst_node_update(nn: int, ptrs: dict, dt=1.0, mut_urf=1.0, constants: SstConstants | None = None, stream=0):

@@ -183,6 +183,9 @@ void orc_sst_default_constants(orc_sst_constants* c);
 /* mu_t, F1, P_k and the steady k / omega node-term diagonal and rhs per node */
 void orc_sst_nodes(int nn, const orc_sst_constants* c, double dt, double mut_urf, const orc_sst_in* in,
                    orc_sst_out* out);
+/* mu_eff = mu + mu_t and the F1-blended k / omega diffusivities per node */
+void orc_sst_diffusivities(int nn, const orc_sst_constants* c, const double* mu, const double* mut, const double* F1,
+                           double* mu_eff, double* gamma_k, double* gamma_w);
 
 #ifdef __cplusplus
 }

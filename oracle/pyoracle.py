@@ -179,6 +179,7 @@ def lib():
         L.orc_diff_bicgstab.argtypes = [C.c_void_p, dp, dp, dp, C.c_double, C.c_int, dp]
         L.orc_sst_default_constants.argtypes = [P(SstConstants)]
         L.orc_sst_nodes.argtypes = [C.c_int, P(SstConstants), C.c_double, C.c_double, P(SstIn), P(SstOut)]
+        L.orc_sst_diffusivities.argtypes = [C.c_int, P(SstConstants)] + [dp] * 6
         L.orc_diff_step.restype = C.c_int
         L.orc_diff_step.argtypes = [C.c_void_p, dp]
         _lib = L
@@ -483,3 +484,12 @@ def sst_nodes(fields: dict, dt=1.0, mut_urf=1.0, constants: SstConstants | None 
     c = constants or sst_constants()
     lib().orc_sst_nodes(nn, C.byref(c), dt, mut_urf, C.byref(si), C.byref(so))
     return outs
+
+
+def sst_diffusivities(mu, mut, F1, constants: SstConstants | None = None):
+    """(mu_eff, gamma_k, gamma_omega) of the SST driver's viscosity updates."""
+    mu, mut, F1 = (np.ascontiguousarray(a, np.float64) for a in (mu, mut, F1))
+    out = [np.zeros(mu.shape[0]) for _ in range(3)]
+    c = constants or sst_constants()
+    lib().orc_sst_diffusivities(mu.shape[0], C.byref(c), _dp(mu), _dp(mut), _dp(F1), *[_dp(a) for a in out])
+    return tuple(out)

@@ -135,4 +135,20 @@ void orc_sst_nodes(int nn, const orc_sst_constants* C, double dt, double mut_urf
   }
 }
 
+// turbulenceModel::updateEffectiveDynamicViscosity
+// (src/model/turbulence/turbulenceModel.cpp:121-150): mu_eff = mu + mu_t; the
+// diffusivity setup of turbulentKineticEnergySSTEquation.cpp:55-75 and
+// turbulentEddyFrequencySSTEquation.cpp:55-75: mu + mu_t times the constant
+// blended by F1 between the inner (1) and outer (2) values.
+void orc_sst_diffusivities(int nn, const orc_sst_constants* C, const double* mu, const double* mut, const double* F1,
+                           double* mu_eff, double* gamma_k, double* gamma_w) {
+  for (int i = 0; i < nn; ++i) {
+    const double bk = F1[i] * C->sigma_k1 + (1.0 - F1[i]) * C->sigma_k2;
+    const double bw = F1[i] * C->sigma_w1 + (1.0 - F1[i]) * C->sigma_w2;
+    gamma_k[i] = mu[i] + mut[i] * bk;
+    gamma_w[i] = mu[i] + mut[i] * bw;
+    mu_eff[i] = mu[i] + mut[i];
+  }
+}
+
 }  // extern "C"

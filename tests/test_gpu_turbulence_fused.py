@@ -170,3 +170,84 @@ def test_sst_node_update_feeds_the_fused_assembly(oracle_mod):
     Aw_o, bw_o = oc.assemble_transport(turb["omega"], turb["gammaOmega"], src["srcDiagOmega"], src["srcRhsOmega"], 0.9)
     assert rel(A_k, Ak_o) < 1e-12 and rel(b_k, bk_o) < 1e-12
     assert rel(A_w, Aw_o) < 1e-12 and rel(b_w, bw_o) < 1e-12
+
+
+@pytest.mark.parametrize("mesh", ["cavity", "star5", "symmetry"])
+def test_turbulence_field_gradients(oracle_mod, mesh):
+    # Green-Gauss gradients of k and omega (the SST driver's post-correction
+    # gradient updates) against the oracle's scalar gradient on the same field,
+    # with the turbulence fields' linear_linear operator and the relaxation;
+    # on the symmetry box with the gradient correction at the symmetry nodes
+    if mesh == "cavity":
+        m = meshgen.cavity(7, perturb=0.2, seed=3)
+    elif mesh == "star5":
+        m = meshgen.star_prism(5, 4, 3, perturb=0.2)
+    else:
+        m = meshgen.symmetry_box(6, perturb=0.2, seed=3)
+    oc, gf, turb = setup(oracle_mod, m, rt.OA_PREC_FP64, seed=3)
+    with pytest.raises(rt.OpenAccelError) as ei:
+        gf.update_gradient("k")
+    assert ei.value.status == 6
+    if mesh == "symmetry":
+        types = [rt.OA_BTYPE_WALL, rt.OA_BTYPE_WALL, rt.OA_BTYPE_SYMMETRY, rt.OA_BTYPE_SYMMETRY]
+        oc.set_boundary_types(types, correct_gradients=True)
+        gf.set_boundary_types(types, correct_gradients=True)
+    gf.enable_turbulence(0.8, 0.8)
+    for name, grad in (("k", "gradK"), ("omega", "gradOmega")):
+        gf.set_field(name, turb[name])
+        oc.field("p")[:] = turb[name]
+        oc.field("gradP")[:] = 0.0
+        for _ in range(2):
+            oc.update_grad_p()
+            gf.update_gradient(name)
+        assert rel(gf.get_field(grad), oc.field("gradP")) < 1e-12, name
+
+
+def test_sst_chain_on_device(oracle_mod):
+    # one SST update entirely on the device, through the library's own fields:
+    # k / omega gradients (oa_update_gradient), the node update (mu_t, F1,
+    # node terms written into the flow's source fields), then mu_eff and the
+    # F1-blended diffusivities written into the flow's "mu", "gammaK" and
+    # "gammaOmega"; each stage against the oracle on the same inputs
+    import torch
+
+    m = meshgen.cavity(6, perturb=0.2, seed=12)
+    oc, gf, turb = setup(oracle_mod, m, rt.OA_PREC_FP64, seed=12)
+    gf.enable_turbulence(0.9, 0.9)
+    for k in ("k", "omega"):
+        gf.set_field(k, turb[k])
+    gf.update_gradient("k")
+    gf.update_gradient("omega")
+    grads = {}
+    for name in ("k", "omega"):
+        oc.field("p")[:] = turb[name]
+        oc.field("gradP")[:] = 0.0
+        oc.update_grad_p()
+        grads[name] = oc.field("gradP").copy()
+    assert rel(gf.get_field("gradK"), grads["k"]) < 1e-12 and rel(gf.get_field("gradOmega"), grads["omega"]) < 1e-12
+    rng = np.random.default_rng(4)
+    dev = torch.device("cuda")
+    host = {"k_prev": turb["k"], "rho": np.ones(m.nn), "mu": np.full(m.nn, 1e-2), "ymin": rng.uniform(1e-3, 0.5, m.nn),
+            "gradU": rng.normal(0, 1, 9 * m.nn), "div": np.zeros(m.nn), "vol": gf.mesh.dual_volume(),
+            "mut_old": np.zeros(m.nn)}
+    t = {n: torch.from_numpy(np.ascontiguousarray(v)).to(dev) for n, v in host.items()}
+    t["wall_node"] = torch.zeros(m.nn, dtype=torch.int32, device=dev)
+    for n in ("mut", "F1", "Pk"):
+        t[n] = torch.empty(m.nn, dtype=torch.float64, device=dev)
+    ptrs = {n: v.data_ptr() for n, v in t.items()}
+    ptrs.update(k=gf.device_ptr("k"), omega=gf.device_ptr("omega"), gradK=gf.device_ptr("gradK"),
+                gradW=gf.device_ptr("gradOmega"), k_diag=gf.device_ptr("srcDiagK"), k_rhs=gf.device_ptr("srcRhsK"),
+                w_diag=gf.device_ptr("srcDiagOmega"), w_rhs=gf.device_ptr("srcRhsOmega"))
+    rt.sst_node_update(m.nn, ptrs)
+    rt.sst_diffusivities(m.nn, ptrs["mu"], ptrs["mut"], ptrs["F1"], gf.device_ptr("mu"), gf.device_ptr("gammaK"),
+                         gf.device_ptr("gammaOmega"))
+    torch.cuda.synchronize()
+    ref = oracle_mod.sst_nodes(dict(host, k=turb["k"], omega=turb["omega"], gradK=grads["k"], gradW=grads["omega"],
+                                    wall_node=np.zeros(m.nn, np.int32), pk_wall=None))
+    for n in ("mut", "F1"):
+        assert rel(t[n].cpu().numpy(), ref[n]) < 1e-12, n
+    for n, g in (("k_diag", "srcDiagK"), ("k_rhs", "srcRhsK"), ("w_diag", "srcDiagOmega"), ("w_rhs", "srcRhsOmega")):
+        assert rel(gf.get_field(g), ref[n]) < 1e-12, n
+    mu_eff, gk, gw = oracle_mod.sst_diffusivities(host["mu"], ref["mut"], ref["F1"])
+    assert rel(gf.get_field("mu"), mu_eff) < 1e-12
+    assert rel(gf.get_field("gammaK"), gk) < 1e-12 and rel(gf.get_field("gammaOmega"), gw) < 1e-12

@@ -55,3 +55,16 @@ def test_negative_divergence_goes_to_the_diagonal(oracle_mod):
     o0 = oracle_mod.sst_nodes(f0)
     np.testing.assert_allclose(o["k_diag"] - o0["k_diag"], [0.5, 0.0], atol=1e-15)
     np.testing.assert_allclose(o["k_rhs"] - o0["k_rhs"], [-0.5 * 1e-2, 0.5 * 1e-2], rtol=1e-12)
+
+
+def test_sst_diffusivities_known_answers(oracle_mod):
+    # F1 = 1 takes the inner constants, F1 = 0 the outer ones, mu_eff = mu + mu_t
+    c = oracle_mod.sst_constants()
+    mu = np.array([1e-3, 1e-3, 2e-3])
+    mut = np.array([0.5, 0.5, 0.0])
+    F1 = np.array([1.0, 0.0, 0.3])
+    mu_eff, gk, gw = oracle_mod.sst_diffusivities(mu, mut, F1, c)
+    np.testing.assert_allclose(mu_eff, mu + mut, rtol=0, atol=0)
+    np.testing.assert_allclose(gk[:2], [1e-3 + 0.5 * c.sigma_k1, 1e-3 + 0.5 * c.sigma_k2], rtol=1e-15)
+    np.testing.assert_allclose(gw[:2], [1e-3 + 0.5 * c.sigma_w1, 1e-3 + 0.5 * c.sigma_w2], rtol=1e-15)
+    assert gk[2] == mu[2] and gw[2] == mu[2]
