@@ -442,6 +442,29 @@ int oa_flow_turbulence_systems(oa_flow* f, double* A_k, double* b_k, double* A_o
  * and the lower clip SMALL, src/equation/equation.h:204-286). Iteration counts
  * may be NULL. OA_ERR_NOT_READY before oa_flow_enable_turbulence. */
 int oa_flow_solve_turbulence(oa_flow* f, double rtol, int maxit, int* iters_k, int* iters_omega);
+/* n outer iterations of the flow with the k-omega SST equations
+ * (segregatedFlowEquations::solve followed by
+ * segregatedShearStressTransportEquations::preSolve / solve,
+ * segregatedShearStressTransportEquations.cpp:63-99), all on the device. Each
+ * iteration: k.prevIter = k; one SIMPLE outer iteration whose momentum launch
+ * also assembles the k and omega systems (oa_simple_iterate; stats[it] when
+ * stats is not NULL); the k and omega solves to rtol with the clipped
+ * correction (oa_flow_solve_turbulence); their gradients (oa_update_gradient 2
+ * and 3); the SST node update (oa_sst_node_update with dt = settings.dt, the
+ * flow's k, omega, gradients, U gradient, divergence, density and dual volumes,
+ * the caller's laminar viscosity mu_lam, wall distance ymin and wall flags,
+ * mu_t relaxed by mut_urf against its previous value, node terms into the
+ * flow's source fields); then mu_eff into the flow's "mu" and the diffusivities
+ * into "gammaK" / "gammaOmega" (oa_sst_diffusivities). The flow owns mu_t, F1
+ * and P_k (fields "mut", "F1", "Pk" [nn], zero before the first call). The k
+ * and omega systems of an iteration are assembled from the node terms of the
+ * previous update, on the iteration's starting mass flows (the reference
+ * assembles them after the pressure correction). Wall functions are not
+ * modelled: wall production comes from the node kernel's wall treatment.
+ * ymin, wall_node, mu_lam: device pointers [nn]. OA_ERR_NOT_READY before
+ * oa_flow_enable_turbulence. */
+int oa_flow_sst_iterate(oa_flow* f, int n, const oa_sst_constants* c, const double* ymin, const int* wall_node,
+                        const double* mu_lam, double mut_urf, double rtol, int maxit, oa_iter_stats* stats);
 
 #ifdef __cplusplus
 }

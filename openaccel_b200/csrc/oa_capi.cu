@@ -184,6 +184,10 @@ double* field_ptr(Flow& f, const std::string& n, size_t* len) {
   if (f.duT && n == "duTilde") { *len = 3 * nn; return f.duT; }
   if (f.Uold && n == "Uold") { *len = 3 * nn; return f.Uold; }
   if (f.Uoldold && n == "Uoldold") { *len = 3 * nn; return f.Uoldold; }
+  if (f.mut && (n == "mut" || n == "F1" || n == "Pk")) {
+    *len = nn;
+    return n == "mut" ? f.mut : (n == "F1" ? f.F1 : f.Pk);
+  }
   if (f.turb && (n == "gradK" || n == "gradOmega")) {
     *len = 3 * nn;
     return n == "gradK" ? f.gradK : f.gradW;
@@ -878,7 +882,7 @@ void oa_flow_destroy(oa_flow* H) {
                   f.betaU,   f.minU,    f.maxU,    f.duT,     f.Uold,    f.Uoldold, f.kf,      f.wf,
                   f.gkf,     f.gwf,     f.sdk,     f.srk,     f.sdw,     f.srw,     f.A_k,     f.b_k,
                   f.A_w,     f.b_w,     f.sym_mask, f.sym_nodes, f.sym_area, f.wall_face_node,
-                  f.gradK,   f.gradW};
+                  f.gradK,   f.gradW,   f.mut,     f.F1,      f.Pk,      f.k_prev};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (H->hscal) cudaFreeHost(H->hscal);
@@ -1310,6 +1314,60 @@ int oa_flow_solve_turbulence(oa_flow* H, double rtol, int maxit, int* iters_k, i
   OA_CUDA(cudaGetLastError());
   OA_CUDA(cudaStreamSynchronize(f.stream));
   return OA_OK;
+}
+
+int oa_flow_sst_iterate(oa_flow* H, int n, const oa_sst_constants* c, const double* ymin, const int* wall_node,
+                        const double* mu_lam, double mut_urf, double rtol, int maxit, oa_iter_stats* stats) {
+  if (!H || n < 0 || !c || !ymin || !wall_node || !mu_lam || !(mut_urf > 0 && mut_urf <= 1) || !(rtol > 0) ||
+      maxit <= 0)
+    return fail(OA_ERR_ARG, "oa_flow_sst_iterate: bad arguments");
+  Flow& f = H->f;
+  if (!f.turb) return fail(OA_ERR_NOT_READY, "oa_flow_sst_iterate: turbulence transport not enabled");
+  const size_t nn = f.mesh->nn;
+  for (double** p : {&f.mut, &f.F1, &f.Pk, &f.k_prev}) {
+    if (*p) continue;
+    if (int s = dalloc(p, nn)) return s;
+    OA_CUDA(cudaMemsetAsync(*p, 0, sizeof(double) * nn, f.stream));
+  }
+  for (int it = 0; it < n; ++it) {
+    // the previous-iteration k of the omega node terms (k.prevIter)
+    OA_CUDA(cudaMemcpyAsync(f.k_prev, f.kf, sizeof(double) * nn, cudaMemcpyDeviceToDevice, f.stream));
+    // flow: u/v/w/k/omega assembled in one launch, momentum and pressure
+    // correction solved and corrected
+    if (int s = oa_simple_iterate(H, 1, stats ? stats + it : nullptr)) return s;
+    // k and omega solved and corrected, then their gradients
+    if (int s = oa_flow_solve_turbulence(H, rtol, maxit, nullptr, nullptr)) return s;
+    if (int s = launch_gradient(f, 2)) return s;
+    if (int s = launch_gradient(f, 3)) return s;
+    // mu_t, F1, production and the node terms of the next assembly, then
+    // mu_eff and the diffusivities
+    oa_sst_fields sf{};
+    sf.k = f.kf;
+    sf.omega = f.wf;
+    sf.k_prev = f.k_prev;
+    sf.rho = f.rho;
+    sf.mu = mu_lam;
+    sf.ymin = ymin;
+    sf.gradU = f.gradU;
+    sf.gradK = f.gradK;
+    sf.gradW = f.gradW;
+    sf.div = f.div;
+    sf.vol = f.mesh->vol;
+    sf.mut_old = f.mut;
+    sf.pk_wall = nullptr;
+    sf.wall_node = wall_node;
+    sf.mut = f.mut;
+    sf.F1 = f.F1;
+    sf.Pk = f.Pk;
+    sf.k_diag = f.sdk;
+    sf.k_rhs = f.srk;
+    sf.w_diag = f.sdw;
+    sf.w_rhs = f.srw;
+    if (int s = oa_sst_node_update((int)nn, c, f.s.dt, mut_urf, &sf, f.stream)) return s;
+    if (int s = oa_sst_diffusivities((int)nn, c, mu_lam, f.mut, f.F1, f.mu, f.gkf, f.gwf, f.stream)) return s;
+  }
+  OA_CUDA(cudaStreamSynchronize(f.stream));
+  return check_err_flag(f, "oa_flow_sst_iterate");
 }
 
 int oa_flow_set_tuning(oa_flow* H, const oa_tuning* t) {

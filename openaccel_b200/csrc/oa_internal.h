@@ -109,6 +109,9 @@ struct Flow {
   void *A_k = nullptr, *b_k = nullptr, *A_w = nullptr, *b_w = nullptr;
   // gradients of k and omega [nn][3] (oa_update_gradient 2 and 3)
   double *gradK = nullptr, *gradW = nullptr;
+  // SST outer loop (oa_flow_sst_iterate): turbulent viscosity, F1 blending,
+  // production and the previous-iteration k [nn]
+  double *mut = nullptr, *F1 = nullptr, *Pk = nullptr, *k_prev = nullptr;
   double urf_k = 1.0, urf_w = 1.0;
   // [ne][12] Rhie-Chow mass flux of each SCS ip with the pressure-correction
   // equation's upwind density (its right-hand side), written by the mass-flow

@@ -36,7 +36,7 @@ EXPORTS = [
     "oa_diffusion_field_device_ptr", "oa_diffusion_assemble", "oa_diffusion_solve", "oa_diffusion_step",
     "oa_diffusion_stream", "oa_diffusion_time_assembly", "oa_sst_default_constants", "oa_sst_node_update", "oa_sst_diffusivities",
     "oa_flow_last_control", "oa_flow_scales", "oa_flow_advance_time", "oa_flow_autotune", "oa_flow_set_tuning",
-    "oa_flow_enable_turbulence", "oa_flow_turbulence_systems", "oa_flow_solve_turbulence",
+    "oa_flow_enable_turbulence", "oa_flow_turbulence_systems", "oa_flow_solve_turbulence", "oa_flow_sst_iterate",
 ]
 
 OA_BND_FIXED_VALUE = 0
@@ -229,6 +229,8 @@ def lib():
         "oa_flow_enable_turbulence": (C.c_int, [vp, C.c_double, C.c_double]),
         "oa_flow_turbulence_systems": (C.c_int, [vp, dp, dp, dp, dp]),
         "oa_flow_solve_turbulence": (C.c_int, [vp, C.c_double, C.c_int, ip, ip]),
+        "oa_flow_sst_iterate": (C.c_int, [vp, C.c_int, P(SstConstants), vp, vp, vp, C.c_double, C.c_double,
+                                          C.c_int, vp]),
         "oa_flow_sync": (C.c_int, [vp]),
         "oa_flow_stream": (C.c_int, [vp, P(vp)]),
         "oa_launch_count": (C.c_int, [P(C.c_longlong)]),
@@ -324,7 +326,7 @@ class Flow:
     FIELD_SHAPES = {"U": 3, "p": 1, "gradU": 9, "gradP": 3, "du": 3, "div": 1, "sideU": 3, "rho": 1, "mu": 1,
                     "betaU": 3, "minU": 3, "maxU": 3, "duTilde": 3, "Uold": 3, "Uoldold": 3,
                     "k": 1, "omega": 1, "gammaK": 1, "gammaOmega": 1, "srcDiagK": 1, "srcRhsK": 1,
-                    "srcDiagOmega": 1, "srcRhsOmega": 1, "gradK": 3, "gradOmega": 3}
+                    "srcDiagOmega": 1, "srcRhsOmega": 1, "gradK": 3, "gradOmega": 3, "mut": 1, "F1": 1, "Pk": 1}
 
     def __init__(self, mesh: Mesh, settings: FlowSettings | None = None):
         self.mesh = mesh
@@ -428,6 +430,17 @@ class Flow:
         ik, iw = C.c_int(), C.c_int()
         _check(lib().oa_flow_solve_turbulence(self.h, float(rtol), int(maxit), C.byref(ik), C.byref(iw)))
         return ik.value, iw.value
+
+    def sst_iterate(self, n, ymin, wall_node, mu_lam, mut_urf=1.0, rtol=1e-8, maxit=500, constants=None):
+        """n outer iterations with the SST equations (oa_flow_sst_iterate);
+        ymin, wall_node, mu_lam are device pointers (ints). Returns the flow
+        stats of each iteration."""
+        st = (IterStats * max(n, 1))()
+        c = constants or sst_constants()
+        _check(lib().oa_flow_sst_iterate(self.h, int(n), C.byref(c), C.c_void_p(int(ymin)),
+                                         C.c_void_p(int(wall_node)), C.c_void_p(int(mu_lam)), float(mut_urf),
+                                         float(rtol), int(maxit), C.cast(st, C.c_void_p)))
+        return [dict(mom_iters=s.mom_iters, pc_iters=s.pc_iters, continuity_rms=s.continuity_rms) for s in st[:n]]
 
     def autotune(self, iters=3):
         """Tune launch shapes and the pressure-solve schedule; the flow state is

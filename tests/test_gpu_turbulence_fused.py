@@ -251,3 +251,64 @@ def test_sst_chain_on_device(oracle_mod):
     mu_eff, gk, gw = oracle_mod.sst_diffusivities(host["mu"], ref["mut"], ref["F1"])
     assert rel(gf.get_field("mu"), mu_eff) < 1e-12
     assert rel(gf.get_field("gammaK"), gk) < 1e-12 and rel(gf.get_field("gammaOmega"), gw) < 1e-12
+
+
+@pytest.mark.parametrize("graphs", [1, 2])
+def test_sst_iterate_driver_matches_its_steps(graphs):
+    # oa_flow_sst_iterate against the same sequence made of the public calls:
+    # k_prev = k, one SIMPLE iteration (fused assembly), the k / omega solves,
+    # their gradients, the node update and the diffusivities; bit for bit
+    import torch
+
+    m = meshgen.channel(12, 8, 6, ratio=1.1)
+    rng = np.random.default_rng(3)
+    k0 = 1e-3 * np.exp(0.2 * rng.standard_normal(m.nn))
+    w0 = 1e2 * np.exp(0.2 * rng.standard_normal(m.nn))
+    y = m.coords[:, 1]
+    dev = torch.device("cuda")
+    t = {"ymin": torch.from_numpy(np.minimum(y, 1.0 - y) + 1e-3).to(dev),
+         "wall": torch.from_numpy((np.isclose(y, 0.0) | np.isclose(y, 1.0)).astype(np.int32)).to(dev),
+         "mu": torch.full((m.nn,), 1e-3, dtype=torch.float64, device=dev)}
+    U0 = meshgen.initial_velocity(m, sigma=0.1, seed=3)
+    flows = []
+    for _ in range(2):
+        f = rt.Flow(rt.Mesh(m), rt.default_settings(use_graphs=graphs, mu=1e-3))
+        f.set_boundary_types([rt.OA_BTYPE_WALL, rt.OA_BTYPE_WALL, rt.OA_BTYPE_SYMMETRY])
+        f.set_field("U", U0)
+        f.initialize()
+        f.enable_turbulence(0.8, 0.8)
+        f.set_field("k", k0)
+        f.set_field("omega", w0)
+        f.set_field("gammaK", np.full(m.nn, 1e-3))
+        f.set_field("gammaOmega", np.full(m.nn, 1e-3))
+        flows.append(f)
+    a, b = flows
+    n = 3
+    a.sst_iterate(n, t["ymin"].data_ptr(), t["wall"].data_ptr(), t["mu"].data_ptr(), mut_urf=0.7, rtol=1e-10)
+    # the same steps by hand on the second flow
+    work = {nm: torch.zeros(m.nn, dtype=torch.float64, device=dev) for nm in ("mut", "F1", "Pk", "k_prev")}
+    vol = torch.from_numpy(b.mesh.dual_volume()).to(dev)
+    for _ in range(n):
+        torch.cuda.synchronize()
+        work["k_prev"].copy_(torch.from_numpy(b.get_field("k")).to(dev))
+        b.simple_iterate(1)
+        b.solve_turbulence(1e-10, 500)
+        b.update_gradient("k")
+        b.update_gradient("omega")
+        ptrs = {nm: v.data_ptr() for nm, v in work.items()}
+        ptrs.update(k=b.device_ptr("k"), omega=b.device_ptr("omega"), rho=b.device_ptr("rho"),
+                    mu=t["mu"].data_ptr(), ymin=t["ymin"].data_ptr(), gradU=b.device_ptr("gradU"),
+                    gradK=b.device_ptr("gradK"), gradW=b.device_ptr("gradOmega"), div=b.device_ptr("div"),
+                    vol=vol.data_ptr(), mut_old=work["mut"].data_ptr(),
+                    wall_node=t["wall"].data_ptr(), k_diag=b.device_ptr("srcDiagK"), k_rhs=b.device_ptr("srcRhsK"),
+                    w_diag=b.device_ptr("srcDiagOmega"), w_rhs=b.device_ptr("srcRhsOmega"))
+        rt.sst_node_update(m.nn, ptrs, dt=rt.default_settings().dt, mut_urf=0.7, stream=b.stream_handle())
+        rt.sst_diffusivities(m.nn, t["mu"].data_ptr(), work["mut"].data_ptr(), work["F1"].data_ptr(),
+                             b.device_ptr("mu"), b.device_ptr("gammaK"), b.device_ptr("gammaOmega"),
+                             stream=b.stream_handle())
+        b.sync()
+    for name in ("U", "p", "k", "omega", "mu", "gammaK", "gammaOmega", "srcRhsK", "srcRhsOmega"):
+        np.testing.assert_array_equal(a.get_field(name), b.get_field(name), err_msg=name)
+    np.testing.assert_array_equal(a.get_field("mut"), work["mut"].cpu().numpy())
+    assert np.all(a.get_field("k") > 0) and np.all(a.get_field("omega") > 0)
+    assert np.all(np.isfinite(a.get_field("U"))) and a.get_field("mut").max() > 0
