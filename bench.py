@@ -547,7 +547,8 @@ def run_channel(args, rank, world):
     for the channel's inlet/outlet conditions), mu = 1e-5, k0 = 1e-3 LN(0.2), omega0 = 1e2
     LN(0.2) seeded, diffusivities mu + sigma mu_t with mu_t = rho k / omega and
     the SST inner-layer sigmas. A step is one assembly launch of all five
-    equations; the momentum-only launch is timed beside it."""
+    equations; the momentum-only launch is timed beside it, and whole outer
+    iterations with the SST equations (oa_flow_sst_iterate) are reported."""
     import torch
 
     from openaccel_b200 import meshgen
@@ -579,6 +580,28 @@ def run_channel(args, rank, world):
             t_fused = f.time_kernel("momentum", reps=args.steps)
         out[name] = {"ms_fused": t_fused, "ms_momentum_only": t_plain, "launches": rt.launch_count() - l0,
                      "clocks": clk.summary()}
+        # whole outer iterations with the SST equations (oa_flow_sst_iterate:
+        # flow iteration with the fused launch, k/omega solves, gradients,
+        # node update, diffusivities), CUDA events on the flow's stream
+        y = m.coords[:, 1]
+        sst_in = {"ymin": torch.from_numpy(np.minimum(y, 1.0 - y) + 1e-4).to(dev),
+                  "wall": torch.from_numpy((np.isclose(y, 0.0) | np.isclose(y, 1.0)).astype(np.int32)).to(dev),
+                  "mu": torch.full((m.nn,), mu, dtype=torch.float64, device=dev)}
+        sst_args = (sst_in["ymin"].data_ptr(), sst_in["wall"].data_ptr(), sst_in["mu"].data_ptr())
+        try:
+            f.sst_iterate(1, *sst_args, mut_urf=0.7, rtol=1e-6)
+            stream = torch.cuda.ExternalStream(f.stream_handle(), device=dev)
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            n_sst = 3
+            e0.record(stream)
+            sst_stats = f.sst_iterate(n_sst, *sst_args, mut_urf=0.7, rtol=1e-6)
+            e1.record(stream)
+            e1.synchronize()
+            out[name]["sst_outer_iteration_ms"] = e0.elapsed_time(e1) / n_sst
+            out[name]["sst_pc_iters"] = [st["pc_iters"] for st in sst_stats]
+        except rt.OpenAccelError as exc:
+            out[name]["sst_outer_iteration_error"] = str(exc)
         f.close()
     ms = max_over_ranks(out["mixed"]["ms_fused"], dev, world)
     ne, nn, nnz = m.ne, m.nn, gm.nnz

@@ -24,12 +24,57 @@ __global__ void k_narrow(int n, const double* __restrict__ a, float* __restrict_
 
 // ---- graph form: the host decisions of solve() as one-thread kernels ----
 
+// Largest relative change of the diagonal since the last numeric refresh,
+// max_i |a_ii / ref_i - 1|, into *out (zeroed before) as the bits of a
+// non-negative double, whose integer order is the numeric one.
+template <class T>
+__global__ void k_diag_drift(int n, const int* __restrict__ rp, const int* __restrict__ dg, const T* __restrict__ A,
+                             const double* __restrict__ ref, unsigned long long* out) {
+  double m = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double d = double(A[rp[i] + dg[i]]), r = ref[i];
+    const double c = r != 0.0 ? fabs(d / r - 1.0) : (d != 0.0 ? INFINITY : 0.0);
+    m = fmax(m, c);
+  }
+  for (int o = 16; o; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(out, (unsigned long long)__double_as_longlong(m));
+}
+
+// the diagonal the next drift test compares against
+template <class T>
+__global__ void k_diag_store(int n, const int* __restrict__ rp, const int* __restrict__ dg, const T* __restrict__ A,
+                             double* __restrict__ ref) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) ref[i] = double(A[rp[i] + dg[i]]);
+}
+
 // AMG numeric phase on every refresh-th solve (the counter persists across
-// graph launches)
-__global__ void k_refresh_if(cudaGraphConditionalHandle h, ScalarGraphState* S, int refresh) {
-  const int go = refresh <= 1 || (S->refresh_ctr % refresh) == 0;
+// graph launches) and on any solve whose matrix drifted
+__global__ void k_refresh_if(cudaGraphConditionalHandle h, ScalarGraphState* S, int refresh,
+                             const unsigned long long* drift, double drift_max) {
+  const double dr = __longlong_as_double((long long)*drift);
+  const int go = refresh <= 1 || (S->refresh_ctr % refresh) == 0 || dr > drift_max;
   S->refresh_ctr += 1;
   cudaGraphSetConditional(h, go ? 1u : 0u);
+}
+
+constexpr int DRIFT_BLOCKS = 4 * 148;
+
+template <class T>
+int launch_drift(const ScalarGraph& g, const void* A, const double* ref, unsigned long long* drift, cudaStream_t st) {
+  OA_CUDA(cudaMemsetAsync(drift, 0, sizeof(unsigned long long), st));
+  k_diag_drift<T><<<DRIFT_BLOCKS, 256, 0, st>>>(g.nn, g.rp, g.diag, static_cast<const T*>(A), ref, drift);
+  count_launches(1);
+  OA_CUDA(cudaGetLastError());
+  return OA_OK;
+}
+
+template <class T>
+int launch_store(const ScalarGraph& g, const void* A, double* ref, cudaStream_t st) {
+  k_diag_store<T><<<(g.nn + 255) / 256, 256, 0, st>>>(g.nn, g.rp, g.diag, static_cast<const T*>(A), ref);
+  count_launches(1);
+  OA_CUDA(cudaGetLastError());
+  return OA_OK;
 }
 
 // FP64: a GCR(2) solve that stagnated or broke down is redone by BiCGStab
@@ -107,6 +152,7 @@ __global__ void k_ir_next(cudaGraphConditionalHandle h, ScalarGraphState* S, Bod
 
 int ScalarSolve::init(int nn) {
   if (const char* e = std::getenv("OA_AMG_REFRESH")) refresh = std::max(1, std::atoi(e));
+  if (const char* e = std::getenv("OA_AMG_DRIFT")) drift_max = std::atof(e);
   if (const char* e = std::getenv("OA_IR_INNER")) inner_floor = std::atof(e);
   if (const char* e = std::getenv("OA_KRYLOV")) gcr = std::strcmp(e, "bicgstab") != 0;
   if (const char* e = std::getenv("OA_GCR_CHUNK")) gcr_chunk = std::max(2, std::atoi(e) / 2 * 2);
@@ -117,6 +163,9 @@ int ScalarSolve::init(int nn) {
       cudaMalloc(&r32, sizeof(float) * (nn ? nn : 1)) != cudaSuccess ||
       cudaMalloc(&scal, sizeof(double) * 2) != cudaSuccess ||
       cudaMalloc(&partials, sizeof(double) * partials_size()) != cudaSuccess ||
+      cudaMalloc(&diag_ref, sizeof(double) * (nn ? nn : 1)) != cudaSuccess ||
+      cudaMalloc(&drift, sizeof(unsigned long long)) != cudaSuccess ||
+      cudaMallocHost(&hdrift, sizeof(unsigned long long)) != cudaSuccess ||
       cudaMallocHost(&hscal, sizeof(double) * 2) != cudaSuccess) {
     release();
     return fail(OA_ERR_CUDA, "scalar solve: device allocation failed");
@@ -166,6 +215,12 @@ void ScalarSolve::release() {
   gs = nullptr;
   gs_host = nullptr;
   k_host = nullptr;
+  if (diag_ref) cudaFree(diag_ref);
+  if (drift) cudaFree(drift);
+  if (hdrift) cudaFreeHost(hdrift);
+  diag_ref = nullptr;
+  drift = nullptr;
+  hdrift = nullptr;
   if (r) cudaFree(r);
   if (r32) cudaFree(r32);
   if (scal) cudaFree(scal);
@@ -206,7 +261,19 @@ int ScalarSolve::solve(const ScalarGraph& g, bool mixed, bool amg, bool graphs, 
   int check_every = amg ? (gcr ? gcr_chunk : 5) : 20;
   // AMG numeric phase every refresh-th solve (the fine matrix is always the
   // current one; the coarse operators may lag by refresh - 1 assemblies)
-  const bool reuse = amg && refresh > 1 && (solves++ % refresh) != 0;
+  bool reuse = amg && refresh > 1 && (solves++ % refresh) != 0;
+  if (reuse) {
+    // a matrix that drifted from the hierarchy's refreshes it early
+    if (int s = mixed ? launch_drift<float>(g, A, diag_ref, drift, st) : launch_drift<double>(g, A, diag_ref, drift, st))
+      return s;
+    OA_CUDA(cudaMemcpyAsync(hdrift, drift, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+    OA_CUDA(cudaStreamSynchronize(st));
+    double dr;
+    std::memcpy(&dr, hdrift, sizeof(double));
+    if (dr > drift_max) reuse = false;
+  }
+  if (amg && !reuse)
+    if (int s = mixed ? launch_store<float>(g, A, diag_ref, st) : launch_store<double>(g, A, diag_ref, st)) return s;
   if (!mixed) {
     if (int s = k64.setup(g.nn, g.rp, g.cols, g.diag, st)) return s;
     double* xs = nullptr;
@@ -316,7 +383,11 @@ int ScalarSolve::emit(GraphBuild& gb, cudaGraph_t g, Deps& d, const ScalarGraph&
     cudaGraphConditionalHandle hn;
     if (int s = gb.handle(g, &hn)) return s;
     if (int s = gb.seg(g, d, -1, [&]() -> int {
-          k_refresh_if<<<1, 1, 0, st>>>(hn, gs, refresh);
+          if (refresh > 1)
+            if (int s2 = mixed ? launch_drift<float>(gr, A, diag_ref, drift, st)
+                               : launch_drift<double>(gr, A, diag_ref, drift, st))
+              return s2;
+          k_refresh_if<<<1, 1, 0, st>>>(hn, gs, refresh, drift, refresh > 1 ? drift_max : INFINITY);
           count_launches(1);
           return OA_OK;
         }))
@@ -328,6 +399,8 @@ int ScalarSolve::emit(GraphBuild& gb, cudaGraph_t g, Deps& d, const ScalarGraph&
     Deps nd;
     if (int s = gb.seg(nb, nd, bid, [&]() -> int {
           if (int s2 = launch_count_body(gb, bid)) return s2;
+          if (int s2 = mixed ? launch_store<float>(gr, A, diag_ref, st) : launch_store<double>(gr, A, diag_ref, st))
+            return s2;
           return mixed ? amg32.numeric(static_cast<const float*>(A), st)
                        : amg64.numeric(static_cast<const double*>(A), st);
         }))

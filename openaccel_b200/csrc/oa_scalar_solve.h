@@ -51,6 +51,16 @@ struct ScalarSolve {
   // iteration; with GCR(2) 8 still keeps them (22 per outer iteration) and
   // saves another 2 % (OA_AMG_REFRESH overrides)
   int refresh = 8;
+  // ...and earlier when the matrix has drifted: a solve refreshes whenever
+  // some diagonal entry moved by more than drift_max (relative) since the last
+  // refresh. A hierarchy left from a much different matrix can make the
+  // Chebyshev smoother diverge: on a 64 x 24 x 24 channel at mu = 1e-5 the
+  // pressure solve of the second outer iteration hit maxit with refresh 8 and
+  // took 13 iterations with a refresh on every solve (OA_AMG_DRIFT overrides).
+  double drift_max = 0.5;
+  double* diag_ref = nullptr;           // [n] FP64 diagonal at the last refresh
+  unsigned long long* drift = nullptr;  // device: largest relative change (double bits)
+  unsigned long long* hdrift = nullptr; // pinned mirror
   // lowest relative tolerance asked of an FP32 inner solve (0: the default of
   // floor_default); OA_IR_INNER overrides
   double inner_floor = 0.0;

@@ -100,16 +100,19 @@ def test_static_solve_reports_non_convergence():
     assert st == OA_ERR_SOLVER
 
 
-def test_gcr_stagnation_falls_back_to_bicgstab():
+def test_gcr_stagnation_falls_back_to_bicgstab(monkeypatch):
     """GCR(2) truncated to two directions can stagnate when the symmetric part
     of A M^-1 is not definite. Two random pressure-correction systems (random
     DU, mass flows and pressure on a skewed 12^3 cavity) solved back to back,
     the second with the AMG hierarchy the first one built (the numeric phase is
-    refreshed every eighth solve), make it stagnate: the solve must switch to
-    BiCGStab, say so in its ControlData, count the GCR iterations it spent, and
-    still reach the direct solution."""
+    refreshed every eighth solve, and the drift test that would refresh it for
+    so different a matrix is switched off), make it stagnate: the solve must
+    switch to BiCGStab, say so in its ControlData, count the GCR iterations it
+    spent, and still reach the direct solution."""
     import scipy.sparse as sp
     import scipy.sparse.linalg as spl
+
+    monkeypatch.setenv("OA_AMG_DRIFT", "1e300")
 
     m = meshgen.cavity(12, perturb=0.2, seed=21)
     gm = rt.Mesh(m)
