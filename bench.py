@@ -600,6 +600,11 @@ def run_channel(args, rank, world):
             e1.synchronize()
             out[name]["sst_outer_iteration_ms"] = e0.elapsed_time(e1) / n_sst
             out[name]["sst_pc_iters"] = [st["pc_iters"] for st in sst_stats]
+            # the flow's phases inside it (event nodes); the rest is the k / omega
+            # solves and corrections, their gradients, the node update and the
+            # diffusivities
+            phases = {k[3:]: sum(st[k] for st in sst_stats) / n_sst for k in rt.PHASES}
+            out[name]["sst_phase_ms"] = dict(phases, turbulence=out[name]["sst_outer_iteration_ms"] - sum(phases.values()))
         except rt.OpenAccelError as exc:
             out[name]["sst_outer_iteration_error"] = str(exc)
         f.close()

@@ -440,7 +440,8 @@ class Flow:
         _check(lib().oa_flow_sst_iterate(self.h, int(n), C.byref(c), C.c_void_p(int(ymin)),
                                          C.c_void_p(int(wall_node)), C.c_void_p(int(mu_lam)), float(mut_urf),
                                          float(rtol), int(maxit), C.cast(st, C.c_void_p)))
-        return [dict(mom_iters=s.mom_iters, pc_iters=s.pc_iters, continuity_rms=s.continuity_rms) for s in st[:n]]
+        return [dict(mom_iters=s.mom_iters, pc_iters=s.pc_iters, continuity_rms=s.continuity_rms,
+                     **{k: getattr(s, k) for k in PHASES}) for s in st[:n]]
 
     def autotune(self, iters=3):
         """Tune launch shapes and the pressure-solve schedule; the flow state is
