@@ -265,18 +265,22 @@ __global__ void k_dense_fill(int n, const int* __restrict__ rp, const int* __res
 
 // Gauss-Jordan elimination without pivoting (the coarse Galerkin operators of
 // the grounded Rhie-Chow Laplacian are M-matrices), one block; leaves A^-1 in
-// the right half.
+// the right half. At step k the pivot row is zero left of column k (earlier
+// steps cleared it) and right of column n + k (the identity's later columns
+// are still untouched there), so only its n + 1 columns k .. n + k are
+// normalised and used: the skipped updates would subtract exact zeros.
 __global__ void k_gauss_jordan(int n, double* M) {
   const int w = 2 * n;
   for (int k = 0; k < n; ++k) {
     __syncthreads();
     const double piv = M[(size_t)k * w + k];
     __syncthreads();
-    for (int j = threadIdx.x; j < w; j += blockDim.x) M[(size_t)k * w + j] /= piv;
+    for (int j = k + threadIdx.x; j <= n + k; j += blockDim.x) M[(size_t)k * w + j] /= piv;
     __syncthreads();
-    for (int idx = threadIdx.x; idx < n * w; idx += blockDim.x) {
-      const int i = idx / w, j = idx - i * w;
-      if (i == k || j == k) continue;
+    // columns k + 1 .. n + k of every other row (n of them)
+    for (int idx = threadIdx.x; idx < n * n; idx += blockDim.x) {
+      const int i = idx / n, j = k + 1 + (idx - i * n);
+      if (i == k) continue;
       M[(size_t)i * w + j] -= M[(size_t)i * w + k] * M[(size_t)k * w + j];
     }
     __syncthreads();
