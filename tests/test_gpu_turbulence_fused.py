@@ -312,3 +312,88 @@ def test_sst_iterate_driver_matches_its_steps(graphs):
     np.testing.assert_array_equal(a.get_field("mut"), work["mut"].cpu().numpy())
     assert np.all(a.get_field("k") > 0) and np.all(a.get_field("omega") > 0)
     assert np.all(np.isfinite(a.get_field("U"))) and a.get_field("mut").max() > 0
+
+
+def test_sst_iterate_against_the_oracle(oracle_mod):
+    # two SST outer iterations of the driver against the oracle composed the
+    # same way: k.prevIter = k; the k / omega systems from the node terms of the
+    # previous update on the iteration's starting mass flows; the SIMPLE
+    # iteration; tight k / omega solves with the lower clip; gradients; node
+    # update with relaxed mu_t; mu_eff and the diffusivities
+    import torch
+
+    kw = dict(mom_rtol=1e-13, pc_rtol=1e-13, mom_maxit=500, pc_maxit=5000, mu=1e-3)
+    m = meshgen.channel(10, 8, 6, ratio=1.1)
+    types = [rt.OA_BTYPE_WALL, rt.OA_BTYPE_WALL, rt.OA_BTYPE_SYMMETRY]
+    rng = np.random.default_rng(8)
+    k = 1e-3 * np.exp(0.2 * rng.standard_normal(m.nn))
+    w = 1e2 * np.exp(0.2 * rng.standard_normal(m.nn))
+    y = m.coords[:, 1]
+    ymin = np.minimum(y, 1.0 - y) + 1e-3
+    wall = (np.isclose(y, 0.0) | np.isclose(y, 1.0)).astype(np.int32)
+    mu_lam = np.full(m.nn, 1e-3)
+    U0 = meshgen.initial_velocity(m, sigma=0.1, seed=8)
+    urf_k, urf_w, mut_urf, small = 0.8, 0.7, 0.7, np.finfo(float).eps
+
+    oc = oracle_mod.FlowCase(m, oracle_mod.default_settings(**kw), U0=U0)
+    oc.set_boundary_types(types)
+    oc.initialize()
+    gf = rt.Flow(rt.Mesh(m), rt.default_settings(**kw))
+    gf.set_boundary_types(types)
+    gf.set_field("U", U0)
+    gf.initialize()
+    gf.enable_turbulence(urf_k, urf_w)
+    state = {"k": k.copy(), "omega": w.copy(), "gammaK": mu_lam.copy(), "gammaOmega": mu_lam.copy(),
+             "srcDiagK": np.zeros(m.nn), "srcRhsK": np.zeros(m.nn), "srcDiagOmega": np.zeros(m.nn),
+             "srcRhsOmega": np.zeros(m.nn), "mut": np.zeros(m.nn)}
+    for n in ("k", "omega", "gammaK", "gammaOmega"):
+        gf.set_field(n, state[n])
+    dev = torch.device("cuda")
+    t = {"ymin": torch.from_numpy(ymin).to(dev), "wall": torch.from_numpy(wall).to(dev),
+         "mu": torch.from_numpy(mu_lam).to(dev)}
+    vol = oc.field("vol").copy()
+
+    def grad(phi):
+        p, gp = oc.field("p").copy(), oc.field("gradP").copy()
+        oc.field("p")[:] = phi
+        oc.field("gradP")[:] = 0.0
+        oc.update_grad_p()
+        g = oc.field("gradP").copy()
+        oc.field("p")[:], oc.field("gradP")[:] = p, gp
+        return g
+
+    gk, gw = np.zeros(3 * m.nn), np.zeros(3 * m.nn)
+    for _ in range(2):
+        k_prev = state["k"].copy()
+        Ak, bk = oc.assemble_transport(state["k"], state["gammaK"], state["srcDiagK"], state["srcRhsK"], urf_k)
+        Aw, bw = oc.assemble_transport(state["omega"], state["gammaOmega"], state["srcDiagOmega"],
+                                       state["srcRhsOmega"], urf_w)
+        oc.simple_iteration()
+        for name, A, b in (("k", Ak, bk), ("omega", Aw, bw)):
+            x, _, _ = oc.bicgstab(1, A, b, rtol=1e-13, maxit=5000)
+            old = state[name]
+            new = old + x
+            low = new < small
+            new[low] = old[low] + (small - old[low])
+            state[name] = new
+        # the gradients relax against their previous values (grad() starts from
+        # zero, so it returns the new part, g times the fresh gradient)
+        g = oracle_mod.default_settings().grad_urf
+        gk = (1.0 - g) * gk + grad(state["k"])
+        gw = (1.0 - g) * gw + grad(state["omega"])
+        out = oracle_mod.sst_nodes(dict(k=state["k"], omega=state["omega"], k_prev=k_prev, rho=np.ones(m.nn),
+                                        mu=mu_lam, ymin=ymin, gradU=oc.field("gradU").copy(), gradK=gk, gradW=gw,
+                                        div=oc.field("div").copy(), vol=vol, mut_old=state["mut"], pk_wall=None,
+                                        wall_node=wall), dt=1.0, mut_urf=mut_urf)
+        state["mut"] = out["mut"]
+        state["srcDiagK"], state["srcRhsK"] = out["k_diag"], out["k_rhs"]
+        state["srcDiagOmega"], state["srcRhsOmega"] = out["w_diag"], out["w_rhs"]
+        mu_eff, state["gammaK"], state["gammaOmega"] = oracle_mod.sst_diffusivities(mu_lam, out["mut"], out["F1"])
+        oc.field("mu")[:] = mu_eff
+    gf.sst_iterate(2, t["ymin"].data_ptr(), t["wall"].data_ptr(), t["mu"].data_ptr(), mut_urf=mut_urf, rtol=1e-12,
+                   maxit=5000)
+    for name in ("k", "omega", "gammaK", "gammaOmega", "mut", "srcRhsK", "srcRhsOmega"):
+        assert rel(gf.get_field(name), state[name]) < 1e-9, name
+    assert rel(gf.get_field("mu"), oc.field("mu")) < 1e-9
+    for name in ("U", "p", "mDot"):
+        assert rel(gf.get_field(name), oc.field(name)) < 1e-9, name
