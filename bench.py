@@ -565,7 +565,8 @@ def run_channel(args, rank, world):
     gm = rt.Mesh(m)
     out = {}
     for prec, name in ((rt.OA_PREC_MIXED, "mixed"), (rt.OA_PREC_FP64, "fp64")):
-        f = rt.Flow(gm, rt.default_settings(precision=prec))
+        f = rt.Flow(gm, rt.default_settings(precision=prec, pc_rtol=args.pc_rtol, mom_rtol=args.mom_rtol,
+                                            mom_maxit=args.mom_maxit))
         f.set_boundary_types([rt.OA_BTYPE_WALL, rt.OA_BTYPE_WALL, rt.OA_BTYPE_SYMMETRY])
         f.set_field("U", U0)
         f.set_field("mu", np.full(m.nn, mu))
@@ -622,7 +623,8 @@ def run_channel(args, rank, world):
         "dtype": "f32+f64", "data": "synthetic",
         "config": {"workload": "channel 256x96x96 hex8, wall-normal stretching 1.05, mu 1e-5, k/omega lognormal",
                    "elements": ne, "nodes": nn, "nnz": nnz, "l2": "inputs larger than L2 (no flush)",
-                   "boundaries": "no-slip y walls, symmetry z planes, x planes no-slip (inlet/outlet not modelled)"},
+                   "boundaries": "no-slip y walls, symmetry z planes, x planes no-slip (inlet/outlet not modelled)",
+                   "pc_rtol": args.pc_rtol, "mom_rtol": args.mom_rtol, "mom_maxit": args.mom_maxit},
         "fused": out,
         "fused_over_momentum_only": {p: out[p]["ms_fused"] / out[p]["ms_momentum_only"] for p in out},
         "roofline": {"bound": "hbm", "kernel": "k_momentum (fused u/v/w/k/omega, mixed)", "achieved": alg / ms / 1e6,
