@@ -102,6 +102,13 @@ def test_static_solve_matches_regular_solve_twice(n):
     assert host_residual(rp, cols, A2, b2, x2) < 1e-11
     assert rel(x2, x2_ref) < X_TOL
     assert rel(x2, x1) > 1e-3  # genuinely a different system
+    if m.nn <= 20000:
+        # and against a direct solve on the host, independent of the library's solvers
+        import scipy.sparse as sp
+        import scipy.sparse.linalg as spl
+
+        xd = spl.spsolve(sp.csr_matrix((A2, cols, rp), shape=(m.nn, m.nn)).tocsc(), b2)
+        assert rel(x2, xd) < 1e-9
 
 
 def test_static_solve_rejects_oversized_system():
