@@ -38,6 +38,13 @@ def test_version_and_argument_errors_without_gpu():
     assert st == 1
     assert b"bad arguments" in L.oa_last_error()
     assert L.oa_flow_sync(None) == 1
+    # the boundary-type, SST driver and diffusivity entry points check their
+    # arguments before touching a device
+    assert L.oa_flow_set_boundary_types(None, None, 0, 0) == 1
+    c = runtime.SstConstants()
+    assert L.oa_flow_sst_iterate(None, 1, C.byref(c), None, None, None, 1.0, 1e-8, 10, None) == 1
+    assert L.oa_sst_diffusivities(-1, C.byref(c), None, None, None, None, None, None, None) == 1
+    assert L.oa_update_gradient(None, 2) == 1
 
 
 def test_meshgen_conventions():
