@@ -143,7 +143,8 @@ int oa_mesh_graph(const oa_mesh* m, int* row_ptr, int* cols);
 int oa_mesh_dual_volume(const oa_mesh* m, double* vol);
 
 /* Flow state: replaces the fieldBroker/flowModel fields U, p, mDot, du, grad U,
- * grad p, div (src/realm/fieldBroker.cpp) for one domain of no-slip walls.
+ * grad p, div (src/realm/fieldBroker.cpp) for one domain whose boundaries are
+ * no-slip walls (oa_flow_set_boundary_types may make some symmetry planes).
  * bnd_velocity[nbnd][3] are the wall velocities by boundary index. */
 int oa_flow_create(oa_mesh* m, const oa_flow_settings* s, const double* bnd_velocity, int nbnd,
                    oa_flow** out);
