@@ -86,7 +86,8 @@ void orc_case_graph(void* h, int* row_ptr /*nn+1*/, int* cols /*nnz*/);
 /* initialisation: mDot from U, gradients, divergence */
 void orc_initialize(void* h);
 /* assembled momentum system (BSR 3x3, row-major blocks) incl. node terms,
- * interior, no-slip walls, relaxation; also updates du */
+ * interior, no-slip walls, symmetry planes (face terms, rhs projection and
+ * normal relaxation), relaxation; also updates du */
 void orc_assemble_momentum(void* h, double* A, double* b);
 /* pressure-correction system incl. reference-pressure row */
 void orc_assemble_pcorr(void* h, double* A, double* b);
